@@ -1,0 +1,179 @@
+/*
+ * ncpa_gpu.h -- C ABI of the B200 effective-sound-speed normal-mode library
+ * (Modess / ModBB hot path of ncpaprop).
+ *
+ * Plain C types only: status codes are returned (never thrown), the library
+ * owns device memory, the caller owns every host buffer it passes.  One
+ * context per host thread; a context owns one CUDA stream on one device.
+ *
+ * The reference exposes this path as C++ virtual classes (no C ABI); each
+ * entry point below names the reference interface whose work it replaces.
+ */
+#ifndef NCPA_GPU_H
+#define NCPA_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    NCPA_OK = 0,
+    NCPA_EINVAL = 1,    /* bad argument (message via ncpa_last_error) */
+    NCPA_ENOMEM = 2,    /* device or host allocation failed */
+    NCPA_ECUDA = 3,     /* CUDA runtime error */
+    NCPA_EPARSE = 4,    /* malformed profile / dispersion / source file */
+    NCPA_ETOOMANY = 5,  /* more modes than ncpa_ess_params.max_modes */
+    NCPA_EIO = 6,       /* file could not be opened */
+    NCPA_ETIMEDOUT = 7, /* a bounded device wait gave up */
+    NCPA_ENODEV = 8     /* no CUDA device or the kernels are missing */
+} ncpa_status;
+
+typedef struct ncpa_ctx ncpa_ctx;
+typedef struct ncpa_profile ncpa_profile;
+typedef struct ncpa_modes ncpa_modes;
+
+typedef struct {
+    int device; /* CUDA device ordinal */
+} ncpa_ctx_opts;
+
+/* Context: device, stream, last-error text. */
+ncpa_status ncpa_ctx_create(ncpa_ctx **ctx, const ncpa_ctx_opts *opts);
+ncpa_status ncpa_ctx_destroy(ncpa_ctx *ctx);
+const char *ncpa_status_str(ncpa_status s);
+const char *ncpa_last_error(const ncpa_ctx *ctx);
+ncpa_status ncpa_ctx_synchronize(ncpa_ctx *ctx);
+
+/* ------------------------------------------------------------------------
+ * Atmospheric profile (replaces NCPA::Atmosphere1D(file, header),
+ * src/atmosphere/Atmosphere1D.cpp:44-60, 85-285, plus the derived
+ * properties ESSModeSolver::setParams adds, ESSModeSolver.cpp:159-228).
+ * Knot arrays are SI: z [m], u v [m/s], t [K], p [Pa], rho [kg/m^3],
+ * c0 [m/s] (optional), attn [Np/m] (optional user attenuation at the knots,
+ * replaces --use_attn_file).  The profile is resident in HBM until destroyed.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    int n_knots;
+    const double *z, *u, *v, *t, *p, *rho;
+    const double *c0;   /* NULL: computed from p and rho as the reference does */
+    const double *attn; /* NULL: Sutherland-Bass at each solve frequency */
+    double z0_m;        /* ground height scalar Z0 of the profile file */
+    int has_z0;
+} ncpa_profile_desc;
+
+ncpa_status ncpa_profile_create(ncpa_ctx *ctx, const ncpa_profile_desc *desc, ncpa_profile **out);
+/* Parse an NCPA profile file ("#% col, KEY, units[, value]" header, optional
+ * separate header file) and upload it. */
+ncpa_status ncpa_profile_load(ncpa_ctx *ctx, const char *path, const char *header_path,
+                              ncpa_profile **out);
+ncpa_status ncpa_profile_destroy(ncpa_profile *prof);
+/* Number of knots and the altitude range [m] of a loaded profile. */
+ncpa_status ncpa_profile_info(const ncpa_profile *prof, int *n_knots, double *z_lo, double *z_hi);
+
+/* ------------------------------------------------------------------------
+ * Batched ESS eigen-solve over (frequency x azimuth) problems
+ * (replaces ESSModeSolver::solve loop body: getModalTrace, getNumberOfModes,
+ * EigenEngine::doESSCalculation, doSelect, doPerturb -- ESSModeSolver.cpp:
+ * 320-383, 518-665; EigenEngine.cpp:10-172; ModeSolver.cpp:223-284).
+ * Problem index p = f_index * n_az + az_index.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    int nz_grid;              /* --Nz_grid            [20000] */
+    double maxheight_km;      /* --maxheight_km       [150]   */
+    double zground_km;        /* --zground_km         [0]     */
+    double sourceheight_km;   /* --sourceheight_km    [0]     */
+    double receiverheight_km; /* --receiverheight_km  [0]     */
+    int lamb_wave_bc;         /* --Lamb_wave_BC               */
+    int turnoff_wkb;          /* --turnoff_WKB (or implied by write flags) */
+    int wvnum_filter;         /* --wvnum_filter with c_min, c_max [m/s] */
+    double c_min, c_max;
+    int want_group_speed;     /* compute group speeds (speeds.nm) */
+    int want_vectors;         /* keep full eigenvectors (modes, 2-D TL, starter) */
+    int max_modes;            /* per problem; 0 -> 4000 (reference MAX_MODES) */
+} ncpa_ess_params;
+
+void ncpa_ess_params_default(ncpa_ess_params *p);
+
+ncpa_status ncpa_ess_solve(ncpa_ctx *ctx, const ncpa_profile *prof, const ncpa_ess_params *params,
+                           const double *freqs, int n_freq, const double *az_deg, int n_az,
+                           ncpa_modes **out);
+ncpa_status ncpa_modes_destroy(ncpa_modes *modes);
+ncpa_status ncpa_modes_problems(const ncpa_modes *modes, int *n_problems);
+ncpa_status ncpa_modes_count(const ncpa_modes *modes, int problem, int *n_modes);
+/* scalars of one problem: grid spacing dz [m], window, densities at the
+ * source / receiver grid points, grid indices of source / receiver */
+ncpa_status ncpa_modes_info(const ncpa_modes *modes, int problem, double *freq, double *az,
+                            double *dz, double *k_min, double *k_max, double *rho_src,
+                            double *rho_rcv);
+/* modes of one problem in ascending Re k: k_pert = re_k + i im_k, mode values
+ * at source and receiver (normalised so sum v^2 dz = 1), group speed [m/s]
+ * (NULL to skip; zero unless want_group_speed). */
+ncpa_status ncpa_modes_get(const ncpa_modes *modes, int problem, double *re_k, double *im_k,
+                           double *v_src, double *v_rcv, double *v_group);
+/* full eigenvectors of one problem, layout [z_index * M + mode]
+ * (needs want_vectors) */
+ncpa_status ncpa_modes_get_vectors(const ncpa_modes *modes, int problem, double *v);
+
+/* ------------------------------------------------------------------------
+ * Transmission loss modal sums (ModeSolver::getTLoss1D / getTLoss1DNx2 /
+ * getTLoss2D, ModeSolver.cpp:292-565).  Ranges are (i+1)*dr_m, i < n_ranges.
+ * Outputs carry the reference's 1000 * 4 pi scaling (levels re 1 m).
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    int n_ranges;
+    double dr_m;
+    int lossless; /* use Re k only (tloss_*.lossless.nm) */
+} ncpa_tl_params;
+
+/* all problems at once: re/im/incoh are [n_problems x n_ranges] */
+ncpa_status ncpa_tl_1d(ncpa_ctx *ctx, const ncpa_modes *modes, const ncpa_tl_params *tp,
+                       double *re, double *im, double *incoh);
+/* one problem on the reference's height sampling (every nz/500-th grid
+ * point); heights [m] in z_out (n_heights entries), re/im [n_ranges x n_heights] */
+ncpa_status ncpa_tl_2d_heights(const ncpa_modes *modes, int problem, int *n_heights);
+ncpa_status ncpa_tl_2d(ncpa_ctx *ctx, const ncpa_modes *modes, int problem, const ncpa_tl_params *tp,
+                       double *z_out, double *re, double *im);
+
+/* ------------------------------------------------------------------------
+ * ModBB pulse synthesis (ModalBroadbandPropagator::calculate_waveform and
+ * BroadbandPropagator::fft_pulse_prop, ModalBroadbandPropagator.cpp:141-277,
+ * BroadbandPropagator.cpp:573-662).
+ * Dispersion arrays: n_freq entries of f (f[0] = 0, the DC slot),
+ * mode_off[n_freq+1] CSR offsets into re_k/im_k/v_src/v_rcv.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    int n_freq;
+    const double *f;
+    const int *mode_off;
+    const double *re_k, *im_k, *v_src, *v_rcv;
+    double rho_src, rho_rcv;
+} ncpa_dispersion_desc;
+
+typedef struct {
+    int n_ranges;
+    const double *ranges_m;
+    double max_celerity;  /* t0 = r / max_celerity */
+    int nfft;
+    const double *src_re; /* source spectrum at the n_freq dispersion bins */
+    const double *src_im;
+    int zero_attn;        /* set Im k = 0 */
+} ncpa_bb_params;
+
+/* waveforms: [n_ranges x nfft], 2 Re p(t) at t = i/(nfft df) + t0 */
+ncpa_status ncpa_bb_synthesize(ncpa_ctx *ctx, const ncpa_dispersion_desc *disp,
+                               const ncpa_bb_params *bp, double *waveforms);
+/* same, taking the dispersion of a device-resident batched solve (one
+ * azimuth; frequencies must be uniformly spaced from df): no host round trip */
+ncpa_status ncpa_bb_synthesize_modes(ncpa_ctx *ctx, const ncpa_modes *modes, int az_index,
+                                     const ncpa_bb_params *bp, double *waveforms);
+/* source spectrum of a sampled waveform: sum_n x_n exp(+2 pi i k n / nfft) dt
+ * for k < n_freq (BroadbandPropagator.cpp:327-353) */
+ncpa_status ncpa_source_spectrum_waveform(ncpa_ctx *ctx, const double *x, int n_samples, double dt,
+                                          int nfft, int n_freq, double *s_re, double *s_im);
+
+/* Number of this library's kernels launched on the context so far. */
+long long ncpa_kernel_launches(const ncpa_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,181 @@
+// Device helpers shared by the sm_100a kernels of the ESS normal-mode path.
+//
+// Arithmetic conventions: the library is compiled with --fmad=false, so a
+// fused multiply-add appears only where fma() is written.  The CPU oracle
+// (oracle/ncpa_oracle.c, compiled with -ffp-contract=off) performs the same
+// operations, which makes the profile sampling, matrix build and Sturm counts
+// reproducible bit-for-bit between the two.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "kernels.hpp"
+
+namespace ncpa {
+
+constexpr double kPi = 3.141592653589793;  // value of PI in src/common/util.h:13-14
+
+
+// ---------------------------------------------------------------------------
+// Steffen monotone cubic on non-uniform knots (gsl_interp_steffen as used by
+// src/atmosphere/AtmosphericProperty1D.cpp:72-136).  coef[4i..4i+3] = a,b,c,d
+// with y = d + t (c + t (b + t a)), t = x - x_i.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int knot_search(int n, const double* __restrict__ x, double xq) {
+    int lo = 0, hi = n - 1;
+    while (hi > lo + 1) {
+        int mid = (lo + hi) >> 1;
+        if (x[mid] > xq) hi = mid; else lo = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double spline_get(int n, const double* __restrict__ x,
+                                             const double* __restrict__ y,
+                                             const double* __restrict__ coef, double xq) {
+    if (xq > x[n - 1]) return y[n - 1];
+    if (xq < x[0]) return y[0];
+    int i = knot_search(n, x, xq);
+    const double* c = coef + 4 * i;
+    double t = xq - x[i];
+    return c[3] + t * (c[2] + t * (c[1] + t * c[0]));
+}
+
+__device__ __forceinline__ double spline_deriv(int n, const double* __restrict__ x,
+                                               const double* __restrict__ coef, double xq) {
+    if (xq > x[n - 1] || xq < x[0]) return 0.0;
+    int i = knot_search(n, x, xq);
+    const double* c = coef + 4 * i;
+    double t = xq - x[i];
+    return c[2] + t * (2.0 * c[1] + t * 3.0 * c[0]);
+}
+
+// ---------------------------------------------------------------------------
+// power-of-two rescaling (exact)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int biased_exp(double v) {
+    return (__double2hiint(v) >> 20) & 0x7ff;
+}
+// shift e such that max(|a|,|b|) * 2^-e is near 1, or 0 when inside 2^+-480
+__device__ __forceinline__ int rescale_shift(double a, double b) {
+    int e = max(biased_exp(a), biased_exp(b));
+    if (e == 0) return 0;
+    e -= 1023;
+    return (e > 480 || e < -480) ? e : 0;
+}
+// overflow-only variant for recurrences whose squares are accumulated: keeps
+// |a|,|b| below 2^240 so that sums of squares stay finite
+__device__ __forceinline__ int grow_shift(double a, double b) {
+    int e = max(biased_exp(a), biased_exp(b)) - 1023;
+    return e > 240 ? e : 0;
+}
+// 2^k as a double; 0 below the normal range, +inf above it
+__device__ __forceinline__ double pow2(int k) {
+    if (k < -1022) return 0.0;
+    if (k > 1023) return __longlong_as_double(0x7ff0000000000000ll);
+    return __hiloint2double((k + 1023) << 20, 0);
+}
+
+// ---------------------------------------------------------------------------
+// TMA bulk copies (cp.async.bulk, non-tensor) into shared memory with an
+// mbarrier transaction count, and bounded waits.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// global -> shared bulk copy; dst, src 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after ~2^22 polls (each poll may suspend the thread
+// for a hardware-chosen interval), records kErrTimeout and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned* err) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+    }
+    atomicOr(err, kErrTimeout);
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Division-free Sturm sweep.  Matrix S = h^2 A: diagonal s_i, unit
+// off-diagonal.  p_{-2}=0, p_{-1}=1, p_i = (s_i - x) p_{i-1} - p_{i-2};
+// negative LDL^T pivot i <=> sign(p_i) != sign(p_{i-1}).  The sign bits of
+// 32 consecutive p_i are packed with a funnel shift and the changes counted
+// with one popc per word.
+// ---------------------------------------------------------------------------
+struct SturmState {
+    double p0, p1;      // p_{i-2}, p_{i-1}
+    unsigned prevbit;   // sign bit of p_{i-1}
+    int cnt;
+    __device__ __forceinline__ void reset() {
+        p0 = 0.0;
+        p1 = 1.0;
+        prevbit = 0u;
+        cnt = 0;
+    }
+    // 32 steps from s[0..31] (16-byte aligned shared memory)
+    __device__ __forceinline__ void word32(const double* __restrict__ s, double x) {
+        unsigned w = 0u;
+#pragma unroll
+        for (int u = 0; u < 32; u += 2) {
+            double2 sv = *reinterpret_cast<const double2*>(s + u);
+            double a0 = sv.x - x;
+            double q0 = fma(a0, p1, -p0);
+            double a1 = sv.y - x;
+            double q1 = fma(a1, q0, -p1);
+            w = __funnelshift_l(__double2hiint(q0), w, 1);
+            w = __funnelshift_l(__double2hiint(q1), w, 1);
+            p0 = q0;
+            p1 = q1;
+        }
+        unsigned prev = (w >> 1) | (prevbit << 31);
+        cnt += __popc(w ^ prev);
+        prevbit = w & 1u;
+        int sh = rescale_shift(p0, p1);
+        if (sh) {
+            double sc = pow2(-sh);
+            p0 *= sc;
+            p1 *= sc;
+        }
+    }
+    // single guarded step (ragged tail)
+    __device__ __forceinline__ void step(double si, double x) {
+        double a = si - x;
+        double q = fma(a, p1, -p0);
+        unsigned b = static_cast<unsigned>(__double2hiint(q)) >> 31;
+        cnt += static_cast<int>(b ^ prevbit);
+        prevbit = b;
+        p0 = p1;
+        p1 = q;
+    }
+};
+
+}  // namespace ncpa

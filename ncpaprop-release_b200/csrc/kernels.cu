@@ -1,0 +1,1243 @@
+// sm_100a kernels of the effective-sound-speed (ESS) normal-mode path.
+//
+//  K0  knot-level fields: Steffen coefficients, c0 / wind speed / direction,
+//      c_eff per azimuth, Sutherland-Bass absorption per frequency
+//      (src/atmosphere/{AtmosphericProperty1D,Atmosphere1D,AtmosphericModel}.cpp)
+//  K1  matrix build on the Nz grid (ESSModeSolver::getModalTrace,
+//      ESSModeSolver.cpp:531-559; EigenEngine.cpp:57-83 assembly)
+//  K2  WKB window (ESSModeSolver.cpp:561-621)
+//  K3  Sturm isolation scan + multisection/bisection (replaces the SLEPc
+//      spectrum slice of EigenEngine::doESSCalculation, EigenEngine.cpp:10-172)
+//  K4  twisted-factorisation eigenvectors with the perturbative attenuation
+//      and group-speed integrals fused in (ModeSolver::doPerturb,
+//      ModeSolver.cpp:263-284; ESSModeSolver.cpp:738-744)
+//  K5  modal sums for 1-D / 2-D transmission loss (ModeSolver.cpp:292-565)
+//  K6  ModBB transfer function + pulse synthesis
+//      (ModalBroadbandPropagator.cpp:245-277, BroadbandPropagator.cpp:327-662)
+#include "device_common.cuh"
+#include "kernels.hpp"
+
+#include <cuda/std/complex>
+
+namespace ncpa {
+
+// ===========================================================================
+// K0: knot-level fields
+// ===========================================================================
+__device__ __forceinline__ double sgn1(double v) { return v < 0.0 ? -1.0 : 1.0; }
+
+// Steffen (1990) slope at knot i; one-sided secants at the ends
+__device__ double steffen_slope(int n, const double* __restrict__ x, const double* __restrict__ y, int i) {
+    if (i == 0) return (y[1] - y[0]) / (x[1] - x[0]);
+    if (i == n - 1) return (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]);
+    double hl = x[i] - x[i - 1], hr = x[i + 1] - x[i];
+    double sl = (y[i] - y[i - 1]) / hl, sr = (y[i + 1] - y[i]) / hr;
+    double pp = (sl * hr + sr * hl) / (hl + hr);
+    double m = fabs(sl);
+    if (fabs(sr) < m) m = fabs(sr);
+    if (0.5 * fabs(pp) < m) m = 0.5 * fabs(pp);
+    return (sgn1(sl) + sgn1(sr)) * m;
+}
+
+__global__ void k_steffen(int n, const double* __restrict__ x, const double* __restrict__ yall, int batch,
+                          int ystride, double* __restrict__ call, int cstride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int b = blockIdx.y;
+    if (i >= n - 1 || b >= batch) return;
+    const double* y = yall + (size_t)b * ystride;
+    double y0 = steffen_slope(n, x, y, i), y1 = steffen_slope(n, x, y, i + 1);
+    double h = x[i + 1] - x[i];
+    double s = (y[i + 1] - y[i]) / h;
+    double* c = call + (size_t)b * cstride + 4 * i;
+    c[0] = (y0 + y1 - 2.0 * s) / h / h;
+    c[1] = (3.0 * s - 2.0 * y0 - y1) / h;
+    c[2] = y0;
+    c[3] = y[i];
+}
+
+int launch_steffen(cudaStream_t st, int n, const double* x, const double* y, int batch, int ystride,
+                   double* coef, int cstride) {
+    dim3 grid((n - 1 + 255) / 256, batch);
+    k_steffen<<<grid, 256, 0, st>>>(n, x, y, batch, ystride, coef, cstride);
+    return 1;
+}
+
+// c0 = sqrt(1.4 P/rho) with P, rho read through their splines at the knots
+// (Atmosphere1D.cpp:821-848); wind speed and direction, degrees clockwise
+// from north (Atmosphere1D.cpp:484-544)
+__global__ void k_profile_derived(int n, const double* __restrict__ z, const double* __restrict__ u,
+                                  const double* __restrict__ v, const double* __restrict__ p,
+                                  const double* __restrict__ rho, const double* __restrict__ pcoef,
+                                  const double* __restrict__ rcoef, int have_c0, double* __restrict__ c0,
+                                  double* __restrict__ ws, double* __restrict__ wd) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (!have_c0) {
+        double pv = spline_get(n, z, p, pcoef, z[k]);
+        double rv = spline_get(n, z, rho, rcoef, z[k]);
+        c0[k] = sqrt(1.4 * pv / rv);
+    }
+    ws[k] = sqrt(u[k] * u[k] + v[k] * v[k]);
+    wd[k] = (kPi / 2.0 - atan2(v[k], u[k])) * 180.0 / kPi;
+}
+
+int launch_profile_derived(cudaStream_t st, int n, const double* z, const double* u, const double* v,
+                           const double* p, const double* rho, const double* pcoef, const double* rcoef,
+                           int have_c0, double* c0, double* ws, double* wd) {
+    k_profile_derived<<<(n + 255) / 256, 256, 0, st>>>(n, z, u, v, p, rho, pcoef, rcoef, have_c0, c0, ws, wd);
+    return 1;
+}
+
+// c_eff = c0 + |w| cos(dir - az) at the knots (Atmosphere1D.cpp:546-610)
+__global__ void k_ceff_knots(int n, int n_az, const double* __restrict__ az, const double* __restrict__ c0,
+                             const double* __restrict__ ws, const double* __restrict__ wd,
+                             double* __restrict__ ceff) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int a = blockIdx.y;
+    if (k >= n || a >= n_az) return;
+    double az_rad = az[a] * kPi / 180.0;
+    double dir = wd[k] * kPi / 180.0;
+    double wc = ws[k] * cos(dir - az_rad);
+    ceff[(size_t)a * n + k] = wc + c0[k];
+}
+
+int launch_ceff_knots(cudaStream_t st, int n, int n_az, const double* az, const double* c0, const double* ws,
+                      const double* wd, double* ceff) {
+    dim3 grid((n + 255) / 256, n_az);
+    k_ceff_knots<<<grid, 256, 0, st>>>(n, n_az, az, c0, ws, wd, ceff);
+    return 1;
+}
+
+// Sutherland-Bass absorption [Np/m] (AtmosphericModel.cpp:86-219); z in km
+__device__ double attn_sutherland_bass(double z, double T_z, double P_z, double D_z, double freq) {
+    const double mu_o = 18.192E-6, T_o = 293.15, P_o = 101325, S = 117.0;
+    const double Cv_R[4] = {5.0 / 2.0, 5.0 / 2.0, 3.0, 3.0};
+    const double Cp_R[4] = {7.0 / 2.0, 7.0 / 2.0, 4.0, 4.0};
+    const double theta[4] = {2239.1, 3352.0, 915.0, 1037.0};
+    const double PI = kPi;
+    double c_snd_z = sqrt(1.4 * P_z / D_z);
+    double mu = mu_o * sqrt(T_z / T_o) * ((1.0 + S / T_o) / (1.0 + S / T_z));
+    double nu = (8.0 * PI * freq * mu) / (3.0 * P_z);
+    double z2 = pow(z, 2), z3 = pow(z, 3), z4 = pow(z, 4), z5 = pow(z, 5);
+    double X[7];
+    X[0] = (z > 90.0) ? pow(10.0, 49.296 - (1.5524 * z) + (1.8714E-2 * z2) - (1.1069E-4 * z3) + (3.199E-7 * z4) -
+                                      (3.6211E-10 * z5))
+                      : pow(10.0, -0.67887);
+    X[1] = (z > 76.0) ? pow(10.0, (1.3972E-1) - (5.6269E-3 * z) + (3.9407E-5 * z2) - (1.0737E-7 * z3))
+                      : pow(10.0, -0.10744);
+    X[2] = pow(10.0, -3.3979);
+    X[3] = (z > 80.0) ? pow(10.0, -4.234 - (3.0975E-2 * z))
+                      : pow(10.0, -19.027 + (1.3093 * z) - (4.6496E-2 * z2) + (7.8543E-4 * z3) - (6.5169E-6 * z4) +
+                                      (2.1343E-8 * z5));
+    X[4] = (z > 95.0) ? pow(10.0, -3.2456 + (4.6642E-2 * z) - (2.6894E-4 * z2) + (5.264E-7 * z3))
+                      : pow(10.0, -11.195 + (1.5408E-1 * z) - (1.4348E-3 * z2) + (1.0166E-5 * z3));
+    X[5] = pow(10.0, -53.746 + (1.5439 * z) - (1.8824E-2 * z2) + (1.1587E-4 * z3) - (3.5399E-7 * z4) +
+                         (4.2609E-10 * z5));
+    X[6] = (z > 30.0) ? pow(10.0, -4.2563 + (7.6245E-2 * z) - (2.1824E-3 * z2) - (2.3010E-6 * z3) +
+                                      (2.4265E-7 * z4) - (1.2500E-09 * z5))
+                      : pow(10.0, -1.7491 + (4.4986E-2 * z) - (6.8549E-2 * z2) + (5.4639E-3 * z3) -
+                                      (1.5539E-4 * z4) + (1.5063E-06 * z5));
+    double X_ON = (X[0] + X[1]) / 0.9903;
+    double Z_rot_0 = 54.1 * exp(-17.3 * (pow(T_z, -1.0 / 3.0)));
+    double Z_rot_1 = 63.3 * exp(-16.7 * (pow(T_z, -1.0 / 3.0)));
+    double Z_rot_ = 1.0 / ((X[1] / Z_rot_1) + (X[0] / Z_rot_0));
+    double sigma = 5.0 / sqrt(21.0);
+    double nn = (4.0 / 5.0) * sqrt(3.0 / 7.0) * Z_rot_;
+    double chi = 3.0 * nn * nu / 4.0;
+    double cchi = 2.36 * chi;
+    double nu2 = pow(nu, 2), cchi2 = pow(cchi, 2);
+    double a_cl = (2 * PI * freq / c_snd_z) *
+                  sqrt(0.5 * (sqrt(1 + nu2) - 1) * (1 + cchi2) / ((1 + nu2) * (1 + pow(sigma * cchi, 2))));
+    double a_rot = (2 * PI * freq / c_snd_z) * X_ON * ((pow(sigma, 2) - 1) * chi / (2 * sigma)) *
+                   sqrt(0.5 * (sqrt(1 + nu2) + 1) / ((1 + nu2) * (1 + cchi2)));
+    double a_diff = 0.003 * a_cl;
+    double Tr = pow(T_z / T_o, -1.0 / 3.0) - 1.0;
+    double A1 = (X[0] + X[1]) * 24.0 * exp(-9.16 * Tr);
+    double A2 = (X[4] + X[5]) * 2400.0;
+    double B = 40400.0 * exp(10.0 * Tr);
+    double C = 0.02 * exp(-11.2 * Tr);
+    double Dd = 0.391 * exp(8.41 * Tr);
+    double E = 9.0 * exp(-19.9 * Tr);
+    double F = 60000.0;
+    double G = 28000.0 * exp(-4.17 * Tr);
+    double H = 22000.0 * exp(-7.68 * Tr);
+    double I_ = 15100.0 * exp(-10.4 * Tr);
+    double J = 11500.0 * exp(-9.17 * Tr);
+    double K = (8.48E08) * exp(9.17 * Tr);
+    double L = exp(-7.72 * Tr);
+    double ZZ = H * X[2] + I_ * (X[0] + 0.5 * X[4]) + J * (X[1] + 0.5 * X[5]) + K * (X[6] + X[3]);
+    double hu = 100.0 * (X[3] + X[6]);
+    double f_vib[4];
+    double pf = (P_z / P_o) * (mu_o / mu);
+    f_vib[0] = pf * (A1 + A2 + B * hu * (C + hu) * (Dd + hu));
+    f_vib[1] = pf * (E + F * X[3] + G * X[6]);
+    f_vib[2] = pf * ZZ;
+    f_vib[3] = pf * (1.2E5) * L;
+    double a_vib = 0.0;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        double et = exp(-theta[m] / T_z);
+        double C_R = ((pow(theta[m] / T_z, 2)) * et) / (pow(1 - et, 2));
+        double A_max = (X[m] * (PI / 2) * C_R) / (Cp_R[m] * (Cv_R[m] + C_R));
+        a_vib = a_vib + (A_max / c_snd_z) * ((2 * (pow(freq, 2)) / f_vib[m]) / (1 + pow(freq / f_vib[m], 2)));
+    }
+    return a_cl + a_rot + a_diff + a_vib;
+}
+
+__global__ void k_alpha_knots(int n, int n_f, const double* __restrict__ freqs, const double* __restrict__ z,
+                              const double* __restrict__ t, const double* __restrict__ p,
+                              const double* __restrict__ rho, double* __restrict__ alpha) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = blockIdx.y;
+    if (k >= n || f >= n_f) return;
+    alpha[(size_t)f * n + k] = attn_sutherland_bass(z[k] * 0.001, t[k], p[k], rho[k], freqs[f]);
+}
+
+int launch_alpha_knots(cudaStream_t st, int n, int n_f, const double* freqs, const double* z, const double* t,
+                       const double* p, const double* rho, double* alpha) {
+    dim3 grid((n + 127) / 128, n_f);
+    k_alpha_knots<<<grid, 128, 0, st>>>(n, n_f, freqs, z, t, p, rho, alpha);
+    return 1;
+}
+
+__global__ void k_grid_common(int nk, const double* __restrict__ zk, const double* __restrict__ rho,
+                              const double* __restrict__ rcoef, const double* __restrict__ p,
+                              const double* __restrict__ pcoef, int nz, double z_min, double dz_grid,
+                              double* __restrict__ rho_g, double* __restrict__ ct_g) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nz) return;
+    double h = z_min + i * dz_grid;
+    double r = spline_get(nk, zk, rho, rcoef, h);
+    double pv = spline_get(nk, zk, p, pcoef, h);
+    rho_g[i] = r;
+    ct_g[i] = sqrt(1.4 * pv / r);
+}
+
+int launch_grid_common(cudaStream_t st, int nk, const double* zk, const double* rho, const double* rcoef,
+                       const double* p, const double* pcoef, int nz, double z_min, double dz_grid,
+                       double* rho_g, double* ct_g) {
+    k_grid_common<<<(nz + 255) / 256, 256, 0, st>>>(nk, zk, rho, rcoef, p, pcoef, nz, z_min, dz_grid, rho_g,
+                                                    ct_g);
+    return 1;
+}
+
+// w_i = ((omega / c_T) alpha_i) 2, the integrand weight of doPerturb
+__global__ void k_attn_weight(int nk, const double* __restrict__ zk, const double* __restrict__ alpha,
+                              const double* __restrict__ acoef, int n_f, const double* __restrict__ freqs,
+                              int nz, double z_min, double dz_grid, const double* __restrict__ ct_g,
+                              double* __restrict__ w, int wstride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = blockIdx.y;
+    if (i >= nz || f >= n_f) return;
+    double h = z_min + i * dz_grid;
+    double a = spline_get(nk, zk, alpha + (size_t)f * nk, acoef + (size_t)f * 4 * (nk - 1), h);
+    double omega = 2 * kPi * freqs[f];
+    w[(size_t)f * wstride + i] = ((omega / ct_g[i]) * a) * 2;
+}
+
+int launch_attn_weight(cudaStream_t st, int nk, const double* zk, const double* alpha, const double* acoef,
+                       int n_f, const double* freqs, int nz, double z_min, double dz_grid, const double* ct_g,
+                       double* w, int wstride) {
+    dim3 grid((nz + 255) / 256, n_f);
+    k_attn_weight<<<grid, 256, 0, st>>>(nk, zk, alpha, acoef, n_f, freqs, nz, z_min, dz_grid, ct_g, w, wstride);
+    return 1;
+}
+
+// ===========================================================================
+// K1: matrix build
+// ===========================================================================
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__global__ void __launch_bounds__(256) k_build_matrix(int nk, const double* __restrict__ zk,
+                                                      const double* __restrict__ ceffk,
+                                                      const double* __restrict__ ceffcoef, int n_az,
+                                                      ProblemInfo* __restrict__ pinfo, int nz, int nz_pad,
+                                                      double z_min, double dz_grid, double dz, double admittance,
+                                                      double* __restrict__ s, double* __restrict__ kz2,
+                                                      double* __restrict__ g) {
+    const int p = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = p % n_az;
+    const double* ck = ceffk + (size_t)a * nk;
+    const double* cc = ceffcoef + (size_t)a * 4 * (nk - 1);
+    const double omega = pinfo[p].omega;
+    const double h2 = dz * dz;
+    const double bnd = (1. / (dz * admittance + 1)) / (dz * dz);
+    double cmin = 1e300, cmax = -1e300;
+    if (i < nz) {
+        double c = spline_get(nk, zk, ck, cc, z_min + i * dz_grid);
+        double t = omega / c;
+        double d = t * t;
+        if (kz2) kz2[(size_t)p * nz + i] = d;
+        if (g) g[(size_t)p * nz_pad + i] = 1.0 / (c * c);
+        cmin = cmax = c;
+        double sd;
+        if (i < nz - 1) {
+            sd = (i == 0) ? (bnd + d) : d;
+        } else {  // last row of the assembled matrix repeats diag[nz-2] (EigenEngine.cpp:59-71)
+            double c2 = spline_get(nk, zk, ck, cc, z_min + (nz - 2) * dz_grid);
+            double t2 = omega / c2;
+            sd = t2 * t2;
+            if (nz - 2 == 0) sd = bnd + sd;
+        }
+        s[(size_t)p * nz_pad + i] = sd * h2 - 2.0;
+        if (i == 0) pinfo[p].ceff_grnd = c;
+        int top = nz - (nz / 10);
+        int itop = top + 1 < nz ? top + 1 : nz - 1;
+        if (i == itop) pinfo[p].ceff_top = c;
+    } else if (i < nz_pad) {
+        s[(size_t)p * nz_pad + i] = 0.0;
+        if (g) g[(size_t)p * nz_pad + i] = 0.0;
+    }
+    cmin = warp_min(cmin);
+    cmax = warp_max(cmax);
+    __shared__ double smin[8], smax[8];
+    int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        smin[wid] = cmin;
+        smax[wid] = cmax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < 8; ++k) {
+            cmin = fmin(cmin, smin[k]);
+            cmax = fmax(cmax, smax[k]);
+        }
+        cmin = fmin(cmin, smin[0]);
+        cmax = fmax(cmax, smax[0]);
+        if (cmin < 1e300) {
+            atomicMin(&pinfo[p].ceffmin_bits, (unsigned long long)__double_as_longlong(cmin));
+            atomicMax(&pinfo[p].ceffmax_bits, (unsigned long long)__double_as_longlong(cmax));
+        }
+    }
+}
+
+int launch_build_matrix(cudaStream_t st, int nk, const double* zk, const double* ceffk, const double* ceffcoef,
+                        int n_az, int P, ProblemInfo* pinfo, int nz, int nz_pad, double z_min, double dz_grid,
+                        double dz, double admittance, double* s, double* kz2, double* g) {
+    dim3 grid((nz_pad + 255) / 256, P);
+    k_build_matrix<<<grid, 256, 0, st>>>(nk, zk, ceffk, ceffcoef, n_az, pinfo, nz, nz_pad, z_min, dz_grid, dz,
+                                         admittance, s, kz2, g);
+    return 1;
+}
+
+// ===========================================================================
+// K2: wavenumber window.  Thread j of the CTA evaluates the WKB integral of
+// the j-th trial kk of the reference's loop (kk built by the same repeated
+// additions), sequentially up the grid as the reference does; the first j
+// whose integral reaches 10 sets k_max.
+// ===========================================================================
+constexpr int kWkbThreads = 128;
+
+__global__ void __launch_bounds__(kWkbThreads) k_window(ProblemInfo* __restrict__ pinfo,
+                                                        const double* __restrict__ kz2, int nz, double dz,
+                                                        int wkb, int wvnum, double c_min, double c_max,
+                                                        unsigned* err) {
+    const int p = blockIdx.x;
+    ProblemInfo pi = pinfo[p];
+    const double omega = pi.omega;
+    const double ceffmin = __longlong_as_double((long long)pi.ceffmin_bits);
+    __shared__ int s_hit, s_first_invalid;
+    double k_max;
+    int used_wkb = 0;
+    if (wkb) {
+        used_wkb = 1;
+        double k_max_full = omega / ceffmin;
+        double k_gnd = omega / pi.ceff_grnd;
+        double kmf2 = k_max_full * k_max_full;
+        double dkk = (kmf2 - k_gnd * k_gnd) / 100.0;
+        double kk0 = k_gnd * k_gnd;
+        double kk_sel = kk0;
+        if (dkk > 1.0e-10) {
+            if (threadIdx.x == 0) {
+                s_hit = 1 << 30;
+                s_first_invalid = 1 << 30;
+            }
+            __syncthreads();
+            const int j = threadIdx.x;
+            double kk = kk0;
+            for (int q = 0; q < j; ++q) kk = kk + dkk;
+            bool valid = kk < kmf2;
+            if (!valid) atomicMin(&s_first_invalid, j);
+            if (valid) {
+                const double* row = kz2 + (size_t)p * nz;
+                double integral = 0.0, term = 1.0;
+                int i = 0;
+                while (term > dkk && i < nz) {
+                    term = fabs(kk - row[i]);
+                    integral = integral + dz * sqrt(term);
+                    i++;
+                }
+                if (integral >= 10.0) atomicMin(&s_hit, j);
+            }
+            __syncthreads();
+            int jsel = s_hit < s_first_invalid ? s_hit : s_first_invalid;
+            if (jsel >= kWkbThreads) {
+                if (threadIdx.x == 0) atomicOr(err, kErrWkb);
+                jsel = kWkbThreads - 1;
+            }
+            kk_sel = kk0;
+            for (int q = 0; q < jsel; ++q) kk_sel = kk_sel + dkk;
+        }
+        k_max = sqrt(kk_sel);
+    } else {
+        k_max = omega / ceffmin;
+    }
+    double k_min = omega / pi.ceff_top;
+    if (used_wkb && k_max < k_min) k_max = omega / ceffmin;
+    if (wvnum) {
+        k_min = 2 * kPi * pi.freq / c_max;
+        k_max = 2 * kPi * pi.freq / c_min;
+    }
+    if (threadIdx.x == 0) {
+        double h2 = dz * dz;
+        pinfo[p].k_min = k_min;
+        pinfo[p].k_max = k_max;
+        pinfo[p].lo = (k_min * k_min) * h2;
+        pinfo[p].hi = (k_max * k_max) * h2;
+        pinfo[p].used_wkb = used_wkb;
+    }
+}
+
+int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2, int nz, double dz, int wkb,
+                  int wvnum, double c_min, double c_max, unsigned* err) {
+    k_window<<<P, kWkbThreads, 0, st>>>(pinfo, kz2, nz, dz, wkb, wvnum, c_min, c_max, err);
+    return 1;
+}
+
+// ===========================================================================
+// CTA-cooperative Sturm sweep: the diagonal streams through shared memory in
+// kChunk-double chunks by TMA bulk copies (kNbuf-deep ring, one mbarrier per
+// slot); every thread runs its own recurrence at its own shift x.
+// ===========================================================================
+constexpr int kNbuf = 4;
+
+struct Ring {
+    double* buf;     // [kNbuf][kChunk]
+    uint64_t* bars;  // [kNbuf]
+    unsigned loads;  // loads issued so far; identical in every thread
+};
+
+__device__ __forceinline__ void ring_issue(Ring& r, unsigned k, const double* src) {
+    int slot = k % kNbuf;
+    mbar_expect_tx(&r.bars[slot], kChunk * 8);
+    tma_load_1d(r.buf + slot * kChunk, src, kChunk * 8, &r.bars[slot]);
+}
+
+__device__ int cta_sturm_sweep(const double* __restrict__ s, int nz, double x, Ring& r, unsigned* err) {
+    const int nch = (nz + kChunk - 1) / kChunk;
+    const unsigned base = r.loads;
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < nch && c < kNbuf; ++c) ring_issue(r, base + c, s + (size_t)c * kChunk);
+    }
+    SturmState st;
+    st.reset();
+    for (int c = 0; c < nch; ++c) {
+        const unsigned k = base + c;
+        const int slot = k % kNbuf;
+        mbar_wait_bounded(&r.bars[slot], (k / kNbuf) & 1u, err);
+        const double* b = r.buf + slot * kChunk;
+        const int valid = min(kChunk, nz - c * kChunk);
+        const int nw = valid >> 5;
+        for (int w = 0; w < nw; ++w) st.word32(b + 32 * w, x);
+        for (int i = nw * 32; i < valid; ++i) st.step(b[i], x);
+        __syncthreads();
+        if (threadIdx.x == 0 && c + kNbuf < nch) {
+            fence_proxy_async();
+            ring_issue(r, base + c + kNbuf, s + (size_t)(c + kNbuf) * kChunk);
+        }
+    }
+    r.loads = base + nch;
+    return st.cnt;
+}
+
+__device__ __forceinline__ void ring_init(Ring& r, double* buf, uint64_t* bars) {
+    r.buf = buf;
+    r.bars = bars;
+    r.loads = 0;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kNbuf; ++k) mbar_init(&bars[k], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double scan_x(double lo, double hi, int t) {
+    if (t == 0) return lo;
+    if (t == kScanPoints - 1) return hi;
+    return lo + (hi - lo) * ((double)t / (double)(kScanPoints - 1));
+}
+
+// K3a: kScanPoints counts per problem on an even grid of [lo, hi]
+__global__ void __launch_bounds__(kScanPoints) k_scan(const ProblemInfo* __restrict__ pinfo,
+                                                      const double* __restrict__ s, int nz, int nz_pad,
+                                                      int* __restrict__ counts, unsigned* err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    double* buf = reinterpret_cast<double*>(smem_raw);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + kNbuf * kChunk * 8);
+    Ring r;
+    ring_init(r, buf, bars);
+    const int p = blockIdx.x;
+    const double lo = pinfo[p].lo, hi = pinfo[p].hi;
+    const double x = scan_x(lo, hi, threadIdx.x);
+    int c = cta_sturm_sweep(s + (size_t)p * nz_pad, nz, x, r, err);
+    counts[(size_t)p * kScanPoints + threadIdx.x] = c;
+}
+
+int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
+                int* counts, unsigned* err) {
+    size_t sm = kNbuf * kChunk * 8 + kNbuf * 8;
+    k_scan<<<P, kScanPoints, sm, st>>>(pinfo, s, nz, nz_pad, counts, err);
+    return 1;
+}
+
+// K3: persistent multisection.  A work item holds m <= 256 consecutive
+// eigen-indices of one problem; G = 2^k threads share an eigenvalue so that
+// G*m <= 256, and each round cuts every bracket into G+1 pieces.
+__global__ void __launch_bounds__(kThreads) k_bisect(const ProblemInfo* __restrict__ pinfo,
+                                                     const double* __restrict__ s, int nz, int nz_pad,
+                                                     const int* __restrict__ counts,
+                                                     const WorkItem* __restrict__ items, int n_items,
+                                                     int* counter, double tol, double* __restrict__ mu,
+                                                     unsigned* err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    double* buf = reinterpret_cast<double*>(smem_raw);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + kNbuf * kChunk * 8);
+    __shared__ double sa[kThreads], sb[kThreads];
+    __shared__ int sbest[kThreads];
+    __shared__ int s_item;
+    Ring r;
+    ring_init(r, buf, bars);
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= n_items) break;
+        const WorkItem w = items[it];
+        const ProblemInfo pi = pinfo[w.problem];
+        const int* cnt = counts + (size_t)w.problem * kScanPoints;
+        const double* sp = s + (size_t)w.problem * nz_pad;
+        int G = 1;
+        while (G * 2 * w.m <= kThreads) G *= 2;
+        if (tid < w.m) {  // initial bracket from the isolation scan
+            const int J = pi.c_lo + w.j0 + tid;
+            int t0 = 0;
+            for (int t = 0; t < kScanPoints; ++t)
+                if (cnt[t] <= J) t0 = t;
+            int t1 = kScanPoints - 1;
+            for (int t = kScanPoints - 1; t > t0; --t)
+                if (cnt[t] > J) t1 = t;
+            if (cnt[t1] <= J) atomicOr(err, kErrBracket);
+            sa[tid] = scan_x(pi.lo, pi.hi, t0);
+            sb[tid] = scan_x(pi.lo, pi.hi, t1);
+        }
+        __syncthreads();
+        const int e = tid / G, gi = tid % G;
+        const bool active = e < w.m;
+        const int J = pi.c_lo + w.j0 + e;
+        const double frac = (double)(gi + 1) / (double)(G + 1);
+        for (int round = 0; round < 256; ++round) {
+            double a = active ? sa[e] : pi.lo, b = active ? sb[e] : pi.hi;
+            double x = a + (b - a) * frac;
+            int c = cta_sturm_sweep(sp, nz, x, r, err);
+            if (tid < w.m) sbest[tid] = -1;
+            __syncthreads();
+            if (active && c <= J) atomicMax(&sbest[e], gi);
+            __syncthreads();
+            bool done = true;
+            if (tid < w.m) {
+                double A = sa[tid], B = sb[tid];
+                int gb = sbest[tid];
+                double na = gb >= 0 ? A + (B - A) * ((double)(gb + 1) / (double)(G + 1)) : A;
+                double nb = gb + 1 < G ? A + (B - A) * ((double)(gb + 2) / (double)(G + 1)) : B;
+                sa[tid] = na;
+                sb[tid] = nb;
+                done = !(nb - na > tol) || (na == A && nb == B);
+            }
+            if (__syncthreads_and(done)) break;
+        }
+        if (tid < w.m) mu[pi.off + w.j0 + tid] = 0.5 * (sa[tid] + sb[tid]);
+        __syncthreads();
+    }
+}
+
+int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
+                  const int* counts, const WorkItem* items, int n_items, int* counter, double tol, double* mu,
+                  unsigned* err) {
+    size_t sm = kNbuf * kChunk * 8 + kNbuf * 8;
+    k_bisect<<<grid, kThreads, sm, st>>>(pinfo, s, nz, nz_pad, counts, items, n_items, counter, tol, mu, err);
+    return 1;
+}
+
+// ===========================================================================
+// K4: eigenvectors by twisted factorisation (see oracle/ncpa_oracle.c for the
+// derivation).  Pass 1 runs the backward recurrence q top-down and stores a
+// checkpoint (q_c, q_{c+1}, exponent) every kBlk rows; pass 2 runs the forward
+// recurrence p bottom-up, re-creates each block's q from its checkpoint in
+// registers, tracks the twist r = argmax |p_{r-1} q_{r+1}| and accumulates
+//   sum z^2, sum z^2 w, sum z^2 g   below r (forward) and above r (backward).
+// ===========================================================================
+constexpr int kEvNbuf = 2;
+
+struct EvRing {
+    double* sbuf;    // [kEvNbuf][kChunk]
+    double* wbuf;
+    double* gbuf;
+    uint64_t* bars;  // [kEvNbuf]
+    unsigned loads;
+};
+
+__device__ __forceinline__ void evring_issue(EvRing& r, unsigned k, int c, const double* sp, const double* wp,
+                                             const double* gp) {
+    int slot = k % kEvNbuf;
+    uint32_t bytes = kChunk * 8 * (1 + (wp ? 1 : 0) + (gp ? 1 : 0));
+    mbar_expect_tx(&r.bars[slot], bytes);
+    tma_load_1d(r.sbuf + slot * kChunk, sp + (size_t)c * kChunk, kChunk * 8, &r.bars[slot]);
+    if (wp) tma_load_1d(r.wbuf + slot * kChunk, wp + (size_t)c * kChunk, kChunk * 8, &r.bars[slot]);
+    if (gp) tma_load_1d(r.gbuf + slot * kChunk, gp + (size_t)c * kChunk, kChunk * 8, &r.bars[slot]);
+}
+
+__device__ __forceinline__ cuda::std::complex<double> csqrt_principal(double x, double y) {
+    // principal square root of x + i y for x > 0 (k^2 + i absorption)
+    double m = hypot(x, y);
+    double t = sqrt(0.5 * (m + fabs(x)));
+    if (x >= 0.0) return cuda::std::complex<double>(t, y / (2.0 * t));
+    return cuda::std::complex<double>(fabs(y) / (2.0 * t), copysign(t, y));
+}
+
+template <bool kGroup, bool kVec>
+__global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    EvRing R;
+    R.sbuf = reinterpret_cast<double*>(smem_raw);
+    R.wbuf = R.sbuf + kEvNbuf * kChunk;
+    R.gbuf = R.wbuf + kEvNbuf * kChunk;
+    R.bars = reinterpret_cast<uint64_t*>(R.gbuf + kEvNbuf * kChunk);
+    R.loads = 0;
+    __shared__ int s_item;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int k = 0; k < kEvNbuf; ++k) mbar_init(&R.bars[k], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const int nz = A.nz;
+    const int nch = (nz + kChunk - 1) / kChunk;
+    const int nblk = (nz + kBlk - 1) / kBlk;
+    double* ck1 = A.ck_q1 + (size_t)blockIdx.x * A.ck_slot_stride;
+    double* ck2 = A.ck_q2 + (size_t)blockIdx.x * A.ck_slot_stride;
+    int* cke = A.ck_e + (size_t)blockIdx.x * A.ck_slot_stride;
+
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(A.counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= A.n_items) break;
+        const WorkItem w = A.items[it];
+        const ProblemInfo pi = A.pinfo[w.problem];
+        const double* sp = A.s + (size_t)w.problem * A.nz_pad;
+        const double* wp = A.w + (size_t)(w.problem / A.n_az) * A.wstride;
+        const double* gp = kGroup ? A.g + (size_t)w.problem * A.nz_pad : nullptr;
+        const bool active = tid < w.m;
+        const double mu = active ? A.mu[pi.off + w.j0 + tid] : pi.lo;
+
+        // ---------------- pass 1: backward recurrence, checkpoints ----------
+        {
+            const unsigned base = R.loads;
+            if (tid == 0)
+                for (int o = 0; o < nch && o < kEvNbuf; ++o) evring_issue(R, base + o, nch - 1 - o, sp, nullptr, nullptr);
+            double q1 = 1.0, q2 = 0.0;  // q_{i}, q_{i+1} after each step; q_n = 1, q_{n+1} = 0
+            int E = 0;
+            for (int o = 0; o < nch; ++o) {
+                const int c = nch - 1 - o;
+                const unsigned k = base + o;
+                const int slot = k % kEvNbuf;
+                mbar_wait_bounded(&R.bars[slot], (k / kEvNbuf) & 1u, A.err);
+                const double* sb = R.sbuf + slot * kChunk;
+                const int valid = min(kChunk, nz - c * kChunk);
+                for (int lb = ((valid - 1) / kBlk) * kBlk; lb >= 0; lb -= kBlk) {
+#pragma unroll
+                    for (int u = kBlk - 1; u >= 0; --u) {
+                        const int li = lb + u;
+                        if (li < valid) {
+                            double qi = fma(sb[li] - mu, q1, -q2);
+                            q2 = q1;
+                            q1 = qi;
+                        }
+                    }
+                    const int gbase = c * kChunk + lb;
+                    if (gbase > 0) {
+                        const size_t ci = (size_t)(gbase / kBlk - 1) * kThreads + tid;
+                        ck1[ci] = q1;
+                        ck2[ci] = q2;
+                        cke[ci] = E;
+                    }
+                    int sh = grow_shift(q1, q2);
+                    if (sh) {
+                        double sc = pow2(-sh);
+                        q1 *= sc;
+                        q2 *= sc;
+                        E += sh;
+                    }
+                }
+                __syncthreads();
+                if (tid == 0 && o + kEvNbuf < nch) {
+                    fence_proxy_async();
+                    evring_issue(R, base + o + kEvNbuf, nch - 1 - (o + kEvNbuf), sp, nullptr, nullptr);
+                }
+            }
+            R.loads = base + nch;
+        }
+
+        // ---------------- pass 2: forward recurrence + twist + sums ---------
+        double pm2 = 0.0, pm1 = 1.0;
+        int Ep = 0;
+        double An = 0.0, Aw = 0.0, Ag = 0.0;
+        double thr = -1.0;
+        int Ethr = 0;
+        int r = 0, Epr = 0, Eqr = 0;
+        double Anr = 1.0, Awr = 0.0, Agr = 0.0, sqr_ = 1.0, pr = 1.0, qr = 1.0;
+        double Tn = 0.0, Tw = 0.0, Tg = 0.0, fq = 1.0;
+        double ps = 1.0, qs = 1.0, prc = 1.0, qrc = 1.0;
+        int Eps = 0, Eqs = 0, Eprc = 0, Eqrc = 0;
+        {
+            const unsigned base = R.loads;
+            if (tid == 0)
+                for (int c = 0; c < nch && c < kEvNbuf; ++c) evring_issue(R, base + c, c, sp, wp, gp);
+            // checkpoint of block 0
+            double nq1, nq2;
+            int nE;
+            auto load_ck = [&](int kb, double& a1, double& a2, int& ae) {
+                int ctop = min((kb + 1) * kBlk, nz);
+                if (ctop >= nz) {
+                    a1 = 1.0;
+                    a2 = 0.0;
+                    ae = 0;
+                } else {
+                    size_t ci = (size_t)kb * kThreads + tid;
+                    a1 = ck1[ci];
+                    a2 = ck2[ci];
+                    ae = cke[ci];
+                }
+            };
+            load_ck(0, nq1, nq2, nE);
+            for (int c = 0; c < nch; ++c) {
+                const unsigned k = base + c;
+                const int slot = k % kEvNbuf;
+                mbar_wait_bounded(&R.bars[slot], (k / kEvNbuf) & 1u, A.err);
+                const double* sb = R.sbuf + slot * kChunk;
+                const double* wb = R.wbuf + slot * kChunk;
+                const double* gb = R.gbuf + slot * kChunk;
+                const int valid = min(kChunk, nz - c * kChunk);
+                for (int lb = 0; lb < valid; lb += kBlk) {
+                    const int gbase = c * kChunk + lb;
+                    const int kb = gbase / kBlk;
+                    double q1 = nq1, q2 = nq2;
+                    const int Eb = nE;
+                    if (kb + 1 < nblk) load_ck(kb + 1, nq1, nq2, nE);
+                    // re-scale threshold and the backward-part scale factor
+                    {
+                        const int Enew = Ep + Eb;
+                        if (Enew != Ethr) {
+                            thr *= pow2(Ethr - Enew);
+                            Ethr = Enew;
+                        }
+                        fq = pow2(Eb - Eqr);
+                    }
+                    // q_{gbase+1 .. gbase+kBlk} of this block, relative to 2^Eb
+                    double qb[kBlk];
+                    const int ctop = min(gbase + kBlk, nz);
+#pragma unroll
+                    for (int jj = kBlk - 1; jj >= 0; --jj) {
+                        const int idx = gbase + 1 + jj;
+                        if (idx == ctop) {
+                            qb[jj] = q1;
+                        } else if (idx < ctop) {
+                            double qi = fma(sb[idx - c * kChunk] - mu, q1, -q2);
+                            qb[jj] = qi;
+                            q2 = q1;
+                            q1 = qi;
+                        } else {
+                            qb[jj] = 0.0;
+                        }
+                    }
+#pragma unroll
+                    for (int jj = 0; jj < kBlk; ++jj) {
+                        const int i = gbase + jj;
+                        if (i < nz) {
+                            const int li = lb + jj;
+                            const double wi = wb[li];
+                            const double sq = pm1 * pm1;
+                            An = An + sq;
+                            Aw = fma(sq, wi, Aw);
+                            const double qn = qb[jj];
+                            const double t = qn * fq;
+                            const double t2 = t * t;
+                            Tn = Tn + t2;
+                            Tw = fma(t2, wi, Tw);
+                            double gi = 0.0;
+                            if (kGroup) {
+                                gi = gb[li];
+                                Ag = fma(sq, gi, Ag);
+                                Tg = fma(t2, gi, Tg);
+                            }
+                            const double prod = fabs(pm1 * qn);
+                            if (prod > thr) {
+                                thr = prod;
+                                r = i;
+                                Anr = An;
+                                Awr = Aw;
+                                Agr = Ag;
+                                sqr_ = sq;
+                                pr = pm1;
+                                Epr = Ep;
+                                qr = qn;
+                                Eqr = Eb;
+                                fq = 1.0;
+                                Tn = 0.0;
+                                Tw = 0.0;
+                                Tg = 0.0;
+                            }
+                            if (i == A.isrc) {
+                                ps = pm1;
+                                Eps = Ep;
+                                qs = qn;
+                                Eqs = Eb;
+                            }
+                            if (i == A.ircv) {
+                                prc = pm1;
+                                Eprc = Ep;
+                                qrc = qn;
+                                Eqrc = Eb;
+                            }
+                            const double a = sb[li] - mu;
+                            const double pn = fma(a, pm1, -pm2);
+                            pm2 = pm1;
+                            pm1 = pn;
+                        }
+                    }
+                    int sh = grow_shift(pm1, pm2);
+                    if (sh) {
+                        double sc = pow2(-sh), sc2 = pow2(-2 * sh);
+                        pm1 *= sc;
+                        pm2 *= sc;
+                        An *= sc2;
+                        Aw *= sc2;
+                        Ag *= sc2;
+                        Ep += sh;
+                    }
+                }
+                __syncthreads();
+                if (tid == 0 && c + kEvNbuf < nch) {
+                    fence_proxy_async();
+                    evring_issue(R, base + c + kEvNbuf, c + kEvNbuf, sp, wp, gp);
+                }
+            }
+            R.loads = base + nch;
+        }
+        // ---------------- combine ----------------------------------------
+        const double iq2 = 1.0 / (qr * qr);
+        const double isq = 1.0 / sqr_;
+        const double nrm = Anr * isq + Tn * iq2;
+        const double scale = 1.0 / sqrt(nrm * A.dz);
+        double zs = (A.isrc <= r) ? (ps / pr) * pow2(Eps - Epr) : (qs / qr) * pow2(Eqs - Eqr);
+        double zr = (A.ircv <= r) ? (prc / pr) * pow2(Eprc - Epr) : (qrc / qr) * pow2(Eqrc - Eqr);
+        if ((A.isrc - r) & 1) zs = -zs;
+        if ((A.ircv - r) & 1) zr = -zr;
+        const double absorption = (Awr * isq + Tw * iq2) / nrm;
+        const double ks = sqrt(mu / A.h2);
+        const double kk = ks * ks;
+        const auto kp = csqrt_principal(kk, absorption);
+        if (active) {
+            const int o = pi.off + w.j0 + tid;
+            A.kr[o] = kp.real();
+            A.ki[o] = kp.imag();
+            A.vs[o] = zs * scale;
+            A.vr[o] = zr * scale;
+            if (kGroup) {
+                const double gsum = (Agr * isq + Tg * iq2) / nrm;
+                const double vph = pi.omega / kp.real();
+                A.vg[o] = 1.0 / (vph * gsum);
+            } else if (A.vg) {
+                A.vg[o] = 0.0;
+            }
+        }
+        // ---------------- pass 3 (optional): full eigenvector --------------
+        if (kVec) {
+            double* vout = A.vfull + A.vfull_off[w.problem];
+            const int M = pi.M;
+            const unsigned base = R.loads;
+            if (tid == 0)
+                for (int c = 0; c < nch && c < kEvNbuf; ++c) evring_issue(R, base + c, c, sp, nullptr, nullptr);
+            double pa = 0.0, pb = 1.0;
+            int Ea = 0;
+            double nq1, nq2;
+            int nE;
+            auto load_ck2 = [&](int kb, double& a1, double& a2, int& ae) {
+                int ctop = min((kb + 1) * kBlk, nz);
+                if (ctop >= nz) {
+                    a1 = 1.0;
+                    a2 = 0.0;
+                    ae = 0;
+                } else {
+                    size_t ci = (size_t)kb * kThreads + tid;
+                    a1 = ck1[ci];
+                    a2 = ck2[ci];
+                    ae = cke[ci];
+                }
+            };
+            load_ck2(0, nq1, nq2, nE);
+            const double ipr = 1.0 / pr, iqr = 1.0 / qr;
+            for (int c = 0; c < nch; ++c) {
+                const unsigned k = base + c;
+                const int slot = k % kEvNbuf;
+                mbar_wait_bounded(&R.bars[slot], (k / kEvNbuf) & 1u, A.err);
+                const double* sb = R.sbuf + slot * kChunk;
+                const int valid = min(kChunk, nz - c * kChunk);
+                for (int lb = 0; lb < valid; lb += kBlk) {
+                    const int gbase = c * kChunk + lb;
+                    const int kb = gbase / kBlk;
+                    double q1 = nq1, q2 = nq2;
+                    const int Eb = nE;
+                    if (kb + 1 < nblk) load_ck2(kb + 1, nq1, nq2, nE);
+                    double qb[kBlk];
+                    const int ctop = min(gbase + kBlk, nz);
+#pragma unroll
+                    for (int jj = kBlk - 1; jj >= 0; --jj) {
+                        const int idx = gbase + 1 + jj;
+                        if (idx == ctop) {
+                            qb[jj] = q1;
+                        } else if (idx < ctop) {
+                            double qi = fma(sb[idx - c * kChunk] - mu, q1, -q2);
+                            qb[jj] = qi;
+                            q2 = q1;
+                            q1 = qi;
+                        } else {
+                            qb[jj] = 0.0;
+                        }
+                    }
+                    const double fp = pow2(Ea - Epr) * ipr * scale;
+                    const double fqq = pow2(Eb - Eqr) * iqr * scale;
+#pragma unroll
+                    for (int jj = 0; jj < kBlk; ++jj) {
+                        const int i = gbase + jj;
+                        if (i < nz) {
+                            double zi = (i <= r) ? pb * fp : qb[jj] * fqq;
+                            if ((i - r) & 1) zi = -zi;
+                            if (active) vout[(size_t)i * M + w.j0 + tid] = zi;
+                            const double a = sb[lb + jj] - mu;
+                            const double pn = fma(a, pb, -pa);
+                            pa = pb;
+                            pb = pn;
+                        }
+                    }
+                    int sh = grow_shift(pb, pa);
+                    if (sh) {
+                        double sc = pow2(-sh);
+                        pa *= sc;
+                        pb *= sc;
+                        Ea += sh;
+                    }
+                }
+                __syncthreads();
+                if (tid == 0 && c + kEvNbuf < nch) {
+                    fence_proxy_async();
+                    evring_issue(R, base + c + kEvNbuf, c + kEvNbuf, sp, nullptr, nullptr);
+                }
+            }
+            R.loads = base + nch;
+        }
+        __syncthreads();
+    }
+}
+
+int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a) {
+    size_t sm = 3 * kEvNbuf * kChunk * 8 + kEvNbuf * 8;
+    const bool grp = a.g != nullptr, vec = a.vfull != nullptr;
+    if (grp && vec) {
+        cudaFuncSetAttribute(k_eigvec<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_eigvec<true, true><<<grid, kThreads, sm, st>>>(a);
+    } else if (grp) {
+        cudaFuncSetAttribute(k_eigvec<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_eigvec<true, false><<<grid, kThreads, sm, st>>>(a);
+    } else if (vec) {
+        cudaFuncSetAttribute(k_eigvec<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_eigvec<false, true><<<grid, kThreads, sm, st>>>(a);
+    } else {
+        cudaFuncSetAttribute(k_eigvec<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_eigvec<false, false><<<grid, kThreads, sm, st>>>(a);
+    }
+    return 1;
+}
+
+// ===========================================================================
+// K5: 1-D transmission loss, one thread per range, modes staged in shared
+// memory.  Phase k r is formed and reduced in FP64.
+// ===========================================================================
+constexpr int kTlTile = 128;
+
+__global__ void __launch_bounds__(256) k_tl1d(const ProblemInfo* __restrict__ pinfo, const double* __restrict__ kr,
+                                              const double* __restrict__ ki, const double* __restrict__ vs,
+                                              const double* __restrict__ vr, int nr, double dr, int lossless,
+                                              double* __restrict__ re, double* __restrict__ im,
+                                              double* __restrict__ incoh) {
+    const int p = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const ProblemInfo pi = pinfo[p];
+    __shared__ double m_kr[kTlTile], m_ki[kTlTile], m_vv[kTlTile], m_sr[kTlTile], m_si[kTlTile], m_ia[kTlTile];
+    const double r = (i + 1) * dr;
+    double sre = 0.0, sim = 0.0, sinc = 0.0;
+    for (int m0 = 0; m0 < pi.M; m0 += kTlTile) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < kTlTile && m0 + t < pi.M; t += blockDim.x) {
+            const int o = pi.off + m0 + t;
+            const double a = kr[o], b = lossless ? 0.0 : ki[o];
+            // 1/sqrt(k): principal root of k, then the reciprocal
+            const auto sk = csqrt_principal(a, b);
+            const double den = sk.real() * sk.real() + sk.imag() * sk.imag();
+            m_kr[t] = a;
+            m_ki[t] = b;
+            m_vv[t] = vs[o] * vr[o];
+            m_sr[t] = sk.real() / den;
+            m_si[t] = -sk.imag() / den;
+            m_ia[t] = lossless ? 1.0 / a : 1.0 / hypot(a, b);
+        }
+        __syncthreads();
+        const int mt = min(kTlTile, pi.M - m0);
+        if (i < nr) {
+            for (int t = 0; t < mt; ++t) {
+                double sn, cs;
+                sincos(m_kr[t] * r, &sn, &cs);
+                const double amp = exp(-m_ki[t] * r);
+                const double vv = m_vv[t];
+                const double er = vv * amp * cs, ei = vv * amp * sn;
+                sre += er * m_sr[t] - ei * m_si[t];
+                sim += er * m_si[t] + ei * m_sr[t];
+                sinc += (vv * vv) * (amp * amp) * m_ia[t];
+            }
+        }
+    }
+    if (i < nr) {
+        // 1000 * 4 pi i e^{-i pi/4} / sqrt(8 pi) / sqrt(r)
+        const double c0 = 1000.0 * 4 * kPi / sqrt(8.0 * kPi) / sqrt(r);
+        const double ang = kPi * 0.25;
+        const double fr = c0 * sin(ang), fi = c0 * cos(ang);
+        const size_t o = (size_t)p * nr + i;
+        re[o] = fr * sre - fi * sim;
+        im[o] = fr * sim + fi * sre;
+        incoh[o] = 1000.0 * 4 * kPi * sqrt(sinc) * sqrt(1. / 8. / kPi / r);
+    }
+}
+
+int launch_tl1d(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* kr, const double* ki,
+                const double* vs, const double* vr, int nr, double dr, int lossless, double* re, double* im,
+                double* incoh) {
+    dim3 grid((nr + 255) / 256, P);
+    k_tl1d<<<grid, 256, 0, st>>>(pinfo, kr, ki, vs, vr, nr, dr, lossless, re, im, incoh);
+    return 1;
+}
+
+// 2-D TL on the sampled heights: P(r_i, z_j) = sum_m vz[j][m] b_m(r_i) with
+// b_m = v_m(z_s) e^{i k r}/sqrt(k); one CTA per range, threads over heights.
+__global__ void __launch_bounds__(256) k_tl2d(int M, const double* __restrict__ kr, const double* __restrict__ ki,
+                                              const double* __restrict__ vs_src, const double* __restrict__ vz,
+                                              int nzo, int nr, double dr, int lossless, double* __restrict__ re,
+                                              double* __restrict__ im) {
+    const int ir = blockIdx.x;
+    const double r = (ir + 1) * dr;
+    __shared__ double br[kTlTile], bi[kTlTile];
+    double accr[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
+    for (int m0 = 0; m0 < M; m0 += kTlTile) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < kTlTile && m0 + t < M; t += blockDim.x) {
+            const int m = m0 + t;
+            const double a = kr[m], b = lossless ? 0.0 : ki[m];
+            const auto sk = csqrt_principal(a, b);
+            const double den = sk.real() * sk.real() + sk.imag() * sk.imag();
+            const double isr = sk.real() / den, isi = -sk.imag() / den;
+            double sn, cs;
+            sincos(a * r, &sn, &cs);
+            const double amp = exp(-b * r) * vs_src[m];
+            const double er = amp * cs, ei = amp * sn;
+            br[t] = er * isr - ei * isi;
+            bi[t] = er * isi + ei * isr;
+        }
+        __syncthreads();
+        const int mt = min(kTlTile, M - m0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = threadIdx.x + u * blockDim.x;
+            if (j < nzo) {
+                const double* row = vz + (size_t)j * M + m0;
+                for (int t = 0; t < mt; ++t) {
+                    accr[u] += row[t] * br[t];
+                    acci[u] += row[t] * bi[t];
+                }
+            }
+        }
+    }
+    const double c0 = 1000.0 * 4 * kPi / sqrt(8.0 * kPi) / sqrt(r);
+    const double ang = kPi * 0.25;
+    const double fr = c0 * sin(ang), fi = c0 * cos(ang);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int j = threadIdx.x + u * blockDim.x;
+        if (j < nzo) {
+            const size_t o = (size_t)ir * nzo + j;
+            re[o] = fr * accr[u] - fi * acci[u];
+            im[o] = fr * acci[u] + fi * accr[u];
+        }
+    }
+}
+
+int launch_tl2d(cudaStream_t st, int M, const double* kr, const double* ki, const double* vs_src,
+                const double* vz, int nzo, int nr, double dr, int lossless, double* re, double* im) {
+    if (nzo > 1024) return -1;  // four heights per thread
+    k_tl2d<<<nr, 256, 0, st>>>(M, kr, ki, vs_src, vz, nzo, nr, dr, lossless, re, im);
+    return 1;
+}
+
+// ===========================================================================
+// K6: ModBB synthesis
+// ===========================================================================
+__global__ void k_twiddle(int nfft, double* __restrict__ tw) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nfft) return;
+    double ang = -2.0 * kPi * (double)m / (double)nfft;
+    double sn, cs;
+    sincos(ang, &sn, &cs);
+    tw[2 * m] = cs;
+    tw[2 * m + 1] = sn;
+}
+
+int launch_twiddle(cudaStream_t st, int nfft, double* tw) {
+    k_twiddle<<<(nfft + 255) / 256, 256, 0, st>>>(nfft, tw);
+    return 1;
+}
+
+// transfer function H(f, r) = i e^{-i pi/4}/sqrt(8 pi r) sqrt(rho_r/rho_s)
+//   sum_j V_s V_r e^{i k r}/sqrt(k), half-Hann over the top 10 % of bins
+__global__ void k_bb_transfer(int nfreq, const int* __restrict__ off, const double* __restrict__ re_k,
+                              const double* __restrict__ im_k, const double* __restrict__ vs,
+                              const double* __restrict__ vr, double rho_ratio, int nr,
+                              const double* __restrict__ ranges, int zero_attn, double* __restrict__ h) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ir = blockIdx.y;
+    if (f >= nfreq || ir >= nr) return;
+    const double r = ranges[ir];
+    double cr = 0.0, ci = 0.0;
+    for (int j = off[f]; j < off[f + 1]; ++j) {
+        const double a = re_k[j], b = zero_attn ? 0.0 : im_k[j];
+        double sn, cs;
+        sincos(r * a, &sn, &cs);
+        const double amp = exp(-r * b) * (vs[j] * vr[j]);
+        const double er = amp * cs, ei = amp * sn;
+        const auto sk = csqrt_principal(a, b);
+        const double den = sk.real() * sk.real() + sk.imag() * sk.imag();
+        const double isr = sk.real() / den, isi = -sk.imag() / den;
+        cr += er * isr - ei * isi;
+        ci += er * isi + ei * isr;
+    }
+    // i e^{-i pi/4} = sin(pi/4) + i cos(pi/4)
+    const double c0 = sqrt(rho_ratio) / sqrt(8.0 * kPi * r);
+    const double ang = kPi * 0.25;
+    const double fr = c0 * sin(ang), fi = c0 * cos(ang);
+    double hr = fr * cr - fi * ci, hi = fr * ci + fi * cr;
+    const int smooth = (int)floor(0.1 * nfreq);
+    const int begin = nfreq - smooth, end = nfreq - 1;
+    if (smooth > 0 && f >= begin) {
+        const double hh = 0.5 * (cos(kPi * (f - begin) / (end - begin)) + 1.0);
+        hr *= hh;
+        hi *= hh;
+    }
+    h[((size_t)ir * nfreq + f) * 2] = hr;
+    h[((size_t)ir * nfreq + f) * 2 + 1] = hi;
+}
+
+int launch_bb_transfer(cudaStream_t st, int nfreq, const int* off, const double* re_k, const double* im_k,
+                       const double* vs, const double* vr, double rho_ratio, int nr, const double* ranges,
+                       int zero_attn, double* h) {
+    dim3 grid((nfreq + 127) / 128, nr);
+    k_bb_transfer<<<grid, 128, 0, st>>>(nfreq, off, re_k, im_k, vs, vr, rho_ratio, nr, ranges, zero_attn, h);
+    return 1;
+}
+
+// p(t_k) = 2 Re( df sum_n e^{-2 pi i f_n t0} S_n H_n e^{-2 pi i k n / nfft} )
+constexpr int kPulseMaxFreq = 4096;
+
+__global__ void __launch_bounds__(256) k_bb_pulse(int nfreq, const double* __restrict__ f,
+                                                  const double* __restrict__ s_src, const double* __restrict__ h,
+                                                  int nr, const double* __restrict__ t0s, int nfft,
+                                                  const double* __restrict__ tw, double* __restrict__ out) {
+    extern __shared__ double arg[];  // 2 * nfreq
+    const int ir = blockIdx.y;
+    const double t0 = t0s[ir];
+    for (int n = threadIdx.x; n < nfreq; n += blockDim.x) {
+        double sn, cs;
+        sincos(((-2.0 * kPi) * f[n]) * t0, &sn, &cs);
+        const double sr = s_src[2 * n], si = s_src[2 * n + 1];
+        const double hr = h[((size_t)ir * nfreq + n) * 2], hi = h[((size_t)ir * nfreq + n) * 2 + 1];
+        const double ar = cs * sr - sn * si, ai = cs * si + sn * sr;
+        arg[2 * n] = ar * hr - ai * hi;
+        arg[2 * n + 1] = ar * hi + ai * hr;
+    }
+    __syncthreads();
+    const double df = f[1] - f[0];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nfft; k += gridDim.x * blockDim.x) {
+        double accr = 0.0;
+        int idx = 0;
+        for (int n = 0; n < nfreq; ++n) {
+            accr += arg[2 * n] * tw[2 * idx] - arg[2 * n + 1] * tw[2 * idx + 1];
+            idx += k;
+            if (idx >= nfft) idx -= nfft;
+        }
+        out[(size_t)ir * nfft + k] = 2.0 * (df * accr);
+    }
+}
+
+int launch_bb_pulse(cudaStream_t st, int nfreq, const double* f, const double* s_src, const double* h, int nr,
+                    const double* t0, int nfft, const double* tw, double* out) {
+    dim3 grid((nfft + 255) / 256, nr);
+    size_t sm = (size_t)2 * nfreq * sizeof(double);
+    if (sm > 48 * 1024) cudaFuncSetAttribute(k_bb_pulse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_bb_pulse<<<grid, 256, sm, st>>>(nfreq, f, s_src, h, nr, t0, nfft, tw, out);
+    return 1;
+}
+
+// source spectrum of a sampled waveform: dt sum_n x_n e^{+2 pi i k n/nfft}
+__global__ void k_src_dft(int n, const double* __restrict__ x, double dt, int nfft, int nfreq,
+                          const double* __restrict__ tw, double* __restrict__ s) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nfreq) return;
+    double ar = 0.0, ai = 0.0;
+    long long idx = 0;
+    const int nn = min(n, nfft);
+    for (int j = 0; j < nn; ++j) {
+        ar += x[j] * tw[2 * idx];
+        ai -= x[j] * tw[2 * idx + 1];  // conjugate twiddle: e^{+i}
+        idx += k;
+        if (idx >= nfft) idx -= nfft;
+    }
+    s[2 * k] = ar * dt;
+    s[2 * k + 1] = ai * dt;
+}
+
+int launch_src_dft(cudaStream_t st, int n, const double* x, double dt, int nfft, int nfreq, const double* tw,
+                   double* s) {
+    k_src_dft<<<(nfreq + 127) / 128, 128, 0, st>>>(n, x, dt, nfft, nfreq, tw, s);
+    return 1;
+}
+
+}  // namespace ncpa

@@ -1,0 +1,118 @@
+// Launchers of the sm_100a kernels of the ESS normal-mode path.  Host code in
+// ncpa_api.cu calls these; each returns the number of kernels it launched.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ncpa {
+
+// error flags written by kernels into the context's device status word
+enum : unsigned {
+    kErrTimeout = 1u,  // a bounded mbarrier wait gave up
+    kErrBracket = 2u,  // bisection bracket inconsistent with the Sturm counts
+    kErrWkb = 4u,      // WKB search needed more trial wavenumbers than threads
+};
+
+// Per (frequency, azimuth) problem, device resident.
+struct ProblemInfo {
+    double freq, omega, az;
+    double k_min, k_max;   // wavenumber window [1/m]
+    double lo, hi;         // window in units of the scaled matrix S = h^2 A
+    double ceff_grnd, ceff_top;
+    unsigned long long ceffmin_bits, ceffmax_bits;  // positive doubles as ordered bits
+    int c_lo, c_hi;        // Sturm counts at lo, hi
+    int M, off;            // number of modes and offset into the mode arrays
+    int used_wkb, pad;
+};
+
+struct WorkItem {
+    int problem;  // problem index
+    int j0;       // first eigen-index inside the problem (0 = lowest k)
+    int m;        // eigenvalues in this item (<= 256)
+    int pad;
+};
+
+constexpr int kScanPoints = 256;  // Sturm counts per problem in the isolation scan
+constexpr int kChunk = 1024;      // doubles per TMA chunk of the diagonal
+constexpr int kBlk = 16;          // eigenvector checkpoint interval
+constexpr int kThreads = 256;     // threads of the bisection / eigenvector CTAs
+
+// knot-level derived quantities
+int launch_steffen(cudaStream_t st, int n, const double* x, const double* y, int batch, int ystride,
+                   double* coef, int cstride);
+int launch_profile_derived(cudaStream_t st, int n, const double* z, const double* u, const double* v,
+                           const double* p, const double* rho, const double* pcoef, const double* rcoef,
+                           int have_c0, double* c0, double* ws, double* wd);
+int launch_ceff_knots(cudaStream_t st, int n, int n_az, const double* az, const double* c0, const double* ws,
+                      const double* wd, double* ceff);
+int launch_alpha_knots(cudaStream_t st, int n, int n_f, const double* freqs, const double* z, const double* t,
+                       const double* p, const double* rho, double* alpha);
+// grid sampling of the frequency-independent fields: rho, P on the grid and
+// c_T = sqrt(1.4 P / rho)
+int launch_grid_common(cudaStream_t st, int nk, const double* zk, const double* rho, const double* rcoef,
+                       const double* p, const double* pcoef, int nz, double z_min, double dz_grid,
+                       double* rho_g, double* ct_g);
+// attenuation weight w = 2 alpha omega / c_T for every frequency [n_f x nz]
+int launch_attn_weight(cudaStream_t st, int nk, const double* zk, const double* alpha, const double* acoef,
+                       int n_f, const double* freqs, int nz, double z_min, double dz_grid, const double* ct_g,
+                       double* w, int wstride);
+// matrix build (K1): s [P x nz_pad], optional kz2 = (omega/c)^2 and
+// g = 1/c^2 [P x nz]; fills ceff extrema / ground / top in ProblemInfo
+int launch_build_matrix(cudaStream_t st, int nk, const double* zk, const double* ceffk, const double* ceffcoef,
+                        int n_az, int P, ProblemInfo* pinfo, int nz, int nz_pad, double z_min, double dz_grid,
+                        double dz, double admittance, double* s, double* kz2, double* g);
+// WKB window and scaled bounds (K2)
+int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2, int nz, double dz,
+                  int wkb, int wvnum, double c_min, double c_max, unsigned* err);
+// isolation scan: kScanPoints Sturm counts per problem (K3a)
+int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
+                int* counts, unsigned* err);
+// multisection/bisection over work items (K3)
+int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
+                  const int* counts, const WorkItem* items, int n_items, int* counter, double tol, double* mu,
+                  unsigned* err);
+// twisted-factorisation eigenvectors + fused reductions (K4)
+struct EigvecArgs {
+    const ProblemInfo* pinfo;
+    const double* s;
+    const double* w;   // [n_f x wstride]
+    const double* g;   // [P x nz] or null
+    int nz, nz_pad, wstride, n_az;
+    const WorkItem* items;
+    int n_items;
+    int* counter;
+    const double* mu;
+    int isrc, ircv;
+    double dz, h2;
+    double* kr;
+    double* ki;
+    double* vs;
+    double* vr;
+    double* vg;
+    double* vfull;            // optional: per problem [nz x M] at vfull_off[p]
+    const long long* vfull_off;
+    double* ck_q1;            // checkpoint scratch, per CTA slot
+    double* ck_q2;
+    int* ck_e;
+    long long ck_slot_stride; // elements per slot
+    unsigned* err;
+};
+int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a);
+// modal sums
+int launch_tl1d(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* kr, const double* ki,
+                const double* vs, const double* vr, int nr, double dr, int lossless, double* re, double* im,
+                double* incoh);
+int launch_tl2d(cudaStream_t st, int M, const double* kr, const double* ki, const double* vs_src,
+                const double* vz, int nzo, int nr, double dr, int lossless, double* re, double* im);
+// broadband synthesis
+int launch_twiddle(cudaStream_t st, int nfft, double* tw);
+int launch_bb_transfer(cudaStream_t st, int nfreq, const int* off, const double* re_k, const double* im_k,
+                       const double* vs, const double* vr, double rho_ratio, int nr, const double* ranges,
+                       int zero_attn, double* h);
+int launch_bb_pulse(cudaStream_t st, int nfreq, const double* f, const double* s_src, const double* h, int nr,
+                    const double* t0, int nfft, const double* tw, double* out);
+int launch_src_dft(cudaStream_t st, int n, const double* x, double dt, int nfft, int nfreq, const double* tw,
+                   double* s);
+
+}  // namespace ncpa

@@ -1,0 +1,869 @@
+// C ABI of the B200 ESS normal-mode library (include/ncpa_gpu.h): context,
+// resident profiles, the batched (frequency x azimuth) eigen-solve, modal
+// sums and ModBB synthesis.  Host orchestration only; all arithmetic on the
+// path runs in the kernels of kernels.cu.
+#include "ncpa_gpu.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "atmosphere.hpp"
+#include "kernels.hpp"
+
+using ncpa::ProblemInfo;
+using ncpa::WorkItem;
+
+namespace {
+
+constexpr double kPi = 3.141592653589793;
+constexpr double kBisectTol = 1.0e-15;  // bracket width, units of S = h^2 A
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct ApiError : std::runtime_error {
+    ncpa_status code;
+    ApiError(ncpa_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+    } while (0)
+
+// owning device buffer
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) {
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            o.p = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void alloc(size_t b) {
+        if (b <= bytes && p) return;
+        release();
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            throw ApiError(NCPA_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        bytes = b;
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+template <class T>
+void upload(DevBuf& d, const std::vector<T>& h, cudaStream_t st) {
+    d.alloc(h.size() * sizeof(T));
+    if (!h.empty()) CK(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+template <class T>
+void upload(DevBuf& d, const T* h, size_t n, cudaStream_t st) {
+    d.alloc(n * sizeof(T));
+    if (n) CK(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+}  // namespace
+
+struct ncpa_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    long long launches = 0;
+    int num_sms = 148;
+    DevBuf d_err;                  // device status word
+    DevBuf ck1, ck2, cke;          // eigenvector checkpoint scratch
+    std::map<int, DevBuf> twiddle; // per nfft
+    void count(int n) { launches += n; }
+};
+
+struct ncpa_profile {
+    ncpa_ctx* ctx = nullptr;
+    int n = 0;
+    DevBuf z, u, v, t, p, rho, c0, ws, wd, pcoef, rcoef, attn;
+    bool has_attn = false;
+    double z0 = 0.0;
+    int has_z0 = 0;
+    double z_lo = 0.0, z_hi = 0.0;
+};
+
+struct ncpa_modes {
+    ncpa_ctx* ctx = nullptr;
+    int P = 0, nf = 0, na = 0, nz = 0, nz_pad = 0;
+    ncpa_ess_params prm{};
+    std::vector<double> freqs, az;
+    double z_min = 0, dz_grid = 0, dz = 0;
+    int isrc = 0, ircv = 0;
+    double rho_src = 1.0, rho_rcv = 1.0;
+    std::vector<ProblemInfo> info;
+    int Mtot = 0;
+    DevBuf d_pinfo, d_kr, d_ki, d_vs, d_vr, d_vg, d_vfull, d_vfull_off;
+    std::vector<double> kr, ki, vs, vr, vg;
+    std::vector<long long> vfull_off;
+};
+
+namespace {
+
+ncpa_status fail(ncpa_ctx* ctx, ncpa_status s, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return s;
+}
+
+template <class F>
+ncpa_status guarded(ncpa_ctx* ctx, F&& f) {
+    try {
+        return f();
+    } catch (const ApiError& e) {
+        return fail(ctx, e.code, e.what());
+    } catch (const ncpa::ParseError& e) {
+        return fail(ctx, NCPA_EPARSE, e.what());
+    } catch (const CudaError& e) {
+        return fail(ctx, NCPA_ECUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(ctx, NCPA_ENOMEM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(ctx, NCPA_EINVAL, e.what());
+    }
+}
+
+void check_launch(ncpa_ctx* ctx, int n) {
+    if (n < 0) throw ApiError(NCPA_EINVAL, "kernel launch rejected its arguments");
+    ctx->count(n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw CudaError(std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+void check_device_status(ncpa_ctx* ctx) {
+    unsigned h = 0;
+    CK(cudaMemcpyAsync(&h, ctx->d_err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h) {
+        CK(cudaMemsetAsync(ctx->d_err.p, 0, sizeof(unsigned), ctx->stream));
+        if (h & ncpa::kErrTimeout) throw ApiError(NCPA_ETIMEDOUT, "a bounded device wait gave up");
+        if (h & ncpa::kErrBracket) throw ApiError(NCPA_ECUDA, "bisection bracket inconsistent with Sturm counts");
+        if (h & ncpa::kErrWkb) throw ApiError(NCPA_ECUDA, "WKB window search exceeded its trial count");
+    }
+}
+
+const double* twiddle(ncpa_ctx* ctx, int nfft) {
+    auto it = ctx->twiddle.find(nfft);
+    if (it != ctx->twiddle.end()) return it->second.as<double>();
+    DevBuf b;
+    b.alloc((size_t)2 * nfft * sizeof(double));
+    check_launch(ctx, ncpa::launch_twiddle(ctx->stream, nfft, b.as<double>()));
+    const double* p = b.as<double>();
+    ctx->twiddle.emplace(nfft, std::move(b));
+    return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ncpa_status_str(ncpa_status s) {
+    switch (s) {
+        case NCPA_OK: return "ok";
+        case NCPA_EINVAL: return "invalid argument";
+        case NCPA_ENOMEM: return "out of memory";
+        case NCPA_ECUDA: return "CUDA error";
+        case NCPA_EPARSE: return "parse error";
+        case NCPA_ETOOMANY: return "too many modes";
+        case NCPA_EIO: return "I/O error";
+        case NCPA_ETIMEDOUT: return "device wait timed out";
+        case NCPA_ENODEV: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+const char* ncpa_last_error(const ncpa_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+long long ncpa_kernel_launches(const ncpa_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
+    if (!out) return NCPA_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return NCPA_ENODEV;
+    auto ctx = std::make_unique<ncpa_ctx>();
+    ctx->device = opts ? opts->device : 0;
+    if (ctx->device < 0 || ctx->device >= ndev) return NCPA_EINVAL;
+    ncpa_status s = guarded(ctx.get(), [&]() -> ncpa_status {
+        CK(cudaSetDevice(ctx->device));
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, ctx->device));
+        if (prop.major < 10) throw ApiError(NCPA_ENODEV, "this library is built for sm_100a (B200)");
+        ctx->num_sms = prop.multiProcessorCount;
+        CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->d_err.alloc(sizeof(unsigned));
+        CK(cudaMemsetAsync(ctx->d_err.p, 0, sizeof(unsigned), ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return NCPA_OK;
+    });
+    if (s != NCPA_OK) return s;
+    *out = ctx.release();
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_ctx_destroy(ncpa_ctx* ctx) {
+    if (!ctx) return NCPA_EINVAL;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->twiddle.clear();
+    ctx->ck1.release();
+    ctx->ck2.release();
+    ctx->cke.release();
+    ctx->d_err.release();
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_ctx_synchronize(ncpa_ctx* ctx) {
+    if (!ctx) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        CK(cudaStreamSynchronize(ctx->stream));
+        return NCPA_OK;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// profiles
+// ---------------------------------------------------------------------------
+ncpa_status ncpa_profile_create(ncpa_ctx* ctx, const ncpa_profile_desc* d, ncpa_profile** out) {
+    if (!ctx || !d || !out) return NCPA_EINVAL;
+    *out = nullptr;
+    return guarded(ctx, [&]() -> ncpa_status {
+        const int n = d->n_knots;
+        if (n < 3) throw ApiError(NCPA_EINVAL, "profile needs at least 3 knots");
+        if (!d->z || !d->u || !d->v || !d->t || !d->p || !d->rho)
+            throw ApiError(NCPA_EINVAL, "profile arrays z, u, v, t, p, rho are required");
+        for (int i = 1; i < n; ++i)
+            if (!(d->z[i] > d->z[i - 1])) throw ApiError(NCPA_EINVAL, "profile altitudes must increase strictly");
+        CK(cudaSetDevice(ctx->device));
+        auto P = std::make_unique<ncpa_profile>();
+        P->ctx = ctx;
+        P->n = n;
+        cudaStream_t st = ctx->stream;
+        upload(P->z, d->z, n, st);
+        upload(P->u, d->u, n, st);
+        upload(P->v, d->v, n, st);
+        upload(P->t, d->t, n, st);
+        upload(P->p, d->p, n, st);
+        upload(P->rho, d->rho, n, st);
+        P->c0.alloc(n * sizeof(double));
+        if (d->c0) CK(cudaMemcpyAsync(P->c0.p, d->c0, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        P->ws.alloc(n * sizeof(double));
+        P->wd.alloc(n * sizeof(double));
+        P->pcoef.alloc(4 * (n - 1) * sizeof(double));
+        P->rcoef.alloc(4 * (n - 1) * sizeof(double));
+        check_launch(ctx, ncpa::launch_steffen(st, n, P->z.as<double>(), P->p.as<double>(), 1, n,
+                                               P->pcoef.as<double>(), 4 * (n - 1)));
+        check_launch(ctx, ncpa::launch_steffen(st, n, P->z.as<double>(), P->rho.as<double>(), 1, n,
+                                               P->rcoef.as<double>(), 4 * (n - 1)));
+        check_launch(ctx, ncpa::launch_profile_derived(st, n, P->z.as<double>(), P->u.as<double>(),
+                                                       P->v.as<double>(), P->p.as<double>(), P->rho.as<double>(),
+                                                       P->pcoef.as<double>(), P->rcoef.as<double>(),
+                                                       d->c0 ? 1 : 0, P->c0.as<double>(), P->ws.as<double>(),
+                                                       P->wd.as<double>()));
+        if (d->attn) {
+            upload(P->attn, d->attn, n, st);
+            P->has_attn = true;
+        }
+        P->z0 = d->z0_m;
+        P->has_z0 = d->has_z0;
+        P->z_lo = d->z[0];
+        P->z_hi = d->z[n - 1];
+        CK(cudaStreamSynchronize(st));
+        *out = P.release();
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_profile_load(ncpa_ctx* ctx, const char* path, const char* header_path, ncpa_profile** out) {
+    if (!ctx || !path || !out) return NCPA_EINVAL;
+    *out = nullptr;
+    ncpa::SiProfile S;
+    ncpa_status s = guarded(ctx, [&]() -> ncpa_status {
+        auto parsed = ncpa::read_profile(path, header_path ? header_path : "");
+        S = ncpa::to_si_profile(parsed);
+        return NCPA_OK;
+    });
+    if (s != NCPA_OK) return s;
+    ncpa_profile_desc d{};
+    d.n_knots = (int)S.z.size();
+    d.z = S.z.data();
+    d.u = S.u.data();
+    d.v = S.v.data();
+    d.t = S.t.data();
+    d.p = S.p.data();
+    d.rho = S.rho.data();
+    d.c0 = S.has_c0 ? S.c0.data() : nullptr;
+    d.attn = nullptr;
+    d.z0_m = S.z0;
+    d.has_z0 = S.has_z0;
+    return ncpa_profile_create(ctx, &d, out);
+}
+
+ncpa_status ncpa_profile_destroy(ncpa_profile* prof) {
+    if (!prof) return NCPA_EINVAL;
+    cudaSetDevice(prof->ctx->device);
+    cudaStreamSynchronize(prof->ctx->stream);
+    delete prof;
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_profile_info(const ncpa_profile* prof, int* n, double* z_lo, double* z_hi) {
+    if (!prof) return NCPA_EINVAL;
+    if (n) *n = prof->n;
+    if (z_lo) *z_lo = prof->z_lo;
+    if (z_hi) *z_hi = prof->z_hi;
+    return NCPA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batched ESS solve
+// ---------------------------------------------------------------------------
+void ncpa_ess_params_default(ncpa_ess_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->nz_grid = 20000;
+    p->maxheight_km = 150.0;
+    p->max_modes = 4000;
+}
+
+ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_ess_params* prm,
+                           const double* freqs, int n_freq, const double* az_deg, int n_az, ncpa_modes** out) {
+    if (!ctx || !prof || !prm || !freqs || !az_deg || !out) return NCPA_EINVAL;
+    *out = nullptr;
+    return guarded(ctx, [&]() -> ncpa_status {
+        if (n_freq < 1 || n_az < 1) throw ApiError(NCPA_EINVAL, "need at least one frequency and azimuth");
+        if (prm->nz_grid < 10) throw ApiError(NCPA_EINVAL, "Nz_grid must be >= 10");
+        for (int i = 0; i < n_freq; ++i)
+            if (!(freqs[i] > 0.0)) throw ApiError(NCPA_EINVAL, "frequencies must be positive");
+        if (prm->wvnum_filter && !(prm->c_min > 0.0 && prm->c_max > 0.0))
+            throw ApiError(NCPA_EINVAL, "wvnum_filter needs c_min > 0 and c_max > 0");
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        auto M = std::make_unique<ncpa_modes>();
+        M->ctx = ctx;
+        M->prm = *prm;
+        if (M->prm.max_modes <= 0) M->prm.max_modes = 4000;
+        M->nf = n_freq;
+        M->na = n_az;
+        M->P = n_freq * n_az;
+        M->freqs.assign(freqs, freqs + n_freq);
+        M->az.assign(az_deg, az_deg + n_az);
+        const int nz = prm->nz_grid;
+        const int nz_pad = ((nz + ncpa::kChunk - 1) / ncpa::kChunk) * ncpa::kChunk;
+        M->nz = nz;
+        M->nz_pad = nz_pad;
+        // grid geometry (ESSModeSolver.cpp:39-41, 144-151, 212-220, 314)
+        double z_min = prm->zground_km * 1000.0;
+        double maxheight = prm->maxheight_km * 1000.0;
+        if (maxheight >= prof->z_hi) maxheight = prof->z_hi - 1e-6;
+        const double dz_grid = (maxheight - z_min) / (nz - 1);
+        if (prof->has_z0 && z_min < prof->z0) z_min = prof->z0;
+        const double dz = (maxheight - z_min) / (nz - 1);
+        if (!(dz > 0.0)) throw ApiError(NCPA_EINVAL, "maxheight must lie above the ground");
+        M->z_min = z_min;
+        M->dz_grid = dz_grid;
+        M->dz = dz;
+        const double src_h = prm->sourceheight_km * 1000.0, rcv_h = prm->receiverheight_km * 1000.0;
+        M->isrc = (int)std::ceil(src_h / dz);
+        M->ircv = (int)std::ceil(rcv_h / dz);
+        if (M->isrc < 0 || M->isrc >= nz || M->ircv < 0 || M->ircv >= nz)
+            throw ApiError(NCPA_EINVAL, "source/receiver height outside the grid");
+        const int nk = prof->n;
+        const int P = M->P;
+
+        // ---- knot-level fields ----
+        DevBuf d_freqs, d_az;
+        upload(d_freqs, freqs, n_freq, st);
+        upload(d_az, az_deg, n_az, st);
+        DevBuf ceffk, ceffc, alpha, alphac;
+        ceffk.alloc((size_t)n_az * nk * 8);
+        ceffc.alloc((size_t)n_az * 4 * (nk - 1) * 8);
+        check_launch(ctx, ncpa::launch_ceff_knots(st, nk, n_az, d_az.as<double>(), prof->c0.as<double>(),
+                                                  prof->ws.as<double>(), prof->wd.as<double>(), ceffk.as<double>()));
+        check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), ceffk.as<double>(), n_az, nk,
+                                               ceffc.as<double>(), 4 * (nk - 1)));
+        const int n_alpha = prof->has_attn ? 1 : n_freq;
+        alpha.alloc((size_t)n_freq * nk * 8);
+        alphac.alloc((size_t)n_freq * 4 * (nk - 1) * 8);
+        if (prof->has_attn) {
+            for (int f = 0; f < n_freq; ++f)
+                CK(cudaMemcpyAsync(alpha.as<double>() + (size_t)f * nk, prof->attn.p, nk * 8,
+                                   cudaMemcpyDeviceToDevice, st));
+        } else {
+            check_launch(ctx, ncpa::launch_alpha_knots(st, nk, n_freq, d_freqs.as<double>(), prof->z.as<double>(),
+                                                       prof->t.as<double>(), prof->p.as<double>(),
+                                                       prof->rho.as<double>(), alpha.as<double>()));
+        }
+        (void)n_alpha;
+        check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), alpha.as<double>(), n_freq, nk,
+                                               alphac.as<double>(), 4 * (nk - 1)));
+        // ---- grid fields ----
+        DevBuf rho_g, ct_g, w;
+        rho_g.alloc((size_t)nz * 8);
+        ct_g.alloc((size_t)nz * 8);
+        w.alloc((size_t)n_freq * nz_pad * 8);
+        CK(cudaMemsetAsync(w.p, 0, (size_t)n_freq * nz_pad * 8, st));
+        check_launch(ctx, ncpa::launch_grid_common(st, nk, prof->z.as<double>(), prof->rho.as<double>(),
+                                                   prof->rcoef.as<double>(), prof->p.as<double>(),
+                                                   prof->pcoef.as<double>(), nz, z_min, dz_grid, rho_g.as<double>(),
+                                                   ct_g.as<double>()));
+        check_launch(ctx, ncpa::launch_attn_weight(st, nk, prof->z.as<double>(), alpha.as<double>(),
+                                                   alphac.as<double>(), n_freq, d_freqs.as<double>(), nz, z_min,
+                                                   dz_grid, ct_g.as<double>(), w.as<double>(), nz_pad));
+        // admittance for the Lamb wave condition: -rho'(z0) / (2 rho(z0))
+        double admittance = 0.0;
+        std::vector<double> hrho(nz);
+        CK(cudaMemcpyAsync(hrho.data(), rho_g.p, nz * 8, cudaMemcpyDeviceToHost, st));
+        if (prm->lamb_wave_bc) {
+            std::vector<double> hz(nk), hc(4 * (nk - 1)), hr(nk);
+            CK(cudaMemcpyAsync(hz.data(), prof->z.p, nk * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(hr.data(), prof->rho.p, nk * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(hc.data(), prof->rcoef.p, hc.size() * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            // one point of the rho spline and its slope (scalar set-up, as in
+            // ESSModeSolver.cpp:347-349)
+            double zq = z_min, val, der;
+            if (zq > hz[nk - 1] || zq < hz[0]) {
+                val = zq > hz[nk - 1] ? hr[nk - 1] : hr[0];
+                der = 0.0;
+            } else {
+                int lo = 0, hi = nk - 1;
+                while (hi > lo + 1) {
+                    int mid = (lo + hi) / 2;
+                    if (hz[mid] > zq) hi = mid; else lo = mid;
+                }
+                const double* c = &hc[4 * lo];
+                double t = zq - hz[lo];
+                val = c[3] + t * (c[2] + t * (c[1] + t * c[0]));
+                der = c[2] + t * (2.0 * c[1] + t * 3.0 * c[0]);
+            }
+            admittance = -der / val / 2.0;
+        }
+        // ---- per-problem info ----
+        M->info.assign(P, ProblemInfo{});
+        for (int f = 0; f < n_freq; ++f)
+            for (int a = 0; a < n_az; ++a) {
+                ProblemInfo& pi = M->info[f * n_az + a];
+                pi.freq = freqs[f];
+                pi.omega = 2 * kPi * freqs[f];
+                pi.az = az_deg[a];
+                pi.ceffmin_bits = 0x7ff0000000000000ull;
+                pi.ceffmax_bits = 0ull;
+            }
+        upload(M->d_pinfo, M->info, st);
+        ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
+        // ---- K1 matrix ----
+        const bool wkb = !prm->turnoff_wkb && std::fabs(src_h) < 1.0e-3 && std::fabs(rcv_h) < 1.0e-3;
+        DevBuf s, kz2, g;
+        s.alloc((size_t)P * nz_pad * 8);
+        if (wkb) kz2.alloc((size_t)P * nz * 8);
+        if (prm->want_group_speed) g.alloc((size_t)P * nz_pad * 8);
+        check_launch(ctx, ncpa::launch_build_matrix(st, nk, prof->z.as<double>(), ceffk.as<double>(),
+                                                    ceffc.as<double>(), n_az, P, d_pinfo, nz, nz_pad, z_min, dz_grid,
+                                                    dz, admittance, s.as<double>(), wkb ? kz2.as<double>() : nullptr,
+                                                    prm->want_group_speed ? g.as<double>() : nullptr));
+        // ---- K2 window ----
+        check_launch(ctx, ncpa::launch_window(st, P, d_pinfo, wkb ? kz2.as<double>() : nullptr, nz, dz, wkb ? 1 : 0,
+                                              prm->wvnum_filter, prm->c_min, prm->c_max, ctx->d_err.as<unsigned>()));
+        // ---- K3a scan ----
+        DevBuf counts;
+        counts.alloc((size_t)P * ncpa::kScanPoints * 4);
+        check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
+                                            ctx->d_err.as<unsigned>()));
+        std::vector<int> hcounts((size_t)P * ncpa::kScanPoints);
+        CK(cudaMemcpyAsync(hcounts.data(), counts.p, hcounts.size() * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(M->info.data(), d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
+        check_device_status(ctx);
+        // ---- modes per problem, offsets, work items ----
+        std::vector<WorkItem> items;
+        int off = 0;
+        for (int p = 0; p < P; ++p) {
+            ProblemInfo& pi = M->info[p];
+            pi.c_lo = hcounts[(size_t)p * ncpa::kScanPoints];
+            pi.c_hi = hcounts[(size_t)p * ncpa::kScanPoints + ncpa::kScanPoints - 1];
+            pi.M = std::max(0, pi.c_hi - pi.c_lo);
+            if (pi.M > M->prm.max_modes) {
+                char buf[160];
+                std::snprintf(buf, sizeof buf, "problem %d (f=%g Hz, az=%g) has %d modes > max_modes %d", p, pi.freq,
+                              pi.az, pi.M, M->prm.max_modes);
+                throw ApiError(NCPA_ETOOMANY, buf);
+            }
+            pi.off = off;
+            off += pi.M;
+            const int nit = (pi.M + ncpa::kThreads - 1) / ncpa::kThreads;
+            for (int k = 0; k < nit; ++k) {
+                int j0 = (int)((long long)pi.M * k / nit), j1 = (int)((long long)pi.M * (k + 1) / nit);
+                items.push_back(WorkItem{p, j0, j1 - j0, 0});
+            }
+        }
+        M->Mtot = off;
+        // largest items first: they need the most multisection rounds
+        std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.m > b.m; });
+        CK(cudaMemcpyAsync(d_pinfo, M->info.data(), P * sizeof(ProblemInfo), cudaMemcpyHostToDevice, st));
+        const int Mt = std::max(1, M->Mtot);
+        DevBuf mu, d_items, d_counter;
+        mu.alloc((size_t)Mt * 8);
+        M->d_kr.alloc((size_t)Mt * 8);
+        M->d_ki.alloc((size_t)Mt * 8);
+        M->d_vs.alloc((size_t)Mt * 8);
+        M->d_vr.alloc((size_t)Mt * 8);
+        M->d_vg.alloc((size_t)Mt * 8);
+        if (prm->want_vectors) {
+            M->vfull_off.resize(P);
+            long long acc = 0;
+            for (int p = 0; p < P; ++p) {
+                M->vfull_off[p] = acc;
+                acc += (long long)M->info[p].M * nz;
+            }
+            M->d_vfull.alloc((size_t)std::max(1LL, acc) * 8);
+            upload(M->d_vfull_off, M->vfull_off, st);
+        }
+        const int n_items = (int)items.size();
+        if (n_items > 0) {
+            upload(d_items, items, st);
+            d_counter.alloc(2 * sizeof(int));
+            CK(cudaMemsetAsync(d_counter.p, 0, 2 * sizeof(int), st));
+            // ---- K3 bisection ----
+            int grid_b = std::min(n_items, ctx->num_sms * 4);
+            check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
+                                                  d_items.as<WorkItem>(), n_items, d_counter.as<int>(), kBisectTol,
+                                                  mu.as<double>(), ctx->d_err.as<unsigned>()));
+            // ---- K4 eigenvectors ----
+            int grid_e = std::min(n_items, ctx->num_sms * 2);
+            const long long nblk = (nz + ncpa::kBlk - 1) / ncpa::kBlk;
+            const long long slot = nblk * ncpa::kThreads;
+            const size_t need = (size_t)grid_e * slot;
+            if (ctx->ck1.bytes < need * 8) {
+                ctx->ck1.alloc(need * 8);
+                ctx->ck2.alloc(need * 8);
+                ctx->cke.alloc(need * 4);
+            }
+            ncpa::EigvecArgs ea{};
+            ea.pinfo = d_pinfo;
+            ea.s = s.as<double>();
+            ea.w = w.as<double>();
+            ea.g = prm->want_group_speed ? g.as<double>() : nullptr;
+            ea.nz = nz;
+            ea.nz_pad = nz_pad;
+            ea.wstride = nz_pad;
+            ea.n_az = n_az;
+            ea.items = d_items.as<WorkItem>();
+            ea.n_items = n_items;
+            ea.counter = d_counter.as<int>() + 1;
+            ea.mu = mu.as<double>();
+            ea.isrc = M->isrc;
+            ea.ircv = M->ircv;
+            ea.dz = dz;
+            ea.h2 = dz * dz;
+            ea.kr = M->d_kr.as<double>();
+            ea.ki = M->d_ki.as<double>();
+            ea.vs = M->d_vs.as<double>();
+            ea.vr = M->d_vr.as<double>();
+            ea.vg = M->d_vg.as<double>();
+            ea.vfull = prm->want_vectors ? M->d_vfull.as<double>() : nullptr;
+            ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
+            ea.ck_q1 = ctx->ck1.as<double>();
+            ea.ck_q2 = ctx->ck2.as<double>();
+            ea.ck_e = ctx->cke.as<int>();
+            ea.ck_slot_stride = slot;
+            ea.err = ctx->d_err.as<unsigned>();
+            check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
+        }
+        // ---- results to host ----
+        M->kr.resize(M->Mtot);
+        M->ki.resize(M->Mtot);
+        M->vs.resize(M->Mtot);
+        M->vr.resize(M->Mtot);
+        M->vg.resize(M->Mtot);
+        if (M->Mtot > 0) {
+            CK(cudaMemcpyAsync(M->kr.data(), M->d_kr.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(M->ki.data(), M->d_ki.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(M->vs.data(), M->d_vs.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(M->vr.data(), M->d_vr.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(M->vg.data(), M->d_vg.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
+        }
+        check_device_status(ctx);
+        M->rho_src = hrho[M->isrc];
+        M->rho_rcv = hrho[M->ircv];
+        *out = M.release();
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_modes_destroy(ncpa_modes* m) {
+    if (!m) return NCPA_EINVAL;
+    cudaSetDevice(m->ctx->device);
+    cudaStreamSynchronize(m->ctx->stream);
+    delete m;
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_modes_problems(const ncpa_modes* m, int* n) {
+    if (!m || !n) return NCPA_EINVAL;
+    *n = m->P;
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_modes_count(const ncpa_modes* m, int problem, int* n) {
+    if (!m || !n || problem < 0 || problem >= m->P) return NCPA_EINVAL;
+    *n = m->info[problem].M;
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_modes_info(const ncpa_modes* m, int problem, double* freq, double* az, double* dz, double* k_min,
+                            double* k_max, double* rho_src, double* rho_rcv) {
+    if (!m || problem < 0 || problem >= m->P) return NCPA_EINVAL;
+    const ProblemInfo& pi = m->info[problem];
+    if (freq) *freq = pi.freq;
+    if (az) *az = pi.az;
+    if (dz) *dz = m->dz;
+    if (k_min) *k_min = pi.k_min;
+    if (k_max) *k_max = pi.k_max;
+    if (rho_src) *rho_src = m->rho_src;
+    if (rho_rcv) *rho_rcv = m->rho_rcv;
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_modes_get(const ncpa_modes* m, int problem, double* re_k, double* im_k, double* v_src,
+                           double* v_rcv, double* v_group) {
+    if (!m || problem < 0 || problem >= m->P) return NCPA_EINVAL;
+    const ProblemInfo& pi = m->info[problem];
+    const size_t o = pi.off, n = pi.M;
+    if (re_k) std::memcpy(re_k, m->kr.data() + o, n * 8);
+    if (im_k) std::memcpy(im_k, m->ki.data() + o, n * 8);
+    if (v_src) std::memcpy(v_src, m->vs.data() + o, n * 8);
+    if (v_rcv) std::memcpy(v_rcv, m->vr.data() + o, n * 8);
+    if (v_group) std::memcpy(v_group, m->vg.data() + o, n * 8);
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_modes_get_vectors(const ncpa_modes* m, int problem, double* v) {
+    if (!m || !v || problem < 0 || problem >= m->P) return NCPA_EINVAL;
+    if (!m->prm.want_vectors) return fail(m->ctx, NCPA_EINVAL, "solve was run without want_vectors");
+    return guarded(m->ctx, [&]() -> ncpa_status {
+        const size_t n = (size_t)m->info[problem].M * m->nz;
+        if (n) {
+            CK(cudaMemcpyAsync(v, m->d_vfull.as<double>() + m->vfull_off[problem], n * 8, cudaMemcpyDeviceToHost,
+                               m->ctx->stream));
+            CK(cudaStreamSynchronize(m->ctx->stream));
+        }
+        return NCPA_OK;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// transmission loss
+// ---------------------------------------------------------------------------
+ncpa_status ncpa_tl_1d(ncpa_ctx* ctx, const ncpa_modes* m, const ncpa_tl_params* tp, double* re, double* im,
+                       double* incoh) {
+    if (!ctx || !m || !tp || !re || !im || !incoh) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        if (tp->n_ranges < 1 || !(tp->dr_m > 0)) throw ApiError(NCPA_EINVAL, "bad range grid");
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        const size_t n = (size_t)m->P * tp->n_ranges;
+        DevBuf dre, dim, dinc;
+        dre.alloc(n * 8);
+        dim.alloc(n * 8);
+        dinc.alloc(n * 8);
+        check_launch(ctx, ncpa::launch_tl1d(st, m->P, m->d_pinfo.as<ProblemInfo>(), m->d_kr.as<double>(),
+                                            m->d_ki.as<double>(), m->d_vs.as<double>(), m->d_vr.as<double>(),
+                                            tp->n_ranges, tp->dr_m, tp->lossless, dre.as<double>(), dim.as<double>(),
+                                            dinc.as<double>()));
+        CK(cudaMemcpyAsync(re, dre.p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(im, dim.p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(incoh, dinc.p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_tl_2d_heights(const ncpa_modes* m, int problem, int* n_heights) {
+    if (!m || !n_heights || problem < 0 || problem >= m->P) return NCPA_EINVAL;
+    int stepj = m->nz / 500;
+    if (stepj == 0) stepj = 10;
+    *n_heights = (m->nz + stepj - 1) / stepj;
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_tl_2d(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const ncpa_tl_params* tp, double* z_out,
+                       double* re, double* im) {
+    if (!ctx || !m || !tp || !re || !im || problem < 0 || problem >= m->P) return NCPA_EINVAL;
+    if (!m->prm.want_vectors) return fail(ctx, NCPA_EINVAL, "2-D TL needs a solve with want_vectors");
+    return guarded(ctx, [&]() -> ncpa_status {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        const ProblemInfo& pi = m->info[problem];
+        const int Mm = pi.M, nz = m->nz;
+        int stepj = nz / 500;
+        if (stepj == 0) stepj = 10;
+        const int nzo = (nz + stepj - 1) / stepj;
+        if (nzo > 1024) throw ApiError(NCPA_EINVAL, "too many output heights");
+        // rows of the sampled heights, the source row, gathered on the host
+        std::vector<double> vfull((size_t)Mm * nz), vz((size_t)nzo * Mm), vsrc(Mm);
+        if (Mm)
+            CK(cudaMemcpyAsync(vfull.data(), m->d_vfull.as<double>() + m->vfull_off[problem], vfull.size() * 8,
+                               cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int j = 0; j < nzo; ++j) {
+            std::memcpy(&vz[(size_t)j * Mm], &vfull[(size_t)j * stepj * Mm], Mm * 8);
+            if (z_out) z_out[j] = (j * stepj) * m->dz;
+        }
+        if (Mm) std::memcpy(vsrc.data(), &vfull[(size_t)m->isrc * Mm], Mm * 8);
+        DevBuf dvz, dvs, dre, dim;
+        upload(dvz, vz, st);
+        upload(dvs, vsrc, st);
+        const size_t n = (size_t)tp->n_ranges * nzo;
+        dre.alloc(n * 8);
+        dim.alloc(n * 8);
+        check_launch(ctx, ncpa::launch_tl2d(st, Mm, m->d_kr.as<double>() + pi.off, m->d_ki.as<double>() + pi.off,
+                                            dvs.as<double>(), dvz.as<double>(), nzo, tp->n_ranges, tp->dr_m,
+                                            tp->lossless, dre.as<double>(), dim.as<double>()));
+        CK(cudaMemcpyAsync(re, dre.p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(im, dim.p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return NCPA_OK;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// broadband synthesis
+// ---------------------------------------------------------------------------
+namespace {
+ncpa_status bb_common(ncpa_ctx* ctx, int nfreq, const double* d_f, const int* d_off, const double* d_rk,
+                      const double* d_ik, const double* d_vs, const double* d_vr, double rho_ratio,
+                      const ncpa_bb_params* bp, double* waveforms) {
+    cudaStream_t st = ctx->stream;
+    if (bp->n_ranges < 1 || !bp->ranges_m || bp->nfft < nfreq || !(bp->max_celerity > 0) || !bp->src_re ||
+        !bp->src_im)
+        throw ApiError(NCPA_EINVAL, "bad broadband parameters (need nfft >= n_freq, ranges, source spectrum)");
+    const int nr = bp->n_ranges, nfft = bp->nfft;
+    std::vector<double> t0(nr), src(2 * (size_t)nfreq);
+    for (int i = 0; i < nr; ++i) t0[i] = 0.0 + bp->ranges_m[i] / bp->max_celerity;
+    for (int i = 0; i < nfreq; ++i) {
+        src[2 * i] = bp->src_re[i];
+        src[2 * i + 1] = bp->src_im[i];
+    }
+    DevBuf dr, dt0, dsrc, dh, dout;
+    upload(dr, bp->ranges_m, nr, st);
+    upload(dt0, t0, st);
+    upload(dsrc, src, st);
+    dh.alloc((size_t)nr * nfreq * 16);
+    dout.alloc((size_t)nr * nfft * 8);
+    const double* tw = twiddle(ctx, nfft);
+    check_launch(ctx, ncpa::launch_bb_transfer(st, nfreq, d_off, d_rk, d_ik, d_vs, d_vr, rho_ratio, nr,
+                                               dr.as<double>(), bp->zero_attn, dh.as<double>()));
+    check_launch(ctx, ncpa::launch_bb_pulse(st, nfreq, d_f, dsrc.as<double>(), dh.as<double>(), nr, dt0.as<double>(),
+                                            nfft, tw, dout.as<double>()));
+    CK(cudaMemcpyAsync(waveforms, dout.p, (size_t)nr * nfft * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return NCPA_OK;
+}
+}  // namespace
+
+ncpa_status ncpa_bb_synthesize(ncpa_ctx* ctx, const ncpa_dispersion_desc* d, const ncpa_bb_params* bp,
+                               double* waveforms) {
+    if (!ctx || !d || !bp || !waveforms) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        if (d->n_freq < 3 || !d->f || !d->mode_off) throw ApiError(NCPA_EINVAL, "dispersion needs >= 2 frequencies");
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        const int nf = d->n_freq;
+        const int mt = d->mode_off[nf];
+        DevBuf df, doff, drk, dik, dvs, dvr;
+        upload(df, d->f, nf, st);
+        upload(doff, d->mode_off, nf + 1, st);
+        upload(drk, d->re_k, std::max(mt, 1), st);
+        upload(dik, d->im_k, std::max(mt, 1), st);
+        upload(dvs, d->v_src, std::max(mt, 1), st);
+        upload(dvr, d->v_rcv, std::max(mt, 1), st);
+        return bb_common(ctx, nf, df.as<double>(), doff.as<int>(), drk.as<double>(), dik.as<double>(),
+                         dvs.as<double>(), dvr.as<double>(), d->rho_rcv / d->rho_src, bp, waveforms);
+    });
+}
+
+ncpa_status ncpa_bb_synthesize_modes(ncpa_ctx* ctx, const ncpa_modes* m, int az_index, const ncpa_bb_params* bp,
+                                     double* waveforms) {
+    if (!ctx || !m || !bp || !waveforms || az_index < 0 || az_index >= m->na) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        if (m->na != 1) throw ApiError(NCPA_EINVAL, "device-resident synthesis needs a single-azimuth solve");
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        const int nf = m->nf + 1;  // DC slot first
+        std::vector<double> f(nf);
+        std::vector<int> off(nf + 1);
+        f[0] = 0.0;
+        off[0] = 0;
+        off[1] = 0;
+        for (int i = 0; i < m->nf; ++i) {
+            f[i + 1] = m->freqs[i];
+            off[i + 2] = m->info[i].off + m->info[i].M;
+        }
+        DevBuf df, doff;
+        upload(df, f, st);
+        upload(doff, off, st);
+        return bb_common(ctx, nf, df.as<double>(), doff.as<int>(), m->d_kr.as<double>(), m->d_ki.as<double>(),
+                         m->d_vs.as<double>(), m->d_vr.as<double>(), m->rho_rcv / m->rho_src, bp, waveforms);
+    });
+}
+
+ncpa_status ncpa_source_spectrum_waveform(ncpa_ctx* ctx, const double* x, int n, double dt, int nfft, int nfreq,
+                                          double* s_re, double* s_im) {
+    if (!ctx || !x || !s_re || !s_im || n < 1 || nfft < 1 || nfreq < 1) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        DevBuf dx, ds;
+        upload(dx, x, n, st);
+        ds.alloc((size_t)2 * nfreq * 8);
+        const double* tw = twiddle(ctx, nfft);
+        check_launch(ctx, ncpa::launch_src_dft(st, n, dx.as<double>(), dt, nfft, nfreq, tw, ds.as<double>()));
+        std::vector<double> h(2 * (size_t)nfreq);
+        CK(cudaMemcpyAsync(h.data(), ds.p, h.size() * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int k = 0; k < nfreq; ++k) {
+            s_re[k] = h[2 * k];
+            s_im[k] = h[2 * k + 1];
+        }
+        return NCPA_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,306 @@
+"""ctypes binding of the C ABI in include/ncpa_gpu.h (libncpa_gpu.so).
+
+Thin Python view of the B200 library for tests, benchmarks and scripting:
+every call goes straight to the CUDA library; nothing here computes on the
+CPU.  Loading fails loudly if the shared library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libncpa_gpu.so")
+
+_c_int, _c_double, _c_ll = ctypes.c_int, ctypes.c_double, ctypes.c_longlong
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+
+EXPORTED = [
+    "ncpa_ctx_create", "ncpa_ctx_destroy", "ncpa_status_str", "ncpa_last_error", "ncpa_ctx_synchronize",
+    "ncpa_profile_create", "ncpa_profile_load", "ncpa_profile_destroy", "ncpa_profile_info",
+    "ncpa_ess_params_default", "ncpa_ess_solve", "ncpa_modes_destroy", "ncpa_modes_problems", "ncpa_modes_count",
+    "ncpa_modes_info", "ncpa_modes_get", "ncpa_modes_get_vectors", "ncpa_tl_1d", "ncpa_tl_2d_heights",
+    "ncpa_tl_2d", "ncpa_bb_synthesize", "ncpa_bb_synthesize_modes", "ncpa_source_spectrum_waveform",
+    "ncpa_kernel_launches",
+]
+
+
+class NcpaError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s (status %d): %s" % (msg, status, _status_str(status)))
+        self.status = status
+
+
+class _CtxOpts(ctypes.Structure):
+    _fields_ = [("device", _c_int)]
+
+
+class _ProfileDesc(ctypes.Structure):
+    _fields_ = [("n_knots", _c_int), ("z", _dp), ("u", _dp), ("v", _dp), ("t", _dp), ("p", _dp), ("rho", _dp),
+                ("c0", _dp), ("attn", _dp), ("z0_m", _c_double), ("has_z0", _c_int)]
+
+
+class EssParams(ctypes.Structure):
+    _fields_ = [("nz_grid", _c_int), ("maxheight_km", _c_double), ("zground_km", _c_double),
+                ("sourceheight_km", _c_double), ("receiverheight_km", _c_double), ("lamb_wave_bc", _c_int),
+                ("turnoff_wkb", _c_int), ("wvnum_filter", _c_int), ("c_min", _c_double), ("c_max", _c_double),
+                ("want_group_speed", _c_int), ("want_vectors", _c_int), ("max_modes", _c_int)]
+
+
+class _TlParams(ctypes.Structure):
+    _fields_ = [("n_ranges", _c_int), ("dr_m", _c_double), ("lossless", _c_int)]
+
+
+class _DispDesc(ctypes.Structure):
+    _fields_ = [("n_freq", _c_int), ("f", _dp), ("mode_off", _ip), ("re_k", _dp), ("im_k", _dp), ("v_src", _dp),
+                ("v_rcv", _dp), ("rho_src", _c_double), ("rho_rcv", _c_double)]
+
+
+class _BbParams(ctypes.Structure):
+    _fields_ = [("n_ranges", _c_int), ("ranges_m", _dp), ("max_celerity", _c_double), ("nfft", _c_int),
+                ("src_re", _dp), ("src_im", _dp), ("zero_attn", _c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libncpa_gpu.so not built: run `make -C %s`" % _HERE)
+        L = ctypes.CDLL(LIB_PATH)
+        L.ncpa_ctx_create.argtypes = [ctypes.POINTER(_vp), ctypes.POINTER(_CtxOpts)]
+        L.ncpa_ctx_destroy.argtypes = [_vp]
+        L.ncpa_status_str.restype = ctypes.c_char_p
+        L.ncpa_status_str.argtypes = [_c_int]
+        L.ncpa_last_error.restype = ctypes.c_char_p
+        L.ncpa_last_error.argtypes = [_vp]
+        L.ncpa_ctx_synchronize.argtypes = [_vp]
+        L.ncpa_profile_create.argtypes = [_vp, ctypes.POINTER(_ProfileDesc), ctypes.POINTER(_vp)]
+        L.ncpa_profile_load.argtypes = [_vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_vp)]
+        L.ncpa_profile_destroy.argtypes = [_vp]
+        L.ncpa_profile_info.argtypes = [_vp, _ip, _dp, _dp]
+        L.ncpa_ess_params_default.argtypes = [ctypes.POINTER(EssParams)]
+        L.ncpa_ess_params_default.restype = None
+        L.ncpa_ess_solve.argtypes = [_vp, _vp, ctypes.POINTER(EssParams), _dp, _c_int, _dp, _c_int,
+                                     ctypes.POINTER(_vp)]
+        L.ncpa_modes_destroy.argtypes = [_vp]
+        L.ncpa_modes_problems.argtypes = [_vp, _ip]
+        L.ncpa_modes_count.argtypes = [_vp, _c_int, _ip]
+        L.ncpa_modes_info.argtypes = [_vp, _c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.ncpa_modes_get.argtypes = [_vp, _c_int, _dp, _dp, _dp, _dp, _dp]
+        L.ncpa_modes_get_vectors.argtypes = [_vp, _c_int, _dp]
+        L.ncpa_tl_1d.argtypes = [_vp, _vp, ctypes.POINTER(_TlParams), _dp, _dp, _dp]
+        L.ncpa_tl_2d_heights.argtypes = [_vp, _c_int, _ip]
+        L.ncpa_tl_2d.argtypes = [_vp, _vp, _c_int, ctypes.POINTER(_TlParams), _dp, _dp, _dp]
+        L.ncpa_bb_synthesize.argtypes = [_vp, ctypes.POINTER(_DispDesc), ctypes.POINTER(_BbParams), _dp]
+        L.ncpa_bb_synthesize_modes.argtypes = [_vp, _vp, _c_int, ctypes.POINTER(_BbParams), _dp]
+        L.ncpa_source_spectrum_waveform.argtypes = [_vp, _dp, _c_int, _c_double, _c_int, _c_int, _dp, _dp]
+        L.ncpa_kernel_launches.argtypes = [_vp]
+        L.ncpa_kernel_launches.restype = _c_ll
+        _lib = L
+    return _lib
+
+
+def _status_str(s):
+    try:
+        return lib().ncpa_status_str(int(s)).decode()
+    except OSError:
+        return "?"
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def default_params(**kw) -> EssParams:
+    p = EssParams()
+    lib().ncpa_ess_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Context:
+    def __init__(self, device=0):
+        self.h = _vp()
+        opts = _CtxOpts(device)
+        st = lib().ncpa_ctx_create(ctypes.byref(self.h), ctypes.byref(opts))
+        if st != 0:
+            raise NcpaError(st, "ncpa_ctx_create")
+
+    def check(self, st, what):
+        if st != 0:
+            msg = lib().ncpa_last_error(self.h).decode()
+            raise NcpaError(st, "%s: %s" % (what, msg))
+
+    def close(self):
+        if self.h:
+            lib().ncpa_ctx_destroy(self.h)
+            self.h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def synchronize(self):
+        self.check(lib().ncpa_ctx_synchronize(self.h), "synchronize")
+
+    @property
+    def launches(self):
+        return int(lib().ncpa_kernel_launches(self.h))
+
+    # profiles -------------------------------------------------------------
+    def load_profile(self, path, header=""):
+        h = _vp()
+        self.check(lib().ncpa_profile_load(self.h, path.encode(), header.encode() if header else None,
+                                           ctypes.byref(h)), "ncpa_profile_load")
+        return Profile(self, h)
+
+    def profile_from_arrays(self, z, u, v, t, p, rho, c0=None, attn=None, z0=None):
+        arrs = [_f64(x) for x in (z, u, v, t, p, rho)]
+        c0a = _f64(c0) if c0 is not None else None
+        aa = _f64(attn) if attn is not None else None
+        d = _ProfileDesc(len(arrs[0]), *[_p(a) for a in arrs], _p(c0a), _p(aa), float(z0 or 0.0),
+                         int(z0 is not None))
+        h = _vp()
+        self.check(lib().ncpa_profile_create(self.h, ctypes.byref(d), ctypes.byref(h)), "ncpa_profile_create")
+        return Profile(self, h)
+
+    # solve ----------------------------------------------------------------
+    def solve(self, profile, params: EssParams, freqs, azimuths):
+        f = _f64(np.atleast_1d(freqs))
+        a = _f64(np.atleast_1d(azimuths))
+        h = _vp()
+        self.check(lib().ncpa_ess_solve(self.h, profile.h, ctypes.byref(params), _p(f), len(f), _p(a), len(a),
+                                        ctypes.byref(h)), "ncpa_ess_solve")
+        return Modes(self, h, f, a)
+
+    def source_spectrum_waveform(self, x, dt, nfft, nfreq):
+        x = _f64(x)
+        sre, sim = np.empty(nfreq), np.empty(nfreq)
+        self.check(lib().ncpa_source_spectrum_waveform(self.h, _p(x), len(x), float(dt), int(nfft), int(nfreq),
+                                                       _p(sre), _p(sim)), "ncpa_source_spectrum_waveform")
+        return sre, sim
+
+    def bb_synthesize(self, f, mode_off, re_k, im_k, v_src, v_rcv, rho_src, rho_rcv, ranges_m, max_celerity, nfft,
+                      src_re, src_im, zero_attn=False):
+        f, re_k, im_k, v_src, v_rcv = (_f64(x) for x in (f, re_k, im_k, v_src, v_rcv))
+        off = np.ascontiguousarray(mode_off, dtype=np.int32)
+        rng, sre, sim = _f64(ranges_m), _f64(src_re), _f64(src_im)
+        d = _DispDesc(len(f), _p(f), off.ctypes.data_as(_ip), _p(re_k), _p(im_k), _p(v_src), _p(v_rcv),
+                      float(rho_src), float(rho_rcv))
+        bp = _BbParams(len(rng), _p(rng), float(max_celerity), int(nfft), _p(sre), _p(sim), int(zero_attn))
+        out = np.empty((len(rng), nfft))
+        self.check(lib().ncpa_bb_synthesize(self.h, ctypes.byref(d), ctypes.byref(bp), _p(out)),
+                   "ncpa_bb_synthesize")
+        return out
+
+
+class Profile:
+    def __init__(self, ctx, h):
+        self.ctx, self.h = ctx, h
+
+    def info(self):
+        n, lo, hi = _c_int(), _c_double(), _c_double()
+        self.ctx.check(lib().ncpa_profile_info(self.h, ctypes.byref(n), ctypes.byref(lo), ctypes.byref(hi)),
+                       "ncpa_profile_info")
+        return n.value, lo.value, hi.value
+
+    def close(self):
+        if self.h:
+            lib().ncpa_profile_destroy(self.h)
+            self.h = _vp()
+
+
+@dataclass
+class ProblemModes:
+    freq: float
+    az: float
+    dz: float
+    k_min: float
+    k_max: float
+    rho_src: float
+    rho_rcv: float
+    kr: np.ndarray
+    ki: np.ndarray
+    vs: np.ndarray
+    vr: np.ndarray
+    vg: np.ndarray
+
+    @property
+    def M(self):
+        return len(self.kr)
+
+
+class Modes:
+    def __init__(self, ctx, h, freqs, azs):
+        self.ctx, self.h = ctx, h
+        self.freqs, self.azs = freqs, azs
+        n = _c_int()
+        ctx.check(lib().ncpa_modes_problems(h, ctypes.byref(n)), "ncpa_modes_problems")
+        self.P = n.value
+
+    def count(self, p):
+        n = _c_int()
+        self.ctx.check(lib().ncpa_modes_count(self.h, p, ctypes.byref(n)), "ncpa_modes_count")
+        return n.value
+
+    def counts(self):
+        return np.array([self.count(p) for p in range(self.P)])
+
+    def problem(self, p) -> ProblemModes:
+        M = self.count(p)
+        vals = [_c_double() for _ in range(7)]
+        self.ctx.check(lib().ncpa_modes_info(self.h, p, *[ctypes.byref(v) for v in vals]), "ncpa_modes_info")
+        kr, ki, vs, vr, vg = (np.empty(M) for _ in range(5))
+        self.ctx.check(lib().ncpa_modes_get(self.h, p, _p(kr), _p(ki), _p(vs), _p(vr), _p(vg)), "ncpa_modes_get")
+        return ProblemModes(*[v.value for v in vals], kr, ki, vs, vr, vg)
+
+    def vectors(self, p, nz):
+        M = self.count(p)
+        v = np.empty(nz * M)
+        self.ctx.check(lib().ncpa_modes_get_vectors(self.h, p, _p(v)), "ncpa_modes_get_vectors")
+        return v.reshape(nz, M)
+
+    def tl1d(self, n_ranges, dr_m, lossless=False):
+        tp = _TlParams(int(n_ranges), float(dr_m), int(lossless))
+        re, im, inc = (np.empty((self.P, n_ranges)) for _ in range(3))
+        self.ctx.check(lib().ncpa_tl_1d(self.ctx.h, self.h, ctypes.byref(tp), _p(re), _p(im), _p(inc)),
+                       "ncpa_tl_1d")
+        return re, im, inc
+
+    def tl2d(self, p, n_ranges, dr_m, lossless=False):
+        n = _c_int()
+        self.ctx.check(lib().ncpa_tl_2d_heights(self.h, p, ctypes.byref(n)), "ncpa_tl_2d_heights")
+        z = np.empty(n.value)
+        re, im = np.empty((n_ranges, n.value)), np.empty((n_ranges, n.value))
+        tp = _TlParams(int(n_ranges), float(dr_m), int(lossless))
+        self.ctx.check(lib().ncpa_tl_2d(self.ctx.h, self.h, p, ctypes.byref(tp), _p(z), _p(re), _p(im)),
+                       "ncpa_tl_2d")
+        return z, re, im
+
+    def bb_synthesize(self, ranges_m, max_celerity, nfft, src_re, src_im, zero_attn=False):
+        rng, sre, sim = _f64(ranges_m), _f64(src_re), _f64(src_im)
+        bp = _BbParams(len(rng), _p(rng), float(max_celerity), int(nfft), _p(sre), _p(sim), int(zero_attn))
+        out = np.empty((len(rng), nfft))
+        self.ctx.check(lib().ncpa_bb_synthesize_modes(self.ctx.h, self.h, 0, ctypes.byref(bp), _p(out)),
+                       "ncpa_bb_synthesize_modes")
+        return out
+
+    def close(self):
+        if self.h:
+            lib().ncpa_modes_destroy(self.h)
+            self.h = _vp()

@@ -1,0 +1,79 @@
+"""Synthetic inputs for the ESS normal-mode path.
+
+The analytic stratified atmosphere used by the benchmark workloads (no public
+dataset is involved): z = 0-150 km every 0.1 km, temperature piecewise linear
+(288 K at 0 km, 217 K at 11-20 km, 271 K at 50 km, 187 K at 90 km, 700 K at
+150 km), zonal wind 60 exp(-((z-60)/10)^2) + 20 exp(-((z-12)/3)^2) m/s, no
+meridional wind, rho = 1.225 exp(-z/7 km) kg/m^3, p = rho 287 T.  Written in
+the NCPA profile format the Modess/ModBB command lines read.
+
+Also the source waveform of the broadband workload: a Gaussian-windowed
+0.1 Hz Ricker pulse sampled at 1 Hz.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+T_KNOTS_KM = np.array([0.0, 11.0, 20.0, 50.0, 90.0, 150.0])
+T_KNOTS_K = np.array([288.0, 217.0, 217.0, 271.0, 187.0, 700.0])
+
+
+def analytic_profile(top_km=150.0, dz_km=0.1, t_above_150="extend"):
+    """Knot arrays (z km, u, v m/s, T K, rho kg/m3, p Pa).
+
+    Above 150 km (only used by the tall-atmosphere workload) the temperature
+    keeps the 90-150 km slope when ``t_above_150 == "extend"`` or is held at
+    700 K when ``"hold"``.
+    """
+    n = int(round(top_km / dz_km)) + 1
+    z = np.round(np.arange(n) * dz_km, 10)
+    T = np.interp(z, T_KNOTS_KM, T_KNOTS_K)
+    hi = z > 150.0
+    if np.any(hi):
+        slope = (700.0 - 187.0) / 60.0
+        T[hi] = 700.0 + slope * (z[hi] - 150.0) if t_above_150 == "extend" else 700.0
+    u = 60.0 * np.exp(-((z - 60.0) / 10.0) ** 2) + 20.0 * np.exp(-((z - 12.0) / 3.0) ** 2)
+    v = np.zeros_like(z)
+    rho = 1.225 * np.exp(-z / 7.0)
+    p = rho * 287.0 * T
+    return z, u, v, T, rho, p
+
+
+def write_profile(path, top_km=150.0, dz_km=0.1, t_above_150="extend"):
+    z, u, v, T, rho, p = analytic_profile(top_km, dz_km, t_above_150)
+    with open(path, "w") as f:
+        f.write("#% 0, Z0, m, 0.0\n#% 1, Z, km\n#% 2, U, m/s\n#% 3, V, m/s\n#% 4, T, K\n"
+                "#% 5, RHO, kg/m3\n#% 6, P, Pa\n")
+        for row in zip(z, u, v, T, rho, p):
+            f.write(" ".join("%.12e" % x for x in row) + "\n")
+    return path
+
+
+def si_arrays(top_km=150.0, dz_km=0.1, t_above_150="extend"):
+    """Same profile as SI knot arrays (z in m) for ncpa_profile_create."""
+    z, u, v, T, rho, p = analytic_profile(top_km, dz_km, t_above_150)
+    return z * 1000.0, u, v, T, p, rho
+
+
+def ricker_waveform(f0=0.1, dt=1.0, n=256, t_center=30.0, sigma=40.0):
+    """Gaussian-windowed Ricker pulse (time s, amplitude)."""
+    t = np.arange(n) * dt
+    a = (np.pi * f0 * (t - t_center)) ** 2
+    x = (1.0 - 2.0 * a) * np.exp(-a) * np.exp(-0.5 * ((t - t_center) / sigma) ** 2)
+    return t, x
+
+
+def write_waveform(path, **kw):
+    t, x = ricker_waveform(**kw)
+    with open(path, "w") as f:
+        for a, b in zip(t, x):
+            f.write("%12.6f %15.6e\n" % (a, b))
+    return path
+
+
+def broadband_freqs(n=256, f_max=0.5):
+    """f_min = f_step = f_max / n, n frequencies (Nfreq rule of
+    ESSModeSolver.cpp:109)."""
+    df = f_max / n
+    nf = int(np.floor((f_max - df) / df)) + 1
+    return df + np.arange(nf) * df

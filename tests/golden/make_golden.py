@@ -1,0 +1,65 @@
+"""Regenerates the golden fixtures of this directory from the reference tree.
+
+Reads the reference's shipped example outputs and sample profile (run once,
+where the reference checkout is available) and writes compact copies:
+
+  canonical_profile.dat.gz   samples/NCPA_canonical_profile_zuvwtdp.dat
+  modess_tloss_1d.npz        docs/.../modess_gp_files/code_outputs/tloss_1d.nm
+                             and tloss_1d.lossless.nm (Modess, 0.1 Hz, az 90,
+                             pre-2.0.1 TL scaling: +60 dB vs the current code)
+  dispersion_goldens.npz     per-frequency mode counts, plus Re k / Im k /
+                             V_s V_r at a few frequencies, of
+                             samples/disp_256freqs_0p5hz_NCPA_canonic.dat and
+                             docs/.../modbb_gp_files/code_outputs/myDispersionFile.dat
+
+Usage: python tests/golden/make_golden.py [reference_root]
+"""
+import gzip
+import os
+import sys
+
+import numpy as np
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def read_dispersion(path):
+    toks = open(path).read().split()
+    i, rows = 0, []
+    while i < len(toks):
+        f, m = float(toks[i]), int(toks[i + 1])
+        i += 4
+        vals = np.array([float(x) for x in toks[i:i + 4 * m]]).reshape(m, 4)
+        i += 4 * m
+        rows.append((f, vals))
+    return rows
+
+
+def main():
+    prof = os.path.join(REF, "samples", "NCPA_canonical_profile_zuvwtdp.dat")
+    with open(prof, "rb") as fi, gzip.open(os.path.join(OUT, "canonical_profile.dat.gz"), "wb", 9) as fo:
+        fo.write(fi.read())
+    co = os.path.join(REF, "docs", "ncpaprop_run_manual_TeX", "figs", "modess_gp_files", "code_outputs")
+    lossy = np.loadtxt(os.path.join(co, "tloss_1d.nm"))
+    lossless = np.loadtxt(os.path.join(co, "tloss_1d.lossless.nm"))
+    np.savez_compressed(os.path.join(OUT, "modess_tloss_1d.npz"), lossy=lossy, lossless=lossless)
+    sets = {
+        "s256": os.path.join(REF, "samples", "disp_256freqs_0p5hz_NCPA_canonic.dat"),
+        "manual": os.path.join(REF, "docs", "ncpaprop_run_manual_TeX", "figs", "modbb_gp_files", "code_outputs",
+                               "myDispersionFile.dat"),
+    }
+    out = {}
+    for key, path in sets.items():
+        rows = read_dispersion(path)
+        out[key + "_f"] = np.array([r[0] for r in rows])
+        out[key + "_M"] = np.array([len(r[1]) for r in rows])
+        pick = [0, len(rows) // 5, len(rows) // 2, len(rows) - 1]
+        out[key + "_pick"] = np.array(pick)
+        for j in pick:
+            out["%s_modes_%d" % (key, j)] = rows[j][1]
+    np.savez_compressed(os.path.join(OUT, "dispersion_goldens.npz"), **out)
+
+
+if __name__ == "__main__":
+    main()
