@@ -1,0 +1,371 @@
+"""Benchmark of the B200 ESS normal-mode path (ModBB broadband workload).
+
+One step = the whole ModBB job of the 256-frequency case on the analytic
+0-150 km atmosphere: the batched dispersion solve (256 frequencies
+df = 0.5/256 Hz, Nz = 20000, one azimuth), the 1-D transmission loss of every
+frequency on 1000 ranges to 1000 km (ModBB --dispersion writes it per
+frequency), then pulse synthesis at 200-300 km every 10 km from a
+Gaussian-windowed 0.1 Hz Ricker waveform sampled at 1 Hz.
+
+  value  freq-solves/s with the profile resident in HBM and results left in
+         HBM (device-timed with CUDA events on the library's stream; L2
+         flushed between steps by writing a 256 MiB buffer)
+  e2e    the same through the C ABI with host buffers: profile knots and the
+         source waveform go up, dispersion, TL and waveforms come back, every
+         step
+
+Multi-GPU (torchrun): every rank solves its own independent 256-frequency
+job (weak scaling, no data-path collective); time = max over ranks.
+
+--impl reference times the CPU restatement of the reference algorithm (the
+reference itself cannot be built here: PETSc/SLEPc/GSL/FFTW are absent) on
+the host cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "ncpaprop-release_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import workloads  # noqa: E402
+
+METRIC = "freq-solves/s"
+NZ = 20000
+NFREQ = 256
+RANGES_KM = np.arange(200.0, 300.0 + 1e-9, 10.0)
+MAX_CEL = 340.0
+N_TL = 1000
+DR_TL = 1000.0
+
+
+def _dist():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def _nfft(nfreq_with_dc, n_wave):
+    nfft = 4 * nfreq_with_dc
+    while n_wave > nfft:
+        nfft *= 2
+    return nfft
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import ncpa_gpu
+
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    ctx = ncpa_gpu.Context(local)
+    tmp = tempfile.mkdtemp(prefix="ncpa_bench_")
+    prof_path = workloads.write_profile(os.path.join(tmp, "analytic_150km.dat"))
+    z, u, v, t, p, rho = workloads.si_arrays()
+    t_w, x_w = workloads.ricker_waveform()
+    freqs = workloads.broadband_freqs(NFREQ, 0.5)
+    az = [(90.0 + 10.0 * rank) % 360.0]
+    ranges_m = RANGES_KM * 1000.0
+    nf_dc = len(freqs) + 1
+    nfft = _nfft(nf_dc, len(x_w))
+    prof = ctx.load_profile(prof_path)
+    params_dev = ncpa_gpu.default_params(nz_grid=NZ, turnoff_wkb=1, keep_on_device=1)
+    params_host = ncpa_gpu.default_params(nz_grid=NZ, turnoff_wkb=1)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # pinned host buffers for the end-to-end leg
+    pin = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for k, a in
+           dict(z=z, u=u, v=v, t=t, p=p, rho=rho, x=x_w, f=freqs).items()}
+
+    def step_device():
+        sre, sim = ctx.source_spectrum_waveform(x_w, t_w[1] - t_w[0], nfft, nf_dc)
+        m = ctx.solve(prof, params_dev, freqs, az)
+        m.tl1d(N_TL, DR_TL, to_host=False)
+        m.bb_synthesize(ranges_m, MAX_CEL, nfft, sre, sim, to_host=False)
+        m.close()
+
+    h2d = [0]
+    d2h = [0]
+
+    def step_e2e():
+        pr = ctx.profile_from_arrays(*(pin[k].numpy() for k in ("z", "u", "v", "t", "p", "rho")))
+        xw = pin["x"].numpy()
+        sre, sim = ctx.source_spectrum_waveform(xw, t_w[1] - t_w[0], nfft, nf_dc)
+        m = ctx.solve(pr, params_host, pin["f"].numpy(), az)
+        disp = [m.problem(i) for i in range(m.P)]
+        tl = m.tl1d(N_TL, DR_TL)
+        wav = m.bb_synthesize(ranges_m, MAX_CEL, nfft, sre, sim)
+        nm = sum(d.M for d in disp)
+        h2d[0] = 6 * len(z) * 8 + len(xw) * 8 + len(freqs) * 8
+        d2h[0] = nm * 5 * 8 + sum(a.nbytes for a in tl) + wav.nbytes + 2 * nf_dc * 8
+        m.close()
+        pr.close()
+
+    def timed(fn, k):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        barrier()
+        for i in range(k):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev[i][0].record(stream)
+            fn()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return sum(a.elapsed_time(b) for a, b in ev)
+
+    for _ in range(args.warmup):
+        step_device()
+    for _ in range(max(1, min(args.warmup, 2))):
+        step_e2e()
+    # timed device-resident leg, with per-phase kernel timing on
+    ctx.reset_stats()
+    ctx.set_timing(True)
+    l0 = ctx.launches
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    ms_dev = timed(step_device, args.steps)
+    if sampler:
+        clocks = sampler.stop()
+    launches = (ctx.launches - l0) // args.steps
+    ctx.set_timing(False)
+    bis_ms, bis_n = ctx.phase_stats("bisect")
+    seqs, grid_pts = ctx.sturm_sequences()
+    phases = {ph: ctx.phase_stats(ph)[0] / args.steps for ph in
+              ("knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec", "fetch")}
+    ms_e2e = timed(step_e2e, args.steps)
+    # plain per-frequency GPU path: one ncpa_ess_solve per frequency
+    plain_freqs = freqs[::16]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for f in plain_freqs:
+        m = ctx.solve(prof, params_dev, [f], az)
+        m.tl1d(N_TL, DR_TL, to_host=False)
+        m.close()
+    torch.cuda.synchronize()
+    plain_rate = len(plain_freqs) / (time.perf_counter() - t0)
+
+    if world > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([ms_dev, ms_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_dev, ms_e2e = tt.tolist()
+    fp64_peak = ctx.fp64_peak_tflops() if rank == 0 else None
+    if rank == 0:
+        solves = NFREQ * args.steps * world
+        value = solves / (ms_dev / 1e3)
+        e2e_value = solves / (ms_e2e / 1e3)
+        # bisection kernel roofline: 3 FP64 flops per Sturm step (subtract +
+        # fused multiply-add) over the active shifts it swept
+        flops = 3.0 * seqs * (grid_pts / max(bis_n, 1))
+        achieved = flops / (bis_ms / 1e3) / 1e12 if bis_ms > 0 else None
+        cpu = cpu_baseline(freqs, max_seconds=args.cpu_seconds)
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_dev / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "ModBB 256-frequency dispersion + 1-D TL + pulse synthesis",
+                       "profile": "analytic 0-150 km (T piecewise linear, 60+20 m/s jets)", "nz_grid": NZ,
+                       "n_freq": NFREQ, "df_hz": 0.5 / NFREQ, "azimuth_deg": az[0], "tl_ranges": N_TL,
+                       "synthesis_ranges_km": "200-300/10", "nfft": nfft, "l2": "flushed (256 MiB write) between steps",
+                       "parallelism": "replicas (one 256-frequency job per GPU)"},
+            "e2e": {"value": round(e2e_value, 2), "unit": METRIC, "h2d_bytes_per_step": int(h2d[0]),
+                    "d2h_bytes_per_step": int(d2h[0])},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "roofline": {"kernel": "k_bisect (Sturm multisection)", "bound": "fp64",
+                         "achieved": round(achieved, 3) if achieved else None, "peak": round(fp64_peak, 3),
+                         "unit": "TFLOP/s", "frac": round(achieved / fp64_peak, 4) if achieved else None,
+                         "peak_source": "measured in this run (dependent-FMA probe on all SMs)",
+                         "traffic": None, "avg_launch_ms": round(bis_ms / max(bis_n, 1), 4),
+                         "flops_per_launch": flops / max(bis_n, 1) if bis_n else None},
+            "phases_ms": {k: round(v, 4) for k, v in phases.items()},
+            "plain_gpu": {"value": round(plain_rate, 2), "unit": METRIC,
+                          "what": "one ncpa_ess_solve + TL per frequency, same workload"},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    for h in (prof,):
+        h.close()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# CPU (oracle) legs
+# ---------------------------------------------------------------------------
+def _oracle_setup():
+    from oracle import oracle as O
+
+    tmp = tempfile.mkdtemp(prefix="ncpa_cpu_")
+    path = workloads.write_profile(os.path.join(tmp, "analytic_150km.dat"))
+    prof = O.read_profile(path)
+    prm = O.EssParams(Nz_grid=NZ, turnoff_WKB=True)
+    pp = O.prepare(prof, prm)
+    return O, pp, prm
+
+
+def _oracle_freq_solve(O, pp, prm, f, az):
+    ms = O.solve_problem(pp, prm, float(f), az)
+    O.tl1d(ms, N_TL, DR_TL)
+    return ms
+
+
+def cpu_baseline(freqs, max_seconds=20.0, az=90.0):
+    """Oracle on the host cores over a stratified sample of the frequencies
+    (every 16th, i.e. the same mix of small and large mode counts)."""
+    O, pp, prm = _oracle_setup()
+    sample = freqs[::16]
+    t0 = time.perf_counter()
+    done = 0
+    for f in sample:
+        _oracle_freq_solve(O, pp, prm, f, az)
+        done += 1
+        if time.perf_counter() - t0 > max_seconds:
+            break
+    el = time.perf_counter() - t0
+    return {"value": round(done / el, 3), "unit": METRIC, "cores": O.lib().orc_num_threads(), "kind": "port",
+            "sample": "%d of the 256 frequencies (every 16th), Nz=20000, eigen-solve + 1-D TL each" % done}
+
+
+def run_reference(args):
+    rank, world, local = _dist()
+    if rank != 0:
+        return
+    O, pp, prm = _oracle_setup()
+    freqs = workloads.broadband_freqs(NFREQ, 0.5)
+    per_step = 8  # bounded sample per step: 8 frequencies spread over the band
+    order = np.concatenate([freqs[i::32] for i in range(32)])
+    k = 0
+    for _ in range(args.warmup):
+        for f in order[k:k + per_step]:
+            _oracle_freq_solve(O, pp, prm, f, 90.0)
+        k = (k + per_step) % len(order)
+    t0 = time.perf_counter()
+    n = 0
+    for _ in range(args.steps):
+        for f in order[k:k + per_step]:
+            _oracle_freq_solve(O, pp, prm, f, 90.0)
+            n += 1
+        k = (k + per_step) % len(order)
+    el = time.perf_counter() - t0
+    value = n / el
+    cores = O.lib().orc_num_threads()
+    line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(el * 1e3 / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "ModBB 256-frequency dispersion + 1-D TL + pulse synthesis", "nz_grid": NZ,
+                       "n_freq": NFREQ},
+            "cpu_baseline": {"value": round(value, 3), "unit": METRIC, "cores": cores, "kind": "port",
+                             "sample": "%d frequencies per step spread over the 256-frequency band, eigen-solve "
+                                       "+ 1-D TL each (reference binary unbuildable here: PETSc/SLEPc/GSL/FFTW "
+                                       "absent)" % per_step},
+            "e2e": {"value": round(value, 3), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -89,6 +89,8 @@ typedef struct {
     int want_group_speed;     /* compute group speeds (speeds.nm) */
     int want_vectors;         /* keep full eigenvectors (modes, 2-D TL, starter) */
     int max_modes;            /* per problem; 0 -> 4000 (reference MAX_MODES) */
+    int keep_on_device;       /* leave mode arrays in HBM only (ncpa_modes_get
+                                 then fetches them on demand) */
 } ncpa_ess_params;
 
 void ncpa_ess_params_default(ncpa_ess_params *p);
@@ -124,7 +126,8 @@ typedef struct {
     int lossless; /* use Re k only (tloss_*.lossless.nm) */
 } ncpa_tl_params;
 
-/* all problems at once: re/im/incoh are [n_problems x n_ranges] */
+/* all problems at once: re/im/incoh are [n_problems x n_ranges]; pass all
+ * three as NULL to keep the result in HBM (owned by the modes object) */
 ncpa_status ncpa_tl_1d(ncpa_ctx *ctx, const ncpa_modes *modes, const ncpa_tl_params *tp,
                        double *re, double *im, double *incoh);
 /* one problem on the reference's height sampling (every nz/500-th grid
@@ -158,7 +161,8 @@ typedef struct {
     int zero_attn;        /* set Im k = 0 */
 } ncpa_bb_params;
 
-/* waveforms: [n_ranges x nfft], 2 Re p(t) at t = i/(nfft df) + t0 */
+/* waveforms: [n_ranges x nfft], 2 Re p(t) at t = i/(nfft df) + t0; NULL
+ * waveforms keeps the result in HBM */
 ncpa_status ncpa_bb_synthesize(ncpa_ctx *ctx, const ncpa_dispersion_desc *disp,
                                const ncpa_bb_params *bp, double *waveforms);
 /* same, taking the dispersion of a device-resident batched solve (one
@@ -172,6 +176,22 @@ ncpa_status ncpa_source_spectrum_waveform(ncpa_ctx *ctx, const double *x, int n_
 
 /* Number of this library's kernels launched on the context so far. */
 long long ncpa_kernel_launches(const ncpa_ctx *ctx);
+/* The context's CUDA stream (cudaStream_t) for event timing / interop. */
+void *ncpa_ctx_stream(ncpa_ctx *ctx);
+
+/* Diagnostics (no counterpart in the reference): per-phase device times of
+ * ncpa_ess_solve measured with CUDA events on the context stream.  Phases:
+ * "knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec",
+ * "fetch".  stats() returns accumulated milliseconds and calls since the last
+ * reset; sturm_sequences() the number of Sturm sequences (one shift swept over
+ * the whole grid) run by the bisection kernel for active eigenvalues. */
+ncpa_status ncpa_ctx_set_timing(ncpa_ctx *ctx, int on);
+ncpa_status ncpa_ctx_phase_stats(const ncpa_ctx *ctx, const char *phase, double *total_ms, long long *calls);
+ncpa_status ncpa_ctx_reset_stats(ncpa_ctx *ctx);
+ncpa_status ncpa_ctx_sturm_sequences(ncpa_ctx *ctx, long long *sequences, long long *grid_points);
+/* Measured FP64 FMA throughput of this device [TFLOP/s, FMA = 2 flops]: a
+ * dependent-FMA kernel on every SM for about 50 ms. */
+ncpa_status ncpa_probe_fp64_peak(ncpa_ctx *ctx, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(kThreads) k_bisect(const ProblemInfo* __restri
                                                      const int* __restrict__ counts,
                                                      const WorkItem* __restrict__ items, int n_items,
                                                      int* counter, double tol, double* __restrict__ mu,
-                                                     unsigned* err) {
+                                                     unsigned* err, unsigned long long* seq_counter) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     double* buf = reinterpret_cast<double*>(smem_raw);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + kNbuf * kChunk * 8);
@@ -551,6 +551,7 @@ __global__ void __launch_bounds__(kThreads) k_bisect(const ProblemInfo* __restri
             double a = active ? sa[e] : pi.lo, b = active ? sb[e] : pi.hi;
             double x = a + (b - a) * frac;
             int c = cta_sturm_sweep(sp, nz, x, r, err);
+            if (seq_counter && tid == 0) atomicAdd(seq_counter, (unsigned long long)(G * w.m));
             if (tid < w.m) sbest[tid] = -1;
             __syncthreads();
             if (active && c <= J) atomicMax(&sbest[e], gi);
@@ -574,9 +575,33 @@ __global__ void __launch_bounds__(kThreads) k_bisect(const ProblemInfo* __restri
 
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
                   const int* counts, const WorkItem* items, int n_items, int* counter, double tol, double* mu,
-                  unsigned* err) {
+                  unsigned* err, unsigned long long* seq_counter) {
     size_t sm = kNbuf * kChunk * 8 + kNbuf * 8;
-    k_bisect<<<grid, kThreads, sm, st>>>(pinfo, s, nz, nz_pad, counts, items, n_items, counter, tol, mu, err);
+    k_bisect<<<grid, kThreads, sm, st>>>(pinfo, s, nz, nz_pad, counts, items, n_items, counter, tol, mu, err,
+                                         seq_counter);
+    return 1;
+}
+
+// ===========================================================================
+// FP64 FMA throughput probe (denominator of the bisection roofline)
+// ===========================================================================
+__global__ void k_fp64_probe(int n_iter, double* out) {
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = 1.0 + 1e-9 * (threadIdx.x + k);
+    const double m = 0.999999999, c = 1e-12;
+    for (int it = 0; it < n_iter; ++it) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fma(a[k], m, c);
+    }
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += a[k];
+    if (t == 12345.0) out[0] = t;  // practically never: keeps the chains live
+}
+
+int launch_fp64_probe(cudaStream_t st, int grid, int block, int n_iter, double* out) {
+    k_fp64_probe<<<grid, block, 0, st>>>(n_iter, out);
     return 1;
 }
 

@@ -71,7 +71,10 @@ int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* 
 // multisection/bisection over work items (K3)
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
                   const int* counts, const WorkItem* items, int n_items, int* counter, double tol, double* mu,
-                  unsigned* err);
+                  unsigned* err, unsigned long long* seq_counter);
+// FP64 throughput probe: each thread runs n_iter iterations of 8 independent
+// FMA chains; out receives a value that keeps the chains live
+int launch_fp64_probe(cudaStream_t st, int grid, int block, int n_iter, double* out);
 // twisted-factorisation eigenvectors + fused reductions (K4)
 struct EigvecArgs {
     const ProblemInfo* pinfo;

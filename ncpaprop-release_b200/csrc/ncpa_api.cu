@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -40,14 +41,16 @@ struct ApiError : std::runtime_error {
             throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));                    \
     } while (0)
 
-// owning device buffer
+// owning device buffer on the stream-ordered allocator (pooled, so the
+// per-solve temporaries cost no cudaMalloc round trips after warm-up)
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    cudaStream_t st = nullptr;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) {
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes), st(o.st) {
         o.p = nullptr;
         o.bytes = 0;
     }
@@ -56,6 +59,7 @@ struct DevBuf {
             release();
             p = o.p;
             bytes = o.bytes;
+            st = o.st;
             o.p = nullptr;
             o.bytes = 0;
         }
@@ -63,18 +67,19 @@ struct DevBuf {
     }
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, st);
         p = nullptr;
         bytes = 0;
     }
-    void alloc(size_t b) {
+    void alloc(size_t b, cudaStream_t stream) {
         if (b <= bytes && p) return;
         release();
+        st = stream;
         if (b == 0) b = 16;
-        cudaError_t e = cudaMalloc(&p, b);
+        cudaError_t e = cudaMallocAsync(&p, b, st);
         if (e != cudaSuccess) {
             p = nullptr;
-            throw ApiError(NCPA_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            throw ApiError(NCPA_ENOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
         }
         bytes = b;
     }
@@ -86,12 +91,12 @@ struct DevBuf {
 
 template <class T>
 void upload(DevBuf& d, const std::vector<T>& h, cudaStream_t st) {
-    d.alloc(h.size() * sizeof(T));
+    d.alloc(h.size() * sizeof(T), st);
     if (!h.empty()) CK(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
 }
 template <class T>
 void upload(DevBuf& d, const T* h, size_t n, cudaStream_t st) {
-    d.alloc(n * sizeof(T));
+    d.alloc(n * sizeof(T), st);
     if (n) CK(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, st));
 }
 
@@ -106,8 +111,46 @@ struct ncpa_ctx {
     DevBuf d_err;                  // device status word
     DevBuf ck1, ck2, cke;          // eigenvector checkpoint scratch
     std::map<int, DevBuf> twiddle; // per nfft
+    DevBuf bb_out;                 // waveforms kept in HBM (NULL host buffer)
+    DevBuf d_stats;                // device counters (Sturm sequences)
+    bool timing = false;           // NCPA_TIMING=1: per-phase times on stderr
+    bool stats = false;            // ncpa_ctx_set_timing: accumulate per phase
+    std::map<std::string, std::pair<double, long long>> phase;
+    long long grid_points = 0;     // sum over bisection launches of nz
     void count(int n) { launches += n; }
 };
+
+namespace {
+// per-phase timing with CUDA events on the context stream (diagnostics)
+struct PhaseTimer {
+    ncpa_ctx* ctx;
+    std::vector<std::pair<std::string, cudaEvent_t>> ev;
+    explicit PhaseTimer(ncpa_ctx* c) : ctx(c) {}
+    void mark(const char* name) {
+        if (!ctx->timing && !ctx->stats) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, ctx->stream);
+        ev.emplace_back(name, e);
+    }
+    ~PhaseTimer() {
+        if (ev.size() > 1) {
+            cudaEventSynchronize(ev.back().second);
+            for (size_t i = 1; i < ev.size(); ++i) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[i - 1].second, ev[i].second);
+                if (ctx->timing) std::fprintf(stderr, "[ncpa] %-14s %9.3f ms\n", ev[i].first.c_str(), ms);
+                if (ctx->stats) {
+                    auto& acc = ctx->phase[ev[i].first];
+                    acc.first += ms;
+                    acc.second += 1;
+                }
+            }
+        }
+        for (auto& e : ev) cudaEventDestroy(e.second);
+    }
+};
+}  // namespace
 
 struct ncpa_profile {
     ncpa_ctx* ctx = nullptr;
@@ -130,7 +173,9 @@ struct ncpa_modes {
     std::vector<ProblemInfo> info;
     int Mtot = 0;
     DevBuf d_pinfo, d_kr, d_ki, d_vs, d_vr, d_vg, d_vfull, d_vfull_off;
-    std::vector<double> kr, ki, vs, vr, vg;
+    mutable DevBuf tl_re, tl_im, tl_inc;  // 1-D TL kept in HBM
+    mutable bool host_valid = false;      // host copies of the mode arrays
+    mutable std::vector<double> kr, ki, vs, vr, vg;
     std::vector<long long> vfull_off;
 };
 
@@ -181,11 +226,29 @@ const double* twiddle(ncpa_ctx* ctx, int nfft) {
     auto it = ctx->twiddle.find(nfft);
     if (it != ctx->twiddle.end()) return it->second.as<double>();
     DevBuf b;
-    b.alloc((size_t)2 * nfft * sizeof(double));
+    b.alloc((size_t)2 * nfft * sizeof(double), ctx->stream);
     check_launch(ctx, ncpa::launch_twiddle(ctx->stream, nfft, b.as<double>()));
     const double* p = b.as<double>();
     ctx->twiddle.emplace(nfft, std::move(b));
     return p;
+}
+
+// copy the mode arrays of a solve to its host mirror (stream-ordered)
+void fetch_modes(const ncpa_modes* M) {
+    cudaStream_t st = M->ctx->stream;
+    M->kr.resize(M->Mtot);
+    M->ki.resize(M->Mtot);
+    M->vs.resize(M->Mtot);
+    M->vr.resize(M->Mtot);
+    M->vg.resize(M->Mtot);
+    if (M->Mtot > 0) {
+        CK(cudaMemcpyAsync(M->kr.data(), M->d_kr.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(M->ki.data(), M->d_ki.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(M->vs.data(), M->d_vs.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(M->vr.data(), M->d_vr.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(M->vg.data(), M->d_vg.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
+    }
+    M->host_valid = true;
 }
 
 }  // namespace
@@ -211,6 +274,75 @@ const char* ncpa_last_error(const ncpa_ctx* ctx) { return ctx ? ctx->err.c_str()
 
 long long ncpa_kernel_launches(const ncpa_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+void* ncpa_ctx_stream(ncpa_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+ncpa_status ncpa_ctx_set_timing(ncpa_ctx* ctx, int on) {
+    if (!ctx) return NCPA_EINVAL;
+    ctx->stats = on != 0;
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_ctx_reset_stats(ncpa_ctx* ctx) {
+    if (!ctx) return NCPA_EINVAL;
+    ctx->phase.clear();
+    ctx->grid_points = 0;
+    return guarded(ctx, [&]() -> ncpa_status {
+        CK(cudaMemsetAsync(ctx->d_stats.p, 0, 4 * sizeof(unsigned long long), ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_ctx_phase_stats(const ncpa_ctx* ctx, const char* phase, double* total_ms, long long* calls) {
+    if (!ctx || !phase) return NCPA_EINVAL;
+    auto it = ctx->phase.find(phase);
+    if (total_ms) *total_ms = it == ctx->phase.end() ? 0.0 : it->second.first;
+    if (calls) *calls = it == ctx->phase.end() ? 0 : it->second.second;
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_ctx_sturm_sequences(ncpa_ctx* ctx, long long* sequences, long long* grid_points) {
+    if (!ctx) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        unsigned long long h = 0;
+        CK(cudaMemcpyAsync(&h, ctx->d_stats.p, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (sequences) *sequences = (long long)h;
+        if (grid_points) *grid_points = ctx->grid_points;
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_probe_fp64_peak(ncpa_ctx* ctx, double* tflops) {
+    if (!ctx || !tflops) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        DevBuf out;
+        out.alloc(8, st);
+        const int block = 256, grid = ctx->num_sms * 8;
+        cudaEvent_t a, b;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        int iters = 1 << 12;
+        float ms = 0.f;
+        for (int rep = 0; rep < 8; ++rep) {  // grow until ~50 ms
+            CK(cudaEventRecord(a, st));
+            check_launch(ctx, ncpa::launch_fp64_probe(st, grid, block, iters, out.as<double>()));
+            CK(cudaEventRecord(b, st));
+            CK(cudaEventSynchronize(b));
+            CK(cudaEventElapsedTime(&ms, a, b));
+            if (ms > 40.f) break;
+            iters *= 2;
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        const double flops = 2.0 * 8.0 * (double)iters * grid * block;
+        *tflops = flops / (ms * 1e-3) / 1e12;
+        return NCPA_OK;
+    });
+}
+
 ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
     if (!out) return NCPA_EINVAL;
     *out = nullptr;
@@ -226,9 +358,18 @@ ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
         if (prop.major < 10) throw ApiError(NCPA_ENODEV, "this library is built for sm_100a (B200)");
         ctx->num_sms = prop.multiProcessorCount;
         CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-        ctx->d_err.alloc(sizeof(unsigned));
+        // keep freed blocks of the stream-ordered allocator cached in the pool
+        cudaMemPool_t pool;
+        CK(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+        unsigned long long thr = ~0ull;
+        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+        ctx->d_err.alloc(sizeof(unsigned), ctx->stream);
         CK(cudaMemsetAsync(ctx->d_err.p, 0, sizeof(unsigned), ctx->stream));
+        ctx->d_stats.alloc(4 * sizeof(unsigned long long), ctx->stream);
+        CK(cudaMemsetAsync(ctx->d_stats.p, 0, 4 * sizeof(unsigned long long), ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        const char* tv = std::getenv("NCPA_TIMING");
+        ctx->timing = tv && tv[0] == '1';
         return NCPA_OK;
     });
     if (s != NCPA_OK) return s;
@@ -241,6 +382,8 @@ ncpa_status ncpa_ctx_destroy(ncpa_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->twiddle.clear();
+    ctx->bb_out.release();
+    ctx->d_stats.release();
     ctx->ck1.release();
     ctx->ck2.release();
     ctx->cke.release();
@@ -282,12 +425,12 @@ ncpa_status ncpa_profile_create(ncpa_ctx* ctx, const ncpa_profile_desc* d, ncpa_
         upload(P->t, d->t, n, st);
         upload(P->p, d->p, n, st);
         upload(P->rho, d->rho, n, st);
-        P->c0.alloc(n * sizeof(double));
+        P->c0.alloc(n * sizeof(double), st);
         if (d->c0) CK(cudaMemcpyAsync(P->c0.p, d->c0, n * sizeof(double), cudaMemcpyHostToDevice, st));
-        P->ws.alloc(n * sizeof(double));
-        P->wd.alloc(n * sizeof(double));
-        P->pcoef.alloc(4 * (n - 1) * sizeof(double));
-        P->rcoef.alloc(4 * (n - 1) * sizeof(double));
+        P->ws.alloc(n * sizeof(double), st);
+        P->wd.alloc(n * sizeof(double), st);
+        P->pcoef.alloc(4 * (n - 1) * sizeof(double), st);
+        P->rcoef.alloc(4 * (n - 1) * sizeof(double), st);
         check_launch(ctx, ncpa::launch_steffen(st, n, P->z.as<double>(), P->p.as<double>(), 1, n,
                                                P->pcoef.as<double>(), 4 * (n - 1)));
         check_launch(ctx, ncpa::launch_steffen(st, n, P->z.as<double>(), P->rho.as<double>(), 1, n,
@@ -376,6 +519,8 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
             throw ApiError(NCPA_EINVAL, "wvnum_filter needs c_min > 0 and c_max > 0");
         CK(cudaSetDevice(ctx->device));
         cudaStream_t st = ctx->stream;
+        PhaseTimer tm(ctx);
+        tm.mark("start");
         auto M = std::make_unique<ncpa_modes>();
         M->ctx = ctx;
         M->prm = *prm;
@@ -413,15 +558,15 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
         upload(d_freqs, freqs, n_freq, st);
         upload(d_az, az_deg, n_az, st);
         DevBuf ceffk, ceffc, alpha, alphac;
-        ceffk.alloc((size_t)n_az * nk * 8);
-        ceffc.alloc((size_t)n_az * 4 * (nk - 1) * 8);
+        ceffk.alloc((size_t)n_az * nk * 8, st);
+        ceffc.alloc((size_t)n_az * 4 * (nk - 1) * 8, st);
         check_launch(ctx, ncpa::launch_ceff_knots(st, nk, n_az, d_az.as<double>(), prof->c0.as<double>(),
                                                   prof->ws.as<double>(), prof->wd.as<double>(), ceffk.as<double>()));
         check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), ceffk.as<double>(), n_az, nk,
                                                ceffc.as<double>(), 4 * (nk - 1)));
         const int n_alpha = prof->has_attn ? 1 : n_freq;
-        alpha.alloc((size_t)n_freq * nk * 8);
-        alphac.alloc((size_t)n_freq * 4 * (nk - 1) * 8);
+        alpha.alloc((size_t)n_freq * nk * 8, st);
+        alphac.alloc((size_t)n_freq * 4 * (nk - 1) * 8, st);
         if (prof->has_attn) {
             for (int f = 0; f < n_freq; ++f)
                 CK(cudaMemcpyAsync(alpha.as<double>() + (size_t)f * nk, prof->attn.p, nk * 8,
@@ -436,9 +581,9 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
                                                alphac.as<double>(), 4 * (nk - 1)));
         // ---- grid fields ----
         DevBuf rho_g, ct_g, w;
-        rho_g.alloc((size_t)nz * 8);
-        ct_g.alloc((size_t)nz * 8);
-        w.alloc((size_t)n_freq * nz_pad * 8);
+        rho_g.alloc((size_t)nz * 8, st);
+        ct_g.alloc((size_t)nz * 8, st);
+        w.alloc((size_t)n_freq * nz_pad * 8, st);
         CK(cudaMemsetAsync(w.p, 0, (size_t)n_freq * nz_pad * 8, st));
         check_launch(ctx, ncpa::launch_grid_common(st, nk, prof->z.as<double>(), prof->rho.as<double>(),
                                                    prof->rcoef.as<double>(), prof->p.as<double>(),
@@ -489,24 +634,28 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
             }
         upload(M->d_pinfo, M->info, st);
         ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
+        tm.mark("knots+grid");
         // ---- K1 matrix ----
         const bool wkb = !prm->turnoff_wkb && std::fabs(src_h) < 1.0e-3 && std::fabs(rcv_h) < 1.0e-3;
         DevBuf s, kz2, g;
-        s.alloc((size_t)P * nz_pad * 8);
-        if (wkb) kz2.alloc((size_t)P * nz * 8);
-        if (prm->want_group_speed) g.alloc((size_t)P * nz_pad * 8);
+        s.alloc((size_t)P * nz_pad * 8, st);
+        if (wkb) kz2.alloc((size_t)P * nz * 8, st);
+        if (prm->want_group_speed) g.alloc((size_t)P * nz_pad * 8, st);
         check_launch(ctx, ncpa::launch_build_matrix(st, nk, prof->z.as<double>(), ceffk.as<double>(),
                                                     ceffc.as<double>(), n_az, P, d_pinfo, nz, nz_pad, z_min, dz_grid,
                                                     dz, admittance, s.as<double>(), wkb ? kz2.as<double>() : nullptr,
                                                     prm->want_group_speed ? g.as<double>() : nullptr));
+        tm.mark("matrix");
         // ---- K2 window ----
         check_launch(ctx, ncpa::launch_window(st, P, d_pinfo, wkb ? kz2.as<double>() : nullptr, nz, dz, wkb ? 1 : 0,
                                               prm->wvnum_filter, prm->c_min, prm->c_max, ctx->d_err.as<unsigned>()));
+        tm.mark("window");
         // ---- K3a scan ----
         DevBuf counts;
-        counts.alloc((size_t)P * ncpa::kScanPoints * 4);
+        counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
         check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
                                             ctx->d_err.as<unsigned>()));
+        tm.mark("scan");
         std::vector<int> hcounts((size_t)P * ncpa::kScanPoints);
         CK(cudaMemcpyAsync(hcounts.data(), counts.p, hcounts.size() * 4, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(M->info.data(), d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
@@ -539,12 +688,12 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
         CK(cudaMemcpyAsync(d_pinfo, M->info.data(), P * sizeof(ProblemInfo), cudaMemcpyHostToDevice, st));
         const int Mt = std::max(1, M->Mtot);
         DevBuf mu, d_items, d_counter;
-        mu.alloc((size_t)Mt * 8);
-        M->d_kr.alloc((size_t)Mt * 8);
-        M->d_ki.alloc((size_t)Mt * 8);
-        M->d_vs.alloc((size_t)Mt * 8);
-        M->d_vr.alloc((size_t)Mt * 8);
-        M->d_vg.alloc((size_t)Mt * 8);
+        mu.alloc((size_t)Mt * 8, st);
+        M->d_kr.alloc((size_t)Mt * 8, st);
+        M->d_ki.alloc((size_t)Mt * 8, st);
+        M->d_vs.alloc((size_t)Mt * 8, st);
+        M->d_vr.alloc((size_t)Mt * 8, st);
+        M->d_vg.alloc((size_t)Mt * 8, st);
         if (prm->want_vectors) {
             M->vfull_off.resize(P);
             long long acc = 0;
@@ -552,28 +701,32 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
                 M->vfull_off[p] = acc;
                 acc += (long long)M->info[p].M * nz;
             }
-            M->d_vfull.alloc((size_t)std::max(1LL, acc) * 8);
+            M->d_vfull.alloc((size_t)std::max(1LL, acc) * 8, st);
             upload(M->d_vfull_off, M->vfull_off, st);
         }
         const int n_items = (int)items.size();
         if (n_items > 0) {
             upload(d_items, items, st);
-            d_counter.alloc(2 * sizeof(int));
+            d_counter.alloc(2 * sizeof(int), st);
             CK(cudaMemsetAsync(d_counter.p, 0, 2 * sizeof(int), st));
             // ---- K3 bisection ----
             int grid_b = std::min(n_items, ctx->num_sms * 4);
+            tm.mark("host-items");
             check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
                                                   d_items.as<WorkItem>(), n_items, d_counter.as<int>(), kBisectTol,
-                                                  mu.as<double>(), ctx->d_err.as<unsigned>()));
+                                                  mu.as<double>(), ctx->d_err.as<unsigned>(),
+                                                  ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr));
+            if (ctx->stats) ctx->grid_points += nz;
+            tm.mark("bisect");
             // ---- K4 eigenvectors ----
             int grid_e = std::min(n_items, ctx->num_sms * 2);
             const long long nblk = (nz + ncpa::kBlk - 1) / ncpa::kBlk;
             const long long slot = nblk * ncpa::kThreads;
             const size_t need = (size_t)grid_e * slot;
             if (ctx->ck1.bytes < need * 8) {
-                ctx->ck1.alloc(need * 8);
-                ctx->ck2.alloc(need * 8);
-                ctx->cke.alloc(need * 4);
+                ctx->ck1.alloc(need * 8, st);
+                ctx->ck2.alloc(need * 8, st);
+                ctx->cke.alloc(need * 4, st);
             }
             ncpa::EigvecArgs ea{};
             ea.pinfo = d_pinfo;
@@ -606,20 +759,11 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
             ea.err = ctx->d_err.as<unsigned>();
             check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
         }
+        tm.mark("eigvec");
         // ---- results to host ----
-        M->kr.resize(M->Mtot);
-        M->ki.resize(M->Mtot);
-        M->vs.resize(M->Mtot);
-        M->vr.resize(M->Mtot);
-        M->vg.resize(M->Mtot);
-        if (M->Mtot > 0) {
-            CK(cudaMemcpyAsync(M->kr.data(), M->d_kr.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(M->ki.data(), M->d_ki.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(M->vs.data(), M->d_vs.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(M->vr.data(), M->d_vr.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(M->vg.data(), M->d_vg.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
-        }
+        if (!prm->keep_on_device) fetch_modes(M.get());
         check_device_status(ctx);
+        tm.mark("fetch");
         M->rho_src = hrho[M->isrc];
         M->rho_rcv = hrho[M->ircv];
         *out = M.release();
@@ -664,6 +808,14 @@ ncpa_status ncpa_modes_info(const ncpa_modes* m, int problem, double* freq, doub
 ncpa_status ncpa_modes_get(const ncpa_modes* m, int problem, double* re_k, double* im_k, double* v_src,
                            double* v_rcv, double* v_group) {
     if (!m || problem < 0 || problem >= m->P) return NCPA_EINVAL;
+    if (!m->host_valid) {
+        ncpa_status s = guarded(m->ctx, [&]() -> ncpa_status {
+            fetch_modes(m);
+            CK(cudaStreamSynchronize(m->ctx->stream));
+            return NCPA_OK;
+        });
+        if (s != NCPA_OK) return s;
+    }
     const ProblemInfo& pi = m->info[problem];
     const size_t o = pi.off, n = pi.M;
     if (re_k) std::memcpy(re_k, m->kr.data() + o, n * 8);
@@ -693,23 +845,29 @@ ncpa_status ncpa_modes_get_vectors(const ncpa_modes* m, int problem, double* v) 
 // ---------------------------------------------------------------------------
 ncpa_status ncpa_tl_1d(ncpa_ctx* ctx, const ncpa_modes* m, const ncpa_tl_params* tp, double* re, double* im,
                        double* incoh) {
-    if (!ctx || !m || !tp || !re || !im || !incoh) return NCPA_EINVAL;
+    if (!ctx || !m || !tp) return NCPA_EINVAL;
+    const bool keep = !re && !im && !incoh;
+    if (!keep && (!re || !im || !incoh)) return NCPA_EINVAL;
     return guarded(ctx, [&]() -> ncpa_status {
         if (tp->n_ranges < 1 || !(tp->dr_m > 0)) throw ApiError(NCPA_EINVAL, "bad range grid");
         CK(cudaSetDevice(ctx->device));
         cudaStream_t st = ctx->stream;
         const size_t n = (size_t)m->P * tp->n_ranges;
-        DevBuf dre, dim, dinc;
-        dre.alloc(n * 8);
-        dim.alloc(n * 8);
-        dinc.alloc(n * 8);
+        DevBuf& dre = m->tl_re;
+        DevBuf& dim = m->tl_im;
+        DevBuf& dinc = m->tl_inc;
+        dre.alloc(n * 8, st);
+        dim.alloc(n * 8, st);
+        dinc.alloc(n * 8, st);
         check_launch(ctx, ncpa::launch_tl1d(st, m->P, m->d_pinfo.as<ProblemInfo>(), m->d_kr.as<double>(),
                                             m->d_ki.as<double>(), m->d_vs.as<double>(), m->d_vr.as<double>(),
                                             tp->n_ranges, tp->dr_m, tp->lossless, dre.as<double>(), dim.as<double>(),
                                             dinc.as<double>()));
-        CK(cudaMemcpyAsync(re, dre.p, n * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(im, dim.p, n * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(incoh, dinc.p, n * 8, cudaMemcpyDeviceToHost, st));
+        if (!keep) {
+            CK(cudaMemcpyAsync(re, dre.p, n * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(im, dim.p, n * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(incoh, dinc.p, n * 8, cudaMemcpyDeviceToHost, st));
+        }
         CK(cudaStreamSynchronize(st));
         return NCPA_OK;
     });
@@ -751,8 +909,8 @@ ncpa_status ncpa_tl_2d(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const nc
         upload(dvz, vz, st);
         upload(dvs, vsrc, st);
         const size_t n = (size_t)tp->n_ranges * nzo;
-        dre.alloc(n * 8);
-        dim.alloc(n * 8);
+        dre.alloc(n * 8, st);
+        dim.alloc(n * 8, st);
         check_launch(ctx, ncpa::launch_tl2d(st, Mm, m->d_kr.as<double>() + pi.off, m->d_ki.as<double>() + pi.off,
                                             dvs.as<double>(), dvz.as<double>(), nzo, tp->n_ranges, tp->dr_m,
                                             tp->lossless, dre.as<double>(), dim.as<double>()));
@@ -781,18 +939,19 @@ ncpa_status bb_common(ncpa_ctx* ctx, int nfreq, const double* d_f, const int* d_
         src[2 * i] = bp->src_re[i];
         src[2 * i + 1] = bp->src_im[i];
     }
-    DevBuf dr, dt0, dsrc, dh, dout;
+    DevBuf dr, dt0, dsrc, dh;
+    DevBuf& dout = ctx->bb_out;
     upload(dr, bp->ranges_m, nr, st);
     upload(dt0, t0, st);
     upload(dsrc, src, st);
-    dh.alloc((size_t)nr * nfreq * 16);
-    dout.alloc((size_t)nr * nfft * 8);
+    dh.alloc((size_t)nr * nfreq * 16, st);
+    dout.alloc((size_t)nr * nfft * 8, st);
     const double* tw = twiddle(ctx, nfft);
     check_launch(ctx, ncpa::launch_bb_transfer(st, nfreq, d_off, d_rk, d_ik, d_vs, d_vr, rho_ratio, nr,
                                                dr.as<double>(), bp->zero_attn, dh.as<double>()));
     check_launch(ctx, ncpa::launch_bb_pulse(st, nfreq, d_f, dsrc.as<double>(), dh.as<double>(), nr, dt0.as<double>(),
                                             nfft, tw, dout.as<double>()));
-    CK(cudaMemcpyAsync(waveforms, dout.p, (size_t)nr * nfft * 8, cudaMemcpyDeviceToHost, st));
+    if (waveforms) CK(cudaMemcpyAsync(waveforms, dout.p, (size_t)nr * nfft * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return NCPA_OK;
 }
@@ -800,7 +959,7 @@ ncpa_status bb_common(ncpa_ctx* ctx, int nfreq, const double* d_f, const int* d_
 
 ncpa_status ncpa_bb_synthesize(ncpa_ctx* ctx, const ncpa_dispersion_desc* d, const ncpa_bb_params* bp,
                                double* waveforms) {
-    if (!ctx || !d || !bp || !waveforms) return NCPA_EINVAL;
+    if (!ctx || !d || !bp) return NCPA_EINVAL;
     return guarded(ctx, [&]() -> ncpa_status {
         if (d->n_freq < 3 || !d->f || !d->mode_off) throw ApiError(NCPA_EINVAL, "dispersion needs >= 2 frequencies");
         CK(cudaSetDevice(ctx->device));
@@ -821,7 +980,7 @@ ncpa_status ncpa_bb_synthesize(ncpa_ctx* ctx, const ncpa_dispersion_desc* d, con
 
 ncpa_status ncpa_bb_synthesize_modes(ncpa_ctx* ctx, const ncpa_modes* m, int az_index, const ncpa_bb_params* bp,
                                      double* waveforms) {
-    if (!ctx || !m || !bp || !waveforms || az_index < 0 || az_index >= m->na) return NCPA_EINVAL;
+    if (!ctx || !m || !bp || az_index < 0 || az_index >= m->na) return NCPA_EINVAL;
     return guarded(ctx, [&]() -> ncpa_status {
         if (m->na != 1) throw ApiError(NCPA_EINVAL, "device-resident synthesis needs a single-azimuth solve");
         CK(cudaSetDevice(ctx->device));
@@ -852,7 +1011,7 @@ ncpa_status ncpa_source_spectrum_waveform(ncpa_ctx* ctx, const double* x, int n,
         cudaStream_t st = ctx->stream;
         DevBuf dx, ds;
         upload(dx, x, n, st);
-        ds.alloc((size_t)2 * nfreq * 8);
+        ds.alloc((size_t)2 * nfreq * 8, st);
         const double* tw = twiddle(ctx, nfft);
         check_launch(ctx, ncpa::launch_src_dft(st, n, dx.as<double>(), dt, nfft, nfreq, tw, ds.as<double>()));
         std::vector<double> h(2 * (size_t)nfreq);

@@ -26,7 +26,8 @@ EXPORTED = [
     "ncpa_ess_params_default", "ncpa_ess_solve", "ncpa_modes_destroy", "ncpa_modes_problems", "ncpa_modes_count",
     "ncpa_modes_info", "ncpa_modes_get", "ncpa_modes_get_vectors", "ncpa_tl_1d", "ncpa_tl_2d_heights",
     "ncpa_tl_2d", "ncpa_bb_synthesize", "ncpa_bb_synthesize_modes", "ncpa_source_spectrum_waveform",
-    "ncpa_kernel_launches",
+    "ncpa_kernel_launches", "ncpa_ctx_stream", "ncpa_ctx_set_timing", "ncpa_ctx_phase_stats",
+    "ncpa_ctx_reset_stats", "ncpa_ctx_sturm_sequences", "ncpa_probe_fp64_peak",
 ]
 
 
@@ -49,7 +50,8 @@ class EssParams(ctypes.Structure):
     _fields_ = [("nz_grid", _c_int), ("maxheight_km", _c_double), ("zground_km", _c_double),
                 ("sourceheight_km", _c_double), ("receiverheight_km", _c_double), ("lamb_wave_bc", _c_int),
                 ("turnoff_wkb", _c_int), ("wvnum_filter", _c_int), ("c_min", _c_double), ("c_max", _c_double),
-                ("want_group_speed", _c_int), ("want_vectors", _c_int), ("max_modes", _c_int)]
+                ("want_group_speed", _c_int), ("want_vectors", _c_int), ("max_modes", _c_int),
+                ("keep_on_device", _c_int)]
 
 
 class _TlParams(ctypes.Structure):
@@ -104,6 +106,13 @@ def lib():
         L.ncpa_source_spectrum_waveform.argtypes = [_vp, _dp, _c_int, _c_double, _c_int, _c_int, _dp, _dp]
         L.ncpa_kernel_launches.argtypes = [_vp]
         L.ncpa_kernel_launches.restype = _c_ll
+        L.ncpa_ctx_stream.argtypes = [_vp]
+        L.ncpa_ctx_stream.restype = _vp
+        L.ncpa_ctx_set_timing.argtypes = [_vp, _c_int]
+        L.ncpa_ctx_phase_stats.argtypes = [_vp, ctypes.c_char_p, _dp, ctypes.POINTER(_c_ll)]
+        L.ncpa_ctx_reset_stats.argtypes = [_vp]
+        L.ncpa_ctx_sturm_sequences.argtypes = [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]
+        L.ncpa_probe_fp64_peak.argtypes = [_vp, _dp]
         _lib = L
     return _lib
 
@@ -161,6 +170,33 @@ class Context:
     @property
     def launches(self):
         return int(lib().ncpa_kernel_launches(self.h))
+
+    @property
+    def stream_ptr(self):
+        return int(lib().ncpa_ctx_stream(self.h) or 0)
+
+    def set_timing(self, on=True):
+        self.check(lib().ncpa_ctx_set_timing(self.h, int(on)), "ncpa_ctx_set_timing")
+
+    def reset_stats(self):
+        self.check(lib().ncpa_ctx_reset_stats(self.h), "ncpa_ctx_reset_stats")
+
+    def phase_stats(self, phase):
+        ms, n = _c_double(), _c_ll()
+        self.check(lib().ncpa_ctx_phase_stats(self.h, phase.encode(), ctypes.byref(ms), ctypes.byref(n)),
+                   "ncpa_ctx_phase_stats")
+        return ms.value, n.value
+
+    def sturm_sequences(self):
+        a, b = _c_ll(), _c_ll()
+        self.check(lib().ncpa_ctx_sturm_sequences(self.h, ctypes.byref(a), ctypes.byref(b)),
+                   "ncpa_ctx_sturm_sequences")
+        return a.value, b.value
+
+    def fp64_peak_tflops(self):
+        t = _c_double()
+        self.check(lib().ncpa_probe_fp64_peak(self.h, ctypes.byref(t)), "ncpa_probe_fp64_peak")
+        return t.value
 
     # profiles -------------------------------------------------------------
     def load_profile(self, path, header=""):
@@ -275,8 +311,11 @@ class Modes:
         self.ctx.check(lib().ncpa_modes_get_vectors(self.h, p, _p(v)), "ncpa_modes_get_vectors")
         return v.reshape(nz, M)
 
-    def tl1d(self, n_ranges, dr_m, lossless=False):
+    def tl1d(self, n_ranges, dr_m, lossless=False, to_host=True):
         tp = _TlParams(int(n_ranges), float(dr_m), int(lossless))
+        if not to_host:
+            self.ctx.check(lib().ncpa_tl_1d(self.ctx.h, self.h, ctypes.byref(tp), None, None, None), "ncpa_tl_1d")
+            return None
         re, im, inc = (np.empty((self.P, n_ranges)) for _ in range(3))
         self.ctx.check(lib().ncpa_tl_1d(self.ctx.h, self.h, ctypes.byref(tp), _p(re), _p(im), _p(inc)),
                        "ncpa_tl_1d")
@@ -292,10 +331,10 @@ class Modes:
                        "ncpa_tl_2d")
         return z, re, im
 
-    def bb_synthesize(self, ranges_m, max_celerity, nfft, src_re, src_im, zero_attn=False):
+    def bb_synthesize(self, ranges_m, max_celerity, nfft, src_re, src_im, zero_attn=False, to_host=True):
         rng, sre, sim = _f64(ranges_m), _f64(src_re), _f64(src_im)
         bp = _BbParams(len(rng), _p(rng), float(max_celerity), int(nfft), _p(sre), _p(sim), int(zero_attn))
-        out = np.empty((len(rng), nfft))
+        out = np.empty((len(rng), nfft)) if to_host else None
         self.ctx.check(lib().ncpa_bb_synthesize_modes(self.ctx.h, self.h, 0, ctypes.byref(bp), _p(out)),
                        "ncpa_bb_synthesize_modes")
         return out
