@@ -198,8 +198,9 @@ def run_ours(args):
 
     for _ in range(args.warmup):
         step_device()
-    for _ in range(max(1, min(args.warmup, 2))):
-        step_e2e()
+    if not args.quick:
+        for _ in range(max(1, min(args.warmup, 2))):
+            step_e2e()
     # timed device-resident leg, with per-phase kernel timing on
     ctx.reset_stats()
     ctx.set_timing(True)
@@ -216,17 +217,25 @@ def run_ours(args):
     seqs, grid_pts = ctx.sturm_sequences()
     phases = {ph: ctx.phase_stats(ph)[0] / args.steps for ph in
               ("knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec", "fetch")}
+    if args.quick:
+        print(json.dumps({"quick": True, "ms_per_step": ms_dev / args.steps,
+                          "phases_ms": {k: round(v, 4) for k, v in phases.items()}}), flush=True)
+        prof.close()
+        ctx.close()
+        return
     ms_e2e = timed(step_e2e, args.steps)
     # plain per-frequency GPU path: one ncpa_ess_solve per frequency
     plain_freqs = freqs[::16]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    ev0.record(stream)
     for f in plain_freqs:
         m = ctx.solve(prof, params_dev, [f], az)
         m.tl1d(N_TL, DR_TL, to_host=False)
         m.close()
+    ev1.record(stream)
     torch.cuda.synchronize()
-    plain_rate = len(plain_freqs) / (time.perf_counter() - t0)
+    plain_rate = len(plain_freqs) / (ev0.elapsed_time(ev1) / 1e3)
 
     if world > 1:
         import torch.distributed as dist
@@ -358,6 +367,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--quick", action="store_true",
+                    help="device-resident leg only (no e2e, plain-path or CPU legs); for profiler runs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -166,6 +166,50 @@ struct SturmState {
             p1 *= sc;
         }
     }
+    // 32 steps carrying the x-derivative of the recurrence as well:
+    // d_i = (s_i - x) d_{i-1} - p_{i-1} - d_{i-2}; rescaled with p
+    __device__ __forceinline__ void word32_deriv(const double* __restrict__ s, double x, double& d0, double& d1) {
+        unsigned w = 0u;
+#pragma unroll
+        for (int u = 0; u < 32; u += 2) {
+            double2 sv = *reinterpret_cast<const double2*>(s + u);
+            double a0 = sv.x - x;
+            double q0 = fma(a0, p1, -p0);
+            double e0 = fma(a0, d1, -p1) - d0;
+            double a1 = sv.y - x;
+            double q1 = fma(a1, q0, -p1);
+            double e1 = fma(a1, e0, -q0) - d1;
+            w = __funnelshift_l(__double2hiint(q0), w, 1);
+            w = __funnelshift_l(__double2hiint(q1), w, 1);
+            p0 = q0;
+            p1 = q1;
+            d0 = e0;
+            d1 = e1;
+        }
+        unsigned prev = (w >> 1) | (prevbit << 31);
+        cnt += __popc(w ^ prev);
+        prevbit = w & 1u;
+        int sh = rescale_shift(fmax(fabs(p0), fabs(d0)), fmax(fabs(p1), fabs(d1)));
+        if (sh) {
+            double sc = pow2(-sh);
+            p0 *= sc;
+            p1 *= sc;
+            d0 *= sc;
+            d1 *= sc;
+        }
+    }
+    __device__ __forceinline__ void step_deriv(double si, double x, double& d0, double& d1) {
+        double a = si - x;
+        double q = fma(a, p1, -p0);
+        double e = fma(a, d1, -p1) - d0;
+        unsigned b = static_cast<unsigned>(__double2hiint(q)) >> 31;
+        cnt += static_cast<int>(b ^ prevbit);
+        prevbit = b;
+        p0 = p1;
+        p1 = q;
+        d0 = d1;
+        d1 = e;
+    }
     // single guarded step (ragged tail)
     __device__ __forceinline__ void step(double si, double x) {
         double a = si - x;

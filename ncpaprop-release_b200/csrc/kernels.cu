@@ -460,6 +460,43 @@ __device__ int cta_sturm_sweep(const double* __restrict__ s, int nz, double x, R
     return st.cnt;
 }
 
+// Same sweep; warps with deriv set also carry d/dx of the recurrence and
+// return the Newton ratio p_{n-1} / p'_{n-1} = det(S - x) / (d/dx det(S - x)).
+__device__ int cta_sturm_sweep_newton(const double* __restrict__ s, int nz, double x, bool deriv, Ring& r,
+                                      unsigned* err, double& ratio) {
+    const int nch = (nz + kChunk - 1) / kChunk;
+    const unsigned base = r.loads;
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < nch && c < kNbuf; ++c) ring_issue(r, base + c, s + (size_t)c * kChunk);
+    }
+    SturmState st;
+    st.reset();
+    double d0 = 0.0, d1 = 0.0;  // derivatives of p_{-2}, p_{-1}
+    for (int c = 0; c < nch; ++c) {
+        const unsigned k = base + c;
+        const int slot = k % kNbuf;
+        mbar_wait_bounded(&r.bars[slot], (k / kNbuf) & 1u, err);
+        const double* b = r.buf + slot * kChunk;
+        const int valid = min(kChunk, nz - c * kChunk);
+        const int nw = valid >> 5;
+        if (deriv) {
+            for (int w = 0; w < nw; ++w) st.word32_deriv(b + 32 * w, x, d0, d1);
+            for (int i = nw * 32; i < valid; ++i) st.step_deriv(b[i], x, d0, d1);
+        } else {
+            for (int w = 0; w < nw; ++w) st.word32(b + 32 * w, x);
+            for (int i = nw * 32; i < valid; ++i) st.step(b[i], x);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && c + kNbuf < nch) {
+            fence_proxy_async();
+            ring_issue(r, base + c + kNbuf, s + (size_t)(c + kNbuf) * kChunk);
+        }
+    }
+    r.loads = base + nch;
+    ratio = deriv ? st.p1 / d1 : 0.0;
+    return st.cnt;
+}
+
 __device__ __forceinline__ void ring_init(Ring& r, double* buf, uint64_t* bars) {
     r.buf = buf;
     r.bars = bars;
@@ -500,9 +537,18 @@ int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* 
     return 1;
 }
 
-// K3: persistent multisection.  A work item holds m <= 256 consecutive
-// eigen-indices of one problem; G = 2^k threads share an eigenvalue so that
-// G*m <= 256, and each round cuts every bracket into G+1 pieces.
+// K3: persistent multisection + safeguarded Newton.  A work item holds
+// m <= 256 consecutive eigen-indices of one problem.  Every round:
+//  * eigenvalues already isolated in a narrow bracket ("Newton slots") get one
+//    lane each, which sweeps the recurrence with its x-derivative and takes a
+//    Newton step on det(S - x) from the current iterate; the Sturm count at the
+//    iterate shrinks the bracket, and a step leaving the bracket falls back to
+//    its midpoint;
+//  * the remaining lanes are dealt round-robin over the other unconverged
+//    eigenvalues (G_e lanes each), which cut their bracket into G_e + 1 pieces.
+// Newton lanes occupy the first warps so that derivative sweeps stay
+// warp-uniform.  An eigenvalue converges when its bracket or its last Newton
+// step is below tol.
 __global__ void __launch_bounds__(kThreads) k_bisect(const ProblemInfo* __restrict__ pinfo,
                                                      const double* __restrict__ s, int nz, int nz_pad,
                                                      const int* __restrict__ counts,
@@ -512,12 +558,16 @@ __global__ void __launch_bounds__(kThreads) k_bisect(const ProblemInfo* __restri
     extern __shared__ __align__(128) unsigned char smem_raw[];
     double* buf = reinterpret_cast<double*>(smem_raw);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + kNbuf * kChunk * 8);
-    __shared__ double sa[kThreads], sb[kThreads];
-    __shared__ int sbest[kThreads];
+    __shared__ double sa[kThreads], sb[kThreads], sx[kThreads];
+    __shared__ int sca[kThreads], scb[kThreads];  // Sturm counts at the bracket ends
+    __shared__ int smode[kThreads];               // 0 multisection, 1 Newton, 2 converged
+    __shared__ int sbest[kThreads], slcnt[kThreads];
+    __shared__ int sact[kThreads], srank[kThreads];
+    __shared__ int swarp[2][kThreads / 32];
     __shared__ int s_item;
     Ring r;
     ring_init(r, buf, bars);
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (;;) {
         if (tid == 0) s_item = atomicAdd(counter, 1);
         __syncthreads();
@@ -528,47 +578,133 @@ __global__ void __launch_bounds__(kThreads) k_bisect(const ProblemInfo* __restri
         const ProblemInfo pi = pinfo[w.problem];
         const int* cnt = counts + (size_t)w.problem * kScanPoints;
         const double* sp = s + (size_t)w.problem * nz_pad;
-        int G = 1;
-        while (G * 2 * w.m <= kThreads) G *= 2;
-        if (tid < w.m) {  // initial bracket from the isolation scan
-            const int J = pi.c_lo + w.j0 + tid;
+        const bool own = tid < w.m;          // thread owns eigen slot tid
+        const int Jown = pi.c_lo + w.j0 + tid;
+        if (own) {  // initial bracket from the isolation scan
             int t0 = 0;
             for (int t = 0; t < kScanPoints; ++t)
-                if (cnt[t] <= J) t0 = t;
+                if (cnt[t] <= Jown) t0 = t;
             int t1 = kScanPoints - 1;
             for (int t = kScanPoints - 1; t > t0; --t)
-                if (cnt[t] > J) t1 = t;
-            if (cnt[t1] <= J) atomicOr(err, kErrBracket);
+                if (cnt[t] > Jown) t1 = t;
+            if (cnt[t1] <= Jown) atomicOr(err, kErrBracket);
             sa[tid] = scan_x(pi.lo, pi.hi, t0);
             sb[tid] = scan_x(pi.lo, pi.hi, t1);
+            sca[tid] = cnt[t0];
+            scb[tid] = cnt[t1];
+            smode[tid] = !(sb[tid] - sa[tid] > tol) ? 2 : 0;
+            sx[tid] = 0.5 * (sa[tid] + sb[tid]);
         }
         __syncthreads();
-        const int e = tid / G, gi = tid % G;
-        const bool active = e < w.m;
-        const int J = pi.c_lo + w.j0 + e;
-        const double frac = (double)(gi + 1) / (double)(G + 1);
-        for (int round = 0; round < 256; ++round) {
-            double a = active ? sa[e] : pi.lo, b = active ? sb[e] : pi.hi;
-            double x = a + (b - a) * frac;
-            int c = cta_sturm_sweep(sp, nz, x, r, err);
-            if (seq_counter && tid == 0) atomicAdd(seq_counter, (unsigned long long)(G * w.m));
-            if (tid < w.m) sbest[tid] = -1;
+        for (int round = 0; round < 512; ++round) {
+            // compact Newton slots, then multisection slots (ballot prefix)
+            const int md = own ? smode[tid] : 2;
+            const unsigned balN = __ballot_sync(0xffffffffu, md == 1);
+            const unsigned balB = __ballot_sync(0xffffffffu, md == 0);
+            if (lane == 0) {
+                swarp[0][wid] = __popc(balN);
+                swarp[1][wid] = __popc(balB);
+            }
             __syncthreads();
-            if (active && c <= J) atomicMax(&sbest[e], gi);
+            int baseN = 0, baseB = 0, nN = 0, nB = 0;
+            for (int k = 0; k < kThreads / 32; ++k) {
+                if (k < wid) {
+                    baseN += swarp[0][k];
+                    baseB += swarp[1][k];
+                }
+                nN += swarp[0][k];
+                nB += swarp[1][k];
+            }
+            const unsigned below = (1u << lane) - 1u;
+            if (md == 1) {
+                const int pos = baseN + __popc(balN & below);
+                sact[pos] = tid;
+                srank[tid] = pos;
+            } else if (md == 0) {
+                const int pos = nN + baseB + __popc(balB & below);
+                sact[pos] = tid;
+                srank[tid] = pos - nN;
+            }
+            if (own) sbest[tid] = -1;
             __syncthreads();
-            bool done = true;
-            if (tid < w.m) {
-                double A = sa[tid], B = sb[tid];
-                int gb = sbest[tid];
-                double na = gb >= 0 ? A + (B - A) * ((double)(gb + 1) / (double)(G + 1)) : A;
-                double nb = gb + 1 < G ? A + (B - A) * ((double)(gb + 2) / (double)(G + 1)) : B;
+            if (nN + nB == 0) break;
+            // this lane's role
+            const int nlanesB = kThreads - nN;
+            int e, gi = 0, G = 1;
+            bool newton = tid < nN;
+            if (newton) {
+                e = sact[tid];
+            } else if (nB > 0) {
+                const int t = tid - nN;
+                const int k = t % nB;
+                e = sact[nN + k];
+                gi = t / nB;
+                G = (nlanesB - 1 - k) / nB + 1;
+            } else {
+                e = sact[0];  // spare lane: repeat a Newton point, result unused
+                newton = false;
+            }
+            double x;
+            if (newton) {
+                x = sx[e];
+            } else {
+                const double a = sa[e], b = sb[e];
+                x = a + (b - a) * ((double)(gi + 1) / (double)(G + 1));
+            }
+            const bool warp_deriv = (wid * 32) < nN;
+            double ratio = 0.0;
+            const int c = cta_sturm_sweep_newton(sp, nz, x, warp_deriv, r, err, ratio);
+            if (seq_counter && tid == 0) atomicAdd(seq_counter, (unsigned long long)kThreads);
+            const int Je = pi.c_lo + w.j0 + e;
+            if (!newton && nB > 0) {
+                slcnt[tid] = c;
+                if (c <= Je) atomicMax(&sbest[e], gi);
+            }
+            if (newton) {  // one lane per Newton slot: update it directly
+                double A = sa[e], B = sb[e];
+                if (c <= Je) {
+                    A = x;
+                    sca[e] = c;
+                } else {
+                    B = x;
+                    scb[e] = c;
+                }
+                sa[e] = A;
+                sb[e] = B;
+                if (fabs(ratio) <= tol) {  // converged: final step stays inside the bracket
+                    sx[e] = fmin(fmax(x - ratio, A), B);
+                    smode[e] = 2;
+                } else {
+                    double xn = x - ratio;
+                    const bool ok = isfinite(xn) && xn > A && xn < B;
+                    sx[e] = ok ? xn : 0.5 * (A + B);
+                    if (!(B - A > tol)) smode[e] = 2;
+                }
+            }
+            __syncthreads();
+            if (own && md == 0) {
+                const int kk = srank[tid];
+                const int Gs = (nlanesB - 1 - kk) / nB + 1;
+                const double A = sa[tid], B = sb[tid];
+                const int gb = sbest[tid];
+                const double na = gb >= 0 ? A + (B - A) * ((double)(gb + 1) / (double)(Gs + 1)) : A;
+                const double nb = gb + 1 < Gs ? A + (B - A) * ((double)(gb + 2) / (double)(Gs + 1)) : B;
+                // counts at the new ends: lanes of this slot are nN + kk + g * nB
+                if (gb >= 0) sca[tid] = slcnt[nN + kk + gb * nB];
+                if (gb + 1 < Gs) scb[tid] = slcnt[nN + kk + (gb + 1) * nB];
                 sa[tid] = na;
                 sb[tid] = nb;
-                done = !(nb - na > tol) || (na == A && nb == B);
+                sx[tid] = 0.5 * (na + nb);
+                if (!(nb - na > tol) || (na == A && nb == B)) {
+                    smode[tid] = 2;
+                } else if (sca[tid] == Jown && scb[tid] == Jown + 1 &&
+                           nb - na <= 1.0e-6 * fmax(fabs(na), fabs(nb))) {
+                    smode[tid] = 1;  // isolated and narrow: Newton from here
+                }
             }
-            if (__syncthreads_and(done)) break;
+            __syncthreads();
         }
-        if (tid < w.m) mu[pi.off + w.j0 + tid] = 0.5 * (sa[tid] + sb[tid]);
+        if (own) mu[pi.off + w.j0 + tid] = sx[tid];
         __syncthreads();
     }
 }
@@ -616,7 +752,7 @@ int launch_fp64_probe(cudaStream_t st, int grid, int block, int n_iter, double* 
 constexpr int kEvNbuf = 2;
 
 struct EvRing {
-    double* sbuf;    // [kEvNbuf][kChunk]
+    double* sbuf;    // [kEvNbuf][kEvChunk]
     double* wbuf;
     double* gbuf;
     uint64_t* bars;  // [kEvNbuf]
@@ -626,11 +762,11 @@ struct EvRing {
 __device__ __forceinline__ void evring_issue(EvRing& r, unsigned k, int c, const double* sp, const double* wp,
                                              const double* gp) {
     int slot = k % kEvNbuf;
-    uint32_t bytes = kChunk * 8 * (1 + (wp ? 1 : 0) + (gp ? 1 : 0));
+    uint32_t bytes = kEvChunk * 8 * (1 + (wp ? 1 : 0) + (gp ? 1 : 0));
     mbar_expect_tx(&r.bars[slot], bytes);
-    tma_load_1d(r.sbuf + slot * kChunk, sp + (size_t)c * kChunk, kChunk * 8, &r.bars[slot]);
-    if (wp) tma_load_1d(r.wbuf + slot * kChunk, wp + (size_t)c * kChunk, kChunk * 8, &r.bars[slot]);
-    if (gp) tma_load_1d(r.gbuf + slot * kChunk, gp + (size_t)c * kChunk, kChunk * 8, &r.bars[slot]);
+    tma_load_1d(r.sbuf + slot * kEvChunk, sp + (size_t)c * kEvChunk, kEvChunk * 8, &r.bars[slot]);
+    if (wp) tma_load_1d(r.wbuf + slot * kEvChunk, wp + (size_t)c * kEvChunk, kEvChunk * 8, &r.bars[slot]);
+    if (gp) tma_load_1d(r.gbuf + slot * kEvChunk, gp + (size_t)c * kEvChunk, kEvChunk * 8, &r.bars[slot]);
 }
 
 __device__ __forceinline__ cuda::std::complex<double> csqrt_principal(double x, double y) {
@@ -642,13 +778,13 @@ __device__ __forceinline__ cuda::std::complex<double> csqrt_principal(double x, 
 }
 
 template <bool kGroup, bool kVec>
-__global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
+__global__ void __launch_bounds__(kEvThreads) k_eigvec(EigvecArgs A) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     EvRing R;
     R.sbuf = reinterpret_cast<double*>(smem_raw);
-    R.wbuf = R.sbuf + kEvNbuf * kChunk;
-    R.gbuf = R.wbuf + kEvNbuf * kChunk;
-    R.bars = reinterpret_cast<uint64_t*>(R.gbuf + kEvNbuf * kChunk);
+    R.wbuf = R.sbuf + kEvNbuf * kEvChunk;
+    R.gbuf = R.wbuf + kEvNbuf * kEvChunk;
+    R.bars = reinterpret_cast<uint64_t*>(R.gbuf + kEvNbuf * kEvChunk);
     R.loads = 0;
     __shared__ int s_item;
     const int tid = threadIdx.x;
@@ -658,7 +794,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
     }
     __syncthreads();
     const int nz = A.nz;
-    const int nch = (nz + kChunk - 1) / kChunk;
+    const int nch = (nz + kEvChunk - 1) / kEvChunk;
     const int nblk = (nz + kBlk - 1) / kBlk;
     double* ck1 = A.ck_q1 + (size_t)blockIdx.x * A.ck_slot_stride;
     double* ck2 = A.ck_q2 + (size_t)blockIdx.x * A.ck_slot_stride;
@@ -690,8 +826,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
                 const unsigned k = base + o;
                 const int slot = k % kEvNbuf;
                 mbar_wait_bounded(&R.bars[slot], (k / kEvNbuf) & 1u, A.err);
-                const double* sb = R.sbuf + slot * kChunk;
-                const int valid = min(kChunk, nz - c * kChunk);
+                const double* sb = R.sbuf + slot * kEvChunk;
+                const int valid = min(kEvChunk, nz - c * kEvChunk);
                 for (int lb = ((valid - 1) / kBlk) * kBlk; lb >= 0; lb -= kBlk) {
 #pragma unroll
                     for (int u = kBlk - 1; u >= 0; --u) {
@@ -702,9 +838,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
                             q1 = qi;
                         }
                     }
-                    const int gbase = c * kChunk + lb;
+                    const int gbase = c * kEvChunk + lb;
                     if (gbase > 0) {
-                        const size_t ci = (size_t)(gbase / kBlk - 1) * kThreads + tid;
+                        const size_t ci = (size_t)(gbase / kBlk - 1) * kEvThreads + tid;
                         ck1[ci] = q1;
                         ck2[ci] = q2;
                         cke[ci] = E;
@@ -751,7 +887,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
                     a2 = 0.0;
                     ae = 0;
                 } else {
-                    size_t ci = (size_t)kb * kThreads + tid;
+                    size_t ci = (size_t)kb * kEvThreads + tid;
                     a1 = ck1[ci];
                     a2 = ck2[ci];
                     ae = cke[ci];
@@ -762,12 +898,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
                 const unsigned k = base + c;
                 const int slot = k % kEvNbuf;
                 mbar_wait_bounded(&R.bars[slot], (k / kEvNbuf) & 1u, A.err);
-                const double* sb = R.sbuf + slot * kChunk;
-                const double* wb = R.wbuf + slot * kChunk;
-                const double* gb = R.gbuf + slot * kChunk;
-                const int valid = min(kChunk, nz - c * kChunk);
+                const double* sb = R.sbuf + slot * kEvChunk;
+                const double* wb = R.wbuf + slot * kEvChunk;
+                const double* gb = R.gbuf + slot * kEvChunk;
+                const int valid = min(kEvChunk, nz - c * kEvChunk);
                 for (int lb = 0; lb < valid; lb += kBlk) {
-                    const int gbase = c * kChunk + lb;
+                    const int gbase = c * kEvChunk + lb;
                     const int kb = gbase / kBlk;
                     double q1 = nq1, q2 = nq2;
                     const int Eb = nE;
@@ -790,7 +926,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
                         if (idx == ctop) {
                             qb[jj] = q1;
                         } else if (idx < ctop) {
-                            double qi = fma(sb[idx - c * kChunk] - mu, q1, -q2);
+                            double qi = fma(sb[idx - c * kEvChunk] - mu, q1, -q2);
                             qb[jj] = qi;
                             q2 = q1;
                             q1 = qi;
@@ -917,7 +1053,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
                     a2 = 0.0;
                     ae = 0;
                 } else {
-                    size_t ci = (size_t)kb * kThreads + tid;
+                    size_t ci = (size_t)kb * kEvThreads + tid;
                     a1 = ck1[ci];
                     a2 = ck2[ci];
                     ae = cke[ci];
@@ -929,10 +1065,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
                 const unsigned k = base + c;
                 const int slot = k % kEvNbuf;
                 mbar_wait_bounded(&R.bars[slot], (k / kEvNbuf) & 1u, A.err);
-                const double* sb = R.sbuf + slot * kChunk;
-                const int valid = min(kChunk, nz - c * kChunk);
+                const double* sb = R.sbuf + slot * kEvChunk;
+                const int valid = min(kEvChunk, nz - c * kEvChunk);
                 for (int lb = 0; lb < valid; lb += kBlk) {
-                    const int gbase = c * kChunk + lb;
+                    const int gbase = c * kEvChunk + lb;
                     const int kb = gbase / kBlk;
                     double q1 = nq1, q2 = nq2;
                     const int Eb = nE;
@@ -945,7 +1081,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
                         if (idx == ctop) {
                             qb[jj] = q1;
                         } else if (idx < ctop) {
-                            double qi = fma(sb[idx - c * kChunk] - mu, q1, -q2);
+                            double qi = fma(sb[idx - c * kEvChunk] - mu, q1, -q2);
                             qb[jj] = qi;
                             q2 = q1;
                             q1 = qi;
@@ -988,22 +1124,37 @@ __global__ void __launch_bounds__(kThreads, 1) k_eigvec(EigvecArgs A) {
     }
 }
 
-int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a) {
-    size_t sm = 3 * kEvNbuf * kChunk * 8 + kEvNbuf * 8;
+template <bool G, bool V>
+static void* eigvec_fn() {
+    return (void*)k_eigvec<G, V>;
+}
+
+static size_t eigvec_smem() { return 3 * kEvNbuf * kEvChunk * 8 + kEvNbuf * 8; }
+
+static void* eigvec_select(const EigvecArgs& a) {
     const bool grp = a.g != nullptr, vec = a.vfull != nullptr;
-    if (grp && vec) {
-        cudaFuncSetAttribute(k_eigvec<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_eigvec<true, true><<<grid, kThreads, sm, st>>>(a);
-    } else if (grp) {
-        cudaFuncSetAttribute(k_eigvec<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_eigvec<true, false><<<grid, kThreads, sm, st>>>(a);
-    } else if (vec) {
-        cudaFuncSetAttribute(k_eigvec<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_eigvec<false, true><<<grid, kThreads, sm, st>>>(a);
-    } else {
-        cudaFuncSetAttribute(k_eigvec<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_eigvec<false, false><<<grid, kThreads, sm, st>>>(a);
-    }
+    if (grp && vec) return eigvec_fn<true, true>();
+    if (grp) return eigvec_fn<true, false>();
+    if (vec) return eigvec_fn<false, true>();
+    return eigvec_fn<false, false>();
+}
+
+int eigvec_ctas_per_sm(const EigvecArgs& a) {
+    int n = 1;
+    void* f = eigvec_select(a);
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eigvec_smem());
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kEvThreads, eigvec_smem()) != cudaSuccess) n = 1;
+    return n < 1 ? 1 : n;
+}
+
+int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a) {
+    const size_t sm = eigvec_smem();
+    const bool grp = a.g != nullptr, vec = a.vfull != nullptr;
+    cudaFuncSetAttribute(eigvec_select(a), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (grp && vec) k_eigvec<true, true><<<grid, kEvThreads, sm, st>>>(a);
+    else if (grp) k_eigvec<true, false><<<grid, kEvThreads, sm, st>>>(a);
+    else if (vec) k_eigvec<false, true><<<grid, kEvThreads, sm, st>>>(a);
+    else k_eigvec<false, false><<<grid, kEvThreads, sm, st>>>(a);
     return 1;
 }
 

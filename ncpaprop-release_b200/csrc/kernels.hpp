@@ -36,7 +36,9 @@ struct WorkItem {
 constexpr int kScanPoints = 256;  // Sturm counts per problem in the isolation scan
 constexpr int kChunk = 1024;      // doubles per TMA chunk of the diagonal
 constexpr int kBlk = 16;          // eigenvector checkpoint interval
-constexpr int kThreads = 256;     // threads of the bisection / eigenvector CTAs
+constexpr int kThreads = 256;     // threads of the scan / bisection CTAs
+constexpr int kEvThreads = 64;    // threads (= eigenvalues) of an eigenvector CTA
+constexpr int kEvChunk = 512;     // doubles per TMA chunk in the eigenvector kernel
 
 // knot-level derived quantities
 int launch_steffen(cudaStream_t st, int n, const double* x, const double* y, int batch, int ystride,
@@ -102,6 +104,8 @@ struct EigvecArgs {
     unsigned* err;
 };
 int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a);
+// resident eigenvector CTAs per SM for the variant selected by a
+int eigvec_ctas_per_sm(const EigvecArgs& a);
 // modal sums
 int launch_tl1d(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* kr, const double* ki,
                 const double* vs, const double* vr, int nr, double dr, int lossless, double* re, double* im,

@@ -718,16 +718,16 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
                                                   ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr));
             if (ctx->stats) ctx->grid_points += nz;
             tm.mark("bisect");
-            // ---- K4 eigenvectors ----
-            int grid_e = std::min(n_items, ctx->num_sms * 2);
-            const long long nblk = (nz + ncpa::kBlk - 1) / ncpa::kBlk;
-            const long long slot = nblk * ncpa::kThreads;
-            const size_t need = (size_t)grid_e * slot;
-            if (ctx->ck1.bytes < need * 8) {
-                ctx->ck1.alloc(need * 8, st);
-                ctx->ck2.alloc(need * 8, st);
-                ctx->cke.alloc(need * 4, st);
+            // ---- K4 eigenvectors: items of <= kEvThreads eigenvalues ----
+            std::vector<WorkItem> ev_items;
+            for (int p = 0; p < P; ++p) {
+                const int Mp = M->info[p].M;
+                for (int j0 = 0; j0 < Mp; j0 += ncpa::kEvThreads)
+                    ev_items.push_back(WorkItem{p, j0, std::min(ncpa::kEvThreads, Mp - j0), 0});
             }
+            DevBuf d_ev_items;
+            upload(d_ev_items, ev_items, st);
+            const int n_ev = (int)ev_items.size();
             ncpa::EigvecArgs ea{};
             ea.pinfo = d_pinfo;
             ea.s = s.as<double>();
@@ -737,8 +737,8 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
             ea.nz_pad = nz_pad;
             ea.wstride = nz_pad;
             ea.n_az = n_az;
-            ea.items = d_items.as<WorkItem>();
-            ea.n_items = n_items;
+            ea.items = d_ev_items.as<WorkItem>();
+            ea.n_items = n_ev;
             ea.counter = d_counter.as<int>() + 1;
             ea.mu = mu.as<double>();
             ea.isrc = M->isrc;
@@ -752,6 +752,15 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
             ea.vg = M->d_vg.as<double>();
             ea.vfull = prm->want_vectors ? M->d_vfull.as<double>() : nullptr;
             ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
+            const int grid_e = std::min(n_ev, ctx->num_sms * ncpa::eigvec_ctas_per_sm(ea));
+            const long long nblk = (nz + ncpa::kBlk - 1) / ncpa::kBlk;
+            const long long slot = nblk * ncpa::kEvThreads;
+            const size_t need = (size_t)grid_e * slot;
+            if (ctx->ck1.bytes < need * 8) {
+                ctx->ck1.alloc(need * 8, st);
+                ctx->ck2.alloc(need * 8, st);
+                ctx->cke.alloc(need * 4, st);
+            }
             ea.ck_q1 = ctx->ck1.as<double>();
             ea.ck_q2 = ctx->ck2.as<double>();
             ea.ck_e = ctx->cke.as<int>();
