@@ -114,11 +114,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after ~2^22 polls (each poll may suspend the thread
-// for a hardware-chosen interval), records kErrTimeout and returns false.
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait: gives up after one second of wall time (or at once when
+// another wait of this launch already gave up), records kErrTimeout and
+// returns false.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned* err) {
-    for (int it = 0; it < (1 << 22); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > 1000000000ull || (*((volatile unsigned*)err) & kErrTimeout)) break;
     }
     atomicOr(err, kErrTimeout);
     return false;

@@ -537,185 +537,321 @@ int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* 
     return 1;
 }
 
-// K3: persistent multisection + safeguarded Newton.  A work item holds
-// m <= 256 consecutive eigen-indices of one problem.  Every round:
+// K3: per-warp multisection + safeguarded Newton.
+//
+// Each warp owns a work item of m <= kWItem consecutive eigen-indices of one
+// problem and streams that problem's diagonal through its own TMA ring in
+// shared memory (kWBuf chunks of kWChunk doubles, one mbarrier per slot), so
+// warps never wait on each other.  Every lane runs two independent Sturm
+// chains (virtual lanes v = lane and lane + 32).  Every round:
 //  * eigenvalues already isolated in a narrow bracket ("Newton slots") get one
-//    lane each, which sweeps the recurrence with its x-derivative and takes a
-//    Newton step on det(S - x) from the current iterate; the Sturm count at the
-//    iterate shrinks the bracket, and a step leaving the bracket falls back to
-//    its midpoint;
-//  * the remaining lanes are dealt round-robin over the other unconverged
-//    eigenvalues (G_e lanes each), which cut their bracket into G_e + 1 pieces.
-// Newton lanes occupy the first warps so that derivative sweeps stay
-// warp-uniform.  An eigenvalue converges when its bracket or its last Newton
-// step is below tol.
-__global__ void __launch_bounds__(kThreads) k_bisect(const ProblemInfo* __restrict__ pinfo,
-                                                     const double* __restrict__ s, int nz, int nz_pad,
-                                                     const int* __restrict__ counts,
-                                                     const WorkItem* __restrict__ items, int n_items,
-                                                     int* counter, double tol, double* __restrict__ mu,
-                                                     unsigned* err, unsigned long long* seq_counter) {
+//    virtual lane each, which carries the x-derivative of the recurrence and
+//    takes a Newton step on det(S - x); the Sturm count at the iterate shrinks
+//    the bracket and a step leaving the bracket falls back to its midpoint;
+//  * the other virtual lanes are dealt round-robin over the remaining
+//    unconverged eigenvalues (G_e lanes each), which cut their bracket into
+//    G_e + 1 pieces.
+// Lane l owns eigen slots l and l + 32 (bracket, iterate, end counts, mode).
+constexpr int kWChunk = 512;
+constexpr int kWBuf = 3;
+constexpr int kWarpsPerCta = 4;
+
+struct WarpRing {
+    double* buf;     // [kWBuf][kWChunk]
+    uint64_t* bars;  // [kWBuf]
+    unsigned loads;  // identical in all lanes
+};
+
+__device__ __forceinline__ void wring_issue(WarpRing& r, unsigned k, const double* src) {
+    const int slot = k % kWBuf;
+    mbar_expect_tx(&r.bars[slot], kWChunk * 8);
+    tma_load_1d(r.buf + slot * kWChunk, src, kWChunk * 8, &r.bars[slot]);
+}
+
+// position of the n-th (0-based) set bit of m
+__device__ __forceinline__ int nth_bit(unsigned m, int n) {
+    int pos = 0;
+#pragma unroll
+    for (int sh = 16; sh >= 1; sh >>= 1) {
+        const unsigned low = m & ((1u << sh) - 1u);
+        const int c = __popc(low);
+        if (n >= c) {
+            n -= c;
+            m >>= sh;
+            pos += sh;
+        } else {
+            m = low;
+        }
+    }
+    return pos;
+}
+__device__ __forceinline__ int nth_bit64(unsigned lo, unsigned hi, int n) {
+    const int c = __popc(lo);
+    return n < c ? nth_bit(lo, n) : 32 + nth_bit(hi, n - c);
+}
+__device__ __forceinline__ int rank64(unsigned lo, unsigned hi, int e) {
+    return e < 32 ? __popc(lo & ((1u << e) - 1u)) : __popc(lo) + __popc(hi & ((1u << (e - 32)) - 1u));
+}
+// value held by lane (e & 31) for half (e >> 5)
+__device__ __forceinline__ double fetch2(double v0, double v1, int e) {
+    const double a = __shfl_sync(0xffffffffu, v0, e & 31);
+    const double b = __shfl_sync(0xffffffffu, v1, e & 31);
+    return (e >> 5) ? b : a;
+}
+__device__ __forceinline__ int fetch2i(int v0, int v1, int e) {
+    const int a = __shfl_sync(0xffffffffu, v0, e & 31);
+    const int b = __shfl_sync(0xffffffffu, v1, e & 31);
+    return (e >> 5) ? b : a;
+}
+
+// one sweep of two chains over the diagonal; dflag: 0 none, 1 chain 0 carries
+// the derivative, 2 both chains do
+__device__ void warp_sweep2(const double* __restrict__ s, int nz, double x0, double x1, int dflag, WarpRing& r,
+                            unsigned* err, int& c0, int& c1, double& rat0, double& rat1) {
+    const int lane = threadIdx.x & 31;
+    const int nch = (nz + kWChunk - 1) / kWChunk;
+    const unsigned base = r.loads;
+    if (lane == 0)
+        for (int c = 0; c < nch && c < kWBuf; ++c) wring_issue(r, base + c, s + (size_t)c * kWChunk);
+    __syncwarp();
+    SturmState A, B;
+    A.reset();
+    B.reset();
+    double da0 = 0.0, da1 = 0.0, db0 = 0.0, db1 = 0.0;
+    for (int c = 0; c < nch; ++c) {
+        const unsigned k = base + c;
+        const int slot = k % kWBuf;
+        mbar_wait_bounded(&r.bars[slot], (k / kWBuf) & 1u, err);
+        const double* b = r.buf + slot * kWChunk;
+        const int valid = min(kWChunk, nz - c * kWChunk);
+        const int nw = valid >> 5;
+        if (dflag == 0) {
+            for (int w = 0; w < nw; ++w) {
+                A.word32(b + 32 * w, x0);
+                B.word32(b + 32 * w, x1);
+            }
+            for (int i = nw * 32; i < valid; ++i) {
+                A.step(b[i], x0);
+                B.step(b[i], x1);
+            }
+        } else if (dflag == 1) {
+            for (int w = 0; w < nw; ++w) {
+                A.word32_deriv(b + 32 * w, x0, da0, da1);
+                B.word32(b + 32 * w, x1);
+            }
+            for (int i = nw * 32; i < valid; ++i) {
+                A.step_deriv(b[i], x0, da0, da1);
+                B.step(b[i], x1);
+            }
+        } else {
+            for (int w = 0; w < nw; ++w) {
+                A.word32_deriv(b + 32 * w, x0, da0, da1);
+                B.word32_deriv(b + 32 * w, x1, db0, db1);
+            }
+            for (int i = nw * 32; i < valid; ++i) {
+                A.step_deriv(b[i], x0, da0, da1);
+                B.step_deriv(b[i], x1, db0, db1);
+            }
+        }
+        __syncwarp();
+        if (lane == 0 && c + kWBuf < nch) {
+            fence_proxy_async();
+            wring_issue(r, base + c + kWBuf, s + (size_t)(c + kWBuf) * kWChunk);
+        }
+    }
+    r.loads = base + nch;
+    c0 = A.cnt;
+    c1 = B.cnt;
+    rat0 = dflag >= 1 ? A.p1 / da1 : 0.0;
+    rat1 = dflag >= 2 ? B.p1 / db1 : 0.0;
+}
+
+__global__ void __launch_bounds__(kWarpsPerCta * 32) k_bisect(const ProblemInfo* __restrict__ pinfo,
+                                                              const double* __restrict__ s, int nz, int nz_pad,
+                                                              const int* __restrict__ counts,
+                                                              const WorkItem* __restrict__ items, int n_items,
+                                                              int* counter, double tol, double* __restrict__ mu,
+                                                              unsigned* err, unsigned long long* seq_counter) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    double* buf = reinterpret_cast<double*>(smem_raw);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + kNbuf * kChunk * 8);
-    __shared__ double sa[kThreads], sb[kThreads], sx[kThreads];
-    __shared__ int sca[kThreads], scb[kThreads];  // Sturm counts at the bracket ends
-    __shared__ int smode[kThreads];               // 0 multisection, 1 Newton, 2 converged
-    __shared__ int sbest[kThreads], slcnt[kThreads];
-    __shared__ int sact[kThreads], srank[kThreads];
-    __shared__ int swarp[2][kThreads / 32];
-    __shared__ int s_item;
-    Ring r;
-    ring_init(r, buf, bars);
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpRing r;
+    r.buf = reinterpret_cast<double*>(smem_raw) + (size_t)wid * kWBuf * kWChunk;
+    r.bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarpsPerCta * kWBuf * kWChunk * 8) + wid * kWBuf;
+    r.loads = 0;
+    if (lane == 0) {
+        for (int k = 0; k < kWBuf; ++k) mbar_init(&r.bars[k], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
     for (;;) {
-        if (tid == 0) s_item = atomicAdd(counter, 1);
-        __syncthreads();
-        const int it = s_item;
-        __syncthreads();
+        int it = 0;
+        if (lane == 0) it = atomicAdd(counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= n_items) break;
         const WorkItem w = items[it];
         const ProblemInfo pi = pinfo[w.problem];
         const int* cnt = counts + (size_t)w.problem * kScanPoints;
         const double* sp = s + (size_t)w.problem * nz_pad;
-        const bool own = tid < w.m;          // thread owns eigen slot tid
-        const int Jown = pi.c_lo + w.j0 + tid;
-        if (own) {  // initial bracket from the isolation scan
-            int t0 = 0;
-            for (int t = 0; t < kScanPoints; ++t)
-                if (cnt[t] <= Jown) t0 = t;
-            int t1 = kScanPoints - 1;
-            for (int t = kScanPoints - 1; t > t0; --t)
-                if (cnt[t] > Jown) t1 = t;
-            if (cnt[t1] <= Jown) atomicOr(err, kErrBracket);
-            sa[tid] = scan_x(pi.lo, pi.hi, t0);
-            sb[tid] = scan_x(pi.lo, pi.hi, t1);
-            sca[tid] = cnt[t0];
-            scb[tid] = cnt[t1];
-            smode[tid] = !(sb[tid] - sa[tid] > tol) ? 2 : 0;
-            sx[tid] = 0.5 * (sa[tid] + sb[tid]);
+        // per-lane state of slots e0 = lane, e1 = lane + 32
+        double a[2], b[2], x[2];
+        int ca[2], cb[2], mode[2], J[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int e = lane + 32 * h;
+            mode[h] = 2;
+            a[h] = b[h] = x[h] = pi.lo;
+            ca[h] = cb[h] = 0;
+            J[h] = pi.c_lo + w.j0 + e;
+            if (e < w.m) {  // initial bracket from the isolation scan
+                int t0 = 0;
+                for (int t = 0; t < kScanPoints; ++t)
+                    if (cnt[t] <= J[h]) t0 = t;
+                int t1 = kScanPoints - 1;
+                for (int t = kScanPoints - 1; t > t0; --t)
+                    if (cnt[t] > J[h]) t1 = t;
+                if (cnt[t1] <= J[h]) atomicOr(err, kErrBracket);
+                a[h] = scan_x(pi.lo, pi.hi, t0);
+                b[h] = scan_x(pi.lo, pi.hi, t1);
+                ca[h] = cnt[t0];
+                cb[h] = cnt[t1];
+                x[h] = 0.5 * (a[h] + b[h]);
+                mode[h] = !(b[h] - a[h] > tol) ? 2 : 0;
+            }
         }
-        __syncthreads();
         for (int round = 0; round < 512; ++round) {
-            // compact Newton slots, then multisection slots (ballot prefix)
-            const int md = own ? smode[tid] : 2;
-            const unsigned balN = __ballot_sync(0xffffffffu, md == 1);
-            const unsigned balB = __ballot_sync(0xffffffffu, md == 0);
-            if (lane == 0) {
-                swarp[0][wid] = __popc(balN);
-                swarp[1][wid] = __popc(balB);
-            }
-            __syncthreads();
-            int baseN = 0, baseB = 0, nN = 0, nB = 0;
-            for (int k = 0; k < kThreads / 32; ++k) {
-                if (k < wid) {
-                    baseN += swarp[0][k];
-                    baseB += swarp[1][k];
-                }
-                nN += swarp[0][k];
-                nB += swarp[1][k];
-            }
-            const unsigned below = (1u << lane) - 1u;
-            if (md == 1) {
-                const int pos = baseN + __popc(balN & below);
-                sact[pos] = tid;
-                srank[tid] = pos;
-            } else if (md == 0) {
-                const int pos = nN + baseB + __popc(balB & below);
-                sact[pos] = tid;
-                srank[tid] = pos - nN;
-            }
-            if (own) sbest[tid] = -1;
-            __syncthreads();
+            const unsigned n0 = __ballot_sync(0xffffffffu, mode[0] == 1);
+            const unsigned n1 = __ballot_sync(0xffffffffu, mode[1] == 1);
+            const unsigned b0 = __ballot_sync(0xffffffffu, mode[0] == 0);
+            const unsigned b1 = __ballot_sync(0xffffffffu, mode[1] == 0);
+            const int nN = __popc(n0) + __popc(n1), nB = __popc(b0) + __popc(b1);
             if (nN + nB == 0) break;
-            // this lane's role
-            const int nlanesB = kThreads - nN;
-            int e, gi = 0, G = 1;
-            bool newton = tid < nN;
-            if (newton) {
-                e = sact[tid];
-            } else if (nB > 0) {
-                const int t = tid - nN;
-                const int k = t % nB;
-                e = sact[nN + k];
-                gi = t / nB;
-                G = (nlanesB - 1 - k) / nB + 1;
-            } else {
-                e = sact[0];  // spare lane: repeat a Newton point, result unused
-                newton = false;
-            }
-            double x;
-            if (newton) {
-                x = sx[e];
-            } else {
-                const double a = sa[e], b = sb[e];
-                x = a + (b - a) * ((double)(gi + 1) / (double)(G + 1));
-            }
-            const bool warp_deriv = (wid * 32) < nN;
-            double ratio = 0.0;
-            const int c = cta_sturm_sweep_newton(sp, nz, x, warp_deriv, r, err, ratio);
-            if (seq_counter && tid == 0) atomicAdd(seq_counter, (unsigned long long)kThreads);
-            const int Je = pi.c_lo + w.j0 + e;
-            if (!newton && nB > 0) {
-                slcnt[tid] = c;
-                if (c <= Je) atomicMax(&sbest[e], gi);
-            }
-            if (newton) {  // one lane per Newton slot: update it directly
-                double A = sa[e], B = sb[e];
-                if (c <= Je) {
-                    A = x;
-                    sca[e] = c;
-                } else {
-                    B = x;
-                    scb[e] = c;
-                }
-                sa[e] = A;
-                sb[e] = B;
-                if (fabs(ratio) <= tol) {  // converged: final step stays inside the bracket
-                    sx[e] = fmin(fmax(x - ratio, A), B);
-                    smode[e] = 2;
-                } else {
-                    double xn = x - ratio;
-                    const bool ok = isfinite(xn) && xn > A && xn < B;
-                    sx[e] = ok ? xn : 0.5 * (A + B);
-                    if (!(B - A > tol)) smode[e] = 2;
+            const int nlB = 64 - nN;
+            // roles of the two virtual lanes of this thread
+            double xv[2];
+            int ev[2], gv[2], Gv[2], role[2];  // role: 1 Newton, 0 multisection, -1 idle
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int v = lane + 32 * h;
+                role[h] = -1;
+                ev[h] = 0;
+                gv[h] = 0;
+                Gv[h] = 1;
+                if (v < nN) {
+                    role[h] = 1;
+                    ev[h] = nth_bit64(n0, n1, v);
+                } else if (nB > 0) {
+                    const int t = v - nN, k = t % nB;
+                    role[h] = 0;
+                    ev[h] = nth_bit64(b0, b1, k);
+                    gv[h] = t / nB;
+                    Gv[h] = (nlB - 1 - k) / nB + 1;
                 }
             }
-            __syncthreads();
-            if (own && md == 0) {
-                const int kk = srank[tid];
-                const int Gs = (nlanesB - 1 - kk) / nB + 1;
-                const double A = sa[tid], B = sb[tid];
-                const int gb = sbest[tid];
-                const double na = gb >= 0 ? A + (B - A) * ((double)(gb + 1) / (double)(Gs + 1)) : A;
-                const double nb = gb + 1 < Gs ? A + (B - A) * ((double)(gb + 2) / (double)(Gs + 1)) : B;
-                // counts at the new ends: lanes of this slot are nN + kk + g * nB
-                if (gb >= 0) sca[tid] = slcnt[nN + kk + gb * nB];
-                if (gb + 1 < Gs) scb[tid] = slcnt[nN + kk + (gb + 1) * nB];
-                sa[tid] = na;
-                sb[tid] = nb;
-                sx[tid] = 0.5 * (na + nb);
-                if (!(nb - na > tol) || (na == A && nb == B)) {
-                    smode[tid] = 2;
-                } else if (sca[tid] == Jown && scb[tid] == Jown + 1 &&
-                           nb - na <= 1.0e-6 * fmax(fabs(na), fabs(nb))) {
-                    smode[tid] = 1;  // isolated and narrow: Newton from here
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const double ae = fetch2(a[0], a[1], ev[h]);
+                const double be = fetch2(b[0], b[1], ev[h]);
+                const double xe = fetch2(x[0], x[1], ev[h]);
+                xv[h] = role[h] == 1 ? xe : ae + (be - ae) * ((double)(gv[h] + 1) / (double)(Gv[h] + 1));
+            }
+            int cv[2];
+            double rv[2];
+            const int dflag = nN > 32 ? 2 : (nN > 0 ? 1 : 0);
+            warp_sweep2(sp, nz, xv[0], xv[1], dflag, r, err, cv[0], cv[1], rv[0], rv[1]);
+            if (seq_counter && lane == 0) atomicAdd(seq_counter, (unsigned long long)64);
+            // owners update their slots.  Every __shfl_sync below is executed
+            // by all 32 lanes (no shuffle sits inside a lane-dependent branch).
+            const int Gmax = nB > 0 ? (nlB - 1) / nB + 1 : 0;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int e = lane + 32 * h;
+                const bool isN = mode[h] == 1, isB = mode[h] == 0;
+                // Newton result of this slot: virtual lane v = rank among Newton slots
+                const int vN = isN ? rank64(n0, n1, e) : 0;
+                const int srcN = vN & 31;
+                const int cN0 = __shfl_sync(0xffffffffu, cv[0], srcN), cN1 = __shfl_sync(0xffffffffu, cv[1], srcN);
+                const double rN0 = __shfl_sync(0xffffffffu, rv[0], srcN), rN1 = __shfl_sync(0xffffffffu, rv[1], srcN);
+                // multisection results of this slot: lanes nN + k + g nB, g < G
+                const int k = isB ? rank64(b0, b1, e) : 0;
+                const int G = isB ? (nlB - 1 - k) / nB + 1 : 0;
+                int gb = -1, cgb = ca[h];
+                for (int g = 0; g < Gmax; ++g) {
+                    const int v = nN + k + g * nB;
+                    const int src = v & 31;
+                    const int c0 = __shfl_sync(0xffffffffu, cv[0], src), c1 = __shfl_sync(0xffffffffu, cv[1], src);
+                    const int c = (v >> 5) ? c1 : c0;
+                    if (isB && g < G && c <= J[h]) {
+                        gb = g;
+                        cgb = c;
+                    }
+                }
+                const int g1 = gb + 1;
+                const int v1 = nN + k + g1 * nB;
+                const int src1 = (isB && g1 < G) ? (v1 & 31) : lane;
+                const int cU0 = __shfl_sync(0xffffffffu, cv[0], src1), cU1 = __shfl_sync(0xffffffffu, cv[1], src1);
+                if (isN) {
+                    const int c = (vN >> 5) ? cN1 : cN0;
+                    const double ratio = (vN >> 5) ? rN1 : rN0;
+                    const double xo = x[h];
+                    if (c <= J[h]) {
+                        a[h] = xo;
+                        ca[h] = c;
+                    } else {
+                        b[h] = xo;
+                        cb[h] = c;
+                    }
+                    if (fabs(ratio) <= tol) {
+                        x[h] = fmin(fmax(xo - ratio, a[h]), b[h]);
+                        mode[h] = 2;
+                    } else {
+                        const double xn = xo - ratio;
+                        const bool ok = isfinite(xn) && xn > a[h] && xn < b[h];
+                        x[h] = ok ? xn : 0.5 * (a[h] + b[h]);
+                        if (!(b[h] - a[h] > tol)) mode[h] = 2;
+                    }
+                } else if (isB) {
+                    const double A0 = a[h], B0 = b[h];
+                    const double na = gb >= 0 ? A0 + (B0 - A0) * ((double)(gb + 1) / (double)(G + 1)) : A0;
+                    const double nb = g1 < G ? A0 + (B0 - A0) * ((double)(gb + 2) / (double)(G + 1)) : B0;
+                    if (gb >= 0) ca[h] = cgb;
+                    if (g1 < G) cb[h] = (v1 >> 5) ? cU1 : cU0;
+                    a[h] = na;
+                    b[h] = nb;
+                    x[h] = 0.5 * (na + nb);
+                    if (!(nb - na > tol) || (na == A0 && nb == B0)) {
+                        mode[h] = 2;
+                    } else if (ca[h] == J[h] && cb[h] == J[h] + 1 && nb - na <= 1.0e-6 * fmax(fabs(na), fabs(nb))) {
+                        mode[h] = 1;
+                    }
                 }
             }
-            __syncthreads();
+            // a ring wait gave up: abandon the item (warp-uniform decision)
+            if (__any_sync(0xffffffffu, (*((volatile unsigned*)err) & kErrTimeout) != 0u)) break;
         }
-        if (own) mu[pi.off + w.j0 + tid] = sx[tid];
-        __syncthreads();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int e = lane + 32 * h;
+            if (e < w.m) mu[pi.off + w.j0 + e] = x[h];
+        }
     }
 }
 
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
                   const int* counts, const WorkItem* items, int n_items, int* counter, double tol, double* mu,
                   unsigned* err, unsigned long long* seq_counter) {
-    size_t sm = kNbuf * kChunk * 8 + kNbuf * 8;
-    k_bisect<<<grid, kThreads, sm, st>>>(pinfo, s, nz, nz_pad, counts, items, n_items, counter, tol, mu, err,
-                                         seq_counter);
+    const size_t sm = (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8 + kWBuf * 8);
+    cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_bisect<<<grid, kWarpsPerCta * 32, sm, st>>>(pinfo, s, nz, nz_pad, counts, items, n_items, counter, tol, mu,
+                                                  err, seq_counter);
     return 1;
+}
+
+int bisect_ctas_per_sm() {
+    int n = 1;
+    const size_t sm = (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8 + kWBuf * 8);
+    cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bisect, kWarpsPerCta * 32, sm) != cudaSuccess) n = 1;
+    return n < 1 ? 1 : n;
 }
 
 // ===========================================================================

@@ -29,14 +29,15 @@ struct ProblemInfo {
 struct WorkItem {
     int problem;  // problem index
     int j0;       // first eigen-index inside the problem (0 = lowest k)
-    int m;        // eigenvalues in this item (<= 256)
+    int m;        // eigenvalues in this item (<= kWItem for bisection)
     int pad;
 };
 
 constexpr int kScanPoints = 256;  // Sturm counts per problem in the isolation scan
 constexpr int kChunk = 1024;      // doubles per TMA chunk of the diagonal
 constexpr int kBlk = 16;          // eigenvector checkpoint interval
-constexpr int kThreads = 256;     // threads of the scan / bisection CTAs
+constexpr int kThreads = 256;     // threads of the scan CTAs
+constexpr int kWItem = 64;        // eigenvalues per warp work item of the bisection
 constexpr int kEvThreads = 64;    // threads (= eigenvalues) of an eigenvector CTA
 constexpr int kEvChunk = 512;     // doubles per TMA chunk in the eigenvector kernel
 
@@ -74,6 +75,7 @@ int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* 
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
                   const int* counts, const WorkItem* items, int n_items, int* counter, double tol, double* mu,
                   unsigned* err, unsigned long long* seq_counter);
+int bisect_ctas_per_sm();
 // FP64 throughput probe: each thread runs n_iter iterations of 8 independent
 // FMA chains; out receives a value that keeps the chains live
 int launch_fp64_probe(cudaStream_t st, int grid, int block, int n_iter, double* out);

@@ -676,7 +676,7 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
             }
             pi.off = off;
             off += pi.M;
-            const int nit = (pi.M + ncpa::kThreads - 1) / ncpa::kThreads;
+            const int nit = (pi.M + ncpa::kWItem - 1) / ncpa::kWItem;
             for (int k = 0; k < nit; ++k) {
                 int j0 = (int)((long long)pi.M * k / nit), j1 = (int)((long long)pi.M * (k + 1) / nit);
                 items.push_back(WorkItem{p, j0, j1 - j0, 0});
@@ -710,7 +710,8 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
             d_counter.alloc(2 * sizeof(int), st);
             CK(cudaMemsetAsync(d_counter.p, 0, 2 * sizeof(int), st));
             // ---- K3 bisection ----
-            int grid_b = std::min(n_items, ctx->num_sms * 4);
+            const int wpc = 4;  // warps per bisection CTA
+            int grid_b = std::min((n_items + wpc - 1) / wpc, ctx->num_sms * ncpa::bisect_ctas_per_sm());
             tm.mark("host-items");
             check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
                                                   d_items.as<WorkItem>(), n_items, d_counter.as<int>(), kBisectTol,
