@@ -539,19 +539,20 @@ int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* 
 
 // K3: per-warp multisection + safeguarded Newton.
 //
-// Each warp owns a work item of m <= kWItem consecutive eigen-indices of one
-// problem and streams that problem's diagonal through its own TMA ring in
-// shared memory (kWBuf chunks of kWChunk doubles, one mbarrier per slot), so
-// warps never wait on each other.  Every lane runs two independent Sturm
-// chains (virtual lanes v = lane and lane + 32).  Every round:
-//  * eigenvalues already isolated in a narrow bracket ("Newton slots") get one
-//    virtual lane each, which carries the x-derivative of the recurrence and
-//    takes a Newton step on det(S - x); the Sturm count at the iterate shrinks
-//    the bracket and a step leaving the bracket falls back to its midpoint;
-//  * the other virtual lanes are dealt round-robin over the remaining
-//    unconverged eigenvalues (G_e lanes each), which cut their bracket into
-//    G_e + 1 pieces.
-// Lane l owns eigen slots l and l + 32 (bracket, iterate, end counts, mode).
+// Each warp owns a work item of m <= 32 consecutive eigen-indices of one
+// problem (lane l owns eigenvalue slot l: bracket [a, b] with the Sturm counts
+// at its ends, Newton iterate x, mode) and streams that problem's diagonal
+// through its own TMA ring in shared memory (kWBuf chunks of kWChunk doubles,
+// one mbarrier per slot), so warps never wait on each other.  Each lane runs
+// up to two Sturm chains (virtual lanes v = lane, lane + 32).  Every round:
+//  * eigenvalues isolated in their bracket (Sturm counts J and J + 1 at its
+//    ends) take a safeguarded Newton step on det(S - x): one virtual lane
+//    (chain 0) carries the x-derivative of the recurrence; the Sturm count at
+//    the iterate shrinks the bracket and a step leaving the bracket falls back
+//    to its midpoint;
+//  * the other virtual lanes are dealt round-robin over the eigenvalues not
+//    yet isolated (G_e lanes each), which cut their bracket into G_e + 1
+//    pieces.  Rounds with Newton slots only sweep a single chain.
 constexpr int kWChunk = 512;
 constexpr int kWBuf = 3;
 constexpr int kWarpsPerCta = 4;
@@ -585,29 +586,11 @@ __device__ __forceinline__ int nth_bit(unsigned m, int n) {
     }
     return pos;
 }
-__device__ __forceinline__ int nth_bit64(unsigned lo, unsigned hi, int n) {
-    const int c = __popc(lo);
-    return n < c ? nth_bit(lo, n) : 32 + nth_bit(hi, n - c);
-}
-__device__ __forceinline__ int rank64(unsigned lo, unsigned hi, int e) {
-    return e < 32 ? __popc(lo & ((1u << e) - 1u)) : __popc(lo) + __popc(hi & ((1u << (e - 32)) - 1u));
-}
-// value held by lane (e & 31) for half (e >> 5)
-__device__ __forceinline__ double fetch2(double v0, double v1, int e) {
-    const double a = __shfl_sync(0xffffffffu, v0, e & 31);
-    const double b = __shfl_sync(0xffffffffu, v1, e & 31);
-    return (e >> 5) ? b : a;
-}
-__device__ __forceinline__ int fetch2i(int v0, int v1, int e) {
-    const int a = __shfl_sync(0xffffffffu, v0, e & 31);
-    const int b = __shfl_sync(0xffffffffu, v1, e & 31);
-    return (e >> 5) ? b : a;
-}
 
-// one sweep of two chains over the diagonal; dflag: 0 none, 1 chain 0 carries
-// the derivative, 2 both chains do
-__device__ void warp_sweep2(const double* __restrict__ s, int nz, double x0, double x1, int dflag, WarpRing& r,
-                            unsigned* err, int& c0, int& c1, double& rat0, double& rat1) {
+// One sweep over the diagonal.  mode 0: chains A and B, counts only;
+// 1: chain A with derivative + chain B; 2: chain A with derivative only.
+__device__ void warp_sweep(const double* __restrict__ s, int nz, double x0, double x1, int mode, WarpRing& r,
+                           unsigned* err, int& c0, int& c1, double& rat0) {
     const int lane = threadIdx.x & 31;
     const int nch = (nz + kWChunk - 1) / kWChunk;
     const unsigned base = r.loads;
@@ -617,7 +600,7 @@ __device__ void warp_sweep2(const double* __restrict__ s, int nz, double x0, dou
     SturmState A, B;
     A.reset();
     B.reset();
-    double da0 = 0.0, da1 = 0.0, db0 = 0.0, db1 = 0.0;
+    double da0 = 0.0, da1 = 0.0;
     for (int c = 0; c < nch; ++c) {
         const unsigned k = base + c;
         const int slot = k % kWBuf;
@@ -625,7 +608,7 @@ __device__ void warp_sweep2(const double* __restrict__ s, int nz, double x0, dou
         const double* b = r.buf + slot * kWChunk;
         const int valid = min(kWChunk, nz - c * kWChunk);
         const int nw = valid >> 5;
-        if (dflag == 0) {
+        if (mode == 0) {
             for (int w = 0; w < nw; ++w) {
                 A.word32(b + 32 * w, x0);
                 B.word32(b + 32 * w, x1);
@@ -634,7 +617,7 @@ __device__ void warp_sweep2(const double* __restrict__ s, int nz, double x0, dou
                 A.step(b[i], x0);
                 B.step(b[i], x1);
             }
-        } else if (dflag == 1) {
+        } else if (mode == 1) {
             for (int w = 0; w < nw; ++w) {
                 A.word32_deriv(b + 32 * w, x0, da0, da1);
                 B.word32(b + 32 * w, x1);
@@ -644,14 +627,8 @@ __device__ void warp_sweep2(const double* __restrict__ s, int nz, double x0, dou
                 B.step(b[i], x1);
             }
         } else {
-            for (int w = 0; w < nw; ++w) {
-                A.word32_deriv(b + 32 * w, x0, da0, da1);
-                B.word32_deriv(b + 32 * w, x1, db0, db1);
-            }
-            for (int i = nw * 32; i < valid; ++i) {
-                A.step_deriv(b[i], x0, da0, da1);
-                B.step_deriv(b[i], x1, db0, db1);
-            }
+            for (int w = 0; w < nw; ++w) A.word32_deriv(b + 32 * w, x0, da0, da1);
+            for (int i = nw * 32; i < valid; ++i) A.step_deriv(b[i], x0, da0, da1);
         }
         __syncwarp();
         if (lane == 0 && c + kWBuf < nch) {
@@ -662,16 +639,13 @@ __device__ void warp_sweep2(const double* __restrict__ s, int nz, double x0, dou
     r.loads = base + nch;
     c0 = A.cnt;
     c1 = B.cnt;
-    rat0 = dflag >= 1 ? A.p1 / da1 : 0.0;
-    rat1 = dflag >= 2 ? B.p1 / db1 : 0.0;
+    rat0 = mode >= 1 ? A.p1 / da1 : 0.0;
 }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32) k_bisect(const ProblemInfo* __restrict__ pinfo,
-                                                              const double* __restrict__ s, int nz, int nz_pad,
-                                                              const int* __restrict__ counts,
-                                                              const WorkItem* __restrict__ items, int n_items,
-                                                              int* counter, double tol, double* __restrict__ mu,
-                                                              unsigned* err, unsigned long long* seq_counter) {
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
+    k_bisect(const ProblemInfo* __restrict__ pinfo, const double* __restrict__ s, int nz, int nz_pad,
+             const int* __restrict__ counts, const WorkItem* __restrict__ items, int n_items, int* counter,
+             double tol, double* __restrict__ mu, unsigned* err, unsigned long long* seq_counter) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     WarpRing r;
@@ -692,147 +666,122 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_bisect(const ProblemInfo*
         const ProblemInfo pi = pinfo[w.problem];
         const int* cnt = counts + (size_t)w.problem * kScanPoints;
         const double* sp = s + (size_t)w.problem * nz_pad;
-        // per-lane state of slots e0 = lane, e1 = lane + 32
-        double a[2], b[2], x[2];
-        int ca[2], cb[2], mode[2], J[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int e = lane + 32 * h;
-            mode[h] = 2;
-            a[h] = b[h] = x[h] = pi.lo;
-            ca[h] = cb[h] = 0;
-            J[h] = pi.c_lo + w.j0 + e;
-            if (e < w.m) {  // initial bracket from the isolation scan
-                int t0 = 0;
-                for (int t = 0; t < kScanPoints; ++t)
-                    if (cnt[t] <= J[h]) t0 = t;
-                int t1 = kScanPoints - 1;
-                for (int t = kScanPoints - 1; t > t0; --t)
-                    if (cnt[t] > J[h]) t1 = t;
-                if (cnt[t1] <= J[h]) atomicOr(err, kErrBracket);
-                a[h] = scan_x(pi.lo, pi.hi, t0);
-                b[h] = scan_x(pi.lo, pi.hi, t1);
-                ca[h] = cnt[t0];
-                cb[h] = cnt[t1];
-                x[h] = 0.5 * (a[h] + b[h]);
-                mode[h] = !(b[h] - a[h] > tol) ? 2 : 0;
-            }
+        // state of eigen slot `lane`
+        const int J = pi.c_lo + w.j0 + lane;
+        double a = pi.lo, b = pi.lo, x = pi.lo;
+        int ca = 0, cb = 0, mode = 2;
+        if (lane < w.m) {  // initial bracket from the isolation scan
+            int t0 = 0;
+            for (int t = 0; t < kScanPoints; ++t)
+                if (cnt[t] <= J) t0 = t;
+            int t1 = kScanPoints - 1;
+            for (int t = kScanPoints - 1; t > t0; --t)
+                if (cnt[t] > J) t1 = t;
+            if (cnt[t1] <= J) atomicOr(err, kErrBracket);
+            a = scan_x(pi.lo, pi.hi, t0);
+            b = scan_x(pi.lo, pi.hi, t1);
+            ca = cnt[t0];
+            cb = cnt[t1];
+            x = 0.5 * (a + b);
+            mode = !(b - a > tol) ? 2 : ((ca == J && cb == J + 1) ? 1 : 0);
         }
         for (int round = 0; round < 512; ++round) {
-            const unsigned n0 = __ballot_sync(0xffffffffu, mode[0] == 1);
-            const unsigned n1 = __ballot_sync(0xffffffffu, mode[1] == 1);
-            const unsigned b0 = __ballot_sync(0xffffffffu, mode[0] == 0);
-            const unsigned b1 = __ballot_sync(0xffffffffu, mode[1] == 0);
-            const int nN = __popc(n0) + __popc(n1), nB = __popc(b0) + __popc(b1);
+            const unsigned nm = __ballot_sync(0xffffffffu, mode == 1);
+            const unsigned bm = __ballot_sync(0xffffffffu, mode == 0);
+            const int nN = __popc(nm), nB = __popc(bm);
             if (nN + nB == 0) break;
             const int nlB = 64 - nN;
-            // roles of the two virtual lanes of this thread
+            // roles of this lane's two virtual lanes v = lane + 32 h
             double xv[2];
-            int ev[2], gv[2], Gv[2], role[2];  // role: 1 Newton, 0 multisection, -1 idle
+            int gv[2], Gv[2];
+            bool newton0 = false;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int v = lane + 32 * h;
-                role[h] = -1;
-                ev[h] = 0;
+                int e = 0;
                 gv[h] = 0;
                 Gv[h] = 1;
+                bool nt = false;
                 if (v < nN) {
-                    role[h] = 1;
-                    ev[h] = nth_bit64(n0, n1, v);
+                    nt = true;
+                    e = nth_bit(nm, v);
                 } else if (nB > 0) {
                     const int t = v - nN, k = t % nB;
-                    role[h] = 0;
-                    ev[h] = nth_bit64(b0, b1, k);
+                    e = nth_bit(bm, k);
                     gv[h] = t / nB;
                     Gv[h] = (nlB - 1 - k) / nB + 1;
                 }
+                const double ae = __shfl_sync(0xffffffffu, a, e);
+                const double be = __shfl_sync(0xffffffffu, b, e);
+                const double xe = __shfl_sync(0xffffffffu, x, e);
+                xv[h] = nt ? xe : ae + (be - ae) * ((double)(gv[h] + 1) / (double)(Gv[h] + 1));
+                if (h == 0) newton0 = nt;
             }
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const double ae = fetch2(a[0], a[1], ev[h]);
-                const double be = fetch2(b[0], b[1], ev[h]);
-                const double xe = fetch2(x[0], x[1], ev[h]);
-                xv[h] = role[h] == 1 ? xe : ae + (be - ae) * ((double)(gv[h] + 1) / (double)(Gv[h] + 1));
-            }
-            int cv[2];
-            double rv[2];
-            const int dflag = nN > 32 ? 2 : (nN > 0 ? 1 : 0);
-            warp_sweep2(sp, nz, xv[0], xv[1], dflag, r, err, cv[0], cv[1], rv[0], rv[1]);
-            if (seq_counter && lane == 0) atomicAdd(seq_counter, (unsigned long long)64);
-            // owners update their slots.  Every __shfl_sync below is executed
-            // by all 32 lanes (no shuffle sits inside a lane-dependent branch).
+            (void)newton0;
+            int cv0, cv1;
+            double rat;
+            const int smode = nN == 0 ? 0 : (nB > 0 ? 1 : 2);
+            warp_sweep(sp, nz, xv[0], xv[1], smode, r, err, cv0, cv1, rat);
+            if (seq_counter && lane == 0) atomicAdd(seq_counter, (unsigned long long)(smode == 2 ? 32 : 64));
+            // updates.  Every __shfl_sync is executed by all 32 lanes.
+            const bool isN = mode == 1, isB = mode == 0;
+            const int vN = isN ? __popc(nm & ((1u << lane) - 1u)) : 0;  // Newton virtual lane (chain 0)
+            const int cN = __shfl_sync(0xffffffffu, cv0, vN);
+            const double rN = __shfl_sync(0xffffffffu, rat, vN);
+            const int k = isB ? __popc(bm & ((1u << lane) - 1u)) : 0;
+            const int G = isB ? (nlB - 1 - k) / nB + 1 : 0;
             const int Gmax = nB > 0 ? (nlB - 1) / nB + 1 : 0;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int e = lane + 32 * h;
-                const bool isN = mode[h] == 1, isB = mode[h] == 0;
-                // Newton result of this slot: virtual lane v = rank among Newton slots
-                const int vN = isN ? rank64(n0, n1, e) : 0;
-                const int srcN = vN & 31;
-                const int cN0 = __shfl_sync(0xffffffffu, cv[0], srcN), cN1 = __shfl_sync(0xffffffffu, cv[1], srcN);
-                const double rN0 = __shfl_sync(0xffffffffu, rv[0], srcN), rN1 = __shfl_sync(0xffffffffu, rv[1], srcN);
-                // multisection results of this slot: lanes nN + k + g nB, g < G
-                const int k = isB ? rank64(b0, b1, e) : 0;
-                const int G = isB ? (nlB - 1 - k) / nB + 1 : 0;
-                int gb = -1, cgb = ca[h];
-                for (int g = 0; g < Gmax; ++g) {
-                    const int v = nN + k + g * nB;
-                    const int src = v & 31;
-                    const int c0 = __shfl_sync(0xffffffffu, cv[0], src), c1 = __shfl_sync(0xffffffffu, cv[1], src);
-                    const int c = (v >> 5) ? c1 : c0;
-                    if (isB && g < G && c <= J[h]) {
-                        gb = g;
-                        cgb = c;
-                    }
+            int gb = -1, cgb = ca;
+            for (int g = 0; g < Gmax; ++g) {
+                const int v = nN + k + g * nB;
+                const int c0 = __shfl_sync(0xffffffffu, cv0, v & 31), c1 = __shfl_sync(0xffffffffu, cv1, v & 31);
+                const int c = (v >> 5) ? c1 : c0;
+                if (isB && g < G && c <= J) {
+                    gb = g;
+                    cgb = c;
                 }
-                const int g1 = gb + 1;
-                const int v1 = nN + k + g1 * nB;
-                const int src1 = (isB && g1 < G) ? (v1 & 31) : lane;
-                const int cU0 = __shfl_sync(0xffffffffu, cv[0], src1), cU1 = __shfl_sync(0xffffffffu, cv[1], src1);
-                if (isN) {
-                    const int c = (vN >> 5) ? cN1 : cN0;
-                    const double ratio = (vN >> 5) ? rN1 : rN0;
-                    const double xo = x[h];
-                    if (c <= J[h]) {
-                        a[h] = xo;
-                        ca[h] = c;
-                    } else {
-                        b[h] = xo;
-                        cb[h] = c;
-                    }
-                    if (fabs(ratio) <= tol) {
-                        x[h] = fmin(fmax(xo - ratio, a[h]), b[h]);
-                        mode[h] = 2;
-                    } else {
-                        const double xn = xo - ratio;
-                        const bool ok = isfinite(xn) && xn > a[h] && xn < b[h];
-                        x[h] = ok ? xn : 0.5 * (a[h] + b[h]);
-                        if (!(b[h] - a[h] > tol)) mode[h] = 2;
-                    }
-                } else if (isB) {
-                    const double A0 = a[h], B0 = b[h];
-                    const double na = gb >= 0 ? A0 + (B0 - A0) * ((double)(gb + 1) / (double)(G + 1)) : A0;
-                    const double nb = g1 < G ? A0 + (B0 - A0) * ((double)(gb + 2) / (double)(G + 1)) : B0;
-                    if (gb >= 0) ca[h] = cgb;
-                    if (g1 < G) cb[h] = (v1 >> 5) ? cU1 : cU0;
-                    a[h] = na;
-                    b[h] = nb;
-                    x[h] = 0.5 * (na + nb);
-                    if (!(nb - na > tol) || (na == A0 && nb == B0)) {
-                        mode[h] = 2;
-                    } else if (ca[h] == J[h] && cb[h] == J[h] + 1 && nb - na <= 1.0e-6 * fmax(fabs(na), fabs(nb))) {
-                        mode[h] = 1;
-                    }
+            }
+            const int g1 = gb + 1;
+            const int v1 = nN + k + g1 * nB;
+            const int src1 = (isB && g1 < G) ? (v1 & 31) : lane;
+            const int cU0 = __shfl_sync(0xffffffffu, cv0, src1), cU1 = __shfl_sync(0xffffffffu, cv1, src1);
+            if (isN) {
+                const double xo = x;
+                if (cN <= J) {
+                    a = xo;
+                    ca = cN;
+                } else {
+                    b = xo;
+                    cb = cN;
+                }
+                if (fabs(rN) <= tol) {
+                    x = fmin(fmax(xo - rN, a), b);
+                    mode = 2;
+                } else {
+                    const double xn = xo - rN;
+                    const bool ok = isfinite(xn) && xn > a && xn < b;
+                    x = ok ? xn : 0.5 * (a + b);
+                    if (!(b - a > tol)) mode = 2;
+                }
+            } else if (isB) {
+                const double A0 = a, B0 = b;
+                const double na = gb >= 0 ? A0 + (B0 - A0) * ((double)(gb + 1) / (double)(G + 1)) : A0;
+                const double nb = g1 < G ? A0 + (B0 - A0) * ((double)(gb + 2) / (double)(G + 1)) : B0;
+                if (gb >= 0) ca = cgb;
+                if (g1 < G) cb = (v1 >> 5) ? cU1 : cU0;
+                a = na;
+                b = nb;
+                x = 0.5 * (na + nb);
+                if (!(nb - na > tol) || (na == A0 && nb == B0)) {
+                    mode = 2;
+                } else if (ca == J && cb == J + 1) {
+                    mode = 1;  // isolated: safeguarded Newton from here
                 }
             }
             // a ring wait gave up: abandon the item (warp-uniform decision)
             if (__any_sync(0xffffffffu, (*((volatile unsigned*)err) & kErrTimeout) != 0u)) break;
         }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int e = lane + 32 * h;
-            if (e < w.m) mu[pi.off + w.j0 + e] = x[h];
-        }
+        if (lane < w.m) mu[pi.off + w.j0 + lane] = x;
     }
 }
 

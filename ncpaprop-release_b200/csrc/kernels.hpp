@@ -37,7 +37,7 @@ constexpr int kScanPoints = 256;  // Sturm counts per problem in the isolation s
 constexpr int kChunk = 1024;      // doubles per TMA chunk of the diagonal
 constexpr int kBlk = 16;          // eigenvector checkpoint interval
 constexpr int kThreads = 256;     // threads of the scan CTAs
-constexpr int kWItem = 64;        // eigenvalues per warp work item of the bisection
+constexpr int kWItem = 32;        // eigenvalues per warp work item of the bisection
 constexpr int kEvThreads = 64;    // threads (= eigenvalues) of an eigenvector CTA
 constexpr int kEvChunk = 512;     // doubles per TMA chunk in the eigenvector kernel
 
