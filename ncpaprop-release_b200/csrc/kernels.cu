@@ -828,292 +828,346 @@ int launch_fp64_probe(cudaStream_t st, int grid, int block, int n_iter, double* 
 
 // ===========================================================================
 // K4: eigenvectors by twisted factorisation (see oracle/ncpa_oracle.c for the
-// derivation).  Pass 1 runs the backward recurrence q top-down and stores a
-// checkpoint (q_c, q_{c+1}, exponent) every kBlk rows; pass 2 runs the forward
-// recurrence p bottom-up, re-creates each block's q from its checkpoint in
-// registers, tracks the twist r = argmax |p_{r-1} q_{r+1}| and accumulates
-//   sum z^2, sum z^2 w, sum z^2 g   below r (forward) and above r (backward).
+// derivation), one eigenvalue per lane, one work item (<= 32 eigenvalues of a
+// problem) per warp.  Each warp streams the diagonal s (and the weights w, g)
+// through its own TMA ring, so warps never wait on each other.
+//  pass 1  backward recurrence q top-down; every kBlk rows a checkpoint
+//          (q_c, q_{c+1}, exponent) goes to global scratch;
+//  pass 2  forward recurrence p bottom-up; each block's q values are re-created
+//          from its checkpoint in registers; the twist r = argmax |p_{r-1} q_{r+1}|
+//          is tracked and sum z^2, sum z^2 w, sum z^2 g are accumulated below r
+//          (forward part) and above r (backward part, restarted at each new r);
+//  pass 3  (optional) writes the normalised eigenvector.
 // ===========================================================================
-constexpr int kEvNbuf = 2;
+constexpr int kEvC = 256;     // doubles per chunk and array
+constexpr int kEvB = 3;       // ring slots per warp
+constexpr int kEvWarps = 4;   // warps per CTA
 
 struct EvRing {
-    double* sbuf;    // [kEvNbuf][kEvChunk]
-    double* wbuf;
-    double* gbuf;
-    uint64_t* bars;  // [kEvNbuf]
+    double* s;       // [kEvB][kEvC]
+    double* w;
+    double* g;
+    uint64_t* bars;  // [kEvB]
     unsigned loads;
 };
 
-__device__ __forceinline__ void evring_issue(EvRing& r, unsigned k, int c, const double* sp, const double* wp,
-                                             const double* gp) {
-    int slot = k % kEvNbuf;
-    uint32_t bytes = kEvChunk * 8 * (1 + (wp ? 1 : 0) + (gp ? 1 : 0));
+__device__ __forceinline__ void evr_issue(EvRing& r, unsigned k, int c, const double* sp, const double* wp,
+                                          const double* gp) {
+    const int slot = k % kEvB;
+    const uint32_t bytes = kEvC * 8 * (1 + (wp ? 1 : 0) + (gp ? 1 : 0));
     mbar_expect_tx(&r.bars[slot], bytes);
-    tma_load_1d(r.sbuf + slot * kEvChunk, sp + (size_t)c * kEvChunk, kEvChunk * 8, &r.bars[slot]);
-    if (wp) tma_load_1d(r.wbuf + slot * kEvChunk, wp + (size_t)c * kEvChunk, kEvChunk * 8, &r.bars[slot]);
-    if (gp) tma_load_1d(r.gbuf + slot * kEvChunk, gp + (size_t)c * kEvChunk, kEvChunk * 8, &r.bars[slot]);
+    tma_load_1d(r.s + slot * kEvC, sp + (size_t)c * kEvC, kEvC * 8, &r.bars[slot]);
+    if (wp) tma_load_1d(r.w + slot * kEvC, wp + (size_t)c * kEvC, kEvC * 8, &r.bars[slot]);
+    if (gp) tma_load_1d(r.g + slot * kEvC, gp + (size_t)c * kEvC, kEvC * 8, &r.bars[slot]);
 }
 
 __device__ __forceinline__ cuda::std::complex<double> csqrt_principal(double x, double y) {
-    // principal square root of x + i y for x > 0 (k^2 + i absorption)
+    // principal square root of x + i y
     double m = hypot(x, y);
     double t = sqrt(0.5 * (m + fabs(x)));
     if (x >= 0.0) return cuda::std::complex<double>(t, y / (2.0 * t));
     return cuda::std::complex<double>(fabs(y) / (2.0 * t), copysign(t, y));
 }
 
+// forward-pass state of one eigenvalue
+struct FwdState {
+    double pm2, pm1;     // p_{i-2}, p_{i-1}
+    int Ep;              // exponent of p
+    double An, Aw, Ag;   // running sums of p^2, p^2 w, p^2 g
+    double thr;          // best |p q| so far, in units 2^Ethr
+    int Ethr;
+    int r, Epr, Eqr;     // twist, exponents of p and q at the twist
+    double Anr, Awr, Agr, sqr, pr, qr;
+    double Tn, Tw, Tg;   // sums of (q / q_r)^2 (w, g) above the twist, units 2^(2 Eqr)
+    double fq;           // 2^(Eb - Eqr) for the current block
+    double ps, qs, prc, qrc;
+    int Eps, Eqs, Eprc, Eqrc;
+};
+
+template <bool kGroup, bool kGuard>
+__device__ __forceinline__ void fwd_step(FwdState& F, int i, int nz, double si, double wi, double gi, double qn,
+                                         int Eb, double mu, int isrc, int ircv) {
+    if (kGuard && i >= nz) return;
+    const double sq = F.pm1 * F.pm1;
+    F.An = F.An + sq;
+    F.Aw = fma(sq, wi, F.Aw);
+    const double t = qn * F.fq;
+    const double t2 = t * t;
+    F.Tn = F.Tn + t2;
+    F.Tw = fma(t2, wi, F.Tw);
+    if (kGroup) {
+        F.Ag = fma(sq, gi, F.Ag);
+        F.Tg = fma(t2, gi, F.Tg);
+    }
+    const double prod = fabs(F.pm1 * qn);
+    if (prod > F.thr) {
+        F.thr = prod;
+        F.r = i;
+        F.Anr = F.An;
+        F.Awr = F.Aw;
+        F.Agr = F.Ag;
+        F.sqr = sq;
+        F.pr = F.pm1;
+        F.Epr = F.Ep;
+        F.qr = qn;
+        F.Eqr = Eb;
+        F.fq = 1.0;
+        F.Tn = 0.0;
+        F.Tw = 0.0;
+        F.Tg = 0.0;
+    }
+    if (kGuard) {
+        if (i == isrc) {
+            F.ps = F.pm1;
+            F.Eps = F.Ep;
+            F.qs = qn;
+            F.Eqs = Eb;
+        }
+        if (i == ircv) {
+            F.prc = F.pm1;
+            F.Eprc = F.Ep;
+            F.qrc = qn;
+            F.Eqrc = Eb;
+        }
+    }
+    const double pn = fma(si - mu, F.pm1, -F.pm2);
+    F.pm2 = F.pm1;
+    F.pm1 = pn;
+}
+
 template <bool kGroup, bool kVec>
-__global__ void __launch_bounds__(kEvThreads) k_eigvec(EigvecArgs A) {
+__global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
+    constexpr int NA = kGroup ? 3 : 2;
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double* wb0 = reinterpret_cast<double*>(smem_raw) + (size_t)wid * kEvB * NA * kEvC;
     EvRing R;
-    R.sbuf = reinterpret_cast<double*>(smem_raw);
-    R.wbuf = R.sbuf + kEvNbuf * kEvChunk;
-    R.gbuf = R.wbuf + kEvNbuf * kEvChunk;
-    R.bars = reinterpret_cast<uint64_t*>(R.gbuf + kEvNbuf * kEvChunk);
+    R.s = wb0;
+    R.w = wb0 + kEvB * kEvC;
+    R.g = kGroup ? wb0 + 2 * kEvB * kEvC : nullptr;
+    R.bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kEvWarps * kEvB * NA * kEvC * 8) + wid * kEvB;
     R.loads = 0;
-    __shared__ int s_item;
-    const int tid = threadIdx.x;
-    if (tid == 0) {
-        for (int k = 0; k < kEvNbuf; ++k) mbar_init(&R.bars[k], 1);
+    if (lane == 0) {
+        for (int k = 0; k < kEvB; ++k) mbar_init(&R.bars[k], 1);
         fence_mbar_init();
     }
-    __syncthreads();
+    __syncwarp();
     const int nz = A.nz;
-    const int nch = (nz + kEvChunk - 1) / kEvChunk;
+    const int nch = (nz + kEvC - 1) / kEvC;
     const int nblk = (nz + kBlk - 1) / kBlk;
-    double* ck1 = A.ck_q1 + (size_t)blockIdx.x * A.ck_slot_stride;
-    double* ck2 = A.ck_q2 + (size_t)blockIdx.x * A.ck_slot_stride;
-    int* cke = A.ck_e + (size_t)blockIdx.x * A.ck_slot_stride;
-
+    const size_t gw = (size_t)blockIdx.x * kEvWarps + wid;
+    double* ck1 = A.ck_q1 + gw * A.ck_slot_stride;
+    double* ck2 = A.ck_q2 + gw * A.ck_slot_stride;
+    int* cke = A.ck_e + gw * A.ck_slot_stride;
+    auto load_ck = [&](int kb, double& a1, double& a2, int& ae) {
+        if (min((kb + 1) * kBlk, nz) >= nz) {
+            a1 = 1.0;
+            a2 = 0.0;
+            ae = 0;
+        } else {
+            const size_t ci = (size_t)kb * 32 + lane;
+            a1 = ck1[ci];
+            a2 = ck2[ci];
+            ae = cke[ci];
+        }
+    };
     for (;;) {
-        if (tid == 0) s_item = atomicAdd(A.counter, 1);
-        __syncthreads();
-        const int it = s_item;
-        __syncthreads();
+        int it = 0;
+        if (lane == 0) it = atomicAdd(A.counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= A.n_items) break;
         const WorkItem w = A.items[it];
         const ProblemInfo pi = A.pinfo[w.problem];
         const double* sp = A.s + (size_t)w.problem * A.nz_pad;
         const double* wp = A.w + (size_t)(w.problem / A.n_az) * A.wstride;
         const double* gp = kGroup ? A.g + (size_t)w.problem * A.nz_pad : nullptr;
-        const bool active = tid < w.m;
-        const double mu = active ? A.mu[pi.off + w.j0 + tid] : pi.lo;
+        const bool active = lane < w.m;
+        const double mu = active ? A.mu[pi.off + w.j0 + lane] : pi.lo;
 
         // ---------------- pass 1: backward recurrence, checkpoints ----------
         {
             const unsigned base = R.loads;
-            if (tid == 0)
-                for (int o = 0; o < nch && o < kEvNbuf; ++o) evring_issue(R, base + o, nch - 1 - o, sp, nullptr, nullptr);
-            double q1 = 1.0, q2 = 0.0;  // q_{i}, q_{i+1} after each step; q_n = 1, q_{n+1} = 0
+            if (lane == 0)
+                for (int o = 0; o < nch && o < kEvB; ++o) evr_issue(R, base + o, nch - 1 - o, sp, nullptr, nullptr);
+            __syncwarp();
+            double q1 = 1.0, q2 = 0.0;  // q_i, q_{i+1}; q_n = 1, q_{n+1} = 0
             int E = 0;
             for (int o = 0; o < nch; ++o) {
                 const int c = nch - 1 - o;
                 const unsigned k = base + o;
-                const int slot = k % kEvNbuf;
-                mbar_wait_bounded(&R.bars[slot], (k / kEvNbuf) & 1u, A.err);
-                const double* sb = R.sbuf + slot * kEvChunk;
-                const int valid = min(kEvChunk, nz - c * kEvChunk);
+                const int slot = k % kEvB;
+                mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
+                const double* sb = R.s + slot * kEvC;
+                const int valid = min(kEvC, nz - c * kEvC);
                 for (int lb = ((valid - 1) / kBlk) * kBlk; lb >= 0; lb -= kBlk) {
+                    if (lb + kBlk <= valid) {
 #pragma unroll
-                    for (int u = kBlk - 1; u >= 0; --u) {
-                        const int li = lb + u;
-                        if (li < valid) {
-                            double qi = fma(sb[li] - mu, q1, -q2);
+                        for (int u = kBlk - 1; u >= 0; --u) {
+                            const double qi = fma(sb[lb + u] - mu, q1, -q2);
+                            q2 = q1;
+                            q1 = qi;
+                        }
+                    } else {
+                        for (int u = valid - 1 - lb; u >= 0; --u) {
+                            const double qi = fma(sb[lb + u] - mu, q1, -q2);
                             q2 = q1;
                             q1 = qi;
                         }
                     }
-                    const int gbase = c * kEvChunk + lb;
+                    const int gbase = c * kEvC + lb;
                     if (gbase > 0) {
-                        const size_t ci = (size_t)(gbase / kBlk - 1) * kEvThreads + tid;
+                        const size_t ci = (size_t)(gbase / kBlk - 1) * 32 + lane;
                         ck1[ci] = q1;
                         ck2[ci] = q2;
                         cke[ci] = E;
                     }
-                    int sh = grow_shift(q1, q2);
+                    const int sh = grow_shift(q1, q2);
                     if (sh) {
-                        double sc = pow2(-sh);
+                        const double sc = pow2(-sh);
                         q1 *= sc;
                         q2 *= sc;
                         E += sh;
                     }
                 }
-                __syncthreads();
-                if (tid == 0 && o + kEvNbuf < nch) {
+                __syncwarp();
+                if (lane == 0 && o + kEvB < nch) {
                     fence_proxy_async();
-                    evring_issue(R, base + o + kEvNbuf, nch - 1 - (o + kEvNbuf), sp, nullptr, nullptr);
+                    evr_issue(R, base + o + kEvB, nch - 1 - (o + kEvB), sp, nullptr, nullptr);
                 }
             }
             R.loads = base + nch;
         }
 
-        // ---------------- pass 2: forward recurrence + twist + sums ---------
-        double pm2 = 0.0, pm1 = 1.0;
-        int Ep = 0;
-        double An = 0.0, Aw = 0.0, Ag = 0.0;
-        double thr = -1.0;
-        int Ethr = 0;
-        int r = 0, Epr = 0, Eqr = 0;
-        double Anr = 1.0, Awr = 0.0, Agr = 0.0, sqr_ = 1.0, pr = 1.0, qr = 1.0;
-        double Tn = 0.0, Tw = 0.0, Tg = 0.0, fq = 1.0;
-        double ps = 1.0, qs = 1.0, prc = 1.0, qrc = 1.0;
-        int Eps = 0, Eqs = 0, Eprc = 0, Eqrc = 0;
+        // ---------------- pass 2: forward recurrence, twist, sums ----------
+        FwdState F;
+        F.pm2 = 0.0;
+        F.pm1 = 1.0;
+        F.Ep = 0;
+        F.An = F.Aw = F.Ag = 0.0;
+        F.thr = -1.0;
+        F.Ethr = 0;
+        F.r = 0;
+        F.Epr = F.Eqr = 0;
+        F.Anr = 1.0;
+        F.Awr = F.Agr = 0.0;
+        F.sqr = F.pr = F.qr = 1.0;
+        F.Tn = F.Tw = F.Tg = 0.0;
+        F.fq = 1.0;
+        F.ps = F.qs = F.prc = F.qrc = 1.0;
+        F.Eps = F.Eqs = F.Eprc = F.Eqrc = 0;
         {
             const unsigned base = R.loads;
-            if (tid == 0)
-                for (int c = 0; c < nch && c < kEvNbuf; ++c) evring_issue(R, base + c, c, sp, wp, gp);
-            // checkpoint of block 0
+            if (lane == 0)
+                for (int c = 0; c < nch && c < kEvB; ++c) evr_issue(R, base + c, c, sp, wp, gp);
+            __syncwarp();
             double nq1, nq2;
             int nE;
-            auto load_ck = [&](int kb, double& a1, double& a2, int& ae) {
-                int ctop = min((kb + 1) * kBlk, nz);
-                if (ctop >= nz) {
-                    a1 = 1.0;
-                    a2 = 0.0;
-                    ae = 0;
-                } else {
-                    size_t ci = (size_t)kb * kEvThreads + tid;
-                    a1 = ck1[ci];
-                    a2 = ck2[ci];
-                    ae = cke[ci];
-                }
-            };
             load_ck(0, nq1, nq2, nE);
             for (int c = 0; c < nch; ++c) {
                 const unsigned k = base + c;
-                const int slot = k % kEvNbuf;
-                mbar_wait_bounded(&R.bars[slot], (k / kEvNbuf) & 1u, A.err);
-                const double* sb = R.sbuf + slot * kEvChunk;
-                const double* wb = R.wbuf + slot * kEvChunk;
-                const double* gb = R.gbuf + slot * kEvChunk;
-                const int valid = min(kEvChunk, nz - c * kEvChunk);
+                const int slot = k % kEvB;
+                mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
+                const double* sb = R.s + slot * kEvC;
+                const double* wb = R.w + slot * kEvC;
+                const double* gb = kGroup ? R.g + slot * kEvC : nullptr;
+                const int valid = min(kEvC, nz - c * kEvC);
                 for (int lb = 0; lb < valid; lb += kBlk) {
-                    const int gbase = c * kEvChunk + lb;
+                    const int gbase = c * kEvC + lb;
                     const int kb = gbase / kBlk;
                     double q1 = nq1, q2 = nq2;
                     const int Eb = nE;
                     if (kb + 1 < nblk) load_ck(kb + 1, nq1, nq2, nE);
-                    // re-scale threshold and the backward-part scale factor
-                    {
-                        const int Enew = Ep + Eb;
-                        if (Enew != Ethr) {
-                            thr *= pow2(Ethr - Enew);
-                            Ethr = Enew;
-                        }
-                        fq = pow2(Eb - Eqr);
+                    const int Enew = F.Ep + Eb;
+                    if (Enew != F.Ethr) {
+                        F.thr *= pow2(F.Ethr - Enew);
+                        F.Ethr = Enew;
                     }
-                    // q_{gbase+1 .. gbase+kBlk} of this block, relative to 2^Eb
+                    F.fq = pow2(Eb - F.Eqr);
+                    // q_{gbase+1 .. gbase+kBlk}, units 2^Eb
                     double qb[kBlk];
                     const int ctop = min(gbase + kBlk, nz);
+                    const bool full = gbase + kBlk <= nz;
+                    if (ctop == gbase + kBlk) {
+                        qb[kBlk - 1] = q1;
 #pragma unroll
-                    for (int jj = kBlk - 1; jj >= 0; --jj) {
-                        const int idx = gbase + 1 + jj;
-                        if (idx == ctop) {
-                            qb[jj] = q1;
-                        } else if (idx < ctop) {
-                            double qi = fma(sb[idx - c * kEvChunk] - mu, q1, -q2);
+                        for (int jj = kBlk - 2; jj >= 0; --jj) {
+                            const double qi = fma(sb[lb + jj + 1] - mu, q1, -q2);
                             qb[jj] = qi;
                             q2 = q1;
                             q1 = qi;
-                        } else {
-                            qb[jj] = 0.0;
                         }
-                    }
+                    } else {
 #pragma unroll
-                    for (int jj = 0; jj < kBlk; ++jj) {
-                        const int i = gbase + jj;
-                        if (i < nz) {
-                            const int li = lb + jj;
-                            const double wi = wb[li];
-                            const double sq = pm1 * pm1;
-                            An = An + sq;
-                            Aw = fma(sq, wi, Aw);
-                            const double qn = qb[jj];
-                            const double t = qn * fq;
-                            const double t2 = t * t;
-                            Tn = Tn + t2;
-                            Tw = fma(t2, wi, Tw);
-                            double gi = 0.0;
-                            if (kGroup) {
-                                gi = gb[li];
-                                Ag = fma(sq, gi, Ag);
-                                Tg = fma(t2, gi, Tg);
+                        for (int jj = kBlk - 1; jj >= 0; --jj) {
+                            const int idx = gbase + 1 + jj;
+                            if (idx == ctop) {
+                                qb[jj] = q1;
+                            } else if (idx < ctop) {
+                                const double qi = fma(sb[lb + jj + 1] - mu, q1, -q2);
+                                qb[jj] = qi;
+                                q2 = q1;
+                                q1 = qi;
+                            } else {
+                                qb[jj] = 0.0;
                             }
-                            const double prod = fabs(pm1 * qn);
-                            if (prod > thr) {
-                                thr = prod;
-                                r = i;
-                                Anr = An;
-                                Awr = Aw;
-                                Agr = Ag;
-                                sqr_ = sq;
-                                pr = pm1;
-                                Epr = Ep;
-                                qr = qn;
-                                Eqr = Eb;
-                                fq = 1.0;
-                                Tn = 0.0;
-                                Tw = 0.0;
-                                Tg = 0.0;
-                            }
-                            if (i == A.isrc) {
-                                ps = pm1;
-                                Eps = Ep;
-                                qs = qn;
-                                Eqs = Eb;
-                            }
-                            if (i == A.ircv) {
-                                prc = pm1;
-                                Eprc = Ep;
-                                qrc = qn;
-                                Eqrc = Eb;
-                            }
-                            const double a = sb[li] - mu;
-                            const double pn = fma(a, pm1, -pm2);
-                            pm2 = pm1;
-                            pm1 = pn;
                         }
                     }
-                    int sh = grow_shift(pm1, pm2);
+                    const bool special = !full || (A.isrc >= gbase && A.isrc < gbase + kBlk) ||
+                                         (A.ircv >= gbase && A.ircv < gbase + kBlk);
+                    if (!special) {
+#pragma unroll
+                        for (int jj = 0; jj < kBlk; ++jj)
+                            fwd_step<kGroup, false>(F, gbase + jj, nz, sb[lb + jj], wb[lb + jj],
+                                                    kGroup ? gb[lb + jj] : 0.0, qb[jj], Eb, mu, A.isrc, A.ircv);
+                    } else {
+#pragma unroll
+                        for (int jj = 0; jj < kBlk; ++jj) {
+                            const int li = min(lb + jj, valid - 1);
+                            fwd_step<kGroup, true>(F, gbase + jj, nz, sb[li], wb[li], kGroup ? gb[li] : 0.0, qb[jj],
+                                                   Eb, mu, A.isrc, A.ircv);
+                        }
+                    }
+                    const int sh = grow_shift(F.pm1, F.pm2);
                     if (sh) {
-                        double sc = pow2(-sh), sc2 = pow2(-2 * sh);
-                        pm1 *= sc;
-                        pm2 *= sc;
-                        An *= sc2;
-                        Aw *= sc2;
-                        Ag *= sc2;
-                        Ep += sh;
+                        const double sc = pow2(-sh), sc2 = pow2(-2 * sh);
+                        F.pm1 *= sc;
+                        F.pm2 *= sc;
+                        F.An *= sc2;
+                        F.Aw *= sc2;
+                        F.Ag *= sc2;
+                        F.Ep += sh;
                     }
                 }
-                __syncthreads();
-                if (tid == 0 && c + kEvNbuf < nch) {
+                __syncwarp();
+                if (lane == 0 && c + kEvB < nch) {
                     fence_proxy_async();
-                    evring_issue(R, base + c + kEvNbuf, c + kEvNbuf, sp, wp, gp);
+                    evr_issue(R, base + c + kEvB, c + kEvB, sp, wp, gp);
                 }
             }
             R.loads = base + nch;
         }
         // ---------------- combine ----------------------------------------
-        const double iq2 = 1.0 / (qr * qr);
-        const double isq = 1.0 / sqr_;
-        const double nrm = Anr * isq + Tn * iq2;
+        const double iq2 = 1.0 / (F.qr * F.qr);
+        const double isq = 1.0 / F.sqr;
+        const double nrm = F.Anr * isq + F.Tn * iq2;
         const double scale = 1.0 / sqrt(nrm * A.dz);
-        double zs = (A.isrc <= r) ? (ps / pr) * pow2(Eps - Epr) : (qs / qr) * pow2(Eqs - Eqr);
-        double zr = (A.ircv <= r) ? (prc / pr) * pow2(Eprc - Epr) : (qrc / qr) * pow2(Eqrc - Eqr);
+        const int r = F.r;
+        double zs = (A.isrc <= r) ? (F.ps / F.pr) * pow2(F.Eps - F.Epr) : (F.qs / F.qr) * pow2(F.Eqs - F.Eqr);
+        double zr = (A.ircv <= r) ? (F.prc / F.pr) * pow2(F.Eprc - F.Epr) : (F.qrc / F.qr) * pow2(F.Eqrc - F.Eqr);
         if ((A.isrc - r) & 1) zs = -zs;
         if ((A.ircv - r) & 1) zr = -zr;
-        const double absorption = (Awr * isq + Tw * iq2) / nrm;
+        const double absorption = (F.Awr * isq + F.Tw * iq2) / nrm;
         const double ks = sqrt(mu / A.h2);
         const double kk = ks * ks;
         const auto kp = csqrt_principal(kk, absorption);
         if (active) {
-            const int o = pi.off + w.j0 + tid;
+            const int o = pi.off + w.j0 + lane;
             A.kr[o] = kp.real();
             A.ki[o] = kp.imag();
             A.vs[o] = zs * scale;
             A.vr[o] = zr * scale;
             if (kGroup) {
-                const double gsum = (Agr * isq + Tg * iq2) / nrm;
+                const double gsum = (F.Agr * isq + F.Tg * iq2) / nrm;
                 const double vph = pi.omega / kp.real();
                 A.vg[o] = 1.0 / (vph * gsum);
             } else if (A.vg) {
@@ -1125,39 +1179,27 @@ __global__ void __launch_bounds__(kEvThreads) k_eigvec(EigvecArgs A) {
             double* vout = A.vfull + A.vfull_off[w.problem];
             const int M = pi.M;
             const unsigned base = R.loads;
-            if (tid == 0)
-                for (int c = 0; c < nch && c < kEvNbuf; ++c) evring_issue(R, base + c, c, sp, nullptr, nullptr);
+            if (lane == 0)
+                for (int c = 0; c < nch && c < kEvB; ++c) evr_issue(R, base + c, c, sp, nullptr, nullptr);
+            __syncwarp();
             double pa = 0.0, pb = 1.0;
             int Ea = 0;
             double nq1, nq2;
             int nE;
-            auto load_ck2 = [&](int kb, double& a1, double& a2, int& ae) {
-                int ctop = min((kb + 1) * kBlk, nz);
-                if (ctop >= nz) {
-                    a1 = 1.0;
-                    a2 = 0.0;
-                    ae = 0;
-                } else {
-                    size_t ci = (size_t)kb * kEvThreads + tid;
-                    a1 = ck1[ci];
-                    a2 = ck2[ci];
-                    ae = cke[ci];
-                }
-            };
-            load_ck2(0, nq1, nq2, nE);
-            const double ipr = 1.0 / pr, iqr = 1.0 / qr;
+            load_ck(0, nq1, nq2, nE);
+            const double ipr = 1.0 / F.pr, iqr = 1.0 / F.qr;
             for (int c = 0; c < nch; ++c) {
                 const unsigned k = base + c;
-                const int slot = k % kEvNbuf;
-                mbar_wait_bounded(&R.bars[slot], (k / kEvNbuf) & 1u, A.err);
-                const double* sb = R.sbuf + slot * kEvChunk;
-                const int valid = min(kEvChunk, nz - c * kEvChunk);
+                const int slot = k % kEvB;
+                mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
+                const double* sb = R.s + slot * kEvC;
+                const int valid = min(kEvC, nz - c * kEvC);
                 for (int lb = 0; lb < valid; lb += kBlk) {
-                    const int gbase = c * kEvChunk + lb;
+                    const int gbase = c * kEvC + lb;
                     const int kb = gbase / kBlk;
                     double q1 = nq1, q2 = nq2;
                     const int Eb = nE;
-                    if (kb + 1 < nblk) load_ck2(kb + 1, nq1, nq2, nE);
+                    if (kb + 1 < nblk) load_ck(kb + 1, nq1, nq2, nE);
                     double qb[kBlk];
                     const int ctop = min(gbase + kBlk, nz);
 #pragma unroll
@@ -1166,7 +1208,7 @@ __global__ void __launch_bounds__(kEvThreads) k_eigvec(EigvecArgs A) {
                         if (idx == ctop) {
                             qb[jj] = q1;
                         } else if (idx < ctop) {
-                            double qi = fma(sb[idx - c * kEvChunk] - mu, q1, -q2);
+                            const double qi = fma(sb[lb + jj + 1] - mu, q1, -q2);
                             qb[jj] = qi;
                             q2 = q1;
                             q1 = qi;
@@ -1174,38 +1216,36 @@ __global__ void __launch_bounds__(kEvThreads) k_eigvec(EigvecArgs A) {
                             qb[jj] = 0.0;
                         }
                     }
-                    const double fp = pow2(Ea - Epr) * ipr * scale;
-                    const double fqq = pow2(Eb - Eqr) * iqr * scale;
+                    const double fp = pow2(Ea - F.Epr) * ipr * scale;
+                    const double fqq = pow2(Eb - F.Eqr) * iqr * scale;
 #pragma unroll
                     for (int jj = 0; jj < kBlk; ++jj) {
                         const int i = gbase + jj;
                         if (i < nz) {
                             double zi = (i <= r) ? pb * fp : qb[jj] * fqq;
                             if ((i - r) & 1) zi = -zi;
-                            if (active) vout[(size_t)i * M + w.j0 + tid] = zi;
-                            const double a = sb[lb + jj] - mu;
-                            const double pn = fma(a, pb, -pa);
+                            if (active) vout[(size_t)i * M + w.j0 + lane] = zi;
+                            const double pn = fma(sb[lb + jj] - mu, pb, -pa);
                             pa = pb;
                             pb = pn;
                         }
                     }
-                    int sh = grow_shift(pb, pa);
+                    const int sh = grow_shift(pb, pa);
                     if (sh) {
-                        double sc = pow2(-sh);
+                        const double sc = pow2(-sh);
                         pa *= sc;
                         pb *= sc;
                         Ea += sh;
                     }
                 }
-                __syncthreads();
-                if (tid == 0 && c + kEvNbuf < nch) {
+                __syncwarp();
+                if (lane == 0 && c + kEvB < nch) {
                     fence_proxy_async();
-                    evring_issue(R, base + c + kEvNbuf, c + kEvNbuf, sp, nullptr, nullptr);
+                    evr_issue(R, base + c + kEvB, c + kEvB, sp, nullptr, nullptr);
                 }
             }
             R.loads = base + nch;
         }
-        __syncthreads();
     }
 }
 
@@ -1214,7 +1254,10 @@ static void* eigvec_fn() {
     return (void*)k_eigvec<G, V>;
 }
 
-static size_t eigvec_smem() { return 3 * kEvNbuf * kEvChunk * 8 + kEvNbuf * 8; }
+static size_t eigvec_smem(const EigvecArgs& a) {
+    const int na = a.g ? 3 : 2;
+    return (size_t)kEvWarps * (kEvB * na * kEvC * 8 + kEvB * 8);
+}
 
 static void* eigvec_select(const EigvecArgs& a) {
     const bool grp = a.g != nullptr, vec = a.vfull != nullptr;
@@ -1227,19 +1270,19 @@ static void* eigvec_select(const EigvecArgs& a) {
 int eigvec_ctas_per_sm(const EigvecArgs& a) {
     int n = 1;
     void* f = eigvec_select(a);
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eigvec_smem());
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kEvThreads, eigvec_smem()) != cudaSuccess) n = 1;
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eigvec_smem(a));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kEvWarps * 32, eigvec_smem(a)) != cudaSuccess) n = 1;
     return n < 1 ? 1 : n;
 }
 
 int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a) {
-    const size_t sm = eigvec_smem();
+    const size_t sm = eigvec_smem(a);
     const bool grp = a.g != nullptr, vec = a.vfull != nullptr;
     cudaFuncSetAttribute(eigvec_select(a), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (grp && vec) k_eigvec<true, true><<<grid, kEvThreads, sm, st>>>(a);
-    else if (grp) k_eigvec<true, false><<<grid, kEvThreads, sm, st>>>(a);
-    else if (vec) k_eigvec<false, true><<<grid, kEvThreads, sm, st>>>(a);
-    else k_eigvec<false, false><<<grid, kEvThreads, sm, st>>>(a);
+    if (grp && vec) k_eigvec<true, true><<<grid, kEvWarps * 32, sm, st>>>(a);
+    else if (grp) k_eigvec<true, false><<<grid, kEvWarps * 32, sm, st>>>(a);
+    else if (vec) k_eigvec<false, true><<<grid, kEvWarps * 32, sm, st>>>(a);
+    else k_eigvec<false, false><<<grid, kEvWarps * 32, sm, st>>>(a);
     return 1;
 }
 

@@ -38,8 +38,8 @@ constexpr int kChunk = 1024;      // doubles per TMA chunk of the diagonal
 constexpr int kBlk = 16;          // eigenvector checkpoint interval
 constexpr int kThreads = 256;     // threads of the scan CTAs
 constexpr int kWItem = 32;        // eigenvalues per warp work item of the bisection
-constexpr int kEvThreads = 64;    // threads (= eigenvalues) of an eigenvector CTA
-constexpr int kEvChunk = 512;     // doubles per TMA chunk in the eigenvector kernel
+constexpr int kEvItem = 32;       // eigenvalues per warp work item of the eigenvector kernel
+constexpr int kEvWarpsPerCta = 4; // warps per eigenvector CTA
 
 // knot-level derived quantities
 int launch_steffen(cudaStream_t st, int n, const double* x, const double* y, int batch, int ystride,
@@ -99,10 +99,10 @@ struct EigvecArgs {
     double* vg;
     double* vfull;            // optional: per problem [nz x M] at vfull_off[p]
     const long long* vfull_off;
-    double* ck_q1;            // checkpoint scratch, per CTA slot
+    double* ck_q1;            // checkpoint scratch, one slot per warp of the grid
     double* ck_q2;
     int* ck_e;
-    long long ck_slot_stride; // elements per slot
+    long long ck_slot_stride; // elements per warp slot (blocks x 32)
     unsigned* err;
 };
 int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a);

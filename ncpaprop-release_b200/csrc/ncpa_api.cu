@@ -723,8 +723,8 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
             std::vector<WorkItem> ev_items;
             for (int p = 0; p < P; ++p) {
                 const int Mp = M->info[p].M;
-                for (int j0 = 0; j0 < Mp; j0 += ncpa::kEvThreads)
-                    ev_items.push_back(WorkItem{p, j0, std::min(ncpa::kEvThreads, Mp - j0), 0});
+                for (int j0 = 0; j0 < Mp; j0 += ncpa::kEvItem)
+                    ev_items.push_back(WorkItem{p, j0, std::min(ncpa::kEvItem, Mp - j0), 0});
             }
             DevBuf d_ev_items;
             upload(d_ev_items, ev_items, st);
@@ -753,10 +753,11 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
             ea.vg = M->d_vg.as<double>();
             ea.vfull = prm->want_vectors ? M->d_vfull.as<double>() : nullptr;
             ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
-            const int grid_e = std::min(n_ev, ctx->num_sms * ncpa::eigvec_ctas_per_sm(ea));
+            const int ewpc = ncpa::kEvWarpsPerCta;
+            const int grid_e = std::min((n_ev + ewpc - 1) / ewpc, ctx->num_sms * ncpa::eigvec_ctas_per_sm(ea));
             const long long nblk = (nz + ncpa::kBlk - 1) / ncpa::kBlk;
-            const long long slot = nblk * ncpa::kEvThreads;
-            const size_t need = (size_t)grid_e * slot;
+            const long long slot = nblk * 32;
+            const size_t need = (size_t)grid_e * ewpc * slot;
             if (ctx->ck1.bytes < need * 8) {
                 ctx->ck1.alloc(need * 8, st);
                 ctx->ck2.alloc(need * 8, st);
