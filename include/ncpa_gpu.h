@@ -193,6 +193,28 @@ ncpa_status ncpa_ctx_sturm_sequences(ncpa_ctx *ctx, long long *sequences, long l
  * dependent-FMA kernel on every SM for about 50 ms. */
 ncpa_status ncpa_probe_fp64_peak(ncpa_ctx *ctx, double *tflops);
 
+/* Allocation-free eigenvectors of one problem.  No counterpart in the
+ * reference: this is for callers that cannot allocate device memory once
+ * they run (an application that reserves all GPU memory at start-up, code
+ * inside a memory budget it does not own, a runtime whose allocator must not
+ * be re-entered).  It allocates nothing and needs no context: every pointer
+ * is device memory owned by the caller, `stream` is a cudaStream_t (NULL for
+ * the default stream) on the current device, and the call returns once the
+ * results are in place.
+ *   s[nz]      scaled diagonal of h^2 A (the matrix ncpa_ess_solve builds)
+ *   w[nz]      attenuation weights 2 alpha omega / c_T on the same grid
+ *   mu[n]      eigenvalues of h^2 A, ascending
+ *   outputs    k_pert = re_k + i im_k and the normalised mode values at grid
+ *              points isrc / ircv, n entries each
+ * Scratch is one array inside the library of about 21 MiB per device, held
+ * until the process exits; limits: nz <= 32768 (NCPA_EINVAL beyond),
+ * n <= 4000 (NCPA_ETOOMANY beyond).  All calls share that array, so calls
+ * that overlap on the GPU race.  The first call on a device looks the array
+ * up; make it before any stream capture. */
+ncpa_status ncpa_eigvec_static(const double *s, const double *w, int nz, double dz, const double *mu,
+                               int n, int isrc, int ircv, double omega, double *re_k, double *im_k,
+                               double *v_src, double *v_rcv, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -415,6 +415,7 @@ class ModeSet:
     s: np.ndarray | None = None
     vfull: np.ndarray | None = None
     ceff: np.ndarray | None = None
+    w: np.ndarray | None = None          # attenuation weights on the grid
 
 
 BISECT_TOL = 1.0e-15  # absolute, in units of the scaled matrix h^2 A
@@ -459,6 +460,7 @@ def solve_problem(pp: Prepared, prm: EssParams, freq: float, az: float, want_gro
     if keep_matrix:
         ms.s = s
         ms.ceff = ceff
+        ms.w = w
         lo_c = L.orc_sturm_count(nz, _p(s), lo)
         mu = np.empty(max(M, 1))
         L.orc_bisect(nz, _p(s), lo, hi, lo_c, M, BISECT_TOL, _p(mu))
