@@ -117,6 +117,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def reduce_max(values):
+    """Element-wise max over the ranks of the initialised process group (the
+    slowest rank's device time is the job's time)."""
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(values, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -238,11 +250,7 @@ def run_ours(args):
     plain_rate = len(plain_freqs) / (ev0.elapsed_time(ev1) / 1e3)
 
     if world > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([ms_dev, ms_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_dev, ms_e2e = tt.tolist()
+        ms_dev, ms_e2e = reduce_max([ms_dev, ms_e2e])
     fp64_peak = ctx.fp64_peak_tflops() if rank == 0 else None
     if rank == 0:
         solves = NFREQ * args.steps * world
