@@ -169,6 +169,12 @@ ncpa_status ncpa_bb_synthesize(ncpa_ctx *ctx, const ncpa_dispersion_desc *disp,
  * azimuth; frequencies must be uniformly spaced from df): no host round trip */
 ncpa_status ncpa_bb_synthesize_modes(ncpa_ctx *ctx, const ncpa_modes *modes, int az_index,
                                      const ncpa_bb_params *bp, double *waveforms);
+/* built-in source spectra at the n_freq dispersion bins f (f[0] = 0):
+ * kind 0 impulse, 1 pulse1, 2 pulse2 (BroadbandPropagator::get_source_spectrum,
+ * BroadbandPropagator.cpp:260-311, pulse_spec_fit :420-438, model_pulse_fft
+ * :440-476); f_center < 0 selects f_max/5 */
+ncpa_status ncpa_source_spectrum_builtin(ncpa_ctx *ctx, int kind, const double *f, int n_freq,
+                                         double f_center, int nfft, double *s_re, double *s_im);
 /* source spectrum of a sampled waveform: sum_n x_n exp(+2 pi i k n / nfft) dt
  * for k < n_freq (BroadbandPropagator.cpp:327-353) */
 ncpa_status ncpa_source_spectrum_waveform(ncpa_ctx *ctx, const double *x, int n_samples, double dt,

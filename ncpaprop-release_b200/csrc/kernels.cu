@@ -1431,29 +1431,48 @@ int launch_twiddle(cudaStream_t st, int nfft, double* tw) {
     return 1;
 }
 
+// per-mode factors of the transfer function: V_s V_r and 1/sqrt(k) (principal)
+__global__ void k_bb_prep(int n, const double* __restrict__ re_k, const double* __restrict__ im_k,
+                          const double* __restrict__ vs, const double* __restrict__ vr, int zero_attn,
+                          double* __restrict__ fac) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double a = re_k[j], b = zero_attn ? 0.0 : im_k[j];
+    const auto sk = csqrt_principal(a, b);
+    const double den = sk.real() * sk.real() + sk.imag() * sk.imag();
+    fac[4 * j + 0] = vs[j] * vr[j];
+    fac[4 * j + 1] = sk.real() / den;
+    fac[4 * j + 2] = -sk.imag() / den;
+    fac[4 * j + 3] = b;
+}
+
 // transfer function H(f, r) = i e^{-i pi/4}/sqrt(8 pi r) sqrt(rho_r/rho_s)
-//   sum_j V_s V_r e^{i k r}/sqrt(k), half-Hann over the top 10 % of bins
+//   sum_j V_s V_r e^{i k r}/sqrt(k), half-Hann over the top 10 % of bins;
+// one warp per (frequency, range), lanes over the modes of that frequency
 __global__ void k_bb_transfer(int nfreq, const int* __restrict__ off, const double* __restrict__ re_k,
-                              const double* __restrict__ im_k, const double* __restrict__ vs,
-                              const double* __restrict__ vr, double rho_ratio, int nr,
-                              const double* __restrict__ ranges, int zero_attn, double* __restrict__ h) {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    const int ir = blockIdx.y;
-    if (f >= nfreq || ir >= nr) return;
+                              const double* __restrict__ fac, double rho_ratio, int nr,
+                              const double* __restrict__ ranges, double* __restrict__ h) {
+    const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wg >= nfreq * nr) return;
+    const int f = wg % nfreq, ir = wg / nfreq;
     const double r = ranges[ir];
     double cr = 0.0, ci = 0.0;
-    for (int j = off[f]; j < off[f + 1]; ++j) {
-        const double a = re_k[j], b = zero_attn ? 0.0 : im_k[j];
+    for (int j = off[f] + lane; j < off[f + 1]; j += 32) {
         double sn, cs;
-        sincos(r * a, &sn, &cs);
-        const double amp = exp(-r * b) * (vs[j] * vr[j]);
+        sincos(r * re_k[j], &sn, &cs);
+        const double amp = exp(-r * fac[4 * j + 3]) * fac[4 * j];
         const double er = amp * cs, ei = amp * sn;
-        const auto sk = csqrt_principal(a, b);
-        const double den = sk.real() * sk.real() + sk.imag() * sk.imag();
-        const double isr = sk.real() / den, isi = -sk.imag() / den;
+        const double isr = fac[4 * j + 1], isi = fac[4 * j + 2];
         cr += er * isr - ei * isi;
         ci += er * isi + ei * isr;
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        cr += __shfl_xor_sync(0xffffffffu, cr, o);
+        ci += __shfl_xor_sync(0xffffffffu, ci, o);
+    }
+    if (lane != 0) return;
     // i e^{-i pi/4} = sin(pi/4) + i cos(pi/4)
     const double c0 = sqrt(rho_ratio) / sqrt(8.0 * kPi * r);
     const double ang = kPi * 0.25;
@@ -1472,9 +1491,62 @@ __global__ void k_bb_transfer(int nfreq, const int* __restrict__ off, const doub
 
 int launch_bb_transfer(cudaStream_t st, int nfreq, const int* off, const double* re_k, const double* im_k,
                        const double* vs, const double* vr, double rho_ratio, int nr, const double* ranges,
-                       int zero_attn, double* h) {
-    dim3 grid((nfreq + 127) / 128, nr);
-    k_bb_transfer<<<grid, 128, 0, st>>>(nfreq, off, re_k, im_k, vs, vr, rho_ratio, nr, ranges, zero_attn, h);
+                       int zero_attn, int n_modes, double* fac, double* h) {
+    int launches = 0;
+    if (n_modes > 0) {
+        k_bb_prep<<<(n_modes + 255) / 256, 256, 0, st>>>(n_modes, re_k, im_k, vs, vr, zero_attn, fac);
+        ++launches;
+    }
+    const long long threads = (long long)nfreq * nr * 32;
+    k_bb_transfer<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(nfreq, off, re_k, fac, rho_ratio, nr, ranges,
+                                                                     h);
+    return launches + 1;
+}
+
+// built-in source spectra at the dispersion bins (BroadbandPropagator.cpp:
+// 260-297, 420-438): 0 impulse e^{2 pi i f Nfreq/2}; 1 pulse1 (analytic fit,
+// scale = 1/f_center); the returned spectrum is interleaved (re, im)
+__global__ void k_src_builtin(int kind, int nfreq, const double* __restrict__ f, double scale,
+                              double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfreq) return;
+    const double PI = kPi;
+    double re, im;
+    if (kind == 0) {
+        double sn, cs;
+        sincos(2.0 * PI * f[i] * (double)nfreq / 2.0, &sn, &cs);
+        re = cs;
+        im = sn;
+    } else {
+        const double fnorm = 0.780776406404415;
+        const double x = scale * fnorm * f[i];
+        // x e^{(-x - x^2)/2} e^{-i pi/2} scale / 33.4336, times 4 pi 5 e^{2 pi i x 0.01}
+        const double mag = 4.0 * PI * 5.0 * (x * exp((-x - x * x) / 2) * scale / 33.4336);
+        double ph = -0.5 * PI + 2.0 * PI * x * 0.01 + 2.0 * PI * f[i] * scale;
+        double sn, cs;
+        sincos(ph, &sn, &cs);
+        re = mag * cs / 2.0;
+        im = mag * sn / 2.0;
+    }
+    out[2 * i] = re;
+    out[2 * i + 1] = im;
+}
+
+// power-law pulse model of source type pulse2, sampled at t = i dt
+__global__ void k_src_pulse2(int n, double dt, double scale, double power, double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double xx = 2.094 * (1.0 + power) * (i * dt) / scale;
+    x[i] = pow(xx, power) * (1 - xx / (1.0 + power)) * exp(-xx) / 1.387566e+03;
+}
+
+int launch_src_builtin(cudaStream_t st, int kind, int nfreq, const double* f, double scale, double* out) {
+    k_src_builtin<<<(nfreq + 127) / 128, 128, 0, st>>>(kind, nfreq, f, scale, out);
+    return 1;
+}
+
+int launch_src_pulse2(cudaStream_t st, int n, double dt, double scale, double* x) {
+    k_src_pulse2<<<(n + 255) / 256, 256, 0, st>>>(n, dt, scale, 8.0, x);
     return 1;
 }
 

@@ -116,9 +116,12 @@ int launch_tl2d(cudaStream_t st, int M, const double* kr, const double* ki, cons
                 const double* vz, int nzo, int nr, double dr, int lossless, double* re, double* im);
 // broadband synthesis
 int launch_twiddle(cudaStream_t st, int nfft, double* tw);
+// fac: scratch of 4 doubles per mode
 int launch_bb_transfer(cudaStream_t st, int nfreq, const int* off, const double* re_k, const double* im_k,
                        const double* vs, const double* vr, double rho_ratio, int nr, const double* ranges,
-                       int zero_attn, double* h);
+                       int zero_attn, int n_modes, double* fac, double* h);
+int launch_src_builtin(cudaStream_t st, int kind, int nfreq, const double* f, double scale, double* out);
+int launch_src_pulse2(cudaStream_t st, int n, double dt, double scale, double* x);
 int launch_bb_pulse(cudaStream_t st, int nfreq, const double* f, const double* s_src, const double* h, int nr,
                     const double* t0, int nfft, const double* tw, double* out);
 int launch_src_dft(cudaStream_t st, int n, const double* x, double dt, int nfft, int nfreq, const double* tw,

@@ -936,7 +936,7 @@ ncpa_status ncpa_tl_2d(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const nc
 // broadband synthesis
 // ---------------------------------------------------------------------------
 namespace {
-ncpa_status bb_common(ncpa_ctx* ctx, int nfreq, const double* d_f, const int* d_off, const double* d_rk,
+ncpa_status bb_common(ncpa_ctx* ctx, int nfreq, const double* d_f, const int* d_off, int n_modes, const double* d_rk,
                       const double* d_ik, const double* d_vs, const double* d_vr, double rho_ratio,
                       const ncpa_bb_params* bp, double* waveforms) {
     cudaStream_t st = ctx->stream;
@@ -950,8 +950,9 @@ ncpa_status bb_common(ncpa_ctx* ctx, int nfreq, const double* d_f, const int* d_
         src[2 * i] = bp->src_re[i];
         src[2 * i + 1] = bp->src_im[i];
     }
-    DevBuf dr, dt0, dsrc, dh;
+    DevBuf dr, dt0, dsrc, dh, dfac;
     DevBuf& dout = ctx->bb_out;
+    dfac.alloc((size_t)std::max(n_modes, 1) * 4 * 8, st);
     upload(dr, bp->ranges_m, nr, st);
     upload(dt0, t0, st);
     upload(dsrc, src, st);
@@ -959,7 +960,8 @@ ncpa_status bb_common(ncpa_ctx* ctx, int nfreq, const double* d_f, const int* d_
     dout.alloc((size_t)nr * nfft * 8, st);
     const double* tw = twiddle(ctx, nfft);
     check_launch(ctx, ncpa::launch_bb_transfer(st, nfreq, d_off, d_rk, d_ik, d_vs, d_vr, rho_ratio, nr,
-                                               dr.as<double>(), bp->zero_attn, dh.as<double>()));
+                                               dr.as<double>(), bp->zero_attn, n_modes, dfac.as<double>(),
+                                               dh.as<double>()));
     check_launch(ctx, ncpa::launch_bb_pulse(st, nfreq, d_f, dsrc.as<double>(), dh.as<double>(), nr, dt0.as<double>(),
                                             nfft, tw, dout.as<double>()));
     if (waveforms) CK(cudaMemcpyAsync(waveforms, dout.p, (size_t)nr * nfft * 8, cudaMemcpyDeviceToHost, st));
@@ -984,7 +986,7 @@ ncpa_status ncpa_bb_synthesize(ncpa_ctx* ctx, const ncpa_dispersion_desc* d, con
         upload(dik, d->im_k, std::max(mt, 1), st);
         upload(dvs, d->v_src, std::max(mt, 1), st);
         upload(dvr, d->v_rcv, std::max(mt, 1), st);
-        return bb_common(ctx, nf, df.as<double>(), doff.as<int>(), drk.as<double>(), dik.as<double>(),
+        return bb_common(ctx, nf, df.as<double>(), doff.as<int>(), mt, drk.as<double>(), dik.as<double>(),
                          dvs.as<double>(), dvr.as<double>(), d->rho_rcv / d->rho_src, bp, waveforms);
     });
 }
@@ -1009,8 +1011,48 @@ ncpa_status ncpa_bb_synthesize_modes(ncpa_ctx* ctx, const ncpa_modes* m, int az_
         DevBuf df, doff;
         upload(df, f, st);
         upload(doff, off, st);
-        return bb_common(ctx, nf, df.as<double>(), doff.as<int>(), m->d_kr.as<double>(), m->d_ki.as<double>(),
-                         m->d_vs.as<double>(), m->d_vr.as<double>(), m->rho_rcv / m->rho_src, bp, waveforms);
+        return bb_common(ctx, nf, df.as<double>(), doff.as<int>(), m->Mtot, m->d_kr.as<double>(),
+                         m->d_ki.as<double>(), m->d_vs.as<double>(), m->d_vr.as<double>(), m->rho_rcv / m->rho_src,
+                         bp, waveforms);
+    });
+}
+
+ncpa_status ncpa_source_spectrum_builtin(ncpa_ctx* ctx, int kind, const double* f, int nfreq, double f_center,
+                                         int nfft, double* s_re, double* s_im) {
+    if (!ctx || !f || !s_re || !s_im || nfreq < 3 || kind < 0 || kind > 2) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        const double fmax = f[nfreq - 1];
+        double scale = 0.0;
+        if (kind >= 1) {  // BroadbandPropagator.cpp:268-283
+            double fc = f_center < 0.0 ? fmax / 5.0 : f_center;
+            if (!(fc > 0 && fc <= fmax / 5.0 + 1.0E-16))
+                throw ApiError(NCPA_EINVAL, "f_center is too large: the built-in pulse needs f_center <= f_max/5");
+            scale = 1.0 / fc;
+        }
+        DevBuf df, ds;
+        upload(df, f, nfreq, st);
+        ds.alloc((size_t)2 * nfreq * 8, st);
+        if (kind <= 1) {
+            check_launch(ctx, ncpa::launch_src_builtin(st, kind, nfreq, df.as<double>(), scale, ds.as<double>()));
+        } else {  // pulse2: transform of the sampled power-law pulse, dt = 1/(nfft df)
+            if (nfft < nfreq) throw ApiError(NCPA_EINVAL, "nfft must be >= the number of frequencies");
+            const double dt = 1.0 / ((double)nfft * (f[2] - f[1]));
+            DevBuf dx;
+            dx.alloc((size_t)nfft * 8, st);
+            check_launch(ctx, ncpa::launch_src_pulse2(st, nfft, dt, scale, dx.as<double>()));
+            const double* tw = twiddle(ctx, nfft);
+            check_launch(ctx, ncpa::launch_src_dft(st, nfft, dx.as<double>(), dt, nfft, nfreq, tw, ds.as<double>()));
+        }
+        std::vector<double> h(2 * (size_t)nfreq);
+        CK(cudaMemcpyAsync(h.data(), ds.p, h.size() * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int k = 0; k < nfreq; ++k) {
+            s_re[k] = h[2 * k];
+            s_im[k] = h[2 * k + 1];
+        }
+        return NCPA_OK;
     });
 }
 

@@ -27,7 +27,8 @@ EXPORTED = [
     "ncpa_modes_info", "ncpa_modes_get", "ncpa_modes_get_vectors", "ncpa_tl_1d", "ncpa_tl_2d_heights",
     "ncpa_tl_2d", "ncpa_bb_synthesize", "ncpa_bb_synthesize_modes", "ncpa_source_spectrum_waveform",
     "ncpa_kernel_launches", "ncpa_ctx_stream", "ncpa_ctx_set_timing", "ncpa_ctx_phase_stats",
-    "ncpa_ctx_reset_stats", "ncpa_ctx_sturm_sequences", "ncpa_probe_fp64_peak",
+    "ncpa_ctx_reset_stats", "ncpa_ctx_sturm_sequences", "ncpa_probe_fp64_peak", "ncpa_source_spectrum_builtin",
+    "ncpa_eigvec_static",
 ]
 
 
@@ -113,6 +114,7 @@ def lib():
         L.ncpa_ctx_reset_stats.argtypes = [_vp]
         L.ncpa_ctx_sturm_sequences.argtypes = [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]
         L.ncpa_probe_fp64_peak.argtypes = [_vp, _dp]
+        L.ncpa_source_spectrum_builtin.argtypes = [_vp, _c_int, _dp, _c_int, _c_double, _c_int, _dp, _dp]
         _lib = L
     return _lib
 
@@ -223,6 +225,15 @@ class Context:
         self.check(lib().ncpa_ess_solve(self.h, profile.h, ctypes.byref(params), _p(f), len(f), _p(a), len(a),
                                         ctypes.byref(h)), "ncpa_ess_solve")
         return Modes(self, h, f, a)
+
+    SOURCES = {"impulse": 0, "pulse1": 1, "pulse2": 2}
+
+    def source_spectrum_builtin(self, kind, f, nfft, f_center=-1.0):
+        f = _f64(f)
+        sre, sim = np.empty(len(f)), np.empty(len(f))
+        self.check(lib().ncpa_source_spectrum_builtin(self.h, self.SOURCES[kind], _p(f), len(f), float(f_center),
+                                                      int(nfft), _p(sre), _p(sim)), "ncpa_source_spectrum_builtin")
+        return sre, sim
 
     def source_spectrum_waveform(self, x, dt, nfft, nfreq):
         x = _f64(x)
