@@ -66,6 +66,21 @@ ncpa_status ncpa_profile_create(ncpa_ctx *ctx, const ncpa_profile_desc *desc, nc
 ncpa_status ncpa_profile_load(ncpa_ctx *ctx, const char *path, const char *header_path,
                               ncpa_profile **out);
 ncpa_status ncpa_profile_destroy(ncpa_profile *prof);
+/* User attenuation table (height km, Np/m), interpolated onto the profile
+ * knots and used at every frequency instead of Sutherland-Bass (replaces
+ * Atmosphere1D::read_attenuation_from_file, Atmosphere1D.cpp:307-424). */
+ncpa_status ncpa_profile_set_attn(ncpa_profile *prof, const double *z_km, const double *attn, int n);
+/* same, from a two-column text file "height_km  attenuation_Np/m" */
+ncpa_status ncpa_profile_load_attn(ncpa_profile *prof, const char *path);
+/* Knot columns in SI units (z [m], u, v [m/s], t [K], p [Pa], rho [kg/m^3]),
+ * the static sound speed c0 and the effective sound speed for one azimuth at
+ * the knots -- the columns of atm_profile.nm (ESSModeSolver.cpp:468-484,
+ * Atmosphere1D::print_atmosphere, Atmosphere1D.cpp:924-970); any output
+ * pointer may be NULL. */
+ncpa_status ncpa_profile_knots(ncpa_profile *prof, double az_deg, double *z, double *u, double *v,
+                               double *t, double *p, double *rho, double *c0, double *ceff);
+/* ground height scalar Z0 [m] of the profile, if it has one */
+ncpa_status ncpa_profile_z0(const ncpa_profile *prof, double *z0_m, int *has_z0);
 /* Number of knots and the altitude range [m] of a loaded profile. */
 ncpa_status ncpa_profile_info(const ncpa_profile *prof, int *n_knots, double *z_lo, double *z_hi);
 
@@ -136,6 +151,12 @@ ncpa_status ncpa_tl_2d_heights(const ncpa_modes *modes, int problem, int *n_heig
 ncpa_status ncpa_tl_2d(ncpa_ctx *ctx, const ncpa_modes *modes, int problem, const ncpa_tl_params *tp,
                        double *z_out, double *re, double *im);
 
+/* Modal starter of one problem (ESSModeSolver::getModalStarter,
+ * ESSModeSolver.cpp:670-723; needs want_vectors).  Call with NULL outputs to
+ * get the number of heights in *n_out. */
+ncpa_status ncpa_modal_starter(ncpa_ctx *ctx, const ncpa_modes *modes, int problem, int *n_out,
+                               double *z_km, double *re, double *im);
+
 /* ------------------------------------------------------------------------
  * ModBB pulse synthesis (ModalBroadbandPropagator::calculate_waveform and
  * BroadbandPropagator::fft_pulse_prop, ModalBroadbandPropagator.cpp:141-277,
@@ -175,6 +196,10 @@ ncpa_status ncpa_bb_synthesize_modes(ncpa_ctx *ctx, const ncpa_modes *modes, int
  * :440-476); f_center < 0 selects f_max/5 */
 ncpa_status ncpa_source_spectrum_builtin(ncpa_ctx *ctx, int kind, const double *f, int n_freq,
                                          double f_center, int nfft, double *s_re, double *s_im);
+/* time series of a source spectrum: 2 Re( df sum_n S_n exp(-2 pi i k n / nfft) ),
+ * k < nfft (the source_waveform_input.dat of BroadbandPropagator.cpp:360-404) */
+ncpa_status ncpa_source_waveform(ncpa_ctx *ctx, const double *f, int n_freq, const double *s_re,
+                                 const double *s_im, int nfft, double *out);
 /* source spectrum of a sampled waveform: sum_n x_n exp(+2 pi i k n / nfft) dt
  * for k < n_freq (BroadbandPropagator.cpp:327-353) */
 ncpa_status ncpa_source_spectrum_waveform(ncpa_ctx *ctx, const double *x, int n_samples, double dt,

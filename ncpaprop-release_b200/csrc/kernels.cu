@@ -1570,7 +1570,7 @@ __global__ void __launch_bounds__(256) k_bb_pulse(int nfreq, const double* __res
         arg[2 * n + 1] = ar * hi + ai * hr;
     }
     __syncthreads();
-    const double df = f[1] - f[0];
+    const double df = f[2] - f[1];  // f_step of ModalBroadbandPropagator.cpp:65
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nfft; k += gridDim.x * blockDim.x) {
         double accr = 0.0;
         int idx = 0;
@@ -1608,6 +1608,53 @@ __global__ void k_src_dft(int n, const double* __restrict__ x, double dt, int nf
     }
     s[2 * k] = ar * dt;
     s[2 * k + 1] = ai * dt;
+}
+
+// values of a Steffen spline at m points (clamped outside the knots)
+__global__ void k_spline_eval(int n, const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ coef, int m, const double* __restrict__ xq,
+                              double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) out[k] = spline_get(n, x, y, coef, xq[k]);
+}
+
+int launch_spline_eval(cudaStream_t st, int n, const double* x, const double* y, const double* coef, int m,
+                       const double* xq, double* out) {
+    k_spline_eval<<<(m + 255) / 256, 256, 0, st>>>(n, x, y, coef, m, xq, out);
+    return 1;
+}
+
+// modal starter field (ESSModeSolver::getModalStarter, ESSModeSolver.cpp:
+// 670-723): psi(z_j) = pi sqrt(k0) sum_m v_m(z_s) v_m(z_j) / sqrt(Re k_m)
+__global__ void k_starter(int M, int nz, int step, int isrc, const double* __restrict__ v,
+                          const double* __restrict__ kr, double k0, double* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int zi = j * step;
+    if (zi >= nz) return;
+    double acc = 0.0;
+    for (int m = 0; m < M; ++m) acc += v[(size_t)isrc * M + m] * v[(size_t)zi * M + m] / sqrt(kr[m]);
+    out[j] = acc * kPi * sqrt(k0);
+}
+
+int launch_starter(cudaStream_t st, int M, int nz, int step, int isrc, const double* v, const double* kr,
+                   double k0, double* out) {
+    const int nout = (nz + step - 1) / step;
+    k_starter<<<(nout + 127) / 128, 128, 0, st>>>(M, nz, step, isrc, v, kr, k0, out);
+    return 1;
+}
+
+// unit transfer function (complex 1) for [nr x nfreq] bins
+__global__ void k_fill_unit(int n, double* __restrict__ h) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        h[2 * k] = 1.0;
+        h[2 * k + 1] = 0.0;
+    }
+}
+
+int launch_fill_unit(cudaStream_t st, int n, double* h) {
+    k_fill_unit<<<(n + 255) / 256, 256, 0, st>>>(n, h);
+    return 1;
 }
 
 int launch_src_dft(cudaStream_t st, int n, const double* x, double dt, int nfft, int nfreq, const double* tw,

@@ -121,6 +121,11 @@ int launch_bb_transfer(cudaStream_t st, int nfreq, const int* off, const double*
                        const double* vs, const double* vr, double rho_ratio, int nr, const double* ranges,
                        int zero_attn, int n_modes, double* fac, double* h);
 int launch_src_builtin(cudaStream_t st, int kind, int nfreq, const double* f, double scale, double* out);
+int launch_spline_eval(cudaStream_t st, int n, const double* x, const double* y, const double* coef, int m,
+                       const double* xq, double* out);
+int launch_starter(cudaStream_t st, int M, int nz, int step, int isrc, const double* v, const double* kr,
+                   double k0, double* out);
+int launch_fill_unit(cudaStream_t st, int n, double* h);
 int launch_src_pulse2(cudaStream_t st, int n, double dt, double scale, double* x);
 int launch_bb_pulse(cudaStream_t st, int nfreq, const double* f, const double* s_src, const double* h, int nr,
                     const double* t0, int nfft, const double* tw, double* out);

@@ -479,6 +479,90 @@ ncpa_status ncpa_profile_load(ncpa_ctx* ctx, const char* path, const char* heade
     return ncpa_profile_create(ctx, &d, out);
 }
 
+ncpa_status ncpa_profile_set_attn(ncpa_profile* prof, const double* z_km, const double* attn, int n) {
+    if (!prof || !z_km || !attn || n < 2) return NCPA_EINVAL;
+    ncpa_ctx* ctx = prof->ctx;
+    return guarded(ctx, [&]() -> ncpa_status {
+        for (int i = 1; i < n; ++i)
+            if (!(z_km[i] > z_km[i - 1])) throw ApiError(NCPA_EINVAL, "attenuation heights must increase strictly");
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        // extend the table to the profile's range with its end values, in
+        // km like the reference (Atmosphere1D.cpp:365-396)
+        std::vector<double> hz(prof->n);
+        CK(cudaMemcpyAsync(hz.data(), prof->z.p, prof->n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (auto& z : hz) z = z * 0.001;
+        std::vector<double> za(z_km, z_km + n), aa(attn, attn + n);
+        if (za.front() > hz.front()) {
+            za.insert(za.begin(), hz.front());
+            aa.insert(aa.begin(), aa.front());
+        }
+        if (za.back() < hz.back()) {
+            za.push_back(hz.back());
+            aa.push_back(aa.back());
+        }
+        const int na = (int)za.size();
+        DevBuf dza, daa, dcoef, dq;
+        upload(dza, za, st);
+        upload(daa, aa, st);
+        upload(dq, hz, st);
+        dcoef.alloc((size_t)4 * (na - 1) * 8, st);
+        check_launch(ctx, ncpa::launch_steffen(st, na, dza.as<double>(), daa.as<double>(), 1, na, dcoef.as<double>(),
+                                               4 * (na - 1)));
+        prof->attn.alloc((size_t)prof->n * 8, st);
+        check_launch(ctx, ncpa::launch_spline_eval(st, na, dza.as<double>(), daa.as<double>(), dcoef.as<double>(),
+                                                   prof->n, dq.as<double>(), prof->attn.as<double>()));
+        prof->has_attn = true;
+        CK(cudaStreamSynchronize(st));
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_profile_load_attn(ncpa_profile* prof, const char* path) {
+    if (!prof || !path) return NCPA_EINVAL;
+    std::vector<double> zk, a;
+    ncpa_status s = guarded(prof->ctx, [&]() -> ncpa_status {
+        ncpa::read_attn_file(path, zk, a);
+        return NCPA_OK;
+    });
+    if (s != NCPA_OK) return s;
+    return ncpa_profile_set_attn(prof, zk.data(), a.data(), (int)zk.size());
+}
+
+ncpa_status ncpa_profile_knots(ncpa_profile* prof, double az_deg, double* z, double* u, double* v, double* t,
+                               double* p, double* rho, double* c0, double* ceff) {
+    if (!prof) return NCPA_EINVAL;
+    ncpa_ctx* ctx = prof->ctx;
+    return guarded(ctx, [&]() -> ncpa_status {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        const int n = prof->n;
+        DevBuf daz, dce;
+        if (ceff) {
+            upload(daz, &az_deg, 1, st);
+            dce.alloc((size_t)n * 8, st);
+            check_launch(ctx, ncpa::launch_ceff_knots(st, n, 1, daz.as<double>(), prof->c0.as<double>(),
+                                                      prof->ws.as<double>(), prof->wd.as<double>(),
+                                                      dce.as<double>()));
+        }
+        const std::pair<double*, const DevBuf*> cols[] = {{z, &prof->z},   {u, &prof->u},     {v, &prof->v},
+                                                          {t, &prof->t},   {p, &prof->p},     {rho, &prof->rho},
+                                                          {c0, &prof->c0}, {ceff, &dce}};
+        for (const auto& c : cols)
+            if (c.first) CK(cudaMemcpyAsync(c.first, c.second->p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_profile_z0(const ncpa_profile* prof, double* z0_m, int* has_z0) {
+    if (!prof) return NCPA_EINVAL;
+    if (z0_m) *z0_m = prof->z0;
+    if (has_z0) *has_z0 = prof->has_z0;
+    return NCPA_OK;
+}
+
 ncpa_status ncpa_profile_destroy(ncpa_profile* prof) {
     if (!prof) return NCPA_EINVAL;
     cudaSetDevice(prof->ctx->device);
@@ -1014,6 +1098,67 @@ ncpa_status ncpa_bb_synthesize_modes(ncpa_ctx* ctx, const ncpa_modes* m, int az_
         return bb_common(ctx, nf, df.as<double>(), doff.as<int>(), m->Mtot, m->d_kr.as<double>(),
                          m->d_ki.as<double>(), m->d_vs.as<double>(), m->d_vr.as<double>(), m->rho_rcv / m->rho_src,
                          bp, waveforms);
+    });
+}
+
+ncpa_status ncpa_modal_starter(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int* n_out, double* z_km,
+                               double* re, double* im) {
+    if (!ctx || !m || !n_out || problem < 0 || problem >= m->P) return NCPA_EINVAL;
+    if (!m->prm.want_vectors) return fail(ctx, NCPA_EINVAL, "the modal starter needs a solve with want_vectors");
+    return guarded(ctx, [&]() -> ncpa_status {
+        const ProblemInfo& pi = m->info[problem];
+        const double freq = pi.freq;
+        int step = (int)((340.0 / freq) / 10 / m->dz);  // ESSModeSolver.cpp:692-693
+        if (step < 1) step = 1;
+        const int nout = (m->nz + step - 1) / step;
+        if (!z_km || !re || !im) {
+            *n_out = nout;
+            return NCPA_OK;
+        }
+        if (*n_out < nout) throw ApiError(NCPA_EINVAL, "output arrays too short for the modal starter");
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        DevBuf dout;
+        dout.alloc((size_t)nout * 8, st);
+        const double k0 = 2 * kPi * freq / 340.0;
+        check_launch(ctx, ncpa::launch_starter(st, pi.M, m->nz, step, m->isrc,
+                                               m->d_vfull.as<double>() + m->vfull_off[problem],
+                                               m->d_kr.as<double>() + pi.off, k0, dout.as<double>()));
+        CK(cudaMemcpyAsync(re, dout.p, nout * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int j = 0; j < nout; ++j) {
+            z_km[j] = (j * step) * m->dz / 1000.0;
+            im[j] = 0.0;
+        }
+        *n_out = nout;
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_source_waveform(ncpa_ctx* ctx, const double* f, int nfreq, const double* s_re, const double* s_im,
+                                 int nfft, double* out) {
+    if (!ctx || !f || !s_re || !s_im || !out || nfreq < 3 || nfft < nfreq) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        std::vector<double> src(2 * (size_t)nfreq), t0(1, 0.0);
+        for (int i = 0; i < nfreq; ++i) {
+            src[2 * i] = s_re[i];
+            src[2 * i + 1] = s_im[i];
+        }
+        DevBuf df, dsrc, dh, dt0, dout;
+        upload(df, f, nfreq, st);
+        upload(dsrc, src, st);
+        upload(dt0, t0, st);
+        dh.alloc((size_t)nfreq * 16, st);
+        dout.alloc((size_t)nfft * 8, st);
+        check_launch(ctx, ncpa::launch_fill_unit(st, nfreq, dh.as<double>()));
+        const double* tw = twiddle(ctx, nfft);
+        check_launch(ctx, ncpa::launch_bb_pulse(st, nfreq, df.as<double>(), dsrc.as<double>(), dh.as<double>(), 1,
+                                                dt0.as<double>(), nfft, tw, dout.as<double>()));
+        CK(cudaMemcpyAsync(out, dout.p, (size_t)nfft * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return NCPA_OK;
     });
 }
 

@@ -28,7 +28,8 @@ EXPORTED = [
     "ncpa_tl_2d", "ncpa_bb_synthesize", "ncpa_bb_synthesize_modes", "ncpa_source_spectrum_waveform",
     "ncpa_kernel_launches", "ncpa_ctx_stream", "ncpa_ctx_set_timing", "ncpa_ctx_phase_stats",
     "ncpa_ctx_reset_stats", "ncpa_ctx_sturm_sequences", "ncpa_probe_fp64_peak", "ncpa_source_spectrum_builtin",
-    "ncpa_eigvec_static",
+    "ncpa_eigvec_static", "ncpa_profile_set_attn", "ncpa_profile_load_attn", "ncpa_profile_knots", "ncpa_profile_z0",
+    "ncpa_modal_starter", "ncpa_source_waveform",
 ]
 
 

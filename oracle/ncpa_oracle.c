@@ -673,7 +673,7 @@ void orc_bb_transfer(int nfreq, const int *mode_off, const double *re_k, const d
 void orc_bb_pulse(int nfreq, const double *f_vec, const double *s_re, const double *s_im,
                   const double *h_re, const double *h_im, double t0, int nfft, double *out) {
     const double PI = ORC_PI;
-    double df = f_vec[1] - f_vec[0];
+    double df = f_vec[2] - f_vec[1]; /* f_step, ModalBroadbandPropagator.cpp:65 */
     double complex *arg = (double complex *)malloc(sizeof(double complex) * (size_t)nfreq);
     for (int i = 0; i < nfreq; i++) {
         double complex tph = cexp(-I * 2.0 * PI * f_vec[i] * t0);
