@@ -1481,7 +1481,9 @@ __global__ void k_bb_transfer(int nfreq, const int* __restrict__ off, const doub
     const int smooth = (int)floor(0.1 * nfreq);
     const int begin = nfreq - smooth, end = nfreq - 1;
     if (smooth > 0 && f >= begin) {
-        const double hh = 0.5 * (cos(kPi * (f - begin) / (end - begin)) + 1.0);
+        // one-bin window (end == begin): the limit value 1 instead of the
+        // reference's 0/0 (BroadbandPropagator.cpp:654-662)
+        const double hh = end == begin ? 1.0 : 0.5 * (cos(kPi * (f - begin) / (end - begin)) + 1.0);
         hr *= hh;
         hi *= hh;
     }

@@ -633,8 +633,12 @@ void orc_tl2d(int M, const double *kr, const double *ki, const double *vs_src, c
 /* ------------------------------------------------------------------------ */
 /* ModBB synthesis                                                            */
 /* ------------------------------------------------------------------------ */
+/* BroadbandPropagator::half_hann (BroadbandPropagator.cpp:654-662).  With a
+ * one-bin window (end == begin, 10 <= nfreq < 20) the reference divides 0 by
+ * 0 and its waveforms come out NaN; here that bin keeps the limit value 1. */
 static double half_hann(int begin, int end, int i) {
     if (i < begin) return 1.0;
+    if (end == begin) return i == begin ? 1.0 : 0.0;
     if (begin <= i && i <= end) return 0.5 * (cos(ORC_PI * (i - begin) / (end - begin)) + 1.0);
     return 0.0;
 }

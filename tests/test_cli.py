@@ -221,11 +221,11 @@ def test_modess_atm_profile(modess_single, analytic_profile):
                          "#% 6, P, Pa", "#% 7, C0, m/s", "#% 8, CEFF, m/s"]
     a = np.loadtxt(d / "run.atm_profile.nm", comments="#")
     prof = O.read_profile(analytic_profile)
-    assert a.shape[1] == 9
+    assert a.shape[1] == 8  # Z U V T RHO P C0 CEFF
     assert np.allclose(a[:, 0], np.asarray(prof.z) * 1000.0, rtol=1e-6)
-    c0 = np.sqrt(1.4 * a[:, 6] / a[:, 5])
-    assert np.allclose(a[:, 7], c0, rtol=2e-6)
-    assert np.allclose(a[:, 8], a[:, 7] + a[:, 1], rtol=2e-6, atol=1e-5)
+    c0 = np.sqrt(1.4 * a[:, 5] / a[:, 4])
+    assert np.allclose(a[:, 6], c0, rtol=2e-6)
+    assert np.allclose(a[:, 7], a[:, 6] + a[:, 1], rtol=2e-6, atol=1e-5)  # azimuth 90: c_eff = c0 + u
 
 
 @pytest.mark.gpu
@@ -253,7 +253,8 @@ def test_modess_multiprop(binaries, analytic_profile, tmp_path):
 @pytest.fixture(scope="module")
 def modbb_dispersion(binaries, analytic_profile, tmp_path_factory):
     d = tmp_path_factory.mktemp("modbb")
-    args = ["--dispersion", "--dispersion_file", "disp.dat", "--atmosfile", analytic_profile, "--azimuth", "90",
+    args = ["--dispersion", "--method", "modess", "--dispersion_file", "disp.dat", "--atmosfile", analytic_profile,
+            "--azimuth", "90",
             "--f_min", "0.01", "--f_step", "0.005", "--f_max", "0.085", "--Nz_grid", str(NZ)]
     (d / "disp.dat").write_text("stale line that --dispersion truncates\n")
     run(binaries, "ModBB", args, d, check_rc=0)
