@@ -151,6 +151,21 @@ ncpa_status ncpa_tl_2d_heights(const ncpa_modes *modes, int problem, int *n_heig
 ncpa_status ncpa_tl_2d(ncpa_ctx *ctx, const ncpa_modes *modes, int problem, const ncpa_tl_params *tp,
                        double *z_out, double *re, double *im);
 
+/* Modal sum at many receivers (ModeSolver::getTLoss2D's contraction,
+ * ModeSolver.cpp:492-565, at arbitrary receiver heights): re/im are
+ * [n_rcv x n_ranges], receiver j at grid point ceil(rcv_height_m[j] / dz),
+ * ranges (i+1)*dr_m, with the 1000 * 4 pi scaling of the 1-D TL.  Needs
+ * want_vectors.  NULL re and im keep the result in HBM.
+ *   NCPA_SUM_FP64        FP64 sum on the CUDA cores (at most 1024 receivers)
+ *   NCPA_SUM_TC_BF16X3   tcgen05 tensor cores: 3-term split-BF16 products with
+ *                        FP32 accumulation; phases k r reduced mod 2 pi in
+ *                        FP64 per 128-range tile (relative error ~1e-5 of
+ *                        the modal terms' magnitude) */
+enum { NCPA_SUM_FP64 = 0, NCPA_SUM_TC_BF16X3 = 1 };
+ncpa_status ncpa_tl_multi(ncpa_ctx *ctx, const ncpa_modes *modes, int problem, int n_rcv,
+                          const double *rcv_height_m, const ncpa_tl_params *tp, int method, double *re,
+                          double *im);
+
 /* Modal starter of one problem (ESSModeSolver::getModalStarter,
  * ESSModeSolver.cpp:670-723; needs want_vectors).  Call with NULL outputs to
  * get the number of heights in *n_out. */

@@ -10,6 +10,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <cuda/std/complex>
+
 #include "kernels.hpp"
 
 namespace ncpa {
@@ -133,6 +135,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
+// Bounded wait for copies this block issued itself, used on the way out after
+// another wait gave up: one second of wall time whatever the error word says.
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t* bar, uint32_t parity) {
+    const uint64_t t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > 1000000000ull) return false;
+    return true;
+}
+
 // ---------------------------------------------------------------------------
 // Division-free Sturm sweep.  Matrix S = h^2 A: diagonal s_i, unit
 // off-diagonal.  p_{-2}=0, p_{-1}=1, p_i = (s_i - x) p_{i-1} - p_{i-2};
@@ -230,5 +241,13 @@ struct SturmState {
         p1 = q;
     }
 };
+
+// principal square root of x + i y
+__device__ __forceinline__ cuda::std::complex<double> csqrt_principal(double x, double y) {
+    double m = hypot(x, y);
+    double t = sqrt(0.5 * (m + fabs(x)));
+    if (x >= 0.0) return cuda::std::complex<double>(t, y / (2.0 * t));
+    return cuda::std::complex<double>(fabs(y) / (2.0 * t), copysign(t, y));
+}
 
 }  // namespace ncpa

@@ -861,14 +861,6 @@ __device__ __forceinline__ void evr_issue(EvRing& r, unsigned k, int c, const do
     if (gp) tma_load_1d(r.g + slot * kEvC, gp + (size_t)c * kEvC, kEvC * 8, &r.bars[slot]);
 }
 
-__device__ __forceinline__ cuda::std::complex<double> csqrt_principal(double x, double y) {
-    // principal square root of x + i y
-    double m = hypot(x, y);
-    double t = sqrt(0.5 * (m + fabs(x)));
-    if (x >= 0.0) return cuda::std::complex<double>(t, y / (2.0 * t));
-    return cuda::std::complex<double>(fabs(y) / (2.0 * t), copysign(t, y));
-}
-
 // forward-pass state of one eigenvalue
 struct FwdState {
     double pm2, pm1;     // p_{i-2}, p_{i-1}
@@ -1357,8 +1349,8 @@ int launch_tl1d(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* 
 // b_m = v_m(z_s) e^{i k r}/sqrt(k); one CTA per range, threads over heights.
 __global__ void __launch_bounds__(256) k_tl2d(int M, const double* __restrict__ kr, const double* __restrict__ ki,
                                               const double* __restrict__ vs_src, const double* __restrict__ vz,
-                                              int nzo, int nr, double dr, int lossless, double* __restrict__ re,
-                                              double* __restrict__ im) {
+                                              int nzo, int nr, double dr, int lossless, long long sr,
+                                              long long sj, double* __restrict__ re, double* __restrict__ im) {
     const int ir = blockIdx.x;
     const double r = (ir + 1) * dr;
     __shared__ double br[kTlTile], bi[kTlTile];
@@ -1399,7 +1391,7 @@ __global__ void __launch_bounds__(256) k_tl2d(int M, const double* __restrict__ 
     for (int u = 0; u < 4; ++u) {
         const int j = threadIdx.x + u * blockDim.x;
         if (j < nzo) {
-            const size_t o = (size_t)ir * nzo + j;
+            const size_t o = (size_t)ir * sr + (size_t)j * sj;
             re[o] = fr * accr[u] - fi * acci[u];
             im[o] = fr * acci[u] + fi * accr[u];
         }
@@ -1409,7 +1401,14 @@ __global__ void __launch_bounds__(256) k_tl2d(int M, const double* __restrict__ 
 int launch_tl2d(cudaStream_t st, int M, const double* kr, const double* ki, const double* vs_src,
                 const double* vz, int nzo, int nr, double dr, int lossless, double* re, double* im) {
     if (nzo > 1024) return -1;  // four heights per thread
-    k_tl2d<<<nr, 256, 0, st>>>(M, kr, ki, vs_src, vz, nzo, nr, dr, lossless, re, im);
+    k_tl2d<<<nr, 256, 0, st>>>(M, kr, ki, vs_src, vz, nzo, nr, dr, lossless, nzo, 1, re, im);
+    return 1;
+}
+
+int launch_tl2d_rcv_major(cudaStream_t st, int M, const double* kr, const double* ki, const double* vs_src,
+                          const double* vz, int n_rcv, int nr, double dr, int lossless, double* re, double* im) {
+    if (n_rcv > 1024) return -1;
+    k_tl2d<<<nr, 256, 0, st>>>(M, kr, ki, vs_src, vz, n_rcv, nr, dr, lossless, 1, nr, re, im);
     return 1;
 }
 

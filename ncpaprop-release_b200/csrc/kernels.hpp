@@ -114,6 +114,9 @@ int launch_tl1d(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* 
                 double* incoh);
 int launch_tl2d(cudaStream_t st, int M, const double* kr, const double* ki, const double* vs_src,
                 const double* vz, int nzo, int nr, double dr, int lossless, double* re, double* im);
+// same sum with [n_rcv x nr] output (receiver-major)
+int launch_tl2d_rcv_major(cudaStream_t st, int M, const double* kr, const double* ki, const double* vs_src,
+                          const double* vz, int n_rcv, int nr, double dr, int lossless, double* re, double* im);
 // broadband synthesis
 int launch_twiddle(cudaStream_t st, int nfft, double* tw);
 // fac: scratch of 4 doubles per mode
@@ -131,5 +134,18 @@ int launch_bb_pulse(cudaStream_t st, int nfreq, const double* f, const double* s
                     const double* t0, int nfft, const double* tw, double* out);
 int launch_src_dft(cudaStream_t st, int n, const double* x, double dt, int nfft, int nfreq, const double* tw,
                    double* s);
+
+// K5 modal sum on the tensor cores (modal_sum.cu)
+struct MsPlan {
+    int groups, n_chunks, M_pad, n_tiles, chunks_per_split, n_splits;
+    size_t a_img_bytes, q_bytes, tab_bytes, raw_bytes;
+};
+MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms);
+int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const double* vfull, double* vz);
+int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int n_rcv, int M, const double* kr, const double* ki,
+                      const double* vs, const double* vz, double dr, int lossless, void* a_img, void* q, void* tab);
+int launch_ms_tc(cudaStream_t st, const MsPlan& p, int n_ranges, const void* a_img, const void* q, const void* tab,
+                 float* raw, unsigned* err);
+int launch_ms_finish(cudaStream_t st, int n_rcv, int n_ranges, double dr, const float* raw, double* re, double* im);
 
 }  // namespace ncpa

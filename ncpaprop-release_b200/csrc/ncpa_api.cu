@@ -112,6 +112,7 @@ struct ncpa_ctx {
     DevBuf ck1, ck2, cke;          // eigenvector checkpoint scratch
     std::map<int, DevBuf> twiddle; // per nfft
     DevBuf bb_out;                 // waveforms kept in HBM (NULL host buffer)
+    DevBuf ms_img, ms_q, ms_tab, ms_raw, ms_vz, ms_idx, ms_re, ms_im;  // modal-sum scratch (grow-only)
     DevBuf d_stats;                // device counters (Sturm sequences)
     bool timing = false;           // NCPA_TIMING=1: per-phase times on stderr
     bool stats = false;            // ncpa_ctx_set_timing: accumulate per phase
@@ -388,6 +389,10 @@ ncpa_status ncpa_ctx_destroy(ncpa_ctx* ctx) {
     ctx->ck2.release();
     ctx->cke.release();
     ctx->d_err.release();
+    for (DevBuf* b : {&ctx->ms_img, &ctx->ms_q, &ctx->ms_tab, &ctx->ms_raw, &ctx->ms_vz, &ctx->ms_idx, &ctx->ms_re,
+                      &ctx->ms_im})
+        b->release();  // stream-ordered frees need the stream alive
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NCPA_OK;
@@ -1012,6 +1017,77 @@ ncpa_status ncpa_tl_2d(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const nc
         CK(cudaMemcpyAsync(re, dre.p, n * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(im, dim.p, n * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n_rcv, const double* rcv_height_m,
+                          const ncpa_tl_params* tp, int method, double* re, double* im) {
+    if (!ctx || !m || !tp || !rcv_height_m || n_rcv < 1 || problem < 0 || problem >= m->P) return NCPA_EINVAL;
+    if ((re == nullptr) != (im == nullptr)) return NCPA_EINVAL;
+    if (method != NCPA_SUM_FP64 && method != NCPA_SUM_TC_BF16X3) return NCPA_EINVAL;
+    if (!m->prm.want_vectors) return fail(ctx, NCPA_EINVAL, "the modal sum at receivers needs want_vectors");
+    return guarded(ctx, [&]() -> ncpa_status {
+        if (tp->n_ranges < 1 || !(tp->dr_m > 0)) throw ApiError(NCPA_EINVAL, "bad range grid");
+        if (method == NCPA_SUM_FP64 && n_rcv > 1024) throw ApiError(NCPA_EINVAL, "FP64 sum: at most 1024 receivers");
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        PhaseTimer tm(ctx);
+        tm.mark("start");
+        const ProblemInfo& pi = m->info[problem];
+        const int M = pi.M, nr = tp->n_ranges;
+        // receiver grid points: ceil(z / dz) as ModeSolver.cpp:301 does
+        std::vector<int> idx(n_rcv);
+        for (int j = 0; j < n_rcv; ++j) {
+            const int k = (int)std::ceil(rcv_height_m[j] / m->dz);
+            if (k < 0 || k >= m->nz) throw ApiError(NCPA_EINVAL, "receiver height outside the grid");
+            idx[j] = k;
+        }
+        const size_t nout = (size_t)n_rcv * nr;
+        ctx->ms_re.alloc(nout * 8, st);
+        ctx->ms_im.alloc(nout * 8, st);
+        if (M == 0) {
+            CK(cudaMemsetAsync(ctx->ms_re.p, 0, nout * 8, st));
+            CK(cudaMemsetAsync(ctx->ms_im.p, 0, nout * 8, st));
+        } else {
+            ctx->ms_idx.alloc((size_t)n_rcv * 4, st);
+            CK(cudaMemcpyAsync(ctx->ms_idx.p, idx.data(), (size_t)n_rcv * 4, cudaMemcpyHostToDevice, st));
+            ctx->ms_vz.alloc((size_t)n_rcv * M * 8, st);
+            check_launch(ctx, ncpa::launch_ms_gather(st, n_rcv, M, ctx->ms_idx.as<int>(),
+                                                     m->d_vfull.as<double>() + m->vfull_off[problem],
+                                                     ctx->ms_vz.as<double>()));
+            const double* kr = m->d_kr.as<double>() + pi.off;
+            const double* ki = m->d_ki.as<double>() + pi.off;
+            const double* vs = m->d_vs.as<double>() + pi.off;
+            if (method == NCPA_SUM_FP64) {
+                tm.mark("ms-prep");
+                check_launch(ctx, ncpa::launch_tl2d_rcv_major(st, M, kr, ki, vs, ctx->ms_vz.as<double>(), n_rcv, nr,
+                                                              tp->dr_m, tp->lossless, ctx->ms_re.as<double>(),
+                                                              ctx->ms_im.as<double>()));
+                tm.mark("ms-fp64");
+            } else {
+                const ncpa::MsPlan pl = ncpa::ms_plan(n_rcv, M, nr, ctx->num_sms);
+                ctx->ms_img.alloc(pl.a_img_bytes, st);
+                ctx->ms_q.alloc(pl.q_bytes, st);
+                ctx->ms_tab.alloc(pl.tab_bytes, st);
+                ctx->ms_raw.alloc(pl.raw_bytes, st);
+                check_launch(ctx, ncpa::launch_ms_prepare(st, pl, n_rcv, M, kr, ki, vs, ctx->ms_vz.as<double>(),
+                                                          tp->dr_m, tp->lossless, ctx->ms_img.p, ctx->ms_q.p,
+                                                          ctx->ms_tab.p));
+                tm.mark("ms-prep");
+                check_launch(ctx, ncpa::launch_ms_tc(st, pl, nr, ctx->ms_img.p, ctx->ms_q.p, ctx->ms_tab.p,
+                                                     ctx->ms_raw.as<float>(), ctx->d_err.as<unsigned>()));
+                tm.mark("ms-tc");
+                check_launch(ctx, ncpa::launch_ms_finish(st, n_rcv, nr, tp->dr_m, ctx->ms_raw.as<float>(),
+                                                         ctx->ms_re.as<double>(), ctx->ms_im.as<double>()));
+                tm.mark("ms-finish");
+            }
+        }
+        if (re) {
+            CK(cudaMemcpyAsync(re, ctx->ms_re.p, nout * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(im, ctx->ms_im.p, nout * 8, cudaMemcpyDeviceToHost, st));
+        }
+        check_device_status(ctx);
         return NCPA_OK;
     });
 }

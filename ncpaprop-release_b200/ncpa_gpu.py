@@ -29,7 +29,7 @@ EXPORTED = [
     "ncpa_kernel_launches", "ncpa_ctx_stream", "ncpa_ctx_set_timing", "ncpa_ctx_phase_stats",
     "ncpa_ctx_reset_stats", "ncpa_ctx_sturm_sequences", "ncpa_probe_fp64_peak", "ncpa_source_spectrum_builtin",
     "ncpa_eigvec_static", "ncpa_profile_set_attn", "ncpa_profile_load_attn", "ncpa_profile_knots", "ncpa_profile_z0",
-    "ncpa_modal_starter", "ncpa_source_waveform",
+    "ncpa_modal_starter", "ncpa_source_waveform", "ncpa_tl_multi",
 ]
 
 
@@ -103,6 +103,7 @@ def lib():
         L.ncpa_tl_1d.argtypes = [_vp, _vp, ctypes.POINTER(_TlParams), _dp, _dp, _dp]
         L.ncpa_tl_2d_heights.argtypes = [_vp, _c_int, _ip]
         L.ncpa_tl_2d.argtypes = [_vp, _vp, _c_int, ctypes.POINTER(_TlParams), _dp, _dp, _dp]
+        L.ncpa_tl_multi.argtypes = [_vp, _vp, _c_int, _c_int, _dp, ctypes.POINTER(_TlParams), _c_int, _dp, _dp]
         L.ncpa_bb_synthesize.argtypes = [_vp, ctypes.POINTER(_DispDesc), ctypes.POINTER(_BbParams), _dp]
         L.ncpa_bb_synthesize_modes.argtypes = [_vp, _vp, _c_int, ctypes.POINTER(_BbParams), _dp]
         L.ncpa_source_spectrum_waveform.argtypes = [_vp, _dp, _c_int, _c_double, _c_int, _c_int, _dp, _dp]
@@ -342,6 +343,18 @@ class Modes:
         self.ctx.check(lib().ncpa_tl_2d(self.ctx.h, self.h, p, ctypes.byref(tp), _p(z), _p(re), _p(im)),
                        "ncpa_tl_2d")
         return z, re, im
+
+    SUM_FP64, SUM_TC_BF16X3 = 0, 1
+
+    def tl_multi(self, p, heights_m, n_ranges, dr_m, method=1, lossless=False, to_host=True):
+        """Modal sum at many receivers: complex P [n_rcv x n_ranges]."""
+        h = _f64(heights_m)
+        tp = _TlParams(int(n_ranges), float(dr_m), int(lossless))
+        re = np.empty((len(h), n_ranges)) if to_host else None
+        im = np.empty((len(h), n_ranges)) if to_host else None
+        self.ctx.check(lib().ncpa_tl_multi(self.ctx.h, self.h, p, len(h), _p(h), ctypes.byref(tp), int(method),
+                                           _p(re), _p(im)), "ncpa_tl_multi")
+        return (re + 1j * im) if to_host else None
 
     def bb_synthesize(self, ranges_m, max_celerity, nfft, src_re, src_im, zero_attn=False, to_host=True):
         rng, sre, sim = _f64(ranges_m), _f64(src_re), _f64(src_im)
