@@ -137,7 +137,8 @@ int launch_src_dft(cudaStream_t st, int n, const double* x, double dt, int nfft,
 
 // K5 modal sum on the tensor cores (modal_sum.cu)
 struct MsPlan {
-    int groups, n_chunks, M_pad, n_tiles, chunks_per_split, n_splits;
+    int groups, n_chunks, M_pad, n_tiles, n_ctas, n_parts;
+    long long n_units;  // (receiver group, range tile, mode chunk) units
     size_t a_img_bytes, q_bytes, tab_bytes, raw_bytes;
 };
 MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms);
@@ -146,6 +147,7 @@ int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int n_rcv, int M, const 
                       const double* vs, const double* vz, double dr, int lossless, void* a_img, void* q, void* tab);
 int launch_ms_tc(cudaStream_t st, const MsPlan& p, int n_ranges, const void* a_img, const void* q, const void* tab,
                  float* raw, unsigned* err);
-int launch_ms_finish(cudaStream_t st, int n_rcv, int n_ranges, double dr, const float* raw, double* re, double* im);
+int launch_ms_finish(cudaStream_t st, const MsPlan& p, int n_rcv, int n_ranges, double dr, const float* raw,
+                     double* re, double* im);
 
 }  // namespace ncpa

@@ -13,12 +13,16 @@
 // Each operand is split into bf16 hi + lo parts and D accumulates
 //   A_hi B_hi + A_hi B_lo + A_lo B_hi   in FP32 (3-term split-BF16, ~2^-16).
 //
-// One CTA = one tile of 128 ranges x one K-range of modes (split-K when the
-// tiles alone cannot fill the SMs).  Warp 0: TMEM allocation, bulk-TMA of
-// the prepared A' chunks, tcgen05.mma issue.  Warps 1-4: generate B' in
-// shared memory from FP64-reduced tile phases (e^{i k r_n0}, computed in
-// FP64 with the phase reduced mod 2 pi) times short FP32 recurrences
-// e^{i k 8 dr}, then read the accumulator out of TMEM.
+// Persistent kernel: the (receiver group, 128-range tile, 32-mode chunk)
+// units are split evenly over one CTA per SM; a CTA accumulates the chunks of
+// one (group, tile) in TMEM (two accumulators, so a finished tile's epilogue
+// overlaps the next tile's MMAs) and stores its partial sum of the tile in
+// its own slot; the finishing kernel adds the slots of the CTAs that shared
+// the tile.  Warp 0: TMEM allocation, bulk-TMA of the prepared A' chunk
+// together with the chunk's per-mode factor rows and tile phases, and
+// tcgen05.mma issue.  Warps 1-8: generate B' in shared memory from
+// FP64-reduced tile phases e^{i k r_n0} (phase reduced mod 2 pi in FP64)
+// times per-mode FP32 factors e^{i k o dr}, and read the accumulators out.
 //
 // Shared-memory operand layout (no swizzle, K-major core matrices): element
 // (row, k) of a 128-row x 64-k bf16 tile sits at byte
@@ -26,6 +30,8 @@
 // i.e. leading-byte offset 128 (next 8 k) and stride-byte offset 1024 (next 8
 // rows); one MMA (K = 16) starts 256 bytes further per K-step.
 #include <cuda_bf16.h>
+
+#include <algorithm>
 
 #include "device_common.cuh"
 
@@ -40,10 +46,19 @@ constexpr int kMsModes = 32;        // modes per K-chunk
 constexpr int kMsKC = 2 * kMsModes; // K per chunk
 constexpr int kMsStages = 3;
 constexpr int kMsOpBytes = kMsRows * kMsKC * 2;  // one operand part: 16 KB
-constexpr int kMsStageBytes = 4 * kMsOpBytes;    // A hi, A lo, B hi, B lo
+constexpr int kMsTabW = 34;         // per-mode row: e^{ik o dr} for the 32 thread offsets, e^{ik 8 dr}, pad
+constexpr int kMsTabBytes = kMsModes * kMsTabW * 8;  // factor rows of one chunk: 8704 B
+constexpr int kMsQBytes = kMsModes * 8;              // tile phases of one chunk
+constexpr int kMsTxBytes = 2 * kMsOpBytes + kMsTabBytes + kMsQBytes;
+// stage: A hi, A lo, B hi, B lo, factor rows, tile phases (1 KB aligned)
+constexpr int kMsStageBytes = (4 * kMsOpBytes + kMsTabBytes + kMsQBytes + 1023) / 1024 * 1024;
 constexpr int kMsSmem = kMsStages * kMsStageBytes + 1024;
-constexpr int kMsThreads = 160;
-constexpr int kMsTabW = 10;         // per-mode table: 8 x e^{ik i dr}, e^{ik 64dr}, e^{ik 8dr}
+constexpr int kMsGenWarps = 8;      // B' generators / epilogue
+constexpr int kMsGenThreads = 32 * kMsGenWarps;
+constexpr int kMsThreads = 32 + kMsGenThreads;
+constexpr int kMsAcc = 2;           // TMEM accumulators (kMsNT columns each)
+static_assert(kMsSmem <= 232448, "shared memory per block");
+static_assert(kMsTabBytes % 16 == 0 && kMsQBytes % 16 == 0, "bulk copies move 16-byte multiples");
 static_assert(kMsNT == kMsRows, "square operand tiles share one layout");
 
 __device__ __forceinline__ uint32_t core_off(int row, int k) {
@@ -104,26 +119,26 @@ __device__ __forceinline__ void sts128(uint32_t addr, uint32_t a, uint32_t b, ui
 // ---------------------------------------------------------------------------
 // preparation
 // ---------------------------------------------------------------------------
-// per-mode FP32 factors from FP64: e^{i k i dr} (i < 8), e^{i k 64 dr},
-// e^{i k 8 dr}; zero for the padding modes m >= M
+// per-mode FP32 factors from FP64: entry 8 * quarter + i holds
+// e^{i k (i + 32 quarter) dr} (the start offset of generator thread (i,
+// quarter) inside a tile), entry 32 holds the step e^{i k 8 dr}; zero for the
+// padding modes m >= M and the pad entry
 __global__ void k_ms_tables(int M, int M_pad, const double* __restrict__ kr, const double* __restrict__ ki,
                             double dr, int lossless, float2* __restrict__ tab) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= M_pad) return;
-    float2* t = tab + (size_t)m * kMsTabW;
-    if (m >= M) {
-        for (int i = 0; i < kMsTabW; ++i) t[i] = make_float2(0.f, 0.f);
-        return;
-    }
-    const double a = kr[m], b = lossless ? 0.0 : ki[m];
-    const double steps[kMsTabW] = {0, 1, 2, 3, 4, 5, 6, 7, 64, 8};
-    for (int i = 0; i < kMsTabW; ++i) {
-        const double x = steps[i] * dr;
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= M_pad * kMsTabW) return;
+    const int m = id / kMsTabW, e = id % kMsTabW;
+    float2 v = make_float2(0.f, 0.f);
+    if (m < M && e <= 32) {
+        const double a = kr[m], b = lossless ? 0.0 : ki[m];
+        const double off = e < 32 ? (double)((e & 7) + 32 * (e >> 3)) : 8.0;
+        const double x = off * dr;
         double sn, cs;
         sincos(a * x, &sn, &cs);
         const double amp = exp(-b * x);
-        t[i] = make_float2((float)(amp * cs), (float)(amp * sn));
+        v = make_float2((float)(amp * cs), (float)(amp * sn));
     }
+    tab[id] = v;
 }
 
 // tile phases e^{i k_m r_n0}, r_n0 = (tile * 128 + 1) dr: the phase k r is
@@ -185,39 +200,50 @@ __global__ void k_ms_a(int n_rcv, int M, int n_chunks, const double* __restrict_
 // ---------------------------------------------------------------------------
 // the tensor-core kernel
 // ---------------------------------------------------------------------------
+// CTA that owns unit u when U units are split evenly over G CTAs (CTA b owns
+// [floor(U b / G), floor(U (b + 1) / G)))
+__host__ __device__ __forceinline__ int ms_cta_of(long long u, long long U, int G) {
+    return (int)(((u + 1) * G - 1) / U);
+}
+
 struct MsArgs {
     const unsigned char* a_img;  // [groups][n_chunks][hi, lo][16 KB]
     const float2* q;             // [n_tiles][M_pad]
-    const float2* tab;           // [M_pad][10]
-    int M_pad, n_chunks, chunks_per_split, n_splits, n_tiles, n_ranges;
-    float* raw;                  // [groups][128][n_ranges] FP32 sums (zeroed when n_splits > 1)
+    const float2* tab;           // [M_pad][kMsTabW]
+    int M_pad, n_chunks, n_tiles, n_ranges, groups;
+    long long n_units;           // groups * n_tiles * n_chunks
+    float* raw;                  // [n_parts][groups][128][n_ranges] per-CTA partial sums of a tile
     unsigned* err;
 };
 
 __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     extern __shared__ unsigned char ms_dyn[];
-    __shared__ __align__(8) uint64_t full_a[kMsStages], full_b[kMsStages], empty[kMsStages], acc_full;
+    __shared__ __align__(8) uint64_t full_a[kMsStages], full_b[kMsStages], empty[kMsStages];
+    __shared__ __align__(8) uint64_t acc_full[kMsAcc], acc_empty[kMsAcc], drain;
     __shared__ uint32_t tmem_base_sh;
     unsigned char* sm = (unsigned char*)(((uintptr_t)ms_dyn + 1023) & ~(uintptr_t)1023);
     const uint32_t sm_addr = smem_u32(sm);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tile = blockIdx.x / a.n_splits, split = blockIdx.x % a.n_splits;
-    const int group = blockIdx.y;
-    const int c_begin = split * a.chunks_per_split;
-    const int nc = min(a.chunks_per_split, a.n_chunks - c_begin);
+    // this CTA's units [u0, u0 + nc), ordered (group, tile, chunk)
+    const long long u0 = a.n_units * blockIdx.x / gridDim.x;
+    const int nc = (int)(a.n_units * (blockIdx.x + 1) / gridDim.x - u0);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kMsStages; ++s) {
             mbar_init(&full_a[s], 1);
-            mbar_init(&full_b[s], 128);
+            mbar_init(&full_b[s], kMsGenThreads);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(&acc_full, 1);
+        for (int b = 0; b < kMsAcc; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], kMsGenThreads);
+        }
+        mbar_init(&drain, 1);
         fence_mbar_init();
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
-                     "r"(kMsNT)
+                     "r"(kMsAcc * kMsNT)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -228,17 +254,38 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
 
     if (warp == 0) {
         if (lane == 0 && nc > 0) {
-            // producer of A' (bulk TMA) and MMA issuer
-            const unsigned char* src = a.a_img + ((size_t)group * a.n_chunks + c_begin) * 2 * kMsOpBytes;
+            // producer (bulk TMA of the A' chunk, factor rows, tile phases) and MMA issuer
+            auto load_stage = [&](int c, int slot) {
+                const long long u = u0 + c;
+                const long long g = u / ((long long)a.n_tiles * a.n_chunks);
+                const int chunk = (int)(u % a.n_chunks);
+                const int tile = (int)((u / a.n_chunks) % a.n_tiles);
+                unsigned char* dst = sm + slot * kMsStageBytes;
+                mbar_expect_tx(&full_a[slot], kMsTxBytes);
+                tma_load_1d(dst, a.a_img + ((size_t)g * a.n_chunks + chunk) * 2 * kMsOpBytes, 2 * kMsOpBytes,
+                            &full_a[slot]);
+                tma_load_1d(dst + 4 * kMsOpBytes, a.tab + (size_t)chunk * kMsModes * kMsTabW, kMsTabBytes,
+                            &full_a[slot]);
+                tma_load_1d(dst + 4 * kMsOpBytes + kMsTabBytes, a.q + (size_t)tile * a.M_pad + chunk * kMsModes,
+                            kMsQBytes, &full_a[slot]);
+            };
             int issued = 0;
-            for (; issued < min(kMsStages, nc); ++issued) {
-                mbar_expect_tx(&full_a[issued], 2 * kMsOpBytes);
-                tma_load_1d(sm + issued * kMsStageBytes, src + (size_t)issued * 2 * kMsOpBytes, 2 * kMsOpBytes,
-                            &full_a[issued]);
-            }
+            for (; issued < min(kMsStages, nc); ++issued) load_stage(issued, issued);
             bool ok = true;
-            int waited_a = 0;  // chunks whose A' copy is known to have landed
+            int waited_a = 0;  // chunks whose copies are known to have landed
+            int sg = -1;       // segment (one group and tile) counter
             for (int c = 0; c < nc && ok; ++c) {
+                const int chunk = (int)((u0 + c) % a.n_chunks);
+                const bool first = c == 0 || chunk == 0;
+                const bool last = c == nc - 1 || chunk == a.n_chunks - 1;
+                if (first) {
+                    ++sg;
+                    if (sg >= kMsAcc) {  // accumulator sg % 2 read out by the epilogue of segment sg - 2
+                        ok = mbar_wait_bounded(&acc_empty[sg & 1], (uint32_t)(((sg >> 1) - 1) & 1), a.err);
+                        if (!ok) break;
+                        tc_fence_after();
+                    }
+                }
                 const int s = c % kMsStages;
                 const uint32_t ph = (uint32_t)((c / kMsStages) & 1);
                 ok = mbar_wait_bounded(&full_a[s], ph, a.err);
@@ -248,82 +295,109 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                 if (!ok) break;
                 tc_fence_after();
                 const uint32_t st = sm_addr + s * kMsStageBytes;
+                const uint32_t d = tmem + (uint32_t)((sg & 1) * kMsNT);
 #pragma unroll
                 for (int kk = 0; kk < kMsKC / 16; ++kk) {
                     const uint32_t ah = st + kk * 256, al = ah + kMsOpBytes;
                     const uint32_t bh = st + 2 * kMsOpBytes + kk * 256, bl = bh + kMsOpBytes;
-                    umma_bf16(tmem, smem_desc(ah), smem_desc(bh), (c > 0 || kk > 0) ? 1u : 0u);
-                    umma_bf16(tmem, smem_desc(ah), smem_desc(bl), 1u);
-                    umma_bf16(tmem, smem_desc(al), smem_desc(bh), 1u);
+                    umma_bf16(d, smem_desc(ah), smem_desc(bh), (!first || kk > 0) ? 1u : 0u);
+                    umma_bf16(d, smem_desc(ah), smem_desc(bl), 1u);
+                    umma_bf16(d, smem_desc(al), smem_desc(bh), 1u);
                 }
                 umma_commit(&empty[s]);
+                if (last) umma_commit(&acc_full[sg & 1]);
                 // refill the slot of chunk c - 1 once its MMAs are done
                 if (c >= 1 && issued < nc) {
                     const int sp = (c - 1) % kMsStages;
                     ok = mbar_wait_bounded(&empty[sp], (uint32_t)(((c - 1) / kMsStages) & 1), a.err);
                     if (!ok) break;
-                    mbar_expect_tx(&full_a[sp], 2 * kMsOpBytes);
-                    tma_load_1d(sm + sp * kMsStageBytes, src + (size_t)issued * 2 * kMsOpBytes, 2 * kMsOpBytes,
-                                &full_a[sp]);
+                    load_stage(issued, sp);
                     ++issued;
                 }
             }
-            umma_commit(&acc_full);
-            // copies still in flight after an early exit: wait for them
+            if (!ok) {
+                // let the epilogue warps leave: a commit arrives once the
+                // MMAs already issued are complete
+                umma_commit(&acc_full[0]);
+                umma_commit(&acc_full[1]);
+            }
             for (int c = waited_a; c < issued; ++c)
                 mbar_wait_drain(&full_a[c % kMsStages], (uint32_t)((c / kMsStages) & 1));
+            // every MMA complete before the accumulators are released
+            umma_commit(&drain);
+            mbar_wait_drain(&drain, 0u);
         }
     } else {
         // B' generators: thread -> (i = range in its 8-group, q = mode quad,
-        // half = which 64 ranges)
+        // quarter = which 32 ranges of the tile)
         const int t = threadIdx.x - 32;
-        const int i = t & 7, q = (t >> 3) & 7, half = t >> 6;
-        const float2* qrow = a.q + (size_t)tile * a.M_pad;
+        const int i = t & 7, q = (t >> 3) & 7, quarter = t >> 6;
+        const int col_half = (warp - 1) >> 2;  // epilogue: accumulator columns [64 col_half, +64)
         bool ok = true;
+        int sg = -1;
         for (int c = 0; c < nc && ok; ++c) {
+            const long long u = u0 + c;
+            const int chunk = (int)(u % a.n_chunks);
+            const long long gt = u / a.n_chunks;  // group * n_tiles + tile
+            const int tile = (int)(gt % a.n_tiles);
+            const bool first = c == 0 || chunk == 0;
+            const bool last = c == nc - 1 || chunk == a.n_chunks - 1;
+            if (first) ++sg;
             const int s = c % kMsStages;
             if (c >= kMsStages) {
                 ok = mbar_wait_bounded(&empty[s], (uint32_t)(((c / kMsStages) - 1) & 1), a.err);
                 if (!ok) break;
             }
-            const int m0 = (c_begin + c) * kMsModes + 4 * q;
+            // factor rows and tile phases of this chunk arrive with its A' copy
+            ok = mbar_wait_bounded(&full_a[s], (uint32_t)((c / kMsStages) & 1), a.err);
+            if (!ok) break;
+            const unsigned char* stg = sm + s * kMsStageBytes;
+            const float2* tab_s = reinterpret_cast<const float2*>(stg + 4 * kMsOpBytes);
+            const float2* q_s = reinterpret_cast<const float2*>(stg + 4 * kMsOpBytes + kMsTabBytes);
             float2 e[4], w[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const float2* tb = a.tab + (size_t)(m0 + u) * kMsTabW;
-                float2 v = cmulf(qrow[m0 + u], tb[i]);
-                if (half) v = cmulf(v, tb[8]);
-                e[u] = v;
-                w[u] = tb[9];
+            for (int v = 0; v < 4; ++v) {
+                const float2* tb = tab_s + (4 * q + v) * kMsTabW;
+                e[v] = cmulf(q_s[4 * q + v], tb[8 * quarter + i]);
+                w[v] = tb[32];
             }
             const uint32_t bh = sm_addr + s * kMsStageBytes + 2 * kMsOpBytes;
 #pragma unroll
-            for (int st8 = 0; st8 < 8; ++st8) {
-                const int grp = half * 8 + st8;  // 8-range group within the tile
+            for (int st8 = 0; st8 < 4; ++st8) {
+                const int grp = quarter * 4 + st8;  // 8-range group within the tile
                 const uint32_t off = (uint32_t)((grp * (kMsKC / 8) + q) * 128 + i * 16);
                 uint32_t h[4], l[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) split2(e[u], h[u], l[u]);
+                for (int v = 0; v < 4; ++v) split2(e[v], h[v], l[v]);
                 sts128(bh + off, h[0], h[1], h[2], h[3]);
                 sts128(bh + kMsOpBytes + off, l[0], l[1], l[2], l[3]);
+                if (st8 < 3) {
 #pragma unroll
-                for (int u = 0; u < 4; ++u) e[u] = cmulf(e[u], w[u]);
+                    for (int v = 0; v < 4; ++v) e[v] = cmulf(e[v], w[v]);
+                }
             }
             fence_proxy_async();
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full_b[s])) : "memory");
-        }
-        // epilogue: TMEM lanes 32 (warp % 4) .. +31 = rows of D
-        bool acc_ok = nc > 0 && mbar_wait_bounded(&acc_full, 0u, a.err);
-        acc_ok = __all_sync(0xffffffffu, acc_ok);  // tcgen05.ld is warp-collective
-        if (acc_ok) {
+            if (!last) continue;
+            // epilogue of segment sg: TMEM lanes 32 (warp % 4) .. +31 = rows;
+            // the partial sum goes to slot (this CTA - first CTA of the tile)
+            bool acc_ok = mbar_wait_bounded(&acc_full[sg & 1], (uint32_t)((sg >> 1) & 1), a.err);
+            acc_ok = __all_sync(0xffffffffu, acc_ok);  // tcgen05.ld is warp-collective
+            if (!acc_ok) {
+                ok = false;
+                break;
+            }
             tc_fence_after();
             const int row = 32 * (warp & 3) + lane;
-            const int n0 = tile * kMsNT;
-            float* out = a.raw + ((size_t)group * kMsRows + row) * a.n_ranges;
+            const int g = (int)(gt / a.n_tiles);
+            const int part = blockIdx.x - ms_cta_of(gt * a.n_chunks, a.n_units, gridDim.x);
+            const int n0 = tile * kMsNT + 64 * col_half;
+            float* out = a.raw + (((size_t)part * a.groups + g) * kMsRows + row) * a.n_ranges;
 #pragma unroll 1
-            for (int cb = 0; cb < kMsNT / 32; ++cb) {
+            for (int cb = 0; cb < 2; ++cb) {
                 uint32_t v[32];
-                const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(cb * 32);
+                const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) +
+                                       (uint32_t)((sg & 1) * kMsNT + 64 * col_half + cb * 32);
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
                     "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
@@ -335,35 +409,49 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                       "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                const int nb = n0 + cb * 32;
+                if (nb + 32 <= a.n_ranges && (a.n_ranges & 3) == 0) {
+                    float4* o4 = reinterpret_cast<float4*>(out + nb);
 #pragma unroll
-                for (int u = 0; u < 32; ++u) {
-                    const int n = n0 + cb * 32 + u;
-                    if (n < a.n_ranges) {
-                        const float x = __uint_as_float(v[u]);
-                        if (a.n_splits > 1) atomicAdd(out + n, x);
-                        else out[n] = x;
-                    }
+                    for (int x = 0; x < 8; ++x)
+                        o4[x] = make_float4(__uint_as_float(v[4 * x]), __uint_as_float(v[4 * x + 1]),
+                                            __uint_as_float(v[4 * x + 2]), __uint_as_float(v[4 * x + 3]));
+                } else {
+#pragma unroll
+                    for (int x = 0; x < 32; ++x)
+                        if (nb + x < a.n_ranges) out[nb + x] = __uint_as_float(v[x]);
                 }
             }
+            tc_fence_before();
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[sg & 1])) : "memory");
         }
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kMsNT) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kMsAcc * kMsNT)
+                     : "memory");
     }
 }
 
-// P = C(r_n) (D_re + i D_im) -> [n_rcv x n_ranges] FP64
-__global__ void k_ms_finish(int n_rcv, int n_ranges, double dr, const float* __restrict__ raw,
-                            double* __restrict__ re, double* __restrict__ im) {
+// P = C(r_n) (D_re + i D_im) -> [n_rcv x n_ranges] FP64, adding the partial
+// slots of the CTAs that shared the tile
+__global__ void k_ms_finish(int n_rcv, int n_ranges, double dr, int groups, int n_tiles, int n_chunks,
+                            long long n_units, int n_ctas, const float* __restrict__ raw, double* __restrict__ re,
+                            double* __restrict__ im) {
     const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= (long long)n_rcv * n_ranges) return;
     const int n = (int)(id % n_ranges), j = (int)(id / n_ranges);
     const int g = j / kMsRcv, jr = j % kMsRcv;
-    const float* base = raw + (size_t)g * kMsRows * n_ranges;
-    const double dre = base[(size_t)jr * n_ranges + n], dim = base[(size_t)(jr + kMsRcv) * n_ranges + n];
+    const long long u_first = ((long long)g * n_tiles + n / kMsNT) * n_chunks;
+    const int parts = ms_cta_of(u_first + n_chunks - 1, n_units, n_ctas) - ms_cta_of(u_first, n_units, n_ctas) + 1;
+    double dre = 0.0, dim = 0.0;
+    for (int p = 0; p < parts; ++p) {
+        const float* base = raw + ((size_t)p * groups + g) * kMsRows * n_ranges;
+        dre += base[(size_t)jr * n_ranges + n];
+        dim += base[(size_t)(jr + kMsRcv) * n_ranges + n];
+    }
     const double r = (n + 1) * dr;
     const double c0 = 1000.0 * 4 * kPi / sqrt(8.0 * kPi) / sqrt(r);
     const double fr = c0 * sin(kPi * 0.25), fi = c0 * cos(kPi * 0.25);
@@ -389,17 +477,19 @@ MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms) {
     p.n_chunks = (M + kMsModes - 1) / kMsModes;
     p.M_pad = p.n_chunks * kMsModes;
     p.n_tiles = (n_ranges + kMsNT - 1) / kMsNT;
-    // split K until the CTAs cover the SMs (about two per SM), keeping at
-    // least four chunks per split so the pipeline fills
-    const int units = p.n_tiles * p.groups;
-    int splits = 1;
-    while (units * splits < 2 * num_sms && p.n_chunks / (splits * 2) >= 4) splits *= 2;
-    p.chunks_per_split = (p.n_chunks + splits - 1) / splits;
-    p.n_splits = (p.n_chunks + p.chunks_per_split - 1) / p.chunks_per_split;
+    p.n_units = (long long)p.groups * p.n_tiles * p.n_chunks;
+    p.n_ctas = (int)std::min<long long>(num_sms, p.n_units);
+    // CTAs sharing one (group, tile): each writes its own partial slot
+    p.n_parts = 1;
+    for (long long gt = 0; p.n_units > 0 && gt < (long long)p.groups * p.n_tiles; ++gt) {
+        const long long uf = gt * p.n_chunks;
+        const int parts = ms_cta_of(uf + p.n_chunks - 1, p.n_units, p.n_ctas) - ms_cta_of(uf, p.n_units, p.n_ctas) + 1;
+        p.n_parts = std::max(p.n_parts, parts);
+    }
     p.a_img_bytes = (size_t)p.groups * p.n_chunks * 2 * kMsOpBytes;
     p.q_bytes = (size_t)p.n_tiles * p.M_pad * sizeof(float2);
     p.tab_bytes = (size_t)p.M_pad * kMsTabW * sizeof(float2);
-    p.raw_bytes = (size_t)p.groups * kMsRows * n_ranges * sizeof(float);
+    p.raw_bytes = (size_t)p.n_parts * p.groups * kMsRows * n_ranges * sizeof(float);
     return p;
 }
 
@@ -412,7 +502,7 @@ int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const do
 
 int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int n_rcv, int M, const double* kr, const double* ki,
                       const double* vs, const double* vz, double dr, int lossless, void* a_img, void* q, void* tab) {
-    k_ms_tables<<<(p.M_pad + 127) / 128, 128, 0, st>>>(M, p.M_pad, kr, ki, dr, lossless, (float2*)tab);
+    k_ms_tables<<<(p.M_pad * kMsTabW + 255) / 256, 256, 0, st>>>(M, p.M_pad, kr, ki, dr, lossless, (float2*)tab);
     const long long nq = (long long)p.n_tiles * p.M_pad;
     k_ms_phase<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(M, p.M_pad, p.n_tiles, kr, ki, dr, lossless,
                                                               (float2*)q);
@@ -424,29 +514,30 @@ int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int n_rcv, int M, const 
 
 int launch_ms_tc(cudaStream_t st, const MsPlan& p, int n_ranges, const void* a_img, const void* q, const void* tab,
                  float* raw, unsigned* err) {
+    if (p.n_units <= 0) return 0;
     if (cudaFuncSetAttribute(k_ms_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kMsSmem) != cudaSuccess)
         return -1;
-    if (p.n_splits > 1) cudaMemsetAsync(raw, 0, p.raw_bytes, st);
     MsArgs a;
     a.a_img = (const unsigned char*)a_img;
     a.q = (const float2*)q;
     a.tab = (const float2*)tab;
     a.M_pad = p.M_pad;
     a.n_chunks = p.n_chunks;
-    a.chunks_per_split = p.chunks_per_split;
-    a.n_splits = p.n_splits;
     a.n_tiles = p.n_tiles;
     a.n_ranges = n_ranges;
+    a.groups = p.groups;
+    a.n_units = p.n_units;
     a.raw = raw;
     a.err = err;
-    dim3 grid(p.n_tiles * p.n_splits, p.groups);
-    k_ms_tc<<<grid, kMsThreads, kMsSmem, st>>>(a);
+    k_ms_tc<<<p.n_ctas, kMsThreads, kMsSmem, st>>>(a);
     return 1;
 }
 
-int launch_ms_finish(cudaStream_t st, int n_rcv, int n_ranges, double dr, const float* raw, double* re, double* im) {
+int launch_ms_finish(cudaStream_t st, const MsPlan& p, int n_rcv, int n_ranges, double dr, const float* raw,
+                     double* re, double* im) {
     const long long n = (long long)n_rcv * n_ranges;
-    k_ms_finish<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n_rcv, n_ranges, dr, raw, re, im);
+    k_ms_finish<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n_rcv, n_ranges, dr, p.groups, p.n_tiles, p.n_chunks,
+                                                              p.n_units, p.n_ctas, raw, re, im);
     return 1;
 }
 

@@ -1078,7 +1078,7 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
                 check_launch(ctx, ncpa::launch_ms_tc(st, pl, nr, ctx->ms_img.p, ctx->ms_q.p, ctx->ms_tab.p,
                                                      ctx->ms_raw.as<float>(), ctx->d_err.as<unsigned>()));
                 tm.mark("ms-tc");
-                check_launch(ctx, ncpa::launch_ms_finish(st, n_rcv, nr, tp->dr_m, ctx->ms_raw.as<float>(),
+                check_launch(ctx, ncpa::launch_ms_finish(st, pl, n_rcv, nr, tp->dr_m, ctx->ms_raw.as<float>(),
                                                          ctx->ms_re.as<double>(), ctx->ms_im.as<double>()));
                 tm.mark("ms-finish");
             }
