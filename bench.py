@@ -7,6 +7,10 @@ frequency on 1000 ranges to 1000 km (ModBB --dispersion writes it per
 frequency), then pulse synthesis at 200-300 km every 10 km from a
 Gaussian-windowed 0.1 Hz Ricker waveform sampled at 1 Hz.
 
+The line also carries "modal_sum": the tensor-core modal sum at 64
+receivers x 20000 ranges of a 2 Hz, Nz = 100000 solve (timed separately,
+not part of the step), with its roofline against the measured bf16 peak.
+
   value  freq-solves/s with the profile resident in HBM and results left in
          HBM (device-timed with CUDA events on the library's stream; L2
          flushed between steps by writing a 256 MiB buffer)
@@ -252,6 +256,7 @@ def run_ours(args):
     if world > 1:
         ms_dev, ms_e2e = reduce_max([ms_dev, ms_e2e])
     fp64_peak = ctx.fp64_peak_tflops() if rank == 0 else None
+    ms_leg = modal_sum_leg(ctx, stream, _bf16_peak()) if rank == 0 and not args.no_modal_sum else None
     if rank == 0:
         solves = NFREQ * args.steps * world
         value = solves / (ms_dev / 1e3)
@@ -284,6 +289,7 @@ def run_ours(args):
             "plain_gpu": {"value": round(plain_rate, 2), "unit": METRIC,
                           "what": "one ncpa_ess_solve + TL per frequency, same workload"},
             "cpu_baseline": cpu,
+            "modal_sum": ms_leg,
         }
         print(json.dumps(line), flush=True)
     for h in (prof,):
@@ -293,6 +299,82 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# modal sum at 64 receivers on the tensor cores (tall-atmosphere workload)
+# ---------------------------------------------------------------------------
+MS_NZ, MS_FREQ, MS_TOP_KM, MS_NR, MS_DR, MS_RCV = 100000, 2.0, 180.0, 20000, 100.0, 64
+
+
+def modal_sum_leg(ctx, stream, bf16_peak, k=10):
+    """Solve the 2 Hz, 180 km, Nz = 100000 problem once (untimed), then time
+    the modal sum at 64 receivers (0-10 km) x 20000 ranges (0.1 km to 2000 km)
+    through ncpa_tl_multi: tensor-core split-BF16 kernel and the FP64 CUDA-core
+    sum, with the tensor-core result's error against the FP64 one."""
+    import torch
+    import ncpa_gpu
+
+    tmp = tempfile.mkdtemp(prefix="ncpa_ms_")
+    path = workloads.write_profile(os.path.join(tmp, "analytic_180km.dat"), top_km=MS_TOP_KM)
+    prof = ctx.load_profile(path)
+    m = ctx.solve(prof, ncpa_gpu.default_params(nz_grid=MS_NZ, maxheight_km=MS_TOP_KM, want_vectors=1,
+                                                turnoff_wkb=1), [MS_FREQ], [90.0])
+    M = m.count(0)
+    h = np.linspace(0.0, 10000.0, MS_RCV)
+
+    def timed(method, reps):
+        for _ in range(2):
+            m.tl_multi(0, h, MS_NR, MS_DR, method=method, to_host=False)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(reps):
+            m.tl_multi(0, h, MS_NR, MS_DR, method=method, to_host=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / reps
+
+    ms_call = timed(1, k)
+    ms_fp64 = timed(0, 2)
+    ctx.reset_stats()
+    ctx.set_timing(True)
+    for _ in range(k):
+        m.tl_multi(0, h, MS_NR, MS_DR, method=1, to_host=False)
+    ctx.set_timing(False)
+    t_tc, n_tc = ctx.phase_stats("ms-tc")
+    ms_kernel = t_tc / max(n_tc, 1)
+    p_tc = m.tl_multi(0, h, 2000, MS_DR, method=1)
+    p_64 = m.tl_multi(0, h, 2000, MS_DR, method=0)
+    m.close()
+    prof.close()
+    alg = 8.0 * MS_RCV * M * MS_NR          # complex multiply-adds x 8 flops
+    tensor = 3.0 * alg                       # three bf16 products per term
+    achieved = tensor / (ms_kernel / 1e3) / 1e12
+    d = np.abs(20 * np.log10(np.abs(p_tc)) - 20 * np.log10(np.abs(p_64)))
+    d = d[20 * np.log10(np.abs(p_64)) > -140.0]
+    rel = np.abs(p_tc - p_64).max(axis=1) / np.abs(p_64).max(axis=1)
+    return {
+        "workload": "2 Hz, analytic 0-180 km, Nz=100000, %d modes; 64 receivers 0-10 km x 20000 ranges to 2000 km"
+                    % M,
+        "modes": int(M),
+        "ms_per_call": round(ms_call, 4), "ms_kernel": round(ms_kernel, 4), "ms_fp64_cuda_cores": round(ms_fp64, 3),
+        "roofline": {"kernel": "k_ms_tc (tcgen05 split-BF16)", "bound": "tensor", "achieved": round(achieved, 1),
+                     "peak": bf16_peak, "unit": "TFLOP/s", "frac": round(achieved / bf16_peak, 4),
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)",
+                     "flops_per_launch": tensor, "algorithmic_flops_per_launch": alg, "traffic": None},
+        "error_vs_fp64": {"max_abs_over_max_P": float(rel.max()), "tl_db_median": float(np.median(d)),
+                          "tl_db_p99_9": float(np.percentile(d, 99.9)), "tl_db_max": float(d.max()),
+                          "where": "TL > -140 dB, first 2000 ranges"},
+    }
+
+
+def _bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except (OSError, KeyError, ValueError):
+        return 1590.0  # earlier measurement on this pool, used when the file is absent
 
 
 # ---------------------------------------------------------------------------
@@ -377,6 +459,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--quick", action="store_true",
                     help="device-resident leg only (no e2e, plain-path or CPU legs); for profiler runs")
+    ap.add_argument("--no-modal-sum", action="store_true", help="skip the tensor-core modal-sum leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
