@@ -113,6 +113,21 @@ void ncpa_ess_params_default(ncpa_ess_params *p);
 ncpa_status ncpa_ess_solve(ncpa_ctx *ctx, const ncpa_profile *prof, const ncpa_ess_params *params,
                            const double *freqs, int n_freq, const double *az_deg, int n_az,
                            ncpa_modes **out);
+/* Batched solve over independent jobs, each with its own profile, frequency
+ * list and one azimuth (the request batch of the serving loop; the reference
+ * solves one (profile, frequency, azimuth) at a time in ESSModeSolver::solve,
+ * ESSModeSolver.cpp:320-383).  All profiles must give the same solver grid
+ * (same ground and top); problems are numbered job by job, frequency by
+ * frequency.  The result behaves like a one-azimuth solve of sum(n_freq)
+ * problems; ncpa_modes_info reports each problem's own densities. */
+typedef struct {
+    const ncpa_profile *profile;
+    const double *freqs;
+    int n_freq;
+    double az_deg;
+} ncpa_ess_job;
+ncpa_status ncpa_ess_solve_jobs(ncpa_ctx *ctx, const ncpa_ess_job *jobs, int n_jobs,
+                                const ncpa_ess_params *params, ncpa_modes **out);
 ncpa_status ncpa_modes_destroy(ncpa_modes *modes);
 ncpa_status ncpa_modes_problems(const ncpa_modes *modes, int *n_problems);
 ncpa_status ncpa_modes_count(const ncpa_modes *modes, int problem, int *n_modes);
@@ -219,6 +234,62 @@ ncpa_status ncpa_source_waveform(ncpa_ctx *ctx, const double *f, int n_freq, con
  * for k < n_freq (BroadbandPropagator.cpp:327-353) */
 ncpa_status ncpa_source_spectrum_waveform(ncpa_ctx *ctx, const double *x, int n_samples, double dt,
                                           int nfft, int n_freq, double *s_re, double *s_im);
+
+/* ------------------------------------------------------------------------
+ * Serving loop (no counterpart in the reference, which runs one solve per
+ * process): requests of different sizes (profile, frequency or band,
+ * azimuth) arrive at any time; worker lanes, each with its own stream, take
+ * every queued request that fits (problem count, HBM footprint) into one
+ * batched solve (ncpa_ess_solve_jobs) plus 1-D TL, so requests that arrive
+ * while others run are admitted as lanes and memory free up and their work
+ * overlaps on the device.  Results stay with the server until released.
+ * ---------------------------------------------------------------------- */
+typedef struct ncpa_server ncpa_server;
+typedef struct {
+    int device;
+    ncpa_ess_params params;  /* shared by every request (grid, heights, flags) */
+    int n_ranges;            /* 1-D TL range grid of every request: (i+1)*dr_m */
+    double dr_m;
+    int lanes;               /* batches in flight at once; 0 -> 2 */
+    int max_batch_problems;  /* problems merged into one solve; 0 -> 1024 */
+    double hbm_budget_bytes; /* admission limit on in-flight requests' estimated
+                                device footprint; 0 -> 8 GiB.  One request is
+                                always admitted when nothing else runs. */
+} ncpa_server_opts;
+
+typedef struct {
+    ncpa_profile_desc profile; /* host knot arrays (SI); copied at submit */
+    const double *freqs;
+    int n_freq;
+    double az_deg;
+} ncpa_request;
+
+typedef struct {
+    int status;                /* ncpa_status of this request */
+    int n_freq;
+    const int *mode_off;       /* [n_freq + 1] offsets into the mode arrays */
+    const double *re_k, *im_k, *v_src, *v_rcv;
+    const double *tl_re, *tl_im, *tl_incoh; /* [n_freq x n_ranges] */
+    double latency_ms;         /* submit -> results ready */
+    int batch_requests;        /* requests in the batch it was solved in */
+} ncpa_result;
+
+typedef struct {
+    long long submitted, completed, batches;
+    double mean_batch_requests;
+    double p50_ms, p99_ms, max_ms; /* latency over completed requests */
+    double peak_admitted_bytes;
+} ncpa_server_stats;
+
+void ncpa_server_opts_default(ncpa_server_opts *opts);
+ncpa_status ncpa_server_create(const ncpa_server_opts *opts, ncpa_server **out);
+ncpa_status ncpa_server_submit(ncpa_server *srv, const ncpa_request *req, unsigned long long *id);
+/* waits up to timeout_ms (< 0: forever); NCPA_ETIMEDOUT if not ready yet.
+ * The result's arrays stay valid until ncpa_server_release. */
+ncpa_status ncpa_server_wait(ncpa_server *srv, unsigned long long id, int timeout_ms, ncpa_result *out);
+ncpa_status ncpa_server_release(ncpa_server *srv, unsigned long long id);
+ncpa_status ncpa_server_stats_get(ncpa_server *srv, ncpa_server_stats *out);
+ncpa_status ncpa_server_destroy(ncpa_server *srv);
 
 /* Number of this library's kernels launched on the context so far. */
 long long ncpa_kernel_launches(const ncpa_ctx *ctx);

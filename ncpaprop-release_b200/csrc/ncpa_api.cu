@@ -113,6 +113,8 @@ struct ncpa_ctx {
     std::map<int, DevBuf> twiddle; // per nfft
     DevBuf bb_out;                 // waveforms kept in HBM (NULL host buffer)
     DevBuf ms_img, ms_q, ms_tab, ms_raw, ms_vz, ms_idx, ms_re, ms_im;  // modal-sum scratch (grow-only)
+    double* h_pin = nullptr;       // small pinned host buffer for scalars read back per solve
+    size_t h_pin_n = 0;
     DevBuf d_stats;                // device counters (Sturm sequences)
     bool timing = false;           // NCPA_TIMING=1: per-phase times on stderr
     bool stats = false;            // ncpa_ctx_set_timing: accumulate per phase
@@ -170,7 +172,8 @@ struct ncpa_modes {
     std::vector<double> freqs, az;
     double z_min = 0, dz_grid = 0, dz = 0;
     int isrc = 0, ircv = 0;
-    double rho_src = 1.0, rho_rcv = 1.0;
+    std::vector<double> rho_src_p, rho_rcv_p;  // rho at the source / receiver grid points, per problem
+    bool multi_job = false;                     // built by ncpa_ess_solve_jobs (one profile per job)
     std::vector<ProblemInfo> info;
     int Mtot = 0;
     DevBuf d_pinfo, d_kr, d_ki, d_vs, d_vr, d_vg, d_vfull, d_vfull_off;
@@ -250,6 +253,310 @@ void fetch_modes(const ncpa_modes* M) {
         CK(cudaMemcpyAsync(M->vg.data(), M->d_vg.p, M->Mtot * 8, cudaMemcpyDeviceToHost, st));
     }
     M->host_valid = true;
+}
+
+}  // namespace
+
+namespace {
+
+// pinned host scratch of at least n doubles (grow-only; the stream must be
+// idle when it grows, which holds at the start of a solve)
+double* pinned(ncpa_ctx* ctx, size_t n) {
+    if (n > ctx->h_pin_n) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
+        ctx->h_pin = nullptr;
+        ctx->h_pin_n = 0;
+        const size_t m = std::max<size_t>(n, 256);
+        CK(cudaHostAlloc((void**)&ctx->h_pin, m * sizeof(double), cudaHostAllocDefault));
+        ctx->h_pin_n = m;
+    }
+    return ctx->h_pin;
+}
+
+// grid geometry of ESSModeSolver.cpp:39-41, 144-151, 212-220, 314
+struct Geometry {
+    double z_min, dz_grid, dz;
+    int isrc, ircv;
+};
+
+void check_ess_params(const ncpa_ess_params* prm) {
+    if (prm->nz_grid < 10) throw ApiError(NCPA_EINVAL, "Nz_grid must be >= 10");
+    if (prm->wvnum_filter && !(prm->c_min > 0.0 && prm->c_max > 0.0))
+        throw ApiError(NCPA_EINVAL, "wvnum_filter needs c_min > 0 and c_max > 0");
+}
+
+Geometry grid_geometry(const ncpa_profile* prof, const ncpa_ess_params* prm) {
+    Geometry g{};
+    const int nz = prm->nz_grid;
+    double z_min = prm->zground_km * 1000.0;
+    double maxheight = prm->maxheight_km * 1000.0;
+    if (maxheight >= prof->z_hi) maxheight = prof->z_hi - 1e-6;
+    g.dz_grid = (maxheight - z_min) / (nz - 1);
+    if (prof->has_z0 && z_min < prof->z0) z_min = prof->z0;
+    g.dz = (maxheight - z_min) / (nz - 1);
+    if (!(g.dz > 0.0)) throw ApiError(NCPA_EINVAL, "maxheight must lie above the ground");
+    g.z_min = z_min;
+    g.isrc = (int)std::ceil(prm->sourceheight_km * 1000.0 / g.dz);
+    g.ircv = (int)std::ceil(prm->receiverheight_km * 1000.0 / g.dz);
+    if (g.isrc < 0 || g.isrc >= nz || g.ircv < 0 || g.ircv >= nz)
+        throw ApiError(NCPA_EINVAL, "source/receiver height outside the grid");
+    return g;
+}
+
+// Knot-level fields, grid fields and matrices of the n_freq x n_az problems
+// of one profile.  d_pinfo, s, g, kz2 point at the group's first problem; w
+// at the group's first frequency slot.  The ProblemInfo records (freq,
+// omega, az) must be on the device already.  rho at the source and receiver
+// grid points is copied to rho_pair[0..1] (pinned host memory, valid after
+// the next stream synchronisation).
+void build_problems(ncpa_ctx* ctx, PhaseTimer& tm, const ncpa_profile* prof, const ncpa_ess_params* prm,
+                    const Geometry& geo, int nz, int nz_pad, const double* freqs, int n_freq, const double* az_deg,
+                    int n_az, bool wkb, ProblemInfo* d_pinfo, double* s, double* w, double* g, double* kz2,
+                    double* rho_pair) {
+    cudaStream_t st = ctx->stream;
+    const int nk = prof->n;
+    const int P = n_freq * n_az;
+    DevBuf d_freqs, d_az;
+    upload(d_freqs, freqs, n_freq, st);
+    upload(d_az, az_deg, n_az, st);
+    DevBuf ceffk, ceffc, alpha, alphac;
+    ceffk.alloc((size_t)n_az * nk * 8, st);
+    ceffc.alloc((size_t)n_az * 4 * (nk - 1) * 8, st);
+    check_launch(ctx, ncpa::launch_ceff_knots(st, nk, n_az, d_az.as<double>(), prof->c0.as<double>(),
+                                              prof->ws.as<double>(), prof->wd.as<double>(), ceffk.as<double>()));
+    check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), ceffk.as<double>(), n_az, nk,
+                                           ceffc.as<double>(), 4 * (nk - 1)));
+    alpha.alloc((size_t)n_freq * nk * 8, st);
+    alphac.alloc((size_t)n_freq * 4 * (nk - 1) * 8, st);
+    if (prof->has_attn) {
+        for (int f = 0; f < n_freq; ++f)
+            CK(cudaMemcpyAsync(alpha.as<double>() + (size_t)f * nk, prof->attn.p, nk * 8, cudaMemcpyDeviceToDevice,
+                               st));
+    } else {
+        check_launch(ctx, ncpa::launch_alpha_knots(st, nk, n_freq, d_freqs.as<double>(), prof->z.as<double>(),
+                                                   prof->t.as<double>(), prof->p.as<double>(),
+                                                   prof->rho.as<double>(), alpha.as<double>()));
+    }
+    check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), alpha.as<double>(), n_freq, nk,
+                                           alphac.as<double>(), 4 * (nk - 1)));
+    // ---- grid fields ----
+    DevBuf rho_g, ct_g;
+    rho_g.alloc((size_t)nz * 8, st);
+    ct_g.alloc((size_t)nz * 8, st);
+    CK(cudaMemsetAsync(w, 0, (size_t)n_freq * nz_pad * 8, st));
+    check_launch(ctx, ncpa::launch_grid_common(st, nk, prof->z.as<double>(), prof->rho.as<double>(),
+                                               prof->rcoef.as<double>(), prof->p.as<double>(),
+                                               prof->pcoef.as<double>(), nz, geo.z_min, geo.dz_grid,
+                                               rho_g.as<double>(), ct_g.as<double>()));
+    check_launch(ctx, ncpa::launch_attn_weight(st, nk, prof->z.as<double>(), alpha.as<double>(), alphac.as<double>(),
+                                               n_freq, d_freqs.as<double>(), nz, geo.z_min, geo.dz_grid,
+                                               ct_g.as<double>(), w, nz_pad));
+    // admittance for the Lamb wave condition: -rho'(z0) / (2 rho(z0))
+    double admittance = 0.0;
+    CK(cudaMemcpyAsync(rho_pair, rho_g.as<double>() + geo.isrc, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(rho_pair + 1, rho_g.as<double>() + geo.ircv, 8, cudaMemcpyDeviceToHost, st));
+    if (prm->lamb_wave_bc) {
+        std::vector<double> hz(nk), hc(4 * (nk - 1)), hr(nk);
+        CK(cudaMemcpyAsync(hz.data(), prof->z.p, nk * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hr.data(), prof->rho.p, nk * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hc.data(), prof->rcoef.p, hc.size() * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        // one point of the rho spline and its slope (scalar set-up, as in
+        // ESSModeSolver.cpp:347-349)
+        double zq = geo.z_min, val, der;
+        if (zq > hz[nk - 1] || zq < hz[0]) {
+            val = zq > hz[nk - 1] ? hr[nk - 1] : hr[0];
+            der = 0.0;
+        } else {
+            int lo = 0, hi = nk - 1;
+            while (hi > lo + 1) {
+                int mid = (lo + hi) / 2;
+                if (hz[mid] > zq) hi = mid; else lo = mid;
+            }
+            const double* c = &hc[4 * lo];
+            double t = zq - hz[lo];
+            val = c[3] + t * (c[2] + t * (c[1] + t * c[0]));
+            der = c[2] + t * (2.0 * c[1] + t * 3.0 * c[0]);
+        }
+        admittance = -der / val / 2.0;
+    }
+    tm.mark("knots+grid");
+    // ---- K1 matrix ----
+    check_launch(ctx, ncpa::launch_build_matrix(st, nk, prof->z.as<double>(), ceffk.as<double>(), ceffc.as<double>(),
+                                                n_az, P, d_pinfo, nz, nz_pad, geo.z_min, geo.dz_grid, geo.dz,
+                                                admittance, s, wkb ? kz2 : nullptr, g));
+    tm.mark("matrix");
+}
+
+// Window, Sturm scan, work items, bisection and eigenvectors over all
+// problems of M (their matrices built).  w holds one weight row per
+// frequency when w_per_az > 0 (problem p uses row p / w_per_az).
+void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_params* prm, bool wkb, DevBuf& s,
+                DevBuf& w, DevBuf& g, DevBuf& kz2, int w_per_az) {
+    cudaStream_t st = ctx->stream;
+    const int P = M->P, nz = M->nz, nz_pad = M->nz_pad;
+    const double dz = M->dz;
+    ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
+    // ---- K2 window ----
+    check_launch(ctx, ncpa::launch_window(st, P, d_pinfo, wkb ? kz2.as<double>() : nullptr, nz, dz, wkb ? 1 : 0,
+                                          prm->wvnum_filter, prm->c_min, prm->c_max, ctx->d_err.as<unsigned>()));
+    tm.mark("window");
+    // ---- K3a scan ----
+    DevBuf counts;
+    counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
+    check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
+                                        ctx->d_err.as<unsigned>()));
+    tm.mark("scan");
+    std::vector<int> hcounts((size_t)P * ncpa::kScanPoints);
+    CK(cudaMemcpyAsync(hcounts.data(), counts.p, hcounts.size() * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(M->info.data(), d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
+    check_device_status(ctx);
+    // ---- modes per problem, offsets, work items ----
+    std::vector<WorkItem> items;
+    int off = 0;
+    for (int p = 0; p < P; ++p) {
+        ProblemInfo& pi = M->info[p];
+        pi.c_lo = hcounts[(size_t)p * ncpa::kScanPoints];
+        pi.c_hi = hcounts[(size_t)p * ncpa::kScanPoints + ncpa::kScanPoints - 1];
+        pi.M = std::max(0, pi.c_hi - pi.c_lo);
+        if (pi.M > M->prm.max_modes) {
+            char buf[160];
+            std::snprintf(buf, sizeof buf, "problem %d (f=%g Hz, az=%g) has %d modes > max_modes %d", p, pi.freq,
+                          pi.az, pi.M, M->prm.max_modes);
+            throw ApiError(NCPA_ETOOMANY, buf);
+        }
+        pi.off = off;
+        off += pi.M;
+        const int nit = (pi.M + ncpa::kWItem - 1) / ncpa::kWItem;
+        for (int k = 0; k < nit; ++k) {
+            int j0 = (int)((long long)pi.M * k / nit), j1 = (int)((long long)pi.M * (k + 1) / nit);
+            items.push_back(WorkItem{p, j0, j1 - j0, 0});
+        }
+    }
+    M->Mtot = off;
+    // largest items first: they need the most multisection rounds
+    std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.m > b.m; });
+    CK(cudaMemcpyAsync(d_pinfo, M->info.data(), P * sizeof(ProblemInfo), cudaMemcpyHostToDevice, st));
+    const int Mt = std::max(1, M->Mtot);
+    DevBuf mu, d_items, d_counter;
+    mu.alloc((size_t)Mt * 8, st);
+    M->d_kr.alloc((size_t)Mt * 8, st);
+    M->d_ki.alloc((size_t)Mt * 8, st);
+    M->d_vs.alloc((size_t)Mt * 8, st);
+    M->d_vr.alloc((size_t)Mt * 8, st);
+    M->d_vg.alloc((size_t)Mt * 8, st);
+    if (prm->want_vectors) {
+        M->vfull_off.resize(P);
+        long long acc = 0;
+        for (int p = 0; p < P; ++p) {
+            M->vfull_off[p] = acc;
+            acc += (long long)M->info[p].M * nz;
+        }
+        M->d_vfull.alloc((size_t)std::max(1LL, acc) * 8, st);
+        upload(M->d_vfull_off, M->vfull_off, st);
+    }
+    const int n_items = (int)items.size();
+    if (n_items > 0) {
+        upload(d_items, items, st);
+        d_counter.alloc(2 * sizeof(int), st);
+        CK(cudaMemsetAsync(d_counter.p, 0, 2 * sizeof(int), st));
+        // ---- K3 bisection ----
+        const int wpc = 4;  // warps per bisection CTA
+        int grid_b = std::min((n_items + wpc - 1) / wpc, ctx->num_sms * ncpa::bisect_ctas_per_sm());
+        tm.mark("host-items");
+        check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
+                                              d_items.as<WorkItem>(), n_items, d_counter.as<int>(), kBisectTol,
+                                              mu.as<double>(), ctx->d_err.as<unsigned>(),
+                                              ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr));
+        if (ctx->stats) ctx->grid_points += nz;
+        tm.mark("bisect");
+        // ---- K4 eigenvectors: items of <= kEvItem eigenvalues ----
+        std::vector<WorkItem> ev_items;
+        for (int p = 0; p < P; ++p) {
+            const int Mp = M->info[p].M;
+            for (int j0 = 0; j0 < Mp; j0 += ncpa::kEvItem)
+                ev_items.push_back(WorkItem{p, j0, std::min(ncpa::kEvItem, Mp - j0), 0});
+        }
+        DevBuf d_ev_items;
+        upload(d_ev_items, ev_items, st);
+        const int n_ev = (int)ev_items.size();
+        ncpa::EigvecArgs ea{};
+        ea.pinfo = d_pinfo;
+        ea.s = s.as<double>();
+        ea.w = w.as<double>();
+        ea.g = prm->want_group_speed ? g.as<double>() : nullptr;
+        ea.nz = nz;
+        ea.nz_pad = nz_pad;
+        ea.wstride = nz_pad;
+        ea.n_az = w_per_az;
+        ea.items = d_ev_items.as<WorkItem>();
+        ea.n_items = n_ev;
+        ea.counter = d_counter.as<int>() + 1;
+        ea.mu = mu.as<double>();
+        ea.isrc = M->isrc;
+        ea.ircv = M->ircv;
+        ea.dz = dz;
+        ea.h2 = dz * dz;
+        ea.kr = M->d_kr.as<double>();
+        ea.ki = M->d_ki.as<double>();
+        ea.vs = M->d_vs.as<double>();
+        ea.vr = M->d_vr.as<double>();
+        ea.vg = M->d_vg.as<double>();
+        ea.vfull = prm->want_vectors ? M->d_vfull.as<double>() : nullptr;
+        ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
+        const int ewpc = ncpa::kEvWarpsPerCta;
+        const int grid_e = std::min((n_ev + ewpc - 1) / ewpc, ctx->num_sms * ncpa::eigvec_ctas_per_sm(ea));
+        const long long nblk = (nz + ncpa::kBlk - 1) / ncpa::kBlk;
+        const long long slot = nblk * 32;
+        const size_t need = (size_t)grid_e * ewpc * slot;
+        if (ctx->ck1.bytes < need * 8) {
+            ctx->ck1.alloc(need * 8, st);
+            ctx->ck2.alloc(need * 8, st);
+            ctx->cke.alloc(need * 4, st);
+        }
+        ea.ck_q1 = ctx->ck1.as<double>();
+        ea.ck_q2 = ctx->ck2.as<double>();
+        ea.ck_e = ctx->cke.as<int>();
+        ea.ck_slot_stride = slot;
+        ea.err = ctx->d_err.as<unsigned>();
+        check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
+    }
+    tm.mark("eigvec");
+    // ---- results to host ----
+    if (!prm->keep_on_device) fetch_modes(M);
+    check_device_status(ctx);
+    tm.mark("fetch");
+}
+
+void init_modes(ncpa_modes* M, ncpa_ctx* ctx, const ncpa_ess_params* prm, const Geometry& geo, int P) {
+    M->ctx = ctx;
+    M->prm = *prm;
+    if (M->prm.max_modes <= 0) M->prm.max_modes = 4000;
+    M->P = P;
+    M->nz = prm->nz_grid;
+    M->nz_pad = ((M->nz + ncpa::kChunk - 1) / ncpa::kChunk) * ncpa::kChunk;
+    M->z_min = geo.z_min;
+    M->dz_grid = geo.dz_grid;
+    M->dz = geo.dz;
+    M->isrc = geo.isrc;
+    M->ircv = geo.ircv;
+    M->info.assign(P, ProblemInfo{});
+    M->rho_src_p.assign(P, 1.0);
+    M->rho_rcv_p.assign(P, 1.0);
+}
+
+void set_problem(ProblemInfo& pi, double freq, double az) {
+    pi.freq = freq;
+    pi.omega = 2 * kPi * freq;
+    pi.az = az;
+    pi.ceffmin_bits = 0x7ff0000000000000ull;
+    pi.ceffmax_bits = 0ull;
+}
+
+bool wants_wkb(const ncpa_ess_params* prm) {
+    return !prm->turnoff_wkb && std::fabs(prm->sourceheight_km * 1000.0) < 1.0e-3 &&
+           std::fabs(prm->receiverheight_km * 1000.0) < 1.0e-3;
 }
 
 }  // namespace
@@ -393,6 +700,7 @@ ncpa_status ncpa_ctx_destroy(ncpa_ctx* ctx) {
                       &ctx->ms_im})
         b->release();  // stream-ordered frees need the stream alive
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NCPA_OK;
@@ -601,271 +909,106 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
     *out = nullptr;
     return guarded(ctx, [&]() -> ncpa_status {
         if (n_freq < 1 || n_az < 1) throw ApiError(NCPA_EINVAL, "need at least one frequency and azimuth");
-        if (prm->nz_grid < 10) throw ApiError(NCPA_EINVAL, "Nz_grid must be >= 10");
+        check_ess_params(prm);
         for (int i = 0; i < n_freq; ++i)
             if (!(freqs[i] > 0.0)) throw ApiError(NCPA_EINVAL, "frequencies must be positive");
-        if (prm->wvnum_filter && !(prm->c_min > 0.0 && prm->c_max > 0.0))
-            throw ApiError(NCPA_EINVAL, "wvnum_filter needs c_min > 0 and c_max > 0");
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        PhaseTimer tm(ctx);
+        tm.mark("start");
+        const Geometry geo = grid_geometry(prof, prm);
+        auto M = std::make_unique<ncpa_modes>();
+        init_modes(M.get(), ctx, prm, geo, n_freq * n_az);
+        M->nf = n_freq;
+        M->na = n_az;
+        M->freqs.assign(freqs, freqs + n_freq);
+        M->az.assign(az_deg, az_deg + n_az);
+        const int P = M->P, nz = M->nz, nz_pad = M->nz_pad;
+        for (int f = 0; f < n_freq; ++f)
+            for (int a = 0; a < n_az; ++a) set_problem(M->info[f * n_az + a], freqs[f], az_deg[a]);
+        upload(M->d_pinfo, M->info, st);
+        const bool wkb = wants_wkb(prm);
+        DevBuf s, w, g, kz2;
+        s.alloc((size_t)P * nz_pad * 8, st);
+        w.alloc((size_t)n_freq * nz_pad * 8, st);
+        if (wkb) kz2.alloc((size_t)P * nz * 8, st);
+        if (prm->want_group_speed) g.alloc((size_t)P * nz_pad * 8, st);
+        double* rho_pair = pinned(ctx, 2);
+        build_problems(ctx, tm, prof, prm, geo, nz, nz_pad, freqs, n_freq, az_deg, n_az, wkb,
+                       M->d_pinfo.as<ProblemInfo>(), s.as<double>(), w.as<double>(),
+                       prm->want_group_speed ? g.as<double>() : nullptr, wkb ? kz2.as<double>() : nullptr, rho_pair);
+        solve_core(ctx, tm, M.get(), prm, wkb, s, w, g, kz2, n_az);
+        M->rho_src_p.assign(P, rho_pair[0]);
+        M->rho_rcv_p.assign(P, rho_pair[1]);
+        *out = M.release();
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_ess_solve_jobs(ncpa_ctx* ctx, const ncpa_ess_job* jobs, int n_jobs, const ncpa_ess_params* prm,
+                                ncpa_modes** out) {
+    if (!ctx || !jobs || n_jobs < 1 || !prm || !out) return NCPA_EINVAL;
+    *out = nullptr;
+    return guarded(ctx, [&]() -> ncpa_status {
+        check_ess_params(prm);
+        int P = 0;
+        for (int j = 0; j < n_jobs; ++j) {
+            const ncpa_ess_job& jb = jobs[j];
+            if (!jb.profile || !jb.freqs || jb.n_freq < 1) throw ApiError(NCPA_EINVAL, "job without profile or frequencies");
+            for (int i = 0; i < jb.n_freq; ++i)
+                if (!(jb.freqs[i] > 0.0)) throw ApiError(NCPA_EINVAL, "frequencies must be positive");
+            if (jb.profile->ctx != ctx) throw ApiError(NCPA_EINVAL, "profile belongs to another context");
+            P += jb.n_freq;
+        }
+        // one grid for the whole batch: every profile must give the same geometry
+        const Geometry geo = grid_geometry(jobs[0].profile, prm);
+        for (int j = 1; j < n_jobs; ++j) {
+            const Geometry gj = grid_geometry(jobs[j].profile, prm);
+            if (gj.z_min != geo.z_min || gj.dz != geo.dz || gj.dz_grid != geo.dz_grid)
+                throw ApiError(NCPA_EINVAL, "jobs of one batch need profiles giving the same solver grid");
+        }
         CK(cudaSetDevice(ctx->device));
         cudaStream_t st = ctx->stream;
         PhaseTimer tm(ctx);
         tm.mark("start");
         auto M = std::make_unique<ncpa_modes>();
-        M->ctx = ctx;
-        M->prm = *prm;
-        if (M->prm.max_modes <= 0) M->prm.max_modes = 4000;
-        M->nf = n_freq;
-        M->na = n_az;
-        M->P = n_freq * n_az;
-        M->freqs.assign(freqs, freqs + n_freq);
-        M->az.assign(az_deg, az_deg + n_az);
-        const int nz = prm->nz_grid;
-        const int nz_pad = ((nz + ncpa::kChunk - 1) / ncpa::kChunk) * ncpa::kChunk;
-        M->nz = nz;
-        M->nz_pad = nz_pad;
-        // grid geometry (ESSModeSolver.cpp:39-41, 144-151, 212-220, 314)
-        double z_min = prm->zground_km * 1000.0;
-        double maxheight = prm->maxheight_km * 1000.0;
-        if (maxheight >= prof->z_hi) maxheight = prof->z_hi - 1e-6;
-        const double dz_grid = (maxheight - z_min) / (nz - 1);
-        if (prof->has_z0 && z_min < prof->z0) z_min = prof->z0;
-        const double dz = (maxheight - z_min) / (nz - 1);
-        if (!(dz > 0.0)) throw ApiError(NCPA_EINVAL, "maxheight must lie above the ground");
-        M->z_min = z_min;
-        M->dz_grid = dz_grid;
-        M->dz = dz;
-        const double src_h = prm->sourceheight_km * 1000.0, rcv_h = prm->receiverheight_km * 1000.0;
-        M->isrc = (int)std::ceil(src_h / dz);
-        M->ircv = (int)std::ceil(rcv_h / dz);
-        if (M->isrc < 0 || M->isrc >= nz || M->ircv < 0 || M->ircv >= nz)
-            throw ApiError(NCPA_EINVAL, "source/receiver height outside the grid");
-        const int nk = prof->n;
-        const int P = M->P;
-
-        // ---- knot-level fields ----
-        DevBuf d_freqs, d_az;
-        upload(d_freqs, freqs, n_freq, st);
-        upload(d_az, az_deg, n_az, st);
-        DevBuf ceffk, ceffc, alpha, alphac;
-        ceffk.alloc((size_t)n_az * nk * 8, st);
-        ceffc.alloc((size_t)n_az * 4 * (nk - 1) * 8, st);
-        check_launch(ctx, ncpa::launch_ceff_knots(st, nk, n_az, d_az.as<double>(), prof->c0.as<double>(),
-                                                  prof->ws.as<double>(), prof->wd.as<double>(), ceffk.as<double>()));
-        check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), ceffk.as<double>(), n_az, nk,
-                                               ceffc.as<double>(), 4 * (nk - 1)));
-        const int n_alpha = prof->has_attn ? 1 : n_freq;
-        alpha.alloc((size_t)n_freq * nk * 8, st);
-        alphac.alloc((size_t)n_freq * 4 * (nk - 1) * 8, st);
-        if (prof->has_attn) {
-            for (int f = 0; f < n_freq; ++f)
-                CK(cudaMemcpyAsync(alpha.as<double>() + (size_t)f * nk, prof->attn.p, nk * 8,
-                                   cudaMemcpyDeviceToDevice, st));
-        } else {
-            check_launch(ctx, ncpa::launch_alpha_knots(st, nk, n_freq, d_freqs.as<double>(), prof->z.as<double>(),
-                                                       prof->t.as<double>(), prof->p.as<double>(),
-                                                       prof->rho.as<double>(), alpha.as<double>()));
-        }
-        (void)n_alpha;
-        check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), alpha.as<double>(), n_freq, nk,
-                                               alphac.as<double>(), 4 * (nk - 1)));
-        // ---- grid fields ----
-        DevBuf rho_g, ct_g, w;
-        rho_g.alloc((size_t)nz * 8, st);
-        ct_g.alloc((size_t)nz * 8, st);
-        w.alloc((size_t)n_freq * nz_pad * 8, st);
-        CK(cudaMemsetAsync(w.p, 0, (size_t)n_freq * nz_pad * 8, st));
-        check_launch(ctx, ncpa::launch_grid_common(st, nk, prof->z.as<double>(), prof->rho.as<double>(),
-                                                   prof->rcoef.as<double>(), prof->p.as<double>(),
-                                                   prof->pcoef.as<double>(), nz, z_min, dz_grid, rho_g.as<double>(),
-                                                   ct_g.as<double>()));
-        check_launch(ctx, ncpa::launch_attn_weight(st, nk, prof->z.as<double>(), alpha.as<double>(),
-                                                   alphac.as<double>(), n_freq, d_freqs.as<double>(), nz, z_min,
-                                                   dz_grid, ct_g.as<double>(), w.as<double>(), nz_pad));
-        // admittance for the Lamb wave condition: -rho'(z0) / (2 rho(z0))
-        double admittance = 0.0;
-        std::vector<double> hrho(nz);
-        CK(cudaMemcpyAsync(hrho.data(), rho_g.p, nz * 8, cudaMemcpyDeviceToHost, st));
-        if (prm->lamb_wave_bc) {
-            std::vector<double> hz(nk), hc(4 * (nk - 1)), hr(nk);
-            CK(cudaMemcpyAsync(hz.data(), prof->z.p, nk * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(hr.data(), prof->rho.p, nk * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(hc.data(), prof->rcoef.p, hc.size() * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            // one point of the rho spline and its slope (scalar set-up, as in
-            // ESSModeSolver.cpp:347-349)
-            double zq = z_min, val, der;
-            if (zq > hz[nk - 1] || zq < hz[0]) {
-                val = zq > hz[nk - 1] ? hr[nk - 1] : hr[0];
-                der = 0.0;
-            } else {
-                int lo = 0, hi = nk - 1;
-                while (hi > lo + 1) {
-                    int mid = (lo + hi) / 2;
-                    if (hz[mid] > zq) hi = mid; else lo = mid;
-                }
-                const double* c = &hc[4 * lo];
-                double t = zq - hz[lo];
-                val = c[3] + t * (c[2] + t * (c[1] + t * c[0]));
-                der = c[2] + t * (2.0 * c[1] + t * 3.0 * c[0]);
+        init_modes(M.get(), ctx, prm, geo, P);
+        M->nf = P;
+        M->na = 1;
+        M->multi_job = true;
+        const int nz = M->nz, nz_pad = M->nz_pad;
+        int p0 = 0;
+        for (int j = 0; j < n_jobs; ++j)
+            for (int i = 0; i < jobs[j].n_freq; ++i, ++p0) {
+                set_problem(M->info[p0], jobs[j].freqs[i], jobs[j].az_deg);
+                M->freqs.push_back(jobs[j].freqs[i]);
             }
-            admittance = -der / val / 2.0;
-        }
-        // ---- per-problem info ----
-        M->info.assign(P, ProblemInfo{});
-        for (int f = 0; f < n_freq; ++f)
-            for (int a = 0; a < n_az; ++a) {
-                ProblemInfo& pi = M->info[f * n_az + a];
-                pi.freq = freqs[f];
-                pi.omega = 2 * kPi * freqs[f];
-                pi.az = az_deg[a];
-                pi.ceffmin_bits = 0x7ff0000000000000ull;
-                pi.ceffmax_bits = 0ull;
-            }
+        M->az.assign(1, jobs[0].az_deg);
         upload(M->d_pinfo, M->info, st);
-        ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
-        tm.mark("knots+grid");
-        // ---- K1 matrix ----
-        const bool wkb = !prm->turnoff_wkb && std::fabs(src_h) < 1.0e-3 && std::fabs(rcv_h) < 1.0e-3;
-        DevBuf s, kz2, g;
+        const bool wkb = wants_wkb(prm);
+        DevBuf s, w, g, kz2;
         s.alloc((size_t)P * nz_pad * 8, st);
+        w.alloc((size_t)P * nz_pad * 8, st);  // one row per problem
         if (wkb) kz2.alloc((size_t)P * nz * 8, st);
         if (prm->want_group_speed) g.alloc((size_t)P * nz_pad * 8, st);
-        check_launch(ctx, ncpa::launch_build_matrix(st, nk, prof->z.as<double>(), ceffk.as<double>(),
-                                                    ceffc.as<double>(), n_az, P, d_pinfo, nz, nz_pad, z_min, dz_grid,
-                                                    dz, admittance, s.as<double>(), wkb ? kz2.as<double>() : nullptr,
-                                                    prm->want_group_speed ? g.as<double>() : nullptr));
-        tm.mark("matrix");
-        // ---- K2 window ----
-        check_launch(ctx, ncpa::launch_window(st, P, d_pinfo, wkb ? kz2.as<double>() : nullptr, nz, dz, wkb ? 1 : 0,
-                                              prm->wvnum_filter, prm->c_min, prm->c_max, ctx->d_err.as<unsigned>()));
-        tm.mark("window");
-        // ---- K3a scan ----
-        DevBuf counts;
-        counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
-        check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
-                                            ctx->d_err.as<unsigned>()));
-        tm.mark("scan");
-        std::vector<int> hcounts((size_t)P * ncpa::kScanPoints);
-        CK(cudaMemcpyAsync(hcounts.data(), counts.p, hcounts.size() * 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(M->info.data(), d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
-        check_device_status(ctx);
-        // ---- modes per problem, offsets, work items ----
-        std::vector<WorkItem> items;
-        int off = 0;
-        for (int p = 0; p < P; ++p) {
-            ProblemInfo& pi = M->info[p];
-            pi.c_lo = hcounts[(size_t)p * ncpa::kScanPoints];
-            pi.c_hi = hcounts[(size_t)p * ncpa::kScanPoints + ncpa::kScanPoints - 1];
-            pi.M = std::max(0, pi.c_hi - pi.c_lo);
-            if (pi.M > M->prm.max_modes) {
-                char buf[160];
-                std::snprintf(buf, sizeof buf, "problem %d (f=%g Hz, az=%g) has %d modes > max_modes %d", p, pi.freq,
-                              pi.az, pi.M, M->prm.max_modes);
-                throw ApiError(NCPA_ETOOMANY, buf);
-            }
-            pi.off = off;
-            off += pi.M;
-            const int nit = (pi.M + ncpa::kWItem - 1) / ncpa::kWItem;
-            for (int k = 0; k < nit; ++k) {
-                int j0 = (int)((long long)pi.M * k / nit), j1 = (int)((long long)pi.M * (k + 1) / nit);
-                items.push_back(WorkItem{p, j0, j1 - j0, 0});
-            }
+        double* rho_pairs = pinned(ctx, 2 * (size_t)n_jobs);
+        p0 = 0;
+        for (int j = 0; j < n_jobs; ++j) {
+            const ncpa_ess_job& jb = jobs[j];
+            build_problems(ctx, tm, jb.profile, prm, geo, nz, nz_pad, jb.freqs, jb.n_freq, &jb.az_deg, 1, wkb,
+                           M->d_pinfo.as<ProblemInfo>() + p0, s.as<double>() + (size_t)p0 * nz_pad,
+                           w.as<double>() + (size_t)p0 * nz_pad,
+                           prm->want_group_speed ? g.as<double>() + (size_t)p0 * nz_pad : nullptr,
+                           wkb ? kz2.as<double>() + (size_t)p0 * nz : nullptr, rho_pairs + 2 * j);
+            p0 += jb.n_freq;
         }
-        M->Mtot = off;
-        // largest items first: they need the most multisection rounds
-        std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.m > b.m; });
-        CK(cudaMemcpyAsync(d_pinfo, M->info.data(), P * sizeof(ProblemInfo), cudaMemcpyHostToDevice, st));
-        const int Mt = std::max(1, M->Mtot);
-        DevBuf mu, d_items, d_counter;
-        mu.alloc((size_t)Mt * 8, st);
-        M->d_kr.alloc((size_t)Mt * 8, st);
-        M->d_ki.alloc((size_t)Mt * 8, st);
-        M->d_vs.alloc((size_t)Mt * 8, st);
-        M->d_vr.alloc((size_t)Mt * 8, st);
-        M->d_vg.alloc((size_t)Mt * 8, st);
-        if (prm->want_vectors) {
-            M->vfull_off.resize(P);
-            long long acc = 0;
-            for (int p = 0; p < P; ++p) {
-                M->vfull_off[p] = acc;
-                acc += (long long)M->info[p].M * nz;
+        solve_core(ctx, tm, M.get(), prm, wkb, s, w, g, kz2, 1);
+        p0 = 0;
+        for (int j = 0; j < n_jobs; ++j)
+            for (int i = 0; i < jobs[j].n_freq; ++i, ++p0) {
+                M->rho_src_p[p0] = rho_pairs[2 * j];
+                M->rho_rcv_p[p0] = rho_pairs[2 * j + 1];
             }
-            M->d_vfull.alloc((size_t)std::max(1LL, acc) * 8, st);
-            upload(M->d_vfull_off, M->vfull_off, st);
-        }
-        const int n_items = (int)items.size();
-        if (n_items > 0) {
-            upload(d_items, items, st);
-            d_counter.alloc(2 * sizeof(int), st);
-            CK(cudaMemsetAsync(d_counter.p, 0, 2 * sizeof(int), st));
-            // ---- K3 bisection ----
-            const int wpc = 4;  // warps per bisection CTA
-            int grid_b = std::min((n_items + wpc - 1) / wpc, ctx->num_sms * ncpa::bisect_ctas_per_sm());
-            tm.mark("host-items");
-            check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
-                                                  d_items.as<WorkItem>(), n_items, d_counter.as<int>(), kBisectTol,
-                                                  mu.as<double>(), ctx->d_err.as<unsigned>(),
-                                                  ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr));
-            if (ctx->stats) ctx->grid_points += nz;
-            tm.mark("bisect");
-            // ---- K4 eigenvectors: items of <= kEvThreads eigenvalues ----
-            std::vector<WorkItem> ev_items;
-            for (int p = 0; p < P; ++p) {
-                const int Mp = M->info[p].M;
-                for (int j0 = 0; j0 < Mp; j0 += ncpa::kEvItem)
-                    ev_items.push_back(WorkItem{p, j0, std::min(ncpa::kEvItem, Mp - j0), 0});
-            }
-            DevBuf d_ev_items;
-            upload(d_ev_items, ev_items, st);
-            const int n_ev = (int)ev_items.size();
-            ncpa::EigvecArgs ea{};
-            ea.pinfo = d_pinfo;
-            ea.s = s.as<double>();
-            ea.w = w.as<double>();
-            ea.g = prm->want_group_speed ? g.as<double>() : nullptr;
-            ea.nz = nz;
-            ea.nz_pad = nz_pad;
-            ea.wstride = nz_pad;
-            ea.n_az = n_az;
-            ea.items = d_ev_items.as<WorkItem>();
-            ea.n_items = n_ev;
-            ea.counter = d_counter.as<int>() + 1;
-            ea.mu = mu.as<double>();
-            ea.isrc = M->isrc;
-            ea.ircv = M->ircv;
-            ea.dz = dz;
-            ea.h2 = dz * dz;
-            ea.kr = M->d_kr.as<double>();
-            ea.ki = M->d_ki.as<double>();
-            ea.vs = M->d_vs.as<double>();
-            ea.vr = M->d_vr.as<double>();
-            ea.vg = M->d_vg.as<double>();
-            ea.vfull = prm->want_vectors ? M->d_vfull.as<double>() : nullptr;
-            ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
-            const int ewpc = ncpa::kEvWarpsPerCta;
-            const int grid_e = std::min((n_ev + ewpc - 1) / ewpc, ctx->num_sms * ncpa::eigvec_ctas_per_sm(ea));
-            const long long nblk = (nz + ncpa::kBlk - 1) / ncpa::kBlk;
-            const long long slot = nblk * 32;
-            const size_t need = (size_t)grid_e * ewpc * slot;
-            if (ctx->ck1.bytes < need * 8) {
-                ctx->ck1.alloc(need * 8, st);
-                ctx->ck2.alloc(need * 8, st);
-                ctx->cke.alloc(need * 4, st);
-            }
-            ea.ck_q1 = ctx->ck1.as<double>();
-            ea.ck_q2 = ctx->ck2.as<double>();
-            ea.ck_e = ctx->cke.as<int>();
-            ea.ck_slot_stride = slot;
-            ea.err = ctx->d_err.as<unsigned>();
-            check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
-        }
-        tm.mark("eigvec");
-        // ---- results to host ----
-        if (!prm->keep_on_device) fetch_modes(M.get());
-        check_device_status(ctx);
-        tm.mark("fetch");
-        M->rho_src = hrho[M->isrc];
-        M->rho_rcv = hrho[M->ircv];
         *out = M.release();
         return NCPA_OK;
     });
@@ -900,8 +1043,8 @@ ncpa_status ncpa_modes_info(const ncpa_modes* m, int problem, double* freq, doub
     if (dz) *dz = m->dz;
     if (k_min) *k_min = pi.k_min;
     if (k_max) *k_max = pi.k_max;
-    if (rho_src) *rho_src = m->rho_src;
-    if (rho_rcv) *rho_rcv = m->rho_rcv;
+    if (rho_src) *rho_src = m->rho_src_p[problem];
+    if (rho_rcv) *rho_rcv = m->rho_rcv_p[problem];
     return NCPA_OK;
 }
 
@@ -1155,7 +1298,8 @@ ncpa_status ncpa_bb_synthesize_modes(ncpa_ctx* ctx, const ncpa_modes* m, int az_
                                      double* waveforms) {
     if (!ctx || !m || !bp || az_index < 0 || az_index >= m->na) return NCPA_EINVAL;
     return guarded(ctx, [&]() -> ncpa_status {
-        if (m->na != 1) throw ApiError(NCPA_EINVAL, "device-resident synthesis needs a single-azimuth solve");
+        if (m->na != 1 || m->multi_job)
+            throw ApiError(NCPA_EINVAL, "device-resident synthesis needs a single-azimuth, single-profile solve");
         CK(cudaSetDevice(ctx->device));
         cudaStream_t st = ctx->stream;
         const int nf = m->nf + 1;  // DC slot first
@@ -1172,7 +1316,7 @@ ncpa_status ncpa_bb_synthesize_modes(ncpa_ctx* ctx, const ncpa_modes* m, int az_
         upload(df, f, st);
         upload(doff, off, st);
         return bb_common(ctx, nf, df.as<double>(), doff.as<int>(), m->Mtot, m->d_kr.as<double>(),
-                         m->d_ki.as<double>(), m->d_vs.as<double>(), m->d_vr.as<double>(), m->rho_rcv / m->rho_src,
+                         m->d_ki.as<double>(), m->d_vs.as<double>(), m->d_vr.as<double>(), m->rho_rcv_p[0] / m->rho_src_p[0],
                          bp, waveforms);
     });
 }

@@ -29,7 +29,8 @@ EXPORTED = [
     "ncpa_kernel_launches", "ncpa_ctx_stream", "ncpa_ctx_set_timing", "ncpa_ctx_phase_stats",
     "ncpa_ctx_reset_stats", "ncpa_ctx_sturm_sequences", "ncpa_probe_fp64_peak", "ncpa_source_spectrum_builtin",
     "ncpa_eigvec_static", "ncpa_profile_set_attn", "ncpa_profile_load_attn", "ncpa_profile_knots", "ncpa_profile_z0",
-    "ncpa_modal_starter", "ncpa_source_waveform", "ncpa_tl_multi",
+    "ncpa_modal_starter", "ncpa_source_waveform", "ncpa_tl_multi", "ncpa_ess_solve_jobs", "ncpa_server_opts_default", "ncpa_server_create",
+    "ncpa_server_submit", "ncpa_server_wait", "ncpa_server_release", "ncpa_server_stats_get", "ncpa_server_destroy",
 ]
 
 
@@ -46,6 +47,10 @@ class _CtxOpts(ctypes.Structure):
 class _ProfileDesc(ctypes.Structure):
     _fields_ = [("n_knots", _c_int), ("z", _dp), ("u", _dp), ("v", _dp), ("t", _dp), ("p", _dp), ("rho", _dp),
                 ("c0", _dp), ("attn", _dp), ("z0_m", _c_double), ("has_z0", _c_int)]
+
+
+class _EssJob(ctypes.Structure):
+    _fields_ = [("profile", _vp), ("freqs", _dp), ("n_freq", _c_int), ("az_deg", _c_double)]
 
 
 class EssParams(ctypes.Structure):
@@ -92,6 +97,8 @@ def lib():
         L.ncpa_profile_info.argtypes = [_vp, _ip, _dp, _dp]
         L.ncpa_ess_params_default.argtypes = [ctypes.POINTER(EssParams)]
         L.ncpa_ess_params_default.restype = None
+        L.ncpa_ess_solve_jobs.argtypes = [_vp, ctypes.POINTER(_EssJob), _c_int, ctypes.POINTER(EssParams),
+                                          ctypes.POINTER(_vp)]
         L.ncpa_ess_solve.argtypes = [_vp, _vp, ctypes.POINTER(EssParams), _dp, _c_int, _dp, _c_int,
                                      ctypes.POINTER(_vp)]
         L.ncpa_modes_destroy.argtypes = [_vp]
@@ -227,6 +234,18 @@ class Context:
         self.check(lib().ncpa_ess_solve(self.h, profile.h, ctypes.byref(params), _p(f), len(f), _p(a), len(a),
                                         ctypes.byref(h)), "ncpa_ess_solve")
         return Modes(self, h, f, a)
+
+    def solve_jobs(self, jobs, params: EssParams):
+        """One batched solve over jobs [(profile, freqs, azimuth_deg), ...];
+        problems are numbered job by job."""
+        keep = [_f64(np.atleast_1d(f)) for _, f, _ in jobs]
+        arr = (_EssJob * len(jobs))()
+        for i, ((prof, _, az), f) in enumerate(zip(jobs, keep)):
+            arr[i] = _EssJob(prof.h.value, _p(f), len(f), float(az))
+        h = _vp()
+        self.check(lib().ncpa_ess_solve_jobs(self.h, arr, len(jobs), ctypes.byref(params), ctypes.byref(h)),
+                   "ncpa_ess_solve_jobs")
+        return Modes(self, h, np.concatenate(keep), np.array([j[2] for j in jobs], dtype=np.float64))
 
     SOURCES = {"impulse": 0, "pulse1": 1, "pulse2": 2}
 
@@ -368,3 +387,114 @@ class Modes:
         if self.h:
             lib().ncpa_modes_destroy(self.h)
             self.h = _vp()
+
+
+# ---------------------------------------------------------------------------
+# serving loop (ncpa_server_*)
+# ---------------------------------------------------------------------------
+class _ServerOpts(ctypes.Structure):
+    _fields_ = [("device", _c_int), ("params", EssParams), ("n_ranges", _c_int), ("dr_m", _c_double),
+                ("lanes", _c_int), ("max_batch_problems", _c_int), ("hbm_budget_bytes", _c_double)]
+
+
+class _Request(ctypes.Structure):
+    _fields_ = [("profile", _ProfileDesc), ("freqs", _dp), ("n_freq", _c_int), ("az_deg", _c_double)]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("status", _c_int), ("n_freq", _c_int), ("mode_off", _ip), ("re_k", _dp), ("im_k", _dp),
+                ("v_src", _dp), ("v_rcv", _dp), ("tl_re", _dp), ("tl_im", _dp), ("tl_incoh", _dp),
+                ("latency_ms", _c_double), ("batch_requests", _c_int)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong), ("batches", ctypes.c_longlong),
+                ("mean_batch_requests", _c_double), ("p50_ms", _c_double), ("p99_ms", _c_double),
+                ("max_ms", _c_double), ("peak_admitted_bytes", _c_double)]
+
+
+_SERVER_SIGS = False
+
+
+def _server_sigs():
+    global _SERVER_SIGS
+    if _SERVER_SIGS:
+        return
+    L = lib()
+    L.ncpa_server_opts_default.argtypes = [ctypes.POINTER(_ServerOpts)]
+    L.ncpa_server_opts_default.restype = None
+    L.ncpa_server_create.argtypes = [ctypes.POINTER(_ServerOpts), ctypes.POINTER(_vp)]
+    L.ncpa_server_submit.argtypes = [_vp, ctypes.POINTER(_Request), ctypes.POINTER(ctypes.c_ulonglong)]
+    L.ncpa_server_wait.argtypes = [_vp, ctypes.c_ulonglong, _c_int, ctypes.POINTER(_Result)]
+    L.ncpa_server_release.argtypes = [_vp, ctypes.c_ulonglong]
+    L.ncpa_server_stats_get.argtypes = [_vp, ctypes.POINTER(_ServerStats)]
+    L.ncpa_server_destroy.argtypes = [_vp]
+    _SERVER_SIGS = True
+
+
+class Server:
+    """Serving loop: submit requests (profile knots in SI, frequencies,
+    azimuth) at any time; each returns dispersion and 1-D TL."""
+
+    def __init__(self, device=0, params=None, n_ranges=2000, dr_m=500.0, lanes=2, max_batch_problems=1024,
+                 hbm_budget_bytes=0.0):
+        _server_sigs()
+        o = _ServerOpts()
+        lib().ncpa_server_opts_default(ctypes.byref(o))
+        o.device = device
+        if params is not None:
+            o.params = params
+        o.n_ranges, o.dr_m, o.lanes = int(n_ranges), float(dr_m), int(lanes)
+        o.max_batch_problems, o.hbm_budget_bytes = int(max_batch_problems), float(hbm_budget_bytes)
+        self.n_ranges = int(n_ranges)
+        self.h = _vp()
+        st = lib().ncpa_server_create(ctypes.byref(o), ctypes.byref(self.h))
+        if st != 0:
+            raise NcpaError(st, "ncpa_server_create")
+
+    def submit(self, z, u, v, t, p, rho, freqs, az_deg, z0=None):
+        arrs = [_f64(x) for x in (z, u, v, t, p, rho)]
+        f = _f64(np.atleast_1d(freqs))
+        d = _ProfileDesc(len(arrs[0]), *[_p(a) for a in arrs], None, None, float(z0 or 0.0), int(z0 is not None))
+        req = _Request(d, _p(f), len(f), float(az_deg))
+        rid = ctypes.c_ulonglong()
+        st = lib().ncpa_server_submit(self.h, ctypes.byref(req), ctypes.byref(rid))
+        if st != 0:
+            raise NcpaError(st, "ncpa_server_submit")
+        return rid.value
+
+    def wait(self, rid, timeout_ms=-1, release=True):
+        r = _Result()
+        st = lib().ncpa_server_wait(self.h, ctypes.c_ulonglong(rid), int(timeout_ms), ctypes.byref(r))
+        if st != 0:
+            raise NcpaError(st, "ncpa_server_wait")
+        nf, nr = r.n_freq, self.n_ranges
+        out = {"status": r.status, "latency_ms": r.latency_ms, "batch_requests": r.batch_requests}
+        if r.status == 0:
+            off = np.ctypeslib.as_array(r.mode_off, shape=(nf + 1,)).copy()
+            nm = int(off[-1])
+            out["mode_off"] = off
+            for k in ("re_k", "im_k", "v_src", "v_rcv"):
+                ptr = getattr(r, k)
+                out[k] = np.ctypeslib.as_array(ptr, shape=(nm,)).copy() if nm else np.empty(0)
+            for k in ("tl_re", "tl_im", "tl_incoh"):
+                out[k] = np.ctypeslib.as_array(getattr(r, k), shape=(nf * nr,)).copy().reshape(nf, nr)
+        if release:
+            lib().ncpa_server_release(self.h, ctypes.c_ulonglong(rid))
+        return out
+
+    def stats(self):
+        s = _ServerStats()
+        lib().ncpa_server_stats_get(self.h, ctypes.byref(s))
+        return {k: getattr(s, k) for k, _ in _ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().ncpa_server_destroy(self.h)
+            self.h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

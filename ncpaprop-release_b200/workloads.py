@@ -77,3 +77,54 @@ def broadband_freqs(n=256, f_max=0.5):
     df = f_max / n
     nf = int(np.floor((f_max - df) / df)) + 1
     return df + np.arange(nf) * df
+
+
+# ---------------------------------------------------------------------------
+# served request stream
+# ---------------------------------------------------------------------------
+_GP_CHOL = {}
+
+
+def _gp_factor(z_km, sigma_k=3.0, corr_km=5.0):
+    key = (len(z_km), sigma_k, corr_km)
+    if key not in _GP_CHOL:
+        d = z_km[:, None] - z_km[None, :]
+        cov = sigma_k ** 2 * np.exp(-0.5 * (d / corr_km) ** 2)
+        cov[np.diag_indices_from(cov)] += 1e-6 * sigma_k ** 2
+        _GP_CHOL[key] = np.linalg.cholesky(cov)
+    return _GP_CHOL[key]
+
+
+def perturbed_profile(rng, dz_km=0.1):
+    """One served request's atmosphere as SI knot arrays (z m, u, v, T, p, rho):
+    the analytic profile with the stratospheric jet's amplitude drawn from
+    U(0, 80) m/s at a height from U(40, 70) km, the tropospheric jet's
+    amplitude from U(0, 40) m/s, and Gaussian-process temperature noise
+    (sigma 3 K, squared-exponential correlation of 5 km, Cholesky factor on the
+    knot grid); p = rho 287 T is recomputed."""
+    z, _, v, T, rho, _ = analytic_profile(150.0, dz_km)
+    a_s, h_s, a_t = rng.uniform(0.0, 80.0), rng.uniform(40.0, 70.0), rng.uniform(0.0, 40.0)
+    u = a_s * np.exp(-((z - h_s) / 10.0) ** 2) + a_t * np.exp(-((z - 12.0) / 3.0) ** 2)
+    T = T + _gp_factor(z) @ rng.standard_normal(len(z))
+    p = rho * 287.0 * T
+    return z * 1000.0, u, v, T, p, rho
+
+
+def request_stream(n, rate_hz, seed=0):
+    """n requests with Poisson arrivals at rate_hz: 80 % single frequency
+    (log-uniform 0.05-2 Hz), 20 % broadband (32-256 frequencies, uniform
+    spacing f_max/n up to 0.5 Hz); azimuth uniform in [0, 360).  Yields dicts
+    with the arrival time [s], profile arrays, frequencies and azimuth."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for _ in range(n):
+        t += rng.exponential(1.0 / rate_hz)
+        if rng.uniform() < 0.8:
+            freqs = np.array([np.exp(rng.uniform(np.log(0.05), np.log(2.0)))])
+        else:
+            nf = int(rng.integers(32, 257))
+            freqs = 0.5 / nf * np.arange(1, nf + 1)
+        az = rng.uniform(0.0, 360.0)
+        out.append({"t": t, "profile": perturbed_profile(rng), "freqs": freqs, "az": az})
+    return out

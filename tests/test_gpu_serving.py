@@ -1,0 +1,107 @@
+"""Batched multi-profile solve and the serving loop on the GPU.
+
+- ncpa_ess_solve_jobs over jobs with different profiles, frequencies and
+  azimuths gives, problem by problem, exactly what ncpa_ess_solve gives for
+  each job alone.
+- Every served request's dispersion and 1-D TL are the same whether it was
+  solved alone or in a batch with others (continuous batching), and the HBM
+  admission limit serialises requests when it is tight.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NZ = 4000
+NR, DR = 300, 2000.0
+
+
+def _jobs(seed, n):
+    import workloads
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        prof = workloads.perturbed_profile(rng)
+        if k % 3 == 1:
+            nf = int(rng.integers(8, 24))
+            freqs = 0.25 / nf * np.arange(1, nf + 1)
+        else:
+            freqs = np.array([np.exp(rng.uniform(np.log(0.05), np.log(0.6)))])
+        out.append((prof, freqs, float(rng.uniform(0.0, 360.0))))
+    return out
+
+
+def _params(**kw):
+    import ncpa_gpu
+
+    return ncpa_gpu.default_params(nz_grid=NZ, **kw)
+
+
+def _alone(gpu, prof, freqs, az):
+    p = gpu.profile_from_arrays(*prof)
+    m = gpu.solve(p, _params(), freqs, [az])
+    probs = [m.problem(i) for i in range(m.P)]
+    re, im, inc = m.tl1d(NR, DR)
+    m.close()
+    p.close()
+    return probs, re, im, inc
+
+
+def test_solve_jobs_equals_one_solve_per_job(gpu):
+    jobs = _jobs(11, 5)
+    profs = [gpu.profile_from_arrays(*j[0]) for j in jobs]
+    m = gpu.solve_jobs([(p, f, az) for p, (_, f, az) in zip(profs, jobs)], _params())
+    assert m.P == sum(len(j[1]) for j in jobs)
+    re_b, im_b, _ = m.tl1d(NR, DR)
+    p0 = 0
+    for prof, freqs, az in jobs:
+        probs, re, im, _ = _alone(gpu, prof, freqs, az)
+        for i, a in enumerate(probs):
+            b = m.problem(p0 + i)
+            assert b.M == a.M and b.freq == a.freq and b.az == a.az
+            for k in ("kr", "ki", "vs", "vr"):
+                assert np.array_equal(getattr(a, k), getattr(b, k)), k
+            assert b.rho_src == a.rho_src and b.rho_rcv == a.rho_rcv
+            assert np.array_equal(re[i], re_b[p0 + i]) and np.array_equal(im[i], im_b[p0 + i])
+        p0 += len(freqs)
+    m.close()
+    for p in profs:
+        p.close()
+
+
+def test_served_results_equal_alone_and_in_the_mix(gpu):
+    import ncpa_gpu
+
+    jobs = _jobs(23, 12)
+    with ncpa_gpu.Server(0, params=_params(), n_ranges=NR, dr_m=DR, lanes=2) as srv:
+        ids = [srv.submit(*prof, freqs, az) for prof, freqs, az in jobs]
+        res = [srv.wait(i, timeout_ms=120000) for i in ids]
+        st = srv.stats()
+    assert st["completed"] == len(jobs)
+    assert max(r["batch_requests"] for r in res) >= 2  # some requests shared a batch
+    for (prof, freqs, az), r in zip(jobs, res):
+        assert r["status"] == 0
+        probs, re, im, inc = _alone(gpu, prof, freqs, az)
+        off = r["mode_off"]
+        for i, a in enumerate(probs):
+            sl = slice(off[i], off[i + 1])
+            assert off[i + 1] - off[i] == a.M
+            assert np.array_equal(r["re_k"][sl], a.kr) and np.array_equal(r["im_k"][sl], a.ki)
+            assert np.array_equal(r["v_src"][sl] * r["v_rcv"][sl], a.vs * a.vr)
+        assert np.array_equal(r["tl_re"], re) and np.array_equal(r["tl_im"], im)
+        assert np.array_equal(r["tl_incoh"], inc)
+    assert st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_tight_hbm_budget_admits_one_request_at_a_time(gpu):
+    import ncpa_gpu
+
+    jobs = _jobs(5, 6)
+    with ncpa_gpu.Server(0, params=_params(), n_ranges=NR, dr_m=DR, lanes=2, hbm_budget_bytes=1.0) as srv:
+        ids = [srv.submit(*prof, freqs, az) for prof, freqs, az in jobs]
+        res = [srv.wait(i, timeout_ms=120000) for i in ids]
+        st = srv.stats()
+    assert all(r["status"] == 0 for r in res)
+    assert all(r["batch_requests"] == 1 for r in res)
+    assert st["batches"] == len(jobs)
