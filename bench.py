@@ -9,7 +9,10 @@ Gaussian-windowed 0.1 Hz Ricker waveform sampled at 1 Hz.
 
 The line also carries "modal_sum": the tensor-core modal sum at 64
 receivers x 20000 ranges of a 2 Hz, Nz = 100000 solve (timed separately,
-not part of the step), with its roofline against the measured bf16 peak.
+not part of the step), with its roofline against the measured bf16 peak,
+and "serving": a seeded request stream replayed in real time through the
+serving loop and through the plain one-request-at-a-time path (p50 / p99
+latency, throughput).
 
   value  freq-solves/s with the profile resident in HBM and results left in
          HBM (device-timed with CUDA events on the library's stream; L2
@@ -257,6 +260,7 @@ def run_ours(args):
         ms_dev, ms_e2e = reduce_max([ms_dev, ms_e2e])
     fp64_peak = ctx.fp64_peak_tflops() if rank == 0 else None
     ms_leg = modal_sum_leg(ctx, stream, _bf16_peak()) if rank == 0 and not args.no_modal_sum else None
+    sv_leg = serving_leg(ctx) if rank == 0 and not args.no_serving else None
     if rank == 0:
         solves = NFREQ * args.steps * world
         value = solves / (ms_dev / 1e3)
@@ -290,6 +294,7 @@ def run_ours(args):
                           "what": "one ncpa_ess_solve + TL per frequency, same workload"},
             "cpu_baseline": cpu,
             "modal_sum": ms_leg,
+            "serving": sv_leg,
         }
         print(json.dumps(line), flush=True)
     for h in (prof,):
@@ -367,6 +372,99 @@ def modal_sum_leg(ctx, stream, bf16_peak, k=10):
                           "tl_db_p99_9": float(np.percentile(d, 99.9)), "tl_db_max": float(d.max()),
                           "where": "TL > -140 dB, first 2000 ranges"},
     }
+
+
+SV_N, SV_NR, SV_DR, SV_SEED, SV_LOAD, SV_LANES = 200, 2000, 500.0, 2024, 0.8, 3
+
+
+def serving_leg(ctx, n=SV_N):
+    """Served request stream (seeded Poisson arrivals, per-request perturbed
+    profiles, 80 % single frequency 0.05-2 Hz, 20 % 32-256 frequencies up to
+    0.5 Hz, uniform azimuth, 2000 ranges every 0.5 km, Nz = 20000) replayed in
+    real time twice: through the serving loop (3 lanes, continuous batching)
+    and through the plain path (one request at a time on one context: profile
+    upload, solve, 1-D TL to the host).  The arrival rate is set to load the
+    plain path to 80 % of its measured capacity.  Latency = completion -
+    arrival."""
+    import ncpa_gpu
+
+    prm = ncpa_gpu.default_params(nz_grid=NZ)
+    reqs = workloads.request_stream(n, 1.0, SV_SEED)  # arrival times rescaled below
+
+    def plain_one(r):
+        p = ctx.profile_from_arrays(*r["profile"])
+        m = ctx.solve(p, prm, r["freqs"], [r["az"]])
+        m.tl1d(SV_NR, SV_DR)
+        for i in range(m.P):
+            m.problem(i)
+        m.close()
+        p.close()
+
+    for r in reqs[:5]:
+        plain_one(r)  # warm-up
+    t0 = time.perf_counter()
+    for r in reqs[:40]:
+        plain_one(r)
+    service = (time.perf_counter() - t0) / 40
+    rate = SV_LOAD / service
+    arrivals = np.array([r["t"] for r in reqs]) / rate  # unit-rate times -> rate
+    n_fs = sum(len(r["freqs"]) for r in reqs)
+
+    # plain path, real-time replay
+    lat = []
+    start = time.perf_counter()
+    for r, ta in zip(reqs, arrivals):
+        now = time.perf_counter() - start
+        if now < ta:
+            time.sleep(ta - now)
+        plain_one(r)
+        lat.append((time.perf_counter() - start - ta) * 1e3)
+    plain_wall = time.perf_counter() - start
+    plain = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+             "requests_per_s": n / plain_wall, "freq_solves_per_s": n_fs / plain_wall}
+
+    # served, real-time replay from a submitting thread
+    srv = ncpa_gpu.Server(0, params=prm, n_ranges=SV_NR, dr_m=SV_DR, lanes=SV_LANES)
+    # warm-up burst: every lane gets work, so each lane's stream-ordered pool
+    # and scratch reach their working size before the timed replay
+    for i in [srv.submit(*r["profile"], r["freqs"], r["az"]) for r in reqs[:24]]:
+        srv.wait(i)
+    ids = [None] * n
+
+    def submitter():
+        st0 = time.perf_counter()
+        for i, (r, ta) in enumerate(zip(reqs, arrivals)):
+            now = time.perf_counter() - st0
+            if now < ta:
+                time.sleep(ta - now)
+            ids[i] = srv.submit(*r["profile"], r["freqs"], r["az"])
+
+    start = time.perf_counter()
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    res = [srv.wait(i) for i in ids]
+    served_wall = time.perf_counter() - start
+    slat = [r["latency_ms"] for r in res]
+    served = {"p50_ms": float(np.percentile(slat, 50)), "p99_ms": float(np.percentile(slat, 99)),
+              "requests_per_s": n / served_wall, "freq_solves_per_s": n_fs / served_wall,
+              "mean_batch_requests": float(np.mean([r["batch_requests"] for r in res])),
+              "failed": int(sum(r["status"] != 0 for r in res))}
+    # capacity: the whole stream submitted at once
+    start = time.perf_counter()
+    ids = [srv.submit(*r["profile"], r["freqs"], r["az"]) for r in reqs]
+    res = [srv.wait(i) for i in ids]
+    cap_wall = time.perf_counter() - start
+    served["capacity_requests_per_s"] = n / cap_wall
+    served["capacity_freq_solves_per_s"] = n_fs / cap_wall
+    served["capacity_mean_batch_requests"] = float(np.mean([r["batch_requests"] for r in res]))
+    plain["capacity_requests_per_s"] = 1.0 / service
+    plain["capacity_freq_solves_per_s"] = n_fs / (service * n)
+    srv.close()
+    return {"workload": "%d requests, seed %d, Poisson at %.1f req/s (80%% of the plain path's capacity), Nz=%d, "
+                        "%d ranges x %.1f km" % (n, SV_SEED, rate, NZ, SV_NR, SV_DR / 1000.0),
+            "freq_solves": int(n_fs), "plain_service_ms": round(service * 1e3, 3), "plain": plain, "served": served,
+            "p99_speedup": plain["p99_ms"] / served["p99_ms"] if served["p99_ms"] > 0 else None}
 
 
 def _bf16_peak():
@@ -460,6 +558,7 @@ def main():
     ap.add_argument("--quick", action="store_true",
                     help="device-resident leg only (no e2e, plain-path or CPU legs); for profiler runs")
     ap.add_argument("--no-modal-sum", action="store_true", help="skip the tensor-core modal-sum leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the served request-stream leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -761,7 +761,8 @@ ncpa_status ncpa_profile_create(ncpa_ctx* ctx, const ncpa_profile_desc* d, ncpa_
         P->has_z0 = d->has_z0;
         P->z_lo = d->z[0];
         P->z_hi = d->z[n - 1];
-        CK(cudaStreamSynchronize(st));
+        // no synchronisation: pageable uploads are staged before the copy
+        // calls return, and everything later is ordered on the stream
         *out = P.release();
         return NCPA_OK;
     });
