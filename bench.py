@@ -170,7 +170,6 @@ def run_ours(args):
     nfft = _nfft(nf_dc, len(x_w))
     prof = ctx.load_profile(prof_path)
     params_dev = ncpa_gpu.default_params(nz_grid=NZ, turnoff_wkb=1, keep_on_device=1)
-    params_host = ncpa_gpu.default_params(nz_grid=NZ, turnoff_wkb=1)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -192,11 +191,11 @@ def run_ours(args):
         pr = ctx.profile_from_arrays(*(pin[k].numpy() for k in ("z", "u", "v", "t", "p", "rho")))
         xw = pin["x"].numpy()
         sre, sim = ctx.source_spectrum_waveform(xw, t_w[1] - t_w[0], nfft, nf_dc)
-        m = ctx.solve(pr, params_host, pin["f"].numpy(), az)
-        disp = [m.problem(i) for i in range(m.P)]
+        m = ctx.solve(pr, params_dev, pin["f"].numpy(), az)
+        disp = m.all_modes()  # CSR offsets + k, attenuation, source / receiver values, group speeds
         tl = m.tl1d(N_TL, DR_TL)
         wav = m.bb_synthesize(ranges_m, MAX_CEL, nfft, sre, sim)
-        nm = sum(d.M for d in disp)
+        nm = int(disp[0][-1])
         h2d[0] = 6 * len(z) * 8 + len(xw) * 8 + len(freqs) * 8
         d2h[0] = nm * 5 * 8 + sum(a.nbytes for a in tl) + wav.nbytes + 2 * nf_dc * 8
         m.close()

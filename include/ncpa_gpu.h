@@ -141,6 +141,11 @@ ncpa_status ncpa_modes_info(const ncpa_modes *modes, int problem, double *freq, 
  * (NULL to skip; zero unless want_group_speed). */
 ncpa_status ncpa_modes_get(const ncpa_modes *modes, int problem, double *re_k, double *im_k,
                            double *v_src, double *v_rcv, double *v_group);
+/* all problems at once, in CSR order: mode_off[n_problems + 1] offsets, the
+ * arrays hold mode_off[n_problems] entries (NULL to skip; copied straight
+ * from HBM) */
+ncpa_status ncpa_modes_get_all(const ncpa_modes *modes, int *mode_off, double *re_k, double *im_k,
+                               double *v_src, double *v_rcv, double *v_group);
 /* full eigenvectors of one problem, layout [z_index * M + mode]
  * (needs want_vectors) */
 ncpa_status ncpa_modes_get_vectors(const ncpa_modes *modes, int problem, double *v);

@@ -1070,6 +1070,26 @@ ncpa_status ncpa_modes_get(const ncpa_modes* m, int problem, double* re_k, doubl
     return NCPA_OK;
 }
 
+ncpa_status ncpa_modes_get_all(const ncpa_modes* m, int* mode_off, double* re_k, double* im_k, double* v_src,
+                               double* v_rcv, double* v_group) {
+    if (!m || !mode_off) return NCPA_EINVAL;
+    for (int p = 0; p < m->P; ++p) mode_off[p] = m->info[p].off;
+    mode_off[m->P] = m->Mtot;
+    if (!re_k && !im_k && !v_src && !v_rcv && !v_group) return NCPA_OK;
+    return guarded(m->ctx, [&]() -> ncpa_status {
+        cudaStream_t st = m->ctx->stream;
+        const size_t n = (size_t)m->Mtot * 8;
+        if (n) {
+            const std::pair<double*, const DevBuf*> cols[] = {
+                {re_k, &m->d_kr}, {im_k, &m->d_ki}, {v_src, &m->d_vs}, {v_rcv, &m->d_vr}, {v_group, &m->d_vg}};
+            for (const auto& c : cols)
+                if (c.first) CK(cudaMemcpyAsync(c.first, c.second->p, n, cudaMemcpyDeviceToHost, st));
+        }
+        CK(cudaStreamSynchronize(st));
+        return NCPA_OK;
+    });
+}
+
 ncpa_status ncpa_modes_get_vectors(const ncpa_modes* m, int problem, double* v) {
     if (!m || !v || problem < 0 || problem >= m->P) return NCPA_EINVAL;
     if (!m->prm.want_vectors) return fail(m->ctx, NCPA_EINVAL, "solve was run without want_vectors");

@@ -30,7 +30,7 @@ EXPORTED = [
     "ncpa_ctx_reset_stats", "ncpa_ctx_sturm_sequences", "ncpa_probe_fp64_peak", "ncpa_source_spectrum_builtin",
     "ncpa_eigvec_static", "ncpa_profile_set_attn", "ncpa_profile_load_attn", "ncpa_profile_knots", "ncpa_profile_z0",
     "ncpa_modal_starter", "ncpa_source_waveform", "ncpa_tl_multi", "ncpa_ess_solve_jobs", "ncpa_server_opts_default", "ncpa_server_create",
-    "ncpa_server_submit", "ncpa_server_wait", "ncpa_server_release", "ncpa_server_stats_get", "ncpa_server_destroy",
+    "ncpa_server_submit", "ncpa_server_wait", "ncpa_server_release", "ncpa_server_stats_get", "ncpa_server_destroy", "ncpa_modes_get_all",
 ]
 
 
@@ -107,6 +107,7 @@ def lib():
         L.ncpa_modes_info.argtypes = [_vp, _c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ncpa_modes_get.argtypes = [_vp, _c_int, _dp, _dp, _dp, _dp, _dp]
         L.ncpa_modes_get_vectors.argtypes = [_vp, _c_int, _dp]
+        L.ncpa_modes_get_all.argtypes = [_vp, _ip, _dp, _dp, _dp, _dp, _dp]
         L.ncpa_tl_1d.argtypes = [_vp, _vp, ctypes.POINTER(_TlParams), _dp, _dp, _dp]
         L.ncpa_tl_2d_heights.argtypes = [_vp, _c_int, _ip]
         L.ncpa_tl_2d.argtypes = [_vp, _vp, _c_int, ctypes.POINTER(_TlParams), _dp, _dp, _dp]
@@ -336,6 +337,17 @@ class Modes:
         kr, ki, vs, vr, vg = (np.empty(M) for _ in range(5))
         self.ctx.check(lib().ncpa_modes_get(self.h, p, _p(kr), _p(ki), _p(vs), _p(vr), _p(vg)), "ncpa_modes_get")
         return ProblemModes(*[v.value for v in vals], kr, ki, vs, vr, vg)
+
+    def all_modes(self):
+        """(mode_off, kr, ki, vs, vr, vg) of every problem in CSR order."""
+        off = np.empty(self.P + 1, dtype=np.int32)
+        self.ctx.check(lib().ncpa_modes_get_all(self.h, off.ctypes.data_as(_ip), None, None, None, None, None),
+                       "ncpa_modes_get_all")
+        n = int(off[-1])
+        arrs = [np.empty(n) for _ in range(5)]
+        self.ctx.check(lib().ncpa_modes_get_all(self.h, off.ctypes.data_as(_ip), *[_p(a) for a in arrs]),
+                       "ncpa_modes_get_all")
+        return (off, *arrs)
 
     def vectors(self, p, nz):
         M = self.count(p)

@@ -54,6 +54,11 @@ def test_solve_jobs_equals_one_solve_per_job(gpu):
     m = gpu.solve_jobs([(p, f, az) for p, (_, f, az) in zip(profs, jobs)], _params())
     assert m.P == sum(len(j[1]) for j in jobs)
     re_b, im_b, _ = m.tl1d(NR, DR)
+    off, kr, ki, vs, vr, _ = m.all_modes()  # bulk getter, CSR order
+    for i in range(m.P):
+        b = m.problem(i)
+        assert off[i + 1] - off[i] == b.M
+        assert np.array_equal(kr[off[i]:off[i + 1]], b.kr) and np.array_equal(vr[off[i]:off[i + 1]], b.vr)
     p0 = 0
     for prof, freqs, az in jobs:
         probs, re, im, _ = _alone(gpu, prof, freqs, az)
