@@ -176,6 +176,9 @@ def run_ours(args):
     # pinned host buffers for the end-to-end leg
     pin = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for k, a in
            dict(z=z, u=u, v=v, t=t, p=p, rho=rho, x=x_w, f=freqs).items()}
+    # pinned host buffers the results of the end-to-end leg land in
+    pin_tl = [torch.empty((NFREQ, N_TL), dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
+    pin_wav = torch.empty((len(RANGES_KM), nfft), dtype=torch.float64).pin_memory().numpy()
 
     def step_device():
         sre, sim = ctx.source_spectrum_waveform(x_w, t_w[1] - t_w[0], nfft, nf_dc)
@@ -193,8 +196,8 @@ def run_ours(args):
         sre, sim = ctx.source_spectrum_waveform(xw, t_w[1] - t_w[0], nfft, nf_dc)
         m = ctx.solve(pr, params_dev, pin["f"].numpy(), az)
         disp = m.all_modes()  # CSR offsets + k, attenuation, source / receiver values, group speeds
-        tl = m.tl1d(N_TL, DR_TL)
-        wav = m.bb_synthesize(ranges_m, MAX_CEL, nfft, sre, sim)
+        tl = m.tl1d(N_TL, DR_TL, out=pin_tl)
+        wav = m.bb_synthesize(ranges_m, MAX_CEL, nfft, sre, sim, out=pin_wav)
         nm = int(disp[0][-1])
         h2d[0] = 6 * len(z) * 8 + len(xw) * 8 + len(freqs) * 8
         d2h[0] = nm * 5 * 8 + sum(a.nbytes for a in tl) + wav.nbytes + 2 * nf_dc * 8

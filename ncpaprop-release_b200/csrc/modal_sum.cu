@@ -18,20 +18,20 @@
 // one (group, tile) in TMEM (two accumulators, so a finished tile's epilogue
 // overlaps the next tile's MMAs) and stores its partial sum of the tile in
 // its own slot; the finishing kernel adds the slots of the CTAs that shared
-// the tile.  Warp 0: TMEM allocation, bulk-TMA of the prepared A' chunk
-// together with the chunk's per-mode factor rows and tile phases, and
-// tcgen05.mma issue.  Warps 1-8: generate B' in shared memory from
+// the tile.  Warp 0: TMEM allocation and tcgen05.mma issue.  Warp 9: bulk
+// TMA of the prepared A' chunk together with the chunk's per-mode factor
+// rows and tile phases.  Warps 1-8: generate B' in shared memory from
 // FP64-reduced tile phases e^{i k r_n0} (phase reduced mod 2 pi in FP64)
 // times per-mode FP32 factors e^{i k o dr}, and read the accumulators out.
 //
-// Shared-memory operand layout (no swizzle, K-major core matrices): element
-// (row, k) of a 128-row x 64-k bf16 tile sits at byte
-//   ((row / 8) * 8 + k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2,
-// i.e. leading-byte offset 128 (next 8 k) and stride-byte offset 1024 (next 8
-// rows); one MMA (K = 16) starts 256 bytes further per K-step.
+// Shared-memory operand layout: K-major, 64-byte swizzle (sw64_off below):
+// each operand row holds the 32 k of a chunk (64 B), 8-row atoms of 512 B,
+// 16-byte chunks XOR-permuted by row so that the generators' 16-byte stores
+// and the tensor cores' reads are free of bank conflicts.
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cmath>
 
 #include "device_common.cuh"
 
@@ -41,36 +41,49 @@ namespace {
 
 constexpr int kMsRows = 128;        // UMMA M (Re / Im rows of 64 receivers)
 constexpr int kMsRcv = 64;          // receivers per group
-constexpr int kMsNT = 128;          // ranges per tile (UMMA N)
-constexpr int kMsModes = 32;        // modes per K-chunk
+constexpr int kMsNT = 256;          // ranges per tile (UMMA N)
+constexpr int kMsModes = 16;        // modes per K-chunk
 constexpr int kMsKC = 2 * kMsModes; // K per chunk
-constexpr int kMsStages = 3;
-constexpr int kMsOpBytes = kMsRows * kMsKC * 2;  // one operand part: 16 KB
-constexpr int kMsTabW = 34;         // per-mode row: e^{ik o dr} for the 32 thread offsets, e^{ik 8 dr}, pad
-constexpr int kMsTabBytes = kMsModes * kMsTabW * 8;  // factor rows of one chunk: 8704 B
+constexpr int kMsStages = 4;
+constexpr int kMsABytes = kMsRows * kMsKC * 2;   // one A' part (hi or lo) of a chunk: 8 KB
+constexpr int kMsBBytes = kMsNT * kMsKC * 2;     // one B' part of a chunk: 16 KB
+constexpr int kMsTabW = 18;         // per-mode row: e^{ik i dr} (i < 8), e^{ik 32 j dr} (j < 8), e^{ik 8 dr}, pad
+constexpr int kMsTabBytes = kMsModes * kMsTabW * 8;  // factor rows of one chunk: 2304 B
 constexpr int kMsQBytes = kMsModes * 8;              // tile phases of one chunk
-constexpr int kMsTxBytes = 2 * kMsOpBytes + kMsTabBytes + kMsQBytes;
+constexpr int kMsTxBytes = 2 * kMsABytes + kMsTabBytes + kMsQBytes;
 // stage: A hi, A lo, B hi, B lo, factor rows, tile phases (1 KB aligned)
-constexpr int kMsStageBytes = (4 * kMsOpBytes + kMsTabBytes + kMsQBytes + 1023) / 1024 * 1024;
+constexpr int kMsOffB = 2 * kMsABytes;
+constexpr int kMsOffTab = kMsOffB + 2 * kMsBBytes;
+constexpr int kMsOffQ = kMsOffTab + kMsTabBytes;
+constexpr int kMsStageBytes = (kMsOffQ + kMsQBytes + 1023) / 1024 * 1024;
 constexpr int kMsSmem = kMsStages * kMsStageBytes + 1024;
 constexpr int kMsGenWarps = 8;      // B' generators / epilogue
 constexpr int kMsGenThreads = 32 * kMsGenWarps;
-constexpr int kMsThreads = 32 + kMsGenThreads;
-constexpr int kMsAcc = 2;           // TMEM accumulators (kMsNT columns each)
+constexpr int kMsProducerWarp = 1 + kMsGenWarps;  // warp 0: MMA issuer, 1-8: generators, 9: TMA producer
+constexpr int kMsThreads = 32 * (kMsProducerWarp + 1);
+constexpr int kMsAcc = 2;           // TMEM accumulators (kMsNT columns each): all 512 columns
 static_assert(kMsSmem <= 232448, "shared memory per block");
-static_assert(kMsTabBytes % 16 == 0 && kMsQBytes % 16 == 0, "bulk copies move 16-byte multiples");
-static_assert(kMsNT == kMsRows, "square operand tiles share one layout");
+static_assert(kMsTabBytes % 16 == 0 && kMsQBytes % 16 == 0 && kMsTxBytes % 16 == 0,
+              "bulk copies move 16-byte multiples");
+static_assert(kMsAcc * kMsNT <= 512, "TMEM columns");
+static_assert(kMsGenThreads == 8 * (kMsModes / 4) * (kMsNT / 32), "one generator per (range, mode quad, 32 ranges)");
 
-__device__ __forceinline__ uint32_t core_off(int row, int k) {
-    return (uint32_t)((((row >> 3) * (kMsKC / 8)) + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2);
+// byte offset of element (row, k) in a K-major tile of kMsKC = 32 bf16 per
+// row with the 64-byte swizzle: rows of 64 B in atoms of 8 rows (512 B); the
+// 16-byte chunk index k / 8 is XORed with (row / 2) % 4
+__host__ __device__ __forceinline__ uint32_t sw64_off(int row, int k) {
+    const int r = row & 7;
+    return (uint32_t)((row >> 3) * 512 + r * 64 + ((((k >> 3) ^ (r >> 1)) & 3) << 4) + (k & 7) * 2);
 }
 
 // shared-memory matrix descriptor (tcgen05 format): start >> 4 in [0,14),
-// leading-byte offset >> 4 in [16,30), stride-byte offset >> 4 in [32,46),
-// descriptor version 1 in [46,48), no swizzle (layout type 0 in [61,64))
+// leading-byte offset in [16,30) (unused by swizzled K-major layouts: 1),
+// stride-byte offset >> 4 in [32,46) (next 8-row atom: 512 B), descriptor
+// version 1 in [46,48), base offset 0, layout type 4 = 64-byte swizzle in
+// [61,64).  A K-step of 16 elements advances the start address by 32 B.
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
-           (1ull << 46);
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46) |
+           (4ull << 61);
 }
 
 // instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and
@@ -119,19 +132,18 @@ __device__ __forceinline__ void sts128(uint32_t addr, uint32_t a, uint32_t b, ui
 // ---------------------------------------------------------------------------
 // preparation
 // ---------------------------------------------------------------------------
-// per-mode FP32 factors from FP64: entry 8 * quarter + i holds
-// e^{i k (i + 32 quarter) dr} (the start offset of generator thread (i,
-// quarter) inside a tile), entry 32 holds the step e^{i k 8 dr}; zero for the
-// padding modes m >= M and the pad entry
-__global__ void k_ms_tables(int M, int M_pad, const double* __restrict__ kr, const double* __restrict__ ki,
-                            double dr, int lossless, float2* __restrict__ tab) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+// per-mode FP32 factors from FP64: entries 0-7 e^{i k i dr}, 8-15
+// e^{i k 32 j dr} (generator thread (i, part j) starts at range offset
+// i + 32 j of its tile), 16 the step e^{i k 8 dr}, 17 zero; zero rows for the
+// padding modes m >= M
+__device__ void ms_table_entry(int id, int M, int M_pad, const double* __restrict__ kr,
+                               const double* __restrict__ ki, double dr, int lossless, float2* __restrict__ tab) {
     if (id >= M_pad * kMsTabW) return;
     const int m = id / kMsTabW, e = id % kMsTabW;
     float2 v = make_float2(0.f, 0.f);
-    if (m < M && e <= 32) {
+    if (m < M && e <= 16) {
         const double a = kr[m], b = lossless ? 0.0 : ki[m];
-        const double off = e < 32 ? (double)((e & 7) + 32 * (e >> 3)) : 8.0;
+        const double off = e < 8 ? (double)e : e < 16 ? 32.0 * (e - 8) : 8.0;
         const double x = off * dr;
         double sn, cs;
         sincos(a * x, &sn, &cs);
@@ -143,9 +155,8 @@ __global__ void k_ms_tables(int M, int M_pad, const double* __restrict__ kr, con
 
 // tile phases e^{i k_m r_n0}, r_n0 = (tile * 128 + 1) dr: the phase k r is
 // reduced mod 2 pi in FP64 before the sine / cosine and the cast to FP32
-__global__ void k_ms_phase(int M, int M_pad, int n_tiles, const double* __restrict__ kr,
-                           const double* __restrict__ ki, double dr, int lossless, float2* __restrict__ q) {
-    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ void ms_phase_entry(long long id, int M, int M_pad, int n_tiles, const double* __restrict__ kr,
+                               const double* __restrict__ ki, double dr, int lossless, float2* __restrict__ q) {
     if (id >= (long long)n_tiles * M_pad) return;
     const int m = (int)(id % M_pad), tile = (int)(id / M_pad);
     if (m >= M) {
@@ -164,12 +175,11 @@ __global__ void k_ms_phase(int M, int M_pad, int n_tiles, const double* __restri
 }
 
 // A' chunk images (hi, lo) for every receiver group and K-chunk, in the
-// shared-memory layout above; vz is [n_rcv x M] (mode values at the
-// receiver grid points), vs the source values
-__global__ void k_ms_a(int n_rcv, int M, int n_chunks, const double* __restrict__ kr, const double* __restrict__ ki,
-                       const double* __restrict__ vs, const double* __restrict__ vz, int lossless,
-                       __nv_bfloat16* __restrict__ img) {
-    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// shared-memory layout above; mode values at receiver j are row idx[j] of the
+// full eigenvectors vfull [z][mode], vs the source values
+__device__ void ms_a_entry(long long id, int n_rcv, int M, int n_chunks, const double* __restrict__ kr,
+                           const double* __restrict__ ki, const double* __restrict__ vs, const int* __restrict__ idx,
+                           const double* __restrict__ vfull, int lossless, __nv_bfloat16* __restrict__ img) {
     const int n_groups = (n_rcv + kMsRcv - 1) / kMsRcv;
     const long long per_chunk = (long long)kMsRows * kMsKC;
     if (id >= (long long)n_groups * n_chunks * per_chunk) return;
@@ -184,17 +194,35 @@ __global__ void k_ms_a(int n_rcv, int M, int n_chunks, const double* __restrict_
         const double a = kr[m], b = lossless ? 0.0 : ki[m];
         const auto sk = csqrt_principal(a, b);
         const double den = sk.real() * sk.real() + sk.imag() * sk.imag();
-        const double c = vs[m] * vz[(size_t)j * M + m];
+        const double c = vs[m] * vfull[(size_t)idx[j] * M + m];
         const double are = c * sk.real() / den, aim = -c * sk.imag() / den;
         const bool im_row = row >= kMsRcv, im_col = (kl & 1) != 0;
         x = (float)(!im_row ? (im_col ? -aim : are) : (im_col ? are : aim));
     }
     const __nv_bfloat16 hi = __float2bfloat16_rn(x);
     const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-    const size_t base = (size_t)gc * 2 * (kMsOpBytes / 2);  // elements
-    const size_t off = core_off(row, kl) / 2;
+    const size_t base = (size_t)gc * 2 * (kMsABytes / 2);  // elements
+    const size_t off = sw64_off(row, kl) / 2;
     img[base + off] = hi;
-    img[base + kMsOpBytes / 2 + off] = lo;
+    img[base + kMsABytes / 2 + off] = lo;
+}
+
+// the three preparations in one launch: blocks [0, b_tab) fill the factor
+// rows, [b_tab, b_tab + b_q) the tile phases, the rest the A' images
+__global__ void k_ms_prepare(long long b_tab, long long b_q, int n_rcv, int M, int M_pad, int n_tiles, int n_chunks,
+                             const double* __restrict__ kr, const double* __restrict__ ki,
+                             const double* __restrict__ vs, const int* __restrict__ idx,
+                             const double* __restrict__ vfull, double dr, int lossless, float2* __restrict__ tab,
+                             float2* __restrict__ q, __nv_bfloat16* __restrict__ img) {
+    const long long b = blockIdx.x;
+    if (b < b_tab) {
+        ms_table_entry((int)(b * blockDim.x + threadIdx.x), M, M_pad, kr, ki, dr, lossless, tab);
+    } else if (b < b_tab + b_q) {
+        ms_phase_entry((b - b_tab) * blockDim.x + threadIdx.x, M, M_pad, n_tiles, kr, ki, dr, lossless, q);
+    } else {
+        ms_a_entry((b - b_tab - b_q) * blockDim.x + threadIdx.x, n_rcv, M, n_chunks, kr, ki, vs, idx, vfull,
+                   lossless, img);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -216,6 +244,26 @@ struct MsArgs {
     unsigned* err;
 };
 
+// position of a CTA's current unit, advanced chunk by chunk without division
+struct UnitPos {
+    int chunk, tile, group;
+    __device__ void init(long long u, int n_chunks, int n_tiles) {
+        chunk = (int)(u % n_chunks);
+        const long long gt = u / n_chunks;
+        tile = (int)(gt % n_tiles);
+        group = (int)(gt / n_tiles);
+    }
+    __device__ void next(int n_chunks, int n_tiles) {
+        if (++chunk == n_chunks) {
+            chunk = 0;
+            if (++tile == n_tiles) {
+                tile = 0;
+                ++group;
+            }
+        }
+    }
+};
+
 __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     extern __shared__ unsigned char ms_dyn[];
     __shared__ __align__(8) uint64_t full_a[kMsStages], full_b[kMsStages], empty[kMsStages];
@@ -231,12 +279,12 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     if (threadIdx.x == 0) {
         for (int s = 0; s < kMsStages; ++s) {
             mbar_init(&full_a[s], 1);
-            mbar_init(&full_b[s], kMsGenThreads);
+            mbar_init(&full_b[s], kMsGenWarps);
             mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < kMsAcc; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], kMsGenThreads);
+            mbar_init(&acc_empty[b], kMsGenWarps);
         }
         mbar_init(&drain, 1);
         fence_mbar_init();
@@ -252,32 +300,46 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     tc_fence_after();
     const uint32_t tmem = tmem_base_sh;
 
-    if (warp == 0) {
+    if (warp == kMsProducerWarp) {
         if (lane == 0 && nc > 0) {
-            // producer (bulk TMA of the A' chunk, factor rows, tile phases) and MMA issuer
-            auto load_stage = [&](int c, int slot) {
-                const long long u = u0 + c;
-                const long long g = u / ((long long)a.n_tiles * a.n_chunks);
-                const int chunk = (int)(u % a.n_chunks);
-                const int tile = (int)((u / a.n_chunks) % a.n_tiles);
+            // producer: bulk TMA of the A' chunk, factor rows and tile phases
+            // into stage c % kMsStages once the MMAs of chunk c - kMsStages are done
+            UnitPos pos;
+            pos.init(u0, a.n_chunks, a.n_tiles);
+            int issued = 0, landed = 0;
+            bool ok = true;
+            for (int c = 0; c < nc; ++c, pos.next(a.n_chunks, a.n_tiles)) {
+                const int slot = c % kMsStages;
+                if (c >= kMsStages) {
+                    ok = mbar_wait_bounded(&empty[slot], (uint32_t)(((c / kMsStages) - 1) & 1), a.err);
+                    if (!ok) break;
+                    landed = c - kMsStages + 1;  // its copies were consumed, so they landed
+                }
                 unsigned char* dst = sm + slot * kMsStageBytes;
                 mbar_expect_tx(&full_a[slot], kMsTxBytes);
-                tma_load_1d(dst, a.a_img + ((size_t)g * a.n_chunks + chunk) * 2 * kMsOpBytes, 2 * kMsOpBytes,
+                tma_load_1d(dst, a.a_img + ((size_t)pos.group * a.n_chunks + pos.chunk) * 2 * kMsABytes,
+                            2 * kMsABytes, &full_a[slot]);
+                tma_load_1d(dst + kMsOffTab, a.tab + (size_t)pos.chunk * kMsModes * kMsTabW, kMsTabBytes,
                             &full_a[slot]);
-                tma_load_1d(dst + 4 * kMsOpBytes, a.tab + (size_t)chunk * kMsModes * kMsTabW, kMsTabBytes,
+                tma_load_1d(dst + kMsOffQ, a.q + (size_t)pos.tile * a.M_pad + pos.chunk * kMsModes, kMsQBytes,
                             &full_a[slot]);
-                tma_load_1d(dst + 4 * kMsOpBytes + kMsTabBytes, a.q + (size_t)tile * a.M_pad + chunk * kMsModes,
-                            kMsQBytes, &full_a[slot]);
-            };
-            int issued = 0;
-            for (; issued < min(kMsStages, nc); ++issued) load_stage(issued, issued);
+                ++issued;
+            }
+            // copies still in flight after an early exit: wait for them
+            for (int c = landed; c < issued; ++c)
+                mbar_wait_drain(&full_a[c % kMsStages], (uint32_t)((c / kMsStages) & 1));
+        }
+    } else if (warp == 0) {
+        if (lane == 0 && nc > 0) {
+            // MMA issuer
+            UnitPos pos;
+            pos.init(u0, a.n_chunks, a.n_tiles);
             bool ok = true;
-            int waited_a = 0;  // chunks whose copies are known to have landed
-            int sg = -1;       // segment (one group and tile) counter
-            for (int c = 0; c < nc && ok; ++c) {
-                const int chunk = (int)((u0 + c) % a.n_chunks);
-                const bool first = c == 0 || chunk == 0;
-                const bool last = c == nc - 1 || chunk == a.n_chunks - 1;
+            int sg = -1;  // segment (one group and tile) counter
+            const uint64_t dsc0 = smem_desc(sm_addr);
+            for (int c = 0; c < nc && ok; ++c, pos.next(a.n_chunks, a.n_tiles)) {
+                const bool first = c == 0 || pos.chunk == 0;
+                const bool last = c == nc - 1 || pos.chunk == a.n_chunks - 1;
                 if (first) {
                     ++sg;
                     if (sg >= kMsAcc) {  // accumulator sg % 2 read out by the epilogue of segment sg - 2
@@ -288,32 +350,22 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                 }
                 const int s = c % kMsStages;
                 const uint32_t ph = (uint32_t)((c / kMsStages) & 1);
-                ok = mbar_wait_bounded(&full_a[s], ph, a.err);
-                if (!ok) break;
-                waited_a = c + 1;
-                ok = mbar_wait_bounded(&full_b[s], ph, a.err);
+                ok = mbar_wait_bounded(&full_a[s], ph, a.err) && mbar_wait_bounded(&full_b[s], ph, a.err);
                 if (!ok) break;
                 tc_fence_after();
-                const uint32_t st = sm_addr + s * kMsStageBytes;
+                // descriptors: the start-address field counts 16-byte units
+                const uint64_t st = dsc0 + (uint64_t)((s * kMsStageBytes) >> 4);
                 const uint32_t d = tmem + (uint32_t)((sg & 1) * kMsNT);
 #pragma unroll
                 for (int kk = 0; kk < kMsKC / 16; ++kk) {
-                    const uint32_t ah = st + kk * 256, al = ah + kMsOpBytes;
-                    const uint32_t bh = st + 2 * kMsOpBytes + kk * 256, bl = bh + kMsOpBytes;
-                    umma_bf16(d, smem_desc(ah), smem_desc(bh), (!first || kk > 0) ? 1u : 0u);
-                    umma_bf16(d, smem_desc(ah), smem_desc(bl), 1u);
-                    umma_bf16(d, smem_desc(al), smem_desc(bh), 1u);
+                    const uint64_t ah = st + (uint64_t)(kk * 32 >> 4), al = ah + (uint64_t)(kMsABytes >> 4);
+                    const uint64_t bh = st + (uint64_t)((kMsOffB + kk * 32) >> 4), bl = bh + (uint64_t)(kMsBBytes >> 4);
+                    umma_bf16(d, ah, bh, (!first || kk > 0) ? 1u : 0u);
+                    umma_bf16(d, ah, bl, 1u);
+                    umma_bf16(d, al, bh, 1u);
                 }
                 umma_commit(&empty[s]);
                 if (last) umma_commit(&acc_full[sg & 1]);
-                // refill the slot of chunk c - 1 once its MMAs are done
-                if (c >= 1 && issued < nc) {
-                    const int sp = (c - 1) % kMsStages;
-                    ok = mbar_wait_bounded(&empty[sp], (uint32_t)(((c - 1) / kMsStages) & 1), a.err);
-                    if (!ok) break;
-                    load_stage(issued, sp);
-                    ++issued;
-                }
             }
             if (!ok) {
                 // let the epilogue warps leave: a commit arrives once the
@@ -321,27 +373,23 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                 umma_commit(&acc_full[0]);
                 umma_commit(&acc_full[1]);
             }
-            for (int c = waited_a; c < issued; ++c)
-                mbar_wait_drain(&full_a[c % kMsStages], (uint32_t)((c / kMsStages) & 1));
             // every MMA complete before the accumulators are released
             umma_commit(&drain);
             mbar_wait_drain(&drain, 0u);
         }
     } else {
         // B' generators: thread -> (i = range in its 8-group, q = mode quad,
-        // quarter = which 32 ranges of the tile)
+        // part = which 32 ranges of the tile); one warp per part
         const int t = threadIdx.x - 32;
-        const int i = t & 7, q = (t >> 3) & 7, quarter = t >> 6;
-        const int col_half = (warp - 1) >> 2;  // epilogue: accumulator columns [64 col_half, +64)
+        const int i = t & 7, q = (t >> 3) & 3, part = t >> 5;
+        const int col_half = (warp - 1) >> 2;  // epilogue: accumulator columns [128 col_half, +128)
         bool ok = true;
         int sg = -1;
-        for (int c = 0; c < nc && ok; ++c) {
-            const long long u = u0 + c;
-            const int chunk = (int)(u % a.n_chunks);
-            const long long gt = u / a.n_chunks;  // group * n_tiles + tile
-            const int tile = (int)(gt % a.n_tiles);
-            const bool first = c == 0 || chunk == 0;
-            const bool last = c == nc - 1 || chunk == a.n_chunks - 1;
+        UnitPos pos;
+        pos.init(u0, a.n_chunks, a.n_tiles);
+        for (int c = 0; c < nc && ok; ++c, pos.next(a.n_chunks, a.n_tiles)) {
+            const bool first = c == 0 || pos.chunk == 0;
+            const bool last = c == nc - 1 || pos.chunk == a.n_chunks - 1;
             if (first) ++sg;
             const int s = c % kMsStages;
             if (c >= kMsStages) {
@@ -352,32 +400,36 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             ok = mbar_wait_bounded(&full_a[s], (uint32_t)((c / kMsStages) & 1), a.err);
             if (!ok) break;
             const unsigned char* stg = sm + s * kMsStageBytes;
-            const float2* tab_s = reinterpret_cast<const float2*>(stg + 4 * kMsOpBytes);
-            const float2* q_s = reinterpret_cast<const float2*>(stg + 4 * kMsOpBytes + kMsTabBytes);
+            const float2* tab_s = reinterpret_cast<const float2*>(stg + kMsOffTab);
+            const float2* q_s = reinterpret_cast<const float2*>(stg + kMsOffQ);
             float2 e[4], w[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 const float2* tb = tab_s + (4 * q + v) * kMsTabW;
-                e[v] = cmulf(q_s[4 * q + v], tb[8 * quarter + i]);
-                w[v] = tb[32];
+                e[v] = cmulf(cmulf(q_s[4 * q + v], tb[i]), tb[8 + part]);
+                w[v] = tb[16];
             }
-            const uint32_t bh = sm_addr + s * kMsStageBytes + 2 * kMsOpBytes;
+            const uint32_t bh = sm_addr + s * kMsStageBytes + kMsOffB;
 #pragma unroll
             for (int st8 = 0; st8 < 4; ++st8) {
-                const int grp = quarter * 4 + st8;  // 8-range group within the tile
-                const uint32_t off = (uint32_t)((grp * (kMsKC / 8) + q) * 128 + i * 16);
+                const int grp = part * 4 + st8;  // 8-range group within the tile
+                const uint32_t off = sw64_off(grp * 8 + i, 8 * q);
                 uint32_t h[4], l[4];
 #pragma unroll
                 for (int v = 0; v < 4; ++v) split2(e[v], h[v], l[v]);
                 sts128(bh + off, h[0], h[1], h[2], h[3]);
-                sts128(bh + kMsOpBytes + off, l[0], l[1], l[2], l[3]);
+                sts128(bh + kMsBBytes + off, l[0], l[1], l[2], l[3]);
                 if (st8 < 3) {
 #pragma unroll
                     for (int v = 0; v < 4; ++v) e[v] = cmulf(e[v], w[v]);
                 }
             }
+            // every lane's writes visible to the tensor cores, then one
+            // arrival per warp
             fence_proxy_async();
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full_b[s])) : "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full_b[s])) : "memory");
             if (!last) continue;
             // epilogue of segment sg: TMEM lanes 32 (warp % 4) .. +31 = rows;
             // the partial sum goes to slot (this CTA - first CTA of the tile)
@@ -389,15 +441,15 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             }
             tc_fence_after();
             const int row = 32 * (warp & 3) + lane;
-            const int g = (int)(gt / a.n_tiles);
-            const int part = blockIdx.x - ms_cta_of(gt * a.n_chunks, a.n_units, gridDim.x);
-            const int n0 = tile * kMsNT + 64 * col_half;
-            float* out = a.raw + (((size_t)part * a.groups + g) * kMsRows + row) * a.n_ranges;
+            const long long gt = (long long)pos.group * a.n_tiles + pos.tile;
+            const int part_slot = blockIdx.x - ms_cta_of(gt * a.n_chunks, a.n_units, gridDim.x);
+            const int n0 = pos.tile * kMsNT + (kMsNT / 2) * col_half;
+            float* out = a.raw + (((size_t)part_slot * a.groups + pos.group) * kMsRows + row) * a.n_ranges;
 #pragma unroll 1
-            for (int cb = 0; cb < 2; ++cb) {
+            for (int cb = 0; cb < kMsNT / 64; ++cb) {
                 uint32_t v[32];
                 const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) +
-                                       (uint32_t)((sg & 1) * kMsNT + 64 * col_half + cb * 32);
+                                       (uint32_t)((sg & 1) * kMsNT + (kMsNT / 2) * col_half + cb * 32);
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
                     "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
@@ -423,7 +475,9 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                 }
             }
             tc_fence_before();
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[sg & 1])) : "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[sg & 1])) : "memory");
         }
     }
     tc_fence_before();
@@ -436,27 +490,33 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
 }
 
 // P = C(r_n) (D_re + i D_im) -> [n_rcv x n_ranges] FP64, adding the partial
-// slots of the CTAs that shared the tile
-__global__ void k_ms_finish(int n_rcv, int n_ranges, double dr, int groups, int n_tiles, int n_chunks,
-                            long long n_units, int n_ctas, const float* __restrict__ raw, double* __restrict__ re,
-                            double* __restrict__ im) {
-    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= (long long)n_rcv * n_ranges) return;
-    const int n = (int)(id % n_ranges), j = (int)(id / n_ranges);
-    const int g = j / kMsRcv, jr = j % kMsRcv;
-    const long long u_first = ((long long)g * n_tiles + n / kMsNT) * n_chunks;
-    const int parts = ms_cta_of(u_first + n_chunks - 1, n_units, n_ctas) - ms_cta_of(u_first, n_units, n_ctas) + 1;
+// slots of the CTAs that shared the tile; C(r) = (cr + i ci) / sqrt(r).
+// Block (x = group * n_tiles + tile, y = receiver in the group), threads over
+// the tile's ranges.
+__global__ void __launch_bounds__(kMsNT) k_ms_finish(int n_rcv, int n_ranges, double dr, int groups, int n_tiles,
+                                                      int n_chunks, long long n_units, int n_ctas, double cr,
+                                                      double ci, const float* __restrict__ raw,
+                                                      double* __restrict__ re, double* __restrict__ im) {
+    __shared__ int parts_sh;
+    const int tile = blockIdx.x % n_tiles, g = blockIdx.x / n_tiles, jr = blockIdx.y;
+    if (threadIdx.x == 0) {
+        const long long u_first = ((long long)g * n_tiles + tile) * n_chunks;
+        parts_sh = ms_cta_of(u_first + n_chunks - 1, n_units, n_ctas) - ms_cta_of(u_first, n_units, n_ctas) + 1;
+    }
+    __syncthreads();
+    const int n = tile * kMsNT + threadIdx.x;
+    if (n >= n_ranges || g * kMsRcv + jr >= n_rcv) return;
     double dre = 0.0, dim = 0.0;
-    for (int p = 0; p < parts; ++p) {
+    for (int p = 0; p < parts_sh; ++p) {
         const float* base = raw + ((size_t)p * groups + g) * kMsRows * n_ranges;
         dre += base[(size_t)jr * n_ranges + n];
         dim += base[(size_t)(jr + kMsRcv) * n_ranges + n];
     }
-    const double r = (n + 1) * dr;
-    const double c0 = 1000.0 * 4 * kPi / sqrt(8.0 * kPi) / sqrt(r);
-    const double fr = c0 * sin(kPi * 0.25), fi = c0 * cos(kPi * 0.25);
-    re[id] = fr * dre - fi * dim;
-    im[id] = fr * dim + fi * dre;
+    const double sr = 1.0 / sqrt((n + 1) * dr);
+    const double fr = cr * sr, fi = ci * sr;
+    const size_t o = (size_t)(g * kMsRcv + jr) * n_ranges + n;
+    re[o] = fr * dre - fi * dim;
+    im[o] = fr * dim + fi * dre;
 }
 
 // gather of the mode values at the receiver grid points: vz[j][m] = v[idx_j][m]
@@ -486,7 +546,7 @@ MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms) {
         const int parts = ms_cta_of(uf + p.n_chunks - 1, p.n_units, p.n_ctas) - ms_cta_of(uf, p.n_units, p.n_ctas) + 1;
         p.n_parts = std::max(p.n_parts, parts);
     }
-    p.a_img_bytes = (size_t)p.groups * p.n_chunks * 2 * kMsOpBytes;
+    p.a_img_bytes = (size_t)p.groups * p.n_chunks * 2 * kMsABytes;
     p.q_bytes = (size_t)p.n_tiles * p.M_pad * sizeof(float2);
     p.tab_bytes = (size_t)p.M_pad * kMsTabW * sizeof(float2);
     p.raw_bytes = (size_t)p.n_parts * p.groups * kMsRows * n_ranges * sizeof(float);
@@ -501,22 +561,29 @@ int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const do
 }
 
 int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int n_rcv, int M, const double* kr, const double* ki,
-                      const double* vs, const double* vz, double dr, int lossless, void* a_img, void* q, void* tab) {
-    k_ms_tables<<<(p.M_pad * kMsTabW + 255) / 256, 256, 0, st>>>(M, p.M_pad, kr, ki, dr, lossless, (float2*)tab);
-    const long long nq = (long long)p.n_tiles * p.M_pad;
-    k_ms_phase<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(M, p.M_pad, p.n_tiles, kr, ki, dr, lossless,
-                                                              (float2*)q);
-    const long long na = (long long)p.groups * p.n_chunks * kMsRows * kMsKC;
-    k_ms_a<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(n_rcv, M, p.n_chunks, kr, ki, vs, vz, lossless,
-                                                          (__nv_bfloat16*)a_img);
-    return 3;
+                      const double* vs, const int* idx, const double* vfull, double dr, int lossless, void* a_img,
+                      void* q, void* tab) {
+    const long long n_tab = (long long)p.M_pad * kMsTabW;
+    const long long n_q = (long long)p.n_tiles * p.M_pad;
+    const long long n_a = (long long)p.groups * p.n_chunks * kMsRows * kMsKC;
+    const long long b_tab = (n_tab + 255) / 256, b_q = (n_q + 255) / 256, b_a = (n_a + 255) / 256;
+    k_ms_prepare<<<(unsigned)(b_tab + b_q + b_a), 256, 0, st>>>(
+        b_tab, b_q, n_rcv, M, p.M_pad, p.n_tiles, p.n_chunks, kr, ki, vs, idx, vfull, dr, lossless,
+        (float2*)tab, (float2*)q, (__nv_bfloat16*)a_img);
+    return 1;
 }
 
 int launch_ms_tc(cudaStream_t st, const MsPlan& p, int n_ranges, const void* a_img, const void* q, const void* tab,
                  float* raw, unsigned* err) {
     if (p.n_units <= 0) return 0;
-    if (cudaFuncSetAttribute(k_ms_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kMsSmem) != cudaSuccess)
-        return -1;
+    static bool attr_set[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+    if (!attr_set[dev]) {
+        if (cudaFuncSetAttribute(k_ms_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kMsSmem) != cudaSuccess)
+            return -1;
+        attr_set[dev] = true;  // setting it twice from two threads is harmless
+    }
     MsArgs a;
     a.a_img = (const unsigned char*)a_img;
     a.q = (const float2*)q;
@@ -535,9 +602,12 @@ int launch_ms_tc(cudaStream_t st, const MsPlan& p, int n_ranges, const void* a_i
 
 int launch_ms_finish(cudaStream_t st, const MsPlan& p, int n_rcv, int n_ranges, double dr, const float* raw,
                      double* re, double* im) {
-    const long long n = (long long)n_rcv * n_ranges;
-    k_ms_finish<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n_rcv, n_ranges, dr, p.groups, p.n_tiles, p.n_chunks,
-                                                              p.n_units, p.n_ctas, raw, re, im);
+    // 1000 * 4 pi i e^{-i pi/4} / sqrt(8 pi) = c0 (cos pi/4 + i sin pi/4)
+    const double c0 = 1000.0 * 4 * kPi / std::sqrt(8.0 * kPi);
+    const double cr = c0 * std::sin(kPi * 0.25), ci = c0 * std::cos(kPi * 0.25);
+    const dim3 grid((unsigned)(p.groups * p.n_tiles), (unsigned)std::min(n_rcv, kMsRcv));
+    k_ms_finish<<<grid, kMsNT, 0, st>>>(n_rcv, n_ranges, dr, p.groups, p.n_tiles, p.n_chunks, p.n_units, p.n_ctas,
+                                        cr, ci, raw, re, im);
     return 1;
 }
 

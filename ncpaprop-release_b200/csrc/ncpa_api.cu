@@ -1214,16 +1214,19 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
             CK(cudaMemsetAsync(ctx->ms_re.p, 0, nout * 8, st));
             CK(cudaMemsetAsync(ctx->ms_im.p, 0, nout * 8, st));
         } else {
+            // receiver indices through pinned memory: no host synchronisation
+            int* hidx = reinterpret_cast<int*>(pinned(ctx, (size_t)(n_rcv + 1) / 2));
+            std::memcpy(hidx, idx.data(), (size_t)n_rcv * 4);
             ctx->ms_idx.alloc((size_t)n_rcv * 4, st);
-            CK(cudaMemcpyAsync(ctx->ms_idx.p, idx.data(), (size_t)n_rcv * 4, cudaMemcpyHostToDevice, st));
-            ctx->ms_vz.alloc((size_t)n_rcv * M * 8, st);
-            check_launch(ctx, ncpa::launch_ms_gather(st, n_rcv, M, ctx->ms_idx.as<int>(),
-                                                     m->d_vfull.as<double>() + m->vfull_off[problem],
-                                                     ctx->ms_vz.as<double>()));
+            CK(cudaMemcpyAsync(ctx->ms_idx.p, hidx, (size_t)n_rcv * 4, cudaMemcpyHostToDevice, st));
+            const double* vfull = m->d_vfull.as<double>() + m->vfull_off[problem];
             const double* kr = m->d_kr.as<double>() + pi.off;
             const double* ki = m->d_ki.as<double>() + pi.off;
             const double* vs = m->d_vs.as<double>() + pi.off;
             if (method == NCPA_SUM_FP64) {
+                ctx->ms_vz.alloc((size_t)n_rcv * M * 8, st);
+                check_launch(ctx, ncpa::launch_ms_gather(st, n_rcv, M, ctx->ms_idx.as<int>(), vfull,
+                                                         ctx->ms_vz.as<double>()));
                 tm.mark("ms-prep");
                 check_launch(ctx, ncpa::launch_tl2d_rcv_major(st, M, kr, ki, vs, ctx->ms_vz.as<double>(), n_rcv, nr,
                                                               tp->dr_m, tp->lossless, ctx->ms_re.as<double>(),
@@ -1235,7 +1238,7 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
                 ctx->ms_q.alloc(pl.q_bytes, st);
                 ctx->ms_tab.alloc(pl.tab_bytes, st);
                 ctx->ms_raw.alloc(pl.raw_bytes, st);
-                check_launch(ctx, ncpa::launch_ms_prepare(st, pl, n_rcv, M, kr, ki, vs, ctx->ms_vz.as<double>(),
+                check_launch(ctx, ncpa::launch_ms_prepare(st, pl, n_rcv, M, kr, ki, vs, ctx->ms_idx.as<int>(), vfull,
                                                           tp->dr_m, tp->lossless, ctx->ms_img.p, ctx->ms_q.p,
                                                           ctx->ms_tab.p));
                 tm.mark("ms-prep");

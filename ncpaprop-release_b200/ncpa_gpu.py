@@ -355,12 +355,19 @@ class Modes:
         self.ctx.check(lib().ncpa_modes_get_vectors(self.h, p, _p(v)), "ncpa_modes_get_vectors")
         return v.reshape(nz, M)
 
-    def tl1d(self, n_ranges, dr_m, lossless=False, to_host=True):
+    def tl1d(self, n_ranges, dr_m, lossless=False, to_host=True, out=None):
+        """1-D TL of every problem; out = (re, im, inc) C-contiguous float64
+        arrays of shape (P, n_ranges) to fill (e.g. views of pinned memory)."""
         tp = _TlParams(int(n_ranges), float(dr_m), int(lossless))
         if not to_host:
             self.ctx.check(lib().ncpa_tl_1d(self.ctx.h, self.h, ctypes.byref(tp), None, None, None), "ncpa_tl_1d")
             return None
-        re, im, inc = (np.empty((self.P, n_ranges)) for _ in range(3))
+        if out is not None:
+            re, im, inc = out
+            for a in out:
+                assert a.dtype == np.float64 and a.flags.c_contiguous and a.shape == (self.P, n_ranges)
+        else:
+            re, im, inc = (np.empty((self.P, n_ranges)) for _ in range(3))
         self.ctx.check(lib().ncpa_tl_1d(self.ctx.h, self.h, ctypes.byref(tp), _p(re), _p(im), _p(inc)),
                        "ncpa_tl_1d")
         return re, im, inc
@@ -387,10 +394,13 @@ class Modes:
                                            _p(re), _p(im)), "ncpa_tl_multi")
         return (re + 1j * im) if to_host else None
 
-    def bb_synthesize(self, ranges_m, max_celerity, nfft, src_re, src_im, zero_attn=False, to_host=True):
+    def bb_synthesize(self, ranges_m, max_celerity, nfft, src_re, src_im, zero_attn=False, to_host=True, out=None):
         rng, sre, sim = _f64(ranges_m), _f64(src_re), _f64(src_im)
         bp = _BbParams(len(rng), _p(rng), float(max_celerity), int(nfft), _p(sre), _p(sim), int(zero_attn))
-        out = np.empty((len(rng), nfft)) if to_host else None
+        if out is not None:
+            assert out.dtype == np.float64 and out.flags.c_contiguous and out.shape == (len(rng), nfft)
+        elif to_host:
+            out = np.empty((len(rng), nfft))
         self.ctx.check(lib().ncpa_bb_synthesize_modes(self.ctx.h, self.h, 0, ctypes.byref(bp), _p(out)),
                        "ncpa_bb_synthesize_modes")
         return out
