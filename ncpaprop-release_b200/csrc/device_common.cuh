@@ -242,6 +242,97 @@ struct SturmState {
     }
 };
 
+// Sign bits w of 32 steps (first step in bit 31) folded into a chain's count,
+// then the exact power-of-two rescale of its last two values.
+__device__ __forceinline__ void sturm_fold(SturmState& S, unsigned w) {
+    const unsigned prev = (w >> 1) | (S.prevbit << 31);
+    S.cnt += __popc(w ^ prev);
+    S.prevbit = w & 1u;
+    const int sh = rescale_shift(S.p0, S.p1);
+    if (sh) {
+        const double sc = pow2(-sh);
+        S.p0 *= sc;
+        S.p1 *= sc;
+    }
+}
+
+// 32 steps of two independent chains (shifts xa, xb) interleaved step by
+// step, so the warp always has two dependent FMA chains in flight; the
+// arithmetic of each chain is exactly that of SturmState::word32
+__device__ __forceinline__ void sturm_word32_pair(SturmState& A, SturmState& B, const double* __restrict__ s,
+                                                  double xa, double xb) {
+    unsigned wa = 0u, wb = 0u;
+    double pa0 = A.p0, pa1 = A.p1, pb0 = B.p0, pb1 = B.p1;
+#pragma unroll
+    for (int u = 0; u < 32; u += 2) {
+        const double2 sv = *reinterpret_cast<const double2*>(s + u);
+        const double qa0 = fma(sv.x - xa, pa1, -pa0);
+        const double qb0 = fma(sv.x - xb, pb1, -pb0);
+        const double qa1 = fma(sv.y - xa, qa0, -pa1);
+        const double qb1 = fma(sv.y - xb, qb0, -pb1);
+        wa = __funnelshift_l(__double2hiint(qa0), wa, 1);
+        wb = __funnelshift_l(__double2hiint(qb0), wb, 1);
+        wa = __funnelshift_l(__double2hiint(qa1), wa, 1);
+        wb = __funnelshift_l(__double2hiint(qb1), wb, 1);
+        pa0 = qa0;
+        pa1 = qa1;
+        pb0 = qb0;
+        pb1 = qb1;
+    }
+    A.p0 = pa0;
+    A.p1 = pa1;
+    B.p0 = pb0;
+    B.p1 = pb1;
+    sturm_fold(A, wa);
+    sturm_fold(B, wb);
+}
+
+// same with chain A also carrying its x-derivative (SturmState::word32_deriv)
+__device__ __forceinline__ void sturm_word32_deriv_pair(SturmState& A, double& d0, double& d1, SturmState& B,
+                                                        const double* __restrict__ s, double xa, double xb) {
+    unsigned wa = 0u, wb = 0u;
+    double pa0 = A.p0, pa1 = A.p1, pb0 = B.p0, pb1 = B.p1;
+#pragma unroll
+    for (int u = 0; u < 32; u += 2) {
+        const double2 sv = *reinterpret_cast<const double2*>(s + u);
+        const double a0 = sv.x - xa, a1 = sv.y - xa;
+        const double qa0 = fma(a0, pa1, -pa0);
+        const double qb0 = fma(sv.x - xb, pb1, -pb0);
+        const double e0 = fma(a0, d1, -pa1) - d0;
+        const double qa1 = fma(a1, qa0, -pa1);
+        const double qb1 = fma(sv.y - xb, qb0, -pb1);
+        const double e1 = fma(a1, e0, -qa0) - d1;
+        wa = __funnelshift_l(__double2hiint(qa0), wa, 1);
+        wb = __funnelshift_l(__double2hiint(qb0), wb, 1);
+        wa = __funnelshift_l(__double2hiint(qa1), wa, 1);
+        wb = __funnelshift_l(__double2hiint(qb1), wb, 1);
+        pa0 = qa0;
+        pa1 = qa1;
+        pb0 = qb0;
+        pb1 = qb1;
+        d0 = e0;
+        d1 = e1;
+    }
+    A.p0 = pa0;
+    A.p1 = pa1;
+    B.p0 = pb0;
+    B.p1 = pb1;
+    {  // chain A: counts, then the joint rescale of p and its derivative
+        const unsigned prev = (wa >> 1) | (A.prevbit << 31);
+        A.cnt += __popc(wa ^ prev);
+        A.prevbit = wa & 1u;
+        const int sh = rescale_shift(fmax(fabs(A.p0), fabs(d0)), fmax(fabs(A.p1), fabs(d1)));
+        if (sh) {
+            const double sc = pow2(-sh);
+            A.p0 *= sc;
+            A.p1 *= sc;
+            d0 *= sc;
+            d1 *= sc;
+        }
+    }
+    sturm_fold(B, wb);
+}
+
 // principal square root of x + i y
 __device__ __forceinline__ cuda::std::complex<double> csqrt_principal(double x, double y) {
     double m = hypot(x, y);

@@ -609,19 +609,13 @@ __device__ void warp_sweep(const double* __restrict__ s, int nz, double x0, doub
         const int valid = min(kWChunk, nz - c * kWChunk);
         const int nw = valid >> 5;
         if (mode == 0) {
-            for (int w = 0; w < nw; ++w) {
-                A.word32(b + 32 * w, x0);
-                B.word32(b + 32 * w, x1);
-            }
+            for (int w = 0; w < nw; ++w) sturm_word32_pair(A, B, b + 32 * w, x0, x1);
             for (int i = nw * 32; i < valid; ++i) {
                 A.step(b[i], x0);
                 B.step(b[i], x1);
             }
         } else if (mode == 1) {
-            for (int w = 0; w < nw; ++w) {
-                A.word32_deriv(b + 32 * w, x0, da0, da1);
-                B.word32(b + 32 * w, x1);
-            }
+            for (int w = 0; w < nw; ++w) sturm_word32_deriv_pair(A, da0, da1, B, b + 32 * w, x0, x1);
             for (int i = nw * 32; i < valid; ++i) {
                 A.step_deriv(b[i], x0, da0, da1);
                 B.step(b[i], x1);

@@ -113,6 +113,7 @@ struct ncpa_ctx {
     std::map<int, DevBuf> twiddle; // per nfft
     DevBuf bb_out;                 // waveforms kept in HBM (NULL host buffer)
     DevBuf ms_img, ms_q, ms_tab, ms_raw, ms_vz, ms_idx, ms_re, ms_im;  // modal-sum scratch (grow-only)
+    int item_override = 0;         // eigenvalues per bisection item (0: chosen per solve); NCPA_BISECT_ITEM
     double* h_pin = nullptr;       // small pinned host buffer for scalars read back per solve
     size_t h_pin_n = 0;
     DevBuf d_stats;                // device counters (Sturm sequences)
@@ -428,7 +429,15 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
         }
         pi.off = off;
         off += pi.M;
-        const int nit = (pi.M + ncpa::kWItem - 1) / ncpa::kWItem;
+    }
+    // eigenvalues per bisection item: 32 (one per lane).  Smaller items give
+    // each eigenvalue more shifts per round but cost more Sturm sequences in
+    // total, which measured slower on the 256-frequency workload (16: +26 %,
+    // 8: +100 %); NCPA_BISECT_ITEM overrides it for tuning.
+    const int item_sz = ctx->item_override > 0 ? ctx->item_override : ncpa::kWItem;
+    for (int p = 0; p < P; ++p) {
+        const ProblemInfo& pi = M->info[p];
+        const int nit = (pi.M + item_sz - 1) / item_sz;
         for (int k = 0; k < nit; ++k) {
             int j0 = (int)((long long)pi.M * k / nit), j1 = (int)((long long)pi.M * (k + 1) / nit);
             items.push_back(WorkItem{p, j0, j1 - j0, 0});
@@ -678,6 +687,11 @@ ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
         CK(cudaStreamSynchronize(ctx->stream));
         const char* tv = std::getenv("NCPA_TIMING");
         ctx->timing = tv && tv[0] == '1';
+        // tuning override of the eigenvalues per bisection item (1..32)
+        if (const char* iv = std::getenv("NCPA_BISECT_ITEM")) {
+            const int v = std::atoi(iv);
+            if (v >= 1 && v <= 32) ctx->item_override = v;
+        }
         return NCPA_OK;
     });
     if (s != NCPA_OK) return s;
