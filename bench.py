@@ -561,7 +561,18 @@ def main():
                     help="device-resident leg only (no e2e, plain-path or CPU legs); for profiler runs")
     ap.add_argument("--no-modal-sum", action="store_true", help="skip the tensor-core modal-sum leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the served request-stream leg")
+    ap.add_argument("--only-modal-sum", action="store_true",
+                    help="run only the tensor-core modal-sum leg and print its JSON (for profiler runs)")
     args = ap.parse_args()
+    if args.only_modal_sum:
+        import torch
+        import ncpa_gpu
+
+        ctx = ncpa_gpu.Context(0)
+        print(json.dumps(modal_sum_leg(ctx, torch.cuda.ExternalStream(ctx.stream_ptr), _bf16_peak(), k=3)),
+              flush=True)
+        ctx.close()
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
