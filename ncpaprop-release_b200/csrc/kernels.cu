@@ -639,8 +639,10 @@ __device__ void warp_sweep(const double* __restrict__ s, int nz, double x0, doub
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
     k_bisect(const ProblemInfo* __restrict__ pinfo, const double* __restrict__ s, int nz, int nz_pad,
              const int* __restrict__ counts, const WorkItem* __restrict__ items, int n_items, int* counter,
-             double tol, double* __restrict__ mu, unsigned* err, unsigned long long* seq_counter) {
+             double tol, double* __restrict__ mu, unsigned* err, unsigned long long* seq_counter,
+             const int* __restrict__ n_items_dev) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    if (n_items_dev) n_items = *n_items_dev;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     WarpRing r;
     r.buf = reinterpret_cast<double*>(smem_raw) + (size_t)wid * kWBuf * kWChunk;
@@ -651,11 +653,11 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
         fence_mbar_init();
     }
     __syncwarp();
-    for (;;) {
-        int it = 0;
-        if (lane == 0) it = atomicAdd(counter, 1);
-        it = __shfl_sync(0xffffffffu, it, 0);
-        if (it >= n_items) break;
+    // static round-robin over the grid's warps: item g goes to warp g of the
+    // first wave, so the items spread evenly over the SMs whatever the grid
+    (void)counter;
+    const int warps_total = gridDim.x * kWarpsPerCta;
+    for (int it = blockIdx.x * kWarpsPerCta + wid; it < n_items; it += warps_total) {
         const WorkItem w = items[it];
         const ProblemInfo pi = pinfo[w.problem];
         const int* cnt = counts + (size_t)w.problem * kScanPoints;
@@ -781,11 +783,11 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
 
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
                   const int* counts, const WorkItem* items, int n_items, int* counter, double tol, double* mu,
-                  unsigned* err, unsigned long long* seq_counter) {
+                  unsigned* err, unsigned long long* seq_counter, const int* n_items_dev) {
     const size_t sm = (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8 + kWBuf * 8);
     cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_bisect<<<grid, kWarpsPerCta * 32, sm, st>>>(pinfo, s, nz, nz_pad, counts, items, n_items, counter, tol, mu,
-                                                  err, seq_counter);
+                                                  err, seq_counter, n_items_dev);
     return 1;
 }
 
@@ -795,6 +797,87 @@ int bisect_ctas_per_sm() {
     cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bisect, kWarpsPerCta * 32, sm) != cudaSuccess) n = 1;
     return n < 1 ? 1 : n;
+}
+
+// ===========================================================================
+// Work items on the device (one CTA): the host-side item building of the
+// solve without a round trip
+// ===========================================================================
+constexpr int kItemThreads = 1024;
+
+// exclusive block scan of v over the CTA; returns the prefix, *total the sum
+__device__ int block_exclusive_scan(int v, int* sh, int* total) {
+    const int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int o = 1; o < kItemThreads; o <<= 1) {
+        const int a = t >= o ? sh[t - o] : 0;
+        __syncthreads();
+        sh[t] += a;
+        __syncthreads();
+    }
+    const int incl = sh[t];
+    *total = sh[kItemThreads - 1];
+    __syncthreads();
+    return incl - v;
+}
+
+__global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo* __restrict__ pinfo,
+                                                             const int* __restrict__ counts, int max_modes,
+                                                             WorkItem* __restrict__ bis, WorkItem* __restrict__ ev,
+                                                             int item_cap, int* __restrict__ tot,
+                                                             unsigned* __restrict__ err) {
+    __shared__ int sh[kItemThreads];
+    int base_m = 0, base_b = 0, base_e = 0;
+    for (int p0 = 0; p0 < P; p0 += kItemThreads) {
+        const int p = p0 + threadIdx.x;
+        int M = 0, nb = 0, ne = 0;
+        if (p < P) {
+            const int c_lo = counts[(size_t)p * kScanPoints];
+            const int c_hi = counts[(size_t)p * kScanPoints + kScanPoints - 1];
+            M = max(0, c_hi - c_lo);
+            if (M > max_modes) {
+                atomicOr(err, kErrTooMany);
+                M = max_modes;
+            }
+            pinfo[p].c_lo = c_lo;
+            pinfo[p].c_hi = c_hi;
+            pinfo[p].M = M;
+            nb = (M + kWItem - 1) / kWItem;
+            ne = (M + kEvItem - 1) / kEvItem;
+        }
+        int tm, tb, te;
+        const int om = block_exclusive_scan(M, sh, &tm);
+        const int ob = block_exclusive_scan(nb, sh, &tb);
+        const int oe = block_exclusive_scan(ne, sh, &te);
+        if (p < P) {
+            pinfo[p].off = base_m + om;
+            for (int k = 0; k < nb; ++k) {
+                const int j0 = (int)((long long)M * k / nb), j1 = (int)((long long)M * (k + 1) / nb);
+                const int q = base_b + ob + k;
+                if (q < item_cap) bis[q] = WorkItem{p, j0, j1 - j0, 0};
+            }
+            for (int k = 0; k < ne; ++k) {
+                const int q = base_e + oe + k;
+                if (q < item_cap) ev[q] = WorkItem{p, k * kEvItem, min(kEvItem, M - k * kEvItem), 0};
+            }
+        }
+        base_m += tm;
+        base_b += tb;
+        base_e += te;
+    }
+    if (threadIdx.x == 0) {
+        if (base_b > item_cap || base_e > item_cap) atomicOr(err, kErrTooMany);
+        tot[0] = min(base_b, item_cap);
+        tot[1] = min(base_e, item_cap);
+        tot[2] = base_m;
+    }
+}
+
+int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes,
+                      WorkItem* bis_items, WorkItem* ev_items, int item_cap, int* tot, unsigned* err) {
+    k_make_items<<<1, kItemThreads, 0, st>>>(P, pinfo, counts, max_modes, bis_items, ev_items, item_cap, tot, err);
+    return 1;
 }
 
 // ===========================================================================
@@ -957,11 +1040,10 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
             ae = cke[ci];
         }
     };
-    for (;;) {
-        int it = 0;
-        if (lane == 0) it = atomicAdd(A.counter, 1);
-        it = __shfl_sync(0xffffffffu, it, 0);
-        if (it >= A.n_items) break;
+    const int n_items_all = A.n_items_dev ? *A.n_items_dev : A.n_items;
+    // static round-robin over the grid's warps (see k_bisect)
+    const int warps_total = gridDim.x * kEvWarps;
+    for (int it = blockIdx.x * kEvWarps + wid; it < n_items_all; it += warps_total) {
         const WorkItem w = A.items[it];
         const ProblemInfo pi = A.pinfo[w.problem];
         const double* sp = A.s + (size_t)w.problem * A.nz_pad;

@@ -12,6 +12,7 @@ enum : unsigned {
     kErrTimeout = 1u,  // a bounded mbarrier wait gave up
     kErrBracket = 2u,  // bisection bracket inconsistent with the Sturm counts
     kErrWkb = 4u,      // WKB search needed more trial wavenumbers than threads
+    kErrTooMany = 8u,  // a problem has more modes than allowed (device-built work items)
 };
 
 // Per (frequency, azimuth) problem, device resident.
@@ -74,7 +75,8 @@ int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* 
 // multisection/bisection over work items (K3)
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
                   const int* counts, const WorkItem* items, int n_items, int* counter, double tol, double* mu,
-                  unsigned* err, unsigned long long* seq_counter);
+                  unsigned* err, unsigned long long* seq_counter,
+                  const int* n_items_dev = nullptr);
 int bisect_ctas_per_sm();
 // FP64 throughput probe: each thread runs n_iter iterations of 8 independent
 // FMA chains; out receives a value that keeps the chains live
@@ -88,6 +90,7 @@ struct EigvecArgs {
     int nz, nz_pad, wstride, n_az;
     const WorkItem* items;
     int n_items;
+    const int* n_items_dev;  // when set, the item count is read here (built on the device)
     int* counter;
     const double* mu;
     int isrc, ircv;
@@ -106,6 +109,13 @@ struct EigvecArgs {
     unsigned* err;
 };
 int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a);
+// Work items built on the device from the Sturm scan: per problem c_lo, c_hi,
+// M and CSR offset in pinfo; bisection items (32 eigenvalues, balanced) and
+// eigenvector items (kEvItem) appended; tot = {n_bisect_items, n_eigvec_items,
+// total modes}.  Sets kErrTooMany if a problem exceeds max_modes (its M is
+// then clamped) or the item capacity is exceeded.
+int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes,
+                      WorkItem* bis_items, WorkItem* ev_items, int item_cap, int* tot, unsigned* err);
 // resident eigenvector CTAs per SM for the variant selected by a
 int eigvec_ctas_per_sm(const EigvecArgs& a);
 // modal sums

@@ -115,6 +115,7 @@ struct ncpa_ctx {
     DevBuf ms_img, ms_q, ms_tab, ms_raw, ms_vz, ms_idx, ms_re, ms_im;  // modal-sum scratch (grow-only)
     int item_override = 0;         // eigenvalues per bisection item (0: chosen per solve); NCPA_BISECT_ITEM
     double* h_pin = nullptr;       // small pinned host buffer for scalars read back per solve
+    int* h_tot = nullptr;          // pinned: item and mode totals of a device-built solve
     size_t h_pin_n = 0;
     DevBuf d_stats;                // device counters (Sturm sequences)
     bool timing = false;           // NCPA_TIMING=1: per-phase times on stderr
@@ -390,6 +391,105 @@ void build_problems(ncpa_ctx* ctx, PhaseTimer& tm, const ncpa_profile* prof, con
     tm.mark("matrix");
 }
 
+// Bisection and eigenvectors with the work items built on the device from
+// the scan counts (k_make_items): the host enqueues everything without a
+// round trip and reads the mode counts back once at the end.  Output arrays
+// are sized for max_modes per problem.
+void solve_core_device_items(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_params* prm, DevBuf& s,
+                             DevBuf& w, DevBuf& g, DevBuf& counts, int w_per_az) {
+    cudaStream_t st = ctx->stream;
+    const int P = M->P, nz = M->nz, nz_pad = M->nz_pad;
+    const double dz = M->dz;
+    ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
+    const int cap_modes = M->prm.max_modes;
+    const size_t mcap = (size_t)P * cap_modes;
+    const int item_cap = P * ((cap_modes + ncpa::kWItem - 1) / ncpa::kWItem);
+    DevBuf bis, ev, tot, mu, d_counter;
+    bis.alloc((size_t)item_cap * sizeof(WorkItem), st);
+    ev.alloc((size_t)item_cap * sizeof(WorkItem), st);
+    tot.alloc(4 * sizeof(int), st);
+    check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, counts.as<int>(), cap_modes, bis.as<WorkItem>(),
+                                              ev.as<WorkItem>(), item_cap, tot.as<int>(), ctx->d_err.as<unsigned>()));
+    mu.alloc(mcap * 8, st);
+    M->d_kr.alloc(mcap * 8, st);
+    M->d_ki.alloc(mcap * 8, st);
+    M->d_vs.alloc(mcap * 8, st);
+    M->d_vr.alloc(mcap * 8, st);
+    M->d_vg.alloc(mcap * 8, st);
+    d_counter.alloc(2 * sizeof(int), st);
+    CK(cudaMemsetAsync(d_counter.p, 0, 2 * sizeof(int), st));
+    tm.mark("host-items");
+    const int grid_b = ctx->num_sms * ncpa::bisect_ctas_per_sm();
+    check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
+                                          bis.as<WorkItem>(), 0, d_counter.as<int>(), kBisectTol, mu.as<double>(),
+                                          ctx->d_err.as<unsigned>(),
+                                          ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr,
+                                          tot.as<int>()));
+    if (ctx->stats) ctx->grid_points += nz;
+    tm.mark("bisect");
+    ncpa::EigvecArgs ea{};
+    ea.pinfo = d_pinfo;
+    ea.s = s.as<double>();
+    ea.w = w.as<double>();
+    ea.g = prm->want_group_speed ? g.as<double>() : nullptr;
+    ea.nz = nz;
+    ea.nz_pad = nz_pad;
+    ea.wstride = nz_pad;
+    ea.n_az = w_per_az;
+    ea.items = ev.as<WorkItem>();
+    ea.n_items = 0;
+    ea.n_items_dev = tot.as<int>() + 1;
+    ea.counter = d_counter.as<int>() + 1;
+    ea.mu = mu.as<double>();
+    ea.isrc = M->isrc;
+    ea.ircv = M->ircv;
+    ea.dz = dz;
+    ea.h2 = dz * dz;
+    ea.kr = M->d_kr.as<double>();
+    ea.ki = M->d_ki.as<double>();
+    ea.vs = M->d_vs.as<double>();
+    ea.vr = M->d_vr.as<double>();
+    ea.vg = M->d_vg.as<double>();
+    const int ewpc = ncpa::kEvWarpsPerCta;
+    const int grid_e = std::min(item_cap / ewpc + 1, ctx->num_sms * ncpa::eigvec_ctas_per_sm(ea));
+    const long long nblk = (nz + ncpa::kBlk - 1) / ncpa::kBlk;
+    const long long slot = nblk * 32;
+    const size_t need = (size_t)grid_e * ewpc * slot;
+    if (ctx->ck1.bytes < need * 8) {
+        ctx->ck1.alloc(need * 8, st);
+        ctx->ck2.alloc(need * 8, st);
+        ctx->cke.alloc(need * 4, st);
+    }
+    ea.ck_q1 = ctx->ck1.as<double>();
+    ea.ck_q2 = ctx->ck2.as<double>();
+    ea.ck_e = ctx->cke.as<int>();
+    ea.ck_slot_stride = slot;
+    ea.err = ctx->d_err.as<unsigned>();
+    check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
+    tm.mark("eigvec");
+    // ---- counts and offsets back, then the modes ----
+    int* h_tot = ctx->h_tot;
+    CK(cudaMemcpyAsync(h_tot, tot.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(M->info.data(), d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
+    unsigned h_err = 0;
+    CK(cudaMemcpyAsync(&h_err, ctx->d_err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h_err & ncpa::kErrTooMany) {
+        CK(cudaMemsetAsync(ctx->d_err.p, 0, sizeof(unsigned), st));
+        int worst = 0;
+        for (int p = 0; p < P; ++p)
+            if (M->info[p].c_hi - M->info[p].c_lo > M->info[worst].c_hi - M->info[worst].c_lo) worst = p;
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "problem %d (f=%g Hz, az=%g) has %d modes > max_modes %d", worst,
+                      M->info[worst].freq, M->info[worst].az, M->info[worst].c_hi - M->info[worst].c_lo, cap_modes);
+        throw ApiError(NCPA_ETOOMANY, buf);
+    }
+    M->Mtot = h_tot[2];
+    if (!prm->keep_on_device) fetch_modes(M);
+    check_device_status(ctx);
+    tm.mark("fetch");
+}
+
 // Window, Sturm scan, work items, bisection and eigenvectors over all
 // problems of M (their matrices built).  w holds one weight row per
 // frequency when w_per_az > 0 (problem p uses row p / w_per_az).
@@ -409,6 +509,10 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
     check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
                                         ctx->d_err.as<unsigned>()));
     tm.mark("scan");
+    if (!prm->want_vectors) {
+        solve_core_device_items(ctx, tm, M, prm, s, w, g, counts, w_per_az);
+        return;
+    }
     std::vector<int> hcounts((size_t)P * ncpa::kScanPoints);
     CK(cudaMemcpyAsync(hcounts.data(), counts.p, hcounts.size() * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(M->info.data(), d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
@@ -685,6 +789,7 @@ ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
         ctx->d_stats.alloc(4 * sizeof(unsigned long long), ctx->stream);
         CK(cudaMemsetAsync(ctx->d_stats.p, 0, 4 * sizeof(unsigned long long), ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        CK(cudaHostAlloc((void**)&ctx->h_tot, 64, cudaHostAllocDefault));
         const char* tv = std::getenv("NCPA_TIMING");
         ctx->timing = tv && tv[0] == '1';
         // tuning override of the eigenvalues per bisection item (1..32)
@@ -715,6 +820,7 @@ ncpa_status ncpa_ctx_destroy(ncpa_ctx* ctx) {
         b->release();  // stream-ordered frees need the stream alive
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
+    if (ctx->h_tot) cudaFreeHost(ctx->h_tot);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NCPA_OK;
