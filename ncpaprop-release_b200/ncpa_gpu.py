@@ -97,6 +97,7 @@ def lib():
         L.ncpa_profile_info.argtypes = [_vp, _ip, _dp, _dp]
         L.ncpa_ess_params_default.argtypes = [ctypes.POINTER(EssParams)]
         L.ncpa_ess_params_default.restype = None
+        L.ncpa_profile_load_attn.argtypes = [_vp, ctypes.c_char_p]
         L.ncpa_ess_solve_jobs.argtypes = [_vp, ctypes.POINTER(_EssJob), _c_int, ctypes.POINTER(EssParams),
                                           ctypes.POINTER(_vp)]
         L.ncpa_ess_solve.argtypes = [_vp, _vp, ctypes.POINTER(EssParams), _dp, _c_int, _dp, _c_int,
@@ -287,6 +288,10 @@ class Profile:
         self.ctx.check(lib().ncpa_profile_info(self.h, ctypes.byref(n), ctypes.byref(lo), ctypes.byref(hi)),
                        "ncpa_profile_info")
         return n.value, lo.value, hi.value
+
+    def load_attn(self, path):
+        """User attenuation table (height km, Np/m), the --use_attn_file option."""
+        self.ctx.check(lib().ncpa_profile_load_attn(self.h, str(path).encode()), "ncpa_profile_load_attn")
 
     def close(self):
         if self.h:
