@@ -10,6 +10,7 @@
 #include "cli_common.hpp"
 #include "cli_ess.hpp"
 #include "cli_params.hpp"
+#include "solvers.hpp"
 
 using ncpa_cli::Params;
 
@@ -115,7 +116,9 @@ int main(int argc, char** argv) {
     }
     const std::time_t t1 = std::time(nullptr);
     try {
-        ncpa_cli::run_ess(param);
+        ncpa_gpu_solvers::ESSModeSolver a(&param);  // as Modess_main.cpp:87-97
+        a.solve();
+        a.printParams();
     } catch (const std::exception& e) {
         std::cerr << "Modess: " << e.what() << std::endl;
         return 2;
