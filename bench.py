@@ -73,18 +73,61 @@ def _nfft(nfreq_with_dc, n_wave):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 2 ms from a thread (the same counters
+    nvidia-smi reports), or nvidia-smi -lms 20 where NVML is unavailable.
+    Read-only: nothing here changes a GPU setting."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device):
         self.device = device
         self.proc = None
         self.lines = []
+        self.samples = []  # (sm MHz, max sm MHz, set of reason names)
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        u = str(torch.cuda.get_device_properties(self.device).uuid)
+        return pynvml, pynvml.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+
+    def _poll_nvml(self, nv, h):
+        bits = ((nv.nvmlClocksEventReasonHwSlowdown, "hw_slowdown"),
+                (nv.nvmlClocksEventReasonHwThermalSlowdown, "hw_thermal_slowdown"),
+                (nv.nvmlClocksEventReasonSwThermalSlowdown, "sw_thermal_slowdown"),
+                (nv.nvmlClocksEventReasonSwPowerCap, "sw_power_cap"))
+        smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self.halt.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:
+                break
+            self.samples.append((sm, smax, {nm for b, nm in bits if r & b}))
+            self.halt.wait(0.002)
 
     def start(self):
+        self.halt = threading.Event()
+        try:
+            nv, h = self._nvml_handle()
+            self.t = threading.Thread(target=self._poll_nvml, args=(nv, h), daemon=True)
+            self.t.start()
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 5.0 and self.t.is_alive():
+                time.sleep(0.001)
+            if self.samples:
+                self.source = "nvml, 2 ms"
+                return
+            self.halt.set()
+        except Exception:
+            pass
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "20"],
@@ -96,6 +139,7 @@ class ClockSampler:
             while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
                 time.sleep(0.005)
             self.n_before = len(self.lines)
+            self.source = "nvidia-smi -lms 20"
         except OSError:
             self.proc = None
 
@@ -104,29 +148,34 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        for ln in self.lines[getattr(self, "n_before", 0):] or self.lines[-1:]:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
+        if self.source and self.source.startswith("nvml"):
+            self.halt.set()
+            self.t.join(timeout=5)
+            got = self.samples[1:] or self.samples
+        elif self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
-            except ValueError:
-                continue
-            names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            got = []
+            for ln in self.lines[getattr(self, "n_before", 0):] or self.lines[-1:]:
+                f = [x.strip() for x in ln.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    got.append((float(f[1]), float(f[2]),
+                                {nm for nm, v in zip(self.NAMES, f[5:9]) if v.lower() == "active"}))
+                except ValueError:
+                    continue
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        sm = [g[0] for g in got]
+        reasons = set().union(*(g[2] for g in got)) if got else set()
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_min_mhz": min(sm) if sm else None,
+                "sm_max_mhz": max(g[1] for g in got) if got else None,
+                "reasons": sorted(reasons), "samples": len(sm), "source": self.source}
 
 
 def reduce_max(values):
@@ -566,7 +615,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
