@@ -12,7 +12,8 @@ receivers x 20000 ranges of a 2 Hz, Nz = 100000 solve (timed separately,
 not part of the step), with its roofline against the measured bf16 peak,
 and "serving": a seeded request stream replayed in real time through the
 serving loop and through the plain one-request-at-a-time path (p50 / p99
-latency, throughput).
+latency, throughput), and "sweep": 360 azimuths x 8 frequencies with Nz per
+frequency (5000-60000) as one batched solve.
 
   value  freq-solves/s with the profile resident in HBM and results left in
          HBM (device-timed with CUDA events on the library's stream; L2
@@ -293,7 +294,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     ctx.set_timing(False)
     bis_ms, bis_n = ctx.phase_stats("bisect")
-    seqs, grid_pts = ctx.sturm_sequences()
+    sturm_steps = ctx.sturm_steps()
     phases = {ph: ctx.phase_stats(ph)[0] / n_ph for ph in
               ("knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec", "fetch")}
     if args.quick:
@@ -325,13 +326,14 @@ def run_ours(args):
     fp64_peak = ctx.fp64_peak_tflops() if rank == 0 else None
     ms_leg = modal_sum_leg(ctx, stream, _bf16_peak()) if rank == 0 and not args.no_modal_sum else None
     sv_leg = serving_leg(ctx) if rank == 0 and not args.no_serving else None
+    sw_leg = sweep_leg(ctx, stream) if rank == 0 and not args.no_sweep else None
     if rank == 0:
         solves = NFREQ * args.steps * world
         value = solves / (ms_dev / 1e3)
         e2e_value = solves / (ms_e2e / 1e3)
         # bisection kernel roofline: 3 FP64 flops per Sturm step (subtract +
-        # fused multiply-add) over the active shifts it swept
-        flops = 3.0 * seqs * (grid_pts / max(bis_n, 1))
+        # fused multiply-add), steps counted by the kernel
+        flops = 3.0 * sturm_steps  # over the bis_n timed launches
         achieved = flops / (bis_ms / 1e3) / 1e12 if bis_ms > 0 else None
         cpu = cpu_baseline(freqs, max_seconds=args.cpu_seconds)
         line = {
@@ -352,13 +354,14 @@ def run_ours(args):
                          "unit": "TFLOP/s", "frac": round(achieved / fp64_peak, 4) if achieved else None,
                          "peak_source": "measured in this run (dependent-FMA probe on all SMs)",
                          "traffic": None, "avg_launch_ms": round(bis_ms / max(bis_n, 1), 4),
-                         "flops_per_launch": flops / max(bis_n, 1) if bis_n else None},
+                         "flops_per_launch": flops / bis_n if bis_n else None},
             "phases_ms": {k: round(v, 4) for k, v in phases.items()},
             "plain_gpu": {"value": round(plain_rate, 2), "unit": METRIC,
                           "what": "one ncpa_ess_solve + TL per frequency, same workload"},
             "cpu_baseline": cpu,
             "modal_sum": ms_leg,
             "serving": sv_leg,
+            "sweep": sw_leg,
         }
         print(json.dumps(line), flush=True)
     for h in (prof,):
@@ -435,6 +438,72 @@ def modal_sum_leg(ctx, stream, bf16_peak, k=10):
         "error_vs_fp64": {"max_abs_over_max_P": float(rel.max()), "tl_db_median": float(np.median(d)),
                           "tl_db_p99_9": float(np.percentile(d, 99.9)), "tl_db_max": float(d.max()),
                           "where": "TL > -140 dB, first 2000 ranges"},
+    }
+
+
+# ---------------------------------------------------------------------------
+# azimuth sweep: 360 azimuths x 8 frequencies, Nz per frequency, one batch
+# ---------------------------------------------------------------------------
+SW_NAZ, SW_NR, SW_DR = 360, 2000, 500.0
+
+
+def sweep_leg(ctx, stream, reps=2):
+    """The N x 2-D sweep: 360 azimuths (1 deg) x 8 frequencies log-spaced
+    0.1-2 Hz on the analytic profile, Nz = 60 points per wavelength at 300 m/s
+    (at least 5000: 5000-60000), ground source and receiver, 1-D TL on 2000
+    ranges every 0.5 km.  Timed (CUDA events) as ONE batched solve over all
+    2880 problems on their 7 grids plus one TL launch, against one solve per
+    frequency (one grid each)."""
+    import torch
+    import ncpa_gpu
+
+    prof = ctx.profile_from_arrays(*workloads.si_arrays())
+    freqs = workloads.sweep_freqs()
+    nzs = [workloads.sweep_nz(f) for f in freqs]
+    azs = np.arange(SW_NAZ, dtype=np.float64)
+    P = len(freqs) * SW_NAZ
+
+    def batched():
+        m = ctx.solve_jobs([(prof, [f], azs, nz) for f, nz in zip(freqs, nzs)],
+                           ncpa_gpu.default_params(keep_on_device=1))
+        m.tl1d(SW_NR, SW_DR, to_host=False)
+        return m
+
+    def per_grid():
+        for f, nz in zip(freqs, nzs):
+            m = ctx.solve(prof, ncpa_gpu.default_params(nz_grid=nz, keep_on_device=1), [f], azs)
+            m.tl1d(SW_NR, SW_DR, to_host=False)
+            m.close()
+
+    def timed(fn, n):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(n):
+            r = fn()
+            if r is not None:
+                r.close()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / n
+
+    m = batched()  # warm-up; mode counts from this solve
+    off = m.all_modes()[0]
+    counts = np.diff(off)
+    m.close()
+    ms_b = timed(batched, reps)
+    per_grid()
+    ms_g = timed(per_grid, 1)
+    prof.close()
+    return {
+        "workload": "360 azimuths x 8 frequencies 0.1-2 Hz (log), Nz = max(5000, 60 points per wavelength at "
+                    "300 m/s) = %s, ground source/receiver, 1-D TL at 2000 ranges x 0.5 km" % nzs,
+        "problems": P, "modes_min": int(counts.min()), "modes_max": int(counts.max()),
+        "modes_total": int(counts.sum()),
+        "batched_ms": round(ms_b, 2), "batched_freq_solves_per_s": round(P / (ms_b / 1e3), 1),
+        "per_grid_ms": round(ms_g, 2), "per_grid_freq_solves_per_s": round(P / (ms_g / 1e3), 1),
+        "what": "batched = one ncpa_ess_solve_jobs over all grids + one TL launch; per_grid = one "
+                "ncpa_ess_solve + TL per frequency",
     }
 
 
@@ -623,9 +692,20 @@ def main():
                     help="device-resident leg only (no e2e, plain-path or CPU legs); for profiler runs")
     ap.add_argument("--no-modal-sum", action="store_true", help="skip the tensor-core modal-sum leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the served request-stream leg")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the 360-azimuth mixed-grid sweep leg")
     ap.add_argument("--only-modal-sum", action="store_true",
                     help="run only the tensor-core modal-sum leg and print its JSON (for profiler runs)")
+    ap.add_argument("--only-sweep", action="store_true",
+                    help="run only the mixed-grid sweep leg and print its JSON (for profiler runs)")
     args = ap.parse_args()
+    if args.only_sweep:
+        import torch
+        import ncpa_gpu
+
+        ctx = ncpa_gpu.Context(0)
+        print(json.dumps(sweep_leg(ctx, torch.cuda.ExternalStream(ctx.stream_ptr), reps=1)), flush=True)
+        ctx.close()
+        return
     if args.only_modal_sum:
         import torch
         import ncpa_gpu

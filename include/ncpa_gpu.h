@@ -114,17 +114,23 @@ ncpa_status ncpa_ess_solve(ncpa_ctx *ctx, const ncpa_profile *prof, const ncpa_e
                            const double *freqs, int n_freq, const double *az_deg, int n_az,
                            ncpa_modes **out);
 /* Batched solve over independent jobs, each with its own profile, frequency
- * list and one azimuth (the request batch of the serving loop; the reference
- * solves one (profile, frequency, azimuth) at a time in ESSModeSolver::solve,
- * ESSModeSolver.cpp:320-383).  All profiles must give the same solver grid
- * (same ground and top); problems are numbered job by job, frequency by
- * frequency.  The result behaves like a one-azimuth solve of sum(n_freq)
- * problems; ncpa_modes_info reports each problem's own densities. */
+ * list, azimuth(s) and solver grid size, in one pass of the eigen-solve
+ * kernels (the request batch of the serving loop, and sweeps whose grid
+ * follows the wavelength; the reference solves one (profile, frequency,
+ * azimuth) at a time in ESSModeSolver::solve, ESSModeSolver.cpp:320-383).
+ * Each job's grid comes from its profile and nz_grid (0: params->nz_grid)
+ * with the other params; problems are numbered job by job, frequency-major
+ * then azimuth inside a job.  The result behaves like a one-azimuth solve of
+ * sum(n_freq * n_az) problems; ncpa_modes_info reports each problem's own
+ * grid spacing and densities. */
 typedef struct {
     const ncpa_profile *profile;
     const double *freqs;
     int n_freq;
-    double az_deg;
+    double az_deg;            /* the job's azimuth when n_az == 0 */
+    int nz_grid;              /* grid points of this job; 0 -> params->nz_grid */
+    int n_az;                 /* > 0: the job sweeps az_list[0 .. n_az-1] */
+    const double *az_list;
 } ncpa_ess_job;
 ncpa_status ncpa_ess_solve_jobs(ncpa_ctx *ctx, const ncpa_ess_job *jobs, int n_jobs,
                                 const ncpa_ess_params *params, ncpa_modes **out);
@@ -305,12 +311,12 @@ void *ncpa_ctx_stream(ncpa_ctx *ctx);
  * ncpa_ess_solve measured with CUDA events on the context stream.  Phases:
  * "knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec",
  * "fetch".  stats() returns accumulated milliseconds and calls since the last
- * reset; sturm_sequences() the number of Sturm sequences (one shift swept over
- * the whole grid) run by the bisection kernel for active eigenvalues. */
+ * reset; sturm_steps() the number of Sturm recurrence steps (one shift over
+ * one grid point) run by the bisection kernel since the last reset. */
 ncpa_status ncpa_ctx_set_timing(ncpa_ctx *ctx, int on);
 ncpa_status ncpa_ctx_phase_stats(const ncpa_ctx *ctx, const char *phase, double *total_ms, long long *calls);
 ncpa_status ncpa_ctx_reset_stats(ncpa_ctx *ctx);
-ncpa_status ncpa_ctx_sturm_sequences(ncpa_ctx *ctx, long long *sequences, long long *grid_points);
+ncpa_status ncpa_ctx_sturm_steps(ncpa_ctx *ctx, long long *steps);
 /* Measured FP64 FMA throughput of this device [TFLOP/s, FMA = 2 flops]: a
  * dependent-FMA kernel on every SM for about 50 ms. */
 ncpa_status ncpa_probe_fp64_peak(ncpa_ctx *ctx, double *tflops);

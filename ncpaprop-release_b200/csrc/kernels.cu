@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(256) k_build_matrix(int nk, const double* __re
         double c = spline_get(nk, zk, ck, cc, z_min + i * dz_grid);
         double t = omega / c;
         double d = t * t;
-        if (kz2) kz2[(size_t)p * nz + i] = d;
+        if (kz2) kz2[(size_t)p * nz_pad + i] = d;
         if (g) g[(size_t)p * nz_pad + i] = 1.0 / (c * c);
         cmin = cmax = c;
         double sd;
@@ -339,11 +339,12 @@ int launch_build_matrix(cudaStream_t st, int nk, const double* zk, const double*
 constexpr int kWkbThreads = 128;
 
 __global__ void __launch_bounds__(kWkbThreads) k_window(ProblemInfo* __restrict__ pinfo,
-                                                        const double* __restrict__ kz2, int nz, double dz,
-                                                        int wkb, int wvnum, double c_min, double c_max,
-                                                        unsigned* err) {
+                                                        const double* __restrict__ kz2, int wkb, int wvnum,
+                                                        double c_min, double c_max, unsigned* err) {
     const int p = blockIdx.x;
     ProblemInfo pi = pinfo[p];
+    const int nz = pi.nz;
+    const double dz = pi.dz;
     const double omega = pi.omega;
     const double ceffmin = __longlong_as_double((long long)pi.ceffmin_bits);
     __shared__ int s_hit, s_first_invalid;
@@ -369,7 +370,7 @@ __global__ void __launch_bounds__(kWkbThreads) k_window(ProblemInfo* __restrict_
             bool valid = kk < kmf2;
             if (!valid) atomicMin(&s_first_invalid, j);
             if (valid) {
-                const double* row = kz2 + (size_t)p * nz;
+                const double* row = kz2 + pi.s_off;
                 double integral = 0.0, term = 1.0;
                 int i = 0;
                 while (term > dkk && i < nz) {
@@ -408,9 +409,9 @@ __global__ void __launch_bounds__(kWkbThreads) k_window(ProblemInfo* __restrict_
     }
 }
 
-int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2, int nz, double dz, int wkb,
-                  int wvnum, double c_min, double c_max, unsigned* err) {
-    k_window<<<P, kWkbThreads, 0, st>>>(pinfo, kz2, nz, dz, wkb, wvnum, c_min, c_max, err);
+int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2, int wkb, int wvnum,
+                  double c_min, double c_max, unsigned* err) {
+    k_window<<<P, kWkbThreads, 0, st>>>(pinfo, kz2, wkb, wvnum, c_min, c_max, err);
     return 1;
 }
 
@@ -516,8 +517,8 @@ __device__ __forceinline__ double scan_x(double lo, double hi, int t) {
 
 // K3a: kScanPoints counts per problem on an even grid of [lo, hi]
 __global__ void __launch_bounds__(kScanPoints) k_scan(const ProblemInfo* __restrict__ pinfo,
-                                                      const double* __restrict__ s, int nz, int nz_pad,
-                                                      int* __restrict__ counts, unsigned* err) {
+                                                      const double* __restrict__ s, int* __restrict__ counts,
+                                                      unsigned* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     double* buf = reinterpret_cast<double*>(smem_raw);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + kNbuf * kChunk * 8);
@@ -526,14 +527,13 @@ __global__ void __launch_bounds__(kScanPoints) k_scan(const ProblemInfo* __restr
     const int p = blockIdx.x;
     const double lo = pinfo[p].lo, hi = pinfo[p].hi;
     const double x = scan_x(lo, hi, threadIdx.x);
-    int c = cta_sturm_sweep(s + (size_t)p * nz_pad, nz, x, r, err);
+    int c = cta_sturm_sweep(s + pinfo[p].s_off, pinfo[p].nz, x, r, err);
     counts[(size_t)p * kScanPoints + threadIdx.x] = c;
 }
 
-int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
-                int* counts, unsigned* err) {
+int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* s, int* counts, unsigned* err) {
     size_t sm = kNbuf * kChunk * 8 + kNbuf * 8;
-    k_scan<<<P, kScanPoints, sm, st>>>(pinfo, s, nz, nz_pad, counts, err);
+    k_scan<<<P, kScanPoints, sm, st>>>(pinfo, s, counts, err);
     return 1;
 }
 
@@ -637,10 +637,9 @@ __device__ void warp_sweep(const double* __restrict__ s, int nz, double x0, doub
 }
 
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
-    k_bisect(const ProblemInfo* __restrict__ pinfo, const double* __restrict__ s, int nz, int nz_pad,
-             const int* __restrict__ counts, const WorkItem* __restrict__ items, int n_items, int* counter,
-             double tol, double* __restrict__ mu, unsigned* err, unsigned long long* seq_counter,
-             const int* __restrict__ n_items_dev) {
+    k_bisect(const ProblemInfo* __restrict__ pinfo, const double* __restrict__ s, const int* __restrict__ counts,
+             const WorkItem* __restrict__ items, int n_items, int* counter, double tol, double* __restrict__ mu,
+             unsigned* err, unsigned long long* step_counter, const int* __restrict__ n_items_dev) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     if (n_items_dev) n_items = *n_items_dev;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -661,7 +660,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
         const WorkItem w = items[it];
         const ProblemInfo pi = pinfo[w.problem];
         const int* cnt = counts + (size_t)w.problem * kScanPoints;
-        const double* sp = s + (size_t)w.problem * nz_pad;
+        const double* sp = s + pi.s_off;
+        const int nz = pi.nz;
         // state of eigen slot `lane`
         const int J = pi.c_lo + w.j0 + lane;
         double a = pi.lo, b = pi.lo, x = pi.lo;
@@ -718,7 +718,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
             double rat;
             const int smode = nN == 0 ? 0 : (nB > 0 ? 1 : 2);
             warp_sweep(sp, nz, xv[0], xv[1], smode, r, err, cv0, cv1, rat);
-            if (seq_counter && lane == 0) atomicAdd(seq_counter, (unsigned long long)(smode == 2 ? 32 : 64));
+            if (step_counter && lane == 0)
+                atomicAdd(step_counter, (unsigned long long)(smode == 2 ? 32 : 64) * (unsigned long long)nz);
             // updates.  Every __shfl_sync is executed by all 32 lanes.
             const bool isN = mode == 1, isB = mode == 0;
             const int vN = isN ? __popc(nm & ((1u << lane) - 1u)) : 0;  // Newton virtual lane (chain 0)
@@ -781,13 +782,13 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
     }
 }
 
-int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
-                  const int* counts, const WorkItem* items, int n_items, int* counter, double tol, double* mu,
-                  unsigned* err, unsigned long long* seq_counter, const int* n_items_dev) {
+int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
+                  const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
+                  unsigned long long* step_counter, const int* n_items_dev) {
     const size_t sm = (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8 + kWBuf * 8);
     cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_bisect<<<grid, kWarpsPerCta * 32, sm, st>>>(pinfo, s, nz, nz_pad, counts, items, n_items, counter, tol, mu,
-                                                  err, seq_counter, n_items_dev);
+    k_bisect<<<grid, kWarpsPerCta * 32, sm, st>>>(pinfo, s, counts, items, n_items, counter, tol, mu, err,
+                                                  step_counter, n_items_dev);
     return 1;
 }
 
@@ -1021,13 +1022,11 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
         fence_mbar_init();
     }
     __syncwarp();
-    const int nz = A.nz;
-    const int nch = (nz + kEvC - 1) / kEvC;
-    const int nblk = (nz + kBlk - 1) / kBlk;
     const size_t gw = (size_t)blockIdx.x * kEvWarps + wid;
     double* ck1 = A.ck_q1 + gw * A.ck_slot_stride;
     double* ck2 = A.ck_q2 + gw * A.ck_slot_stride;
     int* cke = A.ck_e + gw * A.ck_slot_stride;
+    int nz = 0;  // grid of the current item
     auto load_ck = [&](int kb, double& a1, double& a2, int& ae) {
         if (min((kb + 1) * kBlk, nz) >= nz) {
             a1 = 1.0;
@@ -1046,9 +1045,13 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
     for (int it = blockIdx.x * kEvWarps + wid; it < n_items_all; it += warps_total) {
         const WorkItem w = A.items[it];
         const ProblemInfo pi = A.pinfo[w.problem];
-        const double* sp = A.s + (size_t)w.problem * A.nz_pad;
-        const double* wp = A.w + (size_t)(w.problem / A.n_az) * A.wstride;
-        const double* gp = kGroup ? A.g + (size_t)w.problem * A.nz_pad : nullptr;
+        nz = pi.nz;
+        const int nch = (nz + kEvC - 1) / kEvC;
+        const int nblk = (nz + kBlk - 1) / kBlk;
+        const int isrc = pi.isrc, ircv = pi.ircv;
+        const double* sp = A.s + pi.s_off;
+        const double* wp = A.w + pi.w_off;
+        const double* gp = kGroup ? A.g + pi.s_off : nullptr;
         const bool active = lane < w.m;
         const double mu = active ? A.mu[pi.off + w.j0 + lane] : pi.lo;
 
@@ -1180,19 +1183,19 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                             }
                         }
                     }
-                    const bool special = !full || (A.isrc >= gbase && A.isrc < gbase + kBlk) ||
-                                         (A.ircv >= gbase && A.ircv < gbase + kBlk);
+                    const bool special = !full || (isrc >= gbase && isrc < gbase + kBlk) ||
+                                         (ircv >= gbase && ircv < gbase + kBlk);
                     if (!special) {
 #pragma unroll
                         for (int jj = 0; jj < kBlk; ++jj)
                             fwd_step<kGroup, false>(F, gbase + jj, nz, sb[lb + jj], wb[lb + jj],
-                                                    kGroup ? gb[lb + jj] : 0.0, qb[jj], Eb, mu, A.isrc, A.ircv);
+                                                    kGroup ? gb[lb + jj] : 0.0, qb[jj], Eb, mu, isrc, ircv);
                     } else {
 #pragma unroll
                         for (int jj = 0; jj < kBlk; ++jj) {
                             const int li = min(lb + jj, valid - 1);
                             fwd_step<kGroup, true>(F, gbase + jj, nz, sb[li], wb[li], kGroup ? gb[li] : 0.0, qb[jj],
-                                                   Eb, mu, A.isrc, A.ircv);
+                                                   Eb, mu, isrc, ircv);
                         }
                     }
                     const int sh = grow_shift(F.pm1, F.pm2);
@@ -1218,14 +1221,14 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
         const double iq2 = 1.0 / (F.qr * F.qr);
         const double isq = 1.0 / F.sqr;
         const double nrm = F.Anr * isq + F.Tn * iq2;
-        const double scale = 1.0 / sqrt(nrm * A.dz);
+        const double scale = 1.0 / sqrt(nrm * pi.dz);
         const int r = F.r;
-        double zs = (A.isrc <= r) ? (F.ps / F.pr) * pow2(F.Eps - F.Epr) : (F.qs / F.qr) * pow2(F.Eqs - F.Eqr);
-        double zr = (A.ircv <= r) ? (F.prc / F.pr) * pow2(F.Eprc - F.Epr) : (F.qrc / F.qr) * pow2(F.Eqrc - F.Eqr);
-        if ((A.isrc - r) & 1) zs = -zs;
-        if ((A.ircv - r) & 1) zr = -zr;
+        double zs = (isrc <= r) ? (F.ps / F.pr) * pow2(F.Eps - F.Epr) : (F.qs / F.qr) * pow2(F.Eqs - F.Eqr);
+        double zr = (ircv <= r) ? (F.prc / F.pr) * pow2(F.Eprc - F.Epr) : (F.qrc / F.qr) * pow2(F.Eqrc - F.Eqr);
+        if ((isrc - r) & 1) zs = -zs;
+        if ((ircv - r) & 1) zr = -zr;
         const double absorption = (F.Awr * isq + F.Tw * iq2) / nrm;
-        const double ks = sqrt(mu / A.h2);
+        const double ks = sqrt(mu / (pi.dz * pi.dz));
         const double kk = ks * ks;
         const auto kp = csqrt_principal(kk, absorption);
         if (active) {

@@ -15,16 +15,23 @@ enum : unsigned {
     kErrTooMany = 8u,  // a problem has more modes than allowed (device-built work items)
 };
 
-// Per (frequency, azimuth) problem, device resident.
+// Per (frequency, azimuth) problem, device resident.  Every problem carries
+// its own solver grid (size, spacing, source/receiver rows and the offsets of
+// its rows in the batch arrays), so one batch may mix grid sizes.
 struct ProblemInfo {
     double freq, omega, az;
     double k_min, k_max;   // wavenumber window [1/m]
     double lo, hi;         // window in units of the scaled matrix S = h^2 A
     double ceff_grnd, ceff_top;
+    double dz;             // grid spacing [m]
     unsigned long long ceffmin_bits, ceffmax_bits;  // positive doubles as ordered bits
+    long long s_off;       // offset (doubles) of the problem's row in s, g and kz2 (rows padded to kChunk)
+    long long w_off;       // offset (doubles) of its attenuation-weight row in w
+    int nz;                // grid points
+    int isrc, ircv;        // source / receiver grid rows
     int c_lo, c_hi;        // Sturm counts at lo, hi
     int M, off;            // number of modes and offset into the mode arrays
-    int used_wkb, pad;
+    int used_wkb;
 };
 
 struct WorkItem {
@@ -61,22 +68,22 @@ int launch_grid_common(cudaStream_t st, int nk, const double* zk, const double* 
 int launch_attn_weight(cudaStream_t st, int nk, const double* zk, const double* alpha, const double* acoef,
                        int n_f, const double* freqs, int nz, double z_min, double dz_grid, const double* ct_g,
                        double* w, int wstride);
-// matrix build (K1): s [P x nz_pad], optional kz2 = (omega/c)^2 and
-// g = 1/c^2 [P x nz]; fills ceff extrema / ground / top in ProblemInfo
+// matrix build (K1): s, optional kz2 = (omega/c)^2 and g = 1/c^2, each
+// [P x nz_pad]; fills ceff extrema / ground / top in ProblemInfo (the P
+// problems of one launch share one grid; their rows are nz_pad apart)
 int launch_build_matrix(cudaStream_t st, int nk, const double* zk, const double* ceffk, const double* ceffcoef,
                         int n_az, int P, ProblemInfo* pinfo, int nz, int nz_pad, double z_min, double dz_grid,
                         double dz, double admittance, double* s, double* kz2, double* g);
 // WKB window and scaled bounds (K2)
-int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2, int nz, double dz,
-                  int wkb, int wvnum, double c_min, double c_max, unsigned* err);
+int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2, int wkb, int wvnum,
+                  double c_min, double c_max, unsigned* err);
 // isolation scan: kScanPoints Sturm counts per problem (K3a)
-int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
-                int* counts, unsigned* err);
-// multisection/bisection over work items (K3)
-int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, int nz, int nz_pad,
-                  const int* counts, const WorkItem* items, int n_items, int* counter, double tol, double* mu,
-                  unsigned* err, unsigned long long* seq_counter,
-                  const int* n_items_dev = nullptr);
+int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* s, int* counts, unsigned* err);
+// multisection/bisection over work items (K3); step_counter (optional)
+// accumulates the Sturm recurrence steps swept
+int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
+                  const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
+                  unsigned long long* step_counter, const int* n_items_dev = nullptr);
 int bisect_ctas_per_sm();
 // FP64 throughput probe: each thread runs n_iter iterations of 8 independent
 // FMA chains; out receives a value that keeps the chains live
@@ -84,17 +91,14 @@ int launch_fp64_probe(cudaStream_t st, int grid, int block, int n_iter, double* 
 // twisted-factorisation eigenvectors + fused reductions (K4)
 struct EigvecArgs {
     const ProblemInfo* pinfo;
-    const double* s;
-    const double* w;   // [n_f x wstride]
-    const double* g;   // [P x nz] or null
-    int nz, nz_pad, wstride, n_az;
+    const double* s;   // rows at pinfo[p].s_off
+    const double* w;   // rows at pinfo[p].w_off
+    const double* g;   // rows at pinfo[p].s_off, or null
     const WorkItem* items;
     int n_items;
     const int* n_items_dev;  // when set, the item count is read here (built on the device)
     int* counter;
     const double* mu;
-    int isrc, ircv;
-    double dz, h2;
     double* kr;
     double* ki;
     double* vs;
@@ -105,7 +109,7 @@ struct EigvecArgs {
     double* ck_q1;            // checkpoint scratch, one slot per warp of the grid
     double* ck_q2;
     int* ck_e;
-    long long ck_slot_stride; // elements per warp slot (blocks x 32)
+    long long ck_slot_stride; // elements per warp slot (blocks of the largest grid x 32)
     unsigned* err;
 };
 int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a);

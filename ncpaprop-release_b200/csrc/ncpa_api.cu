@@ -121,7 +121,6 @@ struct ncpa_ctx {
     bool timing = false;           // NCPA_TIMING=1: per-phase times on stderr
     bool stats = false;            // ncpa_ctx_set_timing: accumulate per phase
     std::map<std::string, std::pair<double, long long>> phase;
-    long long grid_points = 0;     // sum over bisection launches of nz
     void count(int n) { launches += n; }
 };
 
@@ -169,11 +168,10 @@ struct ncpa_profile {
 
 struct ncpa_modes {
     ncpa_ctx* ctx = nullptr;
-    int P = 0, nf = 0, na = 0, nz = 0, nz_pad = 0;
+    int P = 0, nf = 0, na = 0;
+    int nz_max = 0;  // largest grid of the batch (each problem's own grid is in info[p])
     ncpa_ess_params prm{};
     std::vector<double> freqs, az;
-    double z_min = 0, dz_grid = 0, dz = 0;
-    int isrc = 0, ircv = 0;
     std::vector<double> rho_src_p, rho_rcv_p;  // rho at the source / receiver grid points, per problem
     bool multi_job = false;                     // built by ncpa_ess_solve_jobs (one profile per job)
     std::vector<ProblemInfo> info;
@@ -288,9 +286,8 @@ void check_ess_params(const ncpa_ess_params* prm) {
         throw ApiError(NCPA_EINVAL, "wvnum_filter needs c_min > 0 and c_max > 0");
 }
 
-Geometry grid_geometry(const ncpa_profile* prof, const ncpa_ess_params* prm) {
+Geometry grid_geometry(const ncpa_profile* prof, const ncpa_ess_params* prm, int nz) {
     Geometry g{};
-    const int nz = prm->nz_grid;
     double z_min = prm->zground_km * 1000.0;
     double maxheight = prm->maxheight_km * 1000.0;
     if (maxheight >= prof->z_hi) maxheight = prof->z_hi - 1e-6;
@@ -396,10 +393,9 @@ void build_problems(ncpa_ctx* ctx, PhaseTimer& tm, const ncpa_profile* prof, con
 // round trip and reads the mode counts back once at the end.  Output arrays
 // are sized for max_modes per problem.
 void solve_core_device_items(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_params* prm, DevBuf& s,
-                             DevBuf& w, DevBuf& g, DevBuf& counts, int w_per_az) {
+                             DevBuf& w, DevBuf& g, DevBuf& counts) {
     cudaStream_t st = ctx->stream;
-    const int P = M->P, nz = M->nz, nz_pad = M->nz_pad;
-    const double dz = M->dz;
+    const int P = M->P;
     ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
     const int cap_modes = M->prm.max_modes;
     const size_t mcap = (size_t)P * cap_modes;
@@ -420,31 +416,22 @@ void solve_core_device_items(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const
     CK(cudaMemsetAsync(d_counter.p, 0, 2 * sizeof(int), st));
     tm.mark("host-items");
     const int grid_b = ctx->num_sms * ncpa::bisect_ctas_per_sm();
-    check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
-                                          bis.as<WorkItem>(), 0, d_counter.as<int>(), kBisectTol, mu.as<double>(),
+    check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), counts.as<int>(), bis.as<WorkItem>(),
+                                          0, d_counter.as<int>(), kBisectTol, mu.as<double>(),
                                           ctx->d_err.as<unsigned>(),
                                           ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr,
                                           tot.as<int>()));
-    if (ctx->stats) ctx->grid_points += nz;
     tm.mark("bisect");
     ncpa::EigvecArgs ea{};
     ea.pinfo = d_pinfo;
     ea.s = s.as<double>();
     ea.w = w.as<double>();
     ea.g = prm->want_group_speed ? g.as<double>() : nullptr;
-    ea.nz = nz;
-    ea.nz_pad = nz_pad;
-    ea.wstride = nz_pad;
-    ea.n_az = w_per_az;
     ea.items = ev.as<WorkItem>();
     ea.n_items = 0;
     ea.n_items_dev = tot.as<int>() + 1;
     ea.counter = d_counter.as<int>() + 1;
     ea.mu = mu.as<double>();
-    ea.isrc = M->isrc;
-    ea.ircv = M->ircv;
-    ea.dz = dz;
-    ea.h2 = dz * dz;
     ea.kr = M->d_kr.as<double>();
     ea.ki = M->d_ki.as<double>();
     ea.vs = M->d_vs.as<double>();
@@ -452,7 +439,7 @@ void solve_core_device_items(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const
     ea.vg = M->d_vg.as<double>();
     const int ewpc = ncpa::kEvWarpsPerCta;
     const int grid_e = std::min(item_cap / ewpc + 1, ctx->num_sms * ncpa::eigvec_ctas_per_sm(ea));
-    const long long nblk = (nz + ncpa::kBlk - 1) / ncpa::kBlk;
+    const long long nblk = (M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk;
     const long long slot = nblk * 32;
     const size_t need = (size_t)grid_e * ewpc * slot;
     if (ctx->ck1.bytes < need * 8) {
@@ -491,26 +478,24 @@ void solve_core_device_items(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const
 }
 
 // Window, Sturm scan, work items, bisection and eigenvectors over all
-// problems of M (their matrices built).  w holds one weight row per
-// frequency when w_per_az > 0 (problem p uses row p / w_per_az).
+// problems of M (their matrices built; each problem's rows of s, w, g and kz2
+// at the offsets in its ProblemInfo).
 void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_params* prm, bool wkb, DevBuf& s,
-                DevBuf& w, DevBuf& g, DevBuf& kz2, int w_per_az) {
+                DevBuf& w, DevBuf& g, DevBuf& kz2) {
     cudaStream_t st = ctx->stream;
-    const int P = M->P, nz = M->nz, nz_pad = M->nz_pad;
-    const double dz = M->dz;
+    const int P = M->P;
     ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
     // ---- K2 window ----
-    check_launch(ctx, ncpa::launch_window(st, P, d_pinfo, wkb ? kz2.as<double>() : nullptr, nz, dz, wkb ? 1 : 0,
+    check_launch(ctx, ncpa::launch_window(st, P, d_pinfo, wkb ? kz2.as<double>() : nullptr, wkb ? 1 : 0,
                                           prm->wvnum_filter, prm->c_min, prm->c_max, ctx->d_err.as<unsigned>()));
     tm.mark("window");
     // ---- K3a scan ----
     DevBuf counts;
     counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
-    check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
-                                        ctx->d_err.as<unsigned>()));
+    check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), counts.as<int>(), ctx->d_err.as<unsigned>()));
     tm.mark("scan");
     if (!prm->want_vectors) {
-        solve_core_device_items(ctx, tm, M, prm, s, w, g, counts, w_per_az);
+        solve_core_device_items(ctx, tm, M, prm, s, w, g, counts);
         return;
     }
     std::vector<int> hcounts((size_t)P * ncpa::kScanPoints);
@@ -564,7 +549,7 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
         long long acc = 0;
         for (int p = 0; p < P; ++p) {
             M->vfull_off[p] = acc;
-            acc += (long long)M->info[p].M * nz;
+            acc += (long long)M->info[p].M * M->info[p].nz;
         }
         M->d_vfull.alloc((size_t)std::max(1LL, acc) * 8, st);
         upload(M->d_vfull_off, M->vfull_off, st);
@@ -578,11 +563,10 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
         const int wpc = 4;  // warps per bisection CTA
         int grid_b = std::min((n_items + wpc - 1) / wpc, ctx->num_sms * ncpa::bisect_ctas_per_sm());
         tm.mark("host-items");
-        check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), nz, nz_pad, counts.as<int>(),
+        check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), counts.as<int>(),
                                               d_items.as<WorkItem>(), n_items, d_counter.as<int>(), kBisectTol,
                                               mu.as<double>(), ctx->d_err.as<unsigned>(),
                                               ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr));
-        if (ctx->stats) ctx->grid_points += nz;
         tm.mark("bisect");
         // ---- K4 eigenvectors: items of <= kEvItem eigenvalues ----
         std::vector<WorkItem> ev_items;
@@ -599,18 +583,10 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
         ea.s = s.as<double>();
         ea.w = w.as<double>();
         ea.g = prm->want_group_speed ? g.as<double>() : nullptr;
-        ea.nz = nz;
-        ea.nz_pad = nz_pad;
-        ea.wstride = nz_pad;
-        ea.n_az = w_per_az;
         ea.items = d_ev_items.as<WorkItem>();
         ea.n_items = n_ev;
         ea.counter = d_counter.as<int>() + 1;
         ea.mu = mu.as<double>();
-        ea.isrc = M->isrc;
-        ea.ircv = M->ircv;
-        ea.dz = dz;
-        ea.h2 = dz * dz;
         ea.kr = M->d_kr.as<double>();
         ea.ki = M->d_ki.as<double>();
         ea.vs = M->d_vs.as<double>();
@@ -620,7 +596,7 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
         ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
         const int ewpc = ncpa::kEvWarpsPerCta;
         const int grid_e = std::min((n_ev + ewpc - 1) / ewpc, ctx->num_sms * ncpa::eigvec_ctas_per_sm(ea));
-        const long long nblk = (nz + ncpa::kBlk - 1) / ncpa::kBlk;
+        const long long nblk = (M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk;
         const long long slot = nblk * 32;
         const size_t need = (size_t)grid_e * ewpc * slot;
         if (ctx->ck1.bytes < need * 8) {
@@ -642,29 +618,105 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
     tm.mark("fetch");
 }
 
-void init_modes(ncpa_modes* M, ncpa_ctx* ctx, const ncpa_ess_params* prm, const Geometry& geo, int P) {
+void init_modes(ncpa_modes* M, ncpa_ctx* ctx, const ncpa_ess_params* prm, int P) {
     M->ctx = ctx;
     M->prm = *prm;
     if (M->prm.max_modes <= 0) M->prm.max_modes = 4000;
     M->P = P;
-    M->nz = prm->nz_grid;
-    M->nz_pad = ((M->nz + ncpa::kChunk - 1) / ncpa::kChunk) * ncpa::kChunk;
-    M->z_min = geo.z_min;
-    M->dz_grid = geo.dz_grid;
-    M->dz = geo.dz;
-    M->isrc = geo.isrc;
-    M->ircv = geo.ircv;
     M->info.assign(P, ProblemInfo{});
     M->rho_src_p.assign(P, 1.0);
     M->rho_rcv_p.assign(P, 1.0);
 }
 
-void set_problem(ProblemInfo& pi, double freq, double az) {
-    pi.freq = freq;
-    pi.omega = 2 * kPi * freq;
-    pi.az = az;
-    pi.ceffmin_bits = 0x7ff0000000000000ull;
-    pi.ceffmax_bits = 0ull;
+// One group of problems: one profile on one solver grid, n_freq x n_az
+// problems numbered frequency-major from p0.  Its rows start at s_base in
+// s, g and kz2 (nz_pad apart) and at w_base in w (one row per frequency).
+struct Group {
+    const ncpa_profile* prof;
+    Geometry geo;
+    int nz, nz_pad;
+    const double* freqs;
+    int n_freq;
+    const double* az;
+    int n_az;
+    int p0;
+    long long s_base, w_base;
+};
+
+Group make_group(const ncpa_profile* prof, const ncpa_ess_params* prm, int nz, const double* freqs, int n_freq,
+                 const double* az, int n_az) {
+    Group g{};
+    g.prof = prof;
+    g.geo = grid_geometry(prof, prm, nz);
+    g.nz = nz;
+    g.nz_pad = ((nz + ncpa::kChunk - 1) / ncpa::kChunk) * ncpa::kChunk;
+    g.freqs = freqs;
+    g.n_freq = n_freq;
+    g.az = az;
+    g.n_az = n_az;
+    return g;
+}
+
+bool wants_wkb(const ncpa_ess_params* prm);
+
+// Lays the groups out in one batch (problem records, row offsets), builds
+// every group's matrices and runs the window, scan, bisection and
+// eigenvector kernels once over all problems.
+void solve_groups(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::vector<Group>& groups) {
+    cudaStream_t st = ctx->stream;
+    PhaseTimer tm(ctx);
+    tm.mark("start");
+    long long s_tot = 0, w_tot = 0;
+    int p = 0;
+    M->nz_max = 0;
+    for (Group& g : groups) {
+        g.p0 = p;
+        g.s_base = s_tot;
+        g.w_base = w_tot;
+        for (int f = 0; f < g.n_freq; ++f)
+            for (int a = 0; a < g.n_az; ++a, ++p) {
+                ProblemInfo& pi = M->info[p];
+                pi.freq = g.freqs[f];
+                pi.omega = 2 * kPi * g.freqs[f];
+                pi.az = g.az[a];
+                pi.ceffmin_bits = 0x7ff0000000000000ull;
+                pi.ceffmax_bits = 0ull;
+                pi.dz = g.geo.dz;
+                pi.nz = g.nz;
+                pi.isrc = g.geo.isrc;
+                pi.ircv = g.geo.ircv;
+                pi.s_off = g.s_base + (long long)(f * g.n_az + a) * g.nz_pad;
+                pi.w_off = g.w_base + (long long)f * g.nz_pad;
+            }
+        s_tot += (long long)g.n_freq * g.n_az * g.nz_pad;
+        w_tot += (long long)g.n_freq * g.nz_pad;
+        M->nz_max = std::max(M->nz_max, g.nz);
+    }
+    upload(M->d_pinfo, M->info, st);
+    const bool wkb = wants_wkb(prm);
+    DevBuf s, w, gs, kz2;
+    s.alloc((size_t)s_tot * 8, st);
+    w.alloc((size_t)w_tot * 8, st);
+    if (wkb) kz2.alloc((size_t)s_tot * 8, st);
+    if (prm->want_group_speed) gs.alloc((size_t)s_tot * 8, st);
+    double* rho_pairs = pinned(ctx, 2 * groups.size());
+    ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& g = groups[gi];
+        build_problems(ctx, tm, g.prof, prm, g.geo, g.nz, g.nz_pad, g.freqs, g.n_freq, g.az, g.n_az, wkb,
+                       d_pinfo + g.p0, s.as<double>() + g.s_base, w.as<double>() + g.w_base,
+                       prm->want_group_speed ? gs.as<double>() + g.s_base : nullptr,
+                       wkb ? kz2.as<double>() + g.s_base : nullptr, rho_pairs + 2 * gi);
+    }
+    solve_core(ctx, tm, M, prm, wkb, s, w, gs, kz2);
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& g = groups[gi];
+        const int np = g.n_freq * g.n_az;
+        for (int k = 0; k < np; ++k) {
+            M->rho_src_p[g.p0 + k] = rho_pairs[2 * gi];
+            M->rho_rcv_p[g.p0 + k] = rho_pairs[2 * gi + 1];
+        }
+    }
 }
 
 bool wants_wkb(const ncpa_ess_params* prm) {
@@ -706,7 +758,6 @@ ncpa_status ncpa_ctx_set_timing(ncpa_ctx* ctx, int on) {
 ncpa_status ncpa_ctx_reset_stats(ncpa_ctx* ctx) {
     if (!ctx) return NCPA_EINVAL;
     ctx->phase.clear();
-    ctx->grid_points = 0;
     return guarded(ctx, [&]() -> ncpa_status {
         CK(cudaMemsetAsync(ctx->d_stats.p, 0, 4 * sizeof(unsigned long long), ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
@@ -722,14 +773,13 @@ ncpa_status ncpa_ctx_phase_stats(const ncpa_ctx* ctx, const char* phase, double*
     return NCPA_OK;
 }
 
-ncpa_status ncpa_ctx_sturm_sequences(ncpa_ctx* ctx, long long* sequences, long long* grid_points) {
-    if (!ctx) return NCPA_EINVAL;
+ncpa_status ncpa_ctx_sturm_steps(ncpa_ctx* ctx, long long* steps) {
+    if (!ctx || !steps) return NCPA_EINVAL;
     return guarded(ctx, [&]() -> ncpa_status {
         unsigned long long h = 0;
         CK(cudaMemcpyAsync(&h, ctx->d_stats.p, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
-        if (sequences) *sequences = (long long)h;
-        if (grid_points) *grid_points = ctx->grid_points;
+        *steps = (long long)h;
         return NCPA_OK;
     });
 }
@@ -1034,33 +1084,14 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
         for (int i = 0; i < n_freq; ++i)
             if (!(freqs[i] > 0.0)) throw ApiError(NCPA_EINVAL, "frequencies must be positive");
         CK(cudaSetDevice(ctx->device));
-        cudaStream_t st = ctx->stream;
-        PhaseTimer tm(ctx);
-        tm.mark("start");
-        const Geometry geo = grid_geometry(prof, prm);
+        std::vector<Group> groups{make_group(prof, prm, prm->nz_grid, freqs, n_freq, az_deg, n_az)};
         auto M = std::make_unique<ncpa_modes>();
-        init_modes(M.get(), ctx, prm, geo, n_freq * n_az);
+        init_modes(M.get(), ctx, prm, n_freq * n_az);
         M->nf = n_freq;
         M->na = n_az;
         M->freqs.assign(freqs, freqs + n_freq);
         M->az.assign(az_deg, az_deg + n_az);
-        const int P = M->P, nz = M->nz, nz_pad = M->nz_pad;
-        for (int f = 0; f < n_freq; ++f)
-            for (int a = 0; a < n_az; ++a) set_problem(M->info[f * n_az + a], freqs[f], az_deg[a]);
-        upload(M->d_pinfo, M->info, st);
-        const bool wkb = wants_wkb(prm);
-        DevBuf s, w, g, kz2;
-        s.alloc((size_t)P * nz_pad * 8, st);
-        w.alloc((size_t)n_freq * nz_pad * 8, st);
-        if (wkb) kz2.alloc((size_t)P * nz * 8, st);
-        if (prm->want_group_speed) g.alloc((size_t)P * nz_pad * 8, st);
-        double* rho_pair = pinned(ctx, 2);
-        build_problems(ctx, tm, prof, prm, geo, nz, nz_pad, freqs, n_freq, az_deg, n_az, wkb,
-                       M->d_pinfo.as<ProblemInfo>(), s.as<double>(), w.as<double>(),
-                       prm->want_group_speed ? g.as<double>() : nullptr, wkb ? kz2.as<double>() : nullptr, rho_pair);
-        solve_core(ctx, tm, M.get(), prm, wkb, s, w, g, kz2, n_az);
-        M->rho_src_p.assign(P, rho_pair[0]);
-        M->rho_rcv_p.assign(P, rho_pair[1]);
+        solve_groups(ctx, M.get(), prm, groups);
         *out = M.release();
         return NCPA_OK;
     });
@@ -1073,63 +1104,32 @@ ncpa_status ncpa_ess_solve_jobs(ncpa_ctx* ctx, const ncpa_ess_job* jobs, int n_j
     return guarded(ctx, [&]() -> ncpa_status {
         check_ess_params(prm);
         int P = 0;
+        std::vector<Group> groups;
+        groups.reserve(n_jobs);
         for (int j = 0; j < n_jobs; ++j) {
             const ncpa_ess_job& jb = jobs[j];
             if (!jb.profile || !jb.freqs || jb.n_freq < 1) throw ApiError(NCPA_EINVAL, "job without profile or frequencies");
             for (int i = 0; i < jb.n_freq; ++i)
                 if (!(jb.freqs[i] > 0.0)) throw ApiError(NCPA_EINVAL, "frequencies must be positive");
             if (jb.profile->ctx != ctx) throw ApiError(NCPA_EINVAL, "profile belongs to another context");
-            P += jb.n_freq;
-        }
-        // one grid for the whole batch: every profile must give the same geometry
-        const Geometry geo = grid_geometry(jobs[0].profile, prm);
-        for (int j = 1; j < n_jobs; ++j) {
-            const Geometry gj = grid_geometry(jobs[j].profile, prm);
-            if (gj.z_min != geo.z_min || gj.dz != geo.dz || gj.dz_grid != geo.dz_grid)
-                throw ApiError(NCPA_EINVAL, "jobs of one batch need profiles giving the same solver grid");
+            if (jb.n_az < 0 || (jb.n_az > 0 && !jb.az_list)) throw ApiError(NCPA_EINVAL, "job azimuth list missing");
+            if (jb.nz_grid != 0 && jb.nz_grid < 10) throw ApiError(NCPA_EINVAL, "Nz_grid must be >= 10");
+            const int n_az = jb.n_az > 0 ? jb.n_az : 1;
+            groups.push_back(make_group(jb.profile, prm, jb.nz_grid > 0 ? jb.nz_grid : prm->nz_grid, jb.freqs,
+                                        jb.n_freq, jb.n_az > 0 ? jb.az_list : &jb.az_deg, n_az));
+            P += jb.n_freq * n_az;
         }
         CK(cudaSetDevice(ctx->device));
-        cudaStream_t st = ctx->stream;
-        PhaseTimer tm(ctx);
-        tm.mark("start");
         auto M = std::make_unique<ncpa_modes>();
-        init_modes(M.get(), ctx, prm, geo, P);
+        init_modes(M.get(), ctx, prm, P);
         M->nf = P;
         M->na = 1;
         M->multi_job = true;
-        const int nz = M->nz, nz_pad = M->nz_pad;
-        int p0 = 0;
-        for (int j = 0; j < n_jobs; ++j)
-            for (int i = 0; i < jobs[j].n_freq; ++i, ++p0) {
-                set_problem(M->info[p0], jobs[j].freqs[i], jobs[j].az_deg);
-                M->freqs.push_back(jobs[j].freqs[i]);
-            }
-        M->az.assign(1, jobs[0].az_deg);
-        upload(M->d_pinfo, M->info, st);
-        const bool wkb = wants_wkb(prm);
-        DevBuf s, w, g, kz2;
-        s.alloc((size_t)P * nz_pad * 8, st);
-        w.alloc((size_t)P * nz_pad * 8, st);  // one row per problem
-        if (wkb) kz2.alloc((size_t)P * nz * 8, st);
-        if (prm->want_group_speed) g.alloc((size_t)P * nz_pad * 8, st);
-        double* rho_pairs = pinned(ctx, 2 * (size_t)n_jobs);
-        p0 = 0;
-        for (int j = 0; j < n_jobs; ++j) {
-            const ncpa_ess_job& jb = jobs[j];
-            build_problems(ctx, tm, jb.profile, prm, geo, nz, nz_pad, jb.freqs, jb.n_freq, &jb.az_deg, 1, wkb,
-                           M->d_pinfo.as<ProblemInfo>() + p0, s.as<double>() + (size_t)p0 * nz_pad,
-                           w.as<double>() + (size_t)p0 * nz_pad,
-                           prm->want_group_speed ? g.as<double>() + (size_t)p0 * nz_pad : nullptr,
-                           wkb ? kz2.as<double>() + (size_t)p0 * nz : nullptr, rho_pairs + 2 * j);
-            p0 += jb.n_freq;
-        }
-        solve_core(ctx, tm, M.get(), prm, wkb, s, w, g, kz2, 1);
-        p0 = 0;
-        for (int j = 0; j < n_jobs; ++j)
-            for (int i = 0; i < jobs[j].n_freq; ++i, ++p0) {
-                M->rho_src_p[p0] = rho_pairs[2 * j];
-                M->rho_rcv_p[p0] = rho_pairs[2 * j + 1];
-            }
+        for (const Group& g : groups)
+            for (int f = 0; f < g.n_freq; ++f)
+                for (int a = 0; a < g.n_az; ++a) M->freqs.push_back(g.freqs[f]);
+        M->az.assign(1, groups[0].az[0]);
+        solve_groups(ctx, M.get(), prm, groups);
         *out = M.release();
         return NCPA_OK;
     });
@@ -1161,7 +1161,7 @@ ncpa_status ncpa_modes_info(const ncpa_modes* m, int problem, double* freq, doub
     const ProblemInfo& pi = m->info[problem];
     if (freq) *freq = pi.freq;
     if (az) *az = pi.az;
-    if (dz) *dz = m->dz;
+    if (dz) *dz = pi.dz;
     if (k_min) *k_min = pi.k_min;
     if (k_max) *k_max = pi.k_max;
     if (rho_src) *rho_src = m->rho_src_p[problem];
@@ -1214,7 +1214,7 @@ ncpa_status ncpa_modes_get_vectors(const ncpa_modes* m, int problem, double* v) 
     if (!m || !v || problem < 0 || problem >= m->P) return NCPA_EINVAL;
     if (!m->prm.want_vectors) return fail(m->ctx, NCPA_EINVAL, "solve was run without want_vectors");
     return guarded(m->ctx, [&]() -> ncpa_status {
-        const size_t n = (size_t)m->info[problem].M * m->nz;
+        const size_t n = (size_t)m->info[problem].M * m->info[problem].nz;
         if (n) {
             CK(cudaMemcpyAsync(v, m->d_vfull.as<double>() + m->vfull_off[problem], n * 8, cudaMemcpyDeviceToHost,
                                m->ctx->stream));
@@ -1259,9 +1259,10 @@ ncpa_status ncpa_tl_1d(ncpa_ctx* ctx, const ncpa_modes* m, const ncpa_tl_params*
 
 ncpa_status ncpa_tl_2d_heights(const ncpa_modes* m, int problem, int* n_heights) {
     if (!m || !n_heights || problem < 0 || problem >= m->P) return NCPA_EINVAL;
-    int stepj = m->nz / 500;
+    const int nz = m->info[problem].nz;
+    int stepj = nz / 500;
     if (stepj == 0) stepj = 10;
-    *n_heights = (m->nz + stepj - 1) / stepj;
+    *n_heights = (nz + stepj - 1) / stepj;
     return NCPA_OK;
 }
 
@@ -1273,7 +1274,7 @@ ncpa_status ncpa_tl_2d(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const nc
         CK(cudaSetDevice(ctx->device));
         cudaStream_t st = ctx->stream;
         const ProblemInfo& pi = m->info[problem];
-        const int Mm = pi.M, nz = m->nz;
+        const int Mm = pi.M, nz = pi.nz;
         int stepj = nz / 500;
         if (stepj == 0) stepj = 10;
         const int nzo = (nz + stepj - 1) / stepj;
@@ -1286,9 +1287,9 @@ ncpa_status ncpa_tl_2d(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const nc
         CK(cudaStreamSynchronize(st));
         for (int j = 0; j < nzo; ++j) {
             std::memcpy(&vz[(size_t)j * Mm], &vfull[(size_t)j * stepj * Mm], Mm * 8);
-            if (z_out) z_out[j] = (j * stepj) * m->dz;
+            if (z_out) z_out[j] = (j * stepj) * pi.dz;
         }
-        if (Mm) std::memcpy(vsrc.data(), &vfull[(size_t)m->isrc * Mm], Mm * 8);
+        if (Mm) std::memcpy(vsrc.data(), &vfull[(size_t)pi.isrc * Mm], Mm * 8);
         DevBuf dvz, dvs, dre, dim;
         upload(dvz, vz, st);
         upload(dvs, vsrc, st);
@@ -1323,8 +1324,8 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
         // receiver grid points: ceil(z / dz) as ModeSolver.cpp:301 does
         std::vector<int> idx(n_rcv);
         for (int j = 0; j < n_rcv; ++j) {
-            const int k = (int)std::ceil(rcv_height_m[j] / m->dz);
-            if (k < 0 || k >= m->nz) throw ApiError(NCPA_EINVAL, "receiver height outside the grid");
+            const int k = (int)std::ceil(rcv_height_m[j] / pi.dz);
+            if (k < 0 || k >= pi.nz) throw ApiError(NCPA_EINVAL, "receiver height outside the grid");
             idx[j] = k;
         }
         const size_t nout = (size_t)n_rcv * nr;
@@ -1472,9 +1473,9 @@ ncpa_status ncpa_modal_starter(ncpa_ctx* ctx, const ncpa_modes* m, int problem, 
     return guarded(ctx, [&]() -> ncpa_status {
         const ProblemInfo& pi = m->info[problem];
         const double freq = pi.freq;
-        int step = (int)((340.0 / freq) / 10 / m->dz);  // ESSModeSolver.cpp:692-693
+        int step = (int)((340.0 / freq) / 10 / pi.dz);  // ESSModeSolver.cpp:692-693
         if (step < 1) step = 1;
-        const int nout = (m->nz + step - 1) / step;
+        const int nout = (pi.nz + step - 1) / step;
         if (!z_km || !re || !im) {
             *n_out = nout;
             return NCPA_OK;
@@ -1485,13 +1486,13 @@ ncpa_status ncpa_modal_starter(ncpa_ctx* ctx, const ncpa_modes* m, int problem, 
         DevBuf dout;
         dout.alloc((size_t)nout * 8, st);
         const double k0 = 2 * kPi * freq / 340.0;
-        check_launch(ctx, ncpa::launch_starter(st, pi.M, m->nz, step, m->isrc,
+        check_launch(ctx, ncpa::launch_starter(st, pi.M, pi.nz, step, pi.isrc,
                                                m->d_vfull.as<double>() + m->vfull_off[problem],
                                                m->d_kr.as<double>() + pi.off, k0, dout.as<double>()));
         CK(cudaMemcpyAsync(re, dout.p, nout * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         for (int j = 0; j < nout; ++j) {
-            z_km[j] = (j * step) * m->dz / 1000.0;
+            z_km[j] = (j * step) * pi.dz / 1000.0;
             im[j] = 0.0;
         }
         *n_out = nout;

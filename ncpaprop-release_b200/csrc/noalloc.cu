@@ -61,7 +61,7 @@ namespace {
 // copies the caller's diagonal and weights into the padded scratch copies and
 // writes the work list, the problem record and zeroed counters
 __global__ void k_static_setup(unsigned char* base, const double* __restrict__ s, const double* __restrict__ w,
-                               int nz, int n, double omega, double lo) {
+                               int nz, int n, double omega, double lo, double dz, int isrc, int ircv) {
     double* sc = reinterpret_cast<double*>(base + kOffS);
     double* wc = reinterpret_cast<double*>(base + kOffW);
     const int nz_pad = (nz + kStaticChunk - 1) / kStaticChunk * kStaticChunk;
@@ -81,6 +81,12 @@ __global__ void k_static_setup(unsigned char* base, const double* __restrict__ s
             *pi = ProblemInfo{};
             pi->omega = omega;
             pi->lo = lo;
+            pi->dz = dz;
+            pi->nz = nz;
+            pi->isrc = isrc;
+            pi->ircv = ircv;
+            pi->s_off = 0;
+            pi->w_off = 0;
             pi->M = n;
             pi->off = 0;
             int* counter = reinterpret_cast<int*>(base + kOffCounter);
@@ -116,25 +122,18 @@ extern "C" ncpa_status ncpa_eigvec_static(const double* s, const double* w, int 
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int nz_pad = (nz + kStaticChunk - 1) / kStaticChunk * kStaticChunk;
-    k_static_setup<<<(nz_pad + 255) / 256, 256, 0, st>>>(base, s, w, nz, n_modes, omega, 0.0);
+    k_static_setup<<<(nz_pad + 255) / 256, 256, 0, st>>>(base, s, w, nz, n_modes, omega, 0.0, dz, isrc,
+                                                             ircv);
     if (cudaGetLastError() != cudaSuccess) return NCPA_ECUDA;
     ncpa::EigvecArgs a{};
     a.pinfo = reinterpret_cast<const ProblemInfo*>(base + kOffInfo);
     a.s = reinterpret_cast<const double*>(base + kOffS);
     a.w = reinterpret_cast<const double*>(base + kOffW);
     a.g = nullptr;
-    a.nz = nz;
-    a.nz_pad = nz_pad;
-    a.wstride = nz_pad;
-    a.n_az = 1;
     a.items = reinterpret_cast<const WorkItem*>(base + kOffItems);
     a.n_items = (n_modes + ncpa::kEvItem - 1) / ncpa::kEvItem;
     a.counter = reinterpret_cast<int*>(base + kOffCounter);
     a.mu = mu;
-    a.isrc = isrc;
-    a.ircv = ircv;
-    a.dz = dz;
-    a.h2 = dz * dz;
     a.kr = re_k;
     a.ki = im_k;
     a.vs = v_src;

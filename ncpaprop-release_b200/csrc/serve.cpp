@@ -3,10 +3,11 @@
 // Requests (profile knots, frequencies, azimuth) are copied at submit and
 // queued.  Each worker lane owns one library context (one device stream) and
 // a host thread; a free lane takes the oldest queued request and every
-// further queued request that shares its solver grid, fits the per-batch
-// problem limit and fits the HBM budget, solves them in one
-// ncpa_ess_solve_jobs call plus one ncpa_tl_1d call, and hands each request
-// its slice.  With two or more lanes, requests that arrive while a batch is
+// further queued request that fits the per-batch problem limit and the HBM
+// budget, solves them in one ncpa_ess_solve_jobs call (requests whose
+// profiles give different solver grids share the batch: every problem
+// carries its own grid) plus one ncpa_tl_1d call, and hands each request its
+// slice.  With two or more lanes, requests that arrive while a batch is
 // on the device are admitted into the next batch on another lane, so their
 // work overlaps on the GPU.  A batch that fails is re-run request by
 // request so one bad request does not fail the others.
@@ -40,7 +41,6 @@ struct Request {
     std::vector<double> freqs;
     double az = 0.0;
     double est_bytes = 0.0;
-    double grid_key_top = 0.0, grid_key_ground = 0.0;  // requests sharing both share a solver grid
     Clock::time_point t_submit;
     // results
     bool done = false;
@@ -76,16 +76,6 @@ double estimate_bytes(const ncpa_server* s, const Request& r) {
     // modes (up to 2048 of 5 doubles), 1-D TL; plus the profile
     const double per_problem = 4.0 * 8.0 * s->nz_pad + 256 * 4 + 2048.0 * 5 * 8 + 3.0 * 8 * s->opts.n_ranges;
     return per_problem * (double)r.freqs.size() + 12.0 * 8 * r.n_knots;
-}
-
-// keys of the solver grid a request's profile gives (ESSModeSolver.cpp:
-// 144-151, 212-220): clamped top and raised ground
-void grid_keys(const ncpa_server* s, Request& r) {
-    const double top = std::min(s->opts.params.maxheight_km * 1000.0, r.z.back() - 1e-6);
-    double ground = s->opts.params.zground_km * 1000.0;
-    if (r.has_z0 && ground < r.z0) ground = r.z0;
-    r.grid_key_top = top;
-    r.grid_key_ground = ground;
 }
 
 ncpa_status create_profile(ncpa_ctx* ctx, const Request& r, ncpa_profile** out) {
@@ -180,24 +170,19 @@ void lane_main(ncpa_server* s, int lane) {
             };
             s->cv_work.wait(lk, [&] { return (s->stop && s->queue.empty()) || can_take(); });
             if (s->queue.empty()) return;  // stopping; queued work is finished before a lane stops
-            Request* first = s->queue.front();
             int problems = 0;
             for (auto it = s->queue.begin(); it != s->queue.end();) {
-                Request* r = *it;
-                const bool same_grid =
-                    r->grid_key_top == first->grid_key_top && r->grid_key_ground == first->grid_key_ground;
+                Request* r = *it;  // taken in arrival order while the batch limits hold
                 const bool fits_batch = batch.empty() || problems + (int)r->freqs.size() <= s->opts.max_batch_problems;
                 const bool fits_mem = (s->admitted_bytes == 0.0 && batch.empty()) ||
                                       s->admitted_bytes + bytes + r->est_bytes <= s->opts.hbm_budget_bytes;
-                if (same_grid && fits_batch && fits_mem) {
+                if (fits_batch && fits_mem) {
                     batch.push_back(r);
                     problems += (int)r->freqs.size();
                     bytes += r->est_bytes;
                     it = s->queue.erase(it);
-                } else if (!fits_batch || !fits_mem) {
-                    break;  // keep arrival order for what is left
                 } else {
-                    ++it;
+                    break;  // keep arrival order for what is left
                 }
             }
             s->admitted_bytes += bytes;
@@ -312,7 +297,6 @@ ncpa_status ncpa_server_submit(ncpa_server* s, const ncpa_request* req, unsigned
     r->freqs.assign(req->freqs, req->freqs + req->n_freq);
     r->az = req->az_deg;
     r->est_bytes = estimate_bytes(s, *r);
-    grid_keys(s, *r);
     {
         std::lock_guard<std::mutex> lk(s->mu);
         r->id = s->next_id++;

@@ -27,7 +27,7 @@ EXPORTED = [
     "ncpa_modes_info", "ncpa_modes_get", "ncpa_modes_get_vectors", "ncpa_tl_1d", "ncpa_tl_2d_heights",
     "ncpa_tl_2d", "ncpa_bb_synthesize", "ncpa_bb_synthesize_modes", "ncpa_source_spectrum_waveform",
     "ncpa_kernel_launches", "ncpa_ctx_stream", "ncpa_ctx_set_timing", "ncpa_ctx_phase_stats",
-    "ncpa_ctx_reset_stats", "ncpa_ctx_sturm_sequences", "ncpa_probe_fp64_peak", "ncpa_source_spectrum_builtin",
+    "ncpa_ctx_reset_stats", "ncpa_ctx_sturm_steps", "ncpa_probe_fp64_peak", "ncpa_source_spectrum_builtin",
     "ncpa_eigvec_static", "ncpa_profile_set_attn", "ncpa_profile_load_attn", "ncpa_profile_knots", "ncpa_profile_z0",
     "ncpa_modal_starter", "ncpa_source_waveform", "ncpa_tl_multi", "ncpa_ess_solve_jobs", "ncpa_server_opts_default", "ncpa_server_create",
     "ncpa_server_submit", "ncpa_server_wait", "ncpa_server_release", "ncpa_server_stats_get", "ncpa_server_destroy", "ncpa_modes_get_all",
@@ -50,7 +50,8 @@ class _ProfileDesc(ctypes.Structure):
 
 
 class _EssJob(ctypes.Structure):
-    _fields_ = [("profile", _vp), ("freqs", _dp), ("n_freq", _c_int), ("az_deg", _c_double)]
+    _fields_ = [("profile", _vp), ("freqs", _dp), ("n_freq", _c_int), ("az_deg", _c_double), ("nz_grid", _c_int),
+                ("n_az", _c_int), ("az_list", _dp)]
 
 
 class EssParams(ctypes.Structure):
@@ -123,7 +124,7 @@ def lib():
         L.ncpa_ctx_set_timing.argtypes = [_vp, _c_int]
         L.ncpa_ctx_phase_stats.argtypes = [_vp, ctypes.c_char_p, _dp, ctypes.POINTER(_c_ll)]
         L.ncpa_ctx_reset_stats.argtypes = [_vp]
-        L.ncpa_ctx_sturm_sequences.argtypes = [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]
+        L.ncpa_ctx_sturm_steps.argtypes = [_vp, ctypes.POINTER(_c_ll)]
         L.ncpa_probe_fp64_peak.argtypes = [_vp, _dp]
         L.ncpa_source_spectrum_builtin.argtypes = [_vp, _c_int, _dp, _c_int, _c_double, _c_int, _dp, _dp]
         _lib = L
@@ -200,11 +201,12 @@ class Context:
                    "ncpa_ctx_phase_stats")
         return ms.value, n.value
 
-    def sturm_sequences(self):
-        a, b = _c_ll(), _c_ll()
-        self.check(lib().ncpa_ctx_sturm_sequences(self.h, ctypes.byref(a), ctypes.byref(b)),
-                   "ncpa_ctx_sturm_sequences")
-        return a.value, b.value
+    def sturm_steps(self):
+        """Sturm recurrence steps run by the bisection kernel since the last
+        reset (counted while per-phase timing is on)."""
+        a = _c_ll()
+        self.check(lib().ncpa_ctx_sturm_steps(self.h, ctypes.byref(a)), "ncpa_ctx_sturm_steps")
+        return a.value
 
     def fp64_peak_tflops(self):
         t = _c_double()
@@ -238,16 +240,31 @@ class Context:
         return Modes(self, h, f, a)
 
     def solve_jobs(self, jobs, params: EssParams):
-        """One batched solve over jobs [(profile, freqs, azimuth_deg), ...];
-        problems are numbered job by job."""
-        keep = [_f64(np.atleast_1d(f)) for _, f, _ in jobs]
+        """One batched solve over jobs [(profile, freqs, azimuth_deg[, nz_grid]), ...].
+        azimuth_deg is a number or a list of azimuths (the job sweeps them);
+        nz_grid (optional, 0 = params.nz_grid) sets the job's own grid.
+        Problems are numbered job by job, frequency-major then azimuth."""
+        keep, azs, fr, az_all = [], [], [], []
         arr = (_EssJob * len(jobs))()
-        for i, ((prof, _, az), f) in enumerate(zip(jobs, keep)):
-            arr[i] = _EssJob(prof.h.value, _p(f), len(f), float(az))
+        for i, job in enumerate(jobs):
+            prof, freqs, az = job[0], job[1], job[2]
+            nz = int(job[3]) if len(job) > 3 else 0
+            f = _f64(np.atleast_1d(freqs))
+            keep.append(f)
+            if np.ndim(az) == 0:
+                arr[i] = _EssJob(prof.h.value, _p(f), len(f), float(az), nz, 0, None)
+                fr.append(f)
+                az_all.append(np.full(len(f), float(az)))
+            else:
+                a = _f64(np.atleast_1d(az))
+                azs.append(a)
+                arr[i] = _EssJob(prof.h.value, _p(f), len(f), float(a[0]), nz, len(a), _p(a))
+                fr.append(np.repeat(f, len(a)))
+                az_all.append(np.tile(a, len(f)))
         h = _vp()
         self.check(lib().ncpa_ess_solve_jobs(self.h, arr, len(jobs), ctypes.byref(params), ctypes.byref(h)),
                    "ncpa_ess_solve_jobs")
-        return Modes(self, h, np.concatenate(keep), np.array([j[2] for j in jobs], dtype=np.float64))
+        return Modes(self, h, np.concatenate(fr), np.concatenate(az_all))
 
     SOURCES = {"impulse": 0, "pulse1": 1, "pulse2": 2}
 

@@ -80,6 +80,21 @@ def broadband_freqs(n=256, f_max=0.5):
 
 
 # ---------------------------------------------------------------------------
+# azimuth sweep (one batch of mixed grid sizes)
+# ---------------------------------------------------------------------------
+def sweep_freqs(n=8, f_lo=0.1, f_hi=2.0):
+    """Frequencies of the azimuth-sweep workload: n log-spaced in [f_lo, f_hi]."""
+    return np.exp(np.linspace(np.log(f_lo), np.log(f_hi), n))
+
+
+def sweep_nz(f, top_km=150.0, c=300.0, points_per_wavelength=60, nz_min=5000):
+    """Grid size of the azimuth sweep: points_per_wavelength points per
+    wavelength c / f over the atmosphere, at least nz_min.  With the defaults
+    Nz runs from 5000 (0.1 Hz, floor) to 60000 (2 Hz)."""
+    return max(nz_min, int(np.ceil(points_per_wavelength * top_km * 1000.0 * f / c)))
+
+
+# ---------------------------------------------------------------------------
 # served request stream
 # ---------------------------------------------------------------------------
 _GP_CHOL = {}
