@@ -307,6 +307,44 @@ long long ncpa_kernel_launches(const ncpa_ctx *ctx);
 /* The context's CUDA stream (cudaStream_t) for event timing / interop. */
 void *ncpa_ctx_stream(ncpa_ctx *ctx);
 
+/* Captured solves ("plans"; no counterpart in the reference, whose
+ * ESSModeSolver::solve, ESSModeSolver.cpp:291-510, re-runs setParams and the
+ * SLEPc solve per problem).  A plan fixes the shape of a batched solve
+ * without eigenvectors -- the jobs' profiles, frequencies, azimuths and grids,
+ * the params and an optional 1-D TL range grid -- allocates every buffer once
+ * and records the whole device sequence (knot splines, matrices, window,
+ * Sturm scan, device-built work items, bisection, eigenvectors, 1-D TL) as ONE
+ * CUDA graph.  ncpa_ess_plan_run replays it with one launch and waits once
+ * for the totals.  The graph reads the profiles' device arrays, so
+ * ncpa_profile_update followed by a run re-solves new atmospheric data of the
+ * same shape.  With tune != 0 the plan times candidate launch shapes
+ * (eigenvalues per bisection item; CTAs per SM of the bisection and of the
+ * eigenvector kernel) by replaying captured graphs and keeps the fastest; the
+ * choice is cached in the context per batch shape.  Another item size than
+ * the default changes the bisection's bracketing, so eigenvalues may differ
+ * from ncpa_ess_solve's in the last bits (well inside the 1e-9 relative
+ * parity bound).  Plans need want_vectors = 0 and lamb_wave_bc = 0 (both
+ * need host work inside the solve).  The profiles and the context must
+ * outlive the plan. */
+typedef struct ncpa_plan ncpa_plan;
+ncpa_status ncpa_ess_plan_create(ncpa_ctx *ctx, const ncpa_ess_job *jobs, int n_jobs,
+                                 const ncpa_ess_params *params, const ncpa_tl_params *tl, int tune,
+                                 ncpa_plan **out);
+ncpa_status ncpa_ess_plan_run(ncpa_plan *plan);
+/* the result of the last run; owned by the plan (do not destroy it) */
+ncpa_status ncpa_ess_plan_modes(ncpa_plan *plan, ncpa_modes **modes);
+/* 1-D TL of the last run, [problem][range] on the plan's range grid */
+ncpa_status ncpa_ess_plan_tl(ncpa_plan *plan, double *re, double *im, double *incoh);
+/* launch shapes in use; ms = replay time of the chosen graph when tuned, else 0 */
+ncpa_status ncpa_ess_plan_tuning(const ncpa_plan *plan, int *bis_item, int *bis_ctas_per_sm,
+                                 int *ev_ctas_per_sm, double *ms);
+ncpa_status ncpa_ess_plan_destroy(ncpa_plan *plan);
+/* New knot values for a profile, in place: same knot count, altitudes and
+ * ground height, and an attenuation column exactly when the profile has one
+ * (desc->attn replaces it).  Plans that read the profile see the new data at
+ * their next run. */
+ncpa_status ncpa_profile_update(ncpa_profile *prof, const ncpa_profile_desc *desc);
+
 /* Diagnostics (no counterpart in the reference): per-phase device times of
  * ncpa_ess_solve measured with CUDA events on the context stream.  Phases:
  * "knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec",

@@ -825,9 +825,9 @@ __device__ int block_exclusive_scan(int v, int* sh, int* total) {
 
 __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo* __restrict__ pinfo,
                                                              const int* __restrict__ counts, int max_modes,
-                                                             WorkItem* __restrict__ bis, WorkItem* __restrict__ ev,
-                                                             int item_cap, int* __restrict__ tot,
-                                                             unsigned* __restrict__ err) {
+                                                             int bis_item, WorkItem* __restrict__ bis, int bis_cap,
+                                                             WorkItem* __restrict__ ev, int ev_cap,
+                                                             int* __restrict__ tot, unsigned* __restrict__ err) {
     __shared__ int sh[kItemThreads];
     int base_m = 0, base_b = 0, base_e = 0;
     for (int p0 = 0; p0 < P; p0 += kItemThreads) {
@@ -844,7 +844,7 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
             pinfo[p].c_lo = c_lo;
             pinfo[p].c_hi = c_hi;
             pinfo[p].M = M;
-            nb = (M + kWItem - 1) / kWItem;
+            nb = (M + bis_item - 1) / bis_item;
             ne = (M + kEvItem - 1) / kEvItem;
         }
         int tm, tb, te;
@@ -856,11 +856,11 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
             for (int k = 0; k < nb; ++k) {
                 const int j0 = (int)((long long)M * k / nb), j1 = (int)((long long)M * (k + 1) / nb);
                 const int q = base_b + ob + k;
-                if (q < item_cap) bis[q] = WorkItem{p, j0, j1 - j0, 0};
+                if (q < bis_cap) bis[q] = WorkItem{p, j0, j1 - j0, 0};
             }
             for (int k = 0; k < ne; ++k) {
                 const int q = base_e + oe + k;
-                if (q < item_cap) ev[q] = WorkItem{p, k * kEvItem, min(kEvItem, M - k * kEvItem), 0};
+                if (q < ev_cap) ev[q] = WorkItem{p, k * kEvItem, min(kEvItem, M - k * kEvItem), 0};
             }
         }
         base_m += tm;
@@ -868,16 +868,18 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
         base_e += te;
     }
     if (threadIdx.x == 0) {
-        if (base_b > item_cap || base_e > item_cap) atomicOr(err, kErrTooMany);
-        tot[0] = min(base_b, item_cap);
-        tot[1] = min(base_e, item_cap);
+        if (base_b > bis_cap || base_e > ev_cap) atomicOr(err, kErrTooMany);
+        tot[0] = min(base_b, bis_cap);
+        tot[1] = min(base_e, ev_cap);
         tot[2] = base_m;
     }
 }
 
-int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes,
-                      WorkItem* bis_items, WorkItem* ev_items, int item_cap, int* tot, unsigned* err) {
-    k_make_items<<<1, kItemThreads, 0, st>>>(P, pinfo, counts, max_modes, bis_items, ev_items, item_cap, tot, err);
+int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes, int bis_item,
+                      WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err) {
+    if (bis_item < 1 || bis_item > kWItem) return -1;
+    k_make_items<<<1, kItemThreads, 0, st>>>(P, pinfo, counts, max_modes, bis_item, bis_items, bis_cap, ev_items,
+                                             ev_cap, tot, err);
     return 1;
 }
 

@@ -114,12 +114,12 @@ struct EigvecArgs {
 };
 int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a);
 // Work items built on the device from the Sturm scan: per problem c_lo, c_hi,
-// M and CSR offset in pinfo; bisection items (32 eigenvalues, balanced) and
-// eigenvector items (kEvItem) appended; tot = {n_bisect_items, n_eigvec_items,
-// total modes}.  Sets kErrTooMany if a problem exceeds max_modes (its M is
-// then clamped) or the item capacity is exceeded.
-int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes,
-                      WorkItem* bis_items, WorkItem* ev_items, int item_cap, int* tot, unsigned* err);
+// M and CSR offset in pinfo; bisection items (<= bis_item eigenvalues, sizes
+// balanced inside a problem) and eigenvector items (kEvItem) appended;
+// tot = {n_bisect_items, n_eigvec_items, total modes}.  Sets kErrTooMany if a
+// problem exceeds max_modes (its M is then clamped) or a capacity is exceeded.
+int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes, int bis_item,
+                      WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err);
 // resident eigenvector CTAs per SM for the variant selected by a
 int eigvec_ctas_per_sm(const EigvecArgs& a);
 // modal sums

@@ -5,6 +5,7 @@
 #include "ncpa_gpu.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -121,6 +122,7 @@ struct ncpa_ctx {
     bool timing = false;           // NCPA_TIMING=1: per-phase times on stderr
     bool stats = false;            // ncpa_ctx_set_timing: accumulate per phase
     std::map<std::string, std::pair<double, long long>> phase;
+    std::map<std::string, std::array<int, 3>> tune_cache;  // plan shape -> tuned launch shapes
     void count(int n) { launches += n; }
 };
 
@@ -164,6 +166,7 @@ struct ncpa_profile {
     double z0 = 0.0;
     int has_z0 = 0;
     double z_lo = 0.0, z_hi = 0.0;
+    int plan_refs = 0;  // plans whose graphs read this profile's arrays
 };
 
 struct ncpa_modes {
@@ -174,6 +177,7 @@ struct ncpa_modes {
     std::vector<double> freqs, az;
     std::vector<double> rho_src_p, rho_rcv_p;  // rho at the source / receiver grid points, per problem
     bool multi_job = false;                     // built by ncpa_ess_solve_jobs (one profile per job)
+    bool plan_owned = false;                    // the arrays are a plan's graph buffers
     std::vector<ProblemInfo> info;
     int Mtot = 0;
     DevBuf d_pinfo, d_kr, d_ki, d_vs, d_vr, d_vg, d_vfull, d_vfull_off;
@@ -303,176 +307,278 @@ Geometry grid_geometry(const ncpa_profile* prof, const ncpa_ess_params* prm, int
     return g;
 }
 
-// Knot-level fields, grid fields and matrices of the n_freq x n_az problems
-// of one profile.  d_pinfo, s, g, kz2 point at the group's first problem; w
-// at the group's first frequency slot.  The ProblemInfo records (freq,
-// omega, az) must be on the device already.  rho at the source and receiver
-// grid points is copied to rho_pair[0..1] (pinned host memory, valid after
-// the next stream synchronisation).
-void build_problems(ncpa_ctx* ctx, PhaseTimer& tm, const ncpa_profile* prof, const ncpa_ess_params* prm,
-                    const Geometry& geo, int nz, int nz_pad, const double* freqs, int n_freq, const double* az_deg,
-                    int n_az, bool wkb, ProblemInfo* d_pinfo, double* s, double* w, double* g, double* kz2,
-                    double* rho_pair) {
+// One group of problems: one profile on one solver grid, n_freq x n_az
+// problems numbered frequency-major from p0.  Its rows start at s_base in
+// s, g and kz2 (nz_pad apart) and at w_base in w (one row per frequency).
+struct Group {
+    const ncpa_profile* prof;
+    Geometry geo;
+    int nz, nz_pad;
+    const double* freqs;
+    int n_freq;
+    const double* az;
+    int n_az;
+    int p0;
+    long long s_base, w_base;
+};
+
+Group make_group(const ncpa_profile* prof, const ncpa_ess_params* prm, int nz, const double* freqs, int n_freq,
+                 const double* az, int n_az) {
+    Group g{};
+    g.prof = prof;
+    g.geo = grid_geometry(prof, prm, nz);
+    g.nz = nz;
+    g.nz_pad = ((nz + ncpa::kChunk - 1) / ncpa::kChunk) * ncpa::kChunk;
+    g.freqs = freqs;
+    g.n_freq = n_freq;
+    g.az = az;
+    g.n_az = n_az;
+    return g;
+}
+
+// Ground admittance of the Lamb-wave condition, -rho'(z0) / (2 rho(z0)), from
+// one point of the profile's rho spline and its slope (scalar set-up, as in
+// ESSModeSolver.cpp:347-349).  Synchronises the stream.
+double lamb_admittance(ncpa_ctx* ctx, const ncpa_profile* prof, double z_min) {
     cudaStream_t st = ctx->stream;
     const int nk = prof->n;
-    const int P = n_freq * n_az;
-    DevBuf d_freqs, d_az;
-    upload(d_freqs, freqs, n_freq, st);
-    upload(d_az, az_deg, n_az, st);
-    DevBuf ceffk, ceffc, alpha, alphac;
-    ceffk.alloc((size_t)n_az * nk * 8, st);
-    ceffc.alloc((size_t)n_az * 4 * (nk - 1) * 8, st);
-    check_launch(ctx, ncpa::launch_ceff_knots(st, nk, n_az, d_az.as<double>(), prof->c0.as<double>(),
-                                              prof->ws.as<double>(), prof->wd.as<double>(), ceffk.as<double>()));
-    check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), ceffk.as<double>(), n_az, nk,
-                                           ceffc.as<double>(), 4 * (nk - 1)));
-    alpha.alloc((size_t)n_freq * nk * 8, st);
-    alphac.alloc((size_t)n_freq * 4 * (nk - 1) * 8, st);
+    std::vector<double> hz(nk), hc(4 * (nk - 1)), hr(nk);
+    CK(cudaMemcpyAsync(hz.data(), prof->z.p, nk * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hr.data(), prof->rho.p, nk * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hc.data(), prof->rcoef.p, hc.size() * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double zq = z_min, val, der;
+    if (zq > hz[nk - 1] || zq < hz[0]) {
+        val = zq > hz[nk - 1] ? hr[nk - 1] : hr[0];
+        der = 0.0;
+    } else {
+        int lo = 0, hi = nk - 1;
+        while (hi > lo + 1) {
+            int mid = (lo + hi) / 2;
+            if (hz[mid] > zq) hi = mid; else lo = mid;
+        }
+        const double* c = &hc[4 * lo];
+        double t = zq - hz[lo];
+        val = c[3] + t * (c[2] + t * (c[1] + t * c[0]));
+        der = c[2] + t * (2.0 * c[1] + t * 3.0 * c[0]);
+    }
+    return -der / val / 2.0;
+}
+
+// Device buffers of one group's knot-level and grid-level stages.
+struct GroupBufs {
+    DevBuf freqs, az, ceffk, ceffc, alpha, alphac, rho_g, ct_g;
+    double admittance = 0.0;
+};
+
+// Allocates a group's buffers, uploads its frequencies and azimuths and, with
+// the Lamb-wave condition, computes the ground admittance (host work that
+// stays outside any captured graph).
+void prepare_group(ncpa_ctx* ctx, const ncpa_ess_params* prm, const Group& g, GroupBufs& b) {
+    cudaStream_t st = ctx->stream;
+    const int nk = g.prof->n;
+    upload(b.freqs, g.freqs, g.n_freq, st);
+    upload(b.az, g.az, g.n_az, st);
+    b.ceffk.alloc((size_t)g.n_az * nk * 8, st);
+    b.ceffc.alloc((size_t)g.n_az * 4 * (nk - 1) * 8, st);
+    b.alpha.alloc((size_t)g.n_freq * nk * 8, st);
+    b.alphac.alloc((size_t)g.n_freq * 4 * (nk - 1) * 8, st);
+    b.rho_g.alloc((size_t)g.nz * 8, st);
+    b.ct_g.alloc((size_t)g.nz * 8, st);
+    b.admittance = prm->lamb_wave_bc ? lamb_admittance(ctx, g.prof, g.geo.z_min) : 0.0;
+}
+
+// Knot-level fields, grid fields and matrices of one group's problems: only
+// kernel launches, device copies and memsets, plus one copy of rho at the
+// source and receiver grid points to rho_pair[0..1] (pinned host memory when
+// captured).  d_pinfo, s, w, gs, kz2 point at the group's first problem / row.
+void enqueue_group(ncpa_ctx* ctx, PhaseTimer& tm, const Group& g, GroupBufs& b, bool wkb, ProblemInfo* d_pinfo,
+                   double* s, double* w, double* gs, double* kz2, double* rho_pair) {
+    cudaStream_t st = ctx->stream;
+    const ncpa_profile* prof = g.prof;
+    const int nk = prof->n;
+    const int P = g.n_freq * g.n_az;
+    check_launch(ctx, ncpa::launch_ceff_knots(st, nk, g.n_az, b.az.as<double>(), prof->c0.as<double>(),
+                                              prof->ws.as<double>(), prof->wd.as<double>(), b.ceffk.as<double>()));
+    check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), b.ceffk.as<double>(), g.n_az, nk,
+                                           b.ceffc.as<double>(), 4 * (nk - 1)));
     if (prof->has_attn) {
-        for (int f = 0; f < n_freq; ++f)
-            CK(cudaMemcpyAsync(alpha.as<double>() + (size_t)f * nk, prof->attn.p, nk * 8, cudaMemcpyDeviceToDevice,
+        for (int f = 0; f < g.n_freq; ++f)
+            CK(cudaMemcpyAsync(b.alpha.as<double>() + (size_t)f * nk, prof->attn.p, nk * 8, cudaMemcpyDeviceToDevice,
                                st));
     } else {
-        check_launch(ctx, ncpa::launch_alpha_knots(st, nk, n_freq, d_freqs.as<double>(), prof->z.as<double>(),
+        check_launch(ctx, ncpa::launch_alpha_knots(st, nk, g.n_freq, b.freqs.as<double>(), prof->z.as<double>(),
                                                    prof->t.as<double>(), prof->p.as<double>(),
-                                                   prof->rho.as<double>(), alpha.as<double>()));
+                                                   prof->rho.as<double>(), b.alpha.as<double>()));
     }
-    check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), alpha.as<double>(), n_freq, nk,
-                                           alphac.as<double>(), 4 * (nk - 1)));
+    check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), b.alpha.as<double>(), g.n_freq, nk,
+                                           b.alphac.as<double>(), 4 * (nk - 1)));
     // ---- grid fields ----
-    DevBuf rho_g, ct_g;
-    rho_g.alloc((size_t)nz * 8, st);
-    ct_g.alloc((size_t)nz * 8, st);
-    CK(cudaMemsetAsync(w, 0, (size_t)n_freq * nz_pad * 8, st));
+    CK(cudaMemsetAsync(w, 0, (size_t)g.n_freq * g.nz_pad * 8, st));
     check_launch(ctx, ncpa::launch_grid_common(st, nk, prof->z.as<double>(), prof->rho.as<double>(),
                                                prof->rcoef.as<double>(), prof->p.as<double>(),
-                                               prof->pcoef.as<double>(), nz, geo.z_min, geo.dz_grid,
-                                               rho_g.as<double>(), ct_g.as<double>()));
-    check_launch(ctx, ncpa::launch_attn_weight(st, nk, prof->z.as<double>(), alpha.as<double>(), alphac.as<double>(),
-                                               n_freq, d_freqs.as<double>(), nz, geo.z_min, geo.dz_grid,
-                                               ct_g.as<double>(), w, nz_pad));
-    // admittance for the Lamb wave condition: -rho'(z0) / (2 rho(z0))
-    double admittance = 0.0;
-    CK(cudaMemcpyAsync(rho_pair, rho_g.as<double>() + geo.isrc, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(rho_pair + 1, rho_g.as<double>() + geo.ircv, 8, cudaMemcpyDeviceToHost, st));
-    if (prm->lamb_wave_bc) {
-        std::vector<double> hz(nk), hc(4 * (nk - 1)), hr(nk);
-        CK(cudaMemcpyAsync(hz.data(), prof->z.p, nk * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(hr.data(), prof->rho.p, nk * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(hc.data(), prof->rcoef.p, hc.size() * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        // one point of the rho spline and its slope (scalar set-up, as in
-        // ESSModeSolver.cpp:347-349)
-        double zq = geo.z_min, val, der;
-        if (zq > hz[nk - 1] || zq < hz[0]) {
-            val = zq > hz[nk - 1] ? hr[nk - 1] : hr[0];
-            der = 0.0;
-        } else {
-            int lo = 0, hi = nk - 1;
-            while (hi > lo + 1) {
-                int mid = (lo + hi) / 2;
-                if (hz[mid] > zq) hi = mid; else lo = mid;
-            }
-            const double* c = &hc[4 * lo];
-            double t = zq - hz[lo];
-            val = c[3] + t * (c[2] + t * (c[1] + t * c[0]));
-            der = c[2] + t * (2.0 * c[1] + t * 3.0 * c[0]);
-        }
-        admittance = -der / val / 2.0;
-    }
+                                               prof->pcoef.as<double>(), g.nz, g.geo.z_min, g.geo.dz_grid,
+                                               b.rho_g.as<double>(), b.ct_g.as<double>()));
+    check_launch(ctx, ncpa::launch_attn_weight(st, nk, prof->z.as<double>(), b.alpha.as<double>(),
+                                               b.alphac.as<double>(), g.n_freq, b.freqs.as<double>(), g.nz,
+                                               g.geo.z_min, g.geo.dz_grid, b.ct_g.as<double>(), w, g.nz_pad));
+    CK(cudaMemcpyAsync(rho_pair, b.rho_g.as<double>() + g.geo.isrc, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(rho_pair + 1, b.rho_g.as<double>() + g.geo.ircv, 8, cudaMemcpyDeviceToHost, st));
     tm.mark("knots+grid");
     // ---- K1 matrix ----
-    check_launch(ctx, ncpa::launch_build_matrix(st, nk, prof->z.as<double>(), ceffk.as<double>(), ceffc.as<double>(),
-                                                n_az, P, d_pinfo, nz, nz_pad, geo.z_min, geo.dz_grid, geo.dz,
-                                                admittance, s, wkb ? kz2 : nullptr, g));
+    check_launch(ctx, ncpa::launch_build_matrix(st, nk, prof->z.as<double>(), b.ceffk.as<double>(),
+                                                b.ceffc.as<double>(), g.n_az, P, d_pinfo, g.nz, g.nz_pad,
+                                                g.geo.z_min, g.geo.dz_grid, g.geo.dz, b.admittance, s,
+                                                wkb ? kz2 : nullptr, gs));
     tm.mark("matrix");
 }
 
-// Bisection and eigenvectors with the work items built on the device from
-// the scan counts (k_make_items): the host enqueues everything without a
-// round trip and reads the mode counts back once at the end.  Output arrays
-// are sized for max_modes per problem.
-void solve_core_device_items(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_params* prm, DevBuf& s,
-                             DevBuf& w, DevBuf& g, DevBuf& counts) {
-    cudaStream_t st = ctx->stream;
-    const int P = M->P;
-    ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
-    const int cap_modes = M->prm.max_modes;
-    const size_t mcap = (size_t)P * cap_modes;
-    const int item_cap = P * ((cap_modes + ncpa::kWItem - 1) / ncpa::kWItem);
-    DevBuf bis, ev, tot, mu, d_counter;
-    bis.alloc((size_t)item_cap * sizeof(WorkItem), st);
-    ev.alloc((size_t)item_cap * sizeof(WorkItem), st);
-    tot.alloc(4 * sizeof(int), st);
-    check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, counts.as<int>(), cap_modes, bis.as<WorkItem>(),
-                                              ev.as<WorkItem>(), item_cap, tot.as<int>(), ctx->d_err.as<unsigned>()));
-    mu.alloc(mcap * 8, st);
-    M->d_kr.alloc(mcap * 8, st);
-    M->d_ki.alloc(mcap * 8, st);
-    M->d_vs.alloc(mcap * 8, st);
-    M->d_vr.alloc(mcap * 8, st);
-    M->d_vg.alloc(mcap * 8, st);
-    d_counter.alloc(2 * sizeof(int), st);
-    CK(cudaMemsetAsync(d_counter.p, 0, 2 * sizeof(int), st));
-    tm.mark("host-items");
-    const int grid_b = ctx->num_sms * ncpa::bisect_ctas_per_sm();
-    check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s.as<double>(), counts.as<int>(), bis.as<WorkItem>(),
-                                          0, d_counter.as<int>(), kBisectTol, mu.as<double>(),
-                                          ctx->d_err.as<unsigned>(),
-                                          ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr,
-                                          tot.as<int>()));
-    tm.mark("bisect");
+// Launch shapes of the device-driven eigen-solve (the autotuner's knobs).
+struct Tuning {
+    int bis_item = ncpa::kWItem;  // eigenvalues per bisection work item (<= 32)
+    int bis_ctas = 0;             // bisection CTAs per SM (0: as many as fit)
+    int ev_ctas = 0;              // eigenvector CTAs per SM (0: as many as fit)
+};
+
+// Buffers of the device-driven eigen-solve.  The eigenvector checkpoint
+// scratch is the context's (grown on demand) unless own_ck is set (a
+// captured graph must keep its addresses for good).
+struct SolveBufs {
+    DevBuf counts, bis, ev, tot, mu, counter;
+    DevBuf ck1, ck2, cke;
+    bool own_ck = false;
+    int bis_cap = 0, ev_cap = 0;
+};
+
+ncpa::EigvecArgs eigvec_args(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, double* s, double* w,
+                             double* gs, SolveBufs& b) {
     ncpa::EigvecArgs ea{};
-    ea.pinfo = d_pinfo;
-    ea.s = s.as<double>();
-    ea.w = w.as<double>();
-    ea.g = prm->want_group_speed ? g.as<double>() : nullptr;
-    ea.items = ev.as<WorkItem>();
+    ea.pinfo = M->d_pinfo.as<ProblemInfo>();
+    ea.s = s;
+    ea.w = w;
+    ea.g = prm->want_group_speed ? gs : nullptr;
+    ea.items = b.ev.as<WorkItem>();
     ea.n_items = 0;
-    ea.n_items_dev = tot.as<int>() + 1;
-    ea.counter = d_counter.as<int>() + 1;
-    ea.mu = mu.as<double>();
+    ea.n_items_dev = b.tot.as<int>() + 1;
+    ea.counter = b.counter.as<int>() + 1;
+    ea.mu = b.mu.as<double>();
     ea.kr = M->d_kr.as<double>();
     ea.ki = M->d_ki.as<double>();
     ea.vs = M->d_vs.as<double>();
     ea.vr = M->d_vr.as<double>();
     ea.vg = M->d_vg.as<double>();
-    const int ewpc = ncpa::kEvWarpsPerCta;
-    const int grid_e = std::min(item_cap / ewpc + 1, ctx->num_sms * ncpa::eigvec_ctas_per_sm(ea));
-    const long long nblk = (M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk;
-    const long long slot = nblk * 32;
-    const size_t need = (size_t)grid_e * ewpc * slot;
-    if (ctx->ck1.bytes < need * 8) {
-        ctx->ck1.alloc(need * 8, st);
-        ctx->ck2.alloc(need * 8, st);
-        ctx->cke.alloc(need * 4, st);
-    }
-    ea.ck_q1 = ctx->ck1.as<double>();
-    ea.ck_q2 = ctx->ck2.as<double>();
-    ea.ck_e = ctx->cke.as<int>();
-    ea.ck_slot_stride = slot;
     ea.err = ctx->d_err.as<unsigned>();
+    return ea;
+}
+
+int eigvec_grid(ncpa_ctx* ctx, const ncpa::EigvecArgs& ea, int ev_cap, int ctas_per_sm) {
+    const int fit = ncpa::eigvec_ctas_per_sm(ea);
+    const int per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, fit) : fit;
+    return std::max(1, std::min(ev_cap / ncpa::kEvWarpsPerCta + 1, ctx->num_sms * per_sm));
+}
+
+// Allocates the eigen-solve's buffers and the mode arrays (max_modes per
+// problem) and sizes the eigenvector checkpoint scratch for the largest grid
+// any of the given tunings launches.  min_bis_item sizes the bisection item
+// list for the smallest item size that will run.
+void prepare_solve(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, int min_bis_item, SolveBufs& b,
+                   double* s, double* w, double* gs) {
+    cudaStream_t st = ctx->stream;
+    const int P = M->P;
+    const int cap_modes = M->prm.max_modes;
+    const size_t mcap = (size_t)P * cap_modes;
+    b.counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
+    b.bis_cap = P * ((cap_modes + min_bis_item - 1) / min_bis_item);
+    b.ev_cap = P * ((cap_modes + ncpa::kEvItem - 1) / ncpa::kEvItem);
+    b.bis.alloc((size_t)b.bis_cap * sizeof(WorkItem), st);
+    b.ev.alloc((size_t)b.ev_cap * sizeof(WorkItem), st);
+    b.tot.alloc(4 * sizeof(int), st);
+    b.mu.alloc(mcap * 8, st);
+    b.counter.alloc(2 * sizeof(int), st);
+    M->d_kr.alloc(mcap * 8, st);
+    M->d_ki.alloc(mcap * 8, st);
+    M->d_vs.alloc(mcap * 8, st);
+    M->d_vr.alloc(mcap * 8, st);
+    M->d_vg.alloc(mcap * 8, st);
+    const ncpa::EigvecArgs ea = eigvec_args(ctx, M, prm, s, w, gs, b);
+    const int grid_e = eigvec_grid(ctx, ea, b.ev_cap, 0);  // the largest grid
+    const long long slot = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
+    const size_t need = (size_t)grid_e * ncpa::kEvWarpsPerCta * slot;
+    DevBuf& c1 = b.own_ck ? b.ck1 : ctx->ck1;
+    DevBuf& c2 = b.own_ck ? b.ck2 : ctx->ck2;
+    DevBuf& ce = b.own_ck ? b.cke : ctx->cke;
+    if (c1.bytes < need * 8) {
+        c1.alloc(need * 8, st);
+        c2.alloc(need * 8, st);
+        ce.alloc(need * 4, st);
+    }
+}
+
+// Window, Sturm scan, device-built work items, bisection and eigenvectors
+// over all problems of M, then copies of the item/mode totals, the problem
+// records and the device status word to tot_dst, info_dst and err_dst.  No
+// host synchronisation: the whole sequence can be captured in a CUDA graph.
+void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_params* prm, bool wkb, double* s,
+                   double* w, double* gs, double* kz2, SolveBufs& b, const Tuning& t, bool count_steps,
+                   int* tot_dst, ProblemInfo* info_dst, unsigned* err_dst) {
+    cudaStream_t st = ctx->stream;
+    const int P = M->P;
+    ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
+    unsigned* err = ctx->d_err.as<unsigned>();
+    // ---- K2 window ----
+    check_launch(ctx, ncpa::launch_window(st, P, d_pinfo, wkb ? kz2 : nullptr, wkb ? 1 : 0, prm->wvnum_filter,
+                                          prm->c_min, prm->c_max, err));
+    tm.mark("window");
+    // ---- K3a scan ----
+    check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s, b.counts.as<int>(), err));
+    tm.mark("scan");
+    check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, b.counts.as<int>(), M->prm.max_modes, t.bis_item,
+                                              b.bis.as<WorkItem>(), b.bis_cap, b.ev.as<WorkItem>(), b.ev_cap,
+                                              b.tot.as<int>(), err));
+    CK(cudaMemsetAsync(b.counter.p, 0, 2 * sizeof(int), st));
+    tm.mark("host-items");
+    // ---- K3 bisection ----
+    const int fit_b = ncpa::bisect_ctas_per_sm();
+    const int grid_b = ctx->num_sms * (t.bis_ctas > 0 ? std::min(t.bis_ctas, fit_b) : fit_b);
+    check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s, b.counts.as<int>(), b.bis.as<WorkItem>(), 0,
+                                          b.counter.as<int>(), kBisectTol, b.mu.as<double>(), err,
+                                          count_steps ? ctx->d_stats.as<unsigned long long>() : nullptr,
+                                          b.tot.as<int>()));
+    tm.mark("bisect");
+    // ---- K4 eigenvectors ----
+    ncpa::EigvecArgs ea = eigvec_args(ctx, M, prm, s, w, gs, b);
+    const int grid_e = eigvec_grid(ctx, ea, b.ev_cap, t.ev_ctas);
+    ea.ck_q1 = (b.own_ck ? b.ck1 : ctx->ck1).as<double>();
+    ea.ck_q2 = (b.own_ck ? b.ck2 : ctx->ck2).as<double>();
+    ea.ck_e = (b.own_ck ? b.cke : ctx->cke).as<int>();
+    ea.ck_slot_stride = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
     check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
     tm.mark("eigvec");
-    // ---- counts and offsets back, then the modes ----
-    int* h_tot = ctx->h_tot;
-    CK(cudaMemcpyAsync(h_tot, tot.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(M->info.data(), d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
-    unsigned h_err = 0;
-    CK(cudaMemcpyAsync(&h_err, ctx->d_err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(tot_dst, b.tot.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(info_dst, d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(err_dst, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+}
+
+// After enqueue_solve: waits for the stream, reports a problem above
+// max_modes and device errors, records the mode total and fetches the modes
+// to the host mirror unless they stay on the device.
+void finish_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const int* tot, const unsigned* err) {
+    cudaStream_t st = ctx->stream;
     CK(cudaStreamSynchronize(st));
-    if (h_err & ncpa::kErrTooMany) {
+    if (*err & ncpa::kErrTooMany) {
         CK(cudaMemsetAsync(ctx->d_err.p, 0, sizeof(unsigned), st));
         int worst = 0;
-        for (int p = 0; p < P; ++p)
+        for (int p = 0; p < M->P; ++p)
             if (M->info[p].c_hi - M->info[p].c_lo > M->info[worst].c_hi - M->info[worst].c_lo) worst = p;
         char buf[160];
         std::snprintf(buf, sizeof buf, "problem %d (f=%g Hz, az=%g) has %d modes > max_modes %d", worst,
-                      M->info[worst].freq, M->info[worst].az, M->info[worst].c_hi - M->info[worst].c_lo, cap_modes);
+                      M->info[worst].freq, M->info[worst].az, M->info[worst].c_hi - M->info[worst].c_lo,
+                      M->prm.max_modes);
         throw ApiError(NCPA_ETOOMANY, buf);
     }
-    M->Mtot = h_tot[2];
-    if (!prm->keep_on_device) fetch_modes(M);
+    M->Mtot = tot[2];
+    M->host_valid = false;
+    if (!M->prm.keep_on_device) fetch_modes(M);
     check_device_status(ctx);
     tm.mark("fetch");
 }
@@ -485,6 +591,17 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
     cudaStream_t st = ctx->stream;
     const int P = M->P;
     ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
+    if (!prm->want_vectors) {  // device-built work items, one host wait at the end
+        Tuning t;
+        if (ctx->item_override > 0) t.bis_item = std::min(ctx->item_override, ncpa::kWItem);
+        SolveBufs b;
+        prepare_solve(ctx, M, prm, t.bis_item, b, s.as<double>(), w.as<double>(), g.as<double>());
+        unsigned h_err = 0;
+        enqueue_solve(ctx, tm, M, prm, wkb, s.as<double>(), w.as<double>(), g.as<double>(), kz2.as<double>(), b, t,
+                      ctx->stats, ctx->h_tot, M->info.data(), &h_err);
+        finish_solve(ctx, tm, M, ctx->h_tot, &h_err);
+        return;
+    }
     // ---- K2 window ----
     check_launch(ctx, ncpa::launch_window(st, P, d_pinfo, wkb ? kz2.as<double>() : nullptr, wkb ? 1 : 0,
                                           prm->wvnum_filter, prm->c_min, prm->c_max, ctx->d_err.as<unsigned>()));
@@ -494,10 +611,6 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
     counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
     check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), counts.as<int>(), ctx->d_err.as<unsigned>()));
     tm.mark("scan");
-    if (!prm->want_vectors) {
-        solve_core_device_items(ctx, tm, M, prm, s, w, g, counts);
-        return;
-    }
     std::vector<int> hcounts((size_t)P * ncpa::kScanPoints);
     CK(cudaMemcpyAsync(hcounts.data(), counts.p, hcounts.size() * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(M->info.data(), d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
@@ -628,45 +741,16 @@ void init_modes(ncpa_modes* M, ncpa_ctx* ctx, const ncpa_ess_params* prm, int P)
     M->rho_rcv_p.assign(P, 1.0);
 }
 
-// One group of problems: one profile on one solver grid, n_freq x n_az
-// problems numbered frequency-major from p0.  Its rows start at s_base in
-// s, g and kz2 (nz_pad apart) and at w_base in w (one row per frequency).
-struct Group {
-    const ncpa_profile* prof;
-    Geometry geo;
-    int nz, nz_pad;
-    const double* freqs;
-    int n_freq;
-    const double* az;
-    int n_az;
-    int p0;
-    long long s_base, w_base;
-};
-
-Group make_group(const ncpa_profile* prof, const ncpa_ess_params* prm, int nz, const double* freqs, int n_freq,
-                 const double* az, int n_az) {
-    Group g{};
-    g.prof = prof;
-    g.geo = grid_geometry(prof, prm, nz);
-    g.nz = nz;
-    g.nz_pad = ((nz + ncpa::kChunk - 1) / ncpa::kChunk) * ncpa::kChunk;
-    g.freqs = freqs;
-    g.n_freq = n_freq;
-    g.az = az;
-    g.n_az = n_az;
-    return g;
-}
-
 bool wants_wkb(const ncpa_ess_params* prm);
 
 // Lays the groups out in one batch (problem records, row offsets), builds
 // every group's matrices and runs the window, scan, bisection and
 // eigenvector kernels once over all problems.
-void solve_groups(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::vector<Group>& groups) {
-    cudaStream_t st = ctx->stream;
-    PhaseTimer tm(ctx);
-    tm.mark("start");
-    long long s_tot = 0, w_tot = 0;
+// Numbers the groups' problems, fills their records (grid, row offsets) and
+// returns the doubles needed by s (and g, kz2) and by w.
+void layout_groups(ncpa_modes* M, std::vector<Group>& groups, long long& s_tot, long long& w_tot) {
+    s_tot = 0;
+    w_tot = 0;
     int p = 0;
     M->nz_max = 0;
     for (Group& g : groups) {
@@ -692,6 +776,14 @@ void solve_groups(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std:
         w_tot += (long long)g.n_freq * g.nz_pad;
         M->nz_max = std::max(M->nz_max, g.nz);
     }
+}
+
+void solve_groups(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::vector<Group>& groups) {
+    cudaStream_t st = ctx->stream;
+    PhaseTimer tm(ctx);
+    tm.mark("start");
+    long long s_tot = 0, w_tot = 0;
+    layout_groups(M, groups, s_tot, w_tot);
     upload(M->d_pinfo, M->info, st);
     const bool wkb = wants_wkb(prm);
     DevBuf s, w, gs, kz2;
@@ -701,12 +793,13 @@ void solve_groups(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std:
     if (prm->want_group_speed) gs.alloc((size_t)s_tot * 8, st);
     double* rho_pairs = pinned(ctx, 2 * groups.size());
     ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
+    std::vector<GroupBufs> gb(groups.size());
+    for (size_t gi = 0; gi < groups.size(); ++gi) prepare_group(ctx, prm, groups[gi], gb[gi]);
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         const Group& g = groups[gi];
-        build_problems(ctx, tm, g.prof, prm, g.geo, g.nz, g.nz_pad, g.freqs, g.n_freq, g.az, g.n_az, wkb,
-                       d_pinfo + g.p0, s.as<double>() + g.s_base, w.as<double>() + g.w_base,
-                       prm->want_group_speed ? gs.as<double>() + g.s_base : nullptr,
-                       wkb ? kz2.as<double>() + g.s_base : nullptr, rho_pairs + 2 * gi);
+        enqueue_group(ctx, tm, g, gb[gi], wkb, d_pinfo + g.p0, s.as<double>() + g.s_base, w.as<double>() + g.w_base,
+                      prm->want_group_speed ? gs.as<double>() + g.s_base : nullptr,
+                      wkb ? kz2.as<double>() + g.s_base : nullptr, rho_pairs + 2 * gi);
     }
     solve_core(ctx, tm, M, prm, wkb, s, w, gs, kz2);
     for (size_t gi = 0; gi < groups.size(); ++gi) {
@@ -722,6 +815,126 @@ void solve_groups(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std:
 bool wants_wkb(const ncpa_ess_params* prm) {
     return !prm->turnoff_wkb && std::fabs(prm->sourceheight_km * 1000.0) < 1.0e-3 &&
            std::fabs(prm->receiverheight_km * 1000.0) < 1.0e-3;
+}
+
+
+// Plan: buffers, pinned staging and the instantiated graph of one captured
+// batched solve.
+struct PlanData {
+    ncpa_ctx* ctx = nullptr;
+    std::unique_ptr<ncpa_modes> M;
+    ncpa_ess_params prm{};
+    std::vector<std::vector<double>> freqs, azs;  // host copies the groups point at
+    std::vector<Group> groups;
+    std::vector<GroupBufs> gb;
+    DevBuf s, w, gs, kz2, pinfo_init;
+    SolveBufs sb;
+    Tuning tuning;
+    bool wkb = false, with_tl = false, ran = false;
+    ncpa_tl_params tp{};
+    ProblemInfo* h_info = nullptr;  // pinned staging written by the graph
+    int* h_tot = nullptr;
+    unsigned* h_err = nullptr;
+    double* h_rho = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;  // kernel launches in one replay
+    int fit_e = 1;          // eigenvector CTAs per SM that fit
+    double tuned_ms = 0.0;
+};
+
+// The device sequence of a plan (captured into its graph).
+void enqueue_plan(PlanData& pl, const Tuning& t) {
+    ncpa_ctx* ctx = pl.ctx;
+    cudaStream_t st = ctx->stream;
+    ncpa_modes* M = pl.M.get();
+    PhaseTimer tm(ctx);  // records nothing: timing is off while capturing
+    ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
+    CK(cudaMemcpyAsync(d_pinfo, pl.pinfo_init.p, (size_t)M->P * sizeof(ProblemInfo), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(ctx->d_err.p, 0, sizeof(unsigned), st));
+    const bool grp = pl.prm.want_group_speed != 0;
+    for (size_t gi = 0; gi < pl.groups.size(); ++gi) {
+        const Group& g = pl.groups[gi];
+        enqueue_group(ctx, tm, g, pl.gb[gi], pl.wkb, d_pinfo + g.p0, pl.s.as<double>() + g.s_base,
+                      pl.w.as<double>() + g.w_base, grp ? pl.gs.as<double>() + g.s_base : nullptr,
+                      pl.wkb ? pl.kz2.as<double>() + g.s_base : nullptr, pl.h_rho + 2 * gi);
+    }
+    enqueue_solve(ctx, tm, M, &pl.prm, pl.wkb, pl.s.as<double>(), pl.w.as<double>(), grp ? pl.gs.as<double>() : nullptr,
+                  pl.kz2.as<double>(), pl.sb, t, false, pl.h_tot, pl.h_info, pl.h_err);
+    if (pl.with_tl)
+        check_launch(ctx, ncpa::launch_tl1d(st, M->P, d_pinfo, M->d_kr.as<double>(), M->d_ki.as<double>(),
+                                            M->d_vs.as<double>(), M->d_vr.as<double>(), pl.tp.n_ranges, pl.tp.dr_m,
+                                            pl.tp.lossless, M->tl_re.as<double>(), M->tl_im.as<double>(),
+                                            M->tl_inc.as<double>()));
+}
+
+// Captures the plan's sequence with launch shapes t and instantiates it.
+cudaGraphExec_t capture_plan(PlanData& pl, const Tuning& t) {
+    ncpa_ctx* ctx = pl.ctx;
+    cudaStream_t st = ctx->stream;
+    const bool timing = ctx->timing, stats = ctx->stats;
+    const long long l0 = ctx->launches;
+    ctx->timing = ctx->stats = false;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+        enqueue_plan(pl, t);
+    } catch (...) {
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        ctx->timing = timing;
+        ctx->stats = stats;
+        ctx->launches = l0;
+        throw;
+    }
+    ctx->timing = timing;
+    ctx->stats = stats;
+    pl.kernels = ctx->launches - l0;  // counted per replay instead
+    ctx->launches = l0;
+    CK(cudaStreamEndCapture(st, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return exec;
+}
+
+// After a replay: one wait, then the records, totals and errors.
+void finish_plan(PlanData& pl) {
+    ncpa_ctx* ctx = pl.ctx;
+    ncpa_modes* M = pl.M.get();
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(M->info.data(), pl.h_info, (size_t)M->P * sizeof(ProblemInfo));
+    PhaseTimer tm(ctx);
+    finish_solve(ctx, tm, M, pl.h_tot, pl.h_err);
+    for (size_t gi = 0; gi < pl.groups.size(); ++gi) {
+        const Group& g = pl.groups[gi];
+        for (int k = 0; k < g.n_freq * g.n_az; ++k) {
+            M->rho_src_p[g.p0 + k] = pl.h_rho[2 * gi];
+            M->rho_rcv_p[g.p0 + k] = pl.h_rho[2 * gi + 1];
+        }
+    }
+    pl.ran = true;
+}
+
+// Replays exec reps times (after one untimed replay) and returns ms per replay.
+double time_graph(PlanData& pl, cudaGraphExec_t exec, int reps) {
+    cudaStream_t st = pl.ctx->stream;
+    CK(cudaGraphLaunch(exec, st));
+    pl.ctx->launches += pl.kernels;
+    finish_plan(pl);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, st));
+    for (int r = 0; r < reps; ++r) CK(cudaGraphLaunch(exec, st));
+    pl.ctx->launches += pl.kernels * reps;
+    CK(cudaEventRecord(e1, st));
+    finish_plan(pl);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return (double)ms / reps;
 }
 
 }  // namespace
@@ -887,6 +1100,31 @@ ncpa_status ncpa_ctx_synchronize(ncpa_ctx* ctx) {
 // ---------------------------------------------------------------------------
 // profiles
 // ---------------------------------------------------------------------------
+namespace {
+// Copies the knot columns into the profile's allocated arrays and derives
+// the pressure / density splines, c0 and wind speed / direction on the
+// device.  No synchronisation: pageable uploads are staged before the copy
+// calls return, and everything later is ordered on the stream.
+void fill_profile(ncpa_ctx* ctx, ncpa_profile* P, const ncpa_profile_desc* d) {
+    cudaStream_t st = ctx->stream;
+    const int n = P->n;
+    const std::pair<DevBuf*, const double*> cols[] = {{&P->z, d->z}, {&P->u, d->u}, {&P->v, d->v},
+                                                      {&P->t, d->t}, {&P->p, d->p}, {&P->rho, d->rho}};
+    for (const auto& c : cols) CK(cudaMemcpyAsync(c.first->p, c.second, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (d->c0) CK(cudaMemcpyAsync(P->c0.p, d->c0, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (d->attn) CK(cudaMemcpyAsync(P->attn.p, d->attn, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    check_launch(ctx, ncpa::launch_steffen(st, n, P->z.as<double>(), P->p.as<double>(), 1, n, P->pcoef.as<double>(),
+                                           4 * (n - 1)));
+    check_launch(ctx, ncpa::launch_steffen(st, n, P->z.as<double>(), P->rho.as<double>(), 1, n,
+                                           P->rcoef.as<double>(), 4 * (n - 1)));
+    check_launch(ctx, ncpa::launch_profile_derived(st, n, P->z.as<double>(), P->u.as<double>(), P->v.as<double>(),
+                                                   P->p.as<double>(), P->rho.as<double>(), P->pcoef.as<double>(),
+                                                   P->rcoef.as<double>(), d->c0 ? 1 : 0, P->c0.as<double>(),
+                                                   P->ws.as<double>(), P->wd.as<double>()));
+}
+}  // namespace
+
+
 ncpa_status ncpa_profile_create(ncpa_ctx* ctx, const ncpa_profile_desc* d, ncpa_profile** out) {
     if (!ctx || !d || !out) return NCPA_EINVAL;
     *out = nullptr;
@@ -902,31 +1140,15 @@ ncpa_status ncpa_profile_create(ncpa_ctx* ctx, const ncpa_profile_desc* d, ncpa_
         P->ctx = ctx;
         P->n = n;
         cudaStream_t st = ctx->stream;
-        upload(P->z, d->z, n, st);
-        upload(P->u, d->u, n, st);
-        upload(P->v, d->v, n, st);
-        upload(P->t, d->t, n, st);
-        upload(P->p, d->p, n, st);
-        upload(P->rho, d->rho, n, st);
-        P->c0.alloc(n * sizeof(double), st);
-        if (d->c0) CK(cudaMemcpyAsync(P->c0.p, d->c0, n * sizeof(double), cudaMemcpyHostToDevice, st));
-        P->ws.alloc(n * sizeof(double), st);
-        P->wd.alloc(n * sizeof(double), st);
+        for (DevBuf* b : {&P->z, &P->u, &P->v, &P->t, &P->p, &P->rho, &P->c0, &P->ws, &P->wd})
+            b->alloc(n * sizeof(double), st);
         P->pcoef.alloc(4 * (n - 1) * sizeof(double), st);
         P->rcoef.alloc(4 * (n - 1) * sizeof(double), st);
-        check_launch(ctx, ncpa::launch_steffen(st, n, P->z.as<double>(), P->p.as<double>(), 1, n,
-                                               P->pcoef.as<double>(), 4 * (n - 1)));
-        check_launch(ctx, ncpa::launch_steffen(st, n, P->z.as<double>(), P->rho.as<double>(), 1, n,
-                                               P->rcoef.as<double>(), 4 * (n - 1)));
-        check_launch(ctx, ncpa::launch_profile_derived(st, n, P->z.as<double>(), P->u.as<double>(),
-                                                       P->v.as<double>(), P->p.as<double>(), P->rho.as<double>(),
-                                                       P->pcoef.as<double>(), P->rcoef.as<double>(),
-                                                       d->c0 ? 1 : 0, P->c0.as<double>(), P->ws.as<double>(),
-                                                       P->wd.as<double>()));
         if (d->attn) {
-            upload(P->attn, d->attn, n, st);
+            P->attn.alloc(n * sizeof(double), st);
             P->has_attn = true;
         }
+        fill_profile(ctx, P.get(), d);
         P->z0 = d->z0_m;
         P->has_z0 = d->has_z0;
         P->z_lo = d->z[0];
@@ -965,6 +1187,7 @@ ncpa_status ncpa_profile_load(ncpa_ctx* ctx, const char* path, const char* heade
 
 ncpa_status ncpa_profile_set_attn(ncpa_profile* prof, const double* z_km, const double* attn, int n) {
     if (!prof || !z_km || !attn || n < 2) return NCPA_EINVAL;
+    if (prof->plan_refs > 0) return fail(prof->ctx, NCPA_EINVAL, "profile is used by a plan");
     ncpa_ctx* ctx = prof->ctx;
     return guarded(ctx, [&]() -> ncpa_status {
         for (int i = 1; i < n; ++i)
@@ -1049,6 +1272,7 @@ ncpa_status ncpa_profile_z0(const ncpa_profile* prof, double* z0_m, int* has_z0)
 
 ncpa_status ncpa_profile_destroy(ncpa_profile* prof) {
     if (!prof) return NCPA_EINVAL;
+    if (prof->plan_refs > 0) return fail(prof->ctx, NCPA_EINVAL, "profile is used by a plan; destroy the plan first");
     cudaSetDevice(prof->ctx->device);
     cudaStreamSynchronize(prof->ctx->stream);
     delete prof;
@@ -1137,6 +1361,7 @@ ncpa_status ncpa_ess_solve_jobs(ncpa_ctx* ctx, const ncpa_ess_job* jobs, int n_j
 
 ncpa_status ncpa_modes_destroy(ncpa_modes* m) {
     if (!m) return NCPA_EINVAL;
+    if (m->plan_owned) return fail(m->ctx, NCPA_EINVAL, "these modes belong to a plan; destroy the plan");
     cudaSetDevice(m->ctx->device);
     cudaStreamSynchronize(m->ctx->stream);
     delete m;
@@ -1232,14 +1457,16 @@ ncpa_status ncpa_tl_1d(ncpa_ctx* ctx, const ncpa_modes* m, const ncpa_tl_params*
     if (!ctx || !m || !tp) return NCPA_EINVAL;
     const bool keep = !re && !im && !incoh;
     if (!keep && (!re || !im || !incoh)) return NCPA_EINVAL;
+    if (keep && m->plan_owned) return fail(ctx, NCPA_EINVAL, "TL of a plan's modes needs host buffers");
     return guarded(ctx, [&]() -> ncpa_status {
         if (tp->n_ranges < 1 || !(tp->dr_m > 0)) throw ApiError(NCPA_EINVAL, "bad range grid");
         CK(cudaSetDevice(ctx->device));
         cudaStream_t st = ctx->stream;
         const size_t n = (size_t)m->P * tp->n_ranges;
-        DevBuf& dre = m->tl_re;
-        DevBuf& dim = m->tl_im;
-        DevBuf& dinc = m->tl_inc;
+        DevBuf tre, tim, tinc;  // a plan's TL buffers are written by its graph: never reallocated here
+        DevBuf& dre = m->plan_owned ? tre : m->tl_re;
+        DevBuf& dim = m->plan_owned ? tim : m->tl_im;
+        DevBuf& dinc = m->plan_owned ? tinc : m->tl_inc;
         dre.alloc(n * 8, st);
         dim.alloc(n * 8, st);
         dinc.alloc(n * 8, st);
@@ -1586,6 +1813,240 @@ ncpa_status ncpa_source_spectrum_waveform(ncpa_ctx* ctx, const double* x, int n,
         }
         return NCPA_OK;
     });
+}
+
+// ---------------------------------------------------------------------------
+// captured solves (plans)
+// ---------------------------------------------------------------------------
+ncpa_status ncpa_profile_update(ncpa_profile* prof, const ncpa_profile_desc* d) {
+    if (!prof || !d) return NCPA_EINVAL;
+    ncpa_ctx* ctx = prof->ctx;
+    return guarded(ctx, [&]() -> ncpa_status {
+        if (d->n_knots != prof->n) throw ApiError(NCPA_EINVAL, "profile update needs the same number of knots");
+        if (!d->z || !d->u || !d->v || !d->t || !d->p || !d->rho)
+            throw ApiError(NCPA_EINVAL, "profile arrays z, u, v, t, p, rho are required");
+        if (d->z[0] != prof->z_lo || d->z[prof->n - 1] != prof->z_hi)
+            throw ApiError(NCPA_EINVAL, "profile update needs the same altitude range");
+        for (int i = 1; i < prof->n; ++i)
+            if (!(d->z[i] > d->z[i - 1])) throw ApiError(NCPA_EINVAL, "profile altitudes must increase strictly");
+        if (d->has_z0 != prof->has_z0 || (d->has_z0 && d->z0_m != prof->z0))
+            throw ApiError(NCPA_EINVAL, "profile update needs the same ground height");
+        if ((d->attn != nullptr) != prof->has_attn)
+            throw ApiError(NCPA_EINVAL, "profile update needs an attenuation column exactly when the profile has one");
+        CK(cudaSetDevice(ctx->device));
+        fill_profile(ctx, prof, d);
+        return NCPA_OK;
+    });
+}
+
+}  // extern "C"
+
+struct ncpa_plan {
+    PlanData d;
+    ~ncpa_plan() {
+        if (d.ctx) {
+            cudaSetDevice(d.ctx->device);
+            cudaStreamSynchronize(d.ctx->stream);
+        }
+        if (d.exec) cudaGraphExecDestroy(d.exec);
+        for (const Group& g : d.groups) const_cast<ncpa_profile*>(g.prof)->plan_refs--;
+        if (d.h_info) cudaFreeHost(d.h_info);
+        if (d.h_tot) cudaFreeHost(d.h_tot);
+        if (d.h_err) cudaFreeHost(d.h_err);
+        if (d.h_rho) cudaFreeHost(d.h_rho);
+    }
+};
+
+extern "C" {
+
+ncpa_status ncpa_ess_plan_create(ncpa_ctx* ctx, const ncpa_ess_job* jobs, int n_jobs, const ncpa_ess_params* prm,
+                                 const ncpa_tl_params* tl, int tune, ncpa_plan** out) {
+    if (!ctx || !jobs || n_jobs < 1 || !prm || !out) return NCPA_EINVAL;
+    *out = nullptr;
+    return guarded(ctx, [&]() -> ncpa_status {
+        check_ess_params(prm);
+        if (prm->want_vectors) throw ApiError(NCPA_EINVAL, "plans do not keep eigenvectors (want_vectors = 0)");
+        if (prm->lamb_wave_bc) throw ApiError(NCPA_EINVAL, "plans do not take the Lamb-wave condition");
+        if (tl && (tl->n_ranges < 1 || !(tl->dr_m > 0))) throw ApiError(NCPA_EINVAL, "bad range grid");
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        auto plan = std::make_unique<ncpa_plan>();
+        PlanData& pl = plan->d;
+        pl.prm = *prm;
+        if (pl.prm.max_modes <= 0) pl.prm.max_modes = 4000;
+        pl.freqs.reserve(n_jobs);
+        pl.azs.reserve(n_jobs);
+        int P = 0;
+        for (int j = 0; j < n_jobs; ++j) {
+            const ncpa_ess_job& jb = jobs[j];
+            if (!jb.profile || !jb.freqs || jb.n_freq < 1) throw ApiError(NCPA_EINVAL, "job without profile or frequencies");
+            for (int i = 0; i < jb.n_freq; ++i)
+                if (!(jb.freqs[i] > 0.0)) throw ApiError(NCPA_EINVAL, "frequencies must be positive");
+            if (jb.profile->ctx != ctx) throw ApiError(NCPA_EINVAL, "profile belongs to another context");
+            if (jb.n_az < 0 || (jb.n_az > 0 && !jb.az_list)) throw ApiError(NCPA_EINVAL, "job azimuth list missing");
+            if (jb.nz_grid != 0 && jb.nz_grid < 10) throw ApiError(NCPA_EINVAL, "Nz_grid must be >= 10");
+            pl.freqs.emplace_back(jb.freqs, jb.freqs + jb.n_freq);
+            if (jb.n_az > 0) pl.azs.emplace_back(jb.az_list, jb.az_list + jb.n_az);
+            else pl.azs.emplace_back(1, jb.az_deg);
+            const int n_az = (int)pl.azs.back().size();
+            pl.groups.push_back(make_group(jb.profile, prm, jb.nz_grid > 0 ? jb.nz_grid : prm->nz_grid,
+                                           pl.freqs.back().data(), jb.n_freq, pl.azs.back().data(), n_az));
+            const_cast<ncpa_profile*>(jb.profile)->plan_refs++;  // released by ~ncpa_plan
+            P += jb.n_freq * n_az;
+        }
+        pl.ctx = ctx;
+        pl.M = std::make_unique<ncpa_modes>();
+        ncpa_modes* M = pl.M.get();
+        init_modes(M, ctx, &pl.prm, P);
+        M->nf = P;
+        M->na = 1;
+        M->multi_job = true;
+        M->plan_owned = true;
+        for (const Group& g : pl.groups)
+            for (int f = 0; f < g.n_freq; ++f)
+                for (int a = 0; a < g.n_az; ++a) M->freqs.push_back(g.freqs[f]);
+        M->az.assign(1, pl.groups[0].az[0]);
+        long long s_tot = 0, w_tot = 0;
+        layout_groups(M, pl.groups, s_tot, w_tot);
+        upload(pl.pinfo_init, M->info, st);
+        M->d_pinfo.alloc((size_t)P * sizeof(ProblemInfo), st);
+        pl.wkb = wants_wkb(prm);
+        pl.s.alloc((size_t)s_tot * 8, st);
+        pl.w.alloc((size_t)w_tot * 8, st);
+        if (pl.wkb) pl.kz2.alloc((size_t)s_tot * 8, st);
+        if (prm->want_group_speed) pl.gs.alloc((size_t)s_tot * 8, st);
+        CK(cudaHostAlloc((void**)&pl.h_info, (size_t)P * sizeof(ProblemInfo), cudaHostAllocDefault));
+        CK(cudaHostAlloc((void**)&pl.h_tot, 4 * sizeof(int), cudaHostAllocDefault));
+        CK(cudaHostAlloc((void**)&pl.h_err, sizeof(unsigned), cudaHostAllocDefault));
+        CK(cudaHostAlloc((void**)&pl.h_rho, 2 * pl.groups.size() * sizeof(double), cudaHostAllocDefault));
+        pl.gb.resize(pl.groups.size());
+        for (size_t gi = 0; gi < pl.groups.size(); ++gi) prepare_group(ctx, prm, pl.groups[gi], pl.gb[gi]);
+        const int kMinItem = 16;  // smallest bisection item the tuner tries
+        double* gsp = prm->want_group_speed ? pl.gs.as<double>() : nullptr;
+        pl.sb.own_ck = true;
+        prepare_solve(ctx, M, &pl.prm, tune ? kMinItem : ncpa::kWItem, pl.sb, pl.s.as<double>(), pl.w.as<double>(),
+                      gsp);
+        if (tl) {
+            pl.with_tl = true;
+            pl.tp = *tl;
+            const size_t n = (size_t)P * tl->n_ranges * 8;
+            M->tl_re.alloc(n, st);
+            M->tl_im.alloc(n, st);
+            M->tl_inc.alloc(n, st);
+        }
+        ncpa::bisect_ctas_per_sm();  // sets the kernels' shared-memory attributes before any capture
+        const int fit_e = ncpa::eigvec_ctas_per_sm(eigvec_args(ctx, M, &pl.prm, pl.s.as<double>(), pl.w.as<double>(),
+                                                               gsp, pl.sb));
+        pl.fit_e = fit_e;
+        CK(cudaStreamSynchronize(st));
+        char key[160];
+        std::snprintf(key, sizeof key, "P%d s%lld w%lld nz%d m%d g%d t%d", P, s_tot, w_tot, M->nz_max,
+                      pl.prm.max_modes, prm->want_group_speed ? 1 : 0, tl ? tl->n_ranges : 0);
+        if (tune) {
+            auto hit = ctx->tune_cache.find(key);
+            if (hit != ctx->tune_cache.end()) {
+                pl.tuning.bis_item = hit->second[0];
+                pl.tuning.bis_ctas = hit->second[1];
+                pl.tuning.ev_ctas = hit->second[2];
+            } else {
+                // coordinate search: item size, then bisection CTAs per SM, then
+                // eigenvector CTAs per SM, each timed on its captured graph
+                Tuning best;
+                double best_ms = 1e300;
+                auto consider = [&](const Tuning& t) {
+                    cudaGraphExec_t e = capture_plan(pl, t);
+                    double ms;
+                    try {
+                        ms = time_graph(pl, e, 2);
+                    } catch (...) {
+                        cudaGraphExecDestroy(e);
+                        throw;
+                    }
+                    cudaGraphExecDestroy(e);
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = t;
+                    }
+                };
+                consider(Tuning{});
+                for (int item : {24, kMinItem}) {
+                    Tuning t = best;
+                    t.bis_item = item;
+                    consider(t);
+                }
+                const Tuning after_item = best;
+                for (int c = 1; c < ncpa::bisect_ctas_per_sm(); ++c) {
+                    Tuning t = after_item;
+                    t.bis_ctas = c;
+                    consider(t);
+                }
+                const Tuning after_bis = best;
+                for (int c = 1; c < fit_e; ++c) {
+                    Tuning t = after_bis;
+                    t.ev_ctas = c;
+                    consider(t);
+                }
+                pl.tuning = best;
+                ctx->tune_cache[key] = {best.bis_item, best.bis_ctas, best.ev_ctas};
+            }
+        }
+        pl.exec = capture_plan(pl, pl.tuning);
+        if (tune) pl.tuned_ms = time_graph(pl, pl.exec, 3);
+        *out = plan.release();
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_ess_plan_run(ncpa_plan* plan) {
+    if (!plan) return NCPA_EINVAL;
+    PlanData& pl = plan->d;
+    return guarded(pl.ctx, [&]() -> ncpa_status {
+        CK(cudaSetDevice(pl.ctx->device));
+        CK(cudaGraphLaunch(pl.exec, pl.ctx->stream));
+        pl.ctx->launches += pl.kernels;
+        finish_plan(pl);
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_ess_plan_modes(ncpa_plan* plan, ncpa_modes** modes) {
+    if (!plan || !modes) return NCPA_EINVAL;
+    if (!plan->d.ran) return fail(plan->d.ctx, NCPA_EINVAL, "the plan has not run");
+    *modes = plan->d.M.get();
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_ess_plan_tl(ncpa_plan* plan, double* re, double* im, double* incoh) {
+    if (!plan || !re || !im || !incoh) return NCPA_EINVAL;
+    PlanData& pl = plan->d;
+    if (!pl.with_tl) return fail(pl.ctx, NCPA_EINVAL, "the plan has no TL range grid");
+    if (!pl.ran) return fail(pl.ctx, NCPA_EINVAL, "the plan has not run");
+    return guarded(pl.ctx, [&]() -> ncpa_status {
+        cudaStream_t st = pl.ctx->stream;
+        const size_t n = (size_t)pl.M->P * pl.tp.n_ranges * 8;
+        CK(cudaMemcpyAsync(re, pl.M->tl_re.p, n, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(im, pl.M->tl_im.p, n, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(incoh, pl.M->tl_inc.p, n, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_ess_plan_tuning(const ncpa_plan* plan, int* bis_item, int* bis_ctas_per_sm, int* ev_ctas_per_sm,
+                                 double* ms) {
+    if (!plan) return NCPA_EINVAL;
+    const PlanData& pl = plan->d;
+    if (bis_item) *bis_item = pl.tuning.bis_item;
+    if (bis_ctas_per_sm) *bis_ctas_per_sm = pl.tuning.bis_ctas > 0 ? pl.tuning.bis_ctas : ncpa::bisect_ctas_per_sm();
+    if (ev_ctas_per_sm) *ev_ctas_per_sm = pl.tuning.ev_ctas > 0 ? pl.tuning.ev_ctas : pl.fit_e;
+    if (ms) *ms = pl.tuned_ms;
+    return NCPA_OK;
+}
+
+ncpa_status ncpa_ess_plan_destroy(ncpa_plan* plan) {
+    if (!plan) return NCPA_EINVAL;
+    delete plan;
+    return NCPA_OK;
 }
 
 }  // extern "C"

@@ -31,6 +31,8 @@ EXPORTED = [
     "ncpa_eigvec_static", "ncpa_profile_set_attn", "ncpa_profile_load_attn", "ncpa_profile_knots", "ncpa_profile_z0",
     "ncpa_modal_starter", "ncpa_source_waveform", "ncpa_tl_multi", "ncpa_ess_solve_jobs", "ncpa_server_opts_default", "ncpa_server_create",
     "ncpa_server_submit", "ncpa_server_wait", "ncpa_server_release", "ncpa_server_stats_get", "ncpa_server_destroy", "ncpa_modes_get_all",
+    "ncpa_ess_plan_create", "ncpa_ess_plan_run", "ncpa_ess_plan_modes", "ncpa_ess_plan_tl", "ncpa_ess_plan_tuning",
+    "ncpa_ess_plan_destroy", "ncpa_profile_update",
 ]
 
 
@@ -101,6 +103,14 @@ def lib():
         L.ncpa_profile_load_attn.argtypes = [_vp, ctypes.c_char_p]
         L.ncpa_ess_solve_jobs.argtypes = [_vp, ctypes.POINTER(_EssJob), _c_int, ctypes.POINTER(EssParams),
                                           ctypes.POINTER(_vp)]
+        L.ncpa_ess_plan_create.argtypes = [_vp, ctypes.POINTER(_EssJob), _c_int, ctypes.POINTER(EssParams),
+                                           ctypes.POINTER(_TlParams), _c_int, ctypes.POINTER(_vp)]
+        L.ncpa_ess_plan_run.argtypes = [_vp]
+        L.ncpa_ess_plan_modes.argtypes = [_vp, ctypes.POINTER(_vp)]
+        L.ncpa_ess_plan_tl.argtypes = [_vp, _dp, _dp, _dp]
+        L.ncpa_ess_plan_tuning.argtypes = [_vp, _ip, _ip, _ip, ctypes.POINTER(_c_double)]
+        L.ncpa_ess_plan_destroy.argtypes = [_vp]
+        L.ncpa_profile_update.argtypes = [_vp, ctypes.POINTER(_ProfileDesc)]
         L.ncpa_ess_solve.argtypes = [_vp, _vp, ctypes.POINTER(EssParams), _dp, _c_int, _dp, _c_int,
                                      ctypes.POINTER(_vp)]
         L.ncpa_modes_destroy.argtypes = [_vp]
@@ -221,11 +231,7 @@ class Context:
         return Profile(self, h)
 
     def profile_from_arrays(self, z, u, v, t, p, rho, c0=None, attn=None, z0=None):
-        arrs = [_f64(x) for x in (z, u, v, t, p, rho)]
-        c0a = _f64(c0) if c0 is not None else None
-        aa = _f64(attn) if attn is not None else None
-        d = _ProfileDesc(len(arrs[0]), *[_p(a) for a in arrs], _p(c0a), _p(aa), float(z0 or 0.0),
-                         int(z0 is not None))
+        d, _keep = _profile_desc(z, u, v, t, p, rho, c0, attn, z0)
         h = _vp()
         self.check(lib().ncpa_profile_create(self.h, ctypes.byref(d), ctypes.byref(h)), "ncpa_profile_create")
         return Profile(self, h)
@@ -244,27 +250,23 @@ class Context:
         azimuth_deg is a number or a list of azimuths (the job sweeps them);
         nz_grid (optional, 0 = params.nz_grid) sets the job's own grid.
         Problems are numbered job by job, frequency-major then azimuth."""
-        keep, azs, fr, az_all = [], [], [], []
-        arr = (_EssJob * len(jobs))()
-        for i, job in enumerate(jobs):
-            prof, freqs, az = job[0], job[1], job[2]
-            nz = int(job[3]) if len(job) > 3 else 0
-            f = _f64(np.atleast_1d(freqs))
-            keep.append(f)
-            if np.ndim(az) == 0:
-                arr[i] = _EssJob(prof.h.value, _p(f), len(f), float(az), nz, 0, None)
-                fr.append(f)
-                az_all.append(np.full(len(f), float(az)))
-            else:
-                a = _f64(np.atleast_1d(az))
-                azs.append(a)
-                arr[i] = _EssJob(prof.h.value, _p(f), len(f), float(a[0]), nz, len(a), _p(a))
-                fr.append(np.repeat(f, len(a)))
-                az_all.append(np.tile(a, len(f)))
+        arr, keep, fr, az_all = _jobs_array(jobs)
         h = _vp()
         self.check(lib().ncpa_ess_solve_jobs(self.h, arr, len(jobs), ctypes.byref(params), ctypes.byref(h)),
                    "ncpa_ess_solve_jobs")
-        return Modes(self, h, np.concatenate(fr), np.concatenate(az_all))
+        return Modes(self, h, fr, az_all)
+
+    def plan(self, jobs, params: EssParams, tl=None, tune=False):
+        """A captured solve (CUDA graph) of the jobs of solve_jobs; tl =
+        (n_ranges, dr_m[, lossless]) adds the 1-D TL to the graph; tune times
+        launch shapes and keeps the fastest."""
+        arr, keep, fr, az_all = _jobs_array(jobs)
+        tp = _TlParams(int(tl[0]), float(tl[1]), int(tl[2]) if len(tl) > 2 else 0) if tl is not None else None
+        h = _vp()
+        self.check(lib().ncpa_ess_plan_create(self.h, arr, len(jobs), ctypes.byref(params),
+                                              ctypes.byref(tp) if tp is not None else None, int(bool(tune)),
+                                              ctypes.byref(h)), "ncpa_ess_plan_create")
+        return Plan(self, h, fr, az_all, tl)
 
     SOURCES = {"impulse": 0, "pulse1": 1, "pulse2": 2}
 
@@ -296,6 +298,35 @@ class Context:
         return out
 
 
+def _profile_desc(z, u, v, t, p, rho, c0=None, attn=None, z0=None):
+    arrs = [_f64(x) for x in (z, u, v, t, p, rho)]
+    c0a = _f64(c0) if c0 is not None else None
+    aa = _f64(attn) if attn is not None else None
+    d = _ProfileDesc(len(arrs[0]), *[_p(a) for a in arrs], _p(c0a), _p(aa), float(z0 or 0.0), int(z0 is not None))
+    return d, (arrs, c0a, aa)
+
+
+def _jobs_array(jobs):
+    keep, fr, az_all = [], [], []
+    arr = (_EssJob * len(jobs))()
+    for i, job in enumerate(jobs):
+        prof, freqs, az = job[0], job[1], job[2]
+        nz = int(job[3]) if len(job) > 3 else 0
+        f = _f64(np.atleast_1d(freqs))
+        keep.append(f)
+        if np.ndim(az) == 0:
+            arr[i] = _EssJob(prof.h.value, _p(f), len(f), float(az), nz, 0, None)
+            fr.append(f)
+            az_all.append(np.full(len(f), float(az)))
+        else:
+            a = _f64(np.atleast_1d(az))
+            keep.append(a)
+            arr[i] = _EssJob(prof.h.value, _p(f), len(f), float(a[0]), nz, len(a), _p(a))
+            fr.append(np.repeat(f, len(a)))
+            az_all.append(np.tile(a, len(f)))
+    return arr, keep, np.concatenate(fr), np.concatenate(az_all)
+
+
 class Profile:
     def __init__(self, ctx, h):
         self.ctx, self.h = ctx, h
@@ -309,6 +340,11 @@ class Profile:
     def load_attn(self, path):
         """User attenuation table (height km, Np/m), the --use_attn_file option."""
         self.ctx.check(lib().ncpa_profile_load_attn(self.h, str(path).encode()), "ncpa_profile_load_attn")
+
+    def update(self, z, u, v, t, p, rho, c0=None, attn=None, z0=None):
+        """New knot values in place (same knots, altitudes and ground height)."""
+        d, _keep = _profile_desc(z, u, v, t, p, rho, c0, attn, z0)
+        self.ctx.check(lib().ncpa_profile_update(self.h, ctypes.byref(d)), "ncpa_profile_update")
 
     def close(self):
         if self.h:
@@ -337,8 +373,8 @@ class ProblemModes:
 
 
 class Modes:
-    def __init__(self, ctx, h, freqs, azs):
-        self.ctx, self.h = ctx, h
+    def __init__(self, ctx, h, freqs, azs, owned=True):
+        self.ctx, self.h, self.owned = ctx, h, owned
         self.freqs, self.azs = freqs, azs
         n = _c_int()
         ctx.check(lib().ncpa_modes_problems(h, ctypes.byref(n)), "ncpa_modes_problems")
@@ -429,8 +465,49 @@ class Modes:
 
     def close(self):
         if self.h:
-            lib().ncpa_modes_destroy(self.h)
+            if self.owned:
+                lib().ncpa_modes_destroy(self.h)
             self.h = _vp()
+
+
+class Plan:
+    """A captured batched solve (see Context.plan)."""
+
+    def __init__(self, ctx, h, freqs, azs, tl):
+        self.ctx, self.h, self.freqs, self.azs, self.tl_grid = ctx, h, freqs, azs, tl
+        self.P = len(freqs)
+
+    def run(self):
+        self.ctx.check(lib().ncpa_ess_plan_run(self.h), "ncpa_ess_plan_run")
+
+    def modes(self) -> Modes:
+        """Result of the last run (valid until the next run; owned by the plan)."""
+        h = _vp()
+        self.ctx.check(lib().ncpa_ess_plan_modes(self.h, ctypes.byref(h)), "ncpa_ess_plan_modes")
+        return Modes(self.ctx, h, self.freqs, self.azs, owned=False)
+
+    def tl(self):
+        n = int(self.tl_grid[0])
+        re, im, inc = (np.empty((self.P, n)) for _ in range(3))
+        self.ctx.check(lib().ncpa_ess_plan_tl(self.h, _p(re), _p(im), _p(inc)), "ncpa_ess_plan_tl")
+        return re, im, inc
+
+    def tuning(self):
+        a, b, c, ms = _c_int(), _c_int(), _c_int(), _c_double()
+        self.ctx.check(lib().ncpa_ess_plan_tuning(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                                  ctypes.byref(ms)), "ncpa_ess_plan_tuning")
+        return {"bis_item": a.value, "bis_ctas_per_sm": b.value, "ev_ctas_per_sm": c.value, "ms": ms.value}
+
+    def close(self):
+        if self.h:
+            lib().ncpa_ess_plan_destroy(self.h)
+            self.h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 # ---------------------------------------------------------------------------
