@@ -51,6 +51,11 @@ for p in (ROOT, PKG):
 import workloads  # noqa: E402
 
 METRIC = "freq-solves/s"
+# DRAM bytes (read + write) per launch from one ncu capture of the same
+# workloads (profiles/ess_modbb256_dram_bytes.md, k_bisect;
+# profiles/k_ms_tc_modal_sum_64rcv_20000rng.md, k_ms_tc)
+TRAFFIC_BISECT = 42437888
+TRAFFIC_MS_TC = 2512600
 NZ = 20000
 NFREQ = 256
 RANGES_KM = np.arange(200.0, 300.0 + 1e-9, 10.0)
@@ -353,7 +358,8 @@ def run_ours(args):
                          "achieved": round(achieved, 3) if achieved else None, "peak": round(fp64_peak, 3),
                          "unit": "TFLOP/s", "frac": round(achieved / fp64_peak, 4) if achieved else None,
                          "peak_source": "measured in this run (dependent-FMA probe on all SMs)",
-                         "traffic": None, "avg_launch_ms": round(bis_ms / max(bis_n, 1), 4),
+                         "traffic": TRAFFIC_BISECT, "traffic_source": "ncu capture, profiles/ess_modbb256_dram_bytes.md",
+                         "avg_launch_ms": round(bis_ms / max(bis_n, 1), 4),
                          "flops_per_launch": flops / bis_n if bis_n else None},
             "phases_ms": {k: round(v, 4) for k, v in phases.items()},
             "plain_gpu": {"value": round(plain_rate, 2), "unit": METRIC,
@@ -434,7 +440,8 @@ def modal_sum_leg(ctx, stream, bf16_peak, k=10):
         "roofline": {"kernel": "k_ms_tc (tcgen05 split-BF16)", "bound": "tensor", "achieved": round(achieved, 1),
                      "peak": bf16_peak, "unit": "TFLOP/s", "frac": round(achieved / bf16_peak, 4),
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)",
-                     "flops_per_launch": tensor, "algorithmic_flops_per_launch": alg, "traffic": None},
+                     "flops_per_launch": tensor, "algorithmic_flops_per_launch": alg, "traffic": TRAFFIC_MS_TC,
+                     "traffic_source": "ncu capture, profiles/k_ms_tc_modal_sum_64rcv_20000rng.md"},
         "error_vs_fp64": {"max_abs_over_max_P": float(rel.max()), "tl_db_median": float(np.median(d)),
                           "tl_db_p99_9": float(np.percentile(d, 99.9)), "tl_db_max": float(d.max()),
                           "where": "TL > -140 dB, first 2000 ranges"},
@@ -704,9 +711,18 @@ def main():
     ap.add_argument("--no-sweep", action="store_true", help="skip the 360-azimuth mixed-grid sweep leg")
     ap.add_argument("--only-modal-sum", action="store_true",
                     help="run only the tensor-core modal-sum leg and print its JSON (for profiler runs)")
+    ap.add_argument("--only-serving", action="store_true",
+                    help="run only the served request-stream leg and print its JSON")
     ap.add_argument("--only-sweep", action="store_true",
                     help="run only the mixed-grid sweep leg and print its JSON (for profiler runs)")
     args = ap.parse_args()
+    if args.only_serving:
+        import ncpa_gpu
+
+        ctx = ncpa_gpu.Context(0)
+        print(json.dumps(serving_leg(ctx)), flush=True)
+        ctx.close()
+        return
     if args.only_sweep:
         import torch
         import ncpa_gpu
