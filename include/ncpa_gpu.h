@@ -185,9 +185,12 @@ ncpa_status ncpa_tl_2d(ncpa_ctx *ctx, const ncpa_modes *modes, int problem, cons
  *   NCPA_SUM_FP64        FP64 sum on the CUDA cores (at most 1024 receivers)
  *   NCPA_SUM_TC_BF16X3   tcgen05 tensor cores: 3-term split-BF16 products with
  *                        FP32 accumulation; phases k r reduced mod 2 pi in
- *                        FP64 per 128-range tile (relative error ~1e-5 of
- *                        the modal terms' magnitude) */
-enum { NCPA_SUM_FP64 = 0, NCPA_SUM_TC_BF16X3 = 1 };
+ *                        FP64 per 256-range tile (relative error ~1e-5 of
+ *                        the modal terms' magnitude)
+ *   NCPA_SUM_TC_TF32     tcgen05 tensor cores: TF32 products (operands
+ *                        rounded to nearest) with FP32 accumulation, same
+ *                        phase reduction (relative error ~1e-3) */
+enum { NCPA_SUM_FP64 = 0, NCPA_SUM_TC_BF16X3 = 1, NCPA_SUM_TC_TF32 = 2 };
 ncpa_status ncpa_tl_multi(ncpa_ctx *ctx, const ncpa_modes *modes, int problem, int n_rcv,
                           const double *rcv_height_m, const ncpa_tl_params *tp, int method, double *re,
                           double *im);

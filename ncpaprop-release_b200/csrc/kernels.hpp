@@ -157,11 +157,12 @@ struct MsPlan {
 };
 MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms);
 int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const double* vfull, double* vz);
-int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int n_rcv, int M, const double* kr, const double* ki,
-                      const double* vs, const int* idx, const double* vfull, double dr, int lossless, void* a_img,
-                      void* q, void* tab);
-int launch_ms_tc(cudaStream_t st, const MsPlan& p, int n_ranges, const void* a_img, const void* q, const void* tab,
-                 float* raw, unsigned* err);
+// fmt: 0 = 3-term split-BF16 (kind::f16), 1 = TF32 (kind::tf32)
+int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int M, const double* kr,
+                      const double* ki, const double* vs, const int* idx, const double* vfull, double dr, int lossless,
+                      void* a_img, void* q, void* tab);
+int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const void* a_img, const void* q,
+                 const void* tab, float* raw, unsigned* err);
 int launch_ms_finish(cudaStream_t st, const MsPlan& p, int n_rcv, int n_ranges, double dr, const float* raw,
                      double* re, double* im);
 

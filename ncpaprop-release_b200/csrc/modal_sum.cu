@@ -10,8 +10,15 @@
 //   D[128 x N] = A'[128 x 2M] * B'[2M x N],
 //   A' = [[Re A, -Im A], [Im A, Re A]] (rows 0..63 give Re P, 64..127 Im P),
 //   B' = [[Re E], [Im E]] interleaved per mode (k = 2m: Re, 2m + 1: Im).
-// Each operand is split into bf16 hi + lo parts and D accumulates
-//   A_hi B_hi + A_hi B_lo + A_lo B_hi   in FP32 (3-term split-BF16, ~2^-16).
+// Two operand formats (template parameter F of the kernels):
+//  * kMsBf16x3: each operand is split into bf16 hi + lo parts and D
+//    accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32 (3-term
+//    split-BF16, ~2^-16 relative per product; kind::f16, K = 16 per MMA);
+//  * kMsTf32: each operand rounded to TF32 (10-bit mantissa, round to
+//    nearest) and D accumulates A B in FP32 (one product, ~2^-11 relative;
+//    kind::tf32, K = 8 per MMA).
+// Both keep a chunk's A' in 16 KB and its B' in 32 KB of shared memory, so the
+// pipeline, barriers and epilogue are shared.
 //
 // Persistent kernel: the (receiver group, 128-range tile, 32-mode chunk)
 // units are split evenly over one CTA per SM; a CTA accumulates the chunks of
@@ -24,10 +31,11 @@
 // FP64-reduced tile phases e^{i k r_n0} (phase reduced mod 2 pi in FP64)
 // times per-mode FP32 factors e^{i k o dr}, and read the accumulators out.
 //
-// Shared-memory operand layout: K-major, 64-byte swizzle (sw64_off below):
-// each operand row holds the 32 k of a chunk (64 B), 8-row atoms of 512 B,
-// 16-byte chunks XOR-permuted by row so that the generators' 16-byte stores
-// and the tensor cores' reads are free of bank conflicts.
+// Shared-memory operand layout: K-major, each operand row holds the 32 k of a
+// chunk; bf16: 64 B rows, 64-byte swizzle, 8-row atoms of 512 B (sw64_off);
+// TF32: 128 B rows, 128-byte swizzle, 8-row atoms of 1 KB (sw128_off).  The
+// 16-byte chunks are XOR-permuted by row so that the generators' 16-byte
+// stores and the tensor cores' reads are free of bank conflicts.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -76,6 +84,16 @@ __host__ __device__ __forceinline__ uint32_t sw64_off(int row, int k) {
     return (uint32_t)((row >> 3) * 512 + r * 64 + ((((k >> 3) ^ (r >> 1)) & 3) << 4) + (k & 7) * 2);
 }
 
+// byte offset of element (row, k) in a K-major tile of kMsKC = 32 fp32 per
+// row with the 128-byte swizzle: rows of 128 B in atoms of 8 rows (1 KB); the
+// 16-byte chunk index k / 4 is XORed with row % 8
+__host__ __device__ __forceinline__ uint32_t sw128_off(int row, int k) {
+    const int r = row & 7;
+    return (uint32_t)((row >> 3) * 1024 + r * 128 + ((((k >> 2) ^ r) & 7) << 4) + (k & 3) * 4);
+}
+
+enum : int { kMsBf16x3 = 0, kMsTf32 = 1 };
+
 // shared-memory matrix descriptor (tcgen05 format): start >> 4 in [0,14),
 // leading-byte offset in [16,30) (unused by swizzled K-major layouts: 1),
 // stride-byte offset >> 4 in [32,46) (next 8-row atom: 512 B), descriptor
@@ -84,6 +102,11 @@ __host__ __device__ __forceinline__ uint32_t sw64_off(int row, int k) {
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     return (uint64_t)((addr & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46) |
            (4ull << 61);
+}
+// same for the 128-byte swizzle: stride-byte offset 1 KB, layout type 2
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
 }
 
 // instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and
@@ -98,6 +121,27 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint6
         " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(kMsIdesc), "r"(accumulate)
         : "memory");
+}
+
+// instruction descriptor, kind::tf32: FP32 accumulator, A and B TF32 (format
+// 2 in bits 7-9 and 10-12), both K-major, same N and M
+constexpr uint32_t kMsIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kMsNT >> 3) << 17) |
+                                  ((uint32_t)(kMsRows >> 4) << 24);
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kMsIdescTf32), "r"(accumulate)
+        : "memory");
+}
+
+// fp32 -> tf32, round to nearest (ties away), as the 32-bit pattern the
+// tensor cores read
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
 }
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -177,9 +221,10 @@ __device__ void ms_phase_entry(long long id, int M, int M_pad, int n_tiles, cons
 // A' chunk images (hi, lo) for every receiver group and K-chunk, in the
 // shared-memory layout above; mode values at receiver j are row idx[j] of the
 // full eigenvectors vfull [z][mode], vs the source values
+template <int F>
 __device__ void ms_a_entry(long long id, int n_rcv, int M, int n_chunks, const double* __restrict__ kr,
                            const double* __restrict__ ki, const double* __restrict__ vs, const int* __restrict__ idx,
-                           const double* __restrict__ vfull, int lossless, __nv_bfloat16* __restrict__ img) {
+                           const double* __restrict__ vfull, int lossless, unsigned char* __restrict__ img) {
     const int n_groups = (n_rcv + kMsRcv - 1) / kMsRcv;
     const long long per_chunk = (long long)kMsRows * kMsKC;
     if (id >= (long long)n_groups * n_chunks * per_chunk) return;
@@ -199,29 +244,35 @@ __device__ void ms_a_entry(long long id, int n_rcv, int M, int n_chunks, const d
         const bool im_row = row >= kMsRcv, im_col = (kl & 1) != 0;
         x = (float)(!im_row ? (im_col ? -aim : are) : (im_col ? are : aim));
     }
-    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-    const size_t base = (size_t)gc * 2 * (kMsABytes / 2);  // elements
-    const size_t off = sw64_off(row, kl) / 2;
-    img[base + off] = hi;
-    img[base + kMsABytes / 2 + off] = lo;
+    unsigned char* chunk_img = img + (size_t)gc * 2 * kMsABytes;  // 16 KB per (group, chunk)
+    if (F == kMsTf32) {
+        *reinterpret_cast<uint32_t*>(chunk_img + sw128_off(row, kl)) = to_tf32(x);
+    } else {
+        const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+        __nv_bfloat16* im = reinterpret_cast<__nv_bfloat16*>(chunk_img);
+        const size_t off = sw64_off(row, kl) / 2;
+        im[off] = hi;
+        im[kMsABytes / 2 + off] = lo;
+    }
 }
 
 // the three preparations in one launch: blocks [0, b_tab) fill the factor
 // rows, [b_tab, b_tab + b_q) the tile phases, the rest the A' images
+template <int F>
 __global__ void k_ms_prepare(long long b_tab, long long b_q, int n_rcv, int M, int M_pad, int n_tiles, int n_chunks,
                              const double* __restrict__ kr, const double* __restrict__ ki,
                              const double* __restrict__ vs, const int* __restrict__ idx,
                              const double* __restrict__ vfull, double dr, int lossless, float2* __restrict__ tab,
-                             float2* __restrict__ q, __nv_bfloat16* __restrict__ img) {
+                             float2* __restrict__ q, unsigned char* __restrict__ img) {
     const long long b = blockIdx.x;
     if (b < b_tab) {
         ms_table_entry((int)(b * blockDim.x + threadIdx.x), M, M_pad, kr, ki, dr, lossless, tab);
     } else if (b < b_tab + b_q) {
         ms_phase_entry((b - b_tab) * blockDim.x + threadIdx.x, M, M_pad, n_tiles, kr, ki, dr, lossless, q);
     } else {
-        ms_a_entry((b - b_tab - b_q) * blockDim.x + threadIdx.x, n_rcv, M, n_chunks, kr, ki, vs, idx, vfull,
-                   lossless, img);
+        ms_a_entry<F>((b - b_tab - b_q) * blockDim.x + threadIdx.x, n_rcv, M, n_chunks, kr, ki, vs, idx, vfull,
+                      lossless, img);
     }
 }
 
@@ -264,6 +315,7 @@ struct UnitPos {
     }
 };
 
+template <int F>
 __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     extern __shared__ unsigned char ms_dyn[];
     __shared__ __align__(8) uint64_t full_a[kMsStages], full_b[kMsStages], empty[kMsStages];
@@ -336,7 +388,7 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             pos.init(u0, a.n_chunks, a.n_tiles);
             bool ok = true;
             int sg = -1;  // segment (one group and tile) counter
-            const uint64_t dsc0 = smem_desc(sm_addr);
+            const uint64_t dsc0 = F == kMsTf32 ? smem_desc_sw128(sm_addr) : smem_desc(sm_addr);
             for (int c = 0; c < nc && ok; ++c, pos.next(a.n_chunks, a.n_tiles)) {
                 const bool first = c == 0 || pos.chunk == 0;
                 const bool last = c == nc - 1 || pos.chunk == a.n_chunks - 1;
@@ -356,13 +408,24 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                 // descriptors: the start-address field counts 16-byte units
                 const uint64_t st = dsc0 + (uint64_t)((s * kMsStageBytes) >> 4);
                 const uint32_t d = tmem + (uint32_t)((sg & 1) * kMsNT);
+                if (F == kMsTf32) {
+                    // K = 8 tf32 (32 B) per MMA, four per chunk
 #pragma unroll
-                for (int kk = 0; kk < kMsKC / 16; ++kk) {
-                    const uint64_t ah = st + (uint64_t)(kk * 32 >> 4), al = ah + (uint64_t)(kMsABytes >> 4);
-                    const uint64_t bh = st + (uint64_t)((kMsOffB + kk * 32) >> 4), bl = bh + (uint64_t)(kMsBBytes >> 4);
-                    umma_bf16(d, ah, bh, (!first || kk > 0) ? 1u : 0u);
-                    umma_bf16(d, ah, bl, 1u);
-                    umma_bf16(d, al, bh, 1u);
+                    for (int kk = 0; kk < kMsKC / 8; ++kk) {
+                        const uint64_t ad = st + (uint64_t)(kk * 32 >> 4);
+                        const uint64_t bd = st + (uint64_t)((kMsOffB + kk * 32) >> 4);
+                        umma_tf32(d, ad, bd, (!first || kk > 0) ? 1u : 0u);
+                    }
+                } else {
+#pragma unroll
+                    for (int kk = 0; kk < kMsKC / 16; ++kk) {
+                        const uint64_t ah = st + (uint64_t)(kk * 32 >> 4), al = ah + (uint64_t)(kMsABytes >> 4);
+                        const uint64_t bh = st + (uint64_t)((kMsOffB + kk * 32) >> 4),
+                                       bl = bh + (uint64_t)(kMsBBytes >> 4);
+                        umma_bf16(d, ah, bh, (!first || kk > 0) ? 1u : 0u);
+                        umma_bf16(d, ah, bl, 1u);
+                        umma_bf16(d, al, bh, 1u);
+                    }
                 }
                 umma_commit(&empty[s]);
                 if (last) umma_commit(&acc_full[sg & 1]);
@@ -413,12 +476,20 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
 #pragma unroll
             for (int st8 = 0; st8 < 4; ++st8) {
                 const int grp = part * 4 + st8;  // 8-range group within the tile
-                const uint32_t off = sw64_off(grp * 8 + i, 8 * q);
-                uint32_t h[4], l[4];
+                if (F == kMsTf32) {
+                    // modes 4q, 4q+1 -> k = 8q .. 8q+3; modes 4q+2, 4q+3 -> k = 8q+4 .. 8q+7
+                    sts128(bh + sw128_off(grp * 8 + i, 8 * q), to_tf32(e[0].x), to_tf32(e[0].y), to_tf32(e[1].x),
+                           to_tf32(e[1].y));
+                    sts128(bh + sw128_off(grp * 8 + i, 8 * q + 4), to_tf32(e[2].x), to_tf32(e[2].y), to_tf32(e[3].x),
+                           to_tf32(e[3].y));
+                } else {
+                    const uint32_t off = sw64_off(grp * 8 + i, 8 * q);
+                    uint32_t h[4], l[4];
 #pragma unroll
-                for (int v = 0; v < 4; ++v) split2(e[v], h[v], l[v]);
-                sts128(bh + off, h[0], h[1], h[2], h[3]);
-                sts128(bh + kMsBBytes + off, l[0], l[1], l[2], l[3]);
+                    for (int v = 0; v < 4; ++v) split2(e[v], h[v], l[v]);
+                    sts128(bh + off, h[0], h[1], h[2], h[3]);
+                    sts128(bh + kMsBBytes + off, l[0], l[1], l[2], l[3]);
+                }
                 if (st8 < 3) {
 #pragma unroll
                     for (int v = 0; v < 4; ++v) e[v] = cmulf(e[v], w[v]);
@@ -560,29 +631,33 @@ int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const do
     return 1;
 }
 
-int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int n_rcv, int M, const double* kr, const double* ki,
-                      const double* vs, const int* idx, const double* vfull, double dr, int lossless, void* a_img,
-                      void* q, void* tab) {
+int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int M, const double* kr,
+                      const double* ki, const double* vs, const int* idx, const double* vfull, double dr, int lossless,
+                      void* a_img, void* q, void* tab) {
+    if (fmt != kMsBf16x3 && fmt != kMsTf32) return -1;
     const long long n_tab = (long long)p.M_pad * kMsTabW;
     const long long n_q = (long long)p.n_tiles * p.M_pad;
     const long long n_a = (long long)p.groups * p.n_chunks * kMsRows * kMsKC;
     const long long b_tab = (n_tab + 255) / 256, b_q = (n_q + 255) / 256, b_a = (n_a + 255) / 256;
-    k_ms_prepare<<<(unsigned)(b_tab + b_q + b_a), 256, 0, st>>>(
-        b_tab, b_q, n_rcv, M, p.M_pad, p.n_tiles, p.n_chunks, kr, ki, vs, idx, vfull, dr, lossless,
-        (float2*)tab, (float2*)q, (__nv_bfloat16*)a_img);
+    auto kern = fmt == kMsTf32 ? k_ms_prepare<kMsTf32> : k_ms_prepare<kMsBf16x3>;
+    kern<<<(unsigned)(b_tab + b_q + b_a), 256, 0, st>>>(b_tab, b_q, n_rcv, M, p.M_pad, p.n_tiles, p.n_chunks, kr, ki,
+                                                       vs, idx, vfull, dr, lossless, (float2*)tab, (float2*)q,
+                                                       (unsigned char*)a_img);
     return 1;
 }
 
-int launch_ms_tc(cudaStream_t st, const MsPlan& p, int n_ranges, const void* a_img, const void* q, const void* tab,
-                 float* raw, unsigned* err) {
+int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const void* a_img, const void* q,
+                 const void* tab, float* raw, unsigned* err) {
     if (p.n_units <= 0) return 0;
-    static bool attr_set[64] = {};
+    if (fmt != kMsBf16x3 && fmt != kMsTf32) return -1;
+    auto kern = fmt == kMsTf32 ? k_ms_tc<kMsTf32> : k_ms_tc<kMsBf16x3>;
+    static bool attr_set[2][64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
-    if (!attr_set[dev]) {
-        if (cudaFuncSetAttribute(k_ms_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kMsSmem) != cudaSuccess)
+    if (!attr_set[fmt][dev]) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMsSmem) != cudaSuccess)
             return -1;
-        attr_set[dev] = true;  // setting it twice from two threads is harmless
+        attr_set[fmt][dev] = true;  // setting it twice from two threads is harmless
     }
     MsArgs a;
     a.a_img = (const unsigned char*)a_img;
@@ -596,7 +671,7 @@ int launch_ms_tc(cudaStream_t st, const MsPlan& p, int n_ranges, const void* a_i
     a.n_units = p.n_units;
     a.raw = raw;
     a.err = err;
-    k_ms_tc<<<p.n_ctas, kMsThreads, kMsSmem, st>>>(a);
+    kern<<<p.n_ctas, kMsThreads, kMsSmem, st>>>(a);
     return 1;
 }
 

@@ -1537,7 +1537,7 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
                           const ncpa_tl_params* tp, int method, double* re, double* im) {
     if (!ctx || !m || !tp || !rcv_height_m || n_rcv < 1 || problem < 0 || problem >= m->P) return NCPA_EINVAL;
     if ((re == nullptr) != (im == nullptr)) return NCPA_EINVAL;
-    if (method != NCPA_SUM_FP64 && method != NCPA_SUM_TC_BF16X3) return NCPA_EINVAL;
+    if (method != NCPA_SUM_FP64 && method != NCPA_SUM_TC_BF16X3 && method != NCPA_SUM_TC_TF32) return NCPA_EINVAL;
     if (!m->prm.want_vectors) return fail(ctx, NCPA_EINVAL, "the modal sum at receivers needs want_vectors");
     return guarded(ctx, [&]() -> ncpa_status {
         if (tp->n_ranges < 1 || !(tp->dr_m > 0)) throw ApiError(NCPA_EINVAL, "bad range grid");
@@ -1586,11 +1586,12 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
                 ctx->ms_q.alloc(pl.q_bytes, st);
                 ctx->ms_tab.alloc(pl.tab_bytes, st);
                 ctx->ms_raw.alloc(pl.raw_bytes, st);
-                check_launch(ctx, ncpa::launch_ms_prepare(st, pl, n_rcv, M, kr, ki, vs, ctx->ms_idx.as<int>(), vfull,
-                                                          tp->dr_m, tp->lossless, ctx->ms_img.p, ctx->ms_q.p,
+                const int fmt = method == NCPA_SUM_TC_TF32 ? 1 : 0;
+                check_launch(ctx, ncpa::launch_ms_prepare(st, pl, fmt, n_rcv, M, kr, ki, vs, ctx->ms_idx.as<int>(),
+                                                          vfull, tp->dr_m, tp->lossless, ctx->ms_img.p, ctx->ms_q.p,
                                                           ctx->ms_tab.p));
                 tm.mark("ms-prep");
-                check_launch(ctx, ncpa::launch_ms_tc(st, pl, nr, ctx->ms_img.p, ctx->ms_q.p, ctx->ms_tab.p,
+                check_launch(ctx, ncpa::launch_ms_tc(st, pl, fmt, nr, ctx->ms_img.p, ctx->ms_q.p, ctx->ms_tab.p,
                                                      ctx->ms_raw.as<float>(), ctx->d_err.as<unsigned>()));
                 tm.mark("ms-tc");
                 check_launch(ctx, ncpa::launch_ms_finish(st, pl, n_rcv, nr, tp->dr_m, ctx->ms_raw.as<float>(),

@@ -440,7 +440,7 @@ class Modes:
                        "ncpa_tl_2d")
         return z, re, im
 
-    SUM_FP64, SUM_TC_BF16X3 = 0, 1
+    SUM_FP64, SUM_TC_BF16X3, SUM_TC_TF32 = 0, 1, 2
 
     def tl_multi(self, p, heights_m, n_ranges, dr_m, method=1, lossless=False, to_host=True):
         """Modal sum at many receivers: complex P [n_rcv x n_ranges]."""

@@ -2,10 +2,12 @@
 tcgen05 split-BF16 tensor-core sum against an FP64 NumPy sum of the same
 modes, and end to end against the oracle's modes.
 
-Error statement checked here for the tensor-core path: |P_tc - P| is at most
-2e-4 of S = sum_m |A_jm e^{i k_m r}| (the modal terms' magnitude), and TL is
-within 0.05 dB wherever TL > -140 dB and |P| > 1e-3 S (outside deep
-cancellation nulls, where no fixed relative precision suffices)."""
+Error statement checked here for the tensor-core paths: split-BF16 |P_tc - P|
+is at most 2e-4 of S = sum_m |A_jm e^{i k_m r}| (the modal terms' magnitude),
+and TL is within 0.05 dB wherever TL > -140 dB and |P| > 1e-3 S (outside deep
+cancellation nulls, where no fixed relative precision suffices).  TF32
+(10-bit mantissa operands): |P_tf32 - P| at most 2e-3 of S, TL within 0.1 dB
+where TL > -140 dB and |P| > 2e-2 S."""
 import numpy as np
 import pytest
 
@@ -92,3 +94,21 @@ def test_tensor_core_sum_against_oracle_modes(solved, analytic_profile):
     tl_ref = 20 * np.log10(np.abs(P))
     sel = (tl_ref > -140.0) & (np.abs(P) > 1e-3 * S)
     assert np.max(np.abs(20 * np.log10(np.abs(ptc[sel])) - tl_ref[sel])) < 0.05
+
+
+@pytest.mark.parametrize("n_rcv,n_ranges,dr", [(64, 1000, 500.0), (100, 700, 1000.0), (7, 300, 2000.0)])
+def test_tf32_tensor_core_sum(solved, n_rcv, n_ranges, dr):
+    m, g, v, nz = solved
+    h = _heights(n_rcv, g.dz)
+    idx = np.ceil(h / g.dz).astype(int)
+    P, S = _ref_sum(g.kr, g.ki, g.vs, v[idx, :], n_ranges, dr)
+    p32 = m.tl_multi(0, h, n_ranges, dr, method=m.SUM_TC_TF32)
+    err = np.abs(p32 - P) / S
+    assert np.max(err) < 2e-3, np.max(err)
+    tl_ref = 20 * np.log10(np.abs(P))
+    sel = (tl_ref > -140.0) & (np.abs(P) > 2e-2 * S)
+    assert sel.mean() > 0.5
+    assert np.max(np.abs(20 * np.log10(np.abs(p32[sel])) - tl_ref[sel])) < 0.1
+    # the split-BF16 sum is the more accurate of the two
+    ptc = m.tl_multi(0, h, n_ranges, dr, method=m.SUM_TC_BF16X3)
+    assert np.max(np.abs(ptc - P) / S) < np.max(err)
