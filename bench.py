@@ -414,19 +414,21 @@ def modal_sum_leg(ctx, stream, bf16_peak, k=10):
         return ev0.elapsed_time(ev1) / reps
 
     def kernel_ms(method):
+        """ms of the tensor-core kernel per call, and of each phase"""
         ctx.reset_stats()
         ctx.set_timing(True)
         for _ in range(k):
             m.tl_multi(0, h, MS_NR, MS_DR, method=method, to_host=False)
         ctx.set_timing(False)
-        t_tc, n_tc = ctx.phase_stats("ms-tc")
-        return t_tc / max(n_tc, 1)
+        ph = {n: ctx.phase_stats(n) for n in ("ms-prep", "ms-tc", "ms-finish")}
+        per = {n: round(t / max(c, 1), 4) for n, (t, c) in ph.items()}
+        return per["ms-tc"], per
 
     ms_call = timed(1, k)
     ms_call_tf32 = timed(2, k)
     ms_fp64 = timed(0, 2)
-    ms_kernel = kernel_ms(1)
-    ms_kernel_tf32 = kernel_ms(2)
+    ms_kernel, phases = kernel_ms(1)
+    ms_kernel_tf32, phases_tf32 = kernel_ms(2)
     p_tc = m.tl_multi(0, h, 2000, MS_DR, method=1)
     p_32 = m.tl_multi(0, h, 2000, MS_DR, method=2)
     p_64 = m.tl_multi(0, h, 2000, MS_DR, method=0)
@@ -449,13 +451,14 @@ def modal_sum_leg(ctx, stream, bf16_peak, k=10):
                     % M,
         "modes": int(M),
         "ms_per_call": round(ms_call, 4), "ms_kernel": round(ms_kernel, 4), "ms_fp64_cuda_cores": round(ms_fp64, 3),
+        "phases_ms": phases,
         "roofline": {"kernel": "k_ms_tc (tcgen05 split-BF16)", "bound": "tensor", "achieved": round(achieved, 1),
                      "peak": bf16_peak, "unit": "TFLOP/s", "frac": round(achieved / bf16_peak, 4),
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)",
                      "flops_per_launch": tensor, "algorithmic_flops_per_launch": alg, "traffic": TRAFFIC_MS_TC,
                      "traffic_source": "ncu capture, profiles/k_ms_tc_modal_sum_64rcv_20000rng.md"},
         "error_vs_fp64": err(p_tc),
-        "tf32": {"ms_per_call": round(ms_call_tf32, 4), "ms_kernel": round(ms_kernel_tf32, 4),
+        "tf32": {"ms_per_call": round(ms_call_tf32, 4), "ms_kernel": round(ms_kernel_tf32, 4), "phases_ms": phases_tf32,
                  "algorithmic_tflops": round(alg / (ms_kernel_tf32 / 1e3) / 1e12, 1),
                  "frac_of_tf32_peak": round(alg / (ms_kernel_tf32 / 1e3) / 1e12 / (bf16_peak / 2.0), 4),
                  "peak_note": "tf32 dense rate taken as half the measured bf16 peak",

@@ -197,7 +197,7 @@ __device__ void ms_table_entry(int id, int M, int M_pad, const double* __restric
     tab[id] = v;
 }
 
-// tile phases e^{i k_m r_n0}, r_n0 = (tile * 128 + 1) dr: the phase k r is
+// tile phases e^{i k_m r_n0}, r_n0 = (tile * 256 + 1) dr: the phase k r is
 // reduced mod 2 pi in FP64 before the sine / cosine and the cast to FP32
 __device__ void ms_phase_entry(long long id, int M, int M_pad, int n_tiles, const double* __restrict__ kr,
                                const double* __restrict__ ki, double dr, int lossless, float2* __restrict__ q) {
@@ -291,7 +291,7 @@ struct MsArgs {
     const float2* tab;           // [M_pad][kMsTabW]
     int M_pad, n_chunks, n_tiles, n_ranges, groups;
     long long n_units;           // groups * n_tiles * n_chunks
-    float* raw;                  // [n_parts][groups][128][n_ranges] per-CTA partial sums of a tile
+    float* raw;                  // [n_parts][groups][n_tiles][256 columns][128 rows] per-CTA partial tiles
     unsigned* err;
 };
 
@@ -514,8 +514,10 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             const int row = 32 * (warp & 3) + lane;
             const long long gt = (long long)pos.group * a.n_tiles + pos.tile;
             const int part_slot = blockIdx.x - ms_cta_of(gt * a.n_chunks, a.n_units, gridDim.x);
-            const int n0 = pos.tile * kMsNT + (kMsNT / 2) * col_half;
-            float* out = a.raw + (((size_t)part_slot * a.groups + pos.group) * kMsRows + row) * a.n_ranges;
+            // partial tile stored column-major (the 128 rows of a column
+            // contiguous), so each store instruction of the warp writes 128 B
+            float* tcol = a.raw + (((size_t)part_slot * a.groups + pos.group) * a.n_tiles + pos.tile) * kMsNT * kMsRows +
+                          (size_t)((kMsNT / 2) * col_half) * kMsRows + row;
 #pragma unroll 1
             for (int cb = 0; cb < kMsNT / 64; ++cb) {
                 uint32_t v[32];
@@ -532,18 +534,10 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                       "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                const int nb = n0 + cb * 32;
-                if (nb + 32 <= a.n_ranges && (a.n_ranges & 3) == 0) {
-                    float4* o4 = reinterpret_cast<float4*>(out + nb);
+                // columns past n_ranges (last tile) land in the tile's own
+                // padding and are never read
 #pragma unroll
-                    for (int x = 0; x < 8; ++x)
-                        o4[x] = make_float4(__uint_as_float(v[4 * x]), __uint_as_float(v[4 * x + 1]),
-                                            __uint_as_float(v[4 * x + 2]), __uint_as_float(v[4 * x + 3]));
-                } else {
-#pragma unroll
-                    for (int x = 0; x < 32; ++x)
-                        if (nb + x < a.n_ranges) out[nb + x] = __uint_as_float(v[x]);
-                }
+                for (int x = 0; x < 32; ++x) tcol[(size_t)(cb * 32 + x) * kMsRows] = __uint_as_float(v[x]);
             }
             tc_fence_before();
             __syncwarp();
@@ -561,33 +555,55 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
 }
 
 // P = C(r_n) (D_re + i D_im) -> [n_rcv x n_ranges] FP64, adding the partial
-// slots of the CTAs that shared the tile; C(r) = (cr + i ci) / sqrt(r).
-// Block (x = group * n_tiles + tile, y = receiver in the group), threads over
-// the tile's ranges.
-__global__ void __launch_bounds__(kMsNT) k_ms_finish(int n_rcv, int n_ranges, double dr, int groups, int n_tiles,
-                                                      int n_chunks, long long n_units, int n_ctas, double cr,
-                                                      double ci, const float* __restrict__ raw,
-                                                      double* __restrict__ re, double* __restrict__ im) {
+// tiles of the CTAs that shared the tile (in FP64, slot order); C(r) =
+// (cr + i ci) / sqrt(r).  Block = (group, tile, 32-column block): the columns
+// are read contiguously (128 rows each), transposed through shared memory
+// and written along the ranges.
+constexpr int kMsFinCols = 32;
+__global__ void __launch_bounds__(256) k_ms_finish(int n_rcv, int n_ranges, double dr, int groups, int n_tiles,
+                                                   int n_chunks, long long n_units, int n_ctas, double cr, double ci,
+                                                   const float* __restrict__ raw, double* __restrict__ re,
+                                                   double* __restrict__ im) {
+    __shared__ double sum[kMsFinCols][kMsRows + 1];
     __shared__ int parts_sh;
-    const int tile = blockIdx.x % n_tiles, g = blockIdx.x / n_tiles, jr = blockIdx.y;
+    const int cb = blockIdx.x % (kMsNT / kMsFinCols);
+    const int gt = blockIdx.x / (kMsNT / kMsFinCols);
+    const int tile = gt % n_tiles, g = gt / n_tiles;
     if (threadIdx.x == 0) {
-        const long long u_first = ((long long)g * n_tiles + tile) * n_chunks;
+        const long long u_first = (long long)gt * n_chunks;
         parts_sh = ms_cta_of(u_first + n_chunks - 1, n_units, n_ctas) - ms_cta_of(u_first, n_units, n_ctas) + 1;
     }
     __syncthreads();
-    const int n = tile * kMsNT + threadIdx.x;
-    if (n >= n_ranges || g * kMsRcv + jr >= n_rcv) return;
-    double dre = 0.0, dim = 0.0;
+    const int c0 = cb * kMsFinCols;  // first column inside the tile
+    const int row = threadIdx.x & (kMsRows - 1), col0 = threadIdx.x >> 7;
+    // every slot read was written in full (256 columns, padding included)
+    constexpr int kPer = kMsFinCols / 2;  // columns per thread
+    double acc[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) acc[k] = 0.0;
     for (int p = 0; p < parts_sh; ++p) {
-        const float* base = raw + ((size_t)p * groups + g) * kMsRows * n_ranges;
-        dre += base[(size_t)jr * n_ranges + n];
-        dim += base[(size_t)(jr + kMsRcv) * n_ranges + n];
+        const float* base = raw + ((((size_t)p * groups + g) * n_tiles + tile) * kMsNT + c0 + col0) * kMsRows + row;
+        float v[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) v[k] = base[(size_t)(2 * k) * kMsRows];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) acc[k] += v[k];
     }
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) sum[col0 + 2 * k][row] = acc[k];
+    __syncthreads();
+    const int nl = threadIdx.x & (kMsFinCols - 1);
+    const int n = tile * kMsNT + c0 + nl;
+    if (n >= n_ranges) return;
     const double sr = 1.0 / sqrt((n + 1) * dr);
     const double fr = cr * sr, fi = ci * sr;
-    const size_t o = (size_t)(g * kMsRcv + jr) * n_ranges + n;
-    re[o] = fr * dre - fi * dim;
-    im[o] = fr * dim + fi * dre;
+    for (int jr = threadIdx.x >> 5; jr < kMsRcv; jr += 256 / kMsFinCols) {
+        if (g * kMsRcv + jr >= n_rcv) break;
+        const double dre = sum[nl][jr], dim = sum[nl][jr + kMsRcv];
+        const size_t o = (size_t)(g * kMsRcv + jr) * n_ranges + n;
+        re[o] = fr * dre - fi * dim;
+        im[o] = fr * dim + fi * dre;
+    }
 }
 
 // gather of the mode values at the receiver grid points: vz[j][m] = v[idx_j][m]
@@ -620,7 +636,7 @@ MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms) {
     p.a_img_bytes = (size_t)p.groups * p.n_chunks * 2 * kMsABytes;
     p.q_bytes = (size_t)p.n_tiles * p.M_pad * sizeof(float2);
     p.tab_bytes = (size_t)p.M_pad * kMsTabW * sizeof(float2);
-    p.raw_bytes = (size_t)p.n_parts * p.groups * kMsRows * n_ranges * sizeof(float);
+    p.raw_bytes = (size_t)p.n_parts * p.groups * p.n_tiles * kMsNT * kMsRows * sizeof(float);
     return p;
 }
 
@@ -680,9 +696,9 @@ int launch_ms_finish(cudaStream_t st, const MsPlan& p, int n_rcv, int n_ranges, 
     // 1000 * 4 pi i e^{-i pi/4} / sqrt(8 pi) = c0 (cos pi/4 + i sin pi/4)
     const double c0 = 1000.0 * 4 * kPi / std::sqrt(8.0 * kPi);
     const double cr = c0 * std::sin(kPi * 0.25), ci = c0 * std::cos(kPi * 0.25);
-    const dim3 grid((unsigned)(p.groups * p.n_tiles), (unsigned)std::min(n_rcv, kMsRcv));
-    k_ms_finish<<<grid, kMsNT, 0, st>>>(n_rcv, n_ranges, dr, p.groups, p.n_tiles, p.n_chunks, p.n_units, p.n_ctas,
-                                        cr, ci, raw, re, im);
+    const unsigned blocks = (unsigned)(p.groups * p.n_tiles * (kMsNT / kMsFinCols));
+    k_ms_finish<<<blocks, 256, 0, st>>>(n_rcv, n_ranges, dr, p.groups, p.n_tiles, p.n_chunks, p.n_units, p.n_ctas, cr,
+                                        ci, raw, re, im);
     return 1;
 }
 
