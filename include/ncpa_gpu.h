@@ -66,6 +66,15 @@ ncpa_status ncpa_profile_create(ncpa_ctx *ctx, const ncpa_profile_desc *desc, nc
 ncpa_status ncpa_profile_load(ncpa_ctx *ctx, const char *path, const char *header_path,
                               ncpa_profile **out);
 ncpa_status ncpa_profile_destroy(ncpa_profile *prof);
+/* G2S-style profiles (the layout of the reference's samples/g2sprofile.sample,
+ * which its Atmosphere1D reader cannot take as it is): an optional first line
+ * "Profile at (lat, lon)", '#' comments, then rows of Z [km], T [K], U, V
+ * [m/s], P [mbar], RHO [g/cm3].  ncpa_g2s_convert writes the equivalent NCPA
+ * profile file ("#%" header + columns; host only, no device needed) and
+ * returns the location (NaN without a location line; NULL to skip);
+ * ncpa_profile_load_g2s reads it straight into a device profile. */
+ncpa_status ncpa_g2s_convert(const char *g2s_path, const char *ncpa_path, double *lat, double *lon);
+ncpa_status ncpa_profile_load_g2s(ncpa_ctx *ctx, const char *path, ncpa_profile **out);
 /* User attenuation table (height km, Np/m), interpolated onto the profile
  * knots and used at every frequency instead of Sutherland-Bass (replaces
  * Atmosphere1D::read_attenuation_from_file, Atmosphere1D.cpp:307-424). */

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cctype>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <set>
@@ -174,6 +175,81 @@ ParsedProfile read_profile(const std::string& path, const std::string& header_pa
         }
     }
     return P;
+}
+
+ParsedProfile read_g2s_profile(const std::string& path, double& lat, double& lon) {
+    lat = lon = std::nan("");
+    std::ifstream in(path);
+    if (!in.good()) throw ParseError("G2S profile - cannot open " + path);
+    static const char* const kKeys[] = {"T", "U", "V", "P", "RHO"};
+    static const char* const kUnits[] = {"K", "m/s", "m/s", "mbar", "g/cm3"};
+    ParsedProfile P;
+    std::vector<std::vector<double>> cols(5);
+    std::string line;
+    bool first = true;
+    while (std::getline(in, line)) {
+        line = trim(line);
+        if (line.empty() || line[0] == '#') continue;
+        if (first && upper(line).rfind("PROFILE AT", 0) == 0) {
+            const size_t a = line.find('('), b = line.find(')');
+            if (a != std::string::npos && b != std::string::npos && b > a) {
+                auto f = split(line.substr(a + 1, b - a - 1), " ,");
+                if (f.size() == 2) {
+                    lat = parse_double(f[0], line);
+                    lon = parse_double(f[1], line);
+                }
+            }
+            first = false;
+            continue;
+        }
+        first = false;
+        auto f = split(line, " \t,");
+        if (f.size() < 6) {
+            std::ostringstream os;
+            os << "Error parsing data line:\n" << line << "\n6 columns expected (Z T U V P RHO), " << f.size()
+               << " columns found.";
+            throw ParseError(os.str());
+        }
+        P.z.push_back(parse_double(f[0], line));
+        for (int c = 0; c < 5; ++c) cols[c].push_back(parse_double(f[c + 1], line));
+    }
+    if (P.z.size() < 3) throw ParseError("G2S profile - fewer than 3 data rows in " + path);
+    P.z_units = canonical_units("km");
+    for (int c = 0; c < 5; ++c) {
+        P.vectors[kKeys[c]] = cols[c];
+        P.vector_units[kKeys[c]] = canonical_units(kUnits[c]);
+    }
+    return P;
+}
+
+void write_ncpa_profile(const ParsedProfile& prof, const std::vector<std::string>& keys, const std::string& path) {
+    std::ofstream out(path);
+    if (!out.good()) throw ParseError("cannot write " + path);
+    int col = 0;
+    for (const auto& kv : prof.scalars) {
+        auto u = prof.scalar_units.find(kv.first);
+        char buf[256];
+        std::snprintf(buf, sizeof buf, "#%% 0, %s, %s, %.17g\n", kv.first.c_str(),
+                      u == prof.scalar_units.end() || u->second.empty() ? "N/A" : u->second.c_str(), kv.second);
+        out << buf;
+    }
+    out << "#% " << ++col << ", Z, " << prof.z_units << "\n";
+    for (const auto& k : keys) {
+        auto u = prof.vector_units.find(k);
+        if (prof.vectors.find(k) == prof.vectors.end()) throw ParseError("no column " + k + " to write");
+        out << "#% " << ++col << ", " << k << ", " << (u == prof.vector_units.end() ? "N/A" : u->second) << "\n";
+    }
+    char buf[64];
+    for (size_t r = 0; r < prof.z.size(); ++r) {
+        std::snprintf(buf, sizeof buf, "%.17g", prof.z[r]);
+        out << buf;
+        for (const auto& k : keys) {
+            std::snprintf(buf, sizeof buf, " %.17g", prof.vectors.at(k)[r]);
+            out << buf;
+        }
+        out << "\n";
+    }
+    if (!out.good()) throw ParseError("error writing " + path);
 }
 
 SiProfile to_si_profile(const ParsedProfile& prof) {

@@ -45,6 +45,19 @@ struct SiProfile {
 // (ESSModeSolver.cpp:159-220); throws ParseError with the reference's message
 SiProfile to_si_profile(const ParsedProfile& prof);
 
+// G2S-style profile text (the layout of the reference's
+// samples/g2sprofile.sample): an optional first line "Profile at (lat, lon)",
+// '#' comment lines, then rows of at least six columns
+//   Z [km]  T [K]  U [m/s]  V [m/s]  P [mbar]  RHO [g/cm3]
+// (further columns ignored).  The reference's Atmosphere1D reads only
+// "#%"-described files, so this is the conversion step in front of it.
+// Returns the profile as if read from the equivalent NCPA file; lat / lon are
+// NaN when the file has no location line.
+ParsedProfile read_g2s_profile(const std::string& path, double& lat, double& lon);
+// writes an NCPA profile file ("#% col, KEY, units" header + columns) holding
+// the altitude column, the given vector keys in order and the scalars
+void write_ncpa_profile(const ParsedProfile& prof, const std::vector<std::string>& keys, const std::string& path);
+
 // two-column attenuation file (height km, Np/m), extended to the profile's
 // range with end values (Atmosphere1D::read_attenuation_from_file,
 // Atmosphere1D.cpp:307-424); returns (z_km, attn)

@@ -1185,6 +1185,49 @@ ncpa_status ncpa_profile_load(ncpa_ctx* ctx, const char* path, const char* heade
     return ncpa_profile_create(ctx, &d, out);
 }
 
+namespace {
+ncpa_status create_from_si(ncpa_ctx* ctx, const ncpa::SiProfile& S, ncpa_profile** out) {
+    ncpa_profile_desc d{};
+    d.n_knots = (int)S.z.size();
+    d.z = S.z.data();
+    d.u = S.u.data();
+    d.v = S.v.data();
+    d.t = S.t.data();
+    d.p = S.p.data();
+    d.rho = S.rho.data();
+    d.c0 = S.has_c0 ? S.c0.data() : nullptr;
+    d.attn = nullptr;
+    d.z0_m = S.z0;
+    d.has_z0 = S.has_z0;
+    return ncpa_profile_create(ctx, &d, out);
+}
+}  // namespace
+
+ncpa_status ncpa_g2s_convert(const char* g2s_path, const char* ncpa_path, double* lat, double* lon) {
+    if (!g2s_path || !ncpa_path) return NCPA_EINVAL;
+    return guarded(nullptr, [&]() -> ncpa_status {
+        double la, lo;
+        const ncpa::ParsedProfile P = ncpa::read_g2s_profile(g2s_path, la, lo);
+        ncpa::write_ncpa_profile(P, {"U", "V", "T", "RHO", "P"}, ncpa_path);
+        if (lat) *lat = la;
+        if (lon) *lon = lo;
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_profile_load_g2s(ncpa_ctx* ctx, const char* path, ncpa_profile** out) {
+    if (!ctx || !path || !out) return NCPA_EINVAL;
+    *out = nullptr;
+    ncpa::SiProfile S;
+    ncpa_status s = guarded(ctx, [&]() -> ncpa_status {
+        double la, lo;
+        S = ncpa::to_si_profile(ncpa::read_g2s_profile(path, la, lo));
+        return NCPA_OK;
+    });
+    if (s != NCPA_OK) return s;
+    return create_from_si(ctx, S, out);
+}
+
 ncpa_status ncpa_profile_set_attn(ncpa_profile* prof, const double* z_km, const double* attn, int n) {
     if (!prof || !z_km || !attn || n < 2) return NCPA_EINVAL;
     if (prof->plan_refs > 0) return fail(prof->ctx, NCPA_EINVAL, "profile is used by a plan");

@@ -32,8 +32,18 @@ EXPORTED = [
     "ncpa_modal_starter", "ncpa_source_waveform", "ncpa_tl_multi", "ncpa_ess_solve_jobs", "ncpa_server_opts_default", "ncpa_server_create",
     "ncpa_server_submit", "ncpa_server_wait", "ncpa_server_release", "ncpa_server_stats_get", "ncpa_server_destroy", "ncpa_modes_get_all",
     "ncpa_ess_plan_create", "ncpa_ess_plan_run", "ncpa_ess_plan_modes", "ncpa_ess_plan_tl", "ncpa_ess_plan_tuning",
-    "ncpa_ess_plan_destroy", "ncpa_profile_update",
+    "ncpa_ess_plan_destroy", "ncpa_profile_update", "ncpa_g2s_convert", "ncpa_profile_load_g2s",
 ]
+
+
+def g2s_convert(g2s_path, ncpa_path):
+    """Writes the NCPA-format equivalent of a G2S-style profile; returns the
+    (lat, lon) of its location line (NaN when absent).  Host only."""
+    la, lo = _c_double(), _c_double()
+    st = lib().ncpa_g2s_convert(str(g2s_path).encode(), str(ncpa_path).encode(), ctypes.byref(la), ctypes.byref(lo))
+    if st != 0:
+        raise NcpaError(st, "ncpa_g2s_convert")
+    return la.value, lo.value
 
 
 class NcpaError(RuntimeError):
@@ -111,6 +121,9 @@ def lib():
         L.ncpa_ess_plan_tuning.argtypes = [_vp, _ip, _ip, _ip, ctypes.POINTER(_c_double)]
         L.ncpa_ess_plan_destroy.argtypes = [_vp]
         L.ncpa_profile_update.argtypes = [_vp, ctypes.POINTER(_ProfileDesc)]
+        L.ncpa_g2s_convert.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_c_double),
+                                       ctypes.POINTER(_c_double)]
+        L.ncpa_profile_load_g2s.argtypes = [_vp, ctypes.c_char_p, ctypes.POINTER(_vp)]
         L.ncpa_ess_solve.argtypes = [_vp, _vp, ctypes.POINTER(EssParams), _dp, _c_int, _dp, _c_int,
                                      ctypes.POINTER(_vp)]
         L.ncpa_modes_destroy.argtypes = [_vp]
@@ -228,6 +241,12 @@ class Context:
         h = _vp()
         self.check(lib().ncpa_profile_load(self.h, path.encode(), header.encode() if header else None,
                                            ctypes.byref(h)), "ncpa_profile_load")
+        return Profile(self, h)
+
+    def load_profile_g2s(self, path):
+        """G2S-style profile file (location line + Z T U V P RHO columns)."""
+        h = _vp()
+        self.check(lib().ncpa_profile_load_g2s(self.h, str(path).encode(), ctypes.byref(h)), "ncpa_profile_load_g2s")
         return Profile(self, h)
 
     def profile_from_arrays(self, z, u, v, t, p, rho, c0=None, attn=None, z0=None):

@@ -4,6 +4,8 @@ Reads the reference's shipped example outputs and sample profile (run once,
 where the reference checkout is available) and writes compact copies:
 
   canonical_profile.dat.gz   samples/NCPA_canonical_profile_zuvwtdp.dat
+  g2s_profile.sample.gz      samples/g2sprofile.sample (G2S layout: a
+                             "Profile at (lat, lon)" line, then Z T U V P RHO)
   modess_tloss_1d.npz        docs/.../modess_gp_files/code_outputs/tloss_1d.nm
                              and tloss_1d.lossless.nm (Modess, 0.1 Hz, az 90,
                              pre-2.0.1 TL scaling: +60 dB vs the current code)
@@ -38,8 +40,11 @@ def read_dispersion(path):
 
 def main():
     prof = os.path.join(REF, "samples", "NCPA_canonical_profile_zuvwtdp.dat")
-    with open(prof, "rb") as fi, gzip.open(os.path.join(OUT, "canonical_profile.dat.gz"), "wb", 9) as fo:
-        fo.write(fi.read())
+    for src, dst in ((prof, "canonical_profile.dat.gz"),
+                     (os.path.join(REF, "samples", "g2sprofile.sample"), "g2s_profile.sample.gz")):
+        with open(src, "rb") as fi, open(os.path.join(OUT, dst), "wb") as raw, \
+                gzip.GzipFile(fileobj=raw, mode="wb", compresslevel=9, mtime=0) as fo:
+            fo.write(fi.read())
     co = os.path.join(REF, "docs", "ncpaprop_run_manual_TeX", "figs", "modess_gp_files", "code_outputs")
     lossy = np.loadtxt(os.path.join(co, "tloss_1d.nm"))
     lossless = np.loadtxt(os.path.join(co, "tloss_1d.lossless.nm"))
