@@ -237,6 +237,23 @@ typedef struct {
 
 /* waveforms: [n_ranges x nfft], 2 Re p(t) at t = i/(nfft df) + t0; NULL
  * waveforms keeps the result in HBM */
+/* Dispersion file of ModBB --dispersion on the host, read as
+ * ModalBroadbandPropagator::read_dispersion_file does
+ * (ModalBroadbandPropagator.cpp:98-138: "f M rho_src rho_rcv" then M
+ * quadruples per line, at most 4000 modes, reading stops at the first
+ * non-number, the DC slot f = 0 first).  With cache_path, a binary copy of
+ * the parsed arrays stamped with the text file (size, modification time,
+ * FNV-1a hash) is used when it matches, and written when it does not, so
+ * repeated propagation runs skip the text parsing.  NCPA_EPARSE for a
+ * malformed or missing text file; the arrays stay valid until destroy. */
+typedef struct ncpa_dispersion ncpa_dispersion;
+ncpa_status ncpa_dispersion_read(const char *text_path, const char *cache_path, ncpa_dispersion **out);
+/* desc points into the set; text_rows = newline characters of the text
+ * file; from_cache = 1 when the binary cache was used */
+ncpa_status ncpa_dispersion_desc_get(const ncpa_dispersion *disp, ncpa_dispersion_desc *desc, int *text_rows,
+                                     int *from_cache);
+ncpa_status ncpa_dispersion_destroy(ncpa_dispersion *disp);
+
 ncpa_status ncpa_bb_synthesize(ncpa_ctx *ctx, const ncpa_dispersion_desc *disp,
                                const ncpa_bb_params *bp, double *waveforms);
 /* same, taking the dispersion of a device-resident batched solve (one

@@ -24,46 +24,29 @@ int count_newlines(const std::string& path) {
     return n;
 }
 
-struct Dispersion {
-    std::vector<double> f{0.0};  // DC slot first
-    std::vector<int> off{0, 0};
-    std::vector<double> kr, ki, vs, vr;
-    double rho_src = 1.0, rho_rcv = 1.0;
-};
-
 // ModalBroadbandPropagator::read_dispersion_file (ModalBroadbandPropagator.cpp:98-138)
-Dispersion read_dispersion(const std::string& path) {
-    std::FILE* fp = std::fopen(path.c_str(), "r");
-    if (!fp) throw RunError("file << " + path + " could not be opened.");
-    std::printf("--> Opening dispersion file %s ...if the program chokes here the file may be corrupt.\n",
-                path.c_str());
-    Dispersion d;
-    double fr;
-    while (std::fscanf(fp, "%lf", &fr) == 1) {
-        int m = 0;
-        if (std::fscanf(fp, "%d", &m) != 1 || std::fscanf(fp, "%lf", &d.rho_src) != 1 ||
-            std::fscanf(fp, "%lf", &d.rho_rcv) != 1 || m < 0 || m > 4000) {
-            std::fclose(fp);
-            throw RunError(path + ": read_dispersion_data format error");
-        }
-        for (int j = 0; j < m; ++j) {
-            double x1, x2, y1, y2;
-            if (std::fscanf(fp, "%lf %lf %lf %lf", &x1, &x2, &y1, &y2) != 4) {
-                std::fclose(fp);
-                throw RunError(path + ": read_dispersion_data format error");
-            }
-            d.kr.push_back(x1);
-            d.ki.push_back(x2);
-            d.vs.push_back(y1);
-            d.vr.push_back(y2);
-        }
-        d.f.push_back(fr);
-        d.off.push_back((int)d.kr.size());
+// through the library reader, with its binary cache when cache is not empty
+struct Dispersion {
+    ncpa_dispersion* h = nullptr;
+    ncpa_dispersion_desc d{};
+    int rows = 0, from_cache = 0;
+    Dispersion(const std::string& path, const std::string& cache) {
+        std::FILE* fp = std::fopen(path.c_str(), "r");
+        if (!fp) throw RunError("file << " + path + " could not be opened.");
+        std::fclose(fp);
+        std::printf("--> Opening dispersion file %s ...if the program chokes here the file may be corrupt.\n",
+                    path.c_str());
+        if (ncpa_dispersion_read(path.c_str(), cache.empty() ? nullptr : cache.c_str(), &h) != NCPA_OK)
+            throw RunError(path + ": read_dispersion_data format error" +
+                           (cache.empty() ? std::string() : " (or dispersion cache " + cache + " not writable)"));
+        ncpa_dispersion_desc_get(h, &d, &rows, &from_cache);
+        if (from_cache) std::printf("--> Parsed arrays taken from the dispersion cache %s\n", cache.c_str());
+        std::printf("--> Found modes at %d positive frequencies in file %s\n", d.n_freq, path.c_str());
     }
-    std::fclose(fp);
-    std::printf("--> Found modes at %d positive frequencies in file %s\n", (int)d.f.size(), path.c_str());
-    return d;
-}
+    ~Dispersion() { ncpa_dispersion_destroy(h); }
+    Dispersion(const Dispersion&) = delete;
+    Dispersion& operator=(const Dispersion&) = delete;
+};
 
 // two-column (time, amplitude) or three-column (f, Re, Im) source files, read
 // the way the reference's stream loops do (BroadbandPropagator.cpp:478-537):
@@ -101,13 +84,15 @@ int run_propagation(const Params& prm) {
         for (int i = 0; i < nr; ++i) ranges.push_back((rmin + (double)i * rstep) * 1000.0);
     }
     const std::string disp_path = prm.get_string("input_dispersion_file");
-    const int rows = count_newlines(disp_path);
-    Dispersion d = read_dispersion(disp_path);
-    const int nfreq = (int)d.f.size();
+    const Dispersion disp(disp_path, prm.get_string("dispersion_cache"));
+    const ncpa_dispersion_desc& dd = disp.d;
+    const int rows = disp.rows;
+    const double* freq = dd.f;
+    const int nfreq = dd.n_freq;
     if (nfreq != rows + 1)
         std::printf("Warning: %d lines but %d frequencies in %s\n", rows, nfreq - 1, disp_path.c_str());
     if (nfreq < 3) throw RunError("the dispersion file needs at least two frequencies");
-    const double f_step = d.f[2] - d.f[1];
+    const double f_step = freq[2] - freq[1];
     // NFFT rule (ModalBroadbandPropagator.cpp:66-84)
     int nfft = prm.get_int("nfft");
     if (nfft < 4 * nfreq) {
@@ -129,14 +114,14 @@ int run_propagation(const Params& prm) {
     if (src_type == "impulse" || src_type == "pulse1" || src_type == "pulse2") {
         const int kind = src_type == "impulse" ? 0 : src_type == "pulse1" ? 1 : 2;
         ncpa_cli::check(ctx,
-                        ncpa_source_spectrum_builtin(ctx, kind, d.f.data(), nfreq, prm.get_float("f_center"), nfft,
+                        ncpa_source_spectrum_builtin(ctx, kind, freq, nfreq, prm.get_float("f_center"), nfft,
                                                      s_re.data(), s_im.data()),
                         "source spectrum");
     } else if (src_type == "spectrum") {
         std::cout << "Loading source spectrum from file " << src_file << std::endl;
         auto c = read_columns(src_file, 3);
         if ((int)c[0].size() > nfft) throw RunError("file " + src_file + " has more points than NFFT");
-        if (c[0].empty() || std::fabs(c[0][0] - d.f[0]) > 1.0e-8)
+        if (c[0].empty() || std::fabs(c[0][0] - freq[0]) > 1.0e-8)
             throw RunError("The frequencies from the source spectrum file " + src_file +
                            " do not appear to match the ones from the provided dispersion file");
         for (int i = 0; i < nfreq && i < (int)c[0].size(); ++i) {
@@ -155,7 +140,7 @@ int run_propagation(const Params& prm) {
                         "source spectrum of the waveform");
     }
     if (src_type != "waveform")  // f_step * FFT of the zero-padded spectrum, x2
-        ncpa_cli::check(ctx, ncpa_source_waveform(ctx, d.f.data(), nfreq, s_re.data(), s_im.data(), nfft,
+        ncpa_cli::check(ctx, ncpa_source_waveform(ctx, freq, nfreq, s_re.data(), s_im.data(), nfft,
                                                   pulse.data()),
                         "source waveform");
     {
@@ -167,22 +152,12 @@ int run_propagation(const Params& prm) {
                   << " with format: | Time (s) | Amplitude |" << std::endl;
         f = std::fopen("source_spectrum_input.dat", "w");
         if (!f) throw RunError("file source_spectrum_input.dat could not be opened.");
-        for (int i = 0; i < nfreq; ++i) std::fprintf(f, "%14.9f %15.6e %15.6e\n", d.f[i], s_re[i], s_im[i]);
+        for (int i = 0; i < nfreq; ++i) std::fprintf(f, "%14.9f %15.6e %15.6e\n", freq[i], s_re[i], s_im[i]);
         std::fclose(f);
         std::cout << "--> The source spectrum is saved in file 'source_spectrum_input.dat' " << std::endl
                   << "with format: | Freq (Hz) | Re(S) | Imag(S) |" << std::endl;
     }
 
-    ncpa_dispersion_desc dd{};
-    dd.n_freq = nfreq;
-    dd.f = d.f.data();
-    dd.mode_off = d.off.data();
-    dd.re_k = d.kr.data();
-    dd.im_k = d.ki.data();
-    dd.v_src = d.vs.data();
-    dd.v_rcv = d.vr.data();
-    dd.rho_src = d.rho_src;
-    dd.rho_rcv = d.rho_rcv;
     ncpa_bb_params bp{};
     bp.n_ranges = (int)ranges.size();
     bp.ranges_m = ranges.data();

@@ -73,6 +73,7 @@ void configure(Params& ps) {
     }
     ps.add_string("input_dispersion_file", "");
     ps.require_if("input_dispersion_file", "propagation");
+    ps.add_string("dispersion_cache", "");  // binary copy of the parsed dispersion file (no reference counterpart)
     ps.add_string("output_waveform_file", "");
     ps.require_if("output_waveform_file", "propagation");
     ps.add_string("source", "impulse");
@@ -106,7 +107,7 @@ void usage(std::ostream& os) {
           "      [--source impulse|pulse1|pulse2|spectrum|waveform] [--source_file F] [--f_center f]\n"
           "      [--receiver single --range_km r | --receiver multiple --start_range_km a\n"
           "       --end_range_km b --range_step_km d] [--nfft n] [--max_celerity 340]\n"
-          "      [--use_zero_attenuation]\n\n"
+          "      [--use_zero_attenuation] [--dispersion_cache F]\n\n"
           "Output files: the dispersion file; source_waveform_input.dat, source_spectrum_input.dat\n"
           "and the waveform file (r [km], t [s], 2 Re p) for --propagation.\n";
 }

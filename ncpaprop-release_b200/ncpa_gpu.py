@@ -33,7 +33,31 @@ EXPORTED = [
     "ncpa_server_submit", "ncpa_server_wait", "ncpa_server_release", "ncpa_server_stats_get", "ncpa_server_destroy", "ncpa_modes_get_all",
     "ncpa_ess_plan_create", "ncpa_ess_plan_run", "ncpa_ess_plan_modes", "ncpa_ess_plan_tl", "ncpa_ess_plan_tuning",
     "ncpa_ess_plan_destroy", "ncpa_profile_update", "ncpa_g2s_convert", "ncpa_profile_load_g2s",
+    "ncpa_dispersion_read", "ncpa_dispersion_desc_get", "ncpa_dispersion_destroy",
 ]
+
+
+def read_dispersion(text_path, cache_path=None):
+    """A ModBB dispersion file parsed by the library (host only), optionally
+    through its binary cache: dict of f (DC slot first), mode_off, kr, ki,
+    vs, vr, rho_src, rho_rcv, rows (newlines of the text), from_cache."""
+    h = _vp()
+    st = lib().ncpa_dispersion_read(str(text_path).encode(), str(cache_path).encode() if cache_path else None,
+                                    ctypes.byref(h))
+    if st != 0:
+        raise NcpaError(st, "ncpa_dispersion_read")
+    try:
+        d, rows, fc = _DispDesc(), _c_int(), _c_int()
+        lib().ncpa_dispersion_desc_get(h, ctypes.byref(d), ctypes.byref(rows), ctypes.byref(fc))
+        nf = d.n_freq
+        off = np.ctypeslib.as_array(d.mode_off, shape=(nf + 1,)).copy()
+        n = int(off[-1])
+        arr = lambda p, k: np.ctypeslib.as_array(p, shape=(k,)).copy() if k else np.empty(0)
+        return {"f": arr(d.f, nf), "mode_off": off, "kr": arr(d.re_k, n), "ki": arr(d.im_k, n),
+                "vs": arr(d.v_src, n), "vr": arr(d.v_rcv, n), "rho_src": d.rho_src, "rho_rcv": d.rho_rcv,
+                "rows": rows.value, "from_cache": fc.value}
+    finally:
+        lib().ncpa_dispersion_destroy(h)
 
 
 def g2s_convert(g2s_path, ncpa_path):
@@ -124,6 +148,9 @@ def lib():
         L.ncpa_g2s_convert.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_c_double),
                                        ctypes.POINTER(_c_double)]
         L.ncpa_profile_load_g2s.argtypes = [_vp, ctypes.c_char_p, ctypes.POINTER(_vp)]
+        L.ncpa_dispersion_read.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_vp)]
+        L.ncpa_dispersion_desc_get.argtypes = [_vp, ctypes.POINTER(_DispDesc), _ip, _ip]
+        L.ncpa_dispersion_destroy.argtypes = [_vp]
         L.ncpa_ess_solve.argtypes = [_vp, _vp, ctypes.POINTER(EssParams), _dp, _c_int, _dp, _c_int,
                                      ctypes.POINTER(_vp)]
         L.ncpa_modes_destroy.argtypes = [_vp]
@@ -239,7 +266,7 @@ class Context:
     # profiles -------------------------------------------------------------
     def load_profile(self, path, header=""):
         h = _vp()
-        self.check(lib().ncpa_profile_load(self.h, path.encode(), header.encode() if header else None,
+        self.check(lib().ncpa_profile_load(self.h, str(path).encode(), str(header).encode() if header else None,
                                            ctypes.byref(h)), "ncpa_profile_load")
         return Profile(self, h)
 

@@ -340,3 +340,22 @@ def test_modbb_propagation_files(binaries, modbb_dispersion, source, tmp_path):
         hre, him = O.bb_transfer(d, r)
         ref = O.bb_pulse(d, sre, sim, hre, him, t0, nfft)
         assert np.linalg.norm(a[:, 2] - ref) <= 1e-4 * np.linalg.norm(ref)
+
+
+@pytest.mark.gpu
+def test_modbb_propagation_with_dispersion_cache(binaries, modbb_dispersion, tmp_path):
+    """--dispersion_cache: the first run writes the binary cache, the second
+    reads it; both write the same waveform file byte for byte as a run
+    without the option."""
+    disp = str(modbb_dispersion / "disp.dat")
+    base = ["--propagation", "--input_dispersion_file", disp, "--output_waveform_file", "wave.dat",
+            "--receiver", "single", "--range_km", "150", "--source", "pulse1", "--max_celerity", "330"]
+    outs = []
+    for i, extra in enumerate(([], ["--dispersion_cache", str(tmp_path / "disp.cache")],
+                               ["--dispersion_cache", str(tmp_path / "disp.cache")])):
+        d = tmp_path / ("run%d" % i)
+        d.mkdir()
+        p = run(binaries, "ModBB", base + extra, d, check_rc=0)
+        outs.append(((d / "wave.dat").read_bytes(), p.stdout))
+    assert outs[0][0] == outs[1][0] == outs[2][0]
+    assert "dispersion cache" not in outs[1][1] and "dispersion cache" in outs[2][1]
