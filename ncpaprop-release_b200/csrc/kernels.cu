@@ -549,7 +549,11 @@ int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* 
 //    ends) take a safeguarded Newton step on det(S - x): one virtual lane
 //    (chain 0) carries the x-derivative of the recurrence; the Sturm count at
 //    the iterate shrinks the bracket and a step leaving the bracket falls back
-//    to its midpoint;
+//    to its midpoint.  An eigenvalue is final when the correction is below
+//    tol, or when two Newton steps in a row stayed inside the bracket, the
+//    correction shrank at least fourfold and the quadratic-convergence model
+//    predicts the next one below tol (|d_k|^3 <= tol |d_{k-1}|^2), which
+//    saves the sweep that would only confirm it;
 //  * the other virtual lanes are dealt round-robin over the eigenvalues not
 //    yet isolated (G_e lanes each), which cut their bracket into G_e + 1
 //    pieces.  Rounds with Newton slots only sweep a single chain.
@@ -665,6 +669,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
         // state of eigen slot `lane`
         const int J = pi.c_lo + w.j0 + lane;
         double a = pi.lo, b = pi.lo, x = pi.lo;
+        double dprev = 0.0;  // size of the previous Newton correction (0: none yet)
         int ca = 0, cb = 0, mode = 2;
         if (lane < w.m) {  // initial bracket from the isolation scan
             int t0 = 0;
@@ -751,14 +756,22 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
                     b = xo;
                     cb = cN;
                 }
-                if (fabs(rN) <= tol) {
+                const double ad = fabs(rN);
+                if (ad <= tol) {
                     x = fmin(fmax(xo - rN, a), b);
                     mode = 2;
                 } else {
                     const double xn = xo - rN;
                     const bool ok = isfinite(xn) && xn > a && xn < b;
                     x = ok ? xn : 0.5 * (a + b);
-                    if (!(b - a > tol)) mode = 2;
+                    if (!(b - a > tol)) {
+                        mode = 2;
+                    } else if (ok && dprev > 0.0 && ad <= 0.25 * dprev && ad * ad * ad <= tol * dprev * dprev) {
+                        // quadratic convergence: the next correction would be
+                        // about ad^2 (ad / dprev^2) <= tol, so x = xn is final
+                        mode = 2;
+                    }
+                    dprev = ok ? ad : 0.0;
                 }
             } else if (isB) {
                 const double A0 = a, B0 = b;
