@@ -418,7 +418,7 @@ int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2,
 // ===========================================================================
 // CTA-cooperative Sturm sweep: the diagonal streams through shared memory in
 // kChunk-double chunks by TMA bulk copies (kNbuf-deep ring, one mbarrier per
-// slot); every thread runs its own recurrence at its own shift x.
+// slot); every thread runs its own recurrences at its own two shifts.
 // ===========================================================================
 constexpr int kNbuf = 4;
 
@@ -434,14 +434,18 @@ __device__ __forceinline__ void ring_issue(Ring& r, unsigned k, const double* sr
     tma_load_1d(r.buf + slot * kChunk, src, kChunk * 8, &r.bars[slot]);
 }
 
-__device__ int cta_sturm_sweep(const double* __restrict__ s, int nz, double x, Ring& r, unsigned* err) {
+// Two shifts per thread: two independent chains interleaved step by step
+// (sturm_word32_pair: each chain's arithmetic is that of SturmState::word32)
+__device__ void cta_sturm_sweep_pair(const double* __restrict__ s, int nz, double x0, double x1, Ring& r,
+                                     unsigned* err, int& c0, int& c1) {
     const int nch = (nz + kChunk - 1) / kChunk;
     const unsigned base = r.loads;
     if (threadIdx.x == 0) {
         for (int c = 0; c < nch && c < kNbuf; ++c) ring_issue(r, base + c, s + (size_t)c * kChunk);
     }
-    SturmState st;
-    st.reset();
+    SturmState A, B;
+    A.reset();
+    B.reset();
     for (int c = 0; c < nch; ++c) {
         const unsigned k = base + c;
         const int slot = k % kNbuf;
@@ -449,43 +453,10 @@ __device__ int cta_sturm_sweep(const double* __restrict__ s, int nz, double x, R
         const double* b = r.buf + slot * kChunk;
         const int valid = min(kChunk, nz - c * kChunk);
         const int nw = valid >> 5;
-        for (int w = 0; w < nw; ++w) st.word32(b + 32 * w, x);
-        for (int i = nw * 32; i < valid; ++i) st.step(b[i], x);
-        __syncthreads();
-        if (threadIdx.x == 0 && c + kNbuf < nch) {
-            fence_proxy_async();
-            ring_issue(r, base + c + kNbuf, s + (size_t)(c + kNbuf) * kChunk);
-        }
-    }
-    r.loads = base + nch;
-    return st.cnt;
-}
-
-// Same sweep; warps with deriv set also carry d/dx of the recurrence and
-// return the Newton ratio p_{n-1} / p'_{n-1} = det(S - x) / (d/dx det(S - x)).
-__device__ int cta_sturm_sweep_newton(const double* __restrict__ s, int nz, double x, bool deriv, Ring& r,
-                                      unsigned* err, double& ratio) {
-    const int nch = (nz + kChunk - 1) / kChunk;
-    const unsigned base = r.loads;
-    if (threadIdx.x == 0) {
-        for (int c = 0; c < nch && c < kNbuf; ++c) ring_issue(r, base + c, s + (size_t)c * kChunk);
-    }
-    SturmState st;
-    st.reset();
-    double d0 = 0.0, d1 = 0.0;  // derivatives of p_{-2}, p_{-1}
-    for (int c = 0; c < nch; ++c) {
-        const unsigned k = base + c;
-        const int slot = k % kNbuf;
-        mbar_wait_bounded(&r.bars[slot], (k / kNbuf) & 1u, err);
-        const double* b = r.buf + slot * kChunk;
-        const int valid = min(kChunk, nz - c * kChunk);
-        const int nw = valid >> 5;
-        if (deriv) {
-            for (int w = 0; w < nw; ++w) st.word32_deriv(b + 32 * w, x, d0, d1);
-            for (int i = nw * 32; i < valid; ++i) st.step_deriv(b[i], x, d0, d1);
-        } else {
-            for (int w = 0; w < nw; ++w) st.word32(b + 32 * w, x);
-            for (int i = nw * 32; i < valid; ++i) st.step(b[i], x);
+        for (int w = 0; w < nw; ++w) sturm_word32_pair(A, B, b + 32 * w, x0, x1);
+        for (int i = nw * 32; i < valid; ++i) {
+            A.step(b[i], x0);
+            B.step(b[i], x1);
         }
         __syncthreads();
         if (threadIdx.x == 0 && c + kNbuf < nch) {
@@ -494,8 +465,8 @@ __device__ int cta_sturm_sweep_newton(const double* __restrict__ s, int nz, doub
         }
     }
     r.loads = base + nch;
-    ratio = deriv ? st.p1 / d1 : 0.0;
-    return st.cnt;
+    c0 = A.cnt;
+    c1 = B.cnt;
 }
 
 __device__ __forceinline__ void ring_init(Ring& r, double* buf, uint64_t* bars) {
@@ -515,8 +486,10 @@ __device__ __forceinline__ double scan_x(double lo, double hi, int t) {
     return lo + (hi - lo) * ((double)t / (double)(kScanPoints - 1));
 }
 
-// K3a: kScanPoints counts per problem on an even grid of [lo, hi]
-__global__ void __launch_bounds__(kScanPoints) k_scan(const ProblemInfo* __restrict__ pinfo,
+// K3a: kScanPoints counts per problem on an even grid of [lo, hi]; thread t
+// sweeps shifts t and t + kScanPoints / 2
+constexpr int kScanThreads = kScanPoints / 2;
+__global__ void __launch_bounds__(kScanThreads) k_scan(const ProblemInfo* __restrict__ pinfo,
                                                       const double* __restrict__ s, int* __restrict__ counts,
                                                       unsigned* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -526,14 +499,16 @@ __global__ void __launch_bounds__(kScanPoints) k_scan(const ProblemInfo* __restr
     ring_init(r, buf, bars);
     const int p = blockIdx.x;
     const double lo = pinfo[p].lo, hi = pinfo[p].hi;
-    const double x = scan_x(lo, hi, threadIdx.x);
-    int c = cta_sturm_sweep(s + pinfo[p].s_off, pinfo[p].nz, x, r, err);
-    counts[(size_t)p * kScanPoints + threadIdx.x] = c;
+    const int t0 = threadIdx.x, t1 = threadIdx.x + kScanThreads;
+    int c0, c1;
+    cta_sturm_sweep_pair(s + pinfo[p].s_off, pinfo[p].nz, scan_x(lo, hi, t0), scan_x(lo, hi, t1), r, err, c0, c1);
+    counts[(size_t)p * kScanPoints + t0] = c0;
+    counts[(size_t)p * kScanPoints + t1] = c1;
 }
 
 int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* s, int* counts, unsigned* err) {
     size_t sm = kNbuf * kChunk * 8 + kNbuf * 8;
-    k_scan<<<P, kScanPoints, sm, st>>>(pinfo, s, counts, err);
+    k_scan<<<P, kScanThreads, sm, st>>>(pinfo, s, counts, err);
     return 1;
 }
 
@@ -1373,22 +1348,29 @@ int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a) {
 }
 
 // ===========================================================================
-// K5: 1-D transmission loss, one thread per range, modes staged in shared
-// memory.  Phase k r is formed and reduced in FP64.
+// K5: 1-D transmission loss, modes staged in shared memory.  Each thread
+// covers kTlRun consecutive ranges: per mode the phase k r of its first range
+// is formed in FP64 (sincos, exp), the next ones follow by the per-mode step
+// e^{(i k_r - k_i) dr} (a few ulps after kTlRun - 1 complex products).
 // ===========================================================================
 constexpr int kTlTile = 128;
+constexpr int kTlRun = 4;      // consecutive ranges per thread
+constexpr int kTlThreads = 256;
 
-__global__ void __launch_bounds__(256) k_tl1d(const ProblemInfo* __restrict__ pinfo, const double* __restrict__ kr,
-                                              const double* __restrict__ ki, const double* __restrict__ vs,
-                                              const double* __restrict__ vr, int nr, double dr, int lossless,
-                                              double* __restrict__ re, double* __restrict__ im,
-                                              double* __restrict__ incoh) {
+__global__ void __launch_bounds__(kTlThreads) k_tl1d(const ProblemInfo* __restrict__ pinfo,
+                                                     const double* __restrict__ kr, const double* __restrict__ ki,
+                                                     const double* __restrict__ vs, const double* __restrict__ vr,
+                                                     int nr, double dr, int lossless, double* __restrict__ re,
+                                                     double* __restrict__ im, double* __restrict__ incoh) {
     const int p = blockIdx.y;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = (blockIdx.x * kTlThreads + threadIdx.x) * kTlRun;  // first range of this thread
     const ProblemInfo pi = pinfo[p];
     __shared__ double m_kr[kTlTile], m_ki[kTlTile], m_vv[kTlTile], m_sr[kTlTile], m_si[kTlTile], m_ia[kTlTile];
-    const double r = (i + 1) * dr;
-    double sre = 0.0, sim = 0.0, sinc = 0.0;
+    __shared__ double m_wr[kTlTile], m_wi[kTlTile];
+    const double r0 = (i0 + 1) * dr;
+    double sre[kTlRun], sim[kTlRun], sinc[kTlRun];
+#pragma unroll
+    for (int j = 0; j < kTlRun; ++j) sre[j] = sim[j] = sinc[j] = 0.0;
     for (int m0 = 0; m0 < pi.M; m0 += kTlTile) {
         __syncthreads();
         for (int t = threadIdx.x; t < kTlTile && m0 + t < pi.M; t += blockDim.x) {
@@ -1403,39 +1385,57 @@ __global__ void __launch_bounds__(256) k_tl1d(const ProblemInfo* __restrict__ pi
             m_sr[t] = sk.real() / den;
             m_si[t] = -sk.imag() / den;
             m_ia[t] = lossless ? 1.0 / a : 1.0 / hypot(a, b);
+            double sn, cs;
+            sincos(a * dr, &sn, &cs);
+            const double w = exp(-b * dr);
+            m_wr[t] = w * cs;
+            m_wi[t] = w * sn;
         }
         __syncthreads();
         const int mt = min(kTlTile, pi.M - m0);
-        if (i < nr) {
+        if (i0 < nr) {
             for (int t = 0; t < mt; ++t) {
                 double sn, cs;
-                sincos(m_kr[t] * r, &sn, &cs);
-                const double amp = exp(-m_ki[t] * r);
-                const double vv = m_vv[t];
-                const double er = vv * amp * cs, ei = vv * amp * sn;
-                sre += er * m_sr[t] - ei * m_si[t];
-                sim += er * m_si[t] + ei * m_sr[t];
-                sinc += (vv * vv) * (amp * amp) * m_ia[t];
+                sincos(m_kr[t] * r0, &sn, &cs);
+                const double amp = exp(-m_ki[t] * r0);
+                const double vv = m_vv[t], sr = m_sr[t], si = m_si[t], ia = m_ia[t];
+                const double wr = m_wr[t], wi = m_wi[t];
+                double er = amp * cs, ei = amp * sn;  // e^{i k r} at the current range
+#pragma unroll
+                for (int j = 0; j < kTlRun; ++j) {
+                    const double ar = vv * er, ai = vv * ei;
+                    sre[j] += ar * sr - ai * si;
+                    sim[j] += ar * si + ai * sr;
+                    sinc[j] += (vv * vv) * (er * er + ei * ei) * ia;
+                    const double nr_ = er * wr - ei * wi;
+                    ei = er * wi + ei * wr;
+                    er = nr_;
+                }
             }
         }
     }
-    if (i < nr) {
-        // 1000 * 4 pi i e^{-i pi/4} / sqrt(8 pi) / sqrt(r)
+    // 1000 * 4 pi i e^{-i pi/4} / sqrt(8 pi) / sqrt(r)
+    const double ang = kPi * 0.25;
+#pragma unroll
+    for (int j = 0; j < kTlRun; ++j) {
+        const int i = i0 + j;
+        if (i >= nr) break;
+        const double r = (i + 1) * dr;
         const double c0 = 1000.0 * 4 * kPi / sqrt(8.0 * kPi) / sqrt(r);
-        const double ang = kPi * 0.25;
         const double fr = c0 * sin(ang), fi = c0 * cos(ang);
         const size_t o = (size_t)p * nr + i;
-        re[o] = fr * sre - fi * sim;
-        im[o] = fr * sim + fi * sre;
-        incoh[o] = 1000.0 * 4 * kPi * sqrt(sinc) * sqrt(1. / 8. / kPi / r);
+        re[o] = fr * sre[j] - fi * sim[j];
+        im[o] = fr * sim[j] + fi * sre[j];
+        incoh[o] = 1000.0 * 4 * kPi * sqrt(sinc[j]) * sqrt(1. / 8. / kPi / r);
     }
 }
 
 int launch_tl1d(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* kr, const double* ki,
                 const double* vs, const double* vr, int nr, double dr, int lossless, double* re, double* im,
                 double* incoh) {
-    dim3 grid((nr + 255) / 256, P);
-    k_tl1d<<<grid, 256, 0, st>>>(pinfo, kr, ki, vs, vr, nr, dr, lossless, re, im, incoh);
+    const int per_block = kTlThreads * kTlRun;
+    dim3 grid((nr + per_block - 1) / per_block, P);
+    k_tl1d<<<grid, kTlThreads, 0, st>>>(pinfo, kr, ki, vs, vr, nr, dr, lossless, re, im, incoh);
     return 1;
 }
 
