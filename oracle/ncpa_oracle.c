@@ -247,6 +247,16 @@ void orc_ceff_knots(int n, const double *c0, const double *ws, const double *wd_
     }
 }
 
+/* wind component along the azimuth at the knots, the wc term of
+ * orc_ceff_knots (Atmosphere1D::calculate_wind_component) */
+void orc_wc_knots(int n, const double *ws, const double *wd_deg, double az_deg, double *wc) {
+    double az_rad = az_deg * ORC_PI / 180.0;
+    for (int i = 0; i < n; i++) {
+        double dir = wd_deg[i] * ORC_PI / 180.0;
+        wc[i] = ws[i] * cos(dir - az_rad);
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* getModalTrace (ESSModeSolver.cpp:518-621) and the scaled matrix            */
 /* ------------------------------------------------------------------------ */
@@ -575,6 +585,105 @@ int orc_solve_modes(int n, const double *s, double h2, double dz, double k_min, 
         }
     }
     free(mu);
+    return M;
+}
+
+/* ------------------------------------------------------------------------ */
+/* WMod: wide-angle modes (WModeSolver.cpp:257-629, EigenEngine.cpp:174-395)  */
+/* ------------------------------------------------------------------------ */
+/* The reference solves (M k^2 + C k + D) v = 0 (M = diag(md), C = diag(cd),
+ * D tridiagonal with diagonal kd - 2/h^2 and off-diagonal 1/h^2) through the
+ * linearised 2N pencil with SLEPc.  Here T(k) h^2 = diag(a2 k^2 + a1 k + a0)
+ * with unit off-diagonal, a2 = md h^2, a1 = cd h^2, a0 = kd h^2 - 2, where
+ *   kd = (omega/c0)^2 (+ the ground term (1/(dz adm + 1))/dz^2 in row 0),
+ *   md = (wc/c0)^2 - 1,  cd = -2 omega wc / c0^2     (WModeSolver.cpp:544-565)
+ * and no last-row repeat (EigenEngine.cpp:266-275).  For real k, dT/dk =
+ * 2 M k + C is negative definite while |wc| is below c0 and k inside the
+ * propagating window, so the number of negative eigenvalues of T(k) grows by
+ * one at each real eigenvalue: Sturm counts in k locate them exactly. */
+void orc_wmod_coeffs(int n, const double *c0g, const double *wcg, double omega, double dz, double admittance,
+                     double *a2, double *a1, double *a0) {
+    double h2 = dz * dz;
+    double bnd = (1. / (dz * admittance + 1)) / (dz * dz);
+    for (int i = 0; i < n; i++) {
+        double t = omega / c0g[i];
+        double kd = t * t;
+        double u = wcg[i] / c0g[i];
+        double md = u * u - 1;
+        double cd = -2 * omega * (wcg[i] / (c0g[i] * c0g[i]));
+        if (i == 0) kd = bnd + kd;
+        a2[i] = md * h2;
+        a1[i] = cd * h2;
+        a0[i] = kd * h2 - 2.0;
+    }
+}
+
+static inline double wmod_diag(const double *a2, const double *a1, const double *a0, int i, double k) {
+    return fma(fma(a2[i], k, a1[i]), k, a0[i]);
+}
+
+/* number of negative eigenvalues of T(k) (sign changes of the division-free
+ * recurrence, as orc_sturm_count) */
+int orc_wmod_count(int n, const double *a2, const double *a1, const double *a0, double k) {
+    double pm = 1.0, p = wmod_diag(a2, a1, a0, 0, k);
+    int cnt = signbit(p) ? 1 : 0;
+    for (int i = 1; i < n; i++) {
+        double pn = fma(wmod_diag(a2, a1, a0, i, k), p, -pm);
+        cnt += (signbit(pn) != 0) != (signbit(p) != 0);
+        pm = p;
+        p = pn;
+        if ((i & 15) == 0) {
+            int sh = rescale_shift(pm, p);
+            if (sh) {
+                pm = ldexp(pm, -sh);
+                p = ldexp(p, -sh);
+            }
+        }
+    }
+    return cnt;
+}
+
+/* wide-angle modes of one problem in [k_min, k_max]: bisection in k to the
+ * relative tolerance tol, eigenvector of T(k) by twisted factorisation, the
+ * normalisation of SLEPc's unit-2-norm eigenvectors of the pencil [v; k v]
+ * (sum v^2 dz = 1/(1+k^2), v = x/sqrt(dz), EigenEngine.cpp:368-379) and the
+ * perturbative attenuation of ModeSolver::doPerturb (ModeSolver.cpp:263-284).
+ * Returns M, or -1 above max_modes. */
+int orc_wmod_solve(int n, const double *a2, const double *a1, const double *a0, double dz, double k_min,
+                   double k_max, const double *w, int isrc, int ircv, double tol, int max_modes, double *kr,
+                   double *ki, double *vs, double *vr, double *vfull) {
+    int c_lo = orc_wmod_count(n, a2, a1, a0, k_min);
+    int c_hi = orc_wmod_count(n, a2, a1, a0, k_max);
+    int M = c_hi - c_lo;
+    if (M < 0) M = 0;
+    if (M > max_modes) return -1;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int e = 0; e < M; e++) {
+        int j = c_lo + e;
+        double a = k_min, b = k_max;
+        while (b - a > tol * b) {
+            double mid = 0.5 * (a + b);
+            if (mid <= a || mid >= b) break;
+            if (orc_wmod_count(n, a2, a1, a0, mid) > j) b = mid; else a = mid;
+        }
+        double k = 0.5 * (a + b);
+        double *t = (double *)malloc(sizeof(double) * (size_t)n);
+        double *vcol = vfull ? (double *)malloc(sizeof(double) * (size_t)n) : NULL;
+        for (int i = 0; i < n; i++) t[i] = wmod_diag(a2, a1, a0, i, k);
+        double o[5];
+        orc_eigvec(n, t, 0.0, dz, w, NULL, isrc, ircv, o, vcol);
+        double f = 1.0 / sqrt(1.0 + k * k);
+        double complex kp = csqrt_p(k * k + I * (o[2] * f * f));
+        kr[e] = creal(kp);
+        ki[e] = cimag(kp);
+        vs[e] = o[0] * f;
+        vr[e] = o[1] * f;
+        if (vfull) {
+            for (int i = 0; i < n; i++) vfull[(size_t)i * M + e] = vcol[i] * f;
+            free(vcol);
+        }
+        free(t);
+    }
     return M;
 }
 

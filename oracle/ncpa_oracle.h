@@ -36,6 +36,7 @@ double orc_attn_sutherland_bass(double z_km, double T, double P, double D, doubl
 void orc_c0_from_p_rho(int n, const double *z, const double *p, const double *rho, double *c0);
 void orc_c0_from_t(int n, const double *z, const double *t, double *c0);
 void orc_wind_speed_dir(int n, const double *u, const double *v, double *ws, double *wd_deg);
+void orc_wc_knots(int n, const double *ws, const double *wd_deg, double az_deg, double *wc);
 void orc_ceff_knots(int n, const double *c0, const double *ws, const double *wd_deg,
                     double az_deg, double *ceff);
 
@@ -88,6 +89,18 @@ int orc_solve_modes(int n, const double *s, double h2, double dz, double k_min, 
                     double omega, const double *w, const double *g, int isrc, int ircv,
                     double tol, int max_modes, double *kr, double *ki, double *vs, double *vr,
                     double *vg, double *vfull /* optional n*max_modes, [i*M + m] */);
+
+/* ---- WMod (WModeSolver.cpp:257-629, EigenEngine.cpp:174-395) ---------------- */
+/* h^2-scaled coefficients of T(k) = M k^2 + C k + D from c0 and the wind
+ * component on the grid; row 0 carries the ground term */
+void orc_wmod_coeffs(int n, const double *c0g, const double *wcg, double omega, double dz,
+                     double admittance, double *a2, double *a1, double *a0);
+int  orc_wmod_count(int n, const double *a2, const double *a1, const double *a0, double k);
+/* modes in [k_min, k_max] (k relative tolerance tol); outputs as orc_solve_modes
+ * without group speeds; vfull optional [i*M + m].  Returns M or -1. */
+int  orc_wmod_solve(int n, const double *a2, const double *a1, const double *a0, double dz,
+                    double k_min, double k_max, const double *w, int isrc, int ircv, double tol,
+                    int max_modes, double *kr, double *ki, double *vs, double *vr, double *vfull);
 
 /* ---- modal sums (ModeSolver.cpp:292-565) ------------------------------------ */
 void orc_tl1d(int M, const double *kr, const double *ki, const double *vs, const double *vr,

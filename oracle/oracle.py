@@ -64,6 +64,13 @@ def lib():
         L.orc_solve_modes.argtypes = [c_int, dp, c_double, c_double, c_double, c_double, c_double,
                                       dp, dp, c_int, c_int, c_double, c_int, dp, dp, dp, dp, dp, dp]
         L.orc_solve_modes.restype = c_int
+        L.orc_wc_knots.argtypes = [c_int, dp, dp, c_double, dp]
+        L.orc_wmod_coeffs.argtypes = [c_int, dp, dp, c_double, c_double, c_double, dp, dp, dp]
+        L.orc_wmod_count.argtypes = [c_int, dp, dp, dp, c_double]
+        L.orc_wmod_count.restype = c_int
+        L.orc_wmod_solve.argtypes = [c_int, dp, dp, dp, c_double, c_double, c_double, dp, c_int, c_int, c_double,
+                                     c_int, dp, dp, dp, dp, dp]
+        L.orc_wmod_solve.restype = c_int
         L.orc_tl1d.argtypes = [c_int, dp, dp, dp, dp, c_int, c_double, c_int, dp, dp, dp]
         L.orc_tl2d.argtypes = [c_int, dp, dp, dp, dp, c_int, c_int, c_double, c_int, dp, dp]
         L.orc_bb_transfer.argtypes = [c_int, ip, dp, dp, dp, dp, c_double, c_double, c_double, dp, dp]
@@ -465,6 +472,57 @@ def solve_problem(pp: Prepared, prm: EssParams, freq: float, az: float, want_gro
         mu = np.empty(max(M, 1))
         L.orc_bisect(nz, _p(s), lo, hi, lo_c, M, BISECT_TOL, _p(mu))
         ms.mu = mu[:M]
+    if want_full:
+        ms.vfull = vfull[: nz * M].reshape(nz, M)
+    return ms
+
+
+WMOD_TOL = 1.0e-14  # relative bracket width in k
+
+
+def solve_problem_wmod(pp: Prepared, prm: EssParams, freq: float, az: float, want_full=False,
+                       max_modes=1 << 20) -> ModeSet:
+    """One wide-angle (WMod) problem: WModeSolver::solve's grid (matrix
+    spacing (maxheight - z_min) / Nz_grid, WModeSolver.cpp:281; sampling as
+    setParams, :146-208), window of getModalTrace (:514-629: the ESS window
+    on c_eff), the quadratic eigenproblem in k (EigenEngine.cpp:174-395) and
+    doPerturb (ModeSolver.cpp:263-284)."""
+    L = lib()
+    nz = prm.Nz_grid
+    dz = (pp.maxheight - pp.z_min) / nz
+    ceffk, wck = np.empty_like(pp.zk), np.empty_like(pp.zk)
+    L.orc_ceff_knots(len(pp.zk), _p(pp.c0), _p(pp.ws), _p(pp.wd), float(az), _p(ceffk))
+    L.orc_wc_knots(len(pp.zk), _p(pp.ws), _p(pp.wd), float(az), _p(wck))
+    sp = Spline(pp.zk, ceffk)
+    gp = _GridParams(nz, pp.z_min, pp.dz_grid, dz, freq, pp.admittance, prm.sourceheight_km * 1000.0,
+                     prm.receiverheight_km * 1000.0, int(prm.turnoff_WKB or prm.forces_no_wkb),
+                     int(prm.wvnum_filter), prm.c_min, prm.c_max)
+    hgt, ceff, diag, s = (np.empty(nz) for _ in range(4))
+    res = _GridResult()
+    L.orc_build_grid(ctypes.byref(gp), len(pp.zk), _p(pp.zk), _p(ceffk), _p(sp.coef), _p(hgt), _p(ceff),
+                     _p(diag), _p(s), ctypes.byref(res))
+    omega = 2 * PI * freq
+    c0g = _f64(Spline(pp.zk, pp.c0)(pp.hgt))
+    wcg = _f64(Spline(pp.zk, wck)(pp.hgt))
+    a2, a1, a0 = (np.empty(nz) for _ in range(3))
+    L.orc_wmod_coeffs(nz, _p(c0g), _p(wcg), omega, dz, pp.admittance, _p(a2), _p(a1), _p(a0))
+    alpha = Spline(pp.zk, alpha_knots(pp, freq))(pp.hgt)
+    cT = np.sqrt(1.4 * pp.p_g / pp.rho_g)
+    w = _f64(((omega / cT) * alpha) * 2)
+    isrc = int(math.ceil(prm.sourceheight_km * 1000.0 / dz))
+    ircv = int(math.ceil(prm.receiverheight_km * 1000.0 / dz))
+    cap = min(max_modes, max(0, L.orc_wmod_count(nz, _p(a2), _p(a1), _p(a0), res.k_max)
+                             - L.orc_wmod_count(nz, _p(a2), _p(a1), _p(a0), res.k_min)))
+    kr, ki, vs, vr = (np.zeros(max(cap, 1)) for _ in range(4))
+    vfull = np.zeros(nz * max(cap, 1)) if want_full else None
+    M = L.orc_wmod_solve(nz, _p(a2), _p(a1), _p(a0), dz, res.k_min, res.k_max, _p(w), isrc, ircv, WMOD_TOL, cap,
+                         _p(kr), _p(ki), _p(vs), _p(vr), _p(vfull) if vfull is not None else None)
+    if M < 0:
+        raise RuntimeError("too many modes")
+    ms = ModeSet(freq=freq, az=az, M=M, kr=kr[:M], ki=ki[:M], vs=vs[:M], vr=vr[:M], vg=None, k_min=res.k_min,
+                 k_max=res.k_max, rho_s=float(pp.rho_g[isrc]), rho_r=float(pp.rho_g[ircv]), dz=dz, isrc=isrc,
+                 ircv=ircv)
+    ms.coeffs = (a2, a1, a0)
     if want_full:
         ms.vfull = vfull[: nz * M].reshape(nz, M)
     return ms

@@ -9,6 +9,9 @@ where the reference checkout is available) and writes compact copies:
   modess_tloss_1d.npz        docs/.../modess_gp_files/code_outputs/tloss_1d.nm
                              and tloss_1d.lossless.nm (Modess, 0.1 Hz, az 90,
                              pre-2.0.1 TL scaling: +60 dB vs the current code)
+  wmod_tloss_1d.npz          docs/.../wmod_gp_files/code_outputs/wtloss_1d.nm and
+                             wtloss_1d.lossless.nm (WMod, 0.1 Hz, az 90, with
+                             --write_2d_tloss, pre-2.0.1 TL scaling)
   dispersion_goldens.npz     per-frequency mode counts, plus Re k / Im k /
                              V_s V_r at a few frequencies, of
                              samples/disp_256freqs_0p5hz_NCPA_canonic.dat and
@@ -49,6 +52,9 @@ def main():
     lossy = np.loadtxt(os.path.join(co, "tloss_1d.nm"))
     lossless = np.loadtxt(os.path.join(co, "tloss_1d.lossless.nm"))
     np.savez_compressed(os.path.join(OUT, "modess_tloss_1d.npz"), lossy=lossy, lossless=lossless)
+    wo = os.path.join(REF, "docs", "ncpaprop_run_manual_TeX", "figs", "wmod_gp_files", "code_outputs")
+    np.savez_compressed(os.path.join(OUT, "wmod_tloss_1d.npz"), lossy=np.loadtxt(os.path.join(wo, "wtloss_1d.nm")),
+                        lossless=np.loadtxt(os.path.join(wo, "wtloss_1d.lossless.nm")))
     sets = {
         "s256": os.path.join(REF, "samples", "disp_256freqs_0p5hz_NCPA_canonic.dat"),
         "manual": os.path.join(REF, "docs", "ncpaprop_run_manual_TeX", "figs", "modbb_gp_files", "code_outputs",
