@@ -115,7 +115,17 @@ typedef struct {
     int max_modes;            /* per problem; 0 -> 4000 (reference MAX_MODES) */
     int keep_on_device;       /* leave mode arrays in HBM only (ncpa_modes_get
                                  then fetches them on demand) */
+    int method;               /* NCPA_METHOD_ESS (Modess) or NCPA_METHOD_WMOD */
 } ncpa_ess_params;
+
+/* NCPA_METHOD_WMOD: the wide-angle modes of WModeSolver (ModBB --method wmod,
+ * WModeSolver.cpp:257-629): the quadratic eigenproblem
+ * (M k^2 + C k + D) v = 0 with M = (w/c0)^2 - 1, C = -2 omega w / c0^2 (w the
+ * wind component along the azimuth), D the finite-difference operator with
+ * (omega/c0)^2, solved in k by Sturm counts of T(k) = M k^2 + C k + D, plus
+ * the reference's matrix spacing (maxheight - z_min) / Nz_grid.  Available
+ * through ncpa_ess_solve (not through jobs or plans); group speeds are 0. */
+enum { NCPA_METHOD_ESS = 0, NCPA_METHOD_WMOD = 1 };
 
 void ncpa_ess_params_default(ncpa_ess_params *p);
 

@@ -2,7 +2,10 @@
 // handling of ESSModeSolver::setParams (ESSModeSolver.cpp:30-240) and the
 // per-(frequency, azimuth) outputs of ESSModeSolver::solve
 // (ESSModeSolver.cpp:291-510), with every problem of a frequency batch solved
-// in one ncpa_ess_solve call on the GPU.
+// in one ncpa_ess_solve call on the GPU.  ModBB --method wmod runs the same
+// loop with the wide-angle solve (WModeSolver::setParams / solve,
+// WModeSolver.cpp:30-120, 257-486: the same options and outputs, without
+// group speeds).
 #include <cmath>
 #include <cstdio>
 #include <iostream>
@@ -28,13 +31,14 @@ struct ProfileHandle {
 };
 }  // namespace
 
-void run_ess(const Params& prm) {
+void run_ess(const Params& prm, bool wmod) {
     const std::string tag = prm.get_string("filetag");
     const std::string gnd = prm.get_string("ground_impedence_model");
     if (gnd != "rigid") throw RunError("This ground impedance model is not implemented yet: " + gnd);
 
     ncpa_ess_params ep;
     ncpa_ess_params_default(&ep);
+    ep.method = wmod ? NCPA_METHOD_WMOD : NCPA_METHOD_ESS;
     ep.nz_grid = prm.get_int("Nz_grid");
     ep.maxheight_km = prm.get_float("maxheight_km");
     ep.zground_km = prm.get_float("zground_km");
@@ -44,7 +48,7 @@ void run_ess(const Params& prm) {
     const bool write_2d = prm.get_bool("write_2d_tloss");
     const bool write_lossless = prm.get_bool("write_lossless");
     const bool write_phase = prm.get_bool("write_phase_speeds");
-    const bool want_speeds = prm.get_bool("write_speeds");
+    const bool want_speeds = !wmod && prm.get_bool("write_speeds");
     const bool write_modes = prm.get_bool("write_modes");
     const bool write_atm = prm.get_bool("write_atm_profile");
     const bool multiprop = prm.get_bool("multiprop");
@@ -52,7 +56,8 @@ void run_ess(const Params& prm) {
     const bool append_disp = prm.get_bool("append_dispersion_file");
     const std::string starter_file = prm.get_string("modal_starter_file");
     ep.turnoff_wkb = prm.get_bool("turnoff_WKB");
-    // ESSModeSolver.cpp:78-81: any of these outputs turns the WKB estimate off
+    // ESSModeSolver.cpp:78-81 (WModeSolver.cpp:75-77): any of these outputs
+    // turns the WKB estimate off
     if (write_phase || want_speeds || write_2d || write_modes || !disp_file.empty()) ep.turnoff_wkb = 1;
     ep.wvnum_filter = prm.get_bool("wvnum_filter");
     if (ep.wvnum_filter) {
@@ -60,7 +65,7 @@ void run_ess(const Params& prm) {
         ep.c_max = prm.get_float("c_max");
     }
     const bool single = !multiprop;
-    ep.want_group_speed = single && (want_speeds || write_modes);
+    ep.want_group_speed = !wmod && single && (want_speeds || write_modes);
     ep.want_vectors = single && (write_modes || write_2d || !starter_file.empty());
 
     // azimuths (ESSModeSolver.cpp:83-95)
@@ -107,7 +112,8 @@ void run_ess(const Params& prm) {
     for (size_t f0 = 0; f0 < freqs.size(); f0 += per_batch) {
         const int nf = (int)std::min<size_t>(per_batch, freqs.size() - f0);
         ModesHandle mh;
-        check(ctx, ncpa_ess_solve(ctx, prof.p, &ep, &freqs[f0], nf, az.data(), na, &mh.m), "ESS mode solve");
+        check(ctx, ncpa_ess_solve(ctx, prof.p, &ep, &freqs[f0], nf, az.data(), na, &mh.m),
+              wmod ? "wide-angle mode solve" : "ESS mode solve");
         const int P = nf * na;
         ncpa_tl_params tp{nr, dr, 0};
         std::vector<double> re((size_t)P * nr), im((size_t)P * nr), inc((size_t)P * nr);
@@ -165,7 +171,7 @@ void run_ess(const Params& prm) {
                     if (m.M) check(ctx, ncpa_modes_get_vectors(mh.m, p, v.data()), "eigenvectors");
                     write_mode_files(tag, ep.nz_grid, m.dz, m.M, v);
                 }
-                if (write_modes || want_speeds) write_speeds(tag_filename(tag, "speeds.nm"), m);
+                if (!wmod && (write_modes || want_speeds)) write_speeds(tag_filename(tag, "speeds.nm"), m);
                 if (!disp_file.empty()) {
                     std::printf("Writing to file %s: dispersion at freq = %8.3f Hz...\n", disp_file.c_str(), m.freq);
                     std::FILE* df = std::fopen(disp_file.c_str(), append_disp ? "a" : "w");

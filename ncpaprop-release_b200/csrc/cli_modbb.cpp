@@ -137,13 +137,15 @@ int main(int argc, char** argv) {
     const std::time_t t1 = std::time(nullptr);
     try {
         if (param.get_bool("dispersion")) {
-            if (param.get_string("method") != "modess")
-                throw RunError("--method " + param.get_string("method") +
-                               ": only the effective sound speed solver (modess) is provided");
             const std::string disp = param.get_string("dispersion_file");
             if (!disp.empty()) std::ofstream(disp, std::ios_base::trunc).close();
-            ncpa_gpu_solvers::ESSModeSolver solver(&param);  // as ModBB_main.cpp:84-91
-            solver.solve();
+            if (param.get_string("method") == "modess") {  // as ModBB_main.cpp:84-91
+                ncpa_gpu_solvers::ESSModeSolver solver(&param);
+                solver.solve();
+            } else {
+                ncpa_gpu_solvers::WModeSolver solver(&param);
+                solver.solve();
+            }
             std::cout << "Finished computing and saving dispersion data" << std::endl;
         } else if (param.get_bool("propagation")) {
             ncpa_gpu_solvers::ModalBroadbandPropagator prop(&param);  // as ModBB_main.cpp:108-110

@@ -149,6 +149,38 @@ int launch_bb_pulse(cudaStream_t st, int nfreq, const double* f, const double* s
 int launch_src_dft(cudaStream_t st, int n, const double* x, double dt, int nfft, int nfreq, const double* tw,
                    double* s);
 
+// Wide-angle (WMod) modes (wmod.cu).  Coefficient rows a2, a1, a0 of
+// T(k) h^2 = diag(a2 k^2 + a1 k + a0) + offdiag(1) use the s layout
+// (pinfo[p].s_off); pinfo k_min / k_max bound the window in k.
+int launch_wc_knots(cudaStream_t st, int n, int n_az, const double* az, const double* ws, const double* wd,
+                    double* wc);
+int launch_wmod_build(cudaStream_t st, int nk, const double* zk, const double* c0k, const double* c0c,
+                      const double* wck, const double* wcc, const double* ceffk, const double* ceffc, int n_az,
+                      int P, ProblemInfo* pinfo, int nz, int nz_pad, double z_min, double dz_grid, double dz,
+                      double admittance, double* a2, double* a1, double* a0, double* kz2);
+int launch_wscan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* a2, const double* a1,
+                 const double* a0, int* counts);
+// mu receives k (not k^2 h^2); tol is relative to k
+int launch_wbisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* a2, const double* a1,
+                   const double* a0, const int* counts, const WorkItem* items, const int* n_items_dev, double tol,
+                   double* mu);
+struct WmodEvArgs {
+    const ProblemInfo* pinfo;
+    const double *a2, *a1, *a0;
+    const double* w;              // attenuation weights, rows at pinfo[p].w_off
+    const WorkItem* items;
+    const int* n_items_dev;
+    const double* mu;             // k per mode
+    double *kr, *ki, *vs, *vr, *vg;
+    double* vfull;                // optional: per problem [nz x M] at vfull_off[p]
+    const long long* vfull_off;
+    double* q_scr;                // per warp slot: (nz_max + 1) rows x 32 lanes
+    int* e_scr;
+    long long slot_stride;        // elements per warp slot
+};
+int launch_weigvec(cudaStream_t st, int grid, const WmodEvArgs& a);
+int wmod_warps_per_cta();
+
 // K5 modal sum on the tensor cores (modal_sum.cu)
 struct MsPlan {
     int groups, n_chunks, M_pad, n_tiles, n_ctas, n_parts;

@@ -286,6 +286,8 @@ struct Geometry {
 
 void check_ess_params(const ncpa_ess_params* prm) {
     if (prm->nz_grid < 10) throw ApiError(NCPA_EINVAL, "Nz_grid must be >= 10");
+    if (prm->method != NCPA_METHOD_ESS && prm->method != NCPA_METHOD_WMOD)
+        throw ApiError(NCPA_EINVAL, "unknown method");
     if (prm->wvnum_filter && !(prm->c_min > 0.0 && prm->c_max > 0.0))
         throw ApiError(NCPA_EINVAL, "wvnum_filter needs c_min > 0 and c_max > 0");
 }
@@ -806,6 +808,208 @@ void solve_groups(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std:
         const Group& g = groups[gi];
         const int np = g.n_freq * g.n_az;
         for (int k = 0; k < np; ++k) {
+            M->rho_src_p[g.p0 + k] = rho_pairs[2 * gi];
+            M->rho_rcv_p[g.p0 + k] = rho_pairs[2 * gi + 1];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// WMod (wide-angle) solve: WModeSolver::solve (WModeSolver.cpp:257-486)
+// ---------------------------------------------------------------------------
+constexpr double kWmodTol = 1.0e-15;  // relative to k
+constexpr size_t kWmodScratchBytes = size_t(1) << 30;  // eigenvector q scratch bound
+
+// the matrix spacing of WModeSolver::solve, (maxheight - z_min) / Nz_grid
+// (WModeSolver.cpp:281; the sampling grid keeps setParams' spacing), and the
+// source / receiver rows on it
+void wmod_geometry(Group& g, const ncpa_ess_params* prm) {
+    double maxheight = prm->maxheight_km * 1000.0;
+    if (maxheight >= g.prof->z_hi) maxheight = g.prof->z_hi - 1e-6;
+    g.geo.dz = (maxheight - g.geo.z_min) / g.nz;
+    if (!(g.geo.dz > 0.0)) throw ApiError(NCPA_EINVAL, "maxheight must lie above the ground");
+    g.geo.isrc = (int)std::ceil(prm->sourceheight_km * 1000.0 / g.geo.dz);
+    g.geo.ircv = (int)std::ceil(prm->receiverheight_km * 1000.0 / g.geo.dz);
+    if (g.geo.isrc < 0 || g.geo.isrc >= g.nz || g.geo.ircv < 0 || g.geo.ircv >= g.nz)
+        throw ApiError(NCPA_EINVAL, "source/receiver height outside the grid");
+}
+
+struct WmodBufs {
+    GroupBufs gb;           // frequencies, azimuths, c_eff and alpha knots, grid fields
+    DevBuf wck, wcc, c0c;   // wind component knots and splines, c0 spline
+};
+
+// knot-level fields, attenuation weights and coefficient rows of one group
+void enqueue_wmod_group(ncpa_ctx* ctx, PhaseTimer& tm, const Group& g, WmodBufs& wb, bool wkb, ProblemInfo* d_pinfo,
+                        double* a2, double* a1, double* a0, double* w, double* kz2, double* rho_pair) {
+    cudaStream_t st = ctx->stream;
+    const ncpa_profile* prof = g.prof;
+    const int nk = prof->n;
+    GroupBufs& b = wb.gb;
+    check_launch(ctx, ncpa::launch_ceff_knots(st, nk, g.n_az, b.az.as<double>(), prof->c0.as<double>(),
+                                              prof->ws.as<double>(), prof->wd.as<double>(), b.ceffk.as<double>()));
+    check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), b.ceffk.as<double>(), g.n_az, nk,
+                                           b.ceffc.as<double>(), 4 * (nk - 1)));
+    check_launch(ctx, ncpa::launch_wc_knots(st, nk, g.n_az, b.az.as<double>(), prof->ws.as<double>(),
+                                            prof->wd.as<double>(), wb.wck.as<double>()));
+    check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), wb.wck.as<double>(), g.n_az, nk,
+                                           wb.wcc.as<double>(), 4 * (nk - 1)));
+    check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), prof->c0.as<double>(), 1, nk,
+                                           wb.c0c.as<double>(), 4 * (nk - 1)));
+    if (prof->has_attn) {
+        for (int f = 0; f < g.n_freq; ++f)
+            CK(cudaMemcpyAsync(b.alpha.as<double>() + (size_t)f * nk, prof->attn.p, nk * 8, cudaMemcpyDeviceToDevice,
+                               st));
+    } else {
+        check_launch(ctx, ncpa::launch_alpha_knots(st, nk, g.n_freq, b.freqs.as<double>(), prof->z.as<double>(),
+                                                   prof->t.as<double>(), prof->p.as<double>(),
+                                                   prof->rho.as<double>(), b.alpha.as<double>()));
+    }
+    check_launch(ctx, ncpa::launch_steffen(st, nk, prof->z.as<double>(), b.alpha.as<double>(), g.n_freq, nk,
+                                           b.alphac.as<double>(), 4 * (nk - 1)));
+    CK(cudaMemsetAsync(w, 0, (size_t)g.n_freq * g.nz_pad * 8, st));
+    check_launch(ctx, ncpa::launch_grid_common(st, nk, prof->z.as<double>(), prof->rho.as<double>(),
+                                               prof->rcoef.as<double>(), prof->p.as<double>(),
+                                               prof->pcoef.as<double>(), g.nz, g.geo.z_min, g.geo.dz_grid,
+                                               b.rho_g.as<double>(), b.ct_g.as<double>()));
+    check_launch(ctx, ncpa::launch_attn_weight(st, nk, prof->z.as<double>(), b.alpha.as<double>(),
+                                               b.alphac.as<double>(), g.n_freq, b.freqs.as<double>(), g.nz,
+                                               g.geo.z_min, g.geo.dz_grid, b.ct_g.as<double>(), w, g.nz_pad));
+    CK(cudaMemcpyAsync(rho_pair, b.rho_g.as<double>() + g.geo.isrc, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(rho_pair + 1, b.rho_g.as<double>() + g.geo.ircv, 8, cudaMemcpyDeviceToHost, st));
+    tm.mark("knots+grid");
+    check_launch(ctx, ncpa::launch_wmod_build(st, nk, prof->z.as<double>(), prof->c0.as<double>(),
+                                              wb.c0c.as<double>(), wb.wck.as<double>(), wb.wcc.as<double>(),
+                                              b.ceffk.as<double>(), b.ceffc.as<double>(), g.n_az,
+                                              g.n_freq * g.n_az, d_pinfo, g.nz, g.nz_pad, g.geo.z_min,
+                                              g.geo.dz_grid, g.geo.dz, b.admittance, a2, a1, a0,
+                                              wkb ? kz2 : nullptr));
+    tm.mark("matrix");
+}
+
+void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::vector<Group>& groups) {
+    cudaStream_t st = ctx->stream;
+    PhaseTimer tm(ctx);
+    tm.mark("start");
+    for (Group& g : groups) wmod_geometry(g, prm);
+    long long s_tot = 0, w_tot = 0;
+    layout_groups(M, groups, s_tot, w_tot);
+    upload(M->d_pinfo, M->info, st);
+    const bool wkb = wants_wkb(prm);
+    DevBuf a2, a1, a0, w, kz2;
+    for (DevBuf* b : {&a2, &a1, &a0}) b->alloc((size_t)s_tot * 8, st);
+    w.alloc((size_t)w_tot * 8, st);
+    if (wkb) kz2.alloc((size_t)s_tot * 8, st);
+    double* rho_pairs = pinned(ctx, 2 * groups.size());
+    ProblemInfo* d_pinfo = M->d_pinfo.as<ProblemInfo>();
+    std::vector<WmodBufs> wbs(groups.size());
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& g = groups[gi];
+        prepare_group(ctx, prm, g, wbs[gi].gb);
+        const int nk = g.prof->n;
+        wbs[gi].wck.alloc((size_t)g.n_az * nk * 8, st);
+        wbs[gi].wcc.alloc((size_t)g.n_az * 4 * (nk - 1) * 8, st);
+        wbs[gi].c0c.alloc((size_t)4 * (nk - 1) * 8, st);
+    }
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& g = groups[gi];
+        enqueue_wmod_group(ctx, tm, g, wbs[gi], wkb, d_pinfo + g.p0, a2.as<double>() + g.s_base,
+                           a1.as<double>() + g.s_base, a0.as<double>() + g.s_base, w.as<double>() + g.w_base,
+                           wkb ? kz2.as<double>() + g.s_base : nullptr, rho_pairs + 2 * gi);
+    }
+    const int P = M->P;
+    unsigned* err = ctx->d_err.as<unsigned>();
+    check_launch(ctx, ncpa::launch_window(st, P, d_pinfo, wkb ? kz2.as<double>() : nullptr, wkb ? 1 : 0,
+                                          prm->wvnum_filter, prm->c_min, prm->c_max, err));
+    tm.mark("window");
+    DevBuf counts, bis, ev, tot;
+    counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
+    check_launch(ctx, ncpa::launch_wscan(st, P, d_pinfo, a2.as<double>(), a1.as<double>(), a0.as<double>(),
+                                         counts.as<int>()));
+    tm.mark("scan");
+    const int cap_modes = M->prm.max_modes;
+    const int bis_cap = P * ((cap_modes + ncpa::kWItem - 1) / ncpa::kWItem);
+    const int ev_cap = P * ((cap_modes + ncpa::kEvItem - 1) / ncpa::kEvItem);
+    bis.alloc((size_t)bis_cap * sizeof(WorkItem), st);
+    ev.alloc((size_t)ev_cap * sizeof(WorkItem), st);
+    tot.alloc(4 * sizeof(int), st);
+    check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, counts.as<int>(), cap_modes, ncpa::kWItem,
+                                              bis.as<WorkItem>(), bis_cap, ev.as<WorkItem>(), ev_cap,
+                                              tot.as<int>(), err));
+    // mode counts to the host (sizes of the outputs and of the vectors)
+    int* h_tot = ctx->h_tot;
+    unsigned h_err = 0;
+    CK(cudaMemcpyAsync(h_tot, tot.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(M->info.data(), d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h_err & ncpa::kErrTooMany) {
+        CK(cudaMemsetAsync(ctx->d_err.p, 0, sizeof(unsigned), st));
+        throw ApiError(NCPA_ETOOMANY, "a problem has more wide-angle modes than max_modes");
+    }
+    check_device_status(ctx);
+    tm.mark("host-items");
+    const int n_bis = h_tot[0], n_ev = h_tot[1];
+    M->Mtot = h_tot[2];
+    const size_t mt = (size_t)std::max(1, M->Mtot);
+    DevBuf mu;
+    mu.alloc(mt * 8, st);
+    for (DevBuf* b : {&M->d_kr, &M->d_ki, &M->d_vs, &M->d_vr, &M->d_vg}) b->alloc(mt * 8, st);
+    if (prm->want_vectors) {
+        M->vfull_off.resize(P);
+        long long acc = 0;
+        for (int p = 0; p < P; ++p) {
+            M->vfull_off[p] = acc;
+            acc += (long long)M->info[p].M * M->info[p].nz;
+        }
+        M->d_vfull.alloc((size_t)std::max(1LL, acc) * 8, st);
+        upload(M->d_vfull_off, M->vfull_off, st);
+    }
+    const int wpc = ncpa::wmod_warps_per_cta();
+    if (n_bis > 0) {
+        const int grid_b = std::min((n_bis + wpc - 1) / wpc, ctx->num_sms * 8);
+        check_launch(ctx, ncpa::launch_wbisect(st, grid_b, d_pinfo, a2.as<double>(), a1.as<double>(),
+                                               a0.as<double>(), counts.as<int>(), bis.as<WorkItem>(),
+                                               tot.as<int>(), kWmodTol, mu.as<double>()));
+    }
+    tm.mark("bisect");
+    if (n_ev > 0) {
+        const long long slot = (long long)(M->nz_max + 1) * 32;
+        const long long max_slots = std::max<long long>(wpc, (long long)(kWmodScratchBytes / (slot * 12)));
+        const long long want_slots = std::min<long long>((long long)n_ev, (long long)ctx->num_sms * 8 * wpc);
+        const int grid_e = (int)std::max<long long>(1, std::min(want_slots, max_slots) / wpc);
+        DevBuf qscr, escr;
+        qscr.alloc((size_t)grid_e * wpc * slot * 8, st);
+        escr.alloc((size_t)grid_e * wpc * slot * 4, st);
+        ncpa::WmodEvArgs ea{};
+        ea.pinfo = d_pinfo;
+        ea.a2 = a2.as<double>();
+        ea.a1 = a1.as<double>();
+        ea.a0 = a0.as<double>();
+        ea.w = w.as<double>();
+        ea.items = ev.as<WorkItem>();
+        ea.n_items_dev = tot.as<int>() + 1;
+        ea.mu = mu.as<double>();
+        ea.kr = M->d_kr.as<double>();
+        ea.ki = M->d_ki.as<double>();
+        ea.vs = M->d_vs.as<double>();
+        ea.vr = M->d_vr.as<double>();
+        ea.vg = M->d_vg.as<double>();
+        ea.vfull = prm->want_vectors ? M->d_vfull.as<double>() : nullptr;
+        ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
+        ea.q_scr = qscr.as<double>();
+        ea.e_scr = escr.as<int>();
+        ea.slot_stride = slot;
+        check_launch(ctx, ncpa::launch_weigvec(st, grid_e, ea));
+    }
+    tm.mark("eigvec");
+    M->host_valid = false;
+    if (!prm->keep_on_device) fetch_modes(M);
+    check_device_status(ctx);
+    tm.mark("fetch");
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& g = groups[gi];
+        for (int k = 0; k < g.n_freq * g.n_az; ++k) {
             M->rho_src_p[g.p0 + k] = rho_pairs[2 * gi];
             M->rho_rcv_p[g.p0 + k] = rho_pairs[2 * gi + 1];
         }
@@ -1358,7 +1562,8 @@ ncpa_status ncpa_ess_solve(ncpa_ctx* ctx, const ncpa_profile* prof, const ncpa_e
         M->na = n_az;
         M->freqs.assign(freqs, freqs + n_freq);
         M->az.assign(az_deg, az_deg + n_az);
-        solve_groups(ctx, M.get(), prm, groups);
+        if (prm->method == NCPA_METHOD_WMOD) solve_wmod(ctx, M.get(), prm, groups);
+        else solve_groups(ctx, M.get(), prm, groups);
         *out = M.release();
         return NCPA_OK;
     });
@@ -1370,6 +1575,7 @@ ncpa_status ncpa_ess_solve_jobs(ncpa_ctx* ctx, const ncpa_ess_job* jobs, int n_j
     *out = nullptr;
     return guarded(ctx, [&]() -> ncpa_status {
         check_ess_params(prm);
+        if (prm->method != NCPA_METHOD_ESS) throw ApiError(NCPA_EINVAL, "jobs take the ESS method only");
         int P = 0;
         std::vector<Group> groups;
         groups.reserve(n_jobs);
@@ -1909,6 +2115,7 @@ ncpa_status ncpa_ess_plan_create(ncpa_ctx* ctx, const ncpa_ess_job* jobs, int n_
     *out = nullptr;
     return guarded(ctx, [&]() -> ncpa_status {
         check_ess_params(prm);
+        if (prm->method != NCPA_METHOD_ESS) throw ApiError(NCPA_EINVAL, "plans take the ESS method only");
         if (prm->want_vectors) throw ApiError(NCPA_EINVAL, "plans do not keep eigenvectors (want_vectors = 0)");
         if (prm->lamb_wave_bc) throw ApiError(NCPA_EINVAL, "plans do not take the Lamb-wave condition");
         if (tl && (tl->n_ranges < 1 || !(tl->dr_m > 0))) throw ApiError(NCPA_EINVAL, "bad range grid");

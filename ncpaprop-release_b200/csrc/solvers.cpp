@@ -9,7 +9,12 @@
 namespace ncpa_gpu_solvers {
 
 int ESSModeSolver::solve() {
-    ncpa_cli::run_ess(param_);
+    ncpa_cli::run_ess(param_, false);
+    return 0;
+}
+
+int WModeSolver::solve() {
+    ncpa_cli::run_ess(param_, true);
     return 0;
 }
 

@@ -2,6 +2,8 @@
 //   NCPA::ESSModeSolver (src/libmodes/ESSModeSolver.h:53-80, the
 //     AtmosphericTransferFunctionSolver / ModeSolver interface: construct
 //     from the parameter set, solve(), printParams())
+//   NCPA::WModeSolver (src/libmodes/WModeSolver.h:45-61, the same interface
+//     for the wide-angle high-Mach solve; ModBB --method wmod)
 //   NCPA::ModalBroadbandPropagator (src/libbroadband/ModalBroadbandPropagator.h:
 //     10-28, the BroadbandPropagator interface: construct from the parameter
 //     set, calculate_waveform())
@@ -20,6 +22,15 @@ public:
     explicit ESSModeSolver(const ncpa_cli::Params* param) : param_(*param) {}
     int solve();
     void printParams() const;
+
+private:
+    ncpa_cli::Params param_;
+};
+
+class WModeSolver {
+public:
+    explicit WModeSolver(const ncpa_cli::Params* param) : param_(*param) {}
+    int solve();
 
 private:
     ncpa_cli::Params param_;

@@ -95,7 +95,9 @@ class EssParams(ctypes.Structure):
                 ("sourceheight_km", _c_double), ("receiverheight_km", _c_double), ("lamb_wave_bc", _c_int),
                 ("turnoff_wkb", _c_int), ("wvnum_filter", _c_int), ("c_min", _c_double), ("c_max", _c_double),
                 ("want_group_speed", _c_int), ("want_vectors", _c_int), ("max_modes", _c_int),
-                ("keep_on_device", _c_int)]
+                ("keep_on_device", _c_int), ("method", _c_int)]
+
+METHOD_ESS, METHOD_WMOD = 0, 1
 
 
 class _TlParams(ctypes.Structure):
