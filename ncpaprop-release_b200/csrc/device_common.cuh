@@ -333,6 +333,46 @@ __device__ __forceinline__ void sturm_word32_deriv_pair(SturmState& A, double& d
     sturm_fold(B, wb);
 }
 
+// ---------------------------------------------------------------------------
+// Row formats of the scaled tridiagonal matrices (unit off-diagonal) that the
+// eigenvector kernel streams, and the diagonal entry t_i at a shift.
+//  EssRows   S = h^2 A, one double per row: t_i(x) = s_i - x (x = h^2 k^2).
+//  WmodRows  the wide-angle T(k) h^2, two doubles per row (B_i = h omega /
+//            c0_i, U_i = wc_i / c0_i): t_i(kappa) = (B_i - U_i kappa)^2 -
+//            kappa^2 - 2 with kappa = h k, the same polynomial as
+//            h^2 ((wc^2/c0^2 - 1) k^2 - 2 omega wc / c0^2 k + omega^2 / c0^2) - 2
+//            (WModeSolver.cpp:544-565) in factored form.  Row 0 adds the
+//            ground term g0 (independent of kappa), carried into forward
+//            recurrences as the starting value p_{-2} = -g0.
+// ---------------------------------------------------------------------------
+struct EssRows {
+    static constexpr int kW = 1;  // doubles per row
+    struct Shift {
+        double x;
+    };
+    __device__ static __forceinline__ Shift shift(double mu) { return Shift{mu}; }
+    __device__ static __forceinline__ double t(const double* __restrict__ b, int i, const Shift& s) {
+        return b[i] - s.x;
+    }
+    __device__ static __forceinline__ double p_init(const ProblemInfo&) { return 0.0; }
+    __device__ static __forceinline__ double idle_shift(const ProblemInfo& pi) { return pi.lo; }
+};
+
+struct WmodRows {
+    static constexpr int kW = 2;
+    struct Shift {
+        double kap, c;  // kappa and -(kappa^2 + 2)
+    };
+    __device__ static __forceinline__ Shift shift(double kap) { return Shift{kap, fma(-kap, kap, -2.0)}; }
+    __device__ static __forceinline__ double t(const double* __restrict__ b, int i, const Shift& s) {
+        const double2 r = *reinterpret_cast<const double2*>(b + 2 * i);
+        const double d = fma(-r.y, s.kap, r.x);
+        return fma(d, d, s.c);
+    }
+    __device__ static __forceinline__ double p_init(const ProblemInfo& pi) { return -pi.g0; }
+    __device__ static __forceinline__ double idle_shift(const ProblemInfo& pi) { return pi.k_min * pi.dz; }
+};
+
 // principal square root of x + i y
 __device__ __forceinline__ cuda::std::complex<double> csqrt_principal(double x, double y) {
     double m = hypot(x, y);

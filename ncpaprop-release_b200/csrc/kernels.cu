@@ -919,12 +919,14 @@ struct EvRing {
     unsigned loads;
 };
 
+// chunk c of the rows (kW doubles per row) and, when given, of w and g
+template <int kW>
 __device__ __forceinline__ void evr_issue(EvRing& r, unsigned k, int c, const double* sp, const double* wp,
                                           const double* gp) {
     const int slot = k % kEvB;
-    const uint32_t bytes = kEvC * 8 * (1 + (wp ? 1 : 0) + (gp ? 1 : 0));
+    const uint32_t bytes = kEvC * 8 * (kW + (wp ? 1 : 0) + (gp ? 1 : 0));
     mbar_expect_tx(&r.bars[slot], bytes);
-    tma_load_1d(r.s + slot * kEvC, sp + (size_t)c * kEvC, kEvC * 8, &r.bars[slot]);
+    tma_load_1d(r.s + slot * kEvC * kW, sp + (size_t)c * kEvC * kW, kEvC * 8 * kW, &r.bars[slot]);
     if (wp) tma_load_1d(r.w + slot * kEvC, wp + (size_t)c * kEvC, kEvC * 8, &r.bars[slot]);
     if (gp) tma_load_1d(r.g + slot * kEvC, gp + (size_t)c * kEvC, kEvC * 8, &r.bars[slot]);
 }
@@ -944,9 +946,10 @@ struct FwdState {
     int Eps, Eqs, Eprc, Eqrc;
 };
 
-template <bool kGroup, bool kGuard>
-__device__ __forceinline__ void fwd_step(FwdState& F, int i, int nz, double si, double wi, double gi, double qn,
-                                         int Eb, double mu, int isrc, int ircv) {
+// one forward step at row i (local row li of the staged chunk sb)
+template <class Row, bool kGroup, bool kGuard>
+__device__ __forceinline__ void fwd_step(FwdState& F, int i, int nz, const double* sb, int li, double wi, double gi,
+                                         double qn, int Eb, const typename Row::Shift& sh, int isrc, int ircv) {
     if (kGuard && i >= nz) return;
     const double sq = F.pm1 * F.pm1;
     F.An = F.An + sq;
@@ -990,21 +993,24 @@ __device__ __forceinline__ void fwd_step(FwdState& F, int i, int nz, double si, 
             F.Eqrc = Eb;
         }
     }
-    const double pn = fma(si - mu, F.pm1, -F.pm2);
+    const double pn = fma(Row::t(sb, li, sh), F.pm1, -F.pm2);
     F.pm2 = F.pm1;
     F.pm1 = pn;
 }
 
-template <bool kGroup, bool kVec>
+// Row: the row format (EssRows, WmodRows in device_common.cuh); mu holds the
+// shift of each mode in the row format's units (h^2 k^2, or kappa = h k)
+template <class Row, bool kGroup, bool kVec>
 __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
-    constexpr int NA = kGroup ? 3 : 2;
+    constexpr int kW = Row::kW;
+    constexpr int NA = kW + (kGroup ? 2 : 1);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     double* wb0 = reinterpret_cast<double*>(smem_raw) + (size_t)wid * kEvB * NA * kEvC;
     EvRing R;
     R.s = wb0;
-    R.w = wb0 + kEvB * kEvC;
-    R.g = kGroup ? wb0 + 2 * kEvB * kEvC : nullptr;
+    R.w = wb0 + kEvB * kEvC * kW;
+    R.g = kGroup ? wb0 + (kW + 1) * kEvB * kEvC : nullptr;
     R.bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kEvWarps * kEvB * NA * kEvC * 8) + wid * kEvB;
     R.loads = 0;
     if (lane == 0) {
@@ -1039,17 +1045,19 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
         const int nch = (nz + kEvC - 1) / kEvC;
         const int nblk = (nz + kBlk - 1) / kBlk;
         const int isrc = pi.isrc, ircv = pi.ircv;
-        const double* sp = A.s + pi.s_off;
+        const double* sp = A.s + (size_t)pi.s_off * kW;
         const double* wp = A.w + pi.w_off;
         const double* gp = kGroup ? A.g + pi.s_off : nullptr;
         const bool active = lane < w.m;
-        const double mu = active ? A.mu[pi.off + w.j0 + lane] : pi.lo;
+        const double mu = active ? A.mu[pi.off + w.j0 + lane] : Row::idle_shift(pi);
+        const typename Row::Shift sh = Row::shift(mu);
 
         // ---------------- pass 1: backward recurrence, checkpoints ----------
         {
             const unsigned base = R.loads;
             if (lane == 0)
-                for (int o = 0; o < nch && o < kEvB; ++o) evr_issue(R, base + o, nch - 1 - o, sp, nullptr, nullptr);
+                for (int o = 0; o < nch && o < kEvB; ++o)
+                    evr_issue<kW>(R, base + o, nch - 1 - o, sp, nullptr, nullptr);
             __syncwarp();
             double q1 = 1.0, q2 = 0.0;  // q_i, q_{i+1}; q_n = 1, q_{n+1} = 0
             int E = 0;
@@ -1058,19 +1066,19 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                 const unsigned k = base + o;
                 const int slot = k % kEvB;
                 mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
-                const double* sb = R.s + slot * kEvC;
+                const double* sb = R.s + slot * kEvC * kW;
                 const int valid = min(kEvC, nz - c * kEvC);
                 for (int lb = ((valid - 1) / kBlk) * kBlk; lb >= 0; lb -= kBlk) {
                     if (lb + kBlk <= valid) {
 #pragma unroll
                         for (int u = kBlk - 1; u >= 0; --u) {
-                            const double qi = fma(sb[lb + u] - mu, q1, -q2);
+                            const double qi = fma(Row::t(sb, lb + u, sh), q1, -q2);
                             q2 = q1;
                             q1 = qi;
                         }
                     } else {
                         for (int u = valid - 1 - lb; u >= 0; --u) {
-                            const double qi = fma(sb[lb + u] - mu, q1, -q2);
+                            const double qi = fma(Row::t(sb, lb + u, sh), q1, -q2);
                             q2 = q1;
                             q1 = qi;
                         }
@@ -1093,7 +1101,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                 __syncwarp();
                 if (lane == 0 && o + kEvB < nch) {
                     fence_proxy_async();
-                    evr_issue(R, base + o + kEvB, nch - 1 - (o + kEvB), sp, nullptr, nullptr);
+                    evr_issue<kW>(R, base + o + kEvB, nch - 1 - (o + kEvB), sp, nullptr, nullptr);
                 }
             }
             R.loads = base + nch;
@@ -1101,7 +1109,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
 
         // ---------------- pass 2: forward recurrence, twist, sums ----------
         FwdState F;
-        F.pm2 = 0.0;
+        F.pm2 = Row::p_init(pi);
         F.pm1 = 1.0;
         F.Ep = 0;
         F.An = F.Aw = F.Ag = 0.0;
@@ -1119,7 +1127,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
         {
             const unsigned base = R.loads;
             if (lane == 0)
-                for (int c = 0; c < nch && c < kEvB; ++c) evr_issue(R, base + c, c, sp, wp, gp);
+                for (int c = 0; c < nch && c < kEvB; ++c) evr_issue<kW>(R, base + c, c, sp, wp, gp);
             __syncwarp();
             double nq1, nq2;
             int nE;
@@ -1128,7 +1136,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                 const unsigned k = base + c;
                 const int slot = k % kEvB;
                 mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
-                const double* sb = R.s + slot * kEvC;
+                const double* sb = R.s + slot * kEvC * kW;
                 const double* wb = R.w + slot * kEvC;
                 const double* gb = kGroup ? R.g + slot * kEvC : nullptr;
                 const int valid = min(kEvC, nz - c * kEvC);
@@ -1152,7 +1160,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                         qb[kBlk - 1] = q1;
 #pragma unroll
                         for (int jj = kBlk - 2; jj >= 0; --jj) {
-                            const double qi = fma(sb[lb + jj + 1] - mu, q1, -q2);
+                            const double qi = fma(Row::t(sb, lb + jj + 1, sh), q1, -q2);
                             qb[jj] = qi;
                             q2 = q1;
                             q1 = qi;
@@ -1164,7 +1172,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                             if (idx == ctop) {
                                 qb[jj] = q1;
                             } else if (idx < ctop) {
-                                const double qi = fma(sb[lb + jj + 1] - mu, q1, -q2);
+                                const double qi = fma(Row::t(sb, lb + jj + 1, sh), q1, -q2);
                                 qb[jj] = qi;
                                 q2 = q1;
                                 q1 = qi;
@@ -1178,14 +1186,14 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                     if (!special) {
 #pragma unroll
                         for (int jj = 0; jj < kBlk; ++jj)
-                            fwd_step<kGroup, false>(F, gbase + jj, nz, sb[lb + jj], wb[lb + jj],
-                                                    kGroup ? gb[lb + jj] : 0.0, qb[jj], Eb, mu, isrc, ircv);
+                            fwd_step<Row, kGroup, false>(F, gbase + jj, nz, sb, lb + jj, wb[lb + jj],
+                                                         kGroup ? gb[lb + jj] : 0.0, qb[jj], Eb, sh, isrc, ircv);
                     } else {
 #pragma unroll
                         for (int jj = 0; jj < kBlk; ++jj) {
                             const int li = min(lb + jj, valid - 1);
-                            fwd_step<kGroup, true>(F, gbase + jj, nz, sb[li], wb[li], kGroup ? gb[li] : 0.0, qb[jj],
-                                                   Eb, mu, isrc, ircv);
+                            fwd_step<Row, kGroup, true>(F, gbase + jj, nz, sb, li, wb[li], kGroup ? gb[li] : 0.0,
+                                                        qb[jj], Eb, sh, isrc, ircv);
                         }
                     }
                     const int sh = grow_shift(F.pm1, F.pm2);
@@ -1202,7 +1210,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                 __syncwarp();
                 if (lane == 0 && c + kEvB < nch) {
                     fence_proxy_async();
-                    evr_issue(R, base + c + kEvB, c + kEvB, sp, wp, gp);
+                    evr_issue<kW>(R, base + c + kEvB, c + kEvB, sp, wp, gp);
                 }
             }
             R.loads = base + nch;
@@ -1211,14 +1219,17 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
         const double iq2 = 1.0 / (F.qr * F.qr);
         const double isq = 1.0 / F.sqr;
         const double nrm = F.Anr * isq + F.Tn * iq2;
-        const double scale = 1.0 / sqrt(nrm * pi.dz);
+        // the wide-angle vectors carry SLEPc's normalisation of the linearised
+        // pencil's [v; k v] (EigenEngine.cpp:368-379): sum v^2 dz = 1 / (1 + k^2)
+        const double f2 = kW == 1 ? 1.0 : 1.0 / (1.0 + (mu / pi.dz) * (mu / pi.dz));
+        const double scale = kW == 1 ? 1.0 / sqrt(nrm * pi.dz) : sqrt(f2 / (nrm * pi.dz));
         const int r = F.r;
         double zs = (isrc <= r) ? (F.ps / F.pr) * pow2(F.Eps - F.Epr) : (F.qs / F.qr) * pow2(F.Eqs - F.Eqr);
         double zr = (ircv <= r) ? (F.prc / F.pr) * pow2(F.Eprc - F.Epr) : (F.qrc / F.qr) * pow2(F.Eqrc - F.Eqr);
         if ((isrc - r) & 1) zs = -zs;
         if ((ircv - r) & 1) zr = -zr;
-        const double absorption = (F.Awr * isq + F.Tw * iq2) / nrm;
-        const double ks = sqrt(mu / (pi.dz * pi.dz));
+        const double absorption = kW == 1 ? (F.Awr * isq + F.Tw * iq2) / nrm : (F.Awr * isq + F.Tw * iq2) / nrm * f2;
+        const double ks = kW == 1 ? sqrt(mu / (pi.dz * pi.dz)) : mu / pi.dz;
         const double kk = ks * ks;
         const auto kp = csqrt_principal(kk, absorption);
         if (active) {
@@ -1241,9 +1252,9 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
             const int M = pi.M;
             const unsigned base = R.loads;
             if (lane == 0)
-                for (int c = 0; c < nch && c < kEvB; ++c) evr_issue(R, base + c, c, sp, nullptr, nullptr);
+                for (int c = 0; c < nch && c < kEvB; ++c) evr_issue<kW>(R, base + c, c, sp, nullptr, nullptr);
             __syncwarp();
-            double pa = 0.0, pb = 1.0;
+            double pa = Row::p_init(pi), pb = 1.0;
             int Ea = 0;
             double nq1, nq2;
             int nE;
@@ -1253,7 +1264,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                 const unsigned k = base + c;
                 const int slot = k % kEvB;
                 mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
-                const double* sb = R.s + slot * kEvC;
+                const double* sb = R.s + slot * kEvC * kW;
                 const int valid = min(kEvC, nz - c * kEvC);
                 for (int lb = 0; lb < valid; lb += kBlk) {
                     const int gbase = c * kEvC + lb;
@@ -1269,7 +1280,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                         if (idx == ctop) {
                             qb[jj] = q1;
                         } else if (idx < ctop) {
-                            const double qi = fma(sb[lb + jj + 1] - mu, q1, -q2);
+                            const double qi = fma(Row::t(sb, lb + jj + 1, sh), q1, -q2);
                             qb[jj] = qi;
                             q2 = q1;
                             q1 = qi;
@@ -1286,7 +1297,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                             double zi = (i <= r) ? pb * fp : qb[jj] * fqq;
                             if ((i - r) & 1) zi = -zi;
                             if (active) vout[(size_t)i * M + w.j0 + lane] = zi;
-                            const double pn = fma(sb[lb + jj] - mu, pb, -pa);
+                            const double pn = fma(Row::t(sb, lb + jj, sh), pb, -pa);
                             pa = pb;
                             pb = pn;
                         }
@@ -1302,7 +1313,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
                 __syncwarp();
                 if (lane == 0 && c + kEvB < nch) {
                     fence_proxy_async();
-                    evr_issue(R, base + c + kEvB, c + kEvB, sp, nullptr, nullptr);
+                    evr_issue<kW>(R, base + c + kEvB, c + kEvB, sp, nullptr, nullptr);
                 }
             }
             R.loads = base + nch;
@@ -1310,41 +1321,58 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
     }
 }
 
-template <bool G, bool V>
+template <class Row, bool G, bool V>
 static void* eigvec_fn() {
-    return (void*)k_eigvec<G, V>;
+    return (void*)k_eigvec<Row, G, V>;
 }
 
+template <class Row>
 static size_t eigvec_smem(const EigvecArgs& a) {
-    const int na = a.g ? 3 : 2;
+    const int na = Row::kW + (a.g ? 2 : 1);
     return (size_t)kEvWarps * (kEvB * na * kEvC * 8 + kEvB * 8);
 }
 
+template <class Row>
 static void* eigvec_select(const EigvecArgs& a) {
     const bool grp = a.g != nullptr, vec = a.vfull != nullptr;
-    if (grp && vec) return eigvec_fn<true, true>();
-    if (grp) return eigvec_fn<true, false>();
-    if (vec) return eigvec_fn<false, true>();
-    return eigvec_fn<false, false>();
+    if (grp && vec) return eigvec_fn<Row, true, true>();
+    if (grp) return eigvec_fn<Row, true, false>();
+    if (vec) return eigvec_fn<Row, false, true>();
+    return eigvec_fn<Row, false, false>();
 }
 
-int eigvec_ctas_per_sm(const EigvecArgs& a) {
+template <class Row>
+static int eigvec_fit(const EigvecArgs& a) {
     int n = 1;
-    void* f = eigvec_select(a);
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eigvec_smem(a));
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kEvWarps * 32, eigvec_smem(a)) != cudaSuccess) n = 1;
+    void* f = eigvec_select<Row>(a);
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eigvec_smem<Row>(a));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kEvWarps * 32, eigvec_smem<Row>(a)) != cudaSuccess)
+        n = 1;
     return n < 1 ? 1 : n;
 }
 
-int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a) {
-    const size_t sm = eigvec_smem(a);
+template <class Row>
+static int eigvec_launch(cudaStream_t st, int grid, const EigvecArgs& a) {
+    const size_t sm = eigvec_smem<Row>(a);
     const bool grp = a.g != nullptr, vec = a.vfull != nullptr;
-    cudaFuncSetAttribute(eigvec_select(a), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (grp && vec) k_eigvec<true, true><<<grid, kEvWarps * 32, sm, st>>>(a);
-    else if (grp) k_eigvec<true, false><<<grid, kEvWarps * 32, sm, st>>>(a);
-    else if (vec) k_eigvec<false, true><<<grid, kEvWarps * 32, sm, st>>>(a);
-    else k_eigvec<false, false><<<grid, kEvWarps * 32, sm, st>>>(a);
+    cudaFuncSetAttribute(eigvec_select<Row>(a), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (grp && vec) k_eigvec<Row, true, true><<<grid, kEvWarps * 32, sm, st>>>(a);
+    else if (grp) k_eigvec<Row, true, false><<<grid, kEvWarps * 32, sm, st>>>(a);
+    else if (vec) k_eigvec<Row, false, true><<<grid, kEvWarps * 32, sm, st>>>(a);
+    else k_eigvec<Row, false, false><<<grid, kEvWarps * 32, sm, st>>>(a);
     return 1;
+}
+
+int eigvec_ctas_per_sm(const EigvecArgs& a) { return eigvec_fit<EssRows>(a); }
+
+int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a) { return eigvec_launch<EssRows>(st, grid, a); }
+
+int eigvec_wmod_ctas_per_sm(const EigvecArgs& a) { return eigvec_fit<WmodRows>(a); }
+
+// the wide-angle instantiation carries no group speeds
+int launch_eigvec_wmod(cudaStream_t st, int grid, const EigvecArgs& a) {
+    if (a.g) return -1;
+    return eigvec_launch<WmodRows>(st, grid, a);
 }
 
 // ===========================================================================

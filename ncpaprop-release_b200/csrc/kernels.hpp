@@ -32,6 +32,7 @@ struct ProblemInfo {
     int c_lo, c_hi;        // Sturm counts at lo, hi
     int M, off;            // number of modes and offset into the mode arrays
     int used_wkb;
+    double g0;             // wide-angle rows: ground term of row 0, 1 / (dz admittance + 1)
 };
 
 struct WorkItem {
@@ -149,37 +150,26 @@ int launch_bb_pulse(cudaStream_t st, int nfreq, const double* f, const double* s
 int launch_src_dft(cudaStream_t st, int n, const double* x, double dt, int nfft, int nfreq, const double* tw,
                    double* s);
 
-// Wide-angle (WMod) modes (wmod.cu).  Coefficient rows a2, a1, a0 of
-// T(k) h^2 = diag(a2 k^2 + a1 k + a0) + offdiag(1) use the s layout
-// (pinfo[p].s_off); pinfo k_min / k_max bound the window in k.
+// Wide-angle (WMod) modes (wmod.cu).  Rows of T(k) h^2 in the WmodRows
+// format (device_common.cuh): two doubles per row, (B_i, U_i) interleaved, at
+// 2 * pinfo[p].s_off (the s layout, rows padded to kChunk); row 0's ground
+// term goes to pinfo[p].g0.  The eigen-solve runs in kappa = h k: pinfo
+// k_min / k_max bound the window in k, kappa_min = k_min dz.
 int launch_wc_knots(cudaStream_t st, int n, int n_az, const double* az, const double* ws, const double* wd,
                     double* wc);
 int launch_wmod_build(cudaStream_t st, int nk, const double* zk, const double* c0k, const double* c0c,
                       const double* wck, const double* wcc, const double* ceffk, const double* ceffc, int n_az,
                       int P, ProblemInfo* pinfo, int nz, int nz_pad, double z_min, double dz_grid, double dz,
-                      double admittance, double* a2, double* a1, double* a0, double* kz2);
-int launch_wscan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* a2, const double* a1,
-                 const double* a0, int* counts);
-// mu receives k (not k^2 h^2); tol is relative to k
-int launch_wbisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* a2, const double* a1,
-                   const double* a0, const int* counts, const WorkItem* items, const int* n_items_dev, double tol,
-                   double* mu);
-struct WmodEvArgs {
-    const ProblemInfo* pinfo;
-    const double *a2, *a1, *a0;
-    const double* w;              // attenuation weights, rows at pinfo[p].w_off
-    const WorkItem* items;
-    const int* n_items_dev;
-    const double* mu;             // k per mode
-    double *kr, *ki, *vs, *vr, *vg;
-    double* vfull;                // optional: per problem [nz x M] at vfull_off[p]
-    const long long* vfull_off;
-    double* q_scr;                // per warp slot: (nz_max + 1) rows x 32 lanes
-    int* e_scr;
-    long long slot_stride;        // elements per warp slot
-};
-int launch_weigvec(cudaStream_t st, int grid, const WmodEvArgs& a);
-int wmod_warps_per_cta();
+                      double admittance, double* rows, double* kz2);
+int launch_wscan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* rows, int* counts, unsigned* err);
+// mu receives kappa = h k; tol is relative
+int launch_wbisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* rows, const int* counts,
+                   const WorkItem* items, const int* n_items_dev, double tol, double* mu, unsigned* err);
+int wbisect_ctas_per_sm();
+// eigenvectors of the wide-angle rows: EigvecArgs with s = rows, mu = kappa,
+// g = null; vectors normalised to sum v^2 dz = 1 / (1 + k^2)
+int launch_eigvec_wmod(cudaStream_t st, int grid, const EigvecArgs& a);
+int eigvec_wmod_ctas_per_sm(const EigvecArgs& a);
 
 // K5 modal sum on the tensor cores (modal_sum.cu)
 struct MsPlan {

@@ -817,8 +817,7 @@ void solve_groups(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std:
 // ---------------------------------------------------------------------------
 // WMod (wide-angle) solve: WModeSolver::solve (WModeSolver.cpp:257-486)
 // ---------------------------------------------------------------------------
-constexpr double kWmodTol = 1.0e-15;  // relative to k
-constexpr size_t kWmodScratchBytes = size_t(1) << 30;  // eigenvector q scratch bound
+constexpr double kWmodTol = 1.0e-15;  // relative to kappa = h k
 
 // the matrix spacing of WModeSolver::solve, (maxheight - z_min) / Nz_grid
 // (WModeSolver.cpp:281; the sampling grid keeps setParams' spacing), and the
@@ -841,7 +840,7 @@ struct WmodBufs {
 
 // knot-level fields, attenuation weights and coefficient rows of one group
 void enqueue_wmod_group(ncpa_ctx* ctx, PhaseTimer& tm, const Group& g, WmodBufs& wb, bool wkb, ProblemInfo* d_pinfo,
-                        double* a2, double* a1, double* a0, double* w, double* kz2, double* rho_pair) {
+                        double* rows, double* w, double* kz2, double* rho_pair) {
     cudaStream_t st = ctx->stream;
     const ncpa_profile* prof = g.prof;
     const int nk = prof->n;
@@ -882,8 +881,7 @@ void enqueue_wmod_group(ncpa_ctx* ctx, PhaseTimer& tm, const Group& g, WmodBufs&
                                               wb.c0c.as<double>(), wb.wck.as<double>(), wb.wcc.as<double>(),
                                               b.ceffk.as<double>(), b.ceffc.as<double>(), g.n_az,
                                               g.n_freq * g.n_az, d_pinfo, g.nz, g.nz_pad, g.geo.z_min,
-                                              g.geo.dz_grid, g.geo.dz, b.admittance, a2, a1, a0,
-                                              wkb ? kz2 : nullptr));
+                                              g.geo.dz_grid, g.geo.dz, b.admittance, rows, wkb ? kz2 : nullptr));
     tm.mark("matrix");
 }
 
@@ -896,8 +894,8 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
     layout_groups(M, groups, s_tot, w_tot);
     upload(M->d_pinfo, M->info, st);
     const bool wkb = wants_wkb(prm);
-    DevBuf a2, a1, a0, w, kz2;
-    for (DevBuf* b : {&a2, &a1, &a0}) b->alloc((size_t)s_tot * 8, st);
+    DevBuf rows, w, kz2;
+    rows.alloc((size_t)s_tot * 16, st);
     w.alloc((size_t)w_tot * 8, st);
     if (wkb) kz2.alloc((size_t)s_tot * 8, st);
     double* rho_pairs = pinned(ctx, 2 * groups.size());
@@ -913,9 +911,8 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
     }
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         const Group& g = groups[gi];
-        enqueue_wmod_group(ctx, tm, g, wbs[gi], wkb, d_pinfo + g.p0, a2.as<double>() + g.s_base,
-                           a1.as<double>() + g.s_base, a0.as<double>() + g.s_base, w.as<double>() + g.w_base,
-                           wkb ? kz2.as<double>() + g.s_base : nullptr, rho_pairs + 2 * gi);
+        enqueue_wmod_group(ctx, tm, g, wbs[gi], wkb, d_pinfo + g.p0, rows.as<double>() + 2 * g.s_base,
+                           w.as<double>() + g.w_base, wkb ? kz2.as<double>() + g.s_base : nullptr, rho_pairs + 2 * gi);
     }
     const int P = M->P;
     unsigned* err = ctx->d_err.as<unsigned>();
@@ -924,8 +921,7 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
     tm.mark("window");
     DevBuf counts, bis, ev, tot;
     counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
-    check_launch(ctx, ncpa::launch_wscan(st, P, d_pinfo, a2.as<double>(), a1.as<double>(), a0.as<double>(),
-                                         counts.as<int>()));
+    check_launch(ctx, ncpa::launch_wscan(st, P, d_pinfo, rows.as<double>(), counts.as<int>(), err));
     tm.mark("scan");
     const int cap_modes = M->prm.max_modes;
     const int bis_cap = P * ((cap_modes + ncpa::kWItem - 1) / ncpa::kWItem);
@@ -965,29 +961,20 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
         M->d_vfull.alloc((size_t)std::max(1LL, acc) * 8, st);
         upload(M->d_vfull_off, M->vfull_off, st);
     }
-    const int wpc = ncpa::wmod_warps_per_cta();
     if (n_bis > 0) {
-        const int grid_b = std::min((n_bis + wpc - 1) / wpc, ctx->num_sms * 8);
-        check_launch(ctx, ncpa::launch_wbisect(st, grid_b, d_pinfo, a2.as<double>(), a1.as<double>(),
-                                               a0.as<double>(), counts.as<int>(), bis.as<WorkItem>(),
-                                               tot.as<int>(), kWmodTol, mu.as<double>()));
+        const int grid_b = std::min(ctx->num_sms * ncpa::wbisect_ctas_per_sm(), (n_bis + 3) / 4);
+        check_launch(ctx, ncpa::launch_wbisect(st, grid_b, d_pinfo, rows.as<double>(), counts.as<int>(),
+                                               bis.as<WorkItem>(), tot.as<int>(), kWmodTol, mu.as<double>(), err));
     }
     tm.mark("bisect");
     if (n_ev > 0) {
-        const long long slot = (long long)(M->nz_max + 1) * 32;
-        const long long max_slots = std::max<long long>(wpc, (long long)(kWmodScratchBytes / (slot * 12)));
-        const long long want_slots = std::min<long long>((long long)n_ev, (long long)ctx->num_sms * 8 * wpc);
-        const int grid_e = (int)std::max<long long>(1, std::min(want_slots, max_slots) / wpc);
-        DevBuf qscr, escr;
-        qscr.alloc((size_t)grid_e * wpc * slot * 8, st);
-        escr.alloc((size_t)grid_e * wpc * slot * 4, st);
-        ncpa::WmodEvArgs ea{};
+        ncpa::EigvecArgs ea{};
         ea.pinfo = d_pinfo;
-        ea.a2 = a2.as<double>();
-        ea.a1 = a1.as<double>();
-        ea.a0 = a0.as<double>();
+        ea.s = rows.as<double>();
         ea.w = w.as<double>();
+        ea.g = nullptr;
         ea.items = ev.as<WorkItem>();
+        ea.n_items = 0;
         ea.n_items_dev = tot.as<int>() + 1;
         ea.mu = mu.as<double>();
         ea.kr = M->d_kr.as<double>();
@@ -997,10 +984,22 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
         ea.vg = M->d_vg.as<double>();
         ea.vfull = prm->want_vectors ? M->d_vfull.as<double>() : nullptr;
         ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
-        ea.q_scr = qscr.as<double>();
-        ea.e_scr = escr.as<int>();
-        ea.slot_stride = slot;
-        check_launch(ctx, ncpa::launch_weigvec(st, grid_e, ea));
+        ea.err = err;
+        const int fit = ncpa::eigvec_wmod_ctas_per_sm(ea);
+        const int grid_e = std::max(1, std::min((n_ev + ncpa::kEvWarpsPerCta - 1) / ncpa::kEvWarpsPerCta,
+                                                ctx->num_sms * fit));
+        const long long slot = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
+        const size_t need = (size_t)grid_e * ncpa::kEvWarpsPerCta * slot;
+        if (ctx->ck1.bytes < need * 8) {
+            ctx->ck1.alloc(need * 8, st);
+            ctx->ck2.alloc(need * 8, st);
+            ctx->cke.alloc(need * 4, st);
+        }
+        ea.ck_q1 = ctx->ck1.as<double>();
+        ea.ck_q2 = ctx->ck2.as<double>();
+        ea.ck_e = ctx->cke.as<int>();
+        ea.ck_slot_stride = slot;
+        check_launch(ctx, ncpa::launch_eigvec_wmod(st, grid_e, ea));
     }
     tm.mark("eigvec");
     M->host_valid = false;
