@@ -13,7 +13,9 @@ not part of the step), with its roofline against the measured bf16 peak,
 and "serving": a seeded request stream replayed in real time through the
 serving loop and through the plain one-request-at-a-time path (p50 / p99
 latency, throughput), and "sweep": 360 azimuths x 8 frequencies with Nz per
-frequency (5000-60000) as one batched solve.
+frequency (5000-60000) as one batched solve, and "wmod": the same
+256-frequency dispersion + 1-D TL with the wide-angle solver (ModBB
+--method wmod), with its bisection roofline and its own CPU baseline.
 
   value  freq-solves/s with the profile resident in HBM and results left in
          HBM (device-timed with CUDA events on the library's stream; L2
@@ -332,6 +334,8 @@ def run_ours(args):
     ms_leg = modal_sum_leg(ctx, stream, _bf16_peak()) if rank == 0 and not args.no_modal_sum else None
     sv_leg = serving_leg(ctx) if rank == 0 and not args.no_serving else None
     sw_leg = sweep_leg(ctx, stream) if rank == 0 and not args.no_sweep else None
+    wm_leg = wmod_leg(ctx, stream, prof, freqs, az, fp64_peak, flush, args.cpu_seconds) \
+        if rank == 0 and not args.no_wmod else None
     if rank == 0:
         solves = NFREQ * args.steps * world
         value = solves / (ms_dev / 1e3)
@@ -368,6 +372,7 @@ def run_ours(args):
             "modal_sum": ms_leg,
             "serving": sv_leg,
             "sweep": sw_leg,
+            "wmod": wm_leg,
         }
         print(json.dumps(line), flush=True)
     for h in (prof,):
@@ -538,6 +543,82 @@ def sweep_leg(ctx, stream, reps=2):
         "what": "batched = one ncpa_ess_solve_jobs over all grids + one TL launch; per_grid = one "
                 "ncpa_ess_solve + TL per frequency; plan = the batch replayed as one captured CUDA graph "
                 "(launch shapes autotuned)",
+    }
+
+
+# ---------------------------------------------------------------------------
+# wide-angle (WMod) dispersion: ModBB --dispersion --method wmod
+# ---------------------------------------------------------------------------
+def wmod_leg(ctx, stream, prof, freqs, az, fp64_peak, flush, cpu_seconds, k=5):
+    """The 256-frequency dispersion + 1-D TL of the main step solved with the
+    wide-angle solver (WKB off, as --dispersion_file forces), device-resident,
+    L2 flushed before each timed solve; phases and the bisection roofline
+    (3 FMA per counted chain step) from separate untimed solves; the oracle's
+    WMod restatement on every 32nd frequency as the CPU baseline."""
+    import torch
+    import ncpa_gpu
+
+    params = ncpa_gpu.default_params(nz_grid=NZ, turnoff_wkb=1, keep_on_device=1, method=ncpa_gpu.METHOD_WMOD)
+
+    def step():
+        m = ctx.solve(prof, params, freqs, az)
+        m.tl1d(N_TL, DR_TL, to_host=False)
+        return m
+
+    for _ in range(2):
+        step().close()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+    modes = 0
+    for i in range(k):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev[i][0].record(stream)
+        m = step()
+        ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        modes = int(m.counts().sum())
+        m.close()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / k
+    n_ph = 3
+    ctx.reset_stats()
+    ctx.set_timing(True)
+    for _ in range(n_ph):
+        flush.zero_()
+        step().close()
+    torch.cuda.synchronize()
+    ctx.set_timing(False)
+    bis_ms, bis_n = ctx.phase_stats("bisect")
+    steps = ctx.sturm_steps()
+    phases = {ph: round(ctx.phase_stats(ph)[0] / n_ph, 4) for ph in
+              ("knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec", "fetch")}
+    flops = 6.0 * steps
+    achieved = flops / (bis_ms / 1e3) / 1e12 if bis_ms > 0 else None
+    # CPU: the oracle's WMod restatement on a stratified sample
+    O, pp, prm = _oracle_setup()
+    t0 = time.perf_counter()
+    done = 0
+    for f in freqs[::32]:
+        ms_o = O.solve_problem_wmod(pp, prm, float(f), az[0])
+        O.tl1d(ms_o, N_TL, DR_TL)
+        done += 1
+        if time.perf_counter() - t0 > cpu_seconds / 2:
+            break
+    el = time.perf_counter() - t0
+    return {
+        "workload": "ModBB --dispersion --method wmod: 256 frequencies df = 0.5/256 Hz, Nz = %d, WKB off, "
+                    "1-D TL at %d ranges x %g km, analytic 0-150 km profile" % (NZ, N_TL, DR_TL / 1e3),
+        "modes_total": modes, "ms_per_step": round(ms, 4), "value": round(NFREQ / (ms / 1e3), 2), "unit": METRIC,
+        "phases_ms": phases,
+        "roofline": {"kernel": "k_bisect<WmodRows> (Sturm multisection in kappa)", "bound": "fp64",
+                     "achieved": round(achieved, 3) if achieved else None,
+                     "peak": round(fp64_peak, 3) if fp64_peak else None, "unit": "TFLOP/s",
+                     "frac": round(achieved / fp64_peak, 4) if achieved and fp64_peak else None,
+                     "flops": "6 per counted chain step (3 FMA; derivative FMAs not counted)",
+                     "avg_launch_ms": round(bis_ms / max(bis_n, 1), 4)},
+        "cpu_baseline": {"value": round(done / el, 3), "unit": METRIC, "cores": O.lib().orc_num_threads(),
+                         "kind": "port",
+                         "sample": "%d of the 256 frequencies (every 32nd), Nz=%d, WMod eigen-solve + 1-D TL each"
+                                   % (done, NZ)},
     }
 
 
@@ -727,6 +808,9 @@ def main():
     ap.add_argument("--no-modal-sum", action="store_true", help="skip the tensor-core modal-sum leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the served request-stream leg")
     ap.add_argument("--no-sweep", action="store_true", help="skip the 360-azimuth mixed-grid sweep leg")
+    ap.add_argument("--no-wmod", action="store_true", help="skip the wide-angle (WMod) dispersion leg")
+    ap.add_argument("--only-wmod", action="store_true",
+                    help="run only the wide-angle dispersion leg and print its JSON (for profiler runs)")
     ap.add_argument("--only-modal-sum", action="store_true",
                     help="run only the tensor-core modal-sum leg and print its JSON (for profiler runs)")
     ap.add_argument("--only-serving", action="store_true",
@@ -747,6 +831,20 @@ def main():
 
         ctx = ncpa_gpu.Context(0)
         print(json.dumps(sweep_leg(ctx, torch.cuda.ExternalStream(ctx.stream_ptr), reps=1)), flush=True)
+        ctx.close()
+        return
+    if args.only_wmod:
+        import torch
+        import ncpa_gpu
+
+        ctx = ncpa_gpu.Context(0)
+        tmp = tempfile.mkdtemp(prefix="ncpa_bench_")
+        prof = ctx.load_profile(workloads.write_profile(os.path.join(tmp, "analytic_150km.dat")))
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        print(json.dumps(wmod_leg(ctx, torch.cuda.ExternalStream(ctx.stream_ptr), prof,
+                                  workloads.broadband_freqs(NFREQ, 0.5), [90.0], ctx.fp64_peak_tflops(), flush,
+                                  args.cpu_seconds)), flush=True)
+        prof.close()
         ctx.close()
         return
     if args.only_modal_sum:

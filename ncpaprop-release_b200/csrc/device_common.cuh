@@ -256,6 +256,22 @@ __device__ __forceinline__ void sturm_fold(SturmState& S, unsigned w) {
     }
 }
 
+// sign bits of 32 steps folded into a chain's count, then the joint exact
+// power-of-two rescale of the chain and its derivative chain (d0, d1)
+__device__ __forceinline__ void sturm_fold_deriv(SturmState& S, unsigned w, double& d0, double& d1) {
+    const unsigned prev = (w >> 1) | (S.prevbit << 31);
+    S.cnt += __popc(w ^ prev);
+    S.prevbit = w & 1u;
+    const int sh = rescale_shift(fmax(fabs(S.p0), fabs(d0)), fmax(fabs(S.p1), fabs(d1)));
+    if (sh) {
+        const double sc = pow2(-sh);
+        S.p0 *= sc;
+        S.p1 *= sc;
+        d0 *= sc;
+        d1 *= sc;
+    }
+}
+
 // 32 steps of two independent chains (shifts xa, xb) interleaved step by
 // step, so the warp always has two dependent FMA chains in flight; the
 // arithmetic of each chain is exactly that of SturmState::word32
@@ -356,6 +372,32 @@ struct EssRows {
     }
     __device__ static __forceinline__ double p_init(const ProblemInfo&) { return 0.0; }
     __device__ static __forceinline__ double idle_shift(const ProblemInfo& pi) { return pi.lo; }
+    // the bisection interval and the scale of its tolerance
+    __device__ static __forceinline__ double scan_lo(const ProblemInfo& pi) { return pi.lo; }
+    __device__ static __forceinline__ double scan_hi(const ProblemInfo& pi) { return pi.hi; }
+    __device__ static __forceinline__ double tol_scale(const ProblemInfo&) { return 1.0; }
+    // Sturm sweeps over 32 staged rows at b (see SturmState)
+    __device__ static __forceinline__ void pair(SturmState& A, SturmState& B, const double* __restrict__ b,
+                                                double xa, double xb) {
+        sturm_word32_pair(A, B, b, xa, xb);
+    }
+    __device__ static __forceinline__ void deriv_pair(SturmState& A, double& d0, double& d1, SturmState& B,
+                                                      const double* __restrict__ b, double xa, double xb) {
+        sturm_word32_deriv_pair(A, d0, d1, B, b, xa, xb);
+    }
+    __device__ static __forceinline__ void word_deriv(SturmState& A, const double* __restrict__ b, double x,
+                                                      double& d0, double& d1) {
+        A.word32_deriv(b, x, d0, d1);
+    }
+    __device__ static __forceinline__ void step(SturmState& A, const double* __restrict__ b, int i, double x) {
+        A.step(b[i], x);
+    }
+    __device__ static __forceinline__ void step_deriv(SturmState& A, const double* __restrict__ b, int i, double x,
+                                                      double& d0, double& d1) {
+        A.step_deriv(b[i], x, d0, d1);
+    }
+    // Newton correction (subtracted from x) from the last p and its derivative chain
+    __device__ static __forceinline__ double newton(double p, double d) { return p / d; }
 };
 
 struct WmodRows {
@@ -371,6 +413,120 @@ struct WmodRows {
     }
     __device__ static __forceinline__ double p_init(const ProblemInfo& pi) { return -pi.g0; }
     __device__ static __forceinline__ double idle_shift(const ProblemInfo& pi) { return pi.k_min * pi.dz; }
+    __device__ static __forceinline__ double scan_lo(const ProblemInfo& pi) { return pi.k_min * pi.dz; }
+    __device__ static __forceinline__ double scan_hi(const ProblemInfo& pi) { return pi.k_max * pi.dz; }
+    __device__ static __forceinline__ double tol_scale(const ProblemInfo& pi) { return pi.k_max * pi.dz; }
+    // Sturm sweeps over 32 staged rows at b.  The derivative chain carries
+    // e_i = t_i e_{i-1} + (U_i d_i + kappa) p_{i-1} - e_{i-2}, d_i = B_i - U_i
+    // kappa, which is -1/2 of d p_i / d kappa.
+    __device__ static __forceinline__ void pair(SturmState& A, SturmState& B, const double* __restrict__ b,
+                                                double xa, double xb) {
+        const double ca = fma(-xa, xa, -2.0), cb = fma(-xb, xb, -2.0);
+        unsigned wa = 0u, wb = 0u;
+        double pa0 = A.p0, pa1 = A.p1, pb0 = B.p0, pb1 = B.p1;
+#pragma unroll
+        for (int u = 0; u < 32; ++u) {
+            const double2 rv = *reinterpret_cast<const double2*>(b + 2 * u);
+            const double da = fma(-rv.y, xa, rv.x);
+            const double db = fma(-rv.y, xb, rv.x);
+            const double qa = fma(fma(da, da, ca), pa1, -pa0);
+            const double qb = fma(fma(db, db, cb), pb1, -pb0);
+            wa = __funnelshift_l(__double2hiint(qa), wa, 1);
+            wb = __funnelshift_l(__double2hiint(qb), wb, 1);
+            pa0 = pa1;
+            pa1 = qa;
+            pb0 = pb1;
+            pb1 = qb;
+        }
+        A.p0 = pa0;
+        A.p1 = pa1;
+        B.p0 = pb0;
+        B.p1 = pb1;
+        sturm_fold(A, wa);
+        sturm_fold(B, wb);
+    }
+    __device__ static __forceinline__ void deriv_pair(SturmState& A, double& d0, double& d1, SturmState& B,
+                                                      const double* __restrict__ b, double xa, double xb) {
+        const double ca = fma(-xa, xa, -2.0), cb = fma(-xb, xb, -2.0);
+        unsigned wa = 0u, wb = 0u;
+        double pa0 = A.p0, pa1 = A.p1, pb0 = B.p0, pb1 = B.p1;
+#pragma unroll
+        for (int u = 0; u < 32; ++u) {
+            const double2 rv = *reinterpret_cast<const double2*>(b + 2 * u);
+            const double da = fma(-rv.y, xa, rv.x);
+            const double db = fma(-rv.y, xb, rv.x);
+            const double ta = fma(da, da, ca);
+            const double tp = fma(rv.y, da, xa);
+            const double qa = fma(ta, pa1, -pa0);
+            const double qb = fma(fma(db, db, cb), pb1, -pb0);
+            const double ea = fma(ta, d1, fma(tp, pa1, -d0));
+            wa = __funnelshift_l(__double2hiint(qa), wa, 1);
+            wb = __funnelshift_l(__double2hiint(qb), wb, 1);
+            pa0 = pa1;
+            pa1 = qa;
+            pb0 = pb1;
+            pb1 = qb;
+            d0 = d1;
+            d1 = ea;
+        }
+        A.p0 = pa0;
+        A.p1 = pa1;
+        B.p0 = pb0;
+        B.p1 = pb1;
+        sturm_fold_deriv(A, wa, d0, d1);
+        sturm_fold(B, wb);
+    }
+    __device__ static __forceinline__ void word_deriv(SturmState& A, const double* __restrict__ b, double x,
+                                                      double& d0, double& d1) {
+        const double c = fma(-x, x, -2.0);
+        unsigned wa = 0u;
+        double pa0 = A.p0, pa1 = A.p1;
+#pragma unroll
+        for (int u = 0; u < 32; ++u) {
+            const double2 rv = *reinterpret_cast<const double2*>(b + 2 * u);
+            const double da = fma(-rv.y, x, rv.x);
+            const double ta = fma(da, da, c);
+            const double tp = fma(rv.y, da, x);
+            const double qa = fma(ta, pa1, -pa0);
+            const double ea = fma(ta, d1, fma(tp, pa1, -d0));
+            wa = __funnelshift_l(__double2hiint(qa), wa, 1);
+            pa0 = pa1;
+            pa1 = qa;
+            d0 = d1;
+            d1 = ea;
+        }
+        A.p0 = pa0;
+        A.p1 = pa1;
+        sturm_fold_deriv(A, wa, d0, d1);
+    }
+    __device__ static __forceinline__ void step(SturmState& A, const double* __restrict__ b, int i, double x) {
+        const double2 rv = *reinterpret_cast<const double2*>(b + 2 * i);
+        const double d = fma(-rv.y, x, rv.x);
+        const double q = fma(fma(d, d, fma(-x, x, -2.0)), A.p1, -A.p0);
+        const unsigned bit = static_cast<unsigned>(__double2hiint(q)) >> 31;
+        A.cnt += static_cast<int>(bit ^ A.prevbit);
+        A.prevbit = bit;
+        A.p0 = A.p1;
+        A.p1 = q;
+    }
+    __device__ static __forceinline__ void step_deriv(SturmState& A, const double* __restrict__ b, int i, double x,
+                                                      double& d0, double& d1) {
+        const double2 rv = *reinterpret_cast<const double2*>(b + 2 * i);
+        const double d = fma(-rv.y, x, rv.x);
+        const double t = fma(d, d, fma(-x, x, -2.0));
+        const double tp = fma(rv.y, d, x);
+        const double q = fma(t, A.p1, -A.p0);
+        const double e = fma(t, d1, fma(tp, A.p1, -d0));
+        const unsigned bit = static_cast<unsigned>(__double2hiint(q)) >> 31;
+        A.cnt += static_cast<int>(bit ^ A.prevbit);
+        A.prevbit = bit;
+        A.p0 = A.p1;
+        A.p1 = q;
+        d0 = d1;
+        d1 = e;
+    }
+    // d p / d kappa = -2 e: the correction subtracted from kappa is -p / (2 e)
+    __device__ static __forceinline__ double newton(double p, double e) { return -0.5 * (p / e); }
 };
 
 // principal square root of x + i y

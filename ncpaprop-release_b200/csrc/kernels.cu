@@ -566,12 +566,17 @@ __device__ __forceinline__ int nth_bit(unsigned m, int n) {
     return pos;
 }
 
-// One sweep over the diagonal.  mode 0: chains A and B, counts only;
-// 1: chain A with derivative + chain B; 2: chain A with derivative only.
-__device__ void warp_sweep(const double* __restrict__ s, int nz, double x0, double x1, int mode, WarpRing& r,
-                           unsigned* err, int& c0, int& c1, double& rat0) {
+// One sweep over the rows (Row format; kWChunk doubles per ring chunk, so
+// kWChunk / Row::kW rows).  mode 0: chains A and B, counts only; 1: chain A
+// with derivative + chain B; 2: chain A with derivative only.  p_init starts
+// both chains (Row::p_init); rat0 is chain A's Newton correction.
+template <class Row>
+__device__ void warp_sweep(const double* __restrict__ s, int nz, double p_init, double x0, double x1, int mode,
+                           WarpRing& r, unsigned* err, int& c0, int& c1, double& rat0) {
+    constexpr int kW = Row::kW;
+    constexpr int kRows = kWChunk / kW;
     const int lane = threadIdx.x & 31;
-    const int nch = (nz + kWChunk - 1) / kWChunk;
+    const int nch = (nz + kRows - 1) / kRows;
     const unsigned base = r.loads;
     if (lane == 0)
         for (int c = 0; c < nch && c < kWBuf; ++c) wring_issue(r, base + c, s + (size_t)c * kWChunk);
@@ -579,29 +584,33 @@ __device__ void warp_sweep(const double* __restrict__ s, int nz, double x0, doub
     SturmState A, B;
     A.reset();
     B.reset();
+    if (kW != 1) {
+        A.p0 = p_init;
+        B.p0 = p_init;
+    }
     double da0 = 0.0, da1 = 0.0;
     for (int c = 0; c < nch; ++c) {
         const unsigned k = base + c;
         const int slot = k % kWBuf;
         mbar_wait_bounded(&r.bars[slot], (k / kWBuf) & 1u, err);
         const double* b = r.buf + slot * kWChunk;
-        const int valid = min(kWChunk, nz - c * kWChunk);
+        const int valid = min(kRows, nz - c * kRows);
         const int nw = valid >> 5;
         if (mode == 0) {
-            for (int w = 0; w < nw; ++w) sturm_word32_pair(A, B, b + 32 * w, x0, x1);
+            for (int w = 0; w < nw; ++w) Row::pair(A, B, b + 32 * kW * w, x0, x1);
             for (int i = nw * 32; i < valid; ++i) {
-                A.step(b[i], x0);
-                B.step(b[i], x1);
+                Row::step(A, b, i, x0);
+                Row::step(B, b, i, x1);
             }
         } else if (mode == 1) {
-            for (int w = 0; w < nw; ++w) sturm_word32_deriv_pair(A, da0, da1, B, b + 32 * w, x0, x1);
+            for (int w = 0; w < nw; ++w) Row::deriv_pair(A, da0, da1, B, b + 32 * kW * w, x0, x1);
             for (int i = nw * 32; i < valid; ++i) {
-                A.step_deriv(b[i], x0, da0, da1);
-                B.step(b[i], x1);
+                Row::step_deriv(A, b, i, x0, da0, da1);
+                Row::step(B, b, i, x1);
             }
         } else {
-            for (int w = 0; w < nw; ++w) A.word32_deriv(b + 32 * w, x0, da0, da1);
-            for (int i = nw * 32; i < valid; ++i) A.step_deriv(b[i], x0, da0, da1);
+            for (int w = 0; w < nw; ++w) Row::word_deriv(A, b + 32 * kW * w, x0, da0, da1);
+            for (int i = nw * 32; i < valid; ++i) Row::step_deriv(A, b, i, x0, da0, da1);
         }
         __syncwarp();
         if (lane == 0 && c + kWBuf < nch) {
@@ -612,12 +621,15 @@ __device__ void warp_sweep(const double* __restrict__ s, int nz, double x0, doub
     r.loads = base + nch;
     c0 = A.cnt;
     c1 = B.cnt;
-    rat0 = mode >= 1 ? A.p1 / da1 : 0.0;
+    rat0 = mode >= 1 ? Row::newton(A.p1, da1) : 0.0;
 }
 
+// Row: the row format (EssRows: shifts in h^2 k^2; WmodRows: kappa = h k);
+// tol is scaled per problem by Row::tol_scale.
+template <class Row>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
     k_bisect(const ProblemInfo* __restrict__ pinfo, const double* __restrict__ s, const int* __restrict__ counts,
-             const WorkItem* __restrict__ items, int n_items, int* counter, double tol, double* __restrict__ mu,
+             const WorkItem* __restrict__ items, int n_items, int* counter, double tol_in, double* __restrict__ mu,
              unsigned* err, unsigned long long* step_counter, const int* __restrict__ n_items_dev) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     if (n_items_dev) n_items = *n_items_dev;
@@ -639,11 +651,14 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
         const WorkItem w = items[it];
         const ProblemInfo pi = pinfo[w.problem];
         const int* cnt = counts + (size_t)w.problem * kScanPoints;
-        const double* sp = s + pi.s_off;
+        const double* sp = s + (size_t)pi.s_off * Row::kW;
         const int nz = pi.nz;
+        const double lo = Row::scan_lo(pi), hi = Row::scan_hi(pi);
+        const double tol = tol_in * Row::tol_scale(pi);
+        const double p_init = Row::p_init(pi);
         // state of eigen slot `lane`
         const int J = pi.c_lo + w.j0 + lane;
-        double a = pi.lo, b = pi.lo, x = pi.lo;
+        double a = lo, b = lo, x = lo;
         double dprev = 0.0;  // size of the previous Newton correction (0: none yet)
         int ca = 0, cb = 0, mode = 2;
         if (lane < w.m) {  // initial bracket from the isolation scan
@@ -654,8 +669,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
             for (int t = kScanPoints - 1; t > t0; --t)
                 if (cnt[t] > J) t1 = t;
             if (cnt[t1] <= J) atomicOr(err, kErrBracket);
-            a = scan_x(pi.lo, pi.hi, t0);
-            b = scan_x(pi.lo, pi.hi, t1);
+            a = scan_x(lo, hi, t0);
+            b = scan_x(lo, hi, t1);
             ca = cnt[t0];
             cb = cnt[t1];
             x = 0.5 * (a + b);
@@ -697,7 +712,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
             int cv0, cv1;
             double rat;
             const int smode = nN == 0 ? 0 : (nB > 0 ? 1 : 2);
-            warp_sweep(sp, nz, xv[0], xv[1], smode, r, err, cv0, cv1, rat);
+            warp_sweep<Row>(sp, nz, p_init, xv[0], xv[1], smode, r, err, cv0, cv1, rat);
             if (step_counter && lane == 0)
                 atomicAdd(step_counter, (unsigned long long)(smode == 2 ? 32 : 64) * (unsigned long long)nz);
             // updates.  Every __shfl_sync is executed by all 32 lanes.
@@ -770,23 +785,46 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
     }
 }
 
-int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
-                  const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
-                  unsigned long long* step_counter, const int* n_items_dev) {
-    const size_t sm = (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8 + kWBuf * 8);
-    cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_bisect<<<grid, kWarpsPerCta * 32, sm, st>>>(pinfo, s, counts, items, n_items, counter, tol, mu, err,
-                                                  step_counter, n_items_dev);
+static size_t bisect_smem() { return (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8 + kWBuf * 8); }
+
+template <class Row>
+static int bisect_launch(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
+                         const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
+                         unsigned long long* step_counter, const int* n_items_dev) {
+    const size_t sm = bisect_smem();
+    cudaFuncSetAttribute(k_bisect<Row>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_bisect<Row><<<grid, kWarpsPerCta * 32, sm, st>>>(pinfo, s, counts, items, n_items, counter, tol, mu, err,
+                                                       step_counter, n_items_dev);
     return 1;
 }
 
-int bisect_ctas_per_sm() {
+template <class Row>
+static int bisect_fit() {
     int n = 1;
-    const size_t sm = (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8 + kWBuf * 8);
-    cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bisect, kWarpsPerCta * 32, sm) != cudaSuccess) n = 1;
+    const size_t sm = bisect_smem();
+    cudaFuncSetAttribute(k_bisect<Row>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bisect<Row>, kWarpsPerCta * 32, sm) != cudaSuccess)
+        n = 1;
     return n < 1 ? 1 : n;
 }
+
+int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
+                  const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
+                  unsigned long long* step_counter, const int* n_items_dev) {
+    return bisect_launch<EssRows>(st, grid, pinfo, s, counts, items, n_items, counter, tol, mu, err, step_counter,
+                                  n_items_dev);
+}
+
+int bisect_ctas_per_sm() { return bisect_fit<EssRows>(); }
+
+int launch_bisect_wmod(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* rows, const int* counts,
+                       const WorkItem* items, double tol, double* mu, unsigned* err,
+                       unsigned long long* step_counter, const int* n_items_dev) {
+    return bisect_launch<WmodRows>(st, grid, pinfo, rows, counts, items, 0, nullptr, tol, mu, err, step_counter,
+                                   n_items_dev);
+}
+
+int bisect_wmod_ctas_per_sm() { return bisect_fit<WmodRows>(); }
 
 // ===========================================================================
 // Work items on the device (one CTA): the host-side item building of the

@@ -162,10 +162,13 @@ int launch_wmod_build(cudaStream_t st, int nk, const double* zk, const double* c
                       int P, ProblemInfo* pinfo, int nz, int nz_pad, double z_min, double dz_grid, double dz,
                       double admittance, double* rows, double* kz2);
 int launch_wscan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* rows, int* counts, unsigned* err);
-// mu receives kappa = h k; tol is relative
-int launch_wbisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* rows, const int* counts,
-                   const WorkItem* items, const int* n_items_dev, double tol, double* mu, unsigned* err);
-int wbisect_ctas_per_sm();
+// k_bisect on the wide-angle rows: mu receives kappa = h k; tol is relative
+// to kappa_max; step_counter (optional) counts chain steps (3 FMA each) as
+// launch_bisect does
+int launch_bisect_wmod(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* rows, const int* counts,
+                       const WorkItem* items, double tol, double* mu, unsigned* err,
+                       unsigned long long* step_counter, const int* n_items_dev);
+int bisect_wmod_ctas_per_sm();
 // eigenvectors of the wide-angle rows: EigvecArgs with s = rows, mu = kappa,
 // g = null; vectors normalised to sum v^2 dz = 1 / (1 + k^2)
 int launch_eigvec_wmod(cudaStream_t st, int grid, const EigvecArgs& a);

@@ -817,7 +817,7 @@ void solve_groups(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std:
 // ---------------------------------------------------------------------------
 // WMod (wide-angle) solve: WModeSolver::solve (WModeSolver.cpp:257-486)
 // ---------------------------------------------------------------------------
-constexpr double kWmodTol = 1.0e-15;  // relative to kappa = h k
+constexpr double kWmodTol = 1.0e-15;  // relative to kappa_max = h k_max
 
 // the matrix spacing of WModeSolver::solve, (maxheight - z_min) / Nz_grid
 // (WModeSolver.cpp:281; the sampling grid keeps setParams' spacing), and the
@@ -962,9 +962,11 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
         upload(M->d_vfull_off, M->vfull_off, st);
     }
     if (n_bis > 0) {
-        const int grid_b = std::min(ctx->num_sms * ncpa::wbisect_ctas_per_sm(), (n_bis + 3) / 4);
-        check_launch(ctx, ncpa::launch_wbisect(st, grid_b, d_pinfo, rows.as<double>(), counts.as<int>(),
-                                               bis.as<WorkItem>(), tot.as<int>(), kWmodTol, mu.as<double>(), err));
+        const int grid_b = ctx->num_sms * ncpa::bisect_wmod_ctas_per_sm();
+        check_launch(ctx, ncpa::launch_bisect_wmod(st, grid_b, d_pinfo, rows.as<double>(), counts.as<int>(),
+                                                   bis.as<WorkItem>(), kWmodTol, mu.as<double>(), err,
+                                                   ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr,
+                                                   tot.as<int>()));
     }
     tm.mark("bisect");
     if (n_ev > 0) {

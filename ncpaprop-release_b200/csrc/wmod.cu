@@ -12,11 +12,12 @@
 // in factored form, two doubles per row.  For real k inside the propagating
 // window dT/dk is negative definite (subsonic winds), so the number of
 // negative eigenvalues of T grows by one at each real eigenvalue: the modes
-// are found with Sturm counts in kappa (isolation scan, then per-lane
-// bisection / safeguarded Newton on det T with its kappa-derivative) and each
-// eigenvector is the null vector of T by twisted factorisation (k_eigvec with
-// the WmodRows format, kernels.cu).  Every sweep streams the rows through
-// shared memory by TMA bulk copies.
+// are found with Sturm counts in kappa (the isolation scan here, then the
+// multisection / safeguarded Newton of k_bisect on det T with its
+// kappa-derivative) and each eigenvector is the null vector of T by twisted
+// factorisation (k_bisect and k_eigvec with the WmodRows format,
+// kernels.cu).  Every sweep streams the rows through shared memory by TMA
+// bulk copies.
 #include "device_common.cuh"
 #include "kernels.hpp"
 
@@ -27,10 +28,6 @@ namespace {
 constexpr int kWScanThreads = kScanPoints / 2;  // two shifts per thread
 constexpr int kWsRows = 512;                    // rows per scan ring chunk (8 KB)
 constexpr int kWsBuf = 4;                       // scan ring slots
-constexpr int kWbRows = 256;                    // rows per bisection ring chunk (4 KB)
-constexpr int kWbBuf = 3;                       // bisection ring slots per warp
-constexpr int kWbWarps = 4;                     // warps per bisection CTA
-constexpr int kWMaxRounds = 400;                // bound on bisection / Newton rounds
 
 __device__ __forceinline__ double wscan_x(double lo, double hi, int t) {
     if (t == 0) return lo;
@@ -135,152 +132,16 @@ int launch_wmod_build(cudaStream_t st, int nk, const double* zk, const double* c
 
 
 // ---------------------------------------------------------------------------
-// Sturm sweeps over the rows.  p_{-2} = -g0, p_{-1} = 1,
-// p_i = t_i(kappa) p_{i-1} - p_{i-2}; a negative pivot is a sign change of
-// consecutive p.  The kappa-derivative runs as e_i = t_i e_{i-1} +
-// (U_i d_i + kappa) p_{i-1} - e_{i-2} with d_i = B_i - U_i kappa, which is
-// -1/2 of d p_i / d kappa, so Newton's step is kappa + p / (2 e).
-// ---------------------------------------------------------------------------
-struct WChain {
-    double p0, p1;
-    unsigned prevbit;
-    int cnt;
-    __device__ __forceinline__ void reset(double g0) {
-        p0 = -g0;
-        p1 = 1.0;
-        prevbit = 0u;
-        cnt = 0;
-    }
-    __device__ __forceinline__ void fold(unsigned w) {
-        const unsigned prev = (w >> 1) | (prevbit << 31);
-        cnt += __popc(w ^ prev);
-        prevbit = w & 1u;
-    }
-    __device__ __forceinline__ void step(double2 r, const WmodRows::Shift& s) {
-        const double d = fma(-r.y, s.kap, r.x);
-        const double q = fma(fma(d, d, s.c), p1, -p0);
-        const unsigned b = static_cast<unsigned>(__double2hiint(q)) >> 31;
-        cnt += static_cast<int>(b ^ prevbit);
-        prevbit = b;
-        p0 = p1;
-        p1 = q;
-    }
-};
-
-__device__ __forceinline__ void wchain_rescale(WChain& A) {
-    const int sh = rescale_shift(A.p0, A.p1);
-    if (sh) {
-        const double sc = pow2(-sh);
-        A.p0 *= sc;
-        A.p1 *= sc;
-    }
-}
-
-// 32 rows, two chains interleaved (counts only)
-__device__ __forceinline__ void wword32_pair(WChain& A, WChain& B, const double2* __restrict__ r,
-                                             const WmodRows::Shift& sa, const WmodRows::Shift& sb) {
-    unsigned wa = 0u, wb = 0u;
-    double pa0 = A.p0, pa1 = A.p1, pb0 = B.p0, pb1 = B.p1;
-#pragma unroll
-    for (int u = 0; u < 32; ++u) {
-        const double2 rv = r[u];
-        const double da = fma(-rv.y, sa.kap, rv.x);
-        const double db = fma(-rv.y, sb.kap, rv.x);
-        const double qa = fma(fma(da, da, sa.c), pa1, -pa0);
-        const double qb = fma(fma(db, db, sb.c), pb1, -pb0);
-        wa = __funnelshift_l(__double2hiint(qa), wa, 1);
-        wb = __funnelshift_l(__double2hiint(qb), wb, 1);
-        pa0 = pa1;
-        pa1 = qa;
-        pb0 = pb1;
-        pb1 = qb;
-    }
-    A.p0 = pa0;
-    A.p1 = pa1;
-    B.p0 = pb0;
-    B.p1 = pb1;
-    A.fold(wa);
-    B.fold(wb);
-    wchain_rescale(A);
-    wchain_rescale(B);
-}
-
-// 32 rows, one chain (counts only)
-__device__ __forceinline__ void wword32(WChain& A, const double2* __restrict__ r, const WmodRows::Shift& sa) {
-    unsigned wa = 0u;
-    double pa0 = A.p0, pa1 = A.p1;
-#pragma unroll
-    for (int u = 0; u < 32; ++u) {
-        const double2 rv = r[u];
-        const double da = fma(-rv.y, sa.kap, rv.x);
-        const double qa = fma(fma(da, da, sa.c), pa1, -pa0);
-        wa = __funnelshift_l(__double2hiint(qa), wa, 1);
-        pa0 = pa1;
-        pa1 = qa;
-    }
-    A.p0 = pa0;
-    A.p1 = pa1;
-    A.fold(wa);
-    wchain_rescale(A);
-}
-
-// 32 rows, one chain with its derivative chain (e0, e1)
-__device__ __forceinline__ void wword32_deriv(WChain& A, double& e0, double& e1, const double2* __restrict__ r,
-                                              const WmodRows::Shift& sa) {
-    unsigned wa = 0u;
-    double pa0 = A.p0, pa1 = A.p1;
-#pragma unroll
-    for (int u = 0; u < 32; ++u) {
-        const double2 rv = r[u];
-        const double da = fma(-rv.y, sa.kap, rv.x);
-        const double ta = fma(da, da, sa.c);
-        const double tp = fma(rv.y, da, sa.kap);
-        const double qa = fma(ta, pa1, -pa0);
-        const double ea = fma(ta, e1, fma(tp, pa1, -e0));
-        wa = __funnelshift_l(__double2hiint(qa), wa, 1);
-        pa0 = pa1;
-        pa1 = qa;
-        e0 = e1;
-        e1 = ea;
-    }
-    A.p0 = pa0;
-    A.p1 = pa1;
-    A.fold(wa);
-    const int sh = rescale_shift(fmax(fabs(A.p0), fabs(e0)), fmax(fabs(A.p1), fabs(e1)));
-    if (sh) {
-        const double sc = pow2(-sh);
-        A.p0 *= sc;
-        A.p1 *= sc;
-        e0 *= sc;
-        e1 *= sc;
-    }
-}
-
-__device__ __forceinline__ void wstep_deriv(WChain& A, double& e0, double& e1, double2 rv, const WmodRows::Shift& s) {
-    const double d = fma(-rv.y, s.kap, rv.x);
-    const double t = fma(d, d, s.c);
-    const double tp = fma(rv.y, d, s.kap);
-    const double q = fma(t, A.p1, -A.p0);
-    const double e = fma(t, e1, fma(tp, A.p1, -e0));
-    const unsigned b = static_cast<unsigned>(__double2hiint(q)) >> 31;
-    A.cnt += static_cast<int>(b ^ A.prevbit);
-    A.prevbit = b;
-    A.p0 = A.p1;
-    A.p1 = q;
-    e0 = e1;
-    e1 = e;
-}
-
-// ---------------------------------------------------------------------------
 // Isolation scan: kScanPoints counts per problem on an even grid of
 // [kappa_min, kappa_max] (the layout k_make_items reads); the CTA streams the
-// rows through a kWsBuf-deep TMA ring, each thread runs two shifts.
+// rows through a kWsBuf-deep TMA ring, each thread runs two shifts
+// (WmodRows::pair: p_{-2} = -g0, p_{-1} = 1, p_i = t_i p_{i-1} - p_{i-2}).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kWScanThreads) k_wscan(const ProblemInfo* __restrict__ pinfo,
                                                          const double* __restrict__ rows, int* __restrict__ counts,
                                                          unsigned* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    double2* buf = reinterpret_cast<double2*>(smem_raw);
+    double* buf = reinterpret_cast<double*>(smem_raw);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWsBuf * kWsRows * 16);
     if (threadIdx.x == 0) {
         for (int k = 0; k < kWsBuf; ++k) mbar_init(&bars[k], 1);
@@ -289,36 +150,37 @@ __global__ void __launch_bounds__(kWScanThreads) k_wscan(const ProblemInfo* __re
     __syncthreads();
     const int p = blockIdx.x;
     const ProblemInfo pi = pinfo[p];
-    const double2* src = reinterpret_cast<const double2*>(rows) + pi.s_off;
-    const double lo = pi.k_min * pi.dz, hi = pi.k_max * pi.dz;
+    const double* src = rows + 2 * pi.s_off;
+    const double lo = WmodRows::scan_lo(pi), hi = WmodRows::scan_hi(pi);
     const int t0 = threadIdx.x, t1 = threadIdx.x + kWScanThreads;
-    const WmodRows::Shift sa = WmodRows::shift(wscan_x(lo, hi, t0)), sb = WmodRows::shift(wscan_x(lo, hi, t1));
+    const double xa = wscan_x(lo, hi, t0), xb = wscan_x(lo, hi, t1);
     const int nz = pi.nz;
     const int nch = (nz + kWsRows - 1) / kWsRows;
     if (threadIdx.x == 0)
         for (int c = 0; c < nch && c < kWsBuf; ++c) {
             mbar_expect_tx(&bars[c], kWsRows * 16);
-            tma_load_1d(buf + (size_t)c * kWsRows, src + (size_t)c * kWsRows, kWsRows * 16, &bars[c]);
+            tma_load_1d(buf + (size_t)c * 2 * kWsRows, src + (size_t)c * 2 * kWsRows, kWsRows * 16, &bars[c]);
         }
-    WChain A, B;
-    A.reset(pi.g0);
-    B.reset(pi.g0);
+    SturmState A, B;
+    A.reset();
+    B.reset();
+    A.p0 = B.p0 = WmodRows::p_init(pi);
     for (int c = 0; c < nch; ++c) {
         const int slot = c % kWsBuf;
         mbar_wait_bounded(&bars[slot], (c / kWsBuf) & 1u, err);
-        const double2* b = buf + (size_t)slot * kWsRows;
+        const double* b = buf + (size_t)slot * 2 * kWsRows;
         const int valid = min(kWsRows, nz - c * kWsRows);
         const int nw = valid >> 5;
-        for (int w = 0; w < nw; ++w) wword32_pair(A, B, b + 32 * w, sa, sb);
+        for (int w = 0; w < nw; ++w) WmodRows::pair(A, B, b + 64 * w, xa, xb);
         for (int i = nw * 32; i < valid; ++i) {
-            A.step(b[i], sa);
-            B.step(b[i], sb);
+            WmodRows::step(A, b, i, xa);
+            WmodRows::step(B, b, i, xb);
         }
         __syncthreads();
         if (threadIdx.x == 0 && c + kWsBuf < nch) {
             fence_proxy_async();
             mbar_expect_tx(&bars[slot], kWsRows * 16);
-            tma_load_1d(buf + (size_t)slot * kWsRows, src + (size_t)(c + kWsBuf) * kWsRows, kWsRows * 16,
+            tma_load_1d(buf + (size_t)slot * 2 * kWsRows, src + (size_t)(c + kWsBuf) * 2 * kWsRows, kWsRows * 16,
                         &bars[slot]);
         }
     }
@@ -331,182 +193,6 @@ int launch_wscan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double*
     const size_t sm = (size_t)kWsBuf * kWsRows * 16 + kWsBuf * 8;
     k_wscan<<<P, kWScanThreads, sm, st>>>(pinfo, rows, counts, err);
     return 1;
-}
-
-// ---------------------------------------------------------------------------
-// Per-lane bisection / safeguarded Newton in kappa.  A warp owns a work item
-// of <= 32 consecutive eigen-indices of one problem, lane l eigen-index
-// c_lo + j0 + l, bracket [a, b] from the isolation scan, and streams the
-// problem's rows through its own TMA ring (kWbBuf chunks of kWbRows rows), so
-// warps never wait on each other.  Each round every lane sweeps the rows once
-// at its own point: a lane whose bracket still holds more than one eigenvalue
-// moves to the midpoint, an isolated one takes a Newton step on det T
-// (falling back to the midpoint outside the bracket); the derivative chain
-// runs only in rounds with a Newton lane.  A lane is final when the bracket
-// or the correction is below tol relative to kappa, or when the
-// quadratic-convergence model predicts the next correction below it (two
-// in-bracket steps, fourfold shrink).
-// ---------------------------------------------------------------------------
-struct WbRing {
-    double2* buf;    // [kWbBuf][kWbRows]
-    uint64_t* bars;  // [kWbBuf]
-    unsigned loads;  // identical in all lanes
-};
-
-__device__ __forceinline__ void wbr_issue(WbRing& r, unsigned k, const double2* src) {
-    const int slot = k % kWbBuf;
-    mbar_expect_tx(&r.bars[slot], kWbRows * 16);
-    tma_load_1d(r.buf + (size_t)slot * kWbRows, src, kWbRows * 16, &r.bars[slot]);
-}
-
-// one sweep of the warp's rows at this lane's shift; ratio = p / e (when
-// deriv) for the Newton step kappa + ratio / 2
-__device__ void wb_sweep(const double2* __restrict__ src, int nz, double g0, const WmodRows::Shift& sh, bool deriv,
-                         WbRing& r, unsigned* err, int& cnt, double& ratio) {
-    const int lane = threadIdx.x & 31;
-    const int nch = (nz + kWbRows - 1) / kWbRows;
-    const unsigned base = r.loads;
-    if (lane == 0)
-        for (int c = 0; c < nch && c < kWbBuf; ++c) wbr_issue(r, base + c, src + (size_t)c * kWbRows);
-    __syncwarp();
-    WChain A;
-    A.reset(g0);
-    double e0 = 0.0, e1 = 0.0;
-    for (int c = 0; c < nch; ++c) {
-        const unsigned k = base + c;
-        const int slot = k % kWbBuf;
-        mbar_wait_bounded(&r.bars[slot], (k / kWbBuf) & 1u, err);
-        const double2* b = r.buf + (size_t)slot * kWbRows;
-        const int valid = min(kWbRows, nz - c * kWbRows);
-        const int nw = valid >> 5;
-        if (deriv) {
-            for (int w = 0; w < nw; ++w) wword32_deriv(A, e0, e1, b + 32 * w, sh);
-            for (int i = nw * 32; i < valid; ++i) wstep_deriv(A, e0, e1, b[i], sh);
-        } else {
-            for (int w = 0; w < nw; ++w) wword32(A, b + 32 * w, sh);
-            for (int i = nw * 32; i < valid; ++i) A.step(b[i], sh);
-        }
-        __syncwarp();
-        if (lane == 0 && c + kWbBuf < nch) {
-            fence_proxy_async();
-            wbr_issue(r, base + c + kWbBuf, src + (size_t)(c + kWbBuf) * kWbRows);
-        }
-    }
-    r.loads = base + nch;
-    cnt = A.cnt;
-    ratio = deriv ? A.p1 / e1 : 0.0;
-}
-
-__global__ void __launch_bounds__(kWbWarps * 32) k_wbisect(const ProblemInfo* __restrict__ pinfo,
-                                                           const double* __restrict__ rows,
-                                                           const int* __restrict__ counts,
-                                                           const WorkItem* __restrict__ items,
-                                                           const int* __restrict__ n_items_dev, double tol,
-                                                           double* __restrict__ mu, unsigned* err) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    WbRing r;
-    r.buf = reinterpret_cast<double2*>(smem_raw) + (size_t)wid * kWbBuf * kWbRows;
-    r.bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWbWarps * kWbBuf * kWbRows * 16) + wid * kWbBuf;
-    r.loads = 0;
-    if (lane == 0) {
-        for (int k = 0; k < kWbBuf; ++k) mbar_init(&r.bars[k], 1);
-        fence_mbar_init();
-    }
-    __syncwarp();
-    const int n_items = *n_items_dev;
-    const int warps_total = gridDim.x * kWbWarps;
-    for (int it = blockIdx.x * kWbWarps + wid; it < n_items; it += warps_total) {
-        const WorkItem w = items[it];
-        const ProblemInfo pi = pinfo[w.problem];
-        const int* cnt = counts + (size_t)w.problem * kScanPoints;
-        const double2* src = reinterpret_cast<const double2*>(rows) + pi.s_off;
-        const double lo = pi.k_min * pi.dz, hi = pi.k_max * pi.dz;
-        const int J = pi.c_lo + w.j0 + lane;
-        double a = lo, b = lo, x = lo, dprev = 0.0;
-        int ca = 0, cb = 0, mode = 2;  // 0 bisect, 1 Newton, 2 final
-        if (lane < w.m) {
-            int t0 = 0;
-            for (int t = 0; t < kScanPoints; ++t)
-                if (cnt[t] <= J) t0 = t;
-            int t1 = kScanPoints - 1;
-            for (int t = kScanPoints - 1; t > t0; --t)
-                if (cnt[t] > J) t1 = t;
-            if (cnt[t1] <= J) atomicOr(err, kErrBracket);
-            a = wscan_x(lo, hi, t0);
-            b = wscan_x(lo, hi, t1);
-            ca = cnt[t0];
-            cb = cnt[t1];
-            x = 0.5 * (a + b);
-            mode = (ca == J && cb == J + 1) ? 1 : 0;
-        }
-        for (int round = 0; round < kWMaxRounds; ++round) {
-            if (__ballot_sync(0xffffffffu, mode != 2) == 0u) break;
-            const bool deriv = __any_sync(0xffffffffu, mode == 1);
-            int c;
-            double ratio;
-            wb_sweep(src, pi.nz, pi.g0, WmodRows::shift(x), deriv, r, err, c, ratio);
-            if (mode == 0) {
-                if (c <= J) {
-                    a = x;
-                    ca = c;
-                } else {
-                    b = x;
-                    cb = c;
-                }
-                if (!(b - a > tol * b)) mode = 2;
-                else if (ca == J && cb == J + 1) mode = 1;
-                x = 0.5 * (a + b);
-            } else if (mode == 1) {
-                if (c <= J) {
-                    a = x;
-                    ca = c;
-                } else {
-                    b = x;
-                    cb = c;
-                }
-                const double step = 0.5 * ratio;  // kappa_new = x + step
-                const double ad = fabs(step);
-                if (ad <= tol * x) {
-                    x = fmin(fmax(x + step, a), b);
-                    mode = 2;
-                } else {
-                    const double xn = x + step;
-                    const bool ok = isfinite(xn) && xn > a && xn < b;
-                    x = ok ? xn : 0.5 * (a + b);
-                    if (!(b - a > tol * b)) {
-                        mode = 2;
-                    } else if (ok && dprev > 0.0 && ad <= 0.25 * dprev &&
-                               ad * ad * ad <= tol * x * dprev * dprev) {
-                        mode = 2;
-                    }
-                    dprev = ok ? ad : 0.0;
-                }
-            }
-            // a ring wait gave up: abandon the item (warp-uniform decision)
-            if (__any_sync(0xffffffffu, (*((volatile unsigned*)err) & kErrTimeout) != 0u)) break;
-        }
-        if (lane < w.m) mu[pi.off + w.j0 + lane] = x;
-    }
-}
-
-static size_t wbisect_smem() { return (size_t)kWbWarps * (kWbBuf * kWbRows * 16 + kWbBuf * 8); }
-
-int launch_wbisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* rows, const int* counts,
-                   const WorkItem* items, const int* n_items_dev, double tol, double* mu, unsigned* err) {
-    if (grid <= 0) return 0;
-    const size_t sm = wbisect_smem();
-    cudaFuncSetAttribute(k_wbisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_wbisect<<<grid, kWbWarps * 32, sm, st>>>(pinfo, rows, counts, items, n_items_dev, tol, mu, err);
-    return 1;
-}
-
-int wbisect_ctas_per_sm() {
-    int n = 1;
-    const size_t sm = wbisect_smem();
-    cudaFuncSetAttribute(k_wbisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_wbisect, kWbWarps * 32, sm) != cudaSuccess) n = 1;
-    return n < 1 ? 1 : n;
 }
 
 }  // namespace ncpa
