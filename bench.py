@@ -345,6 +345,7 @@ def run_ours(args):
         flops = 3.0 * sturm_steps  # over the bis_n timed launches
         achieved = flops / (bis_ms / 1e3) / 1e12 if bis_ms > 0 else None
         cpu = cpu_baseline(freqs, max_seconds=args.cpu_seconds)
+        cpu_lapack = lapack_baseline(freqs) if not args.no_lapack else None
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_dev / args.steps, 4), "higher_is_better": True,
@@ -369,6 +370,7 @@ def run_ours(args):
             "plain_gpu": {"value": round(plain_rate, 2), "unit": METRIC,
                           "what": "one ncpa_ess_solve + TL per frequency, same workload"},
             "cpu_baseline": cpu,
+            "cpu_lapack": cpu_lapack,
             "modal_sum": ms_leg,
             "serving": sv_leg,
             "sweep": sw_leg,
@@ -760,6 +762,62 @@ def cpu_baseline(freqs, max_seconds=20.0, az=90.0):
             "sample": "%d of the 256 frequencies (every 16th), Nz=20000, eigen-solve + 1-D TL each" % done}
 
 
+def _lapack_eigen(job):
+    """dstebz (bisection, eigenvalues in the window) + dstein (inverse
+    iteration, eigenvectors) on one problem's matrix A = S / h^2."""
+    from scipy.linalg import lapack
+
+    d, e, lo, hi = job
+    m, w, iblock, isplit, info = lapack.dstebz(d, e, 1, lo, hi, 0, 0, 0.0, "E")
+    if info != 0:
+        return -1
+    z, info = lapack.dstein(d, e, w[:m], iblock, isplit)
+    return int(m) if info == 0 else -1
+
+
+def _lapack_ready(_):
+    from scipy.linalg import lapack  # noqa: F401  (import cost outside the timed region)
+
+    return 0
+
+
+def lapack_baseline(freqs, max_seconds=20.0, az=90.0, every=32):
+    """LAPACK on the host cores: the matrices of every 32nd frequency are
+    assembled by the oracle (untimed), then dstebz + dstein run one problem per
+    process of a spawn-started pool (no TL); value = problems per second."""
+    import multiprocessing as mp
+
+    O, pp, prm = _oracle_setup()
+    jobs, modes = [], 0
+    for f in freqs[::every]:
+        ms = O.solve_problem(pp, prm, float(f), az, keep_matrix=True)
+        h2 = ms.dz * ms.dz
+        jobs.append((ms.s / h2, np.full(len(ms.s) - 1, 1.0 / h2), ms.k_min ** 2, ms.k_max ** 2))
+        modes += ms.M
+    n_proc = max(1, min(len(jobs), os.cpu_count() or 1))
+    # one BLAS/OpenMP thread per worker: the pool supplies the parallelism
+    # (threaded BLAS in every worker oversubscribes the cores ~100x)
+    saved = {k: os.environ.get(k) for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS")}
+    os.environ.update({k: "1" for k in saved})
+    try:
+        with mp.get_context("spawn").Pool(n_proc) as pool:
+            pool.map(_lapack_ready, range(n_proc))
+            t0 = time.perf_counter()
+            res = pool.map(_lapack_eigen, jobs, chunksize=1)
+            el = time.perf_counter() - t0
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    return {"value": round(len(jobs) / el, 3), "unit": METRIC, "cores": n_proc, "kind": "lapack",
+            "sample": "%d of the 256 frequencies (one in %d), Nz=%d, %d modes: scipy dstebz + dstein per problem, "
+                      "one problem per process, no TL%s" % (len(jobs), every, NZ, modes,
+                                                            "" if min(res) >= 0 else " (LAPACK reported an error)"),
+            "seconds": round(el, 3)}
+
+
 def run_reference(args):
     rank, world, local = _dist()
     if rank != 0:
@@ -809,6 +867,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the served request-stream leg")
     ap.add_argument("--no-sweep", action="store_true", help="skip the 360-azimuth mixed-grid sweep leg")
     ap.add_argument("--no-wmod", action="store_true", help="skip the wide-angle (WMod) dispersion leg")
+    ap.add_argument("--no-lapack", action="store_true", help="skip the LAPACK (dstebz/dstein) CPU leg")
+    ap.add_argument("--only-lapack", action="store_true", help="run only the LAPACK CPU leg and print its JSON")
     ap.add_argument("--only-wmod", action="store_true",
                     help="run only the wide-angle dispersion leg and print its JSON (for profiler runs)")
     ap.add_argument("--only-modal-sum", action="store_true",
@@ -832,6 +892,9 @@ def main():
         ctx = ncpa_gpu.Context(0)
         print(json.dumps(sweep_leg(ctx, torch.cuda.ExternalStream(ctx.stream_ptr), reps=1)), flush=True)
         ctx.close()
+        return
+    if args.only_lapack:
+        print(json.dumps(lapack_baseline(workloads.broadband_freqs(NFREQ, 0.5))), flush=True)
         return
     if args.only_wmod:
         import torch

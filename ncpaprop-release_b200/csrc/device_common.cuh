@@ -187,7 +187,9 @@ struct SturmState {
         }
     }
     // 32 steps carrying the x-derivative of the recurrence as well:
-    // d_i = (s_i - x) d_{i-1} - p_{i-1} - d_{i-2}; rescaled with p
+    // d_i = (s_i - x) d_{i-1} - (p_{i-1} + d_{i-2}); rescaled with p.  The sum
+    // p_{i-1} + d_{i-2} is ready a step early, so the derivative chain costs
+    // one dependent FMA per step, like p.
     __device__ __forceinline__ void word32_deriv(const double* __restrict__ s, double x, double& d0, double& d1) {
         unsigned w = 0u;
 #pragma unroll
@@ -195,10 +197,10 @@ struct SturmState {
             double2 sv = *reinterpret_cast<const double2*>(s + u);
             double a0 = sv.x - x;
             double q0 = fma(a0, p1, -p0);
-            double e0 = fma(a0, d1, -p1) - d0;
+            double e0 = fma(a0, d1, -(p1 + d0));
             double a1 = sv.y - x;
             double q1 = fma(a1, q0, -p1);
-            double e1 = fma(a1, e0, -q0) - d1;
+            double e1 = fma(a1, e0, -(q0 + d1));
             w = __funnelshift_l(__double2hiint(q0), w, 1);
             w = __funnelshift_l(__double2hiint(q1), w, 1);
             p0 = q0;
@@ -221,7 +223,7 @@ struct SturmState {
     __device__ __forceinline__ void step_deriv(double si, double x, double& d0, double& d1) {
         double a = si - x;
         double q = fma(a, p1, -p0);
-        double e = fma(a, d1, -p1) - d0;
+        double e = fma(a, d1, -(p1 + d0));
         unsigned b = static_cast<unsigned>(__double2hiint(q)) >> 31;
         cnt += static_cast<int>(b ^ prevbit);
         prevbit = b;
@@ -314,10 +316,10 @@ __device__ __forceinline__ void sturm_word32_deriv_pair(SturmState& A, double& d
         const double a0 = sv.x - xa, a1 = sv.y - xa;
         const double qa0 = fma(a0, pa1, -pa0);
         const double qb0 = fma(sv.x - xb, pb1, -pb0);
-        const double e0 = fma(a0, d1, -pa1) - d0;
+        const double e0 = fma(a0, d1, -(pa1 + d0));
         const double qa1 = fma(a1, qa0, -pa1);
         const double qb1 = fma(sv.y - xb, qb0, -pb1);
-        const double e1 = fma(a1, e0, -qa0) - d1;
+        const double e1 = fma(a1, e0, -(qa0 + d1));
         wa = __funnelshift_l(__double2hiint(qa0), wa, 1);
         wb = __funnelshift_l(__double2hiint(qb0), wb, 1);
         wa = __funnelshift_l(__double2hiint(qa1), wa, 1);
