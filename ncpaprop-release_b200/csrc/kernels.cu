@@ -108,17 +108,32 @@ int launch_ceff_knots(cudaStream_t st, int n, int n_az, const double* az, const 
     return 1;
 }
 
-// Sutherland-Bass absorption [Np/m] (AtmosphericModel.cpp:86-219); z in km
-__device__ double attn_sutherland_bass(double z, double T_z, double P_z, double D_z, double freq) {
+// Sutherland-Bass absorption [Np/m] (AtmosphericModel.cpp:86-219), split into
+// its frequency-independent part at a knot (sound speed, viscosity, mole
+// fractions, rotational collision number, vibrational relaxation frequencies
+// and strengths: every pow / exp of the model) and the per-frequency rational
+// part, so a thread evaluates one knot's part once for kSbFreqs frequencies.
+struct SbKnot {
+    double c;       // sound speed sqrt(1.4 P / rho)
+    double nu_f;    // nu / f = 8 pi mu / (3 P)
+    double nn;      // (4/5) sqrt(3/7) Z_rot
+    double x_on;    // (X_O2 + X_N2) / 0.9903
+    double am[4];   // A_max / c of the four vibrational modes
+    double fv[4];   // their relaxation frequencies
+};
+
+// z in km
+__device__ SbKnot sb_knot(double z, double T_z, double P_z, double D_z) {
     const double mu_o = 18.192E-6, T_o = 293.15, P_o = 101325, S = 117.0;
     const double Cv_R[4] = {5.0 / 2.0, 5.0 / 2.0, 3.0, 3.0};
     const double Cp_R[4] = {7.0 / 2.0, 7.0 / 2.0, 4.0, 4.0};
     const double theta[4] = {2239.1, 3352.0, 915.0, 1037.0};
     const double PI = kPi;
-    double c_snd_z = sqrt(1.4 * P_z / D_z);
-    double mu = mu_o * sqrt(T_z / T_o) * ((1.0 + S / T_o) / (1.0 + S / T_z));
-    double nu = (8.0 * PI * freq * mu) / (3.0 * P_z);
-    double z2 = pow(z, 2), z3 = pow(z, 3), z4 = pow(z, 4), z5 = pow(z, 5);
+    SbKnot K;
+    K.c = sqrt(1.4 * P_z / D_z);
+    const double mu = mu_o * sqrt(T_z / T_o) * ((1.0 + S / T_o) / (1.0 + S / T_z));
+    K.nu_f = (8.0 * PI * mu) / (3.0 * P_z);
+    const double z2 = z * z, z3 = z2 * z, z4 = z3 * z, z5 = z4 * z;
     double X[7];
     X[0] = (z > 90.0) ? pow(10.0, 49.296 - (1.5524 * z) + (1.8714E-2 * z2) - (1.1069E-4 * z3) + (3.199E-7 * z4) -
                                       (3.6211E-10 * z5))
@@ -137,65 +152,82 @@ __device__ double attn_sutherland_bass(double z, double T_z, double P_z, double 
                                       (2.4265E-7 * z4) - (1.2500E-09 * z5))
                       : pow(10.0, -1.7491 + (4.4986E-2 * z) - (6.8549E-2 * z2) + (5.4639E-3 * z3) -
                                       (1.5539E-4 * z4) + (1.5063E-06 * z5));
-    double X_ON = (X[0] + X[1]) / 0.9903;
-    double Z_rot_0 = 54.1 * exp(-17.3 * (pow(T_z, -1.0 / 3.0)));
-    double Z_rot_1 = 63.3 * exp(-16.7 * (pow(T_z, -1.0 / 3.0)));
-    double Z_rot_ = 1.0 / ((X[1] / Z_rot_1) + (X[0] / Z_rot_0));
-    double sigma = 5.0 / sqrt(21.0);
-    double nn = (4.0 / 5.0) * sqrt(3.0 / 7.0) * Z_rot_;
-    double chi = 3.0 * nn * nu / 4.0;
-    double cchi = 2.36 * chi;
-    double nu2 = pow(nu, 2), cchi2 = pow(cchi, 2);
-    double a_cl = (2 * PI * freq / c_snd_z) *
-                  sqrt(0.5 * (sqrt(1 + nu2) - 1) * (1 + cchi2) / ((1 + nu2) * (1 + pow(sigma * cchi, 2))));
-    double a_rot = (2 * PI * freq / c_snd_z) * X_ON * ((pow(sigma, 2) - 1) * chi / (2 * sigma)) *
-                   sqrt(0.5 * (sqrt(1 + nu2) + 1) / ((1 + nu2) * (1 + cchi2)));
-    double a_diff = 0.003 * a_cl;
-    double Tr = pow(T_z / T_o, -1.0 / 3.0) - 1.0;
-    double A1 = (X[0] + X[1]) * 24.0 * exp(-9.16 * Tr);
-    double A2 = (X[4] + X[5]) * 2400.0;
-    double B = 40400.0 * exp(10.0 * Tr);
-    double C = 0.02 * exp(-11.2 * Tr);
-    double Dd = 0.391 * exp(8.41 * Tr);
-    double E = 9.0 * exp(-19.9 * Tr);
-    double F = 60000.0;
-    double G = 28000.0 * exp(-4.17 * Tr);
-    double H = 22000.0 * exp(-7.68 * Tr);
-    double I_ = 15100.0 * exp(-10.4 * Tr);
-    double J = 11500.0 * exp(-9.17 * Tr);
-    double K = (8.48E08) * exp(9.17 * Tr);
-    double L = exp(-7.72 * Tr);
-    double ZZ = H * X[2] + I_ * (X[0] + 0.5 * X[4]) + J * (X[1] + 0.5 * X[5]) + K * (X[6] + X[3]);
-    double hu = 100.0 * (X[3] + X[6]);
-    double f_vib[4];
-    double pf = (P_z / P_o) * (mu_o / mu);
-    f_vib[0] = pf * (A1 + A2 + B * hu * (C + hu) * (Dd + hu));
-    f_vib[1] = pf * (E + F * X[3] + G * X[6]);
-    f_vib[2] = pf * ZZ;
-    f_vib[3] = pf * (1.2E5) * L;
+    K.x_on = (X[0] + X[1]) / 0.9903;
+    const double tc = pow(T_z, -1.0 / 3.0);
+    const double Z_rot_0 = 54.1 * exp(-17.3 * tc);
+    const double Z_rot_1 = 63.3 * exp(-16.7 * tc);
+    const double Z_rot_ = 1.0 / ((X[1] / Z_rot_1) + (X[0] / Z_rot_0));
+    K.nn = (4.0 / 5.0) * sqrt(3.0 / 7.0) * Z_rot_;
+    const double Tr = pow(T_z / T_o, -1.0 / 3.0) - 1.0;
+    const double A1 = (X[0] + X[1]) * 24.0 * exp(-9.16 * Tr);
+    const double A2 = (X[4] + X[5]) * 2400.0;
+    const double B = 40400.0 * exp(10.0 * Tr);
+    const double C = 0.02 * exp(-11.2 * Tr);
+    const double Dd = 0.391 * exp(8.41 * Tr);
+    const double E = 9.0 * exp(-19.9 * Tr);
+    const double F = 60000.0;
+    const double G = 28000.0 * exp(-4.17 * Tr);
+    const double H = 22000.0 * exp(-7.68 * Tr);
+    const double I_ = 15100.0 * exp(-10.4 * Tr);
+    const double J = 11500.0 * exp(-9.17 * Tr);
+    const double Kc = (8.48E08) * exp(9.17 * Tr);
+    const double L = exp(-7.72 * Tr);
+    const double ZZ = H * X[2] + I_ * (X[0] + 0.5 * X[4]) + J * (X[1] + 0.5 * X[5]) + Kc * (X[6] + X[3]);
+    const double hu = 100.0 * (X[3] + X[6]);
+    const double pf = (P_z / P_o) * (mu_o / mu);
+    K.fv[0] = pf * (A1 + A2 + B * hu * (C + hu) * (Dd + hu));
+    K.fv[1] = pf * (E + F * X[3] + G * X[6]);
+    K.fv[2] = pf * ZZ;
+    K.fv[3] = pf * (1.2E5) * L;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const double et = exp(-theta[m] / T_z);
+        const double tt = theta[m] / T_z, om = 1 - et;
+        const double C_R = ((tt * tt) * et) / (om * om);
+        const double A_max = (X[m] * (PI / 2) * C_R) / (Cp_R[m] * (Cv_R[m] + C_R));
+        K.am[m] = A_max / K.c;
+    }
+    return K;
+}
+
+__device__ double sb_alpha(const SbKnot& K, double freq) {
+    const double PI = kPi;
+    const double sigma = 5.0 / sqrt(21.0);
+    const double nu = K.nu_f * freq;
+    const double chi = 3.0 * K.nn * nu / 4.0;
+    const double cchi = 2.36 * chi;
+    const double nu2 = nu * nu, cchi2 = cchi * cchi, sc = sigma * cchi;
+    const double r1 = sqrt(1 + nu2);
+    const double kf = 2 * PI * freq / K.c;
+    const double a_cl = kf * sqrt(0.5 * (r1 - 1) * (1 + cchi2) / ((1 + nu2) * (1 + sc * sc)));
+    const double a_rot = kf * K.x_on * ((sigma * sigma - 1) * chi / (2 * sigma)) *
+                         sqrt(0.5 * (r1 + 1) / ((1 + nu2) * (1 + cchi2)));
+    const double a_diff = 0.003 * a_cl;
     double a_vib = 0.0;
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-        double et = exp(-theta[m] / T_z);
-        double C_R = ((pow(theta[m] / T_z, 2)) * et) / (pow(1 - et, 2));
-        double A_max = (X[m] * (PI / 2) * C_R) / (Cp_R[m] * (Cv_R[m] + C_R));
-        a_vib = a_vib + (A_max / c_snd_z) * ((2 * (pow(freq, 2)) / f_vib[m]) / (1 + pow(freq / f_vib[m], 2)));
+        const double q = freq / K.fv[m];
+        a_vib = a_vib + K.am[m] * ((2 * (freq * freq) / K.fv[m]) / (1 + q * q));
     }
     return a_cl + a_rot + a_diff + a_vib;
 }
 
+constexpr int kSbFreqs = 8;  // frequencies per thread of k_alpha_knots
+
 __global__ void k_alpha_knots(int n, int n_f, const double* __restrict__ freqs, const double* __restrict__ z,
                               const double* __restrict__ t, const double* __restrict__ p,
                               const double* __restrict__ rho, double* __restrict__ alpha) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    int f = blockIdx.y;
-    if (k >= n || f >= n_f) return;
-    alpha[(size_t)f * n + k] = attn_sutherland_bass(z[k] * 0.001, t[k], p[k], rho[k], freqs[f]);
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f0 = blockIdx.y * kSbFreqs;
+    if (k >= n) return;
+    const SbKnot K = sb_knot(z[k] * 0.001, t[k], p[k], rho[k]);
+    const int f1 = min(n_f, f0 + kSbFreqs);
+    for (int f = f0; f < f1; ++f) alpha[(size_t)f * n + k] = sb_alpha(K, freqs[f]);
 }
 
 int launch_alpha_knots(cudaStream_t st, int n, int n_f, const double* freqs, const double* z, const double* t,
                        const double* p, const double* rho, double* alpha) {
-    dim3 grid((n + 127) / 128, n_f);
+    dim3 grid((n + 127) / 128, (n_f + kSbFreqs - 1) / kSbFreqs);
     k_alpha_knots<<<grid, 128, 0, st>>>(n, n_f, freqs, z, t, p, rho, alpha);
     return 1;
 }
@@ -221,24 +253,50 @@ int launch_grid_common(cudaStream_t st, int nk, const double* zk, const double* 
     return 1;
 }
 
-// w_i = ((omega / c_T) alpha_i) 2, the integrand weight of doPerturb
+// w_i = ((omega / c_T) alpha_i) 2, the integrand weight of doPerturb.  A
+// thread takes one grid point and kAwFreqs frequencies: the knot search is
+// shared, each alpha_f(z_i) is spline_get's expression.
+constexpr int kAwFreqs = 8;
+
 __global__ void k_attn_weight(int nk, const double* __restrict__ zk, const double* __restrict__ alpha,
                               const double* __restrict__ acoef, int n_f, const double* __restrict__ freqs,
                               int nz, double z_min, double dz_grid, const double* __restrict__ ct_g,
                               double* __restrict__ w, int wstride) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int f = blockIdx.y;
-    if (i >= nz || f >= n_f) return;
-    double h = z_min + i * dz_grid;
-    double a = spline_get(nk, zk, alpha + (size_t)f * nk, acoef + (size_t)f * 4 * (nk - 1), h);
-    double omega = 2 * kPi * freqs[f];
-    w[(size_t)f * wstride + i] = ((omega / ct_g[i]) * a) * 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f0 = blockIdx.y * kAwFreqs;
+    if (i >= nz) return;
+    const double h = z_min + i * dz_grid;
+    int where = 0, kn = 0;  // 0 inside the knots, 1 above, 2 below
+    double t = 0.0;
+    if (h > zk[nk - 1]) {
+        where = 1;
+    } else if (h < zk[0]) {
+        where = 2;
+    } else {
+        kn = knot_search(nk, zk, h);
+        t = h - zk[kn];
+    }
+    const double ct = ct_g[i];
+    const int f1 = min(n_f, f0 + kAwFreqs);
+    for (int f = f0; f < f1; ++f) {
+        double a;
+        if (where == 1) {
+            a = alpha[(size_t)f * nk + nk - 1];
+        } else if (where == 2) {
+            a = alpha[(size_t)f * nk];
+        } else {
+            const double* c = acoef + (size_t)f * 4 * (nk - 1) + 4 * kn;
+            a = c[3] + t * (c[2] + t * (c[1] + t * c[0]));
+        }
+        const double omega = 2 * kPi * freqs[f];
+        w[(size_t)f * wstride + i] = ((omega / ct) * a) * 2;
+    }
 }
 
 int launch_attn_weight(cudaStream_t st, int nk, const double* zk, const double* alpha, const double* acoef,
                        int n_f, const double* freqs, int nz, double z_min, double dz_grid, const double* ct_g,
                        double* w, int wstride) {
-    dim3 grid((nz + 255) / 256, n_f);
+    dim3 grid((nz + 255) / 256, (n_f + kAwFreqs - 1) / kAwFreqs);
     k_attn_weight<<<grid, 256, 0, st>>>(nk, zk, alpha, acoef, n_f, freqs, nz, z_min, dz_grid, ct_g, w, wstride);
     return 1;
 }
@@ -257,46 +315,57 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
+// One thread per (azimuth, grid point) and kBmFreqs frequencies of the group:
+// c_eff is sampled once and every problem's entries use the same expressions.
+constexpr int kBmFreqs = 16;
+
 __global__ void __launch_bounds__(256) k_build_matrix(int nk, const double* __restrict__ zk,
                                                       const double* __restrict__ ceffk,
-                                                      const double* __restrict__ ceffcoef, int n_az,
+                                                      const double* __restrict__ ceffcoef, int n_az, int n_f,
                                                       ProblemInfo* __restrict__ pinfo, int nz, int nz_pad,
                                                       double z_min, double dz_grid, double dz, double admittance,
                                                       double* __restrict__ s, double* __restrict__ kz2,
                                                       double* __restrict__ g) {
-    const int p = blockIdx.y;
+    const int a = blockIdx.y;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int a = p % n_az;
+    const int f0 = blockIdx.z * kBmFreqs, f1 = min(n_f, f0 + kBmFreqs);
     const double* ck = ceffk + (size_t)a * nk;
     const double* cc = ceffcoef + (size_t)a * 4 * (nk - 1);
-    const double omega = pinfo[p].omega;
     const double h2 = dz * dz;
     const double bnd = (1. / (dz * admittance + 1)) / (dz * dz);
     double cmin = 1e300, cmax = -1e300;
+    const int top = nz - (nz / 10);
+    const int itop = top + 1 < nz ? top + 1 : nz - 1;
     if (i < nz) {
-        double c = spline_get(nk, zk, ck, cc, z_min + i * dz_grid);
-        double t = omega / c;
-        double d = t * t;
-        if (kz2) kz2[(size_t)p * nz_pad + i] = d;
-        if (g) g[(size_t)p * nz_pad + i] = 1.0 / (c * c);
+        const double c = spline_get(nk, zk, ck, cc, z_min + i * dz_grid);
+        // last row of the assembled matrix repeats diag[nz-2] (EigenEngine.cpp:59-71)
+        const double c2 = i < nz - 1 ? c : spline_get(nk, zk, ck, cc, z_min + (nz - 2) * dz_grid);
         cmin = cmax = c;
-        double sd;
-        if (i < nz - 1) {
-            sd = (i == 0) ? (bnd + d) : d;
-        } else {  // last row of the assembled matrix repeats diag[nz-2] (EigenEngine.cpp:59-71)
-            double c2 = spline_get(nk, zk, ck, cc, z_min + (nz - 2) * dz_grid);
-            double t2 = omega / c2;
-            sd = t2 * t2;
-            if (nz - 2 == 0) sd = bnd + sd;
+        for (int f = f0; f < f1; ++f) {
+            const int p = f * n_az + a;
+            const double omega = pinfo[p].omega;
+            double t = omega / c;
+            double d = t * t;
+            if (kz2) kz2[(size_t)p * nz_pad + i] = d;
+            if (g) g[(size_t)p * nz_pad + i] = 1.0 / (c * c);
+            double sd;
+            if (i < nz - 1) {
+                sd = (i == 0) ? (bnd + d) : d;
+            } else {
+                double t2 = omega / c2;
+                sd = t2 * t2;
+                if (nz - 2 == 0) sd = bnd + sd;
+            }
+            s[(size_t)p * nz_pad + i] = sd * h2 - 2.0;
+            if (i == 0) pinfo[p].ceff_grnd = c;
+            if (i == itop) pinfo[p].ceff_top = c;
         }
-        s[(size_t)p * nz_pad + i] = sd * h2 - 2.0;
-        if (i == 0) pinfo[p].ceff_grnd = c;
-        int top = nz - (nz / 10);
-        int itop = top + 1 < nz ? top + 1 : nz - 1;
-        if (i == itop) pinfo[p].ceff_top = c;
     } else if (i < nz_pad) {
-        s[(size_t)p * nz_pad + i] = 0.0;
-        if (g) g[(size_t)p * nz_pad + i] = 0.0;
+        for (int f = f0; f < f1; ++f) {
+            const int p = f * n_az + a;
+            s[(size_t)p * nz_pad + i] = 0.0;
+            if (g) g[(size_t)p * nz_pad + i] = 0.0;
+        }
     }
     cmin = warp_min(cmin);
     cmax = warp_max(cmax);
@@ -315,8 +384,11 @@ __global__ void __launch_bounds__(256) k_build_matrix(int nk, const double* __re
         cmin = fmin(cmin, smin[0]);
         cmax = fmax(cmax, smax[0]);
         if (cmin < 1e300) {
-            atomicMin(&pinfo[p].ceffmin_bits, (unsigned long long)__double_as_longlong(cmin));
-            atomicMax(&pinfo[p].ceffmax_bits, (unsigned long long)__double_as_longlong(cmax));
+            for (int f = f0; f < f1; ++f) {
+                const int p = f * n_az + a;
+                atomicMin(&pinfo[p].ceffmin_bits, (unsigned long long)__double_as_longlong(cmin));
+                atomicMax(&pinfo[p].ceffmax_bits, (unsigned long long)__double_as_longlong(cmax));
+            }
         }
     }
 }
@@ -324,8 +396,10 @@ __global__ void __launch_bounds__(256) k_build_matrix(int nk, const double* __re
 int launch_build_matrix(cudaStream_t st, int nk, const double* zk, const double* ceffk, const double* ceffcoef,
                         int n_az, int P, ProblemInfo* pinfo, int nz, int nz_pad, double z_min, double dz_grid,
                         double dz, double admittance, double* s, double* kz2, double* g) {
-    dim3 grid((nz_pad + 255) / 256, P);
-    k_build_matrix<<<grid, 256, 0, st>>>(nk, zk, ceffk, ceffcoef, n_az, pinfo, nz, nz_pad, z_min, dz_grid, dz,
+    if (n_az < 1 || P % n_az != 0) return -1;
+    const int n_f = P / n_az;
+    dim3 grid((nz_pad + 255) / 256, n_az, (n_f + kBmFreqs - 1) / kBmFreqs);
+    k_build_matrix<<<grid, 256, 0, st>>>(nk, zk, ceffk, ceffcoef, n_az, n_f, pinfo, nz, nz_pad, z_min, dz_grid, dz,
                                          admittance, s, kz2, g);
     return 1;
 }
