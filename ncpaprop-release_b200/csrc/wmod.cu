@@ -61,38 +61,45 @@ int launch_wc_knots(cudaStream_t st, int n, int n_az, const double* az, const do
 // (WModeSolver.cpp:196-208), with the matrix spacing dz, and the ground term
 // g0 = h^2 / (dz^2 (dz admittance + 1)); also (omega/c_eff)^2 for the WKB
 // search and the c_eff extrema / ground / top values of getModalTrace
-// (WModeSolver.cpp:530-629).  Padding rows are zero.
+// (WModeSolver.cpp:530-629).  Padding rows are zero.  One thread per
+// (azimuth, grid point) and kWbFreqs frequencies: the profile is sampled once.
+constexpr int kWbFreqs = 16;
+
 __global__ void __launch_bounds__(256) k_wmod_build(int nk, const double* __restrict__ zk,
                                                     const double* __restrict__ c0k, const double* __restrict__ c0c,
                                                     const double* __restrict__ wck, const double* __restrict__ wcc,
                                                     const double* __restrict__ ceffk,
-                                                    const double* __restrict__ ceffc, int n_az,
+                                                    const double* __restrict__ ceffc, int n_az, int n_f,
                                                     ProblemInfo* __restrict__ pinfo, int nz, int nz_pad,
                                                     double z_min, double dz_grid, double dz, double admittance,
                                                     double2* __restrict__ rows, double* __restrict__ kz2) {
-    const int p = blockIdx.y;
+    const int az = blockIdx.y;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int az = p % n_az;
-    const double omega = pinfo[p].omega;
+    const int f0 = blockIdx.z * kWbFreqs, f1 = min(n_f, f0 + kWbFreqs);
     double cmin = 1e300, cmax = -1e300;
-    if (i >= nz && i < nz_pad) rows[(size_t)p * nz_pad + i] = make_double2(0.0, 0.0);
+    const int top = nz - (nz / 10);
+    const int itop = top + 1 < nz ? top + 1 : nz - 1;
+    if (i >= nz && i < nz_pad)
+        for (int f = f0; f < f1; ++f) rows[(size_t)(f * n_az + az) * nz_pad + i] = make_double2(0.0, 0.0);
     if (i < nz) {
         const double z = z_min + i * dz_grid;
         const double c0 = spline_get(nk, zk, c0k, c0c, z);
         const double wc = spline_get(nk, zk, wck + (size_t)az * nk, wcc + (size_t)az * 4 * (nk - 1), z);
         const double ce = spline_get(nk, zk, ceffk + (size_t)az * nk, ceffc + (size_t)az * 4 * (nk - 1), z);
-        const size_t o = (size_t)p * nz_pad + i;
-        rows[o] = make_double2(dz * (omega / c0), wc / c0);
-        if (i == 0) pinfo[p].g0 = 1.0 / (dz * admittance + 1.0);
-        if (kz2) {
-            const double te = omega / ce;
-            kz2[o] = te * te;
-        }
         cmin = cmax = ce;
-        if (i == 0) pinfo[p].ceff_grnd = ce;
-        const int top = nz - (nz / 10);
-        const int itop = top + 1 < nz ? top + 1 : nz - 1;
-        if (i == itop) pinfo[p].ceff_top = ce;
+        for (int f = f0; f < f1; ++f) {
+            const int p = f * n_az + az;
+            const double omega = pinfo[p].omega;
+            const size_t o = (size_t)p * nz_pad + i;
+            rows[o] = make_double2(dz * (omega / c0), wc / c0);
+            if (i == 0) pinfo[p].g0 = 1.0 / (dz * admittance + 1.0);
+            if (kz2) {
+                const double te = omega / ce;
+                kz2[o] = te * te;
+            }
+            if (i == 0) pinfo[p].ceff_grnd = ce;
+            if (i == itop) pinfo[p].ceff_top = ce;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -114,8 +121,11 @@ __global__ void __launch_bounds__(256) k_wmod_build(int nk, const double* __rest
         cmin = fmin(cmin, smin[0]);
         cmax = fmax(cmax, smax[0]);
         if (cmin < 1e300) {
-            atomicMin(&pinfo[p].ceffmin_bits, (unsigned long long)__double_as_longlong(cmin));
-            atomicMax(&pinfo[p].ceffmax_bits, (unsigned long long)__double_as_longlong(cmax));
+            for (int f = f0; f < f1; ++f) {
+                const int p = f * n_az + az;
+                atomicMin(&pinfo[p].ceffmin_bits, (unsigned long long)__double_as_longlong(cmin));
+                atomicMax(&pinfo[p].ceffmax_bits, (unsigned long long)__double_as_longlong(cmax));
+            }
         }
     }
 }
@@ -124,12 +134,13 @@ int launch_wmod_build(cudaStream_t st, int nk, const double* zk, const double* c
                       const double* wck, const double* wcc, const double* ceffk, const double* ceffc, int n_az,
                       int P, ProblemInfo* pinfo, int nz, int nz_pad, double z_min, double dz_grid, double dz,
                       double admittance, double* rows, double* kz2) {
-    dim3 grid((nz_pad + 255) / 256, P);
-    k_wmod_build<<<grid, 256, 0, st>>>(nk, zk, c0k, c0c, wck, wcc, ceffk, ceffc, n_az, pinfo, nz, nz_pad, z_min,
+    if (n_az < 1 || P % n_az != 0) return -1;
+    const int n_f = P / n_az;
+    dim3 grid((nz_pad + 255) / 256, n_az, (n_f + kWbFreqs - 1) / kWbFreqs);
+    k_wmod_build<<<grid, 256, 0, st>>>(nk, zk, c0k, c0c, wck, wcc, ceffk, ceffc, n_az, n_f, pinfo, nz, nz_pad, z_min,
                                        dz_grid, dz, admittance, reinterpret_cast<double2*>(rows), kz2);
     return 1;
 }
-
 
 // ---------------------------------------------------------------------------
 // Isolation scan: kScanPoints counts per problem on an even grid of
