@@ -698,6 +698,271 @@ __device__ void warp_sweep(const double* __restrict__ s, int nz, double p_init, 
     rat0 = mode >= 1 ? Row::newton(A.p1, da1) : 0.0;
 }
 
+// ---------------------------------------------------------------------------
+// Twisted Sturm sweep.  The rows [0, h) run the forward recurrence p
+// (top-down) and the rows [h, n) the backward recurrence q (bottom-up,
+// q_n = 1, q_{n+1} = 0) at the same time, so each chain is half as long and a
+// lane carries twice the independent chains.  With the twist at row h
+// (T - x = N Delta N^T, Delta = diag(D+_0..D+_{h-1}, gamma_h, D-_{h+1}..)):
+//   count = sign changes of p_{-1..h-1} + sign changes of q_{n..h+1}
+//           + [gamma_h < 0],  gamma_h = det / (p_{h-1} q_{h+1}),
+//   det = p_{h-1} q_h - p_{h-2} q_{h+1},
+// and det' follows by the product rule from the chains' derivatives.  The
+// inertia is that of the sequential count; the scan's counts, which fix the
+// mode numbers, stay sequential.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned sgnbit(double v) { return static_cast<unsigned>(__double2hiint(v)) >> 31; }
+
+// count of the twisted factorisation from the final forward chain F and
+// backward chain B (B.p1 = q_h, B.p0 = q_{h+1}); det returned
+__device__ __forceinline__ int twist_count(const SturmState& F, const SturmState& B, double& det) {
+    det = F.p1 * B.p1 - F.p0 * B.p0;
+    const int last = static_cast<int>(sgnbit(B.p1) ^ sgnbit(B.p0));
+    const int gam = static_cast<int>(sgnbit(det) ^ sgnbit(F.p1) ^ sgnbit(B.p0));
+    return F.cnt + B.cnt - last + gam;
+}
+
+// 32 front rows (ascending, fb) and 32 back rows (descending, bb) in one
+// loop.  kMode 0: four count chains (A, B forward and backward); 1: A chains
+// with derivatives + B chains; 2: A chains with derivatives only.
+template <int kMode>
+__device__ __forceinline__ void tw_word(EssRows, SturmState& Af, SturmState& Bf, SturmState& Ab, SturmState& Bb,
+                                        double& fd0, double& fd1, double& bd0, double& bd1,
+                                        const double* __restrict__ fb, const double* __restrict__ bb, double xa,
+                                        double xb) {
+    unsigned waf = 0u, wbf = 0u, wab = 0u, wbb = 0u;
+    double af0 = Af.p0, af1 = Af.p1, ab0 = Ab.p0, ab1 = Ab.p1;
+    double bf0 = Bf.p0, bf1 = Bf.p1, bb0 = Bb.p0, bb1 = Bb.p1;
+#pragma unroll
+    for (int u = 0; u < 32; u += 2) {
+        const double2 f = *reinterpret_cast<const double2*>(fb + u);
+        const double2 g = *reinterpret_cast<const double2*>(bb + 30 - u);
+        // front row u, back row 31 - u
+        const double ta = f.x - xa, ua = g.y - xa;
+        const double qaf = fma(ta, af1, -af0), qab = fma(ua, ab1, -ab0);
+        if (kMode >= 1) {
+            const double ef = fma(ta, fd1, -(af1 + fd0)), eb = fma(ua, bd1, -(ab1 + bd0));
+            fd0 = fd1;
+            fd1 = ef;
+            bd0 = bd1;
+            bd1 = eb;
+        }
+        waf = __funnelshift_l(__double2hiint(qaf), waf, 1);
+        wab = __funnelshift_l(__double2hiint(qab), wab, 1);
+        af0 = af1;
+        af1 = qaf;
+        ab0 = ab1;
+        ab1 = qab;
+        if (kMode <= 1) {
+            const double qbf = fma(f.x - xb, bf1, -bf0), qbb = fma(g.y - xb, bb1, -bb0);
+            wbf = __funnelshift_l(__double2hiint(qbf), wbf, 1);
+            wbb = __funnelshift_l(__double2hiint(qbb), wbb, 1);
+            bf0 = bf1;
+            bf1 = qbf;
+            bb0 = bb1;
+            bb1 = qbb;
+        }
+        // front row u + 1, back row 30 - u
+        const double ta2 = f.y - xa, ua2 = g.x - xa;
+        const double qaf2 = fma(ta2, af1, -af0), qab2 = fma(ua2, ab1, -ab0);
+        if (kMode >= 1) {
+            const double ef = fma(ta2, fd1, -(af1 + fd0)), eb = fma(ua2, bd1, -(ab1 + bd0));
+            fd0 = fd1;
+            fd1 = ef;
+            bd0 = bd1;
+            bd1 = eb;
+        }
+        waf = __funnelshift_l(__double2hiint(qaf2), waf, 1);
+        wab = __funnelshift_l(__double2hiint(qab2), wab, 1);
+        af0 = af1;
+        af1 = qaf2;
+        ab0 = ab1;
+        ab1 = qab2;
+        if (kMode <= 1) {
+            const double qbf = fma(f.y - xb, bf1, -bf0), qbb = fma(g.x - xb, bb1, -bb0);
+            wbf = __funnelshift_l(__double2hiint(qbf), wbf, 1);
+            wbb = __funnelshift_l(__double2hiint(qbb), wbb, 1);
+            bf0 = bf1;
+            bf1 = qbf;
+            bb0 = bb1;
+            bb1 = qbb;
+        }
+    }
+    Af.p0 = af0;
+    Af.p1 = af1;
+    Ab.p0 = ab0;
+    Ab.p1 = ab1;
+    if (kMode >= 1) {
+        sturm_fold_deriv(Af, waf, fd0, fd1);
+        sturm_fold_deriv(Ab, wab, bd0, bd1);
+    } else {
+        sturm_fold(Af, waf);
+        sturm_fold(Ab, wab);
+    }
+    if (kMode <= 1) {
+        Bf.p0 = bf0;
+        Bf.p1 = bf1;
+        Bb.p0 = bb0;
+        Bb.p1 = bb1;
+        sturm_fold(Bf, wbf);
+        sturm_fold(Bb, wbb);
+    }
+}
+
+template <int kMode>
+__device__ __forceinline__ void tw_word(WmodRows, SturmState& Af, SturmState& Bf, SturmState& Ab, SturmState& Bb,
+                                        double& fd0, double& fd1, double& bd0, double& bd1,
+                                        const double* __restrict__ fb, const double* __restrict__ bb, double xa,
+                                        double xb) {
+    const double ca = fma(-xa, xa, -2.0), cb = fma(-xb, xb, -2.0);
+    unsigned waf = 0u, wbf = 0u, wab = 0u, wbb = 0u;
+    double af0 = Af.p0, af1 = Af.p1, ab0 = Ab.p0, ab1 = Ab.p1;
+    double bf0 = Bf.p0, bf1 = Bf.p1, bb0 = Bb.p0, bb1 = Bb.p1;
+#pragma unroll
+    for (int u = 0; u < 32; ++u) {
+        const double2 f = *reinterpret_cast<const double2*>(fb + 2 * u);
+        const double2 g = *reinterpret_cast<const double2*>(bb + 2 * (31 - u));
+        const double df = fma(-f.y, xa, f.x), dg = fma(-g.y, xa, g.x);
+        const double ta = fma(df, df, ca), ua = fma(dg, dg, ca);
+        const double qaf = fma(ta, af1, -af0), qab = fma(ua, ab1, -ab0);
+        if (kMode >= 1) {
+            const double ef = fma(ta, fd1, fma(fma(f.y, df, xa), af1, -fd0));
+            const double eb = fma(ua, bd1, fma(fma(g.y, dg, xa), ab1, -bd0));
+            fd0 = fd1;
+            fd1 = ef;
+            bd0 = bd1;
+            bd1 = eb;
+        }
+        waf = __funnelshift_l(__double2hiint(qaf), waf, 1);
+        wab = __funnelshift_l(__double2hiint(qab), wab, 1);
+        af0 = af1;
+        af1 = qaf;
+        ab0 = ab1;
+        ab1 = qab;
+        if (kMode <= 1) {
+            const double dbf = fma(-f.y, xb, f.x), dbb = fma(-g.y, xb, g.x);
+            const double qbf = fma(fma(dbf, dbf, cb), bf1, -bf0), qbb = fma(fma(dbb, dbb, cb), bb1, -bb0);
+            wbf = __funnelshift_l(__double2hiint(qbf), wbf, 1);
+            wbb = __funnelshift_l(__double2hiint(qbb), wbb, 1);
+            bf0 = bf1;
+            bf1 = qbf;
+            bb0 = bb1;
+            bb1 = qbb;
+        }
+    }
+    Af.p0 = af0;
+    Af.p1 = af1;
+    Ab.p0 = ab0;
+    Ab.p1 = ab1;
+    if (kMode >= 1) {
+        sturm_fold_deriv(Af, waf, fd0, fd1);
+        sturm_fold_deriv(Ab, wab, bd0, bd1);
+    } else {
+        sturm_fold(Af, waf);
+        sturm_fold(Ab, wab);
+    }
+    if (kMode <= 1) {
+        Bf.p0 = bf0;
+        Bf.p1 = bf1;
+        Bb.p0 = bb0;
+        Bb.p1 = bb1;
+        sturm_fold(Bf, wbf);
+        sturm_fold(Bb, wbb);
+    }
+}
+
+// one twisted sweep in mode kMode (see warp_sweep); each ring slot holds a
+// front part and a back part of kWChunk / 2 doubles
+template <class Row, int kMode>
+__device__ void warp_sweep_tw_mode(const double* __restrict__ s, int nz, double p_init, double x0, double x1,
+                                   WarpRing& r, unsigned* err, int& c0, int& c1, double& rat0) {
+    constexpr int kW = Row::kW;
+    constexpr int kHD = kWChunk / 2;  // doubles per part
+    constexpr int kHR = kHD / kW;     // rows per part
+    constexpr int kHW = kHR / 32;     // 32-row words per part
+    const int lane = threadIdx.x & 31;
+    const int nparts = (nz + kHR - 1) / kHR;
+    const int nf = (nparts + 1) / 2, nb = nparts - nf;  // front parts 0..nf-1, back parts nparts-1 .. nf
+    const unsigned base = r.loads;
+    auto issue = [&](unsigned k, int j) {
+        const int slot = k % kWBuf;
+        mbar_expect_tx(&r.bars[slot], (j < nb ? 2 : 1) * kHD * 8);
+        tma_load_1d(r.buf + slot * kWChunk, s + (size_t)j * kHD, kHD * 8, &r.bars[slot]);
+        if (j < nb)
+            tma_load_1d(r.buf + slot * kWChunk + kHD, s + (size_t)(nparts - 1 - j) * kHD, kHD * 8, &r.bars[slot]);
+    };
+    if (lane == 0)
+        for (int j = 0; j < nf && j < kWBuf; ++j) issue(base + j, j);
+    __syncwarp();
+    SturmState Af, Bf, Ab, Bb;
+    Af.reset();
+    Bf.reset();
+    Ab.reset();
+    Bb.reset();
+    if (kW != 1) {
+        Af.p0 = p_init;
+        Bf.p0 = p_init;
+    }
+    double fd0 = 0.0, fd1 = 0.0, bd0 = 0.0, bd1 = 0.0;
+    for (int j = 0; j < nf; ++j) {
+        const unsigned k = base + j;
+        const int slot = k % kWBuf;
+        mbar_wait_bounded(&r.bars[slot], (k / kWBuf) & 1u, err);
+        const double* fb = r.buf + slot * kWChunk;
+        const double* bb = fb + kHD;
+        int nwb = 0;
+        if (j < nb) {
+            const int valid_b = min(kHR, nz - (nparts - 1 - j) * kHR);
+            nwb = valid_b >> 5;
+            for (int i = valid_b - 1; i >= nwb * 32; --i) {  // ragged top of the last part, descending
+                if (kMode >= 1) Row::step_deriv(Ab, bb, i, x0, bd0, bd1);
+                else Row::step(Ab, bb, i, x0);
+                if (kMode <= 1) Row::step(Bb, bb, i, x1);
+            }
+            for (int w = 0; w < nwb; ++w)
+                tw_word<kMode>(Row{}, Af, Bf, Ab, Bb, fd0, fd1, bd0, bd1, fb + 32 * kW * w,
+                               bb + 32 * kW * (nwb - 1 - w), x0, x1);
+        }
+        for (int w = nwb; w < kHW; ++w) {  // front words without a back partner
+            if (kMode == 0) Row::pair(Af, Bf, fb + 32 * kW * w, x0, x1);
+            else if (kMode == 1) Row::deriv_pair(Af, fd0, fd1, Bf, fb + 32 * kW * w, x0, x1);
+            else Row::word_deriv(Af, fb + 32 * kW * w, x0, fd0, fd1);
+        }
+        __syncwarp();
+        if (lane == 0 && j + kWBuf < nf) {
+            fence_proxy_async();
+            issue(base + j + kWBuf, j + kWBuf);
+        }
+    }
+    r.loads = base + nf;
+    double det;
+    c0 = twist_count(Af, Ab, det);
+    c1 = 0;
+    if (kMode <= 1) {
+        double detb;
+        c1 = twist_count(Bf, Bb, detb);
+    }
+    rat0 = 0.0;
+    if (kMode >= 1) {
+        const double dd = fd1 * Ab.p1 + Af.p1 * bd1 - fd0 * Ab.p0 - Af.p0 * bd0;
+        rat0 = Row::newton(det, dd);
+    }
+}
+
+// the twisted sweep; grids of one part (nz <= kWChunk / 2 / kW rows) run the
+// sequential sweep
+template <class Row>
+__device__ void warp_sweep_tw(const double* __restrict__ s, int nz, double p_init, double x0, double x1, int mode,
+                              WarpRing& r, unsigned* err, int& c0, int& c1, double& rat0) {
+    if (nz <= kWChunk / 2 / Row::kW) {
+        warp_sweep<Row>(s, nz, p_init, x0, x1, mode, r, err, c0, c1, rat0);
+        return;
+    }
+    if (mode == 0) warp_sweep_tw_mode<Row, 0>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0);
+    else if (mode == 1) warp_sweep_tw_mode<Row, 1>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0);
+    else warp_sweep_tw_mode<Row, 2>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0);
+}
+
 // Row: the row format (EssRows: shifts in h^2 k^2; WmodRows: kappa = h k);
 // tol is scaled per problem by Row::tol_scale.
 template <class Row>
@@ -786,7 +1051,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
             int cv0, cv1;
             double rat;
             const int smode = nN == 0 ? 0 : (nB > 0 ? 1 : 2);
-            warp_sweep<Row>(sp, nz, p_init, xv[0], xv[1], smode, r, err, cv0, cv1, rat);
+            warp_sweep_tw<Row>(sp, nz, p_init, xv[0], xv[1], smode, r, err, cv0, cv1, rat);
             if (step_counter && lane == 0)
                 atomicAdd(step_counter, (unsigned long long)(smode == 2 ? 32 : 64) * (unsigned long long)nz);
             // updates.  Every __shfl_sync is executed by all 32 lanes.
