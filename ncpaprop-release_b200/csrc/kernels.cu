@@ -954,7 +954,7 @@ __device__ void warp_sweep_tw_mode(const double* __restrict__ s, int nz, double 
 template <class Row>
 __device__ void warp_sweep_tw(const double* __restrict__ s, int nz, double p_init, double x0, double x1, int mode,
                               WarpRing& r, unsigned* err, int& c0, int& c1, double& rat0) {
-    if (nz <= kWChunk / 2 / Row::kW) {
+    if (!Row::kTwist || nz <= kWChunk / 2 / Row::kW) {
         warp_sweep<Row>(s, nz, p_init, x0, x1, mode, r, err, c0, c1, rat0);
         return;
     }
