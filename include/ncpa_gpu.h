@@ -124,7 +124,8 @@ typedef struct {
  * wind component along the azimuth), D the finite-difference operator with
  * (omega/c0)^2, solved in k by Sturm counts of T(k) = M k^2 + C k + D, plus
  * the reference's matrix spacing (maxheight - z_min) / Nz_grid.  Available
- * through ncpa_ess_solve (not through jobs or plans); group speeds are 0. */
+ * through ncpa_ess_solve and ncpa_ess_solve_jobs (so also in the serving
+ * loop); plans take the ESS method only.  Group speeds are 0. */
 enum { NCPA_METHOD_ESS = 0, NCPA_METHOD_WMOD = 1 };
 
 void ncpa_ess_params_default(ncpa_ess_params *p);

@@ -1576,7 +1576,6 @@ ncpa_status ncpa_ess_solve_jobs(ncpa_ctx* ctx, const ncpa_ess_job* jobs, int n_j
     *out = nullptr;
     return guarded(ctx, [&]() -> ncpa_status {
         check_ess_params(prm);
-        if (prm->method != NCPA_METHOD_ESS) throw ApiError(NCPA_EINVAL, "jobs take the ESS method only");
         int P = 0;
         std::vector<Group> groups;
         groups.reserve(n_jobs);
@@ -1603,7 +1602,8 @@ ncpa_status ncpa_ess_solve_jobs(ncpa_ctx* ctx, const ncpa_ess_job* jobs, int n_j
             for (int f = 0; f < g.n_freq; ++f)
                 for (int a = 0; a < g.n_az; ++a) M->freqs.push_back(g.freqs[f]);
         M->az.assign(1, groups[0].az[0]);
-        solve_groups(ctx, M.get(), prm, groups);
+        if (prm->method == NCPA_METHOD_WMOD) solve_wmod(ctx, M.get(), prm, groups);
+        else solve_groups(ctx, M.get(), prm, groups);
         *out = M.release();
         return NCPA_OK;
     });

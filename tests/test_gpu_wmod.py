@@ -132,12 +132,30 @@ def test_eigenvectors_and_normalisation(gpu, canonical_profile):
     prof.close()
 
 
-def test_jobs_and_plans_reject_wmod(gpu, canonical_profile):
+def test_jobs_mixed_grids_match_single_solves(gpu, canonical_profile, analytic_profile):
+    """Wide-angle jobs on two profiles and two grids (one with an azimuth
+    list) in one ncpa_ess_solve_jobs call: every problem bit-identical to the
+    same problem solved alone."""
+    pc = gpu.load_profile(canonical_profile)
+    pa = gpu.load_profile(analytic_profile)
+    m = gpu.solve_jobs([(pc, [0.05, 0.1], 90.0, 4000), (pa, [0.08], [0.0, 200.0], 6000)], _wmod(turnoff_wkb=1))
+    s1 = gpu.solve(pc, _wmod(nz_grid=4000, turnoff_wkb=1), [0.05, 0.1], [90.0])
+    s2 = gpu.solve(pa, _wmod(nz_grid=6000, turnoff_wkb=1), [0.08], [0.0, 200.0])
+    singles = [s1.problem(0), s1.problem(1), s2.problem(0), s2.problem(1)]
+    for p, o in enumerate(singles):
+        g = m.problem(p)
+        assert g.M == o.M > 0
+        for f in ("kr", "ki", "vs", "vr"):
+            assert np.array_equal(getattr(g, f), getattr(o, f)), (p, f)
+        assert g.dz == o.dz
+    for h in (m, s1, s2, pc, pa):
+        h.close()
+
+
+def test_plans_reject_wmod(gpu, canonical_profile):
     import ncpa_gpu
 
     prof = gpu.load_profile(canonical_profile)
-    with pytest.raises(ncpa_gpu.NcpaError):
-        gpu.solve_jobs([(prof, [0.1], 90.0)], _wmod())
     with pytest.raises(ncpa_gpu.NcpaError):
         gpu.plan([(prof, [0.1], 90.0)], _wmod())
     bad = _wmod()
