@@ -52,19 +52,23 @@ constexpr int kMsRcv = 64;          // receivers per group
 constexpr int kMsNT = 256;          // ranges per tile (UMMA N)
 constexpr int kMsModes = 16;        // modes per K-chunk
 constexpr int kMsKC = 2 * kMsModes; // K per chunk
-constexpr int kMsStages = 4;
+constexpr int kMsAStages = 6;       // ring of A' chunks (+ factor rows, tile phases) fed by TMA
+constexpr int kMsBStages = 3;       // ring of generated B' chunks
 constexpr int kMsABytes = kMsRows * kMsKC * 2;   // one A' part (hi or lo) of a chunk: 8 KB
 constexpr int kMsBBytes = kMsNT * kMsKC * 2;     // one B' part of a chunk: 16 KB
 constexpr int kMsTabW = 18;         // per-mode row: e^{ik i dr} (i < 8), e^{ik 32 j dr} (j < 8), e^{ik 8 dr}, pad
 constexpr int kMsTabBytes = kMsModes * kMsTabW * 8;  // factor rows of one chunk: 2304 B
 constexpr int kMsQBytes = kMsModes * 8;              // tile phases of one chunk
 constexpr int kMsTxBytes = 2 * kMsABytes + kMsTabBytes + kMsQBytes;
-// stage: A hi, A lo, B hi, B lo, factor rows, tile phases (1 KB aligned)
-constexpr int kMsOffB = 2 * kMsABytes;
-constexpr int kMsOffTab = kMsOffB + 2 * kMsBBytes;
+// A stage: A hi, A lo, factor rows, tile phases (1 KB aligned); B stage:
+// B hi, B lo.  The A ring is deeper than the B ring: its TMA round trip is
+// the long latency, B' generation the short one.
+constexpr int kMsOffTab = 2 * kMsABytes;
 constexpr int kMsOffQ = kMsOffTab + kMsTabBytes;
-constexpr int kMsStageBytes = (kMsOffQ + kMsQBytes + 1023) / 1024 * 1024;
-constexpr int kMsSmem = kMsStages * kMsStageBytes + 1024;
+constexpr int kMsAStageBytes = (kMsOffQ + kMsQBytes + 1023) / 1024 * 1024;
+constexpr int kMsBStageBytes = 2 * kMsBBytes;
+constexpr int kMsOffBRing = kMsAStages * kMsAStageBytes;
+constexpr int kMsSmem = kMsOffBRing + kMsBStages * kMsBStageBytes + 1024;
 constexpr int kMsGenWarps = 8;      // B' generators / epilogue
 constexpr int kMsGenThreads = 32 * kMsGenWarps;
 constexpr int kMsProducerWarp = 1 + kMsGenWarps;  // warp 0: MMA issuer, 1-8: generators, 9: TMA producer
@@ -318,7 +322,7 @@ struct UnitPos {
 template <int F>
 __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     extern __shared__ unsigned char ms_dyn[];
-    __shared__ __align__(8) uint64_t full_a[kMsStages], full_b[kMsStages], empty[kMsStages];
+    __shared__ __align__(8) uint64_t full_a[kMsAStages], empty_a[kMsAStages], full_b[kMsBStages], empty_b[kMsBStages];
     __shared__ __align__(8) uint64_t acc_full[kMsAcc], acc_empty[kMsAcc], drain;
     __shared__ uint32_t tmem_base_sh;
     unsigned char* sm = (unsigned char*)(((uintptr_t)ms_dyn + 1023) & ~(uintptr_t)1023);
@@ -329,10 +333,13 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     const int nc = (int)(a.n_units * (blockIdx.x + 1) / gridDim.x - u0);
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kMsStages; ++s) {
+        for (int s = 0; s < kMsAStages; ++s) {
             mbar_init(&full_a[s], 1);
+            mbar_init(&empty_a[s], 1);
+        }
+        for (int s = 0; s < kMsBStages; ++s) {
             mbar_init(&full_b[s], kMsGenWarps);
-            mbar_init(&empty[s], 1);
+            mbar_init(&empty_b[s], 1);
         }
         for (int b = 0; b < kMsAcc; ++b) {
             mbar_init(&acc_full[b], 1);
@@ -355,19 +362,19 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     if (warp == kMsProducerWarp) {
         if (lane == 0 && nc > 0) {
             // producer: bulk TMA of the A' chunk, factor rows and tile phases
-            // into stage c % kMsStages once the MMAs of chunk c - kMsStages are done
+            // into A stage c % kMsAStages once the MMAs of chunk c - kMsAStages are done
             UnitPos pos;
             pos.init(u0, a.n_chunks, a.n_tiles);
             int issued = 0, landed = 0;
             bool ok = true;
             for (int c = 0; c < nc; ++c, pos.next(a.n_chunks, a.n_tiles)) {
-                const int slot = c % kMsStages;
-                if (c >= kMsStages) {
-                    ok = mbar_wait_bounded(&empty[slot], (uint32_t)(((c / kMsStages) - 1) & 1), a.err);
+                const int slot = c % kMsAStages;
+                if (c >= kMsAStages) {
+                    ok = mbar_wait_bounded(&empty_a[slot], (uint32_t)(((c / kMsAStages) - 1) & 1), a.err);
                     if (!ok) break;
-                    landed = c - kMsStages + 1;  // its copies were consumed, so they landed
+                    landed = c - kMsAStages + 1;  // its copies were consumed, so they landed
                 }
-                unsigned char* dst = sm + slot * kMsStageBytes;
+                unsigned char* dst = sm + slot * kMsAStageBytes;
                 mbar_expect_tx(&full_a[slot], kMsTxBytes);
                 tma_load_1d(dst, a.a_img + ((size_t)pos.group * a.n_chunks + pos.chunk) * 2 * kMsABytes,
                             2 * kMsABytes, &full_a[slot]);
@@ -379,7 +386,7 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             }
             // copies still in flight after an early exit: wait for them
             for (int c = landed; c < issued; ++c)
-                mbar_wait_drain(&full_a[c % kMsStages], (uint32_t)((c / kMsStages) & 1));
+                mbar_wait_drain(&full_a[c % kMsAStages], (uint32_t)((c / kMsAStages) & 1));
         }
     } else if (warp == 0) {
         if (lane == 0 && nc > 0) {
@@ -400,34 +407,35 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                         tc_fence_after();
                     }
                 }
-                const int s = c % kMsStages;
-                const uint32_t ph = (uint32_t)((c / kMsStages) & 1);
-                ok = mbar_wait_bounded(&full_a[s], ph, a.err) && mbar_wait_bounded(&full_b[s], ph, a.err);
+                const int sa = c % kMsAStages, sb = c % kMsBStages;
+                ok = mbar_wait_bounded(&full_a[sa], (uint32_t)((c / kMsAStages) & 1), a.err) &&
+                     mbar_wait_bounded(&full_b[sb], (uint32_t)((c / kMsBStages) & 1), a.err);
                 if (!ok) break;
                 tc_fence_after();
                 // descriptors: the start-address field counts 16-byte units
-                const uint64_t st = dsc0 + (uint64_t)((s * kMsStageBytes) >> 4);
+                const uint64_t st = dsc0 + (uint64_t)((sa * kMsAStageBytes) >> 4);
+                const uint64_t stb = dsc0 + (uint64_t)((kMsOffBRing + sb * kMsBStageBytes) >> 4);
                 const uint32_t d = tmem + (uint32_t)((sg & 1) * kMsNT);
                 if (F == kMsTf32) {
                     // K = 8 tf32 (32 B) per MMA, four per chunk
 #pragma unroll
                     for (int kk = 0; kk < kMsKC / 8; ++kk) {
                         const uint64_t ad = st + (uint64_t)(kk * 32 >> 4);
-                        const uint64_t bd = st + (uint64_t)((kMsOffB + kk * 32) >> 4);
+                        const uint64_t bd = stb + (uint64_t)(kk * 32 >> 4);
                         umma_tf32(d, ad, bd, (!first || kk > 0) ? 1u : 0u);
                     }
                 } else {
 #pragma unroll
                     for (int kk = 0; kk < kMsKC / 16; ++kk) {
                         const uint64_t ah = st + (uint64_t)(kk * 32 >> 4), al = ah + (uint64_t)(kMsABytes >> 4);
-                        const uint64_t bh = st + (uint64_t)((kMsOffB + kk * 32) >> 4),
-                                       bl = bh + (uint64_t)(kMsBBytes >> 4);
+                        const uint64_t bh = stb + (uint64_t)(kk * 32 >> 4), bl = bh + (uint64_t)(kMsBBytes >> 4);
                         umma_bf16(d, ah, bh, (!first || kk > 0) ? 1u : 0u);
                         umma_bf16(d, ah, bl, 1u);
                         umma_bf16(d, al, bh, 1u);
                     }
                 }
-                umma_commit(&empty[s]);
+                umma_commit(&empty_a[sa]);
+                umma_commit(&empty_b[sb]);
                 if (last) umma_commit(&acc_full[sg & 1]);
             }
             if (!ok) {
@@ -454,15 +462,15 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             const bool first = c == 0 || pos.chunk == 0;
             const bool last = c == nc - 1 || pos.chunk == a.n_chunks - 1;
             if (first) ++sg;
-            const int s = c % kMsStages;
-            if (c >= kMsStages) {
-                ok = mbar_wait_bounded(&empty[s], (uint32_t)(((c / kMsStages) - 1) & 1), a.err);
+            const int sa = c % kMsAStages, sb = c % kMsBStages;
+            if (c >= kMsBStages) {  // B stage free once the MMAs of chunk c - kMsBStages are done
+                ok = mbar_wait_bounded(&empty_b[sb], (uint32_t)(((c / kMsBStages) - 1) & 1), a.err);
                 if (!ok) break;
             }
             // factor rows and tile phases of this chunk arrive with its A' copy
-            ok = mbar_wait_bounded(&full_a[s], (uint32_t)((c / kMsStages) & 1), a.err);
+            ok = mbar_wait_bounded(&full_a[sa], (uint32_t)((c / kMsAStages) & 1), a.err);
             if (!ok) break;
-            const unsigned char* stg = sm + s * kMsStageBytes;
+            const unsigned char* stg = sm + sa * kMsAStageBytes;
             const float2* tab_s = reinterpret_cast<const float2*>(stg + kMsOffTab);
             const float2* q_s = reinterpret_cast<const float2*>(stg + kMsOffQ);
             float2 e[4], w[4];
@@ -472,7 +480,7 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                 e[v] = cmulf(cmulf(q_s[4 * q + v], tb[i]), tb[8 + part]);
                 w[v] = tb[16];
             }
-            const uint32_t bh = sm_addr + s * kMsStageBytes + kMsOffB;
+            const uint32_t bh = sm_addr + kMsOffBRing + sb * kMsBStageBytes;
 #pragma unroll
             for (int st8 = 0; st8 < 4; ++st8) {
                 const int grp = part * 4 + st8;  // 8-range group within the tile
@@ -500,7 +508,7 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             fence_proxy_async();
             __syncwarp();
             if (lane == 0)
-                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full_b[s])) : "memory");
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full_b[sb])) : "memory");
             if (!last) continue;
             // epilogue of segment sg: TMEM lanes 32 (warp % 4) .. +31 = rows;
             // the partial sum goes to slot (this CTA - first CTA of the tile)
