@@ -182,7 +182,9 @@ struct MsPlan {
 };
 MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms);
 int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const double* vfull, double* vz);
-// fmt: 0 = 3-term split-BF16 (kind::f16), 1 = TF32 (kind::tf32)
+// fmt: 0 = 3-term split-BF16 (kind::f16), 1 = TF32 (kind::tf32).  Buffers:
+// a_img = A as complex FP32 per (receiver group, mode chunk), q = tile
+// phases, tab = the B' image of each mode chunk (tile-independent)
 int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int M, const double* kr,
                       const double* ki, const double* vs, const int* idx, const double* vfull, double dr, int lossless,
                       void* a_img, void* q, void* tab);

@@ -20,16 +20,22 @@
 // Both keep a chunk's A' in 16 KB and its B' in 32 KB of shared memory, so the
 // pipeline, barriers and epilogue are shared.
 //
-// Persistent kernel: the (receiver group, 128-range tile, 32-mode chunk)
+// Since r_n = r_n0 + o dr inside a 256-range tile (r_n0 its first range),
+// E_mn = e^{i k_m r_n0} e^{i k_m o dr}: the tile's phase is folded into A
+// (A'(tile) = A diag(e^{i k r_n0}), 64 x 16 complex products per chunk) and
+// B' = e^{i k o dr} does not depend on the tile, so it is prepared once per
+// chunk in FP64 and streamed in by TMA.  The tile phases are reduced mod 2 pi
+// in FP64 before their cast to FP32.
+//
+// Persistent kernel: the (receiver group, 256-range tile, 16-mode chunk)
 // units are split evenly over one CTA per SM; a CTA accumulates the chunks of
 // one (group, tile) in TMEM (two accumulators, so a finished tile's epilogue
 // overlaps the next tile's MMAs) and stores its partial sum of the tile in
 // its own slot; the finishing kernel adds the slots of the CTAs that shared
 // the tile.  Warp 0: TMEM allocation and tcgen05.mma issue.  Warp 9: bulk
-// TMA of the prepared A' chunk together with the chunk's per-mode factor
-// rows and tile phases.  Warps 1-8: generate B' in shared memory from
-// FP64-reduced tile phases e^{i k r_n0} (phase reduced mod 2 pi in FP64)
-// times per-mode FP32 factors e^{i k o dr}, and read the accumulators out.
+// TMA of the chunk's B' image, A and tile phases into a 4-deep ring.
+// Warps 1-8: generate A'(tile) into a 3-deep ring of shared memory, and read
+// the accumulators out.
 //
 // Shared-memory operand layout: K-major, each operand row holds the 32 k of a
 // chunk; bf16: 64 B rows, 64-byte swizzle, 8-row atoms of 512 B (sw64_off);
@@ -52,33 +58,30 @@ constexpr int kMsRcv = 64;          // receivers per group
 constexpr int kMsNT = 256;          // ranges per tile (UMMA N)
 constexpr int kMsModes = 16;        // modes per K-chunk
 constexpr int kMsKC = 2 * kMsModes; // K per chunk
-constexpr int kMsAStages = 6;       // ring of A' chunks (+ factor rows, tile phases) fed by TMA
-constexpr int kMsBStages = 3;       // ring of generated B' chunks
 constexpr int kMsABytes = kMsRows * kMsKC * 2;   // one A' part (hi or lo) of a chunk: 8 KB
 constexpr int kMsBBytes = kMsNT * kMsKC * 2;     // one B' part of a chunk: 16 KB
-constexpr int kMsTabW = 18;         // per-mode row: e^{ik i dr} (i < 8), e^{ik 32 j dr} (j < 8), e^{ik 8 dr}, pad
-constexpr int kMsTabBytes = kMsModes * kMsTabW * 8;  // factor rows of one chunk: 2304 B
-constexpr int kMsQBytes = kMsModes * 8;              // tile phases of one chunk
-constexpr int kMsTxBytes = 2 * kMsABytes + kMsTabBytes + kMsQBytes;
-// A stage: A hi, A lo, factor rows, tile phases (1 KB aligned); B stage:
-// B hi, B lo.  The A ring is deeper than the B ring: its TMA round trip is
-// the long latency, B' generation the short one.
-constexpr int kMsOffTab = 2 * kMsABytes;
-constexpr int kMsOffQ = kMsOffTab + kMsTabBytes;
-constexpr int kMsAStageBytes = (kMsOffQ + kMsQBytes + 1023) / 1024 * 1024;
-constexpr int kMsBStageBytes = 2 * kMsBBytes;
-constexpr int kMsOffBRing = kMsAStages * kMsAStageBytes;
-constexpr int kMsSmem = kMsOffBRing + kMsBStages * kMsBStageBytes + 1024;
-constexpr int kMsGenWarps = 8;      // B' generators / epilogue
+constexpr int kMsACBytes = kMsModes * kMsRcv * 8;  // a chunk's A as complex FP32, [mode][receiver]: 8 KB
+constexpr int kMsQBytes = kMsModes * 8;            // tile phases of one chunk
+// TMA stage: B' image (hi, lo), A complex, tile phases (1 KB aligned)
+constexpr int kMsOffAC = 2 * kMsBBytes;
+constexpr int kMsOffQ = kMsOffAC + kMsACBytes;
+constexpr int kMsTxBytes = 2 * kMsBBytes + kMsACBytes + kMsQBytes;
+constexpr int kMsTStageBytes = (kMsOffQ + kMsQBytes + 1023) / 1024 * 1024;
+constexpr int kMsTStages = 4;       // ring of TMA stages
+constexpr int kMsGStageBytes = 2 * kMsABytes;  // generated A' (hi, lo)
+constexpr int kMsGStages = 3;       // ring of generated A' chunks
+constexpr int kMsOffGRing = kMsTStages * kMsTStageBytes;
+constexpr int kMsSmem = kMsOffGRing + kMsGStages * kMsGStageBytes + 1024;
+constexpr int kMsGenWarps = 8;      // A' generators / epilogue
 constexpr int kMsGenThreads = 32 * kMsGenWarps;
 constexpr int kMsProducerWarp = 1 + kMsGenWarps;  // warp 0: MMA issuer, 1-8: generators, 9: TMA producer
 constexpr int kMsThreads = 32 * (kMsProducerWarp + 1);
 constexpr int kMsAcc = 2;           // TMEM accumulators (kMsNT columns each): all 512 columns
-static_assert(kMsSmem <= 232448, "shared memory per block");
-static_assert(kMsTabBytes % 16 == 0 && kMsQBytes % 16 == 0 && kMsTxBytes % 16 == 0,
+static_assert(kMsSmem <= 232448 - 256, "shared memory per block");
+static_assert(kMsACBytes % 16 == 0 && kMsQBytes % 16 == 0 && kMsTxBytes % 16 == 0 && (2 * kMsBBytes) % 1024 == 0,
               "bulk copies move 16-byte multiples");
 static_assert(kMsAcc * kMsNT <= 512, "TMEM columns");
-static_assert(kMsGenThreads == 8 * (kMsModes / 4) * (kMsNT / 32), "one generator per (range, mode quad, 32 ranges)");
+static_assert(kMsGenThreads == kMsRcv * (kMsModes / 4), "one generator per (receiver, mode quad)");
 
 // byte offset of element (row, k) in a K-major tile of kMsKC = 32 bf16 per
 // row with the 64-byte swizzle: rows of 64 B in atoms of 8 rows (512 B); the
@@ -181,24 +184,45 @@ __device__ __forceinline__ void sts128(uint32_t addr, uint32_t a, uint32_t b, ui
 // preparation
 // ---------------------------------------------------------------------------
 // per-mode FP32 factors from FP64: entries 0-7 e^{i k i dr}, 8-15
-// e^{i k 32 j dr} (generator thread (i, part j) starts at range offset
-// i + 32 j of its tile), 16 the step e^{i k 8 dr}, 17 zero; zero rows for the
-// padding modes m >= M
-__device__ void ms_table_entry(int id, int M, int M_pad, const double* __restrict__ kr,
-                               const double* __restrict__ ki, double dr, int lossless, float2* __restrict__ tab) {
-    if (id >= M_pad * kMsTabW) return;
-    const int m = id / kMsTabW, e = id % kMsTabW;
-    float2 v = make_float2(0.f, 0.f);
-    if (m < M && e <= 16) {
-        const double a = kr[m], b = lossless ? 0.0 : ki[m];
-        const double off = e < 8 ? (double)e : e < 16 ? 32.0 * (e - 8) : 8.0;
-        const double x = off * dr;
+// B' chunk images: B'[o][2m] = Re, B'[o][2m + 1] = Im of e^{i k_m o dr}
+// (o = 0 .. 255, the range offset inside a tile; attenuation included unless
+// lossless), in FP64 and then split (bf16 hi, lo) or rounded (TF32), in the
+// shared-memory layout of the operand; zero for the padding modes m >= M.
+// The images do not depend on the tile: the tile's phase e^{i k r_n0} goes
+// into A'.
+template <int F>
+__device__ void ms_b_entry(long long id, int M, int n_chunks, const double* __restrict__ kr,
+                           const double* __restrict__ ki, double dr, int lossless, unsigned char* __restrict__ img) {
+    const long long per_chunk = (long long)kMsNT * kMsModes;
+    if (id >= (long long)n_chunks * per_chunk) return;
+    const int o = (int)(id % kMsNT);
+    const int ml = (int)((id / kMsNT) % kMsModes);
+    const int chunk = (int)(id / per_chunk);
+    const int m = chunk * kMsModes + ml;
+    float re = 0.f, im = 0.f;
+    if (m < M) {
+        const double x = (double)o * dr;
         double sn, cs;
-        sincos(a * x, &sn, &cs);
-        const double amp = exp(-b * x);
-        v = make_float2((float)(amp * cs), (float)(amp * sn));
+        sincos(kr[m] * x, &sn, &cs);
+        const double amp = lossless ? 1.0 : exp(-ki[m] * x);
+        re = (float)(amp * cs);
+        im = (float)(amp * sn);
     }
-    tab[id] = v;
+    unsigned char* ci = img + (size_t)chunk * 2 * kMsBBytes;  // 32 KB per chunk
+    if (F == kMsTf32) {
+        *reinterpret_cast<uint32_t*>(ci + sw128_off(o, 2 * ml)) = to_tf32(re);
+        *reinterpret_cast<uint32_t*>(ci + sw128_off(o, 2 * ml + 1)) = to_tf32(im);
+    } else {
+        const __nv_bfloat16 hr = __float2bfloat16_rn(re), hm = __float2bfloat16_rn(im);
+        const __nv_bfloat16 lr = __float2bfloat16_rn(re - __bfloat162float(hr));
+        const __nv_bfloat16 li = __float2bfloat16_rn(im - __bfloat162float(hm));
+        __nv_bfloat16* bm = reinterpret_cast<__nv_bfloat16*>(ci);
+        const size_t o0 = sw64_off(o, 2 * ml) / 2, o1 = sw64_off(o, 2 * ml + 1) / 2;
+        bm[o0] = hr;
+        bm[o1] = hm;
+        bm[kMsBBytes / 2 + o0] = lr;
+        bm[kMsBBytes / 2 + o1] = li;
+    }
 }
 
 // tile phases e^{i k_m r_n0}, r_n0 = (tile * 256 + 1) dr: the phase k r is
@@ -222,61 +246,49 @@ __device__ void ms_phase_entry(long long id, int M, int M_pad, int n_tiles, cons
     q[id] = make_float2((float)(amp * cs), (float)(amp * sn));
 }
 
-// A' chunk images (hi, lo) for every receiver group and K-chunk, in the
-// shared-memory layout above; mode values at receiver j are row idx[j] of the
-// full eigenvectors vfull [z][mode], vs the source values
-template <int F>
+// A_jm = v_m(z_s) v_m(z_j) / sqrt(k_m) as complex FP32 for every receiver
+// group and K-chunk, [group][chunk][mode m in chunk][receiver j in group];
+// mode values at receiver j are row idx[j] of the full eigenvectors vfull
+// [z][mode], vs the source values; zero for padding modes and receivers
 __device__ void ms_a_entry(long long id, int n_rcv, int M, int n_chunks, const double* __restrict__ kr,
                            const double* __restrict__ ki, const double* __restrict__ vs, const int* __restrict__ idx,
-                           const double* __restrict__ vfull, int lossless, unsigned char* __restrict__ img) {
+                           const double* __restrict__ vfull, int lossless, float2* __restrict__ ac) {
     const int n_groups = (n_rcv + kMsRcv - 1) / kMsRcv;
-    const long long per_chunk = (long long)kMsRows * kMsKC;
+    const long long per_chunk = (long long)kMsModes * kMsRcv;
     if (id >= (long long)n_groups * n_chunks * per_chunk) return;
-    const int row = (int)(id % kMsRows);
-    const int kl = (int)((id / kMsRows) % kMsKC);
+    const int jl = (int)(id % kMsRcv);
+    const int ml = (int)((id / kMsRcv) % kMsModes);
     const long long gc = id / per_chunk;  // group * n_chunks + chunk
     const int chunk = (int)(gc % n_chunks), g = (int)(gc / n_chunks);
-    const int m = chunk * kMsModes + (kl >> 1);
-    const int j = g * kMsRcv + (row & (kMsRcv - 1));
-    float x = 0.f;
+    const int m = chunk * kMsModes + ml;
+    const int j = g * kMsRcv + jl;
+    float2 v = make_float2(0.f, 0.f);
     if (m < M && j < n_rcv) {
         const double a = kr[m], b = lossless ? 0.0 : ki[m];
         const auto sk = csqrt_principal(a, b);
         const double den = sk.real() * sk.real() + sk.imag() * sk.imag();
         const double c = vs[m] * vfull[(size_t)idx[j] * M + m];
-        const double are = c * sk.real() / den, aim = -c * sk.imag() / den;
-        const bool im_row = row >= kMsRcv, im_col = (kl & 1) != 0;
-        x = (float)(!im_row ? (im_col ? -aim : are) : (im_col ? are : aim));
+        v = make_float2((float)(c * sk.real() / den), (float)(-c * sk.imag() / den));
     }
-    unsigned char* chunk_img = img + (size_t)gc * 2 * kMsABytes;  // 16 KB per (group, chunk)
-    if (F == kMsTf32) {
-        *reinterpret_cast<uint32_t*>(chunk_img + sw128_off(row, kl)) = to_tf32(x);
-    } else {
-        const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-        __nv_bfloat16* im = reinterpret_cast<__nv_bfloat16*>(chunk_img);
-        const size_t off = sw64_off(row, kl) / 2;
-        im[off] = hi;
-        im[kMsABytes / 2 + off] = lo;
-    }
+    ac[id] = v;
 }
 
-// the three preparations in one launch: blocks [0, b_tab) fill the factor
-// rows, [b_tab, b_tab + b_q) the tile phases, the rest the A' images
+// the three preparations in one launch: blocks [0, b_b) fill the B' images,
+// [b_b, b_b + b_q) the tile phases, the rest A
 template <int F>
-__global__ void k_ms_prepare(long long b_tab, long long b_q, int n_rcv, int M, int M_pad, int n_tiles, int n_chunks,
+__global__ void k_ms_prepare(long long b_b, long long b_q, int n_rcv, int M, int M_pad, int n_tiles, int n_chunks,
                              const double* __restrict__ kr, const double* __restrict__ ki,
                              const double* __restrict__ vs, const int* __restrict__ idx,
-                             const double* __restrict__ vfull, double dr, int lossless, float2* __restrict__ tab,
-                             float2* __restrict__ q, unsigned char* __restrict__ img) {
+                             const double* __restrict__ vfull, double dr, int lossless,
+                             unsigned char* __restrict__ b_img, float2* __restrict__ q, float2* __restrict__ ac) {
     const long long b = blockIdx.x;
-    if (b < b_tab) {
-        ms_table_entry((int)(b * blockDim.x + threadIdx.x), M, M_pad, kr, ki, dr, lossless, tab);
-    } else if (b < b_tab + b_q) {
-        ms_phase_entry((b - b_tab) * blockDim.x + threadIdx.x, M, M_pad, n_tiles, kr, ki, dr, lossless, q);
+    if (b < b_b) {
+        ms_b_entry<F>(b * blockDim.x + threadIdx.x, M, n_chunks, kr, ki, dr, lossless, b_img);
+    } else if (b < b_b + b_q) {
+        ms_phase_entry((b - b_b) * blockDim.x + threadIdx.x, M, M_pad, n_tiles, kr, ki, dr, lossless, q);
     } else {
-        ms_a_entry<F>((b - b_tab - b_q) * blockDim.x + threadIdx.x, n_rcv, M, n_chunks, kr, ki, vs, idx, vfull,
-                      lossless, img);
+        ms_a_entry((b - b_b - b_q) * blockDim.x + threadIdx.x, n_rcv, M, n_chunks, kr, ki, vs, idx, vfull, lossless,
+                   ac);
     }
 }
 
@@ -290,9 +302,9 @@ __host__ __device__ __forceinline__ int ms_cta_of(long long u, long long U, int 
 }
 
 struct MsArgs {
-    const unsigned char* a_img;  // [groups][n_chunks][hi, lo][16 KB]
+    const float2* ac;            // A: [groups][n_chunks][kMsModes][kMsRcv] complex FP32
     const float2* q;             // [n_tiles][M_pad]
-    const float2* tab;           // [M_pad][kMsTabW]
+    const unsigned char* b_img;  // B' images: [n_chunks][32 KB]
     int M_pad, n_chunks, n_tiles, n_ranges, groups;
     long long n_units;           // groups * n_tiles * n_chunks
     float* raw;                  // [n_parts][groups][n_tiles][256 columns][128 rows] per-CTA partial tiles
@@ -322,7 +334,7 @@ struct UnitPos {
 template <int F>
 __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     extern __shared__ unsigned char ms_dyn[];
-    __shared__ __align__(8) uint64_t full_a[kMsAStages], empty_a[kMsAStages], full_b[kMsBStages], empty_b[kMsBStages];
+    __shared__ __align__(8) uint64_t full_t[kMsTStages], empty_t[kMsTStages], full_g[kMsGStages], empty_g[kMsGStages];
     __shared__ __align__(8) uint64_t acc_full[kMsAcc], acc_empty[kMsAcc], drain;
     __shared__ uint32_t tmem_base_sh;
     unsigned char* sm = (unsigned char*)(((uintptr_t)ms_dyn + 1023) & ~(uintptr_t)1023);
@@ -333,13 +345,13 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     const int nc = (int)(a.n_units * (blockIdx.x + 1) / gridDim.x - u0);
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kMsAStages; ++s) {
-            mbar_init(&full_a[s], 1);
-            mbar_init(&empty_a[s], 1);
+        for (int s = 0; s < kMsTStages; ++s) {
+            mbar_init(&full_t[s], 1);
+            mbar_init(&empty_t[s], 1);
         }
-        for (int s = 0; s < kMsBStages; ++s) {
-            mbar_init(&full_b[s], kMsGenWarps);
-            mbar_init(&empty_b[s], 1);
+        for (int s = 0; s < kMsGStages; ++s) {
+            mbar_init(&full_g[s], kMsGenWarps);
+            mbar_init(&empty_g[s], 1);
         }
         for (int b = 0; b < kMsAcc; ++b) {
             mbar_init(&acc_full[b], 1);
@@ -361,32 +373,31 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
 
     if (warp == kMsProducerWarp) {
         if (lane == 0 && nc > 0) {
-            // producer: bulk TMA of the A' chunk, factor rows and tile phases
-            // into A stage c % kMsAStages once the MMAs of chunk c - kMsAStages are done
+            // producer: bulk TMA of the B' image, A and tile phases of chunk c
+            // into TMA stage c % kMsTStages once the MMAs of chunk c - kMsTStages are done
             UnitPos pos;
             pos.init(u0, a.n_chunks, a.n_tiles);
             int issued = 0, landed = 0;
             bool ok = true;
             for (int c = 0; c < nc; ++c, pos.next(a.n_chunks, a.n_tiles)) {
-                const int slot = c % kMsAStages;
-                if (c >= kMsAStages) {
-                    ok = mbar_wait_bounded(&empty_a[slot], (uint32_t)(((c / kMsAStages) - 1) & 1), a.err);
+                const int slot = c % kMsTStages;
+                if (c >= kMsTStages) {
+                    ok = mbar_wait_bounded(&empty_t[slot], (uint32_t)(((c / kMsTStages) - 1) & 1), a.err);
                     if (!ok) break;
-                    landed = c - kMsAStages + 1;  // its copies were consumed, so they landed
+                    landed = c - kMsTStages + 1;  // its copies were consumed, so they landed
                 }
-                unsigned char* dst = sm + slot * kMsAStageBytes;
-                mbar_expect_tx(&full_a[slot], kMsTxBytes);
-                tma_load_1d(dst, a.a_img + ((size_t)pos.group * a.n_chunks + pos.chunk) * 2 * kMsABytes,
-                            2 * kMsABytes, &full_a[slot]);
-                tma_load_1d(dst + kMsOffTab, a.tab + (size_t)pos.chunk * kMsModes * kMsTabW, kMsTabBytes,
-                            &full_a[slot]);
+                unsigned char* dst = sm + slot * kMsTStageBytes;
+                mbar_expect_tx(&full_t[slot], kMsTxBytes);
+                tma_load_1d(dst, a.b_img + (size_t)pos.chunk * 2 * kMsBBytes, 2 * kMsBBytes, &full_t[slot]);
+                tma_load_1d(dst + kMsOffAC, a.ac + ((size_t)pos.group * a.n_chunks + pos.chunk) * kMsModes * kMsRcv,
+                            kMsACBytes, &full_t[slot]);
                 tma_load_1d(dst + kMsOffQ, a.q + (size_t)pos.tile * a.M_pad + pos.chunk * kMsModes, kMsQBytes,
-                            &full_a[slot]);
+                            &full_t[slot]);
                 ++issued;
             }
             // copies still in flight after an early exit: wait for them
             for (int c = landed; c < issued; ++c)
-                mbar_wait_drain(&full_a[c % kMsAStages], (uint32_t)((c / kMsAStages) & 1));
+                mbar_wait_drain(&full_t[c % kMsTStages], (uint32_t)((c / kMsTStages) & 1));
         }
     } else if (warp == 0) {
         if (lane == 0 && nc > 0) {
@@ -407,14 +418,15 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                         tc_fence_after();
                     }
                 }
-                const int sa = c % kMsAStages, sb = c % kMsBStages;
-                ok = mbar_wait_bounded(&full_a[sa], (uint32_t)((c / kMsAStages) & 1), a.err) &&
-                     mbar_wait_bounded(&full_b[sb], (uint32_t)((c / kMsBStages) & 1), a.err);
+                const int stt = c % kMsTStages, sg_ = c % kMsGStages;
+                ok = mbar_wait_bounded(&full_t[stt], (uint32_t)((c / kMsTStages) & 1), a.err) &&
+                     mbar_wait_bounded(&full_g[sg_], (uint32_t)((c / kMsGStages) & 1), a.err);
                 if (!ok) break;
                 tc_fence_after();
-                // descriptors: the start-address field counts 16-byte units
-                const uint64_t st = dsc0 + (uint64_t)((sa * kMsAStageBytes) >> 4);
-                const uint64_t stb = dsc0 + (uint64_t)((kMsOffBRing + sb * kMsBStageBytes) >> 4);
+                // descriptors: the start-address field counts 16-byte units;
+                // A' from the generated ring, B' from the TMA stage
+                const uint64_t st = dsc0 + (uint64_t)((kMsOffGRing + sg_ * kMsGStageBytes) >> 4);
+                const uint64_t stb = dsc0 + (uint64_t)((stt * kMsTStageBytes) >> 4);
                 const uint32_t d = tmem + (uint32_t)((sg & 1) * kMsNT);
                 if (F == kMsTf32) {
                     // K = 8 tf32 (32 B) per MMA, four per chunk
@@ -434,8 +446,8 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                         umma_bf16(d, al, bh, 1u);
                     }
                 }
-                umma_commit(&empty_a[sa]);
-                umma_commit(&empty_b[sb]);
+                umma_commit(&empty_t[stt]);
+                umma_commit(&empty_g[sg_]);
                 if (last) umma_commit(&acc_full[sg & 1]);
             }
             if (!ok) {
@@ -449,10 +461,12 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             mbar_wait_drain(&drain, 0u);
         }
     } else {
-        // B' generators: thread -> (i = range in its 8-group, q = mode quad,
-        // part = which 32 ranges of the tile); one warp per part
+        // A' generators: thread -> (receiver j of the group, mode quad q4);
+        // A'(tile) = A diag(e^{i k r_n0}) in the real block form
+        // [[Re, -Im], [Im, Re]]: row j holds (Re, -Im) and row j + 64 (Im, Re)
+        // of the 4 modes' products at k = 8 q4 .. 8 q4 + 7
         const int t = threadIdx.x - 32;
-        const int i = t & 7, q = (t >> 3) & 3, part = t >> 5;
+        const int j = t & (kMsRcv - 1), q4 = t >> 6;
         const int col_half = (warp - 1) >> 2;  // epilogue: accumulator columns [128 col_half, +128)
         bool ok = true;
         int sg = -1;
@@ -462,53 +476,47 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             const bool first = c == 0 || pos.chunk == 0;
             const bool last = c == nc - 1 || pos.chunk == a.n_chunks - 1;
             if (first) ++sg;
-            const int sa = c % kMsAStages, sb = c % kMsBStages;
-            if (c >= kMsBStages) {  // B stage free once the MMAs of chunk c - kMsBStages are done
-                ok = mbar_wait_bounded(&empty_b[sb], (uint32_t)(((c / kMsBStages) - 1) & 1), a.err);
+            const int stt = c % kMsTStages, sgs = c % kMsGStages;
+            if (c >= kMsGStages) {  // A' stage free once the MMAs of chunk c - kMsGStages are done
+                ok = mbar_wait_bounded(&empty_g[sgs], (uint32_t)(((c / kMsGStages) - 1) & 1), a.err);
                 if (!ok) break;
             }
-            // factor rows and tile phases of this chunk arrive with its A' copy
-            ok = mbar_wait_bounded(&full_a[sa], (uint32_t)((c / kMsAStages) & 1), a.err);
+            ok = mbar_wait_bounded(&full_t[stt], (uint32_t)((c / kMsTStages) & 1), a.err);
             if (!ok) break;
-            const unsigned char* stg = sm + sa * kMsAStageBytes;
-            const float2* tab_s = reinterpret_cast<const float2*>(stg + kMsOffTab);
+            const unsigned char* stg = sm + stt * kMsTStageBytes;
+            const float2* ac_s = reinterpret_cast<const float2*>(stg + kMsOffAC);
             const float2* q_s = reinterpret_cast<const float2*>(stg + kMsOffQ);
-            float2 e[4], w[4];
+            float2 e[4];
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const float2* tb = tab_s + (4 * q + v) * kMsTabW;
-                e[v] = cmulf(cmulf(q_s[4 * q + v], tb[i]), tb[8 + part]);
-                w[v] = tb[16];
-            }
-            const uint32_t bh = sm_addr + kMsOffBRing + sb * kMsBStageBytes;
+            for (int v = 0; v < 4; ++v) e[v] = cmulf(ac_s[(4 * q4 + v) * kMsRcv + j], q_s[4 * q4 + v]);
+            const uint32_t gb = sm_addr + kMsOffGRing + sgs * kMsGStageBytes;
+            if (F == kMsTf32) {
+                const uint32_t r0 = gb + sw128_off(j, 8 * q4), r1 = gb + sw128_off(j + kMsRcv, 8 * q4);
+                sts128(r0, to_tf32(e[0].x), to_tf32(-e[0].y), to_tf32(e[1].x), to_tf32(-e[1].y));
+                sts128(gb + sw128_off(j, 8 * q4 + 4), to_tf32(e[2].x), to_tf32(-e[2].y), to_tf32(e[3].x),
+                       to_tf32(-e[3].y));
+                sts128(r1, to_tf32(e[0].y), to_tf32(e[0].x), to_tf32(e[1].y), to_tf32(e[1].x));
+                sts128(gb + sw128_off(j + kMsRcv, 8 * q4 + 4), to_tf32(e[2].y), to_tf32(e[2].x), to_tf32(e[3].y),
+                       to_tf32(e[3].x));
+            } else {
+                uint32_t hr[4], lr[4], hm[4], lm[4];
 #pragma unroll
-            for (int st8 = 0; st8 < 4; ++st8) {
-                const int grp = part * 4 + st8;  // 8-range group within the tile
-                if (F == kMsTf32) {
-                    // modes 4q, 4q+1 -> k = 8q .. 8q+3; modes 4q+2, 4q+3 -> k = 8q+4 .. 8q+7
-                    sts128(bh + sw128_off(grp * 8 + i, 8 * q), to_tf32(e[0].x), to_tf32(e[0].y), to_tf32(e[1].x),
-                           to_tf32(e[1].y));
-                    sts128(bh + sw128_off(grp * 8 + i, 8 * q + 4), to_tf32(e[2].x), to_tf32(e[2].y), to_tf32(e[3].x),
-                           to_tf32(e[3].y));
-                } else {
-                    const uint32_t off = sw64_off(grp * 8 + i, 8 * q);
-                    uint32_t h[4], l[4];
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) split2(e[v], h[v], l[v]);
-                    sts128(bh + off, h[0], h[1], h[2], h[3]);
-                    sts128(bh + kMsBBytes + off, l[0], l[1], l[2], l[3]);
+                for (int v = 0; v < 4; ++v) {
+                    split2(make_float2(e[v].x, -e[v].y), hr[v], lr[v]);
+                    split2(make_float2(e[v].y, e[v].x), hm[v], lm[v]);
                 }
-                if (st8 < 3) {
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) e[v] = cmulf(e[v], w[v]);
-                }
+                const uint32_t o0 = sw64_off(j, 8 * q4), o1 = sw64_off(j + kMsRcv, 8 * q4);
+                sts128(gb + o0, hr[0], hr[1], hr[2], hr[3]);
+                sts128(gb + kMsABytes + o0, lr[0], lr[1], lr[2], lr[3]);
+                sts128(gb + o1, hm[0], hm[1], hm[2], hm[3]);
+                sts128(gb + kMsABytes + o1, lm[0], lm[1], lm[2], lm[3]);
             }
             // every lane's writes visible to the tensor cores, then one
             // arrival per warp
             fence_proxy_async();
             __syncwarp();
             if (lane == 0)
-                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full_b[sb])) : "memory");
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full_g[sgs])) : "memory");
             if (!last) continue;
             // epilogue of segment sg: TMEM lanes 32 (warp % 4) .. +31 = rows;
             // the partial sum goes to slot (this CTA - first CTA of the tile)
@@ -641,9 +649,9 @@ MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms) {
         const int parts = ms_cta_of(uf + p.n_chunks - 1, p.n_units, p.n_ctas) - ms_cta_of(uf, p.n_units, p.n_ctas) + 1;
         p.n_parts = std::max(p.n_parts, parts);
     }
-    p.a_img_bytes = (size_t)p.groups * p.n_chunks * 2 * kMsABytes;
+    p.a_img_bytes = (size_t)p.groups * p.n_chunks * kMsACBytes;  // A, complex FP32
     p.q_bytes = (size_t)p.n_tiles * p.M_pad * sizeof(float2);
-    p.tab_bytes = (size_t)p.M_pad * kMsTabW * sizeof(float2);
+    p.tab_bytes = (size_t)p.n_chunks * 2 * kMsBBytes;              // B' images
     p.raw_bytes = (size_t)p.n_parts * p.groups * p.n_tiles * kMsNT * kMsRows * sizeof(float);
     return p;
 }
@@ -655,18 +663,19 @@ int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const do
     return 1;
 }
 
+// a_img receives A (complex FP32), tab the B' images, q the tile phases
 int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int M, const double* kr,
                       const double* ki, const double* vs, const int* idx, const double* vfull, double dr, int lossless,
                       void* a_img, void* q, void* tab) {
     if (fmt != kMsBf16x3 && fmt != kMsTf32) return -1;
-    const long long n_tab = (long long)p.M_pad * kMsTabW;
+    const long long n_b = (long long)p.n_chunks * kMsNT * kMsModes;
     const long long n_q = (long long)p.n_tiles * p.M_pad;
-    const long long n_a = (long long)p.groups * p.n_chunks * kMsRows * kMsKC;
-    const long long b_tab = (n_tab + 255) / 256, b_q = (n_q + 255) / 256, b_a = (n_a + 255) / 256;
+    const long long n_a = (long long)p.groups * p.n_chunks * kMsModes * kMsRcv;
+    const long long b_b = (n_b + 255) / 256, b_q = (n_q + 255) / 256, b_a = (n_a + 255) / 256;
     auto kern = fmt == kMsTf32 ? k_ms_prepare<kMsTf32> : k_ms_prepare<kMsBf16x3>;
-    kern<<<(unsigned)(b_tab + b_q + b_a), 256, 0, st>>>(b_tab, b_q, n_rcv, M, p.M_pad, p.n_tiles, p.n_chunks, kr, ki,
-                                                       vs, idx, vfull, dr, lossless, (float2*)tab, (float2*)q,
-                                                       (unsigned char*)a_img);
+    kern<<<(unsigned)(b_b + b_q + b_a), 256, 0, st>>>(b_b, b_q, n_rcv, M, p.M_pad, p.n_tiles, p.n_chunks, kr, ki, vs,
+                                                     idx, vfull, dr, lossless, (unsigned char*)tab, (float2*)q,
+                                                     (float2*)a_img);
     return 1;
 }
 
@@ -684,9 +693,9 @@ int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const 
         attr_set[fmt][dev] = true;  // setting it twice from two threads is harmless
     }
     MsArgs a;
-    a.a_img = (const unsigned char*)a_img;
+    a.ac = (const float2*)a_img;
     a.q = (const float2*)q;
-    a.tab = (const float2*)tab;
+    a.b_img = (const unsigned char*)tab;
     a.M_pad = p.M_pad;
     a.n_chunks = p.n_chunks;
     a.n_tiles = p.n_tiles;
