@@ -57,7 +57,7 @@ METRIC = "freq-solves/s"
 # workloads (profiles/ess_modbb256_dram_bytes.md, k_bisect;
 # profiles/k_ms_tc_modal_sum_64rcv_20000rng.md, k_ms_tc)
 TRAFFIC_BISECT = 42437888
-TRAFFIC_MS_TC = 2508800
+TRAFFIC_MS_TC = 4422400
 NZ = 20000
 NFREQ = 256
 RANGES_KM = np.arange(200.0, 300.0 + 1e-9, 10.0)
