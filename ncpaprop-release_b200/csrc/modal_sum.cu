@@ -186,42 +186,59 @@ __device__ __forceinline__ void sts128(uint32_t addr, uint32_t a, uint32_t b, ui
 // per-mode FP32 factors from FP64: entries 0-7 e^{i k i dr}, 8-15
 // B' chunk images: B'[o][2m] = Re, B'[o][2m + 1] = Im of e^{i k_m o dr}
 // (o = 0 .. 255, the range offset inside a tile; attenuation included unless
-// lossless), in FP64 and then split (bf16 hi, lo) or rounded (TF32), in the
+// lossless) in FP64, then split (bf16 hi, lo) or rounded (TF32), in the
 // shared-memory layout of the operand; zero for the padding modes m >= M.
 // The images do not depend on the tile: the tile's phase e^{i k r_n0} goes
-// into A'.
+// into A'.  A thread covers kMsBRun consecutive ranges of one mode: one
+// sincos / exp at the first, FP64 complex steps by e^{i k dr} after it.
+constexpr int kMsBRun = 8;
+
 template <int F>
 __device__ void ms_b_entry(long long id, int M, int n_chunks, const double* __restrict__ kr,
                            const double* __restrict__ ki, double dr, int lossless, unsigned char* __restrict__ img) {
-    const long long per_chunk = (long long)kMsNT * kMsModes;
+    constexpr int kRuns = kMsNT / kMsBRun;
+    const long long per_chunk = (long long)kRuns * kMsModes;
     if (id >= (long long)n_chunks * per_chunk) return;
-    const int o = (int)(id % kMsNT);
-    const int ml = (int)((id / kMsNT) % kMsModes);
+    const int o0 = (int)(id % kRuns) * kMsBRun;
+    const int ml = (int)((id / kRuns) % kMsModes);
     const int chunk = (int)(id / per_chunk);
     const int m = chunk * kMsModes + ml;
-    float re = 0.f, im = 0.f;
+    double cr = 0.0, ci = 0.0, sr = 1.0, si = 0.0;  // value at o0 and the step
     if (m < M) {
-        const double x = (double)o * dr;
+        const double b = lossless ? 0.0 : ki[m];
+        const double x = (double)o0 * dr;
         double sn, cs;
         sincos(kr[m] * x, &sn, &cs);
-        const double amp = lossless ? 1.0 : exp(-ki[m] * x);
-        re = (float)(amp * cs);
-        im = (float)(amp * sn);
+        const double amp = exp(-b * x);
+        cr = amp * cs;
+        ci = amp * sn;
+        sincos(kr[m] * dr, &sn, &cs);
+        const double ad = exp(-b * dr);
+        sr = ad * cs;
+        si = ad * sn;
     }
-    unsigned char* ci = img + (size_t)chunk * 2 * kMsBBytes;  // 32 KB per chunk
-    if (F == kMsTf32) {
-        *reinterpret_cast<uint32_t*>(ci + sw128_off(o, 2 * ml)) = to_tf32(re);
-        *reinterpret_cast<uint32_t*>(ci + sw128_off(o, 2 * ml + 1)) = to_tf32(im);
-    } else {
-        const __nv_bfloat16 hr = __float2bfloat16_rn(re), hm = __float2bfloat16_rn(im);
-        const __nv_bfloat16 lr = __float2bfloat16_rn(re - __bfloat162float(hr));
-        const __nv_bfloat16 li = __float2bfloat16_rn(im - __bfloat162float(hm));
-        __nv_bfloat16* bm = reinterpret_cast<__nv_bfloat16*>(ci);
-        const size_t o0 = sw64_off(o, 2 * ml) / 2, o1 = sw64_off(o, 2 * ml + 1) / 2;
-        bm[o0] = hr;
-        bm[o1] = hm;
-        bm[kMsBBytes / 2 + o0] = lr;
-        bm[kMsBBytes / 2 + o1] = li;
+    unsigned char* cimg = img + (size_t)chunk * 2 * kMsBBytes;  // 32 KB per chunk
+#pragma unroll 1
+    for (int u = 0; u < kMsBRun; ++u) {
+        const int o = o0 + u;
+        const float re = (float)cr, im = (float)ci;
+        if (F == kMsTf32) {
+            *reinterpret_cast<uint32_t*>(cimg + sw128_off(o, 2 * ml)) = to_tf32(re);
+            *reinterpret_cast<uint32_t*>(cimg + sw128_off(o, 2 * ml + 1)) = to_tf32(im);
+        } else {
+            const __nv_bfloat16 hr = __float2bfloat16_rn(re), hm = __float2bfloat16_rn(im);
+            const __nv_bfloat16 lr = __float2bfloat16_rn(re - __bfloat162float(hr));
+            const __nv_bfloat16 li = __float2bfloat16_rn(im - __bfloat162float(hm));
+            __nv_bfloat16* bm = reinterpret_cast<__nv_bfloat16*>(cimg);
+            const size_t p0 = sw64_off(o, 2 * ml) / 2, p1 = sw64_off(o, 2 * ml + 1) / 2;
+            bm[p0] = hr;
+            bm[p1] = hm;
+            bm[kMsBBytes / 2 + p0] = lr;
+            bm[kMsBBytes / 2 + p1] = li;
+        }
+        const double nr = fma(cr, sr, -ci * si), ni = fma(cr, si, ci * sr);
+        cr = nr;
+        ci = ni;
     }
 }
 
@@ -668,7 +685,7 @@ int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int 
                       const double* ki, const double* vs, const int* idx, const double* vfull, double dr, int lossless,
                       void* a_img, void* q, void* tab) {
     if (fmt != kMsBf16x3 && fmt != kMsTf32) return -1;
-    const long long n_b = (long long)p.n_chunks * kMsNT * kMsModes;
+    const long long n_b = (long long)p.n_chunks * (kMsNT / kMsBRun) * kMsModes;
     const long long n_q = (long long)p.n_tiles * p.M_pad;
     const long long n_a = (long long)p.groups * p.n_chunks * kMsModes * kMsRcv;
     const long long b_b = (n_b + 255) / 256, b_q = (n_q + 255) / 256, b_a = (n_a + 255) / 256;
