@@ -969,11 +969,9 @@ template <class Row>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
     k_bisect(const ProblemInfo* __restrict__ pinfo, const double* __restrict__ s, const int* __restrict__ counts,
              const WorkItem* __restrict__ items, int n_items, int* counter, double tol_in, double* __restrict__ mu,
-             unsigned* err, unsigned long long* step_counter, const int* __restrict__ n_items_dev,
-             const int* __restrict__ item_lo_dev) {
+             unsigned* err, unsigned long long* step_counter, const int* __restrict__ n_items_dev) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     if (n_items_dev) n_items = *n_items_dev;
-    const int item_lo = item_lo_dev ? *item_lo_dev : 0;  // items [item_lo, n_items)
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     WarpRing r;
     r.buf = reinterpret_cast<double*>(smem_raw) + (size_t)wid * kWBuf * kWChunk;
@@ -988,7 +986,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
     // first wave, so the items spread evenly over the SMs whatever the grid
     (void)counter;
     const int warps_total = gridDim.x * kWarpsPerCta;
-    for (int it = item_lo + blockIdx.x * kWarpsPerCta + wid; it < n_items; it += warps_total) {
+    for (int it = blockIdx.x * kWarpsPerCta + wid; it < n_items; it += warps_total) {
         const WorkItem w = items[it];
         const ProblemInfo pi = pinfo[w.problem];
         const int* cnt = counts + (size_t)w.problem * kScanPoints;
@@ -1131,11 +1129,11 @@ static size_t bisect_smem() { return (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8
 template <class Row>
 static int bisect_launch(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
                          const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
-                         unsigned long long* step_counter, const int* n_items_dev, const int* item_lo_dev) {
+                         unsigned long long* step_counter, const int* n_items_dev) {
     const size_t sm = bisect_smem();
     cudaFuncSetAttribute(k_bisect<Row>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_bisect<Row><<<grid, kWarpsPerCta * 32, sm, st>>>(pinfo, s, counts, items, n_items, counter, tol, mu, err,
-                                                       step_counter, n_items_dev, item_lo_dev);
+                                                       step_counter, n_items_dev);
     return 1;
 }
 
@@ -1151,9 +1149,9 @@ static int bisect_fit() {
 
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
                   const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
-                  unsigned long long* step_counter, const int* n_items_dev, const int* item_lo_dev) {
+                  unsigned long long* step_counter, const int* n_items_dev) {
     return bisect_launch<EssRows>(st, grid, pinfo, s, counts, items, n_items, counter, tol, mu, err, step_counter,
-                                  n_items_dev, item_lo_dev);
+                                  n_items_dev);
 }
 
 int bisect_ctas_per_sm() { return bisect_fit<EssRows>(); }
@@ -1162,7 +1160,7 @@ int launch_bisect_wmod(cudaStream_t st, int grid, const ProblemInfo* pinfo, cons
                        const WorkItem* items, double tol, double* mu, unsigned* err,
                        unsigned long long* step_counter, const int* n_items_dev) {
     return bisect_launch<WmodRows>(st, grid, pinfo, rows, counts, items, 0, nullptr, tol, mu, err, step_counter,
-                                   n_items_dev, nullptr);
+                                   n_items_dev);
 }
 
 int bisect_wmod_ctas_per_sm() { return bisect_fit<WmodRows>(); }
@@ -1194,8 +1192,7 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
                                                              const int* __restrict__ counts, int max_modes,
                                                              int bis_item, WorkItem* __restrict__ bis, int bis_cap,
                                                              WorkItem* __restrict__ ev, int ev_cap,
-                                                             int* __restrict__ tot, unsigned* __restrict__ err,
-                                                             int split_p) {
+                                                             int* __restrict__ tot, unsigned* __restrict__ err) {
     __shared__ int sh[kItemThreads];
     int base_m = 0, base_b = 0, base_e = 0;
     for (int p0 = 0; p0 < P; p0 += kItemThreads) {
@@ -1219,10 +1216,6 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
         const int om = block_exclusive_scan(M, sh, &tm);
         const int ob = block_exclusive_scan(nb, sh, &tb);
         const int oe = block_exclusive_scan(ne, sh, &te);
-        if (p < P && p == split_p) {  // first items of the problems from split_p on
-            tot[3] = min(base_b + ob, bis_cap);
-            tot[4] = min(base_e + oe, ev_cap);
-        }
         if (p < P) {
             pinfo[p].off = base_m + om;
             for (int k = 0; k < nb; ++k) {
@@ -1244,19 +1237,14 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
         tot[0] = min(base_b, bis_cap);
         tot[1] = min(base_e, ev_cap);
         tot[2] = base_m;
-        if (split_p >= P) {  // (split_p < 0: no split offsets; tot may hold 4 ints)
-            tot[3] = tot[0];
-            tot[4] = tot[1];
-        }
     }
 }
 
 int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes, int bis_item,
-                      WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err,
-                      int split_p) {
+                      WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err) {
     if (bis_item < 1 || bis_item > kWItem) return -1;
     k_make_items<<<1, kItemThreads, 0, st>>>(P, pinfo, counts, max_modes, bis_item, bis_items, bis_cap, ev_items,
-                                             ev_cap, tot, err, split_p);
+                                             ev_cap, tot, err);
     return 1;
 }
 
@@ -1425,10 +1413,9 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
         }
     };
     const int n_items_all = A.n_items_dev ? *A.n_items_dev : A.n_items;
-    const int item_lo = A.items_lo_dev ? *A.items_lo_dev : 0;  // items [item_lo, n_items_all)
     // static round-robin over the grid's warps (see k_bisect)
     const int warps_total = gridDim.x * kEvWarps;
-    for (int it = item_lo + blockIdx.x * kEvWarps + wid; it < n_items_all; it += warps_total) {
+    for (int it = blockIdx.x * kEvWarps + wid; it < n_items_all; it += warps_total) {
         const WorkItem w = A.items[it];
         const ProblemInfo pi = A.pinfo[w.problem];
         nz = pi.nz;

@@ -84,8 +84,7 @@ int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* 
 // accumulates the Sturm recurrence steps swept
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
                   const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
-                  unsigned long long* step_counter, const int* n_items_dev = nullptr,
-                  const int* item_lo_dev = nullptr);  // items [*item_lo_dev, n_items)
+                  unsigned long long* step_counter, const int* n_items_dev = nullptr);
 int bisect_ctas_per_sm();
 // FP64 throughput probe: each thread runs n_iter iterations of 8 independent
 // FMA chains; out receives a value that keeps the chains live
@@ -99,7 +98,6 @@ struct EigvecArgs {
     const WorkItem* items;
     int n_items;
     const int* n_items_dev;  // when set, the item count is read here (built on the device)
-    const int* items_lo_dev; // when set, the first item is read here (items [*items_lo_dev, n_items))
     int* counter;
     const double* mu;
     double* kr;
@@ -121,11 +119,8 @@ int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a);
 // balanced inside a problem) and eigenvector items (kEvItem) appended;
 // tot = {n_bisect_items, n_eigvec_items, total modes}.  Sets kErrTooMany if a
 // problem exceeds max_modes (its M is then clamped) or a capacity is exceeded.
-// split_p >= 0 also writes tot[3], tot[4]: the first bisection / eigenvector
-// item of the problems split_p .. P-1 (tot then holds at least 5 ints)
 int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes, int bis_item,
-                      WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err,
-                      int split_p = -1);
+                      WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err);
 // resident eigenvector CTAs per SM for the variant selected by a
 int eigvec_ctas_per_sm(const EigvecArgs& a);
 // modal sums

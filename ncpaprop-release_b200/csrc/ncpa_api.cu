@@ -115,12 +115,6 @@ struct ncpa_ctx {
     DevBuf bb_out;                 // waveforms kept in HBM (NULL host buffer)
     DevBuf ms_img, ms_q, ms_tab, ms_raw, ms_vz, ms_idx, ms_re, ms_im;  // modal-sum scratch (grow-only)
     int item_override = 0;         // eigenvalues per bisection item (0: chosen per solve); NCPA_BISECT_ITEM
-    // second stream of the split eigen-solve: the bisection and eigenvectors
-    // of the second half of the problems run on it, beside the first half's
-    // (NCPA_SPLIT_SOLVE=0 turns the split off)
-    cudaStream_t stream2 = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    bool split_solve = true;
     double* h_pin = nullptr;       // small pinned host buffer for scalars read back per solve
     int* h_tot = nullptr;          // pinned: item and mode totals of a device-built solve
     size_t h_pin_n = 0;
@@ -500,7 +494,7 @@ void prepare_solve(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, int
     b.ev_cap = P * ((cap_modes + ncpa::kEvItem - 1) / ncpa::kEvItem);
     b.bis.alloc((size_t)b.bis_cap * sizeof(WorkItem), st);
     b.ev.alloc((size_t)b.ev_cap * sizeof(WorkItem), st);
-    b.tot.alloc(8 * sizeof(int), st);  // totals and the split offsets
+    b.tot.alloc(4 * sizeof(int), st);
     b.mu.alloc(mcap * 8, st);
     b.counter.alloc(2 * sizeof(int), st);
     M->d_kr.alloc(mcap * 8, st);
@@ -511,9 +505,7 @@ void prepare_solve(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, int
     const ncpa::EigvecArgs ea = eigvec_args(ctx, M, prm, s, w, gs, b);
     const int grid_e = eigvec_grid(ctx, ea, b.ev_cap, 0);  // the largest grid
     const long long slot = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
-    // twice the largest grid's slots: the two halves of a split solve run
-    // their eigenvector kernels at the same time
-    const size_t need = 2 * (size_t)grid_e * ncpa::kEvWarpsPerCta * slot;
+    const size_t need = (size_t)grid_e * ncpa::kEvWarpsPerCta * slot;
     DevBuf& c1 = b.own_ck ? b.ck1 : ctx->ck1;
     DevBuf& c2 = b.own_ck ? b.ck2 : ctx->ck2;
     DevBuf& ce = b.own_ck ? b.cke : ctx->cke;
@@ -542,62 +534,28 @@ void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_
     // ---- K3a scan ----
     check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s, b.counts.as<int>(), err));
     tm.mark("scan");
-    // split solve: the problems [P/2, P) run their bisection and eigenvectors
-    // on the second stream, so the eigenvectors of one half overlap the
-    // other half's bisection tail (not with per-phase timing or step counts,
-    // which time the kernels alone)
-    const bool split = ctx->split_solve && !ctx->timing && !ctx->stats && !count_steps && P >= 2;
     check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, b.counts.as<int>(), M->prm.max_modes, t.bis_item,
                                               b.bis.as<WorkItem>(), b.bis_cap, b.ev.as<WorkItem>(), b.ev_cap,
-                                              b.tot.as<int>(), err, split ? P / 2 : -1));
+                                              b.tot.as<int>(), err));
     CK(cudaMemsetAsync(b.counter.p, 0, 2 * sizeof(int), st));
     tm.mark("host-items");
+    // ---- K3 bisection ----
     const int fit_b = ncpa::bisect_ctas_per_sm();
     const int grid_b = ctx->num_sms * (t.bis_ctas > 0 ? std::min(t.bis_ctas, fit_b) : fit_b);
+    check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s, b.counts.as<int>(), b.bis.as<WorkItem>(), 0,
+                                          b.counter.as<int>(), kBisectTol, b.mu.as<double>(), err,
+                                          count_steps ? ctx->d_stats.as<unsigned long long>() : nullptr,
+                                          b.tot.as<int>()));
+    tm.mark("bisect");
+    // ---- K4 eigenvectors ----
     ncpa::EigvecArgs ea = eigvec_args(ctx, M, prm, s, w, gs, b);
     const int grid_e = eigvec_grid(ctx, ea, b.ev_cap, t.ev_ctas);
     ea.ck_q1 = (b.own_ck ? b.ck1 : ctx->ck1).as<double>();
     ea.ck_q2 = (b.own_ck ? b.ck2 : ctx->ck2).as<double>();
     ea.ck_e = (b.own_ck ? b.cke : ctx->cke).as<int>();
     ea.ck_slot_stride = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
-    int* tot = b.tot.as<int>();
-    if (split) {
-        cudaStream_t s2 = ctx->stream2;
-        CK(cudaEventRecord(ctx->ev_fork, st));
-        CK(cudaStreamWaitEvent(s2, ctx->ev_fork, 0));
-        // second half: items [tot[3], tot[0]) and [tot[4], tot[1]), its own
-        // checkpoint slots (the second half of the scratch)
-        check_launch(ctx, ncpa::launch_bisect(s2, grid_b, d_pinfo, s, b.counts.as<int>(), b.bis.as<WorkItem>(), 0,
-                                              b.counter.as<int>(), kBisectTol, b.mu.as<double>(), err, nullptr, tot,
-                                              tot + 3));
-        ncpa::EigvecArgs eb = ea;
-        eb.n_items_dev = tot + 1;
-        eb.items_lo_dev = tot + 4;
-        const size_t half = (size_t)grid_e * ncpa::kEvWarpsPerCta * (size_t)ea.ck_slot_stride;
-        eb.ck_q1 += half;
-        eb.ck_q2 += half;
-        eb.ck_e += half;
-        check_launch(ctx, ncpa::launch_eigvec(s2, grid_e, eb));
-        CK(cudaEventRecord(ctx->ev_join, s2));
-        // first half: items [0, tot[3]) and [0, tot[4])
-        check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s, b.counts.as<int>(), b.bis.as<WorkItem>(), 0,
-                                              b.counter.as<int>(), kBisectTol, b.mu.as<double>(), err, nullptr,
-                                              tot + 3));
-        tm.mark("bisect");
-        ea.n_items_dev = tot + 4;
-        check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
-        CK(cudaStreamWaitEvent(st, ctx->ev_join, 0));
-        tm.mark("eigvec");
-    } else {
-        // ---- K3 bisection ----
-        check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s, b.counts.as<int>(), b.bis.as<WorkItem>(), 0,
-                                              b.counter.as<int>(), kBisectTol, b.mu.as<double>(), err,
-                                              count_steps ? ctx->d_stats.as<unsigned long long>() : nullptr, tot));
-        tm.mark("bisect");
-        // ---- K4 eigenvectors ----
-        check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
-        tm.mark("eigvec");
-    }
+    check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
+    tm.mark("eigvec");
     CK(cudaMemcpyAsync(tot_dst, b.tot.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(info_dst, d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(err_dst, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
@@ -1302,10 +1260,6 @@ ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
         CK(cudaHostAlloc((void**)&ctx->h_tot, 64, cudaHostAllocDefault));
         const char* tv = std::getenv("NCPA_TIMING");
         ctx->timing = tv && tv[0] == '1';
-        CK(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
-        CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
-        if (const char* sv = std::getenv("NCPA_SPLIT_SOLVE")) ctx->split_solve = sv[0] != '0';
         // tuning override of the eigenvalues per bisection item (1..32)
         if (const char* iv = std::getenv("NCPA_BISECT_ITEM")) {
             const int v = std::atoi(iv);
@@ -1333,12 +1287,8 @@ ncpa_status ncpa_ctx_destroy(ncpa_ctx* ctx) {
                       &ctx->ms_im})
         b->release();  // stream-ordered frees need the stream alive
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
     if (ctx->h_tot) cudaFreeHost(ctx->h_tot);
-    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
-    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
-    if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NCPA_OK;
