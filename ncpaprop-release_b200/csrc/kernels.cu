@@ -963,6 +963,149 @@ __device__ void warp_sweep_tw(const double* __restrict__ s, int nz, double p_ini
     else warp_sweep_tw_mode<Row, 2>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0);
 }
 
+// One bisection work item (<= 32 eigenvalues of one problem) on this warp,
+// with its TMA ring r: the eigenvalues to mu in the row format's units.
+template <class Row>
+__device__ __forceinline__ void bisect_item(const ProblemInfo* __restrict__ pinfo, const double* __restrict__ s,
+                                            const int* __restrict__ counts, const WorkItem w, double tol_in,
+                                            double* __restrict__ mu, unsigned* err,
+                                            unsigned long long* step_counter, WarpRing& r) {
+    const int lane = threadIdx.x & 31;
+    const ProblemInfo pi = pinfo[w.problem];
+    const int* cnt = counts + (size_t)w.problem * kScanPoints;
+    const double* sp = s + (size_t)pi.s_off * Row::kW;
+    const int nz = pi.nz;
+    const double lo = Row::scan_lo(pi), hi = Row::scan_hi(pi);
+    const double tol = tol_in * Row::tol_scale(pi);
+    const double p_init = Row::p_init(pi);
+    // state of eigen slot `lane`
+    const int J = pi.c_lo + w.j0 + lane;
+    double a = lo, b = lo, x = lo;
+    double dprev = 0.0;  // size of the previous Newton correction (0: none yet)
+    int ca = 0, cb = 0, mode = 2;
+    if (lane < w.m) {  // initial bracket from the isolation scan
+        int t0 = 0;
+        for (int t = 0; t < kScanPoints; ++t)
+            if (cnt[t] <= J) t0 = t;
+        int t1 = kScanPoints - 1;
+        for (int t = kScanPoints - 1; t > t0; --t)
+            if (cnt[t] > J) t1 = t;
+        if (cnt[t1] <= J) atomicOr(err, kErrBracket);
+        a = scan_x(lo, hi, t0);
+        b = scan_x(lo, hi, t1);
+        ca = cnt[t0];
+        cb = cnt[t1];
+        x = 0.5 * (a + b);
+        mode = !(b - a > tol) ? 2 : ((ca == J && cb == J + 1) ? 1 : 0);
+    }
+    for (int round = 0; round < 512; ++round) {
+        const unsigned nm = __ballot_sync(0xffffffffu, mode == 1);
+        const unsigned bm = __ballot_sync(0xffffffffu, mode == 0);
+        const int nN = __popc(nm), nB = __popc(bm);
+        if (nN + nB == 0) break;
+        const int nlB = 64 - nN;
+        // roles of this lane's two virtual lanes v = lane + 32 h
+        double xv[2];
+        int gv[2], Gv[2];
+        bool newton0 = false;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int v = lane + 32 * h;
+            int e = 0;
+            gv[h] = 0;
+            Gv[h] = 1;
+            bool nt = false;
+            if (v < nN) {
+                nt = true;
+                e = nth_bit(nm, v);
+            } else if (nB > 0) {
+                const int t = v - nN, k = t % nB;
+                e = nth_bit(bm, k);
+                gv[h] = t / nB;
+                Gv[h] = (nlB - 1 - k) / nB + 1;
+            }
+            const double ae = __shfl_sync(0xffffffffu, a, e);
+            const double be = __shfl_sync(0xffffffffu, b, e);
+            const double xe = __shfl_sync(0xffffffffu, x, e);
+            xv[h] = nt ? xe : ae + (be - ae) * ((double)(gv[h] + 1) / (double)(Gv[h] + 1));
+            if (h == 0) newton0 = nt;
+        }
+        (void)newton0;
+        int cv0, cv1;
+        double rat;
+        const int smode = nN == 0 ? 0 : (nB > 0 ? 1 : 2);
+        warp_sweep_tw<Row>(sp, nz, p_init, xv[0], xv[1], smode, r, err, cv0, cv1, rat);
+        if (step_counter && lane == 0)
+            atomicAdd(step_counter, (unsigned long long)(smode == 2 ? 32 : 64) * (unsigned long long)nz);
+        // updates.  Every __shfl_sync is executed by all 32 lanes.
+        const bool isN = mode == 1, isB = mode == 0;
+        const int vN = isN ? __popc(nm & ((1u << lane) - 1u)) : 0;  // Newton virtual lane (chain 0)
+        const int cN = __shfl_sync(0xffffffffu, cv0, vN);
+        const double rN = __shfl_sync(0xffffffffu, rat, vN);
+        const int k = isB ? __popc(bm & ((1u << lane) - 1u)) : 0;
+        const int G = isB ? (nlB - 1 - k) / nB + 1 : 0;
+        const int Gmax = nB > 0 ? (nlB - 1) / nB + 1 : 0;
+        int gb = -1, cgb = ca;
+        for (int g = 0; g < Gmax; ++g) {
+            const int v = nN + k + g * nB;
+            const int c0 = __shfl_sync(0xffffffffu, cv0, v & 31), c1 = __shfl_sync(0xffffffffu, cv1, v & 31);
+            const int c = (v >> 5) ? c1 : c0;
+            if (isB && g < G && c <= J) {
+                gb = g;
+                cgb = c;
+            }
+        }
+        const int g1 = gb + 1;
+        const int v1 = nN + k + g1 * nB;
+        const int src1 = (isB && g1 < G) ? (v1 & 31) : lane;
+        const int cU0 = __shfl_sync(0xffffffffu, cv0, src1), cU1 = __shfl_sync(0xffffffffu, cv1, src1);
+        if (isN) {
+            const double xo = x;
+            if (cN <= J) {
+                a = xo;
+                ca = cN;
+            } else {
+                b = xo;
+                cb = cN;
+            }
+            const double ad = fabs(rN);
+            if (ad <= tol) {
+                x = fmin(fmax(xo - rN, a), b);
+                mode = 2;
+            } else {
+                const double xn = xo - rN;
+                const bool ok = isfinite(xn) && xn > a && xn < b;
+                x = ok ? xn : 0.5 * (a + b);
+                if (!(b - a > tol)) {
+                    mode = 2;
+                } else if (ok && dprev > 0.0 && ad <= 0.25 * dprev && ad * ad * ad <= tol * dprev * dprev) {
+                    // quadratic convergence: the next correction would be
+                    // about ad^2 (ad / dprev^2) <= tol, so x = xn is final
+                    mode = 2;
+                }
+                dprev = ok ? ad : 0.0;
+            }
+        } else if (isB) {
+            const double A0 = a, B0 = b;
+            const double na = gb >= 0 ? A0 + (B0 - A0) * ((double)(gb + 1) / (double)(G + 1)) : A0;
+            const double nb = g1 < G ? A0 + (B0 - A0) * ((double)(gb + 2) / (double)(G + 1)) : B0;
+            if (gb >= 0) ca = cgb;
+            if (g1 < G) cb = (v1 >> 5) ? cU1 : cU0;
+            a = na;
+            b = nb;
+            x = 0.5 * (na + nb);
+            if (!(nb - na > tol) || (na == A0 && nb == B0)) {
+                mode = 2;
+            } else if (ca == J && cb == J + 1) {
+                mode = 1;  // isolated: safeguarded Newton from here
+            }
+        }
+        // a ring wait gave up: abandon the item (warp-uniform decision)
+        if (__any_sync(0xffffffffu, (*((volatile unsigned*)err) & kErrTimeout) != 0u)) break;
+    }
+    if (lane < w.m) mu[pi.off + w.j0 + lane] = x;
+}
+
 // Row: the row format (EssRows: shifts in h^2 k^2; WmodRows: kappa = h k);
 // tol is scaled per problem by Row::tol_scale.
 template <class Row>
@@ -986,142 +1129,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
     // first wave, so the items spread evenly over the SMs whatever the grid
     (void)counter;
     const int warps_total = gridDim.x * kWarpsPerCta;
-    for (int it = blockIdx.x * kWarpsPerCta + wid; it < n_items; it += warps_total) {
-        const WorkItem w = items[it];
-        const ProblemInfo pi = pinfo[w.problem];
-        const int* cnt = counts + (size_t)w.problem * kScanPoints;
-        const double* sp = s + (size_t)pi.s_off * Row::kW;
-        const int nz = pi.nz;
-        const double lo = Row::scan_lo(pi), hi = Row::scan_hi(pi);
-        const double tol = tol_in * Row::tol_scale(pi);
-        const double p_init = Row::p_init(pi);
-        // state of eigen slot `lane`
-        const int J = pi.c_lo + w.j0 + lane;
-        double a = lo, b = lo, x = lo;
-        double dprev = 0.0;  // size of the previous Newton correction (0: none yet)
-        int ca = 0, cb = 0, mode = 2;
-        if (lane < w.m) {  // initial bracket from the isolation scan
-            int t0 = 0;
-            for (int t = 0; t < kScanPoints; ++t)
-                if (cnt[t] <= J) t0 = t;
-            int t1 = kScanPoints - 1;
-            for (int t = kScanPoints - 1; t > t0; --t)
-                if (cnt[t] > J) t1 = t;
-            if (cnt[t1] <= J) atomicOr(err, kErrBracket);
-            a = scan_x(lo, hi, t0);
-            b = scan_x(lo, hi, t1);
-            ca = cnt[t0];
-            cb = cnt[t1];
-            x = 0.5 * (a + b);
-            mode = !(b - a > tol) ? 2 : ((ca == J && cb == J + 1) ? 1 : 0);
-        }
-        for (int round = 0; round < 512; ++round) {
-            const unsigned nm = __ballot_sync(0xffffffffu, mode == 1);
-            const unsigned bm = __ballot_sync(0xffffffffu, mode == 0);
-            const int nN = __popc(nm), nB = __popc(bm);
-            if (nN + nB == 0) break;
-            const int nlB = 64 - nN;
-            // roles of this lane's two virtual lanes v = lane + 32 h
-            double xv[2];
-            int gv[2], Gv[2];
-            bool newton0 = false;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int v = lane + 32 * h;
-                int e = 0;
-                gv[h] = 0;
-                Gv[h] = 1;
-                bool nt = false;
-                if (v < nN) {
-                    nt = true;
-                    e = nth_bit(nm, v);
-                } else if (nB > 0) {
-                    const int t = v - nN, k = t % nB;
-                    e = nth_bit(bm, k);
-                    gv[h] = t / nB;
-                    Gv[h] = (nlB - 1 - k) / nB + 1;
-                }
-                const double ae = __shfl_sync(0xffffffffu, a, e);
-                const double be = __shfl_sync(0xffffffffu, b, e);
-                const double xe = __shfl_sync(0xffffffffu, x, e);
-                xv[h] = nt ? xe : ae + (be - ae) * ((double)(gv[h] + 1) / (double)(Gv[h] + 1));
-                if (h == 0) newton0 = nt;
-            }
-            (void)newton0;
-            int cv0, cv1;
-            double rat;
-            const int smode = nN == 0 ? 0 : (nB > 0 ? 1 : 2);
-            warp_sweep_tw<Row>(sp, nz, p_init, xv[0], xv[1], smode, r, err, cv0, cv1, rat);
-            if (step_counter && lane == 0)
-                atomicAdd(step_counter, (unsigned long long)(smode == 2 ? 32 : 64) * (unsigned long long)nz);
-            // updates.  Every __shfl_sync is executed by all 32 lanes.
-            const bool isN = mode == 1, isB = mode == 0;
-            const int vN = isN ? __popc(nm & ((1u << lane) - 1u)) : 0;  // Newton virtual lane (chain 0)
-            const int cN = __shfl_sync(0xffffffffu, cv0, vN);
-            const double rN = __shfl_sync(0xffffffffu, rat, vN);
-            const int k = isB ? __popc(bm & ((1u << lane) - 1u)) : 0;
-            const int G = isB ? (nlB - 1 - k) / nB + 1 : 0;
-            const int Gmax = nB > 0 ? (nlB - 1) / nB + 1 : 0;
-            int gb = -1, cgb = ca;
-            for (int g = 0; g < Gmax; ++g) {
-                const int v = nN + k + g * nB;
-                const int c0 = __shfl_sync(0xffffffffu, cv0, v & 31), c1 = __shfl_sync(0xffffffffu, cv1, v & 31);
-                const int c = (v >> 5) ? c1 : c0;
-                if (isB && g < G && c <= J) {
-                    gb = g;
-                    cgb = c;
-                }
-            }
-            const int g1 = gb + 1;
-            const int v1 = nN + k + g1 * nB;
-            const int src1 = (isB && g1 < G) ? (v1 & 31) : lane;
-            const int cU0 = __shfl_sync(0xffffffffu, cv0, src1), cU1 = __shfl_sync(0xffffffffu, cv1, src1);
-            if (isN) {
-                const double xo = x;
-                if (cN <= J) {
-                    a = xo;
-                    ca = cN;
-                } else {
-                    b = xo;
-                    cb = cN;
-                }
-                const double ad = fabs(rN);
-                if (ad <= tol) {
-                    x = fmin(fmax(xo - rN, a), b);
-                    mode = 2;
-                } else {
-                    const double xn = xo - rN;
-                    const bool ok = isfinite(xn) && xn > a && xn < b;
-                    x = ok ? xn : 0.5 * (a + b);
-                    if (!(b - a > tol)) {
-                        mode = 2;
-                    } else if (ok && dprev > 0.0 && ad <= 0.25 * dprev && ad * ad * ad <= tol * dprev * dprev) {
-                        // quadratic convergence: the next correction would be
-                        // about ad^2 (ad / dprev^2) <= tol, so x = xn is final
-                        mode = 2;
-                    }
-                    dprev = ok ? ad : 0.0;
-                }
-            } else if (isB) {
-                const double A0 = a, B0 = b;
-                const double na = gb >= 0 ? A0 + (B0 - A0) * ((double)(gb + 1) / (double)(G + 1)) : A0;
-                const double nb = g1 < G ? A0 + (B0 - A0) * ((double)(gb + 2) / (double)(G + 1)) : B0;
-                if (gb >= 0) ca = cgb;
-                if (g1 < G) cb = (v1 >> 5) ? cU1 : cU0;
-                a = na;
-                b = nb;
-                x = 0.5 * (na + nb);
-                if (!(nb - na > tol) || (na == A0 && nb == B0)) {
-                    mode = 2;
-                } else if (ca == J && cb == J + 1) {
-                    mode = 1;  // isolated: safeguarded Newton from here
-                }
-            }
-            // a ring wait gave up: abandon the item (warp-uniform decision)
-            if (__any_sync(0xffffffffu, (*((volatile unsigned*)err) & kErrTimeout) != 0u)) break;
-        }
-        if (lane < w.m) mu[pi.off + w.j0 + lane] = x;
-    }
+    for (int it = blockIdx.x * kWarpsPerCta + wid; it < n_items; it += warps_total)
+        bisect_item<Row>(pinfo, s, counts, items[it], tol_in, mu, err, step_counter, r);
 }
 
 static size_t bisect_smem() { return (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8 + kWBuf * 8); }
@@ -1192,7 +1201,8 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
                                                              const int* __restrict__ counts, int max_modes,
                                                              int bis_item, WorkItem* __restrict__ bis, int bis_cap,
                                                              WorkItem* __restrict__ ev, int ev_cap,
-                                                             int* __restrict__ tot, unsigned* __restrict__ err) {
+                                                             int* __restrict__ tot, unsigned* __restrict__ err,
+                                                             int* __restrict__ pstat) {
     __shared__ int sh[kItemThreads];
     int base_m = 0, base_b = 0, base_e = 0;
     for (int p0 = 0; p0 < P; p0 += kItemThreads) {
@@ -1216,6 +1226,12 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
         const int om = block_exclusive_scan(M, sh, &tm);
         const int ob = block_exclusive_scan(nb, sh, &tb);
         const int oe = block_exclusive_scan(ne, sh, &te);
+        if (p < P && pstat) {  // readiness data of the fused launch
+            const int e0 = min(base_e + oe, ev_cap);
+            pstat[p] = nb;                          // bisection items still to finish
+            pstat[P + p] = e0;                      // first eigenvector item
+            pstat[2 * P + p] = min(ne, ev_cap - e0);  // eigenvector items
+        }
         if (p < P) {
             pinfo[p].off = base_m + om;
             for (int k = 0; k < nb; ++k) {
@@ -1241,10 +1257,11 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
 }
 
 int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes, int bis_item,
-                      WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err) {
+                      WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err,
+                      int* pstat) {
     if (bis_item < 1 || bis_item > kWItem) return -1;
     k_make_items<<<1, kItemThreads, 0, st>>>(P, pinfo, counts, max_modes, bis_item, bis_items, bis_cap, ev_items,
-                                             ev_cap, tot, err);
+                                             ev_cap, tot, err, pstat);
     return 1;
 }
 
@@ -1375,6 +1392,306 @@ __device__ __forceinline__ void fwd_step(FwdState& F, int i, int nz, const doubl
     F.pm1 = pn;
 }
 
+// One eigenvector work item (<= 32 modes of one problem) on this warp, with
+// its TMA ring R and its checkpoint slot (ck1, ck2, cke).
+template <class Row, bool kGroup, bool kVec>
+__device__ __forceinline__ void eigvec_item(const EigvecArgs& A, const WorkItem w, EvRing& R, double* ck1,
+                                            double* ck2, int* cke) {
+    constexpr int kW = Row::kW;
+    const int lane = threadIdx.x & 31;
+    const ProblemInfo pi = A.pinfo[w.problem];
+    const int nz = pi.nz;
+    auto load_ck = [&](int kb, double& a1, double& a2, int& ae) {
+        if (min((kb + 1) * kBlk, nz) >= nz) {
+            a1 = 1.0;
+            a2 = 0.0;
+            ae = 0;
+        } else {
+            const size_t ci = (size_t)kb * 32 + lane;
+            a1 = ck1[ci];
+            a2 = ck2[ci];
+            ae = cke[ci];
+        }
+    };
+    const int nch = (nz + kEvC - 1) / kEvC;
+    const int nblk = (nz + kBlk - 1) / kBlk;
+    const int isrc = pi.isrc, ircv = pi.ircv;
+    const double* sp = A.s + (size_t)pi.s_off * kW;
+    const double* wp = A.w + pi.w_off;
+    const double* gp = kGroup ? A.g + pi.s_off : nullptr;
+    const bool active = lane < w.m;
+    // through L2: in the fused launch another warp wrote mu in this kernel
+    const double mu = active ? __ldcg(A.mu + pi.off + w.j0 + lane) : Row::idle_shift(pi);
+    const typename Row::Shift sh = Row::shift(mu);
+
+    // ---------------- pass 1: backward recurrence, checkpoints ----------
+    {
+        const unsigned base = R.loads;
+        if (lane == 0)
+            for (int o = 0; o < nch && o < kEvB; ++o)
+                evr_issue<kW>(R, base + o, nch - 1 - o, sp, nullptr, nullptr);
+        __syncwarp();
+        double q1 = 1.0, q2 = 0.0;  // q_i, q_{i+1}; q_n = 1, q_{n+1} = 0
+        int E = 0;
+        for (int o = 0; o < nch; ++o) {
+            const int c = nch - 1 - o;
+            const unsigned k = base + o;
+            const int slot = k % kEvB;
+            mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
+            const double* sb = R.s + slot * kEvC * kW;
+            const int valid = min(kEvC, nz - c * kEvC);
+            for (int lb = ((valid - 1) / kBlk) * kBlk; lb >= 0; lb -= kBlk) {
+                if (lb + kBlk <= valid) {
+#pragma unroll
+                    for (int u = kBlk - 1; u >= 0; --u) {
+                        const double qi = fma(Row::t(sb, lb + u, sh), q1, -q2);
+                        q2 = q1;
+                        q1 = qi;
+                    }
+                } else {
+                    for (int u = valid - 1 - lb; u >= 0; --u) {
+                        const double qi = fma(Row::t(sb, lb + u, sh), q1, -q2);
+                        q2 = q1;
+                        q1 = qi;
+                    }
+                }
+                const int gbase = c * kEvC + lb;
+                if (gbase > 0) {
+                    const size_t ci = (size_t)(gbase / kBlk - 1) * 32 + lane;
+                    ck1[ci] = q1;
+                    ck2[ci] = q2;
+                    cke[ci] = E;
+                }
+                const int sh = grow_shift(q1, q2);
+                if (sh) {
+                    const double sc = pow2(-sh);
+                    q1 *= sc;
+                    q2 *= sc;
+                    E += sh;
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && o + kEvB < nch) {
+                fence_proxy_async();
+                evr_issue<kW>(R, base + o + kEvB, nch - 1 - (o + kEvB), sp, nullptr, nullptr);
+            }
+        }
+        R.loads = base + nch;
+    }
+
+    // ---------------- pass 2: forward recurrence, twist, sums ----------
+    FwdState F;
+    F.pm2 = Row::p_init(pi);
+    F.pm1 = 1.0;
+    F.Ep = 0;
+    F.An = F.Aw = F.Ag = 0.0;
+    F.thr = -1.0;
+    F.Ethr = 0;
+    F.r = 0;
+    F.Epr = F.Eqr = 0;
+    F.Anr = 1.0;
+    F.Awr = F.Agr = 0.0;
+    F.sqr = F.pr = F.qr = 1.0;
+    F.Tn = F.Tw = F.Tg = 0.0;
+    F.fq = 1.0;
+    F.ps = F.qs = F.prc = F.qrc = 1.0;
+    F.Eps = F.Eqs = F.Eprc = F.Eqrc = 0;
+    {
+        const unsigned base = R.loads;
+        if (lane == 0)
+            for (int c = 0; c < nch && c < kEvB; ++c) evr_issue<kW>(R, base + c, c, sp, wp, gp);
+        __syncwarp();
+        double nq1, nq2;
+        int nE;
+        load_ck(0, nq1, nq2, nE);
+        for (int c = 0; c < nch; ++c) {
+            const unsigned k = base + c;
+            const int slot = k % kEvB;
+            mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
+            const double* sb = R.s + slot * kEvC * kW;
+            const double* wb = R.w + slot * kEvC;
+            const double* gb = kGroup ? R.g + slot * kEvC : nullptr;
+            const int valid = min(kEvC, nz - c * kEvC);
+            for (int lb = 0; lb < valid; lb += kBlk) {
+                const int gbase = c * kEvC + lb;
+                const int kb = gbase / kBlk;
+                double q1 = nq1, q2 = nq2;
+                const int Eb = nE;
+                if (kb + 1 < nblk) load_ck(kb + 1, nq1, nq2, nE);
+                const int Enew = F.Ep + Eb;
+                if (Enew != F.Ethr) {
+                    F.thr *= pow2(F.Ethr - Enew);
+                    F.Ethr = Enew;
+                }
+                F.fq = pow2(Eb - F.Eqr);
+                // q_{gbase+1 .. gbase+kBlk}, units 2^Eb
+                double qb[kBlk];
+                const int ctop = min(gbase + kBlk, nz);
+                const bool full = gbase + kBlk <= nz;
+                if (ctop == gbase + kBlk) {
+                    qb[kBlk - 1] = q1;
+#pragma unroll
+                    for (int jj = kBlk - 2; jj >= 0; --jj) {
+                        const double qi = fma(Row::t(sb, lb + jj + 1, sh), q1, -q2);
+                        qb[jj] = qi;
+                        q2 = q1;
+                        q1 = qi;
+                    }
+                } else {
+#pragma unroll
+                    for (int jj = kBlk - 1; jj >= 0; --jj) {
+                        const int idx = gbase + 1 + jj;
+                        if (idx == ctop) {
+                            qb[jj] = q1;
+                        } else if (idx < ctop) {
+                            const double qi = fma(Row::t(sb, lb + jj + 1, sh), q1, -q2);
+                            qb[jj] = qi;
+                            q2 = q1;
+                            q1 = qi;
+                        } else {
+                            qb[jj] = 0.0;
+                        }
+                    }
+                }
+                const bool special = !full || (isrc >= gbase && isrc < gbase + kBlk) ||
+                                     (ircv >= gbase && ircv < gbase + kBlk);
+                if (!special) {
+#pragma unroll
+                    for (int jj = 0; jj < kBlk; ++jj)
+                        fwd_step<Row, kGroup, false>(F, gbase + jj, nz, sb, lb + jj, wb[lb + jj],
+                                                     kGroup ? gb[lb + jj] : 0.0, qb[jj], Eb, sh, isrc, ircv);
+                } else {
+#pragma unroll
+                    for (int jj = 0; jj < kBlk; ++jj) {
+                        const int li = min(lb + jj, valid - 1);
+                        fwd_step<Row, kGroup, true>(F, gbase + jj, nz, sb, li, wb[li], kGroup ? gb[li] : 0.0,
+                                                    qb[jj], Eb, sh, isrc, ircv);
+                    }
+                }
+                const int sh = grow_shift(F.pm1, F.pm2);
+                if (sh) {
+                    const double sc = pow2(-sh), sc2 = pow2(-2 * sh);
+                    F.pm1 *= sc;
+                    F.pm2 *= sc;
+                    F.An *= sc2;
+                    F.Aw *= sc2;
+                    F.Ag *= sc2;
+                    F.Ep += sh;
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && c + kEvB < nch) {
+                fence_proxy_async();
+                evr_issue<kW>(R, base + c + kEvB, c + kEvB, sp, wp, gp);
+            }
+        }
+        R.loads = base + nch;
+    }
+    // ---------------- combine ----------------------------------------
+    const double iq2 = 1.0 / (F.qr * F.qr);
+    const double isq = 1.0 / F.sqr;
+    const double nrm = F.Anr * isq + F.Tn * iq2;
+    // the wide-angle vectors carry SLEPc's normalisation of the linearised
+    // pencil's [v; k v] (EigenEngine.cpp:368-379): sum v^2 dz = 1 / (1 + k^2)
+    const double f2 = kW == 1 ? 1.0 : 1.0 / (1.0 + (mu / pi.dz) * (mu / pi.dz));
+    const double scale = kW == 1 ? 1.0 / sqrt(nrm * pi.dz) : sqrt(f2 / (nrm * pi.dz));
+    const int r = F.r;
+    double zs = (isrc <= r) ? (F.ps / F.pr) * pow2(F.Eps - F.Epr) : (F.qs / F.qr) * pow2(F.Eqs - F.Eqr);
+    double zr = (ircv <= r) ? (F.prc / F.pr) * pow2(F.Eprc - F.Epr) : (F.qrc / F.qr) * pow2(F.Eqrc - F.Eqr);
+    if ((isrc - r) & 1) zs = -zs;
+    if ((ircv - r) & 1) zr = -zr;
+    const double absorption = kW == 1 ? (F.Awr * isq + F.Tw * iq2) / nrm : (F.Awr * isq + F.Tw * iq2) / nrm * f2;
+    const double ks = kW == 1 ? sqrt(mu / (pi.dz * pi.dz)) : mu / pi.dz;
+    const double kk = ks * ks;
+    const auto kp = csqrt_principal(kk, absorption);
+    if (active) {
+        const int o = pi.off + w.j0 + lane;
+        A.kr[o] = kp.real();
+        A.ki[o] = kp.imag();
+        A.vs[o] = zs * scale;
+        A.vr[o] = zr * scale;
+        if (kGroup) {
+            const double gsum = (F.Agr * isq + F.Tg * iq2) / nrm;
+            const double vph = pi.omega / kp.real();
+            A.vg[o] = 1.0 / (vph * gsum);
+        } else if (A.vg) {
+            A.vg[o] = 0.0;
+        }
+    }
+    // ---------------- pass 3 (optional): full eigenvector --------------
+    if (kVec) {
+        double* vout = A.vfull + A.vfull_off[w.problem];
+        const int M = pi.M;
+        const unsigned base = R.loads;
+        if (lane == 0)
+            for (int c = 0; c < nch && c < kEvB; ++c) evr_issue<kW>(R, base + c, c, sp, nullptr, nullptr);
+        __syncwarp();
+        double pa = Row::p_init(pi), pb = 1.0;
+        int Ea = 0;
+        double nq1, nq2;
+        int nE;
+        load_ck(0, nq1, nq2, nE);
+        const double ipr = 1.0 / F.pr, iqr = 1.0 / F.qr;
+        for (int c = 0; c < nch; ++c) {
+            const unsigned k = base + c;
+            const int slot = k % kEvB;
+            mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
+            const double* sb = R.s + slot * kEvC * kW;
+            const int valid = min(kEvC, nz - c * kEvC);
+            for (int lb = 0; lb < valid; lb += kBlk) {
+                const int gbase = c * kEvC + lb;
+                const int kb = gbase / kBlk;
+                double q1 = nq1, q2 = nq2;
+                const int Eb = nE;
+                if (kb + 1 < nblk) load_ck(kb + 1, nq1, nq2, nE);
+                double qb[kBlk];
+                const int ctop = min(gbase + kBlk, nz);
+#pragma unroll
+                for (int jj = kBlk - 1; jj >= 0; --jj) {
+                    const int idx = gbase + 1 + jj;
+                    if (idx == ctop) {
+                        qb[jj] = q1;
+                    } else if (idx < ctop) {
+                        const double qi = fma(Row::t(sb, lb + jj + 1, sh), q1, -q2);
+                        qb[jj] = qi;
+                        q2 = q1;
+                        q1 = qi;
+                    } else {
+                        qb[jj] = 0.0;
+                    }
+                }
+                const double fp = pow2(Ea - F.Epr) * ipr * scale;
+                const double fqq = pow2(Eb - F.Eqr) * iqr * scale;
+#pragma unroll
+                for (int jj = 0; jj < kBlk; ++jj) {
+                    const int i = gbase + jj;
+                    if (i < nz) {
+                        double zi = (i <= r) ? pb * fp : qb[jj] * fqq;
+                        if ((i - r) & 1) zi = -zi;
+                        if (active) vout[(size_t)i * M + w.j0 + lane] = zi;
+                        const double pn = fma(Row::t(sb, lb + jj, sh), pb, -pa);
+                        pa = pb;
+                        pb = pn;
+                    }
+                }
+                const int sh = grow_shift(pb, pa);
+                if (sh) {
+                    const double sc = pow2(-sh);
+                    pa *= sc;
+                    pb *= sc;
+                    Ea += sh;
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && c + kEvB < nch) {
+                fence_proxy_async();
+                evr_issue<kW>(R, base + c + kEvB, c + kEvB, sp, nullptr, nullptr);
+            }
+        }
+        R.loads = base + nch;
+    }
+}
+
 // Row: the row format (EssRows, WmodRows in device_common.cuh); mu holds the
 // shift of each mode in the row format's units (h^2 k^2, or kappa = h k)
 template <class Row, bool kGroup, bool kVec>
@@ -1399,302 +1716,12 @@ __global__ void __launch_bounds__(kEvWarps * 32, 4) k_eigvec(EigvecArgs A) {
     double* ck1 = A.ck_q1 + gw * A.ck_slot_stride;
     double* ck2 = A.ck_q2 + gw * A.ck_slot_stride;
     int* cke = A.ck_e + gw * A.ck_slot_stride;
-    int nz = 0;  // grid of the current item
-    auto load_ck = [&](int kb, double& a1, double& a2, int& ae) {
-        if (min((kb + 1) * kBlk, nz) >= nz) {
-            a1 = 1.0;
-            a2 = 0.0;
-            ae = 0;
-        } else {
-            const size_t ci = (size_t)kb * 32 + lane;
-            a1 = ck1[ci];
-            a2 = ck2[ci];
-            ae = cke[ci];
-        }
-    };
     const int n_items_all = A.n_items_dev ? *A.n_items_dev : A.n_items;
     // static round-robin over the grid's warps (see k_bisect)
     const int warps_total = gridDim.x * kEvWarps;
     for (int it = blockIdx.x * kEvWarps + wid; it < n_items_all; it += warps_total) {
-        const WorkItem w = A.items[it];
-        const ProblemInfo pi = A.pinfo[w.problem];
-        nz = pi.nz;
-        const int nch = (nz + kEvC - 1) / kEvC;
-        const int nblk = (nz + kBlk - 1) / kBlk;
-        const int isrc = pi.isrc, ircv = pi.ircv;
-        const double* sp = A.s + (size_t)pi.s_off * kW;
-        const double* wp = A.w + pi.w_off;
-        const double* gp = kGroup ? A.g + pi.s_off : nullptr;
-        const bool active = lane < w.m;
-        const double mu = active ? A.mu[pi.off + w.j0 + lane] : Row::idle_shift(pi);
-        const typename Row::Shift sh = Row::shift(mu);
-
-        // ---------------- pass 1: backward recurrence, checkpoints ----------
-        {
-            const unsigned base = R.loads;
-            if (lane == 0)
-                for (int o = 0; o < nch && o < kEvB; ++o)
-                    evr_issue<kW>(R, base + o, nch - 1 - o, sp, nullptr, nullptr);
-            __syncwarp();
-            double q1 = 1.0, q2 = 0.0;  // q_i, q_{i+1}; q_n = 1, q_{n+1} = 0
-            int E = 0;
-            for (int o = 0; o < nch; ++o) {
-                const int c = nch - 1 - o;
-                const unsigned k = base + o;
-                const int slot = k % kEvB;
-                mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
-                const double* sb = R.s + slot * kEvC * kW;
-                const int valid = min(kEvC, nz - c * kEvC);
-                for (int lb = ((valid - 1) / kBlk) * kBlk; lb >= 0; lb -= kBlk) {
-                    if (lb + kBlk <= valid) {
-#pragma unroll
-                        for (int u = kBlk - 1; u >= 0; --u) {
-                            const double qi = fma(Row::t(sb, lb + u, sh), q1, -q2);
-                            q2 = q1;
-                            q1 = qi;
-                        }
-                    } else {
-                        for (int u = valid - 1 - lb; u >= 0; --u) {
-                            const double qi = fma(Row::t(sb, lb + u, sh), q1, -q2);
-                            q2 = q1;
-                            q1 = qi;
-                        }
-                    }
-                    const int gbase = c * kEvC + lb;
-                    if (gbase > 0) {
-                        const size_t ci = (size_t)(gbase / kBlk - 1) * 32 + lane;
-                        ck1[ci] = q1;
-                        ck2[ci] = q2;
-                        cke[ci] = E;
-                    }
-                    const int sh = grow_shift(q1, q2);
-                    if (sh) {
-                        const double sc = pow2(-sh);
-                        q1 *= sc;
-                        q2 *= sc;
-                        E += sh;
-                    }
-                }
-                __syncwarp();
-                if (lane == 0 && o + kEvB < nch) {
-                    fence_proxy_async();
-                    evr_issue<kW>(R, base + o + kEvB, nch - 1 - (o + kEvB), sp, nullptr, nullptr);
-                }
-            }
-            R.loads = base + nch;
-        }
-
-        // ---------------- pass 2: forward recurrence, twist, sums ----------
-        FwdState F;
-        F.pm2 = Row::p_init(pi);
-        F.pm1 = 1.0;
-        F.Ep = 0;
-        F.An = F.Aw = F.Ag = 0.0;
-        F.thr = -1.0;
-        F.Ethr = 0;
-        F.r = 0;
-        F.Epr = F.Eqr = 0;
-        F.Anr = 1.0;
-        F.Awr = F.Agr = 0.0;
-        F.sqr = F.pr = F.qr = 1.0;
-        F.Tn = F.Tw = F.Tg = 0.0;
-        F.fq = 1.0;
-        F.ps = F.qs = F.prc = F.qrc = 1.0;
-        F.Eps = F.Eqs = F.Eprc = F.Eqrc = 0;
-        {
-            const unsigned base = R.loads;
-            if (lane == 0)
-                for (int c = 0; c < nch && c < kEvB; ++c) evr_issue<kW>(R, base + c, c, sp, wp, gp);
-            __syncwarp();
-            double nq1, nq2;
-            int nE;
-            load_ck(0, nq1, nq2, nE);
-            for (int c = 0; c < nch; ++c) {
-                const unsigned k = base + c;
-                const int slot = k % kEvB;
-                mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
-                const double* sb = R.s + slot * kEvC * kW;
-                const double* wb = R.w + slot * kEvC;
-                const double* gb = kGroup ? R.g + slot * kEvC : nullptr;
-                const int valid = min(kEvC, nz - c * kEvC);
-                for (int lb = 0; lb < valid; lb += kBlk) {
-                    const int gbase = c * kEvC + lb;
-                    const int kb = gbase / kBlk;
-                    double q1 = nq1, q2 = nq2;
-                    const int Eb = nE;
-                    if (kb + 1 < nblk) load_ck(kb + 1, nq1, nq2, nE);
-                    const int Enew = F.Ep + Eb;
-                    if (Enew != F.Ethr) {
-                        F.thr *= pow2(F.Ethr - Enew);
-                        F.Ethr = Enew;
-                    }
-                    F.fq = pow2(Eb - F.Eqr);
-                    // q_{gbase+1 .. gbase+kBlk}, units 2^Eb
-                    double qb[kBlk];
-                    const int ctop = min(gbase + kBlk, nz);
-                    const bool full = gbase + kBlk <= nz;
-                    if (ctop == gbase + kBlk) {
-                        qb[kBlk - 1] = q1;
-#pragma unroll
-                        for (int jj = kBlk - 2; jj >= 0; --jj) {
-                            const double qi = fma(Row::t(sb, lb + jj + 1, sh), q1, -q2);
-                            qb[jj] = qi;
-                            q2 = q1;
-                            q1 = qi;
-                        }
-                    } else {
-#pragma unroll
-                        for (int jj = kBlk - 1; jj >= 0; --jj) {
-                            const int idx = gbase + 1 + jj;
-                            if (idx == ctop) {
-                                qb[jj] = q1;
-                            } else if (idx < ctop) {
-                                const double qi = fma(Row::t(sb, lb + jj + 1, sh), q1, -q2);
-                                qb[jj] = qi;
-                                q2 = q1;
-                                q1 = qi;
-                            } else {
-                                qb[jj] = 0.0;
-                            }
-                        }
-                    }
-                    const bool special = !full || (isrc >= gbase && isrc < gbase + kBlk) ||
-                                         (ircv >= gbase && ircv < gbase + kBlk);
-                    if (!special) {
-#pragma unroll
-                        for (int jj = 0; jj < kBlk; ++jj)
-                            fwd_step<Row, kGroup, false>(F, gbase + jj, nz, sb, lb + jj, wb[lb + jj],
-                                                         kGroup ? gb[lb + jj] : 0.0, qb[jj], Eb, sh, isrc, ircv);
-                    } else {
-#pragma unroll
-                        for (int jj = 0; jj < kBlk; ++jj) {
-                            const int li = min(lb + jj, valid - 1);
-                            fwd_step<Row, kGroup, true>(F, gbase + jj, nz, sb, li, wb[li], kGroup ? gb[li] : 0.0,
-                                                        qb[jj], Eb, sh, isrc, ircv);
-                        }
-                    }
-                    const int sh = grow_shift(F.pm1, F.pm2);
-                    if (sh) {
-                        const double sc = pow2(-sh), sc2 = pow2(-2 * sh);
-                        F.pm1 *= sc;
-                        F.pm2 *= sc;
-                        F.An *= sc2;
-                        F.Aw *= sc2;
-                        F.Ag *= sc2;
-                        F.Ep += sh;
-                    }
-                }
-                __syncwarp();
-                if (lane == 0 && c + kEvB < nch) {
-                    fence_proxy_async();
-                    evr_issue<kW>(R, base + c + kEvB, c + kEvB, sp, wp, gp);
-                }
-            }
-            R.loads = base + nch;
-        }
-        // ---------------- combine ----------------------------------------
-        const double iq2 = 1.0 / (F.qr * F.qr);
-        const double isq = 1.0 / F.sqr;
-        const double nrm = F.Anr * isq + F.Tn * iq2;
-        // the wide-angle vectors carry SLEPc's normalisation of the linearised
-        // pencil's [v; k v] (EigenEngine.cpp:368-379): sum v^2 dz = 1 / (1 + k^2)
-        const double f2 = kW == 1 ? 1.0 : 1.0 / (1.0 + (mu / pi.dz) * (mu / pi.dz));
-        const double scale = kW == 1 ? 1.0 / sqrt(nrm * pi.dz) : sqrt(f2 / (nrm * pi.dz));
-        const int r = F.r;
-        double zs = (isrc <= r) ? (F.ps / F.pr) * pow2(F.Eps - F.Epr) : (F.qs / F.qr) * pow2(F.Eqs - F.Eqr);
-        double zr = (ircv <= r) ? (F.prc / F.pr) * pow2(F.Eprc - F.Epr) : (F.qrc / F.qr) * pow2(F.Eqrc - F.Eqr);
-        if ((isrc - r) & 1) zs = -zs;
-        if ((ircv - r) & 1) zr = -zr;
-        const double absorption = kW == 1 ? (F.Awr * isq + F.Tw * iq2) / nrm : (F.Awr * isq + F.Tw * iq2) / nrm * f2;
-        const double ks = kW == 1 ? sqrt(mu / (pi.dz * pi.dz)) : mu / pi.dz;
-        const double kk = ks * ks;
-        const auto kp = csqrt_principal(kk, absorption);
-        if (active) {
-            const int o = pi.off + w.j0 + lane;
-            A.kr[o] = kp.real();
-            A.ki[o] = kp.imag();
-            A.vs[o] = zs * scale;
-            A.vr[o] = zr * scale;
-            if (kGroup) {
-                const double gsum = (F.Agr * isq + F.Tg * iq2) / nrm;
-                const double vph = pi.omega / kp.real();
-                A.vg[o] = 1.0 / (vph * gsum);
-            } else if (A.vg) {
-                A.vg[o] = 0.0;
-            }
-        }
-        // ---------------- pass 3 (optional): full eigenvector --------------
-        if (kVec) {
-            double* vout = A.vfull + A.vfull_off[w.problem];
-            const int M = pi.M;
-            const unsigned base = R.loads;
-            if (lane == 0)
-                for (int c = 0; c < nch && c < kEvB; ++c) evr_issue<kW>(R, base + c, c, sp, nullptr, nullptr);
-            __syncwarp();
-            double pa = Row::p_init(pi), pb = 1.0;
-            int Ea = 0;
-            double nq1, nq2;
-            int nE;
-            load_ck(0, nq1, nq2, nE);
-            const double ipr = 1.0 / F.pr, iqr = 1.0 / F.qr;
-            for (int c = 0; c < nch; ++c) {
-                const unsigned k = base + c;
-                const int slot = k % kEvB;
-                mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
-                const double* sb = R.s + slot * kEvC * kW;
-                const int valid = min(kEvC, nz - c * kEvC);
-                for (int lb = 0; lb < valid; lb += kBlk) {
-                    const int gbase = c * kEvC + lb;
-                    const int kb = gbase / kBlk;
-                    double q1 = nq1, q2 = nq2;
-                    const int Eb = nE;
-                    if (kb + 1 < nblk) load_ck(kb + 1, nq1, nq2, nE);
-                    double qb[kBlk];
-                    const int ctop = min(gbase + kBlk, nz);
-#pragma unroll
-                    for (int jj = kBlk - 1; jj >= 0; --jj) {
-                        const int idx = gbase + 1 + jj;
-                        if (idx == ctop) {
-                            qb[jj] = q1;
-                        } else if (idx < ctop) {
-                            const double qi = fma(Row::t(sb, lb + jj + 1, sh), q1, -q2);
-                            qb[jj] = qi;
-                            q2 = q1;
-                            q1 = qi;
-                        } else {
-                            qb[jj] = 0.0;
-                        }
-                    }
-                    const double fp = pow2(Ea - F.Epr) * ipr * scale;
-                    const double fqq = pow2(Eb - F.Eqr) * iqr * scale;
-#pragma unroll
-                    for (int jj = 0; jj < kBlk; ++jj) {
-                        const int i = gbase + jj;
-                        if (i < nz) {
-                            double zi = (i <= r) ? pb * fp : qb[jj] * fqq;
-                            if ((i - r) & 1) zi = -zi;
-                            if (active) vout[(size_t)i * M + w.j0 + lane] = zi;
-                            const double pn = fma(Row::t(sb, lb + jj, sh), pb, -pa);
-                            pa = pb;
-                            pb = pn;
-                        }
-                    }
-                    const int sh = grow_shift(pb, pa);
-                    if (sh) {
-                        const double sc = pow2(-sh);
-                        pa *= sc;
-                        pb *= sc;
-                        Ea += sh;
-                    }
-                }
-                __syncwarp();
-                if (lane == 0 && c + kEvB < nch) {
-                    fence_proxy_async();
-                    evr_issue<kW>(R, base + c + kEvB, c + kEvB, sp, nullptr, nullptr);
-                }
-            }
-            R.loads = base + nch;
-        }
+        if (A.ev_done && A.ev_done[it]) continue;  // done in the fused launch
+        eigvec_item<Row, kGroup, kVec>(A, A.items[it], R, ck1, ck2, cke);
     }
 }
 
@@ -1750,6 +1777,123 @@ int eigvec_wmod_ctas_per_sm(const EigvecArgs& a) { return eigvec_fit<WmodRows>(a
 int launch_eigvec_wmod(cudaStream_t st, int grid, const EigvecArgs& a) {
     if (a.g) return -1;
     return eigvec_launch<WmodRows>(st, grid, a);
+}
+
+// ===========================================================================
+// K3+K4 fused: bisection and eigenvectors in one launch.  Every warp first
+// runs its bisection items (the static mapping of k_bisect); the warp that
+// finishes a problem's last bisection item appends the problem's eigenvector
+// items to a ready queue.  Then every warp takes queue slots in order and
+// runs the eigenvector item it finds there, so eigenvectors of finished
+// problems overlap the bisection of the others.  Producers never wait on
+// consumers; a consumer waits for its slot to be filled (bounded: it gives
+// up after kFuseWaitNs or on a device error), and every item it did not
+// finish is left to the k_eigvec launch that follows (items marked done are
+// skipped there), so no result depends on all CTAs being resident.
+// ===========================================================================
+constexpr unsigned long long kFuseWaitNs = 1000000000ull;  // 1 s
+
+template <class Row>
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 4) k_bisect_eigvec(FusedArgs F) {
+    static_assert(kWarpsPerCta == kEvWarps, "one warp layout for both phases");
+    constexpr int kW = Row::kW;
+    constexpr int kBisD = kWBuf * kWChunk, kEvD = kEvB * (kW + 1) * kEvC;
+    constexpr int kWarpD = kBisD > kEvD ? kBisD : kEvD;  // doubles of one warp's ring buffer
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double* wbuf = reinterpret_cast<double*>(smem_raw) + (size_t)wid * kWarpD;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarpsPerCta * kWarpD * 8) + wid * (kWBuf + kEvB);
+    WarpRing r;
+    r.buf = wbuf;
+    r.bars = bars;
+    r.loads = 0;
+    EvRing R;
+    R.s = wbuf;
+    R.w = wbuf + kEvB * kEvC * kW;
+    R.g = nullptr;
+    R.bars = bars + kWBuf;
+    R.loads = 0;
+    if (lane == 0) {
+        for (int k = 0; k < kWBuf + kEvB; ++k) mbar_init(&bars[k], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    const int P = F.P;
+    // ---- bisection items; the last item of a problem publishes its eigenvector items ----
+    const int n_bis = *F.n_bis_dev;
+    const int warps_total = gridDim.x * kWarpsPerCta;
+    for (int it = blockIdx.x * kWarpsPerCta + wid; it < n_bis; it += warps_total) {
+        const WorkItem w = F.bis[it];
+        bisect_item<Row>(F.pinfo, F.s, F.counts, w, F.tol, F.mu, F.err, nullptr, r);
+        __threadfence();  // this lane's eigenvalues visible before the count below
+        __syncwarp();
+        if (lane == 0 && atomicSub(&F.pstat[w.problem], 1) == 1) {
+            const int e0 = F.pstat[P + w.problem], ne = F.pstat[2 * P + w.problem];
+            if (ne > 0) {
+                const int t = atomicAdd(F.q_tail, ne);
+                for (int i = 0; i < ne; ++i) atomicExch(&F.queue[t + i], e0 + i + 1);
+            }
+        }
+        __syncwarp();
+    }
+    // ---- eigenvector items from the ready queue ----
+    const int n_ev = *F.ea.n_items_dev;
+    const size_t gw = (size_t)blockIdx.x * kEvWarps + wid;
+    double* ck1 = F.ea.ck_q1 + gw * F.ea.ck_slot_stride;
+    double* ck2 = F.ea.ck_q2 + gw * F.ea.ck_slot_stride;
+    int* cke = F.ea.ck_e + gw * F.ea.ck_slot_stride;
+    if (lane == 0) fence_proxy_async();  // the shared buffer now feeds the other ring
+    __syncwarp();
+    for (;;) {
+        int h = 0;
+        if (lane == 0) h = atomicAdd(F.q_head, 1);
+        h = __shfl_sync(0xffffffffu, h, 0);
+        if (h >= n_ev) break;
+        int v = 0;
+        if (lane == 0) {
+            const uint64_t t0 = global_ns();
+            for (;;) {
+                v = *((volatile int*)(F.queue + h));
+                if (v != 0) break;
+                if ((*((volatile unsigned*)F.err) & (kErrTimeout | kErrTooMany)) != 0u ||
+                    global_ns() - t0 > kFuseWaitNs)
+                    break;
+                __nanosleep(2000);
+            }
+        }
+        v = __shfl_sync(0xffffffffu, v, 0);
+        if (v == 0) break;  // gave up: the following k_eigvec launch runs this item
+        __threadfence();   // the item's eigenvalues, written by another warp, before reading them
+        const int it = v - 1;
+        eigvec_item<Row, false, false>(F.ea, F.ea.items[it], R, ck1, ck2, cke);
+        __syncwarp();
+        if (lane == 0) F.ev_done[it] = 1;
+    }
+}
+
+template <class Row>
+static size_t fused_smem() {
+    constexpr int kBisD = kWBuf * kWChunk, kEvD = kEvB * (Row::kW + 1) * kEvC;
+    constexpr int kWarpD = kBisD > kEvD ? kBisD : kEvD;
+    return (size_t)kWarpsPerCta * (kWarpD * 8 + (kWBuf + kEvB) * 8);
+}
+
+int fused_ctas_per_sm() {
+    int n = 1;
+    const size_t sm = fused_smem<EssRows>();
+    cudaFuncSetAttribute(k_bisect_eigvec<EssRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bisect_eigvec<EssRows>, kWarpsPerCta * 32, sm) !=
+        cudaSuccess)
+        n = 1;
+    return n < 1 ? 1 : n;
+}
+
+int launch_bisect_eigvec(cudaStream_t st, int grid, const FusedArgs& a) {
+    if (a.ea.g || a.ea.vfull || !a.ev_done || !a.pstat || !a.queue) return -1;
+    const size_t sm = fused_smem<EssRows>();
+    cudaFuncSetAttribute(k_bisect_eigvec<EssRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_bisect_eigvec<EssRows><<<grid, kWarpsPerCta * 32, sm, st>>>(a);
+    return 1;
 }
 
 // ===========================================================================

@@ -98,6 +98,7 @@ struct EigvecArgs {
     const WorkItem* items;
     int n_items;
     const int* n_items_dev;  // when set, the item count is read here (built on the device)
+    const int* ev_done;      // when set, items with ev_done[it] != 0 are skipped (done in the fused launch)
     int* counter;
     const double* mu;
     double* kr;
@@ -114,13 +115,41 @@ struct EigvecArgs {
     unsigned* err;
 };
 int launch_eigvec(cudaStream_t st, int grid, const EigvecArgs& a);
+// Bisection and eigenvectors in one launch (ESS rows, no group speeds, no
+// full vectors): bisection items as launch_bisect, then eigenvector items of
+// finished problems from a ready queue.  pstat[3 P] from k_make_items;
+// queue[ev_cap], q_head, q_tail and ev_done[ev_cap] zeroed before the launch.
+// A k_eigvec launch with ea.ev_done = ev_done must follow: it runs the items
+// this launch did not finish.
+struct FusedArgs {
+    int P;
+    const ProblemInfo* pinfo;
+    const double* s;
+    const int* counts;
+    const WorkItem* bis;
+    const int* n_bis_dev;
+    double tol;
+    double* mu;
+    unsigned* err;
+    int* pstat;
+    int* queue;
+    int* q_head;
+    int* q_tail;
+    int* ev_done;
+    EigvecArgs ea;
+};
+int launch_bisect_eigvec(cudaStream_t st, int grid, const FusedArgs& a);
+int fused_ctas_per_sm();
 // Work items built on the device from the Sturm scan: per problem c_lo, c_hi,
 // M and CSR offset in pinfo; bisection items (<= bis_item eigenvalues, sizes
 // balanced inside a problem) and eigenvector items (kEvItem) appended;
 // tot = {n_bisect_items, n_eigvec_items, total modes}.  Sets kErrTooMany if a
 // problem exceeds max_modes (its M is then clamped) or a capacity is exceeded.
+// pstat (optional, 3 P ints): per problem the number of bisection items, the
+// first eigenvector item and the number of eigenvector items
 int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes, int bis_item,
-                      WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err);
+                      WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err,
+                      int* pstat = nullptr);
 // resident eigenvector CTAs per SM for the variant selected by a
 int eigvec_ctas_per_sm(const EigvecArgs& a);
 // modal sums

@@ -115,6 +115,7 @@ struct ncpa_ctx {
     DevBuf bb_out;                 // waveforms kept in HBM (NULL host buffer)
     DevBuf ms_img, ms_q, ms_tab, ms_raw, ms_vz, ms_idx, ms_re, ms_im;  // modal-sum scratch (grow-only)
     int item_override = 0;         // eigenvalues per bisection item (0: chosen per solve); NCPA_BISECT_ITEM
+    bool fuse_solve = true;        // fused bisection + eigenvector launch; NCPA_FUSE_SOLVE=0 turns it off
     double* h_pin = nullptr;       // small pinned host buffer for scalars read back per solve
     int* h_tot = nullptr;          // pinned: item and mode totals of a device-built solve
     size_t h_pin_n = 0;
@@ -447,6 +448,7 @@ struct Tuning {
 // captured graph must keep its addresses for good).
 struct SolveBufs {
     DevBuf counts, bis, ev, tot, mu, counter;
+    DevBuf pstat, fq;  // fused launch: per-problem readiness; ready queue, done flags, queue counters
     DevBuf ck1, ck2, cke;
     bool own_ck = false;
     int bis_cap = 0, ev_cap = 0;
@@ -495,6 +497,8 @@ void prepare_solve(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, int
     b.bis.alloc((size_t)b.bis_cap * sizeof(WorkItem), st);
     b.ev.alloc((size_t)b.ev_cap * sizeof(WorkItem), st);
     b.tot.alloc(4 * sizeof(int), st);
+    b.pstat.alloc((size_t)3 * P * sizeof(int), st);
+    b.fq.alloc(((size_t)2 * b.ev_cap + 2) * sizeof(int), st);
     b.mu.alloc(mcap * 8, st);
     b.counter.alloc(2 * sizeof(int), st);
     M->d_kr.alloc(mcap * 8, st);
@@ -534,28 +538,62 @@ void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_
     // ---- K3a scan ----
     check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s, b.counts.as<int>(), err));
     tm.mark("scan");
+    // fused bisection + eigenvectors (one launch, eigenvectors of finished
+    // problems overlapping the others' bisection), unless per-phase timing or
+    // step counts ask for the kernels alone, or group speeds are wanted
+    const bool fuse = ctx->fuse_solve && !ctx->timing && !ctx->stats && !count_steps && !prm->want_group_speed;
     check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, b.counts.as<int>(), M->prm.max_modes, t.bis_item,
                                               b.bis.as<WorkItem>(), b.bis_cap, b.ev.as<WorkItem>(), b.ev_cap,
-                                              b.tot.as<int>(), err));
+                                              b.tot.as<int>(), err, fuse ? b.pstat.as<int>() : nullptr));
     CK(cudaMemsetAsync(b.counter.p, 0, 2 * sizeof(int), st));
     tm.mark("host-items");
-    // ---- K3 bisection ----
     const int fit_b = ncpa::bisect_ctas_per_sm();
     const int grid_b = ctx->num_sms * (t.bis_ctas > 0 ? std::min(t.bis_ctas, fit_b) : fit_b);
-    check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s, b.counts.as<int>(), b.bis.as<WorkItem>(), 0,
-                                          b.counter.as<int>(), kBisectTol, b.mu.as<double>(), err,
-                                          count_steps ? ctx->d_stats.as<unsigned long long>() : nullptr,
-                                          b.tot.as<int>()));
-    tm.mark("bisect");
-    // ---- K4 eigenvectors ----
     ncpa::EigvecArgs ea = eigvec_args(ctx, M, prm, s, w, gs, b);
     const int grid_e = eigvec_grid(ctx, ea, b.ev_cap, t.ev_ctas);
     ea.ck_q1 = (b.own_ck ? b.ck1 : ctx->ck1).as<double>();
     ea.ck_q2 = (b.own_ck ? b.ck2 : ctx->ck2).as<double>();
     ea.ck_e = (b.own_ck ? b.cke : ctx->cke).as<int>();
     ea.ck_slot_stride = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
-    check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
-    tm.mark("eigvec");
+    if (fuse) {
+        int* fq = b.fq.as<int>();
+        CK(cudaMemsetAsync(fq, 0, ((size_t)2 * b.ev_cap + 2) * sizeof(int), st));
+        ncpa::FusedArgs fa{};
+        fa.P = P;
+        fa.pinfo = d_pinfo;
+        fa.s = s;
+        fa.counts = b.counts.as<int>();
+        fa.bis = b.bis.as<WorkItem>();
+        fa.n_bis_dev = b.tot.as<int>();
+        fa.tol = kBisectTol;
+        fa.mu = b.mu.as<double>();
+        fa.err = err;
+        fa.pstat = b.pstat.as<int>();
+        fa.queue = fq;
+        fa.ev_done = fq + b.ev_cap;
+        fa.q_head = fq + 2 * b.ev_cap;
+        fa.q_tail = fq + 2 * b.ev_cap + 1;
+        fa.ea = ea;
+        // no more warps than the checkpoint scratch has slots (sized for grid_e)
+        const int fit_f = ncpa::fused_ctas_per_sm();
+        const int grid_f =
+            std::min(grid_e, ctx->num_sms * (t.bis_ctas > 0 ? std::min(t.bis_ctas, fit_f) : fit_f));
+        check_launch(ctx, ncpa::launch_bisect_eigvec(st, grid_f, fa));
+        tm.mark("bisect");
+        ea.ev_done = fa.ev_done;  // the items the fused launch did not finish
+        check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
+        tm.mark("eigvec");
+    } else {
+        // ---- K3 bisection ----
+        check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s, b.counts.as<int>(), b.bis.as<WorkItem>(), 0,
+                                              b.counter.as<int>(), kBisectTol, b.mu.as<double>(), err,
+                                              count_steps ? ctx->d_stats.as<unsigned long long>() : nullptr,
+                                              b.tot.as<int>()));
+        tm.mark("bisect");
+        // ---- K4 eigenvectors ----
+        check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
+        tm.mark("eigvec");
+    }
     CK(cudaMemcpyAsync(tot_dst, b.tot.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(info_dst, d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(err_dst, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
@@ -1260,6 +1298,7 @@ ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
         CK(cudaHostAlloc((void**)&ctx->h_tot, 64, cudaHostAllocDefault));
         const char* tv = std::getenv("NCPA_TIMING");
         ctx->timing = tv && tv[0] == '1';
+        if (const char* fv = std::getenv("NCPA_FUSE_SOLVE")) ctx->fuse_solve = fv[0] != '0';
         // tuning override of the eigenvalues per bisection item (1..32)
         if (const char* iv = std::getenv("NCPA_BISECT_ITEM")) {
             const int v = std::atoi(iv);
