@@ -354,6 +354,9 @@ def run_ours(args):
                        "profile": "analytic 0-150 km (T piecewise linear, 60+20 m/s jets)", "nz_grid": NZ,
                        "n_freq": NFREQ, "df_hz": 0.5 / NFREQ, "azimuth_deg": az[0], "tl_ranges": N_TL,
                        "synthesis_ranges_km": "200-300/10", "nfft": nfft, "l2": "flushed (256 MiB write) between steps",
+                       "eigen_solve": "fused bisection + eigenvector launch in the timed steps; phases_ms and the "
+                                      "roofline time k_bisect and k_eigvec alone (per-phase timing runs them "
+                                      "separately)",
                        "parallelism": "replicas (one 256-frequency job per GPU)"},
             "e2e": {"value": round(e2e_value, 2), "unit": METRIC, "h2d_bytes_per_step": int(h2d[0]),
                     "d2h_bytes_per_step": int(d2h[0])},
