@@ -1878,22 +1878,31 @@ static size_t fused_smem() {
     return (size_t)kWarpsPerCta * (kWarpD * 8 + (kWBuf + kEvB) * 8);
 }
 
-int fused_ctas_per_sm() {
+template <class Row>
+static int fused_fit() {
     int n = 1;
-    const size_t sm = fused_smem<EssRows>();
-    cudaFuncSetAttribute(k_bisect_eigvec<EssRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bisect_eigvec<EssRows>, kWarpsPerCta * 32, sm) !=
+    const size_t sm = fused_smem<Row>();
+    cudaFuncSetAttribute(k_bisect_eigvec<Row>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bisect_eigvec<Row>, kWarpsPerCta * 32, sm) !=
         cudaSuccess)
         n = 1;
     return n < 1 ? 1 : n;
 }
 
-int launch_bisect_eigvec(cudaStream_t st, int grid, const FusedArgs& a) {
+template <class Row>
+static int fused_launch(cudaStream_t st, int grid, const FusedArgs& a) {
     if (a.ea.g || a.ea.vfull || !a.ev_done || !a.pstat || !a.queue) return -1;
-    const size_t sm = fused_smem<EssRows>();
-    cudaFuncSetAttribute(k_bisect_eigvec<EssRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_bisect_eigvec<EssRows><<<grid, kWarpsPerCta * 32, sm, st>>>(a);
+    const size_t sm = fused_smem<Row>();
+    cudaFuncSetAttribute(k_bisect_eigvec<Row>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_bisect_eigvec<Row><<<grid, kWarpsPerCta * 32, sm, st>>>(a);
     return 1;
+}
+
+int fused_ctas_per_sm() { return fused_fit<EssRows>(); }
+int launch_bisect_eigvec(cudaStream_t st, int grid, const FusedArgs& a) { return fused_launch<EssRows>(st, grid, a); }
+int fused_wmod_ctas_per_sm() { return fused_fit<WmodRows>(); }
+int launch_bisect_eigvec_wmod(cudaStream_t st, int grid, const FusedArgs& a) {
+    return fused_launch<WmodRows>(st, grid, a);
 }
 
 // ===========================================================================

@@ -140,6 +140,9 @@ struct FusedArgs {
 };
 int launch_bisect_eigvec(cudaStream_t st, int grid, const FusedArgs& a);
 int fused_ctas_per_sm();
+// the same on the wide-angle rows (mu = kappa; follow with launch_eigvec_wmod)
+int launch_bisect_eigvec_wmod(cudaStream_t st, int grid, const FusedArgs& a);
+int fused_wmod_ctas_per_sm();
 // Work items built on the device from the Sturm scan: per problem c_lo, c_hi,
 // M and CSR offset in pinfo; bisection items (<= bis_item eigenvalues, sizes
 // balanced inside a problem) and eigenvector items (kEvItem) appended;

@@ -967,9 +967,14 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
     bis.alloc((size_t)bis_cap * sizeof(WorkItem), st);
     ev.alloc((size_t)ev_cap * sizeof(WorkItem), st);
     tot.alloc(4 * sizeof(int), st);
+    // fused bisection + eigenvector launch, as on the ESS path (full vectors
+    // excepted; kernels alone under per-phase timing)
+    const bool fuse = ctx->fuse_solve && !ctx->timing && !ctx->stats && !prm->want_vectors;
+    DevBuf pstat, fq;
+    if (fuse) pstat.alloc((size_t)3 * P * sizeof(int), st);
     check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, counts.as<int>(), cap_modes, ncpa::kWItem,
                                               bis.as<WorkItem>(), bis_cap, ev.as<WorkItem>(), ev_cap,
-                                              tot.as<int>(), err));
+                                              tot.as<int>(), err, fuse ? pstat.as<int>() : nullptr));
     // mode counts to the host (sizes of the outputs and of the vectors)
     int* h_tot = ctx->h_tot;
     unsigned h_err = 0;
@@ -999,47 +1004,74 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
         M->d_vfull.alloc((size_t)std::max(1LL, acc) * 8, st);
         upload(M->d_vfull_off, M->vfull_off, st);
     }
-    if (n_bis > 0) {
-        const int grid_b = ctx->num_sms * ncpa::bisect_wmod_ctas_per_sm();
-        check_launch(ctx, ncpa::launch_bisect_wmod(st, grid_b, d_pinfo, rows.as<double>(), counts.as<int>(),
-                                                   bis.as<WorkItem>(), kWmodTol, mu.as<double>(), err,
-                                                   ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr,
-                                                   tot.as<int>()));
+    ncpa::EigvecArgs ea{};
+    ea.pinfo = d_pinfo;
+    ea.s = rows.as<double>();
+    ea.w = w.as<double>();
+    ea.g = nullptr;
+    ea.items = ev.as<WorkItem>();
+    ea.n_items = 0;
+    ea.n_items_dev = tot.as<int>() + 1;
+    ea.mu = mu.as<double>();
+    ea.kr = M->d_kr.as<double>();
+    ea.ki = M->d_ki.as<double>();
+    ea.vs = M->d_vs.as<double>();
+    ea.vr = M->d_vr.as<double>();
+    ea.vg = M->d_vg.as<double>();
+    ea.vfull = prm->want_vectors ? M->d_vfull.as<double>() : nullptr;
+    ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
+    ea.err = err;
+    const int fit = ncpa::eigvec_wmod_ctas_per_sm(ea);
+    const int grid_e = std::max(1, std::min((n_ev + ncpa::kEvWarpsPerCta - 1) / ncpa::kEvWarpsPerCta,
+                                            ctx->num_sms * fit));
+    const bool fused = fuse && n_ev > 0;
+    // the fused launch runs on every SM (idle warps take eigenvector items from
+    // the start), so the checkpoint scratch has a slot for each of its warps
+    const int grid_f = fused ? ctx->num_sms * ncpa::fused_wmod_ctas_per_sm() : 0;
+    const long long slot = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
+    const size_t need = (size_t)std::max(grid_e, grid_f) * ncpa::kEvWarpsPerCta * slot;
+    if (n_ev > 0 && ctx->ck1.bytes < need * 8) {
+        ctx->ck1.alloc(need * 8, st);
+        ctx->ck2.alloc(need * 8, st);
+        ctx->cke.alloc(need * 4, st);
     }
-    tm.mark("bisect");
-    if (n_ev > 0) {
-        ncpa::EigvecArgs ea{};
-        ea.pinfo = d_pinfo;
-        ea.s = rows.as<double>();
-        ea.w = w.as<double>();
-        ea.g = nullptr;
-        ea.items = ev.as<WorkItem>();
-        ea.n_items = 0;
-        ea.n_items_dev = tot.as<int>() + 1;
-        ea.mu = mu.as<double>();
-        ea.kr = M->d_kr.as<double>();
-        ea.ki = M->d_ki.as<double>();
-        ea.vs = M->d_vs.as<double>();
-        ea.vr = M->d_vr.as<double>();
-        ea.vg = M->d_vg.as<double>();
-        ea.vfull = prm->want_vectors ? M->d_vfull.as<double>() : nullptr;
-        ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
-        ea.err = err;
-        const int fit = ncpa::eigvec_wmod_ctas_per_sm(ea);
-        const int grid_e = std::max(1, std::min((n_ev + ncpa::kEvWarpsPerCta - 1) / ncpa::kEvWarpsPerCta,
-                                                ctx->num_sms * fit));
-        const long long slot = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
-        const size_t need = (size_t)grid_e * ncpa::kEvWarpsPerCta * slot;
-        if (ctx->ck1.bytes < need * 8) {
-            ctx->ck1.alloc(need * 8, st);
-            ctx->ck2.alloc(need * 8, st);
-            ctx->cke.alloc(need * 4, st);
-        }
-        ea.ck_q1 = ctx->ck1.as<double>();
-        ea.ck_q2 = ctx->ck2.as<double>();
-        ea.ck_e = ctx->cke.as<int>();
-        ea.ck_slot_stride = slot;
+    ea.ck_q1 = ctx->ck1.as<double>();
+    ea.ck_q2 = ctx->ck2.as<double>();
+    ea.ck_e = ctx->cke.as<int>();
+    ea.ck_slot_stride = slot;
+    if (fused) {
+        fq.alloc(((size_t)2 * ev_cap + 2) * sizeof(int), st);
+        CK(cudaMemsetAsync(fq.p, 0, ((size_t)2 * ev_cap + 2) * sizeof(int), st));
+        ncpa::FusedArgs fa{};
+        fa.P = P;
+        fa.pinfo = d_pinfo;
+        fa.s = rows.as<double>();
+        fa.counts = counts.as<int>();
+        fa.bis = bis.as<WorkItem>();
+        fa.n_bis_dev = tot.as<int>();
+        fa.tol = kWmodTol;
+        fa.mu = mu.as<double>();
+        fa.err = err;
+        fa.pstat = pstat.as<int>();
+        fa.queue = fq.as<int>();
+        fa.ev_done = fq.as<int>() + ev_cap;
+        fa.q_head = fq.as<int>() + 2 * ev_cap;
+        fa.q_tail = fq.as<int>() + 2 * ev_cap + 1;
+        fa.ea = ea;
+        check_launch(ctx, ncpa::launch_bisect_eigvec_wmod(st, grid_f, fa));
+        tm.mark("bisect");
+        ea.ev_done = fa.ev_done;  // the items the fused launch did not finish
         check_launch(ctx, ncpa::launch_eigvec_wmod(st, grid_e, ea));
+    } else {
+        if (n_bis > 0) {
+            const int grid_b = ctx->num_sms * ncpa::bisect_wmod_ctas_per_sm();
+            check_launch(ctx, ncpa::launch_bisect_wmod(st, grid_b, d_pinfo, rows.as<double>(), counts.as<int>(),
+                                                       bis.as<WorkItem>(), kWmodTol, mu.as<double>(), err,
+                                                       ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr,
+                                                       tot.as<int>()));
+        }
+        tm.mark("bisect");
+        if (n_ev > 0) check_launch(ctx, ncpa::launch_eigvec_wmod(st, grid_e, ea));
     }
     tm.mark("eigvec");
     M->host_valid = false;
