@@ -1787,12 +1787,10 @@ int launch_eigvec_wmod(cudaStream_t st, int grid, const EigvecArgs& a) {
 // runs the eigenvector item it finds there, so eigenvectors of finished
 // problems overlap the bisection of the others.  Producers never wait on
 // consumers; a consumer waits for its slot to be filled (bounded: it gives
-// up after kFuseWaitNs or on a device error), and every item it did not
+// up after F.wait_ns or on a device error), and every item it did not
 // finish is left to the k_eigvec launch that follows (items marked done are
 // skipped there), so no result depends on all CTAs being resident.
 // ===========================================================================
-constexpr unsigned long long kFuseWaitNs = 1000000000ull;  // 1 s
-
 template <class Row>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 4) k_bisect_eigvec(FusedArgs F) {
     static_assert(kWarpsPerCta == kEvWarps, "one warp layout for both phases");
@@ -1856,7 +1854,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4) k_bisect_eigvec(FusedArg
                 v = *((volatile int*)(F.queue + h));
                 if (v != 0) break;
                 if ((*((volatile unsigned*)F.err) & (kErrTimeout | kErrTooMany)) != 0u ||
-                    global_ns() - t0 > kFuseWaitNs)
+                    global_ns() - t0 > F.wait_ns)
                     break;
                 __nanosleep(2000);
             }

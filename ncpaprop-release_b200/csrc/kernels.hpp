@@ -136,6 +136,7 @@ struct FusedArgs {
     int* q_head;
     int* q_tail;
     int* ev_done;
+    unsigned long long wait_ns;  // a consumer gives up on an empty slot after this long
     EigvecArgs ea;
 };
 int launch_bisect_eigvec(cudaStream_t st, int grid, const FusedArgs& a);

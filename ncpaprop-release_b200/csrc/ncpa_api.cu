@@ -116,6 +116,9 @@ struct ncpa_ctx {
     DevBuf ms_img, ms_q, ms_tab, ms_raw, ms_vz, ms_idx, ms_re, ms_im;  // modal-sum scratch (grow-only)
     int item_override = 0;         // eigenvalues per bisection item (0: chosen per solve); NCPA_BISECT_ITEM
     bool fuse_solve = true;        // fused bisection + eigenvector launch; NCPA_FUSE_SOLVE=0 turns it off
+    // how long a consumer of the fused launch waits for an empty queue slot
+    // before leaving the item to the following launch; NCPA_FUSE_WAIT_NS
+    unsigned long long fuse_wait_ns = 1000000000ull;
     double* h_pin = nullptr;       // small pinned host buffer for scalars read back per solve
     int* h_tot = nullptr;          // pinned: item and mode totals of a device-built solve
     size_t h_pin_n = 0;
@@ -571,6 +574,7 @@ void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_
         fa.pstat = b.pstat.as<int>();
         fa.queue = fq;
         fa.ev_done = fq + b.ev_cap;
+        fa.wait_ns = ctx->fuse_wait_ns;
         fa.q_head = fq + 2 * b.ev_cap;
         fa.q_tail = fq + 2 * b.ev_cap + 1;
         fa.ea = ea;
@@ -1055,6 +1059,7 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
         fa.pstat = pstat.as<int>();
         fa.queue = fq.as<int>();
         fa.ev_done = fq.as<int>() + ev_cap;
+        fa.wait_ns = ctx->fuse_wait_ns;
         fa.q_head = fq.as<int>() + 2 * ev_cap;
         fa.q_tail = fq.as<int>() + 2 * ev_cap + 1;
         fa.ea = ea;
@@ -1331,6 +1336,7 @@ ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
         const char* tv = std::getenv("NCPA_TIMING");
         ctx->timing = tv && tv[0] == '1';
         if (const char* fv = std::getenv("NCPA_FUSE_SOLVE")) ctx->fuse_solve = fv[0] != '0';
+        if (const char* wv = std::getenv("NCPA_FUSE_WAIT_NS")) ctx->fuse_wait_ns = std::strtoull(wv, nullptr, 10);
         // tuning override of the eigenvalues per bisection item (1..32)
         if (const char* iv = std::getenv("NCPA_BISECT_ITEM")) {
             const int v = std::atoi(iv);

@@ -1,0 +1,53 @@
+"""The fused bisection + eigenvector launch (k_bisect_eigvec) against the two
+kernels run one after the other, and its fallback: eigenvector items that a
+consumer warp gives up on (empty queue slot after the wait limit) are run by
+the k_eigvec launch that follows.  All three must give the same modes bit for
+bit: the per-item code is shared, only who runs an item changes.
+
+The switches are read when a context is created (NCPA_FUSE_SOLVE,
+NCPA_FUSE_WAIT_NS), so each variant gets its own context."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve(path, env, method=0):
+    import ncpa_gpu
+
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        ctx = ncpa_gpu.Context(0)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    prof = ctx.load_profile(path)
+    freqs = np.linspace(0.01, 0.4, 24)
+    m = ctx.solve(prof, ncpa_gpu.default_params(nz_grid=8000, turnoff_wkb=1, method=method), freqs, [90.0, 200.0])
+    out = [m.problem(p) for p in range(m.P)]
+    m.close()
+    prof.close()
+    ctx.close()
+    return out
+
+
+@pytest.mark.parametrize("method", [0, 1])
+def test_fused_unfused_and_fallback_identical(analytic_profile, method):
+    fused = _solve(analytic_profile, {"NCPA_FUSE_SOLVE": "1"}, method)
+    plain = _solve(analytic_profile, {"NCPA_FUSE_SOLVE": "0"}, method)
+    # consumers give up at once on an empty slot: the items are split
+    # between the fused launch and the following one
+    fallback = _solve(analytic_profile, {"NCPA_FUSE_SOLVE": "1", "NCPA_FUSE_WAIT_NS": "0"}, method)
+    assert len(fused) == len(plain) == len(fallback) == 48
+    assert sum(p.M for p in fused) > 1000
+    for a, b, c in zip(fused, plain, fallback):
+        assert a.M == b.M == c.M
+        for f in ("kr", "ki", "vs", "vr"):
+            assert np.array_equal(getattr(a, f), getattr(b, f))
+            assert np.array_equal(getattr(a, f), getattr(c, f))
