@@ -819,7 +819,7 @@ def lapack_baseline(freqs, max_seconds=20.0, az=90.0, every=32):
             "sample": "%d of the 256 frequencies (one in %d), Nz=%d, %d modes: scipy dstebz + dstein per problem, "
                       "one problem per process, no TL%s" % (len(jobs), every, NZ, modes,
                                                             "" if min(res) >= 0 else " (LAPACK reported an error)"),
-            "seconds": round(el, 3)}
+            "seconds": round(el, 3), "lapack_modes": int(sum(res)), "oracle_modes": int(modes)}
 
 
 def run_reference(args):

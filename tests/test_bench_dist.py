@@ -51,3 +51,19 @@ def test_reference_arm_rank_handling(tmp_path):
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["metric"] == "freq-solves/s" and line["value"] > 0
     assert line["cpu_baseline"]["cores"] >= 1 and line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_lapack_leg_on_two_problems():
+    """The LAPACK CPU leg (dstebz + dstein on the oracle's matrices, one
+    problem per process of a spawn-started pool): mode counts from LAPACK
+    equal the oracle's, and the line carries its fields."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    import bench
+
+    freqs = np.array([0.05, 0.12])
+    out = bench.lapack_baseline(freqs, every=1)
+    assert out["kind"] == "lapack" and out["value"] > 0 and out["cores"] >= 1
+    assert "LAPACK reported an error" not in out["sample"]
+    assert out["lapack_modes"] == out["oracle_modes"] > 0
