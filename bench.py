@@ -53,11 +53,6 @@ for p in (ROOT, PKG):
 import workloads  # noqa: E402
 
 METRIC = "freq-solves/s"
-# DRAM bytes (read + write) per launch from one ncu capture of the same
-# workloads (profiles/ess_modbb256_dram_bytes.md, k_bisect;
-# profiles/k_ms_tc_modal_sum_64rcv_20000rng.md, k_ms_tc)
-TRAFFIC_BISECT = 42437888
-TRAFFIC_MS_TC = 4422400
 NZ = 20000
 NFREQ = 256
 RANGES_KM = np.arange(200.0, 300.0 + 1e-9, 10.0)
@@ -366,7 +361,7 @@ def run_ours(args):
                          "achieved": round(achieved, 3) if achieved else None, "peak": round(fp64_peak, 3),
                          "unit": "TFLOP/s", "frac": round(achieved / fp64_peak, 4) if achieved else None,
                          "peak_source": "measured in this run (dependent-FMA probe on all SMs)",
-                         "traffic": TRAFFIC_BISECT, "traffic_source": "ncu capture, profiles/ess_modbb256_dram_bytes.md",
+                         "traffic": None, "traffic_source": "not measured by this run (DRAM counters need ncu)",
                          "avg_launch_ms": round(bis_ms / max(bis_n, 1), 4),
                          "flops_per_launch": flops / bis_n if bis_n else None},
             "phases_ms": {k: round(v, 4) for k, v in phases.items()},
@@ -465,8 +460,8 @@ def modal_sum_leg(ctx, stream, bf16_peak, k=10):
         "roofline": {"kernel": "k_ms_tc (tcgen05 split-BF16)", "bound": "tensor", "achieved": round(achieved, 1),
                      "peak": bf16_peak, "unit": "TFLOP/s", "frac": round(achieved / bf16_peak, 4),
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)",
-                     "flops_per_launch": tensor, "algorithmic_flops_per_launch": alg, "traffic": TRAFFIC_MS_TC,
-                     "traffic_source": "ncu capture, profiles/k_ms_tc_modal_sum_64rcv_20000rng.md"},
+                     "flops_per_launch": tensor, "algorithmic_flops_per_launch": alg, "traffic": None,
+                     "traffic_source": "not measured by this run (DRAM counters need ncu)"},
         "error_vs_fp64": err(p_tc),
         "tf32": {"ms_per_call": round(ms_call_tf32, 4), "ms_kernel": round(ms_kernel_tf32, 4), "phases_ms": phases_tf32,
                  "algorithmic_tflops": round(alg / (ms_kernel_tf32 / 1e3) / 1e12, 1),

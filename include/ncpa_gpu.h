@@ -416,7 +416,11 @@ ncpa_status ncpa_probe_fp64_peak(ncpa_ctx *ctx, double *tflops);
  * until the process exits; limits: nz <= 32768 (NCPA_EINVAL beyond),
  * n <= 4000 (NCPA_ETOOMANY beyond).  All calls share that array, so calls
  * that overlap on the GPU race.  The first call on a device looks the array
- * up; make it before any stream capture. */
+ * up; make it before any stream capture.  The looked-up address is kept until
+ * the process exits, so do not call this again on a device after
+ * cudaDeviceReset there.  Every call waits for its own work to finish before
+ * returning.  NCPA_ETIMEDOUT: a bounded device wait gave up; NCPA_ECUDA: a
+ * CUDA call failed or the kernel reported another device error. */
 ncpa_status ncpa_eigvec_static(const double *s, const double *w, int nz, double dz, const double *mu,
                                int n, int isrc, int ircv, double omega, double *re_k, double *im_k,
                                double *v_src, double *v_rcv, void *stream);

@@ -1,10 +1,10 @@
 // Device helpers shared by the sm_100a kernels of the ESS normal-mode path.
 //
 // Arithmetic conventions: the library is compiled with --fmad=false, so a
-// fused multiply-add appears only where fma() is written.  The CPU oracle
-// (oracle/ncpa_oracle.c, compiled with -ffp-contract=off) performs the same
-// operations, which makes the profile sampling, matrix build and Sturm counts
-// reproducible bit-for-bit between the two.
+// fused multiply-add appears only where fma() is written.  Any CPU code that
+// performs the same operations in the same order without contraction
+// (-ffp-contract=off) reproduces the profile sampling, matrix build and Sturm
+// counts bit-for-bit.
 #pragma once
 
 #include <cstdint>

@@ -1289,9 +1289,13 @@ int launch_fp64_probe(cudaStream_t st, int grid, int block, int n_iter, double* 
 }
 
 // ===========================================================================
-// K4: eigenvectors by twisted factorisation (see oracle/ncpa_oracle.c for the
-// derivation), one eigenvalue per lane, one work item (<= 32 eigenvalues of a
-// problem) per warp.  Each warp streams the diagonal s (and the weights w, g)
+// K4: eigenvectors by twisted factorisation, one eigenvalue per lane, one work
+// item (<= 32 eigenvalues of a problem) per warp.  For S - mu with unit
+// off-diagonals the forward solution of rows 0..i-1 is z_i = (-1)^i p_{i-1}
+// and the backward solution of rows i+1..n-1 is z_i = (-1)^(n-1-i) q_{i+1}
+// (q_n = 1); with the twist r maximising |p_{r-1} q_{r+1}|,
+//   z_i = (-1)^i p_{i-1} q_{r+1} (i <= r),  z_i = (-1)^i p_{r-1} q_{i+1} (i >= r)
+// solves (S - mu) z = gamma_r e_r: one inverse-iteration step from e_r.  Each warp streams the diagonal s (and the weights w, g)
 // through its own TMA ring, so warps never wait on each other.
 //  pass 1  backward recurrence q top-down; every kBlk rows a checkpoint
 //          (q_c, q_{c+1}, exponent) goes to global scratch;

@@ -18,6 +18,11 @@
 // streams, two host threads) race on it.  The first call on a device looks up
 // the array's device address with cudaGetSymbolAddress (once per device, with
 // that device current); make that first call before any stream capture.
+// The address is kept for the life of the process: after cudaDeviceReset on a
+// device the library image is loaded anew there, so a process that resets a
+// device must not call this entry point on it again.  Every call waits for its
+// own work to finish before it returns (it reads the device error word back
+// and synchronises the stream).
 #include <cstdint>
 #include <mutex>
 
@@ -151,5 +156,7 @@ extern "C" ncpa_status ncpa_eigvec_static(const double* s, const double* w, int 
     unsigned herr = 0;
     if (cudaMemcpyAsync(&herr, a.err, sizeof herr, cudaMemcpyDeviceToHost, st) != cudaSuccess) return NCPA_ECUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return NCPA_ECUDA;
-    return herr ? NCPA_ETIMEDOUT : NCPA_OK;
+    if (herr == 0u) return NCPA_OK;
+    // a ring wait that gave up is a timeout; any other device error bit is not
+    return (herr & ~ncpa::kErrTimeout) ? NCPA_ECUDA : NCPA_ETIMEDOUT;
 }

@@ -17,7 +17,7 @@ where the reference checkout is available) and writes compact copies:
                              samples/disp_256freqs_0p5hz_NCPA_canonic.dat and
                              docs/.../modbb_gp_files/code_outputs/myDispersionFile.dat
 
-Usage: python tests/golden/make_golden.py [reference_root]
+Usage: python tests/golden/make_golden.py <reference_root>
 """
 import gzip
 import os
@@ -25,7 +25,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py <reference_root>")
+REF = sys.argv[1]
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 

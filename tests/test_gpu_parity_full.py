@@ -1,0 +1,218 @@
+"""GPU (C ABI) vs CPU oracle at the full size of the benchmark workloads.
+
+* the 256-frequency broadband job exactly as the benchmark step runs it
+  (df = 0.5/256 Hz up to 0.5 Hz, Nz = 20000, WKB off as ModBB --dispersion
+  forces, azimuth 90): every frequency's mode count, k, Im k and V_s V_r, the
+  1-D TL at 1000 ranges x 1 km, and the pulse synthesis at 200-300 km;
+* the top of the azimuth sweep (2 Hz, Nz = 60000, WKB window on) at several
+  azimuths, solved in one mixed-grid batch with a 0.1 Hz, Nz = 5000 job;
+* the tall-atmosphere solve (2 Hz, 0-180 km, Nz = 100000, >1300 modes):
+  counts, k, Im k, V_s V_r and the modal sum at 64 receivers (0-10 km) x 2000
+  ranges to 2000 km against the oracle's eigenvectors at those receivers.
+
+Tolerances are those of the smaller parity tests: identical mode counts,
+|dk|/k <= max(1e-9, conditioning floor), Im k and V_s V_r within 1e-6, TL
+within 0.05 dB wherever TL > -140 dB, waveforms within 1e-4 relative L2.
+The worst errors seen are written as JSON to the file named by the
+NCPA_PARITY_REPORT environment variable, when it is set.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+EPS = np.finfo(float).eps
+_REPORT = {}
+
+
+def _k_tol(k, dz):
+    return np.maximum(1e-9, 8 * EPS * (4.0 / dz ** 2) / (2 * k ** 2))
+
+
+def _record(name, **vals):
+    _REPORT[name] = {k: (float(v) if np.ndim(v) == 0 else v) for k, v in vals.items()}
+    path = os.environ.get("NCPA_PARITY_REPORT")
+    if path:
+        with open(path, "w") as f:
+            json.dump(_REPORT, f, indent=1)
+
+
+def _mode_errors(g, o):
+    """worst relative errors of one problem (counts must already agree)"""
+    if o.M == 0:
+        return 0.0, 0.0, 0.0, 0.0
+    dk = np.abs(g.kr - o.kr) / o.kr
+    kfrac = np.max(dk / _k_tol(o.kr, o.dz))
+    dki = np.max(np.abs(g.ki - o.ki) / np.maximum(np.abs(o.ki), 1e-300))
+    vv, ov = g.vs * g.vr, o.vs * o.vr
+    dvv = np.max(np.abs(vv - ov) / np.maximum(np.abs(ov), 1e-12 * np.abs(ov).max()))
+    return float(dk.max()), float(kfrac), float(dki), float(dvv)
+
+
+def _tl_db(re, im):
+    return 20 * np.log10(np.hypot(re, im))
+
+
+# ---------------------------------------------------------------------------
+# the 256-frequency job
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def job256(gpu, analytic_profile):
+    import ncpa_gpu
+    import workloads
+    from oracle import oracle as O
+
+    freqs = workloads.broadband_freqs(256, 0.5)
+    prm = O.EssParams(Nz_grid=20000, turnoff_WKB=True)
+    pp = O.prepare(O.read_profile(analytic_profile), prm)
+    oracle_sets = [O.solve_problem(pp, prm, f, 90.0) for f in freqs]
+    prof = gpu.load_profile(analytic_profile)
+    modes = gpu.solve(prof, ncpa_gpu.default_params(nz_grid=20000, turnoff_wkb=1), freqs, [90.0])
+    yield freqs, modes, oracle_sets
+    modes.close()
+    prof.close()
+
+
+def test_job256_modes_every_frequency(job256):
+    freqs, modes, osets = job256
+    counts = modes.counts()
+    ocounts = np.array([o.M for o in osets])
+    assert np.array_equal(counts, ocounts), np.nonzero(counts != ocounts)
+    worst = np.zeros(4)
+    for p, o in enumerate(osets):
+        g = modes.problem(p)
+        assert abs(g.k_min - o.k_min) <= 1e-14 * o.k_min
+        assert abs(g.k_max - o.k_max) <= 1e-14 * o.k_max
+        e = _mode_errors(g, o)
+        worst = np.maximum(worst, e)
+    assert worst[1] <= 1.0, worst
+    assert worst[2] <= 1e-6 and worst[3] <= 1e-6, worst
+    _record("job256_modes", frequencies=len(freqs), modes_total=int(ocounts.sum()), modes_max=int(ocounts.max()),
+            k_rel_max=worst[0], k_over_tol_max=worst[1], im_k_rel_max=worst[2], vsvr_rel_max=worst[3])
+
+
+def test_job256_tl1d_every_frequency(job256):
+    from oracle import oracle as O
+
+    freqs, modes, osets = job256
+    re, im, inc = modes.tl1d(1000, 1000.0)
+    worst, worst_inc, n = 0.0, 0.0, 0
+    for p, o in enumerate(osets):
+        ore, oim, oinc = O.tl1d(o, 1000, 1000.0)
+        tl_o = _tl_db(ore, oim)
+        mask = tl_o > -140
+        if o.M == 0 or not mask.any():
+            continue
+        d = np.abs(_tl_db(re[p], im[p]) - tl_o)[mask]
+        worst = max(worst, float(d.max()))
+        worst_inc = max(worst_inc, float(np.max(np.abs(inc[p] - oinc) / oinc)))
+        n += int(mask.sum())
+    assert worst <= 0.05, worst
+    assert worst_inc <= 1e-6, worst_inc
+    _record("job256_tl1d", points=n, tl_db_max=worst, incoherent_rel_max=worst_inc)
+
+
+def test_job256_synthesis(job256):
+    import workloads
+    from oracle import oracle as O
+
+    freqs, modes, osets = job256
+    d = O.dispersion_from_modesets(osets)
+    t, x = workloads.ricker_waveform()
+    nfft = O.bb_nfft(len(d.f), 0, len(x))
+    sre, sim = O.source_spectrum("waveform", d.f, nfft, waveform=(t, x))
+    ranges = np.arange(200.0, 300.0 + 1e-9, 10.0) * 1000.0
+    out = modes.bb_synthesize(ranges, 340.0, nfft, sre, sim)
+    worst = 0.0
+    for i, r in enumerate(ranges):
+        hre, him = O.bb_transfer(d, r)
+        ref = O.bb_pulse(d, sre, sim, hre, him, r / 340.0, nfft)
+        worst = max(worst, float(np.linalg.norm(out[i] - ref) / np.linalg.norm(ref)))
+    assert worst < 1e-4, worst
+    _record("job256_synthesis", ranges=len(ranges), nfft=nfft, rel_l2_max=worst)
+
+
+# ---------------------------------------------------------------------------
+# top of the azimuth sweep: 2 Hz at Nz = 60000, mixed with a 0.1 Hz grid
+# ---------------------------------------------------------------------------
+def test_sweep_top_vs_oracle(gpu, analytic_profile):
+    import ncpa_gpu
+    import workloads
+    from oracle import oracle as O
+
+    nz_hi = workloads.sweep_nz(2.0)
+    nz_lo = workloads.sweep_nz(0.1)
+    assert nz_hi == 60000 and nz_lo == 5000
+    azs = np.array([0.0, 90.0, 135.0, 270.0])
+    prof = gpu.load_profile(analytic_profile)
+    m = gpu.solve_jobs([(prof, [2.0], azs, nz_hi), (prof, [0.1], azs, nz_lo)], ncpa_gpu.default_params())
+    re, im, _ = m.tl1d(2000, 500.0)
+    op = O.read_profile(analytic_profile)
+    worst, worst_tl, total = np.zeros(4), 0.0, 0
+    p = 0
+    for f, nz in ((2.0, nz_hi), (0.1, nz_lo)):
+        prm = O.EssParams(Nz_grid=nz)
+        pp = O.prepare(op, prm)
+        for a in azs:
+            o = O.solve_problem(pp, prm, f, a)
+            g = m.problem(p)
+            assert g.M == o.M, (f, a, g.M, o.M)
+            total += o.M
+            worst = np.maximum(worst, _mode_errors(g, o))
+            ore, oim, _ = O.tl1d(o, 2000, 500.0)
+            tl_o = _tl_db(ore, oim)
+            mask = tl_o > -140
+            if mask.any():
+                worst_tl = max(worst_tl, float(np.max(np.abs(_tl_db(re[p], im[p]) - tl_o)[mask])))
+            p += 1
+    m.close()
+    prof.close()
+    assert worst[1] <= 1.0, worst
+    assert worst[2] <= 1e-6 and worst[3] <= 1e-6, worst
+    assert worst_tl <= 0.05, worst_tl
+    _record("sweep_top", problems=2 * len(azs), modes_total=total, k_rel_max=worst[0], k_over_tol_max=worst[1],
+            im_k_rel_max=worst[2], vsvr_rel_max=worst[3], tl_db_max=worst_tl)
+
+
+# ---------------------------------------------------------------------------
+# tall atmosphere: 2 Hz, 0-180 km, Nz = 100000
+# ---------------------------------------------------------------------------
+def test_tall_atmosphere_vs_oracle(gpu, workdir):
+    import ncpa_gpu
+    import workloads
+    from oracle import oracle as O
+
+    nz, freq, top = 100000, 2.0, 180.0
+    path = workloads.write_profile(os.path.join(str(workdir), "analytic_180km.dat"), top_km=top)
+    prm = O.EssParams(Nz_grid=nz, maxheight_km=top, turnoff_WKB=True)
+    o = O.solve_problem(O.prepare(O.read_profile(path), prm), prm, freq, 90.0, want_full=True)
+    prof = gpu.load_profile(path)
+    m = gpu.solve(prof, ncpa_gpu.default_params(nz_grid=nz, maxheight_km=top, turnoff_wkb=1, want_vectors=1),
+                  [freq], [90.0])
+    g = m.problem(0)
+    assert g.M == o.M and o.M > 1000, (g.M, o.M)
+    e = _mode_errors(g, o)
+    assert e[1] <= 1.0 and e[2] <= 1e-6 and e[3] <= 1e-6, e
+    # modal sum at 64 receivers 0-10 km x 2000 ranges to 2000 km (FP64 sum)
+    h = np.linspace(0.0, 10000.0, 64)
+    idx = np.ceil(h / g.dz).astype(int)
+    nr, dr = 2000, 1000.0
+    p64 = m.tl_multi(0, h, nr, dr, method=m.SUM_FP64)
+    vz = np.ascontiguousarray(o.vfull[idx, :])
+    ore, oim = np.empty((nr, len(idx))), np.empty((nr, len(idx)))
+    O.lib().orc_tl2d(o.M, O._p(O._f64(o.kr)), O._p(O._f64(o.ki)), O._p(O._f64(o.vs)), O._p(vz), len(idx), nr, dr, 0,
+                     O._p(ore), O._p(oim))
+    tl_o = _tl_db(ore, oim).T
+    tl_g = _tl_db(p64.real, p64.imag)
+    mask = tl_o > -140
+    assert mask.mean() > 0.5
+    d = np.abs(tl_g - tl_o)[mask]
+    m.close()
+    prof.close()
+    assert d.max() <= 0.05, d.max()
+    _record("tall_atmosphere", modes=int(o.M), k_rel_max=e[0], k_over_tol_max=e[1], im_k_rel_max=e[2],
+            vsvr_rel_max=e[3], tl_points=int(mask.sum()), tl_db_max=float(d.max()),
+            tl_db_median=float(np.median(d)))
