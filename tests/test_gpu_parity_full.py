@@ -11,8 +11,9 @@
   ranges to 2000 km against the oracle's eigenvectors at those receivers.
 
 Tolerances are those of the smaller parity tests: identical mode counts,
-|dk|/k <= max(1e-9, conditioning floor), Im k and V_s V_r within 1e-6, TL
-within 0.05 dB wherever TL > -140 dB, waveforms within 1e-4 relative L2.
+|dk|/k <= max(1e-9, conditioning floor), Im k and V_s V_r within 1e-6
+relative (with the same small absolute floors), TL within 0.05 dB wherever
+TL > -140 dB, waveforms within 1e-4 relative L2.
 The worst errors seen are written as JSON to the file named by the
 NCPA_PARITY_REPORT environment variable, when it is set.
 """
@@ -41,15 +42,23 @@ def _record(name, **vals):
 
 
 def _mode_errors(g, o):
-    """worst relative errors of one problem (counts must already agree)"""
+    """worst errors of one problem (counts must already agree): max |dk|/k,
+    max |dk| / k tolerance, and for Im k and V_s V_r the largest
+    |d| / (1e-6 |x| + floor) (<= 1 passes: rtol 1e-6 with an absolute floor of
+    1e-18 for Im k and 1e-12 max|V_s V_r| for V_s V_r, as the other parity
+    tests), plus the plain relative V_s V_r error over the modes with
+    |V_s V_r| >= 1e-3 of the largest"""
     if o.M == 0:
-        return 0.0, 0.0, 0.0, 0.0
+        return np.zeros(5)
     dk = np.abs(g.kr - o.kr) / o.kr
     kfrac = np.max(dk / _k_tol(o.kr, o.dz))
-    dki = np.max(np.abs(g.ki - o.ki) / np.maximum(np.abs(o.ki), 1e-300))
+    dki = np.max(np.abs(g.ki - o.ki) / (1e-6 * np.abs(o.ki) + 1e-18))
     vv, ov = g.vs * g.vr, o.vs * o.vr
-    dvv = np.max(np.abs(vv - ov) / np.maximum(np.abs(ov), 1e-12 * np.abs(ov).max()))
-    return float(dk.max()), float(kfrac), float(dki), float(dvv)
+    big = np.abs(ov).max()
+    dvv = np.max(np.abs(vv - ov) / (1e-6 * np.abs(ov) + 1e-12 * big))
+    sel = np.abs(ov) >= 1e-3 * big
+    rel_big = np.max(np.abs(vv - ov)[sel] / np.abs(ov)[sel])
+    return np.array([dk.max(), kfrac, dki, dvv, rel_big])
 
 
 def _tl_db(re, im):
@@ -81,17 +90,17 @@ def test_job256_modes_every_frequency(job256):
     counts = modes.counts()
     ocounts = np.array([o.M for o in osets])
     assert np.array_equal(counts, ocounts), np.nonzero(counts != ocounts)
-    worst = np.zeros(4)
+    worst = np.zeros(5)
     for p, o in enumerate(osets):
         g = modes.problem(p)
         assert abs(g.k_min - o.k_min) <= 1e-14 * o.k_min
         assert abs(g.k_max - o.k_max) <= 1e-14 * o.k_max
         e = _mode_errors(g, o)
         worst = np.maximum(worst, e)
-    assert worst[1] <= 1.0, worst
-    assert worst[2] <= 1e-6 and worst[3] <= 1e-6, worst
+    assert worst[1] <= 1.0 and worst[2] <= 1.0 and worst[3] <= 1.0, worst
     _record("job256_modes", frequencies=len(freqs), modes_total=int(ocounts.sum()), modes_max=int(ocounts.max()),
-            k_rel_max=worst[0], k_over_tol_max=worst[1], im_k_rel_max=worst[2], vsvr_rel_max=worst[3])
+            k_rel_max=worst[0], k_over_tol_max=worst[1], im_k_over_tol_max=worst[2], vsvr_over_tol_max=worst[3],
+            vsvr_rel_max_large_modes=worst[4])
 
 
 def test_job256_tl1d_every_frequency(job256):
@@ -151,7 +160,7 @@ def test_sweep_top_vs_oracle(gpu, analytic_profile):
     m = gpu.solve_jobs([(prof, [2.0], azs, nz_hi), (prof, [0.1], azs, nz_lo)], ncpa_gpu.default_params())
     re, im, _ = m.tl1d(2000, 500.0)
     op = O.read_profile(analytic_profile)
-    worst, worst_tl, total = np.zeros(4), 0.0, 0
+    worst, worst_tl, total = np.zeros(5), 0.0, 0
     p = 0
     for f, nz in ((2.0, nz_hi), (0.1, nz_lo)):
         prm = O.EssParams(Nz_grid=nz)
@@ -170,11 +179,11 @@ def test_sweep_top_vs_oracle(gpu, analytic_profile):
             p += 1
     m.close()
     prof.close()
-    assert worst[1] <= 1.0, worst
-    assert worst[2] <= 1e-6 and worst[3] <= 1e-6, worst
+    assert worst[1] <= 1.0 and worst[2] <= 1.0 and worst[3] <= 1.0, worst
     assert worst_tl <= 0.05, worst_tl
     _record("sweep_top", problems=2 * len(azs), modes_total=total, k_rel_max=worst[0], k_over_tol_max=worst[1],
-            im_k_rel_max=worst[2], vsvr_rel_max=worst[3], tl_db_max=worst_tl)
+            im_k_over_tol_max=worst[2], vsvr_over_tol_max=worst[3], vsvr_rel_max_large_modes=worst[4],
+            tl_db_max=worst_tl)
 
 
 # ---------------------------------------------------------------------------
@@ -195,7 +204,7 @@ def test_tall_atmosphere_vs_oracle(gpu, workdir):
     g = m.problem(0)
     assert g.M == o.M and o.M > 1000, (g.M, o.M)
     e = _mode_errors(g, o)
-    assert e[1] <= 1.0 and e[2] <= 1e-6 and e[3] <= 1e-6, e
+    assert e[1] <= 1.0 and e[2] <= 1.0 and e[3] <= 1.0, e
     # modal sum at 64 receivers 0-10 km x 2000 ranges to 2000 km (FP64 sum)
     h = np.linspace(0.0, 10000.0, 64)
     idx = np.ceil(h / g.dz).astype(int)
@@ -213,6 +222,6 @@ def test_tall_atmosphere_vs_oracle(gpu, workdir):
     m.close()
     prof.close()
     assert d.max() <= 0.05, d.max()
-    _record("tall_atmosphere", modes=int(o.M), k_rel_max=e[0], k_over_tol_max=e[1], im_k_rel_max=e[2],
-            vsvr_rel_max=e[3], tl_points=int(mask.sum()), tl_db_max=float(d.max()),
+    _record("tall_atmosphere", modes=int(o.M), k_rel_max=e[0], k_over_tol_max=e[1], im_k_over_tol_max=e[2],
+            vsvr_over_tol_max=e[3], vsvr_rel_max_large_modes=e[4], tl_points=int(mask.sum()), tl_db_max=float(d.max()),
             tl_db_median=float(np.median(d)))
