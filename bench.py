@@ -390,14 +390,17 @@ def run_ours(args):
 MS_NZ, MS_FREQ, MS_TOP_KM, MS_NR, MS_DR, MS_RCV = 100000, 2.0, 180.0, 20000, 100.0, 64
 
 
-def modal_sum_leg(ctx, stream, bf16_peak, k=10):
+def modal_sum_leg(ctx, stream, bf16, k=10):
     """Solve the 2 Hz, 180 km, Nz = 100000 problem once (untimed), then time
     the modal sum at 64 receivers (0-10 km) x 20000 ranges (0.1 km to 2000 km)
-    through ncpa_tl_multi: tensor-core split-BF16 kernel and the FP64 CUDA-core
-    sum, with the tensor-core result's error against the FP64 one."""
+    through ncpa_tl_multi: the guarded tensor-core sum (6-term split-BF16 with
+    FP64 recomputation of the points its error bound flags), the unguarded
+    3-term split-BF16 and TF32 sums, and the FP64 CUDA-core sum; errors of
+    each against the FP64 sum over the whole grid."""
     import torch
     import ncpa_gpu
 
+    bf16_peak, peak_source = bf16
     tmp = tempfile.mkdtemp(prefix="ncpa_ms_")
     path = workloads.write_profile(os.path.join(tmp, "analytic_180km.dat"), top_km=MS_TOP_KM)
     prof = ctx.load_profile(path)
@@ -405,6 +408,7 @@ def modal_sum_leg(ctx, stream, bf16_peak, k=10):
                                                 turnoff_wkb=1), [MS_FREQ], [90.0])
     M = m.count(0)
     h = np.linspace(0.0, 10000.0, MS_RCV)
+    G, X3, T32, F64 = m.SUM_TC_GUARDED, m.SUM_TC_BF16X3, m.SUM_TC_TF32, m.SUM_FP64
 
     def timed(method, reps):
         for _ in range(2):
@@ -425,49 +429,62 @@ def modal_sum_leg(ctx, stream, bf16_peak, k=10):
         for _ in range(k):
             m.tl_multi(0, h, MS_NR, MS_DR, method=method, to_host=False)
         ctx.set_timing(False)
-        ph = {n: ctx.phase_stats(n) for n in ("ms-prep", "ms-tc", "ms-finish")}
-        per = {n: round(t / max(c, 1), 4) for n, (t, c) in ph.items()}
+        ph = {n: ctx.phase_stats(n) for n in ("ms-prep", "ms-tc", "ms-finish", "ms-fix")}
+        per = {n: round(t / max(c, 1), 4) for n, (t, c) in ph.items() if c > 0}
         return per["ms-tc"], per
 
-    ms_call = timed(1, k)
-    ms_call_tf32 = timed(2, k)
-    ms_fp64 = timed(0, 2)
-    ms_kernel, phases = kernel_ms(1)
-    ms_kernel_tf32, phases_tf32 = kernel_ms(2)
-    p_tc = m.tl_multi(0, h, 2000, MS_DR, method=1)
-    p_32 = m.tl_multi(0, h, 2000, MS_DR, method=2)
-    p_64 = m.tl_multi(0, h, 2000, MS_DR, method=0)
+    ms_call_g = timed(G, k)
+    ms_call = timed(X3, k)
+    ms_call_tf32 = timed(T32, k)
+    ms_fp64 = timed(F64, 2)
+    ms_kernel_g, phases_g = kernel_ms(G)
+    ms_kernel, phases = kernel_ms(X3)
+    ms_kernel_tf32, phases_tf32 = kernel_ms(T32)
+    p_64 = m.tl_multi(0, h, MS_NR, MS_DR, method=F64)
+    p_g = m.tl_multi(0, h, MS_NR, MS_DR, method=G)
+    fixed, points = ctx.sum_fixups()
+    p_tc = m.tl_multi(0, h, MS_NR, MS_DR, method=X3)
+    p_32 = m.tl_multi(0, h, MS_NR, MS_DR, method=T32)
     m.close()
     prof.close()
     alg = 8.0 * MS_RCV * M * MS_NR          # complex multiply-adds x 8 flops
-    tensor = 3.0 * alg                       # three bf16 products per term
-    achieved = tensor / (ms_kernel / 1e3) / 1e12
-    sel = 20 * np.log10(np.abs(p_64)) > -140.0
+    tl64 = 20 * np.log10(np.abs(p_64))
+    sel = tl64 > -140.0
 
     def err(p):
-        d = np.abs(20 * np.log10(np.abs(p)) - 20 * np.log10(np.abs(p_64)))[sel]
+        d = np.abs(20 * np.log10(np.abs(p)) - tl64)[sel]
         rel = np.abs(p - p_64).max(axis=1) / np.abs(p_64).max(axis=1)
         return {"max_abs_over_max_P": float(rel.max()), "tl_db_median": float(np.median(d)),
                 "tl_db_p99_9": float(np.percentile(d, 99.9)), "tl_db_max": float(d.max()),
-                "where": "TL > -140 dB, first 2000 ranges"}
+                "where": "every point with TL > -140 dB (%d of %d)" % (int(sel.sum()), sel.size)}
 
+    tensor_g = 6.0 * alg                     # six bf16 products per term
+    achieved_g = tensor_g / (ms_kernel_g / 1e3) / 1e12
+    tensor3 = 3.0 * alg
+    achieved3 = tensor3 / (ms_kernel / 1e3) / 1e12
     return {
         "workload": "2 Hz, analytic 0-180 km, Nz=100000, %d modes; 64 receivers 0-10 km x 20000 ranges to 2000 km"
                     % M,
         "modes": int(M),
-        "ms_per_call": round(ms_call, 4), "ms_kernel": round(ms_kernel, 4), "ms_fp64_cuda_cores": round(ms_fp64, 3),
-        "phases_ms": phases,
-        "roofline": {"kernel": "k_ms_tc (tcgen05 split-BF16)", "bound": "tensor", "achieved": round(achieved, 1),
-                     "peak": bf16_peak, "unit": "TFLOP/s", "frac": round(achieved / bf16_peak, 4),
-                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)",
-                     "flops_per_launch": tensor, "algorithmic_flops_per_launch": alg, "traffic": None,
+        "ms_per_call": round(ms_call_g, 4), "ms_kernel": round(ms_kernel_g, 4),
+        "ms_fp64_cuda_cores": round(ms_fp64, 3), "phases_ms": phases_g,
+        "recomputed_fp64": {"points": int(fixed), "of": int(points), "frac": fixed / max(points, 1)},
+        "roofline": {"kernel": "k_ms_tc<guarded> (tcgen05 6-term split-BF16)", "bound": "tensor",
+                     "achieved": round(achieved_g, 1), "peak": bf16_peak, "unit": "TFLOP/s",
+                     "frac": round(achieved_g / bf16_peak, 4),
+                     "frac_whole_call": round(tensor_g / (ms_call_g / 1e3) / 1e12 / bf16_peak, 4),
+                     "peak_source": peak_source,
+                     "flops_per_launch": tensor_g, "algorithmic_flops_per_launch": alg, "traffic": None,
                      "traffic_source": "not measured by this run (DRAM counters need ncu)"},
-        "error_vs_fp64": err(p_tc),
+        "error_vs_fp64": err(p_g),
+        "bf16x3": {"ms_per_call": round(ms_call, 4), "ms_kernel": round(ms_kernel, 4), "phases_ms": phases,
+                   "achieved_tflops": round(achieved3, 1), "frac": round(achieved3 / bf16_peak, 4),
+                   "note": "unguarded: stated error only", "error_vs_fp64": err(p_tc)},
         "tf32": {"ms_per_call": round(ms_call_tf32, 4), "ms_kernel": round(ms_kernel_tf32, 4), "phases_ms": phases_tf32,
                  "algorithmic_tflops": round(alg / (ms_kernel_tf32 / 1e3) / 1e12, 1),
                  "frac_of_tf32_peak": round(alg / (ms_kernel_tf32 / 1e3) / 1e12 / (bf16_peak / 2.0), 4),
                  "peak_note": "tf32 dense rate taken as half the measured bf16 peak",
-                 "error_vs_fp64": err(p_32)},
+                 "note": "unguarded: stated error only", "error_vs_fp64": err(p_32)},
     }
 
 
@@ -717,11 +734,12 @@ def serving_leg(ctx, n=SV_N):
 
 
 def _bf16_peak():
+    """(dense bf16 TFLOP/s, where the figure comes from)"""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            return float(json.load(f)["bf16_tflops"])
+            return float(json.load(f)["bf16_tflops"]), "MEASURED_PEAKS.json bf16_tflops (burst), of measured"
     except (OSError, KeyError, ValueError):
-        return 1590.0  # earlier measurement on this pool, used when the file is absent
+        return 1590.0, "fallback 1590 TFLOP/s (earlier burst measurement on this pool; MEASURED_PEAKS.json absent)"
 
 
 # ---------------------------------------------------------------------------

@@ -209,8 +209,17 @@ ncpa_status ncpa_tl_2d(ncpa_ctx *ctx, const ncpa_modes *modes, int problem, cons
  *                        the modal terms' magnitude)
  *   NCPA_SUM_TC_TF32     tcgen05 tensor cores: TF32 products (operands
  *                        rounded to nearest) with FP32 accumulation, same
- *                        phase reduction (relative error ~1e-3) */
-enum { NCPA_SUM_FP64 = 0, NCPA_SUM_TC_BF16X3 = 1, NCPA_SUM_TC_TF32 = 2 };
+ *                        phase reduction (relative error ~1e-3)
+ *   NCPA_SUM_TC_GUARDED  tcgen05 tensor cores, 6-term split-BF16 (operands
+ *                        split into three bf16 parts, FP32-level products)
+ *                        with an error guard: every point whose |P| is below
+ *                        the bound that keeps its TL within 0.05 dB is
+ *                        recomputed in FP64 on the CUDA cores, so TL agrees
+ *                        with the FP64 sum within 0.05 dB everywhere.
+ * BF16X3 and TF32 carry the stated relative errors only: in cancellation
+ * nulls (|P| far below the modal terms' magnitude) their TL error grows
+ * beyond 0.05 dB; use FP64 or GUARDED where every point must hold it. */
+enum { NCPA_SUM_FP64 = 0, NCPA_SUM_TC_BF16X3 = 1, NCPA_SUM_TC_TF32 = 2, NCPA_SUM_TC_GUARDED = 3 };
 ncpa_status ncpa_tl_multi(ncpa_ctx *ctx, const ncpa_modes *modes, int problem, int n_rcv,
                           const double *rcv_height_m, const ncpa_tl_params *tp, int method, double *re,
                           double *im);
@@ -395,6 +404,9 @@ ncpa_status ncpa_ctx_set_timing(ncpa_ctx *ctx, int on);
 ncpa_status ncpa_ctx_phase_stats(const ncpa_ctx *ctx, const char *phase, double *total_ms, long long *calls);
 ncpa_status ncpa_ctx_reset_stats(ncpa_ctx *ctx);
 ncpa_status ncpa_ctx_sturm_steps(ncpa_ctx *ctx, long long *steps);
+/* Points the last NCPA_SUM_TC_GUARDED modal sum of this context recomputed
+ * in FP64, and its receivers x ranges (waits for the context's stream). */
+ncpa_status ncpa_ctx_sum_fixups(ncpa_ctx *ctx, long long *recomputed, long long *points);
 /* Measured FP64 FMA throughput of this device [TFLOP/s, FMA = 2 flops]: a
  * dependent-FMA kernel on every SM for about 50 ms. */
 ncpa_status ncpa_probe_fp64_peak(ncpa_ctx *ctx, double *tflops);

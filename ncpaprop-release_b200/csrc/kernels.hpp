@@ -212,18 +212,28 @@ struct MsPlan {
     int groups, n_chunks, M_pad, n_tiles, n_ctas, n_parts;
     long long n_units;  // (receiver group, range tile, mode chunk) units
     size_t a_img_bytes, q_bytes, tab_bytes, raw_bytes;
+    // guarded sum (fmt 2): partial sums of |A'|, FP64 tables, flagged points
+    size_t s_part_bytes, b64_bytes, tp64_bytes, a64_bytes, fix_list_bytes;
 };
 MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms);
+// flag threshold of the guarded sum: a point with |P| < tau S is recomputed
+double ms_guard_tau();
 int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const double* vfull, double* vz);
-// fmt: 0 = 3-term split-BF16 (kind::f16), 1 = TF32 (kind::tf32).  Buffers:
-// a_img = A as complex FP32 per (receiver group, mode chunk), q = tile
-// phases, tab = the B' image of each mode chunk (tile-independent)
+// fmt: 0 = 3-term split-BF16 (kind::f16), 1 = TF32 (kind::tf32), 2 = guarded
+// 6-term split-BF16.  Buffers: a_img = A as complex FP32 per (receiver group,
+// mode chunk), q = tile phases, tab = the B' image of each mode chunk
+// (tile-independent); b64, tp64, a64 (fmt 2 only, else NULL) = the FP64
+// offset phases, tile phases and A the fix-up reads
 int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int M, const double* kr,
                       const double* ki, const double* vs, const int* idx, const double* vfull, double dr, int lossless,
-                      void* a_img, void* q, void* tab);
+                      void* a_img, void* q, void* tab, void* b64, void* tp64, void* a64);
 int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const void* a_img, const void* q,
-                 const void* tab, float* raw, unsigned* err);
+                 const void* tab, float* raw, float* s_part, unsigned* err);
+// s_part non-NULL: flag the points the guarded sum must recompute into
+// fix_list / fix_count (zeroed by the caller)
 int launch_ms_finish(cudaStream_t st, const MsPlan& p, int n_rcv, int n_ranges, double dr, const float* raw,
-                     double* re, double* im);
+                     double* re, double* im, const float* s_part, int* fix_count, void* fix_list);
+int launch_ms_fix(cudaStream_t st, int num_sms, int M, int M_pad, int n_ranges, double dr, const int* fix_count,
+                  const void* fix_list, const void* a64, const void* tp64, const void* b64, double* re, double* im);
 
 }  // namespace ncpa

@@ -10,15 +10,23 @@
 //   D[128 x N] = A'[128 x 2M] * B'[2M x N],
 //   A' = [[Re A, -Im A], [Im A, Re A]] (rows 0..63 give Re P, 64..127 Im P),
 //   B' = [[Re E], [Im E]] interleaved per mode (k = 2m: Re, 2m + 1: Im).
-// Two operand formats (template parameter F of the kernels):
+// Three operand formats (template parameter F of the kernels):
 //  * kMsBf16x3: each operand is split into bf16 hi + lo parts and D
 //    accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32 (3-term
 //    split-BF16, ~2^-16 relative per product; kind::f16, K = 16 per MMA);
 //  * kMsTf32: each operand rounded to TF32 (10-bit mantissa, round to
 //    nearest) and D accumulates A B in FP32 (one product, ~2^-11 relative;
-//    kind::tf32, K = 8 per MMA).
-// Both keep a chunk's A' in 16 KB and its B' in 32 KB of shared memory, so the
-// pipeline, barriers and epilogue are shared.
+//    kind::tf32, K = 8 per MMA);
+//  * kMsBf16x6: each operand is split into bf16 hi + mid + lo parts (24
+//    significant bits, an FP32 value exactly) and D accumulates the six
+//    products hi hi, hi mid, mid hi, hi lo, mid mid, lo hi (the dropped ones
+//    are ~2^-24 relative), so the result carries FP32-accumulation error only.
+//    This is the guarded sum: the generators also add up |A'| per receiver
+//    and tile, the finishing kernel flags every point whose |P| is too small
+//    for that error to stay below 0.05 dB in TL, and k_ms_fix recomputes the
+//    flagged points in FP64.
+// A chunk's A' takes 16 KB (24 KB for kMsBf16x6) and its B' 32 KB (48 KB) of
+// shared memory; the pipeline, barriers and epilogue are shared.
 //
 // Since r_n = r_n0 + o dr inside a 256-range tile (r_n0 its first range),
 // E_mn = e^{i k_m r_n0} e^{i k_m o dr}: the tile's phase is folded into A
@@ -62,26 +70,49 @@ constexpr int kMsABytes = kMsRows * kMsKC * 2;   // one A' part (hi or lo) of a 
 constexpr int kMsBBytes = kMsNT * kMsKC * 2;     // one B' part of a chunk: 16 KB
 constexpr int kMsACBytes = kMsModes * kMsRcv * 8;  // a chunk's A as complex FP32, [mode][receiver]: 8 KB
 constexpr int kMsQBytes = kMsModes * 8;            // tile phases of one chunk
-// TMA stage: B' image (hi, lo), A complex, tile phases (1 KB aligned)
-constexpr int kMsOffAC = 2 * kMsBBytes;
-constexpr int kMsOffQ = kMsOffAC + kMsACBytes;
-constexpr int kMsTxBytes = 2 * kMsBBytes + kMsACBytes + kMsQBytes;
-constexpr int kMsTStageBytes = (kMsOffQ + kMsQBytes + 1023) / 1024 * 1024;
-constexpr int kMsTStages = 4;       // ring of TMA stages
-constexpr int kMsGStageBytes = 2 * kMsABytes;  // generated A' (hi, lo)
-constexpr int kMsGStages = 3;       // ring of generated A' chunks
-constexpr int kMsOffGRing = kMsTStages * kMsTStageBytes;
-constexpr int kMsSmem = kMsOffGRing + kMsGStages * kMsGStageBytes + 1024;
 constexpr int kMsGenWarps = 8;      // A' generators / epilogue
 constexpr int kMsGenThreads = 32 * kMsGenWarps;
 constexpr int kMsProducerWarp = 1 + kMsGenWarps;  // warp 0: MMA issuer, 1-8: generators, 9: TMA producer
 constexpr int kMsThreads = 32 * (kMsProducerWarp + 1);
 constexpr int kMsAcc = 2;           // TMEM accumulators (kMsNT columns each): all 512 columns
-static_assert(kMsSmem <= 232448 - 256, "shared memory per block");
-static_assert(kMsACBytes % 16 == 0 && kMsQBytes % 16 == 0 && kMsTxBytes % 16 == 0 && (2 * kMsBBytes) % 1024 == 0,
-              "bulk copies move 16-byte multiples");
+constexpr int kMsMaxStages = 4;     // barrier arrays are sized for the deepest ring
 static_assert(kMsAcc * kMsNT <= 512, "TMEM columns");
 static_assert(kMsGenThreads == kMsRcv * (kMsModes / 4), "one generator per (receiver, mode quad)");
+
+enum : int { kMsBf16x3 = 0, kMsTf32 = 1, kMsBf16x6 = 2 };
+
+// guarded sum: the TL tolerance it keeps, and the bound eps of its error
+// relative to S = sum_m |A'_jm| (the magnitude of the modal terms at the
+// tile's first range): |P_tc - P| <= eps S.  The six-product split drops
+// terms ~2^-24 relative and accumulates in FP32; eps covers the measured
+// worst case of the 64-receiver x 20000-range x 1362-mode workload with a
+// wide margin.
+constexpr double kMsGuardTlDb = 0.05;
+constexpr double kMsGuardEps = 1.0e-6;
+
+// shared-memory plan of a format: a TMA stage holds the chunk's B' image
+// (kParts parts of 16 KB; TF32: one 32-bit image of the same size as two),
+// A as complex FP32 and the tile phases (1 KB aligned); a generated A' stage
+// holds kParts parts of 8 KB
+template <int F>
+struct MsCfg {
+    static constexpr int kParts = F == kMsBf16x6 ? 3 : 2;
+    static constexpr int kBChunk = kParts * kMsBBytes;   // B' image bytes per chunk
+    static constexpr int kOffAC = kBChunk;
+    static constexpr int kOffQ = kOffAC + kMsACBytes;
+    static constexpr int kTx = kBChunk + kMsACBytes + kMsQBytes;
+    static constexpr int kTStageBytes = (kOffQ + kMsQBytes + 1023) / 1024 * 1024;
+    static constexpr int kTStages = F == kMsBf16x6 ? 3 : 4;
+    static constexpr int kGStageBytes = kParts * kMsABytes;
+    static constexpr int kGStages = F == kMsBf16x6 ? 2 : 3;
+    static constexpr int kOffGRing = kTStages * kTStageBytes;
+    static constexpr int kSmem = kOffGRing + kGStages * kGStageBytes + 1024;
+    static_assert(kSmem <= 232448 - 256, "shared memory per block");
+    static_assert(kTStages <= kMsMaxStages && kGStages <= kMsMaxStages, "barrier arrays");
+    static_assert(kMsACBytes % 16 == 0 && kMsQBytes % 16 == 0 && kTx % 16 == 0 && kBChunk % 1024 == 0 &&
+                      kGStageBytes % 1024 == 0,
+                  "bulk copies move 16-byte multiples; operand stages stay 1 KB aligned");
+};
 
 // byte offset of element (row, k) in a K-major tile of kMsKC = 32 bf16 per
 // row with the 64-byte swizzle: rows of 64 B in atoms of 8 rows (512 B); the
@@ -98,8 +129,6 @@ __host__ __device__ __forceinline__ uint32_t sw128_off(int row, int k) {
     const int r = row & 7;
     return (uint32_t)((row >> 3) * 1024 + r * 128 + ((((k >> 2) ^ r) & 7) << 4) + (k & 3) * 4);
 }
-
-enum : int { kMsBf16x3 = 0, kMsTf32 = 1 };
 
 // shared-memory matrix descriptor (tcgen05 format): start >> 4 in [0,14),
 // leading-byte offset in [16,30) (unused by swizzled K-major layouts: 1),
@@ -173,6 +202,18 @@ __device__ __forceinline__ void split2(float2 v, uint32_t& hi, uint32_t& lo) {
     lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
+// hi / mid / lo bf16 pairs of (re, im): 24 significant bits, so the three
+// parts add up to the FP32 value (each remainder is exact in FP32)
+__device__ __forceinline__ void split3(float2 v, uint32_t& hi, uint32_t& mid, uint32_t& lo) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+    const float rx = v.x - __low2float(h), ry = v.y - __high2float(h);
+    const __nv_bfloat162 m = __floats2bfloat162_rn(rx, ry);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(rx - __low2float(m), ry - __high2float(m));
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    mid = *reinterpret_cast<const uint32_t*>(&m);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
 __device__ __forceinline__ void sts128(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
     asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d)
                  : "memory");
@@ -193,9 +234,12 @@ __device__ __forceinline__ void sts128(uint32_t addr, uint32_t a, uint32_t b, ui
 // sincos / exp at the first, FP64 complex steps by e^{i k dr} after it.
 constexpr int kMsBRun = 8;
 
+// b64, when given, receives the same FP64 values as [o][M_pad] complex (the
+// guarded sum's fix-up reads them)
 template <int F>
-__device__ void ms_b_entry(long long id, int M, int n_chunks, const double* __restrict__ kr,
-                           const double* __restrict__ ki, double dr, int lossless, unsigned char* __restrict__ img) {
+__device__ void ms_b_entry(long long id, int M, int M_pad, int n_chunks, const double* __restrict__ kr,
+                           const double* __restrict__ ki, double dr, int lossless, unsigned char* __restrict__ img,
+                           double2* __restrict__ b64) {
     constexpr int kRuns = kMsNT / kMsBRun;
     const long long per_chunk = (long long)kRuns * kMsModes;
     if (id >= (long long)n_chunks * per_chunk) return;
@@ -217,12 +261,28 @@ __device__ void ms_b_entry(long long id, int M, int n_chunks, const double* __re
         sr = ad * cs;
         si = ad * sn;
     }
-    unsigned char* cimg = img + (size_t)chunk * 2 * kMsBBytes;  // 32 KB per chunk
+    unsigned char* cimg = img + (size_t)chunk * MsCfg<F>::kBChunk;
 #pragma unroll 1
     for (int u = 0; u < kMsBRun; ++u) {
         const int o = o0 + u;
         const float re = (float)cr, im = (float)ci;
-        if (F == kMsTf32) {
+        if (b64 && m < M) b64[(size_t)o * M_pad + m] = make_double2(cr, ci);
+        if (F == kMsBf16x6) {
+            // three bf16 parts of the FP64 value: hi, then the remainders
+            const __nv_bfloat16 hr = __double2bfloat16(cr), hm = __double2bfloat16(ci);
+            const double rr = cr - (double)__bfloat162float(hr), ri = ci - (double)__bfloat162float(hm);
+            const __nv_bfloat16 mr = __double2bfloat16(rr), mi = __double2bfloat16(ri);
+            const __nv_bfloat16 lr = __double2bfloat16(rr - (double)__bfloat162float(mr));
+            const __nv_bfloat16 li = __double2bfloat16(ri - (double)__bfloat162float(mi));
+            __nv_bfloat16* bm = reinterpret_cast<__nv_bfloat16*>(cimg);
+            const size_t p0 = sw64_off(o, 2 * ml) / 2, p1 = sw64_off(o, 2 * ml + 1) / 2;
+            bm[p0] = hr;
+            bm[p1] = hm;
+            bm[kMsBBytes / 2 + p0] = mr;
+            bm[kMsBBytes / 2 + p1] = mi;
+            bm[kMsBBytes + p0] = lr;
+            bm[kMsBBytes + p1] = li;
+        } else if (F == kMsTf32) {
             *reinterpret_cast<uint32_t*>(cimg + sw128_off(o, 2 * ml)) = to_tf32(re);
             *reinterpret_cast<uint32_t*>(cimg + sw128_off(o, 2 * ml + 1)) = to_tf32(im);
         } else {
@@ -244,12 +304,15 @@ __device__ void ms_b_entry(long long id, int M, int n_chunks, const double* __re
 
 // tile phases e^{i k_m r_n0}, r_n0 = (tile * 256 + 1) dr: the phase k r is
 // reduced mod 2 pi in FP64 before the sine / cosine and the cast to FP32
+// (tp64, when given, receives them in FP64, [tile][M_pad])
 __device__ void ms_phase_entry(long long id, int M, int M_pad, int n_tiles, const double* __restrict__ kr,
-                               const double* __restrict__ ki, double dr, int lossless, float2* __restrict__ q) {
+                               const double* __restrict__ ki, double dr, int lossless, float2* __restrict__ q,
+                               double2* __restrict__ tp64) {
     if (id >= (long long)n_tiles * M_pad) return;
     const int m = (int)(id % M_pad), tile = (int)(id / M_pad);
     if (m >= M) {
         q[id] = make_float2(0.f, 0.f);
+        if (tp64) tp64[id] = make_double2(0.0, 0.0);
         return;
     }
     const double r = ((double)tile * kMsNT + 1.0) * dr;
@@ -261,15 +324,18 @@ __device__ void ms_phase_entry(long long id, int M, int M_pad, int n_tiles, cons
     sincos(red, &sn, &cs);
     const double amp = exp(-b * r);
     q[id] = make_float2((float)(amp * cs), (float)(amp * sn));
+    if (tp64) tp64[id] = make_double2(amp * cs, amp * sn);
 }
 
 // A_jm = v_m(z_s) v_m(z_j) / sqrt(k_m) as complex FP32 for every receiver
 // group and K-chunk, [group][chunk][mode m in chunk][receiver j in group];
 // mode values at receiver j are row idx[j] of the full eigenvectors vfull
-// [z][mode], vs the source values; zero for padding modes and receivers
-__device__ void ms_a_entry(long long id, int n_rcv, int M, int n_chunks, const double* __restrict__ kr,
+// [z][mode], vs the source values; zero for padding modes and receivers.
+// a64, when given, receives A in FP64 as [receiver][M_pad] complex.
+__device__ void ms_a_entry(long long id, int n_rcv, int M, int M_pad, int n_chunks, const double* __restrict__ kr,
                            const double* __restrict__ ki, const double* __restrict__ vs, const int* __restrict__ idx,
-                           const double* __restrict__ vfull, int lossless, float2* __restrict__ ac) {
+                           const double* __restrict__ vfull, int lossless, float2* __restrict__ ac,
+                           double2* __restrict__ a64) {
     const int n_groups = (n_rcv + kMsRcv - 1) / kMsRcv;
     const long long per_chunk = (long long)kMsModes * kMsRcv;
     if (id >= (long long)n_groups * n_chunks * per_chunk) return;
@@ -285,27 +351,31 @@ __device__ void ms_a_entry(long long id, int n_rcv, int M, int n_chunks, const d
         const auto sk = csqrt_principal(a, b);
         const double den = sk.real() * sk.real() + sk.imag() * sk.imag();
         const double c = vs[m] * vfull[(size_t)idx[j] * M + m];
-        v = make_float2((float)(c * sk.real() / den), (float)(-c * sk.imag() / den));
+        const double are = c * sk.real() / den, aim = -c * sk.imag() / den;
+        v = make_float2((float)are, (float)aim);
+        if (a64) a64[(size_t)j * M_pad + m] = make_double2(are, aim);
     }
     ac[id] = v;
 }
 
 // the three preparations in one launch: blocks [0, b_b) fill the B' images,
 // [b_b, b_b + b_q) the tile phases, the rest A
+// (the FP64 tables b64, tp64, a64 are written only for the guarded sum)
 template <int F>
 __global__ void k_ms_prepare(long long b_b, long long b_q, int n_rcv, int M, int M_pad, int n_tiles, int n_chunks,
                              const double* __restrict__ kr, const double* __restrict__ ki,
                              const double* __restrict__ vs, const int* __restrict__ idx,
                              const double* __restrict__ vfull, double dr, int lossless,
-                             unsigned char* __restrict__ b_img, float2* __restrict__ q, float2* __restrict__ ac) {
+                             unsigned char* __restrict__ b_img, float2* __restrict__ q, float2* __restrict__ ac,
+                             double2* __restrict__ b64, double2* __restrict__ tp64, double2* __restrict__ a64) {
     const long long b = blockIdx.x;
     if (b < b_b) {
-        ms_b_entry<F>(b * blockDim.x + threadIdx.x, M, n_chunks, kr, ki, dr, lossless, b_img);
+        ms_b_entry<F>(b * blockDim.x + threadIdx.x, M, M_pad, n_chunks, kr, ki, dr, lossless, b_img, b64);
     } else if (b < b_b + b_q) {
-        ms_phase_entry((b - b_b) * blockDim.x + threadIdx.x, M, M_pad, n_tiles, kr, ki, dr, lossless, q);
+        ms_phase_entry((b - b_b) * blockDim.x + threadIdx.x, M, M_pad, n_tiles, kr, ki, dr, lossless, q, tp64);
     } else {
-        ms_a_entry((b - b_b - b_q) * blockDim.x + threadIdx.x, n_rcv, M, n_chunks, kr, ki, vs, idx, vfull, lossless,
-                   ac);
+        ms_a_entry((b - b_b - b_q) * blockDim.x + threadIdx.x, n_rcv, M, M_pad, n_chunks, kr, ki, vs, idx, vfull,
+                   lossless, ac, a64);
     }
 }
 
@@ -325,6 +395,7 @@ struct MsArgs {
     int M_pad, n_chunks, n_tiles, n_ranges, groups;
     long long n_units;           // groups * n_tiles * n_chunks
     float* raw;                  // [n_parts][groups][n_tiles][256 columns][128 rows] per-CTA partial tiles
+    float* s_part;               // guarded sum: [n_parts][groups][n_tiles][64 receivers][4] partial sums of |A'|
     unsigned* err;
 };
 
@@ -350,8 +421,11 @@ struct UnitPos {
 
 template <int F>
 __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
+    using C = MsCfg<F>;
+    constexpr int kTStages = C::kTStages, kGStages = C::kGStages;
     extern __shared__ unsigned char ms_dyn[];
-    __shared__ __align__(8) uint64_t full_t[kMsTStages], empty_t[kMsTStages], full_g[kMsGStages], empty_g[kMsGStages];
+    __shared__ __align__(8) uint64_t full_t[kMsMaxStages], empty_t[kMsMaxStages], full_g[kMsMaxStages],
+        empty_g[kMsMaxStages];
     __shared__ __align__(8) uint64_t acc_full[kMsAcc], acc_empty[kMsAcc], drain;
     __shared__ uint32_t tmem_base_sh;
     unsigned char* sm = (unsigned char*)(((uintptr_t)ms_dyn + 1023) & ~(uintptr_t)1023);
@@ -362,11 +436,11 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     const int nc = (int)(a.n_units * (blockIdx.x + 1) / gridDim.x - u0);
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kMsTStages; ++s) {
+        for (int s = 0; s < kTStages; ++s) {
             mbar_init(&full_t[s], 1);
             mbar_init(&empty_t[s], 1);
         }
-        for (int s = 0; s < kMsGStages; ++s) {
+        for (int s = 0; s < kGStages; ++s) {
             mbar_init(&full_g[s], kMsGenWarps);
             mbar_init(&empty_g[s], 1);
         }
@@ -391,30 +465,30 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
     if (warp == kMsProducerWarp) {
         if (lane == 0 && nc > 0) {
             // producer: bulk TMA of the B' image, A and tile phases of chunk c
-            // into TMA stage c % kMsTStages once the MMAs of chunk c - kMsTStages are done
+            // into TMA stage c % kTStages once the MMAs of chunk c - kTStages are done
             UnitPos pos;
             pos.init(u0, a.n_chunks, a.n_tiles);
             int issued = 0, landed = 0;
             bool ok = true;
             for (int c = 0; c < nc; ++c, pos.next(a.n_chunks, a.n_tiles)) {
-                const int slot = c % kMsTStages;
-                if (c >= kMsTStages) {
-                    ok = mbar_wait_bounded(&empty_t[slot], (uint32_t)(((c / kMsTStages) - 1) & 1), a.err);
+                const int slot = c % kTStages;
+                if (c >= kTStages) {
+                    ok = mbar_wait_bounded(&empty_t[slot], (uint32_t)(((c / kTStages) - 1) & 1), a.err);
                     if (!ok) break;
-                    landed = c - kMsTStages + 1;  // its copies were consumed, so they landed
+                    landed = c - kTStages + 1;  // its copies were consumed, so they landed
                 }
-                unsigned char* dst = sm + slot * kMsTStageBytes;
-                mbar_expect_tx(&full_t[slot], kMsTxBytes);
-                tma_load_1d(dst, a.b_img + (size_t)pos.chunk * 2 * kMsBBytes, 2 * kMsBBytes, &full_t[slot]);
-                tma_load_1d(dst + kMsOffAC, a.ac + ((size_t)pos.group * a.n_chunks + pos.chunk) * kMsModes * kMsRcv,
+                unsigned char* dst = sm + slot * C::kTStageBytes;
+                mbar_expect_tx(&full_t[slot], C::kTx);
+                tma_load_1d(dst, a.b_img + (size_t)pos.chunk * C::kBChunk, C::kBChunk, &full_t[slot]);
+                tma_load_1d(dst + C::kOffAC, a.ac + ((size_t)pos.group * a.n_chunks + pos.chunk) * kMsModes * kMsRcv,
                             kMsACBytes, &full_t[slot]);
-                tma_load_1d(dst + kMsOffQ, a.q + (size_t)pos.tile * a.M_pad + pos.chunk * kMsModes, kMsQBytes,
+                tma_load_1d(dst + C::kOffQ, a.q + (size_t)pos.tile * a.M_pad + pos.chunk * kMsModes, kMsQBytes,
                             &full_t[slot]);
                 ++issued;
             }
             // copies still in flight after an early exit: wait for them
             for (int c = landed; c < issued; ++c)
-                mbar_wait_drain(&full_t[c % kMsTStages], (uint32_t)((c / kMsTStages) & 1));
+                mbar_wait_drain(&full_t[c % kTStages], (uint32_t)((c / kTStages) & 1));
         }
     } else if (warp == 0) {
         if (lane == 0 && nc > 0) {
@@ -435,15 +509,15 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                         tc_fence_after();
                     }
                 }
-                const int stt = c % kMsTStages, sg_ = c % kMsGStages;
-                ok = mbar_wait_bounded(&full_t[stt], (uint32_t)((c / kMsTStages) & 1), a.err) &&
-                     mbar_wait_bounded(&full_g[sg_], (uint32_t)((c / kMsGStages) & 1), a.err);
+                const int stt = c % kTStages, sg_ = c % kGStages;
+                ok = mbar_wait_bounded(&full_t[stt], (uint32_t)((c / kTStages) & 1), a.err) &&
+                     mbar_wait_bounded(&full_g[sg_], (uint32_t)((c / kGStages) & 1), a.err);
                 if (!ok) break;
                 tc_fence_after();
                 // descriptors: the start-address field counts 16-byte units;
                 // A' from the generated ring, B' from the TMA stage
-                const uint64_t st = dsc0 + (uint64_t)((kMsOffGRing + sg_ * kMsGStageBytes) >> 4);
-                const uint64_t stb = dsc0 + (uint64_t)((stt * kMsTStageBytes) >> 4);
+                const uint64_t st = dsc0 + (uint64_t)((C::kOffGRing + sg_ * C::kGStageBytes) >> 4);
+                const uint64_t stb = dsc0 + (uint64_t)((stt * C::kTStageBytes) >> 4);
                 const uint32_t d = tmem + (uint32_t)((sg & 1) * kMsNT);
                 if (F == kMsTf32) {
                     // K = 8 tf32 (32 B) per MMA, four per chunk
@@ -452,6 +526,21 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                         const uint64_t ad = st + (uint64_t)(kk * 32 >> 4);
                         const uint64_t bd = stb + (uint64_t)(kk * 32 >> 4);
                         umma_tf32(d, ad, bd, (!first || kk > 0) ? 1u : 0u);
+                    }
+                } else if (F == kMsBf16x6) {
+                    // six products; the three smallest first
+#pragma unroll
+                    for (int kk = 0; kk < kMsKC / 16; ++kk) {
+                        const uint64_t ah = st + (uint64_t)(kk * 32 >> 4), am = ah + (uint64_t)(kMsABytes >> 4),
+                                       al = am + (uint64_t)(kMsABytes >> 4);
+                        const uint64_t bh = stb + (uint64_t)(kk * 32 >> 4), bm = bh + (uint64_t)(kMsBBytes >> 4),
+                                       bl = bm + (uint64_t)(kMsBBytes >> 4);
+                        umma_bf16(d, al, bh, (!first || kk > 0) ? 1u : 0u);
+                        umma_bf16(d, am, bm, 1u);
+                        umma_bf16(d, ah, bl, 1u);
+                        umma_bf16(d, am, bh, 1u);
+                        umma_bf16(d, ah, bm, 1u);
+                        umma_bf16(d, ah, bh, 1u);
                     }
                 } else {
 #pragma unroll
@@ -487,27 +576,47 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
         const int col_half = (warp - 1) >> 2;  // epilogue: accumulator columns [128 col_half, +128)
         bool ok = true;
         int sg = -1;
+        float s_abs = 0.f;  // guarded sum: sum of |A'| over this thread's modes of the segment
         UnitPos pos;
         pos.init(u0, a.n_chunks, a.n_tiles);
         for (int c = 0; c < nc && ok; ++c, pos.next(a.n_chunks, a.n_tiles)) {
             const bool first = c == 0 || pos.chunk == 0;
             const bool last = c == nc - 1 || pos.chunk == a.n_chunks - 1;
-            if (first) ++sg;
-            const int stt = c % kMsTStages, sgs = c % kMsGStages;
-            if (c >= kMsGStages) {  // A' stage free once the MMAs of chunk c - kMsGStages are done
-                ok = mbar_wait_bounded(&empty_g[sgs], (uint32_t)(((c / kMsGStages) - 1) & 1), a.err);
+            if (first) {
+                ++sg;
+                s_abs = 0.f;
+            }
+            const int stt = c % kTStages, sgs = c % kGStages;
+            if (c >= kGStages) {  // A' stage free once the MMAs of chunk c - kGStages are done
+                ok = mbar_wait_bounded(&empty_g[sgs], (uint32_t)(((c / kGStages) - 1) & 1), a.err);
                 if (!ok) break;
             }
-            ok = mbar_wait_bounded(&full_t[stt], (uint32_t)((c / kMsTStages) & 1), a.err);
+            ok = mbar_wait_bounded(&full_t[stt], (uint32_t)((c / kTStages) & 1), a.err);
             if (!ok) break;
-            const unsigned char* stg = sm + stt * kMsTStageBytes;
-            const float2* ac_s = reinterpret_cast<const float2*>(stg + kMsOffAC);
-            const float2* q_s = reinterpret_cast<const float2*>(stg + kMsOffQ);
+            const unsigned char* stg = sm + stt * C::kTStageBytes;
+            const float2* ac_s = reinterpret_cast<const float2*>(stg + C::kOffAC);
+            const float2* q_s = reinterpret_cast<const float2*>(stg + C::kOffQ);
             float2 e[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) e[v] = cmulf(ac_s[(4 * q4 + v) * kMsRcv + j], q_s[4 * q4 + v]);
-            const uint32_t gb = sm_addr + kMsOffGRing + sgs * kMsGStageBytes;
-            if (F == kMsTf32) {
+            const uint32_t gb = sm_addr + C::kOffGRing + sgs * C::kGStageBytes;
+            if (F == kMsBf16x6) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) s_abs += sqrtf(fmaf(e[v].x, e[v].x, e[v].y * e[v].y));
+                uint32_t hr[4], mr[4], lr[4], hm[4], mm[4], lm[4];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    split3(make_float2(e[v].x, -e[v].y), hr[v], mr[v], lr[v]);
+                    split3(make_float2(e[v].y, e[v].x), hm[v], mm[v], lm[v]);
+                }
+                const uint32_t o0 = sw64_off(j, 8 * q4), o1 = sw64_off(j + kMsRcv, 8 * q4);
+                sts128(gb + o0, hr[0], hr[1], hr[2], hr[3]);
+                sts128(gb + kMsABytes + o0, mr[0], mr[1], mr[2], mr[3]);
+                sts128(gb + 2 * kMsABytes + o0, lr[0], lr[1], lr[2], lr[3]);
+                sts128(gb + o1, hm[0], hm[1], hm[2], hm[3]);
+                sts128(gb + kMsABytes + o1, mm[0], mm[1], mm[2], mm[3]);
+                sts128(gb + 2 * kMsABytes + o1, lm[0], lm[1], lm[2], lm[3]);
+            } else if (F == kMsTf32) {
                 const uint32_t r0 = gb + sw128_off(j, 8 * q4), r1 = gb + sw128_off(j + kMsRcv, 8 * q4);
                 sts128(r0, to_tf32(e[0].x), to_tf32(-e[0].y), to_tf32(e[1].x), to_tf32(-e[1].y));
                 sts128(gb + sw128_off(j, 8 * q4 + 4), to_tf32(e[2].x), to_tf32(-e[2].y), to_tf32(e[3].x),
@@ -547,6 +656,9 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             const int row = 32 * (warp & 3) + lane;
             const long long gt = (long long)pos.group * a.n_tiles + pos.tile;
             const int part_slot = blockIdx.x - ms_cta_of(gt * a.n_chunks, a.n_units, gridDim.x);
+            if (F == kMsBf16x6 && a.s_part)
+                a.s_part[(((size_t)part_slot * a.groups + pos.group) * a.n_tiles + pos.tile) * (kMsRcv * 4) + j * 4 +
+                         q4] = s_abs;
             // partial tile stored column-major (the 128 rows of a column
             // contiguous), so each store instruction of the warp writes 128 B
             float* tcol = a.raw + (((size_t)part_slot * a.groups + pos.group) * a.n_tiles + pos.tile) * kMsNT * kMsRows +
@@ -592,12 +704,21 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
 // (cr + i ci) / sqrt(r).  Block = (group, tile, 32-column block): the columns
 // are read contiguously (128 rows each), transposed through shared memory
 // and written along the ranges.
+//
+// Guarded sum (s_part given): S_j = sum_m |A'_jm| over the tile (the sums the
+// generators left in s_part) bounds sum_m |A_jm e^{i k_m r}| for every range
+// of the tile, since |e^{i k r}| = e^{-Im k r} only falls with r.  A point
+// whose |D| < tau S_j could carry more than the allowed TL error; it is
+// appended to fix_list (receiver, range) for k_ms_fix.
 constexpr int kMsFinCols = 32;
 __global__ void __launch_bounds__(256) k_ms_finish(int n_rcv, int n_ranges, double dr, int groups, int n_tiles,
                                                    int n_chunks, long long n_units, int n_ctas, double cr, double ci,
                                                    const float* __restrict__ raw, double* __restrict__ re,
-                                                   double* __restrict__ im) {
+                                                   double* __restrict__ im, const float* __restrict__ s_part,
+                                                   double tau, int* __restrict__ fix_count,
+                                                   int2* __restrict__ fix_list) {
     __shared__ double sum[kMsFinCols][kMsRows + 1];
+    __shared__ double sbound[kMsRcv];
     __shared__ int parts_sh;
     const int cb = blockIdx.x % (kMsNT / kMsFinCols);
     const int gt = blockIdx.x / (kMsNT / kMsFinCols);
@@ -607,6 +728,16 @@ __global__ void __launch_bounds__(256) k_ms_finish(int n_rcv, int n_ranges, doub
         parts_sh = ms_cta_of(u_first + n_chunks - 1, n_units, n_ctas) - ms_cta_of(u_first, n_units, n_ctas) + 1;
     }
     __syncthreads();
+    const bool guard = s_part != nullptr;
+    if (guard && threadIdx.x < kMsRcv) {
+        double t = 0.0;
+        for (int p = 0; p < parts_sh; ++p) {
+            const float4 v = *reinterpret_cast<const float4*>(
+                s_part + (((size_t)p * groups + g) * n_tiles + tile) * (kMsRcv * 4) + threadIdx.x * 4);
+            t += (double)v.x + (double)v.y + (double)v.z + (double)v.w;
+        }
+        sbound[threadIdx.x] = t * tau;
+    }
     const int c0 = cb * kMsFinCols;  // first column inside the tile
     const int row = threadIdx.x & (kMsRows - 1), col0 = threadIdx.x >> 7;
     // every slot read was written in full (256 columns, padding included)
@@ -625,17 +756,76 @@ __global__ void __launch_bounds__(256) k_ms_finish(int n_rcv, int n_ranges, doub
 #pragma unroll
     for (int k = 0; k < kPer; ++k) sum[col0 + 2 * k][row] = acc[k];
     __syncthreads();
+    const int lane = threadIdx.x & 31;
     const int nl = threadIdx.x & (kMsFinCols - 1);
     const int n = tile * kMsNT + c0 + nl;
-    if (n >= n_ranges) return;
-    const double sr = 1.0 / sqrt((n + 1) * dr);
+    const bool valid = n < n_ranges;
+    const double sr = valid ? 1.0 / sqrt((n + 1) * dr) : 0.0;
     const double fr = cr * sr, fi = ci * sr;
     for (int jr = threadIdx.x >> 5; jr < kMsRcv; jr += 256 / kMsFinCols) {
-        if (g * kMsRcv + jr >= n_rcv) break;
+        const int j = g * kMsRcv + jr;
+        if (j >= n_rcv) break;  // the same for the whole warp
         const double dre = sum[nl][jr], dim = sum[nl][jr + kMsRcv];
-        const size_t o = (size_t)(g * kMsRcv + jr) * n_ranges + n;
-        re[o] = fr * dre - fi * dim;
-        im[o] = fr * dim + fi * dre;
+        bool flag = false;
+        if (valid) {
+            const size_t o = (size_t)j * n_ranges + n;
+            re[o] = fr * dre - fi * dim;
+            im[o] = fr * dim + fi * dre;
+            if (guard) {
+                const double b = sbound[jr];
+                flag = fma(dre, dre, dim * dim) < b * b;
+            }
+        }
+        if (guard) {
+            const unsigned bal = __ballot_sync(0xffffffffu, flag);
+            if (bal) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(fix_count, __popc(bal));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (flag) fix_list[base + __popc(bal & ((1u << lane) - 1u))] = make_int2(j, n);
+            }
+        }
+    }
+}
+
+// FP64 recomputation of the flagged points of the guarded sum, one warp per
+// point: P = C(r) sum_m A_jm e^{i k_m r_n} with e^{i k r_n} = (tile phase)
+// (offset phase), both FP64 tables of the preparation, the same
+// factorisation as the tensor-core sum (r_n = r_n0 + o dr).
+__global__ void __launch_bounds__(256) k_ms_fix(const int* __restrict__ fix_count, const int2* __restrict__ fix_list,
+                                                int M, int M_pad, int n_ranges, double dr, double cr, double ci,
+                                                const double2* __restrict__ a64, const double2* __restrict__ tp64,
+                                                const double2* __restrict__ b64, double* __restrict__ re,
+                                                double* __restrict__ im) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    const int cnt = *fix_count;
+    for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < cnt; w += warps) {
+        const int2 pt = fix_list[w];
+        const int j = pt.x, n = pt.y;
+        const int tile = n / kMsNT, o = n % kMsNT;
+        const double2* ar = a64 + (size_t)j * M_pad;
+        const double2* tr = tp64 + (size_t)tile * M_pad;
+        const double2* br = b64 + (size_t)o * M_pad;
+        double sre = 0.0, sim = 0.0;
+        for (int m = lane; m < M; m += 32) {
+            const double2 t = tr[m], b = br[m], av = ar[m];
+            const double er = fma(t.x, b.x, -t.y * b.y), ei = fma(t.x, b.y, t.y * b.x);
+            sre = fma(av.x, er, fma(-av.y, ei, sre));
+            sim = fma(av.x, ei, fma(av.y, er, sim));
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            sre += __shfl_xor_sync(0xffffffffu, sre, off);
+            sim += __shfl_xor_sync(0xffffffffu, sim, off);
+        }
+        if (lane == 0) {
+            const double sr = 1.0 / sqrt((n + 1) * dr);
+            const double fr = cr * sr, fi = ci * sr;
+            const size_t oo = (size_t)j * n_ranges + n;
+            re[oo] = fr * sre - fi * sim;
+            im[oo] = fr * sim + fi * sre;
+        }
     }
 }
 
@@ -668,9 +858,22 @@ MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms) {
     }
     p.a_img_bytes = (size_t)p.groups * p.n_chunks * kMsACBytes;  // A, complex FP32
     p.q_bytes = (size_t)p.n_tiles * p.M_pad * sizeof(float2);
-    p.tab_bytes = (size_t)p.n_chunks * 2 * kMsBBytes;              // B' images
+    p.tab_bytes = (size_t)p.n_chunks * MsCfg<kMsBf16x6>::kBChunk;  // B' images (room for three parts)
     p.raw_bytes = (size_t)p.n_parts * p.groups * p.n_tiles * kMsNT * kMsRows * sizeof(float);
+    // guarded sum
+    p.s_part_bytes = (size_t)p.n_parts * p.groups * p.n_tiles * kMsRcv * 4 * sizeof(float);
+    p.b64_bytes = (size_t)kMsNT * p.M_pad * 16;
+    p.tp64_bytes = (size_t)p.n_tiles * p.M_pad * 16;
+    p.a64_bytes = (size_t)n_rcv * p.M_pad * 16;
+    p.fix_list_bytes = (size_t)n_rcv * n_ranges * sizeof(int2);
     return p;
+}
+
+double ms_guard_tau() {
+    // |dTL| <= 0.05 dB needs |dP| <= d |P| with d = 1 - 10^(-0.05 / 20); with
+    // |dP| <= eps S, a point with |P_tc| >= eps S (1 + 1 / d) satisfies it
+    const double d = 1.0 - std::pow(10.0, -kMsGuardTlDb / 20.0);
+    return kMsGuardEps * (1.0 + 1.0 / d);
 }
 
 int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const double* vfull, double* vz) {
@@ -683,29 +886,32 @@ int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const do
 // a_img receives A (complex FP32), tab the B' images, q the tile phases
 int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int M, const double* kr,
                       const double* ki, const double* vs, const int* idx, const double* vfull, double dr, int lossless,
-                      void* a_img, void* q, void* tab) {
-    if (fmt != kMsBf16x3 && fmt != kMsTf32) return -1;
+                      void* a_img, void* q, void* tab, void* b64, void* tp64, void* a64) {
+    if (fmt != kMsBf16x3 && fmt != kMsTf32 && fmt != kMsBf16x6) return -1;
     const long long n_b = (long long)p.n_chunks * (kMsNT / kMsBRun) * kMsModes;
     const long long n_q = (long long)p.n_tiles * p.M_pad;
     const long long n_a = (long long)p.groups * p.n_chunks * kMsModes * kMsRcv;
     const long long b_b = (n_b + 255) / 256, b_q = (n_q + 255) / 256, b_a = (n_a + 255) / 256;
-    auto kern = fmt == kMsTf32 ? k_ms_prepare<kMsTf32> : k_ms_prepare<kMsBf16x3>;
+    auto kern = fmt == kMsTf32 ? k_ms_prepare<kMsTf32>
+                               : (fmt == kMsBf16x6 ? k_ms_prepare<kMsBf16x6> : k_ms_prepare<kMsBf16x3>);
     kern<<<(unsigned)(b_b + b_q + b_a), 256, 0, st>>>(b_b, b_q, n_rcv, M, p.M_pad, p.n_tiles, p.n_chunks, kr, ki, vs,
                                                      idx, vfull, dr, lossless, (unsigned char*)tab, (float2*)q,
-                                                     (float2*)a_img);
+                                                     (float2*)a_img, (double2*)b64, (double2*)tp64, (double2*)a64);
     return 1;
 }
 
 int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const void* a_img, const void* q,
-                 const void* tab, float* raw, unsigned* err) {
+                 const void* tab, float* raw, float* s_part, unsigned* err) {
     if (p.n_units <= 0) return 0;
-    if (fmt != kMsBf16x3 && fmt != kMsTf32) return -1;
-    auto kern = fmt == kMsTf32 ? k_ms_tc<kMsTf32> : k_ms_tc<kMsBf16x3>;
-    static bool attr_set[2][64] = {};
+    if (fmt != kMsBf16x3 && fmt != kMsTf32 && fmt != kMsBf16x6) return -1;
+    auto kern = fmt == kMsTf32 ? k_ms_tc<kMsTf32> : (fmt == kMsBf16x6 ? k_ms_tc<kMsBf16x6> : k_ms_tc<kMsBf16x3>);
+    const int smem = fmt == kMsTf32 ? MsCfg<kMsTf32>::kSmem
+                                    : (fmt == kMsBf16x6 ? MsCfg<kMsBf16x6>::kSmem : MsCfg<kMsBf16x3>::kSmem);
+    static bool attr_set[3][64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
     if (!attr_set[fmt][dev]) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMsSmem) != cudaSuccess)
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
             return -1;
         attr_set[fmt][dev] = true;  // setting it twice from two threads is harmless
     }
@@ -720,19 +926,38 @@ int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const 
     a.groups = p.groups;
     a.n_units = p.n_units;
     a.raw = raw;
+    a.s_part = fmt == kMsBf16x6 ? s_part : nullptr;
     a.err = err;
-    kern<<<p.n_ctas, kMsThreads, kMsSmem, st>>>(a);
+    kern<<<p.n_ctas, kMsThreads, smem, st>>>(a);
     return 1;
 }
 
-int launch_ms_finish(cudaStream_t st, const MsPlan& p, int n_rcv, int n_ranges, double dr, const float* raw,
-                     double* re, double* im) {
-    // 1000 * 4 pi i e^{-i pi/4} / sqrt(8 pi) = c0 (cos pi/4 + i sin pi/4)
+namespace {
+// 1000 * 4 pi i e^{-i pi/4} / sqrt(8 pi) = c0 (cos pi/4 + i sin pi/4)
+void ms_scale(double& cr, double& ci) {
     const double c0 = 1000.0 * 4 * kPi / std::sqrt(8.0 * kPi);
-    const double cr = c0 * std::sin(kPi * 0.25), ci = c0 * std::cos(kPi * 0.25);
+    cr = c0 * std::sin(kPi * 0.25);
+    ci = c0 * std::cos(kPi * 0.25);
+}
+}  // namespace
+
+int launch_ms_finish(cudaStream_t st, const MsPlan& p, int n_rcv, int n_ranges, double dr, const float* raw,
+                     double* re, double* im, const float* s_part, int* fix_count, void* fix_list) {
+    double cr, ci;
+    ms_scale(cr, ci);
     const unsigned blocks = (unsigned)(p.groups * p.n_tiles * (kMsNT / kMsFinCols));
     k_ms_finish<<<blocks, 256, 0, st>>>(n_rcv, n_ranges, dr, p.groups, p.n_tiles, p.n_chunks, p.n_units, p.n_ctas, cr,
-                                        ci, raw, re, im);
+                                        ci, raw, re, im, s_part, s_part ? ms_guard_tau() : 0.0, fix_count,
+                                        (int2*)fix_list);
+    return 1;
+}
+
+int launch_ms_fix(cudaStream_t st, int num_sms, int M, int M_pad, int n_ranges, double dr, const int* fix_count,
+                  const void* fix_list, const void* a64, const void* tp64, const void* b64, double* re, double* im) {
+    double cr, ci;
+    ms_scale(cr, ci);
+    k_ms_fix<<<2 * num_sms, 256, 0, st>>>(fix_count, (const int2*)fix_list, M, M_pad, n_ranges, dr, cr, ci,
+                                          (const double2*)a64, (const double2*)tp64, (const double2*)b64, re, im);
     return 1;
 }
 

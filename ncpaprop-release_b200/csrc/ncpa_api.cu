@@ -114,6 +114,8 @@ struct ncpa_ctx {
     std::map<int, DevBuf> twiddle; // per nfft
     DevBuf bb_out;                 // waveforms kept in HBM (NULL host buffer)
     DevBuf ms_img, ms_q, ms_tab, ms_raw, ms_vz, ms_idx, ms_re, ms_im;  // modal-sum scratch (grow-only)
+    DevBuf ms_spart, ms_b64, ms_tp64, ms_a64, ms_fix, ms_fixcnt;        // guarded sum: bounds, FP64 tables, flags
+    long long ms_last_points = 0;  // receivers x ranges of the last guarded modal sum
     int item_override = 0;         // eigenvalues per bisection item (0: chosen per solve); NCPA_BISECT_ITEM
     bool fuse_solve = true;        // fused bisection + eigenvector launch; NCPA_FUSE_SOLVE=0 turns it off
     // how long a consumer of the fused launch waits for an empty queue slot
@@ -1277,6 +1279,20 @@ ncpa_status ncpa_ctx_sturm_steps(ncpa_ctx* ctx, long long* steps) {
     });
 }
 
+ncpa_status ncpa_ctx_sum_fixups(ncpa_ctx* ctx, long long* recomputed, long long* points) {
+    if (!ctx || !recomputed || !points) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        int h = 0;
+        if (ctx->ms_fixcnt.p) {
+            CK(cudaMemcpyAsync(&h, ctx->ms_fixcnt.p, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+        *recomputed = h;
+        *points = ctx->ms_last_points;
+        return NCPA_OK;
+    });
+}
+
 ncpa_status ncpa_probe_fp64_peak(ncpa_ctx* ctx, double* tflops) {
     if (!ctx || !tflops) return NCPA_EINVAL;
     return guarded(ctx, [&]() -> ncpa_status {
@@ -1361,7 +1377,8 @@ ncpa_status ncpa_ctx_destroy(ncpa_ctx* ctx) {
     ctx->cke.release();
     ctx->d_err.release();
     for (DevBuf* b : {&ctx->ms_img, &ctx->ms_q, &ctx->ms_tab, &ctx->ms_raw, &ctx->ms_vz, &ctx->ms_idx, &ctx->ms_re,
-                      &ctx->ms_im})
+                      &ctx->ms_im, &ctx->ms_spart, &ctx->ms_b64, &ctx->ms_tp64, &ctx->ms_a64, &ctx->ms_fix,
+                      &ctx->ms_fixcnt})
         b->release();  // stream-ordered frees need the stream alive
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -1864,7 +1881,9 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
                           const ncpa_tl_params* tp, int method, double* re, double* im) {
     if (!ctx || !m || !tp || !rcv_height_m || n_rcv < 1 || problem < 0 || problem >= m->P) return NCPA_EINVAL;
     if ((re == nullptr) != (im == nullptr)) return NCPA_EINVAL;
-    if (method != NCPA_SUM_FP64 && method != NCPA_SUM_TC_BF16X3 && method != NCPA_SUM_TC_TF32) return NCPA_EINVAL;
+    if (method != NCPA_SUM_FP64 && method != NCPA_SUM_TC_BF16X3 && method != NCPA_SUM_TC_TF32 &&
+        method != NCPA_SUM_TC_GUARDED)
+        return NCPA_EINVAL;
     if (!m->prm.want_vectors) return fail(ctx, NCPA_EINVAL, "the modal sum at receivers needs want_vectors");
     return guarded(ctx, [&]() -> ncpa_status {
         if (tp->n_ranges < 1 || !(tp->dr_m > 0)) throw ApiError(NCPA_EINVAL, "bad range grid");
@@ -1913,17 +1932,42 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
                 ctx->ms_q.alloc(pl.q_bytes, st);
                 ctx->ms_tab.alloc(pl.tab_bytes, st);
                 ctx->ms_raw.alloc(pl.raw_bytes, st);
-                const int fmt = method == NCPA_SUM_TC_TF32 ? 1 : 0;
+                const bool guard = method == NCPA_SUM_TC_GUARDED;
+                const int fmt = method == NCPA_SUM_TC_TF32 ? 1 : (guard ? 2 : 0);
+                if (guard) {
+                    ctx->ms_spart.alloc(pl.s_part_bytes, st);
+                    ctx->ms_b64.alloc(pl.b64_bytes, st);
+                    ctx->ms_tp64.alloc(pl.tp64_bytes, st);
+                    ctx->ms_a64.alloc(pl.a64_bytes, st);
+                    ctx->ms_fix.alloc(pl.fix_list_bytes, st);
+                    ctx->ms_fixcnt.alloc(sizeof(int), st);
+                    CK(cudaMemsetAsync(ctx->ms_fixcnt.p, 0, sizeof(int), st));
+                    ctx->ms_last_points = (long long)n_rcv * nr;
+                }
                 check_launch(ctx, ncpa::launch_ms_prepare(st, pl, fmt, n_rcv, M, kr, ki, vs, ctx->ms_idx.as<int>(),
                                                           vfull, tp->dr_m, tp->lossless, ctx->ms_img.p, ctx->ms_q.p,
-                                                          ctx->ms_tab.p));
+                                                          ctx->ms_tab.p, guard ? ctx->ms_b64.p : nullptr,
+                                                          guard ? ctx->ms_tp64.p : nullptr,
+                                                          guard ? ctx->ms_a64.p : nullptr));
                 tm.mark("ms-prep");
                 check_launch(ctx, ncpa::launch_ms_tc(st, pl, fmt, nr, ctx->ms_img.p, ctx->ms_q.p, ctx->ms_tab.p,
-                                                     ctx->ms_raw.as<float>(), ctx->d_err.as<unsigned>()));
+                                                     ctx->ms_raw.as<float>(),
+                                                     guard ? ctx->ms_spart.as<float>() : nullptr,
+                                                     ctx->d_err.as<unsigned>()));
                 tm.mark("ms-tc");
                 check_launch(ctx, ncpa::launch_ms_finish(st, pl, n_rcv, nr, tp->dr_m, ctx->ms_raw.as<float>(),
-                                                         ctx->ms_re.as<double>(), ctx->ms_im.as<double>()));
+                                                         ctx->ms_re.as<double>(), ctx->ms_im.as<double>(),
+                                                         guard ? ctx->ms_spart.as<float>() : nullptr,
+                                                         guard ? ctx->ms_fixcnt.as<int>() : nullptr,
+                                                         guard ? ctx->ms_fix.p : nullptr));
                 tm.mark("ms-finish");
+                if (guard) {
+                    check_launch(ctx, ncpa::launch_ms_fix(st, ctx->num_sms, M, pl.M_pad, nr, tp->dr_m,
+                                                          ctx->ms_fixcnt.as<int>(), ctx->ms_fix.p, ctx->ms_a64.p,
+                                                          ctx->ms_tp64.p, ctx->ms_b64.p, ctx->ms_re.as<double>(),
+                                                          ctx->ms_im.as<double>()));
+                    tm.mark("ms-fix");
+                }
             }
         }
         if (re) {

@@ -33,7 +33,7 @@ EXPORTED = [
     "ncpa_server_submit", "ncpa_server_wait", "ncpa_server_release", "ncpa_server_stats_get", "ncpa_server_destroy", "ncpa_modes_get_all",
     "ncpa_ess_plan_create", "ncpa_ess_plan_run", "ncpa_ess_plan_modes", "ncpa_ess_plan_tl", "ncpa_ess_plan_tuning",
     "ncpa_ess_plan_destroy", "ncpa_profile_update", "ncpa_g2s_convert", "ncpa_profile_load_g2s",
-    "ncpa_dispersion_read", "ncpa_dispersion_desc_get", "ncpa_dispersion_destroy",
+    "ncpa_dispersion_read", "ncpa_dispersion_desc_get", "ncpa_dispersion_destroy", "ncpa_ctx_sum_fixups",
 ]
 
 
@@ -177,6 +177,7 @@ def lib():
         L.ncpa_ctx_phase_stats.argtypes = [_vp, ctypes.c_char_p, _dp, ctypes.POINTER(_c_ll)]
         L.ncpa_ctx_reset_stats.argtypes = [_vp]
         L.ncpa_ctx_sturm_steps.argtypes = [_vp, ctypes.POINTER(_c_ll)]
+        L.ncpa_ctx_sum_fixups.argtypes = [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]
         L.ncpa_probe_fp64_peak.argtypes = [_vp, _dp]
         L.ncpa_source_spectrum_builtin.argtypes = [_vp, _c_int, _dp, _c_int, _c_double, _c_int, _dp, _dp]
         _lib = L
@@ -259,6 +260,13 @@ class Context:
         a = _c_ll()
         self.check(lib().ncpa_ctx_sturm_steps(self.h, ctypes.byref(a)), "ncpa_ctx_sturm_steps")
         return a.value
+
+    def sum_fixups(self):
+        """(points recomputed in FP64, receivers x ranges) of the last guarded
+        tensor-core modal sum"""
+        a, b = _c_ll(), _c_ll()
+        self.check(lib().ncpa_ctx_sum_fixups(self.h, ctypes.byref(a), ctypes.byref(b)), "ncpa_ctx_sum_fixups")
+        return a.value, b.value
 
     def fp64_peak_tflops(self):
         t = _c_double()
@@ -488,7 +496,7 @@ class Modes:
                        "ncpa_tl_2d")
         return z, re, im
 
-    SUM_FP64, SUM_TC_BF16X3, SUM_TC_TF32 = 0, 1, 2
+    SUM_FP64, SUM_TC_BF16X3, SUM_TC_TF32, SUM_TC_GUARDED = 0, 1, 2, 3
 
     def tl_multi(self, p, heights_m, n_ranges, dr_m, method=1, lossless=False, to_host=True):
         """Modal sum at many receivers: complex P [n_rcv x n_ranges]."""

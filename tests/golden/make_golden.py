@@ -16,6 +16,14 @@ where the reference checkout is available) and writes compact copies:
                              V_s V_r at a few frequencies, of
                              samples/disp_256freqs_0p5hz_NCPA_canonic.dat and
                              docs/.../modbb_gp_files/code_outputs/myDispersionFile.dat
+  modbb_synthesis.npz        the ModBB pulse-propagation example of the manual
+                             (docs/.../modbb_gp_files/code_outputs, prop.sh):
+                             the whole myDispersionFile.dat (input), the
+                             source_spectrum.dat of the built-in pulse, the
+                             single-range waveform mywavf.dat (270 km) and the
+                             grid mywavf_grid.dat (220-300 km every 20 km),
+                             all with --max_celerity 320 and 16384-point
+                             transforms; time columns stored as (first, step)
 
 Usage: python tests/golden/make_golden.py <reference_root>
 """
@@ -72,6 +80,31 @@ def main():
         for j in pick:
             out["%s_modes_%d" % (key, j)] = rows[j][1]
     np.savez_compressed(os.path.join(OUT, "dispersion_goldens.npz"), **out)
+
+    # ModBB pulse propagation example
+    bo = os.path.join(REF, "docs", "ncpaprop_run_manual_TeX", "figs", "modbb_gp_files", "code_outputs")
+    rows = read_dispersion(os.path.join(bo, "myDispersionFile.dat"))
+    head = open(os.path.join(bo, "myDispersionFile.dat")).readline().split()
+    modes = np.concatenate([r[1] for r in rows])
+    spec = np.loadtxt(os.path.join(bo, "source_spectrum.dat"))
+    single = np.loadtxt(os.path.join(bo, "mywavf.dat"))
+    grid = np.loadtxt(os.path.join(bo, "mywavf_grid.dat"))
+
+    def regular(t):
+        step = (t[-1] - t[0]) / (len(t) - 1)
+        assert np.max(np.abs(t - (t[0] + step * np.arange(len(t))))) < 1e-5
+        return np.array([t[0], step])
+
+    g_r = np.unique(grid[:, 0])
+    g_amp = np.stack([grid[grid[:, 0] == r][:, 2] for r in g_r])
+    np.savez_compressed(
+        os.path.join(OUT, "modbb_synthesis.npz"),
+        disp_f=np.array([r[0] for r in rows]), disp_M=np.array([len(r[1]) for r in rows], dtype=np.int32),
+        disp_rho=np.array([float(head[2]), float(head[3])]), disp_modes=modes,
+        spec_f=spec[:, 0], spec_re=spec[:, 1], spec_im=spec[:, 2],
+        single_t=regular(single[:, 0]), single_re=single[:, 1].astype(np.float32),
+        single_im=single[:, 2].astype(np.float32),
+        grid_r_km=g_r, grid_t=regular(grid[grid[:, 0] == g_r[0]][:, 1]), grid_amp=g_amp.astype(np.float32))
 
 
 if __name__ == "__main__":

@@ -359,3 +359,39 @@ def test_modbb_propagation_with_dispersion_cache(binaries, modbb_dispersion, tmp
         outs.append(((d / "wave.dat").read_bytes(), p.stdout))
     assert outs[0][0] == outs[1][0] == outs[2][0]
     assert "dispersion cache" not in outs[1][1] and "dispersion cache" in outs[2][1]
+
+
+@pytest.mark.gpu
+def test_modbb_propagation_reference_example(binaries, tmp_path):
+    """ModBB --propagation on the reference's example dispersion file with the
+    built-in pulse, 220-300 km every 20 km, max_celerity 320, 16384-point
+    transform, against the shipped mywavf_grid.dat (older release: times
+    without t0, pulse scale 1.6191256 / 2, taper one bin lower -> ~5e-5)."""
+    z = np.load(os.path.join(ROOT, "tests", "golden", "modbb_synthesis.npz"))
+    disp = tmp_path / "myDispersionFile.dat"
+    md = z["disp_modes"]
+    rho_s, rho_r = z["disp_rho"]
+    with open(disp, "w") as f:
+        k = 0
+        for fr, m in zip(z["disp_f"], z["disp_M"]):
+            f.write("%.7e   %d    %.7e   %.7e" % (fr, m, rho_s, rho_r))
+            for row in md[k:k + m]:
+                f.write("   %.12e   %.12e   %.12e   %.12e" % tuple(row))
+            f.write("\n")
+            k += m
+    args = ["--propagation", "--input_dispersion_file", str(disp), "--output_waveform_file", "wave.dat",
+            "--receiver", "multiple", "--start_range_km", "220", "--end_range_km", "300", "--range_step_km", "20",
+            "--source", "pulse1", "--max_celerity", "320", "--nfft", "16384"]
+    run(binaries, "ModBB", args, tmp_path, check_rc=0)
+    blocks = (tmp_path / "wave.dat").read_text().strip("\n").split("\n\n")
+    assert len(blocks) == 5
+    for i, b in enumerate(blocks):
+        a = np.array([[float(x) for x in ln.split()] for ln in b.splitlines()])
+        assert a.shape == (16384, 3)
+        r_km = z["grid_r_km"][i]
+        assert np.allclose(a[:, 0], r_km)
+        t0 = r_km * 1e3 / 320.0
+        assert np.allclose(a[:, 1] - t0, z["grid_t"][0] + z["grid_t"][1] * np.arange(16384), atol=2e-6)
+        ref = z["grid_amp"][i].astype(float)
+        g = a[:, 2] * (1.6191256 / 2.0)
+        assert np.linalg.norm(g - ref) <= 1e-4 * np.linalg.norm(ref)

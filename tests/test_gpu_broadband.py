@@ -92,3 +92,44 @@ def test_device_resident_synthesis_matches_host_path(gpu, analytic_profile):
     assert _rel_l2(a, b) < 1e-12
     modes.close()
     prof.close()
+
+
+# ---------------------------------------------------------------------------
+# the reference's own pulse-propagation example (older release: see
+# test_oracle_synthesis_golden.py for the three measured differences)
+# ---------------------------------------------------------------------------
+def _manual():
+    import os
+
+    from oracle import oracle as O
+
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "modbb_synthesis.npz"))
+    off = np.concatenate([[0, 0], np.cumsum(z["disp_M"])]).astype(np.int32)
+    md = z["disp_modes"]
+    d = O.Dispersion(np.concatenate([[0.0], z["disp_f"]]), off, md[:, 0].copy(), md[:, 1].copy(), md[:, 2].copy(),
+                     md[:, 3].copy(), float(z["disp_rho"][0]), float(z["disp_rho"][1]))
+    return d, z
+
+
+OLD_SCALE = 1.6191256  # the older release's pulse1 amplitude relative to the current one
+
+
+def test_synthesis_vs_reference_example(gpu):
+    from oracle import oracle as O
+
+    d, z = _manual()
+    nfft, cel = 16384, 320.0
+    sre, sim = gpu.source_spectrum_builtin("pulse1", d.f, nfft)
+    ratio = (z["spec_re"] + 1j * z["spec_im"]) / (sre[1:] + 1j * sim[1:])
+    assert np.max(np.abs(ratio - OLD_SCALE)) <= 2e-6 * OLD_SCALE
+    ranges = np.concatenate([[270e3], z["grid_r_km"] * 1e3])
+    out = gpu.bb_synthesize(d.f, d.mode_off, d.re_k, d.im_k, d.ms, d.mr, d.rho_s, d.rho_r, ranges, cel, nfft, sre, sim)
+    refs = [z["single_re"]] + [z["grid_amp"][i] for i in range(len(z["grid_r_km"]))]
+    osre, osim = O.source_spectrum("pulse1", d.f, nfft)
+    for i, r in enumerate(ranges):
+        ref = refs[i].astype(float)
+        g = out[i] * (OLD_SCALE / 2.0)
+        # the current taper against the older release's: ~5e-5
+        assert _rel_l2(g, ref) < 1e-4, (r, _rel_l2(g, ref))
+        o = O.bb_pulse(d, osre, osim, *O.bb_transfer(d, r), r / cel, nfft)
+        assert _rel_l2(out[i], o) < 1e-9

@@ -8,7 +8,9 @@
   azimuths, solved in one mixed-grid batch with a 0.1 Hz, Nz = 5000 job;
 * the tall-atmosphere solve (2 Hz, 0-180 km, Nz = 100000, >1300 modes):
   counts, k, Im k, V_s V_r and the modal sum at 64 receivers (0-10 km) x 2000
-  ranges to 2000 km against the oracle's eigenvectors at those receivers.
+  ranges to 2000 km against the oracle's eigenvectors at those receivers, and
+  the guarded tensor-core sum on the benchmark's 64 x 20000-range grid (0.1 km
+  steps) at every point.
 
 Tolerances are those of the smaller parity tests: identical mode counts,
 |dk|/k <= max(1e-9, conditioning floor), Im k and V_s V_r within 1e-6
@@ -219,9 +221,23 @@ def test_tall_atmosphere_vs_oracle(gpu, workdir):
     mask = tl_o > -140
     assert mask.mean() > 0.5
     d = np.abs(tl_g - tl_o)[mask]
+    assert d.max() <= 0.05, d.max()
+    # the guarded tensor-core sum on the benchmark's grid: 64 receivers x
+    # 20000 ranges every 0.1 km, every point against the oracle's FP64 sum
+    nr2, dr2 = 20000, 100.0
+    ptc = m.tl_multi(0, h, nr2, dr2, method=m.SUM_TC_GUARDED)
+    fixed, points = gpu.sum_fixups()
     m.close()
     prof.close()
-    assert d.max() <= 0.05, d.max()
+    ore2, oim2 = np.empty((nr2, len(idx))), np.empty((nr2, len(idx)))
+    O.lib().orc_tl2d(o.M, O._p(O._f64(o.kr)), O._p(O._f64(o.ki)), O._p(O._f64(o.vs)), O._p(vz), len(idx), nr2, dr2, 0,
+                     O._p(ore2), O._p(oim2))
+    tl_o2 = _tl_db(ore2, oim2).T
+    mask2 = tl_o2 > -140
+    d2 = np.abs(_tl_db(ptc.real, ptc.imag) - tl_o2)[mask2]
+    assert d2.max() <= 0.05, d2.max()
     _record("tall_atmosphere", modes=int(o.M), k_rel_max=e[0], k_over_tol_max=e[1], im_k_over_tol_max=e[2],
             vsvr_over_tol_max=e[3], vsvr_rel_max_large_modes=e[4], tl_points=int(mask.sum()), tl_db_max=float(d.max()),
-            tl_db_median=float(np.median(d)))
+            tl_db_median=float(np.median(d)), guarded_points=int(mask2.sum()), guarded_tl_db_max=float(d2.max()),
+            guarded_tl_db_median=float(np.median(d2)), guarded_recomputed=int(fixed),
+            guarded_recomputed_frac=fixed / points)
