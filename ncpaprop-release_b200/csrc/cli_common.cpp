@@ -52,6 +52,20 @@ ncpa_profile* load_profile(ncpa_ctx* ctx, const std::string& atmosfile, const st
     return prof;
 }
 
+ncpa_profile* create_profile(ncpa_ctx* ctx, const ncpa_profile_desc* atm, const std::string& attn_file) {
+    ncpa_profile* prof = nullptr;
+    check(ctx, ncpa_profile_create(ctx, atm, &prof), "uploading the caller's atmospheric profile");
+    if (!attn_file.empty()) {
+        ncpa_status s = ncpa_profile_load_attn(prof, attn_file.c_str());
+        if (s != NCPA_OK) {
+            std::string msg = ncpa_last_error(ctx);
+            ncpa_profile_destroy(prof);
+            throw RunError("reading attenuation file " + attn_file + ": " + msg);
+        }
+    }
+    return prof;
+}
+
 std::string tag_filename(const std::string& tag, const std::string& name) {
     return tag.empty() ? name : tag + "." + name;
 }

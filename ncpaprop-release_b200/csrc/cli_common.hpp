@@ -33,6 +33,8 @@ private:
 };
 
 // profile file (+ optional header file and attenuation table file)
+// the caller's in-memory profile (plus an optional attenuation file)
+ncpa_profile* create_profile(ncpa_ctx* ctx, const ncpa_profile_desc* atm, const std::string& attn_file);
 ncpa_profile* load_profile(ncpa_ctx* ctx, const std::string& atmosfile, const std::string& headerfile,
                            const std::string& attn_file);
 

@@ -16,62 +16,6 @@ using ncpa_cli::Params;
 
 namespace {
 
-void configure(Params& ps) {
-    ps.add_flag("help");
-    ps.add_flag("h");
-    ps.add_string("paramfile", "modess.param");
-    ps.add_flag("printparams");
-    ps.add_string_nodefault("atmosfile");
-    ps.require("atmosfile");
-    ps.add_float_nodefault("freq");
-    ps.require("freq");
-    ps.float_gt("freq", 0.0);
-    ps.add_string("atmosheaderfile", "");
-    ps.add_float("maxheight_km", 150.0);
-    ps.float_ge("maxheight_km", 0.1);
-    ps.add_float("zground_km", 0.0);
-    ps.add_int("Nz_grid", 20000);
-    ps.int_ge("Nz_grid", 10);
-    ps.add_float("sourceheight_km", 0.0);
-    ps.add_float("receiverheight_km", 0.0);
-    ps.add_float("maxrange_km", 1000.0);
-    ps.float_ge("maxrange_km", 0.01);
-    ps.add_int("Nrng_steps", 1000);
-    ps.int_gt("Nrng_steps", 0);
-    ps.add_string("ground_impedence_model", "rigid");
-    ps.string_set("ground_impedence_model", {"rigid"});
-    ps.add_string("use_attn_file", "");
-    ps.add_string("modal_starter_file", "");
-    ps.add_string("dispersion_file", "");
-    ps.add_flag("append_dispersion_file");
-    ps.add_string("filetag", "");
-    ps.add_flag("singleprop");
-    ps.add_flag("multiprop");
-    ps.radio("operation_mode", {"singleprop", "multiprop"});
-    ps.add_float_nodefault("azimuth");
-    ps.float_ge("azimuth", 0.0);
-    ps.float_lt("azimuth", 360.0);
-    ps.require_if("azimuth", "singleprop");
-    for (const char* k : {"azimuth_start", "azimuth_end", "azimuth_step"}) {
-        ps.add_float_nodefault(k);
-        ps.float_ge(k, 0.0);
-        ps.float_le(k, 360.0);
-        ps.require_if(k, "multiprop");
-    }
-    for (const char* k : {"write_2d_tloss", "write_lossless", "write_phase_speeds", "write_speeds", "write_modes",
-                          "write_atm_profile", "Lamb_wave_BC", "turnoff_WKB", "wvnum_filter"})
-        ps.add_flag(k);
-    for (const char* k : {"c_min", "c_max"}) {
-        ps.add_float_nodefault(k);
-        ps.float_gt(k, 0.0);
-        ps.require_if(k, "wvnum_filter");
-    }
-    ps.add_flag("broadband");
-    ps.add_float("f_min", 0.0);
-    ps.add_float("f_max", 0.0);
-    ps.add_float("f_step", 0.0);
-}
-
 void usage(std::ostream& os) {
     os << "Modess -- effective sound speed normal modes (GPU)\n\n"
           "Options (command line \"--key value\" or a \"key: value\" line in the parameter file\n"
@@ -96,7 +40,7 @@ void usage(std::ostream& os) {
 
 int main(int argc, char** argv) {
     Params param;
-    configure(param);
+    ncpa_cli::configure_modess(param);
     try {
         param.parse_command_line(argc, argv);
         if (param.found("help") || param.found("h")) {

@@ -2,19 +2,113 @@
 #include "solvers.hpp"
 
 #include <cstdio>
+#include <stdexcept>
 
 #include "cli_bb.hpp"
 #include "cli_ess.hpp"
 
 namespace ncpa_gpu_solvers {
 
+Atmosphere1D::Atmosphere1D(const std::string& file, const std::string& header)
+    : s_(ncpa::to_si_profile(ncpa::read_profile(file, header))) {}
+
+Atmosphere1D::Atmosphere1D(std::vector<double> z, std::vector<double> u, std::vector<double> v,
+                           std::vector<double> t, std::vector<double> p, std::vector<double> rho) {
+    const size_t n = z.size();
+    if (n < 3 || u.size() != n || v.size() != n || t.size() != n || p.size() != n || rho.size() != n)
+        throw std::invalid_argument("Atmosphere1D: need at least 3 knots and arrays of equal length");
+    s_.z = std::move(z);
+    s_.u = std::move(u);
+    s_.v = std::move(v);
+    s_.t = std::move(t);
+    s_.p = std::move(p);
+    s_.rho = std::move(rho);
+}
+
+bool Atmosphere1D::contains(const std::string& key) const {
+    return key == "Z" || key == "U" || key == "V" || key == "T" || key == "P" || key == "RHO" ||
+           (key == "C0" && s_.has_c0);
+}
+
+const std::vector<double>& Atmosphere1D::get(const std::string& key) const {
+    if (key == "Z") return s_.z;
+    if (key == "U") return s_.u;
+    if (key == "V") return s_.v;
+    if (key == "T") return s_.t;
+    if (key == "P") return s_.p;
+    if (key == "RHO") return s_.rho;
+    if (key == "C0" && s_.has_c0) return s_.c0;
+    throw std::out_of_range("Atmosphere1D: no property " + key);
+}
+
+std::vector<double>& Atmosphere1D::get(const std::string& key) {
+    return const_cast<std::vector<double>&>(static_cast<const Atmosphere1D*>(this)->get(key));
+}
+
+void Atmosphere1D::set_z0(double z0_m) {
+    s_.z0 = z0_m;
+    s_.has_z0 = true;
+}
+
+ncpa_profile_desc Atmosphere1D::desc() const {
+    const size_t n = s_.z.size();
+    for (const auto* a : {&s_.u, &s_.v, &s_.t, &s_.p, &s_.rho})
+        if (a->size() != n) throw std::invalid_argument("Atmosphere1D: property arrays changed length");
+    if (s_.has_c0 && s_.c0.size() != n) throw std::invalid_argument("Atmosphere1D: property arrays changed length");
+    ncpa_profile_desc d{};
+    d.n_knots = (int)n;
+    d.z = s_.z.data();
+    d.u = s_.u.data();
+    d.v = s_.v.data();
+    d.t = s_.t.data();
+    d.p = s_.p.data();
+    d.rho = s_.rho.data();
+    d.c0 = s_.has_c0 ? s_.c0.data() : nullptr;
+    d.attn = nullptr;
+    d.z0_m = s_.z0;
+    d.has_z0 = s_.has_z0;
+    return d;
+}
+
+void Atmosphere1D::write(const std::string& path) const {
+    ncpa::ParsedProfile pp;
+    pp.z = s_.z;
+    pp.z_units = "m";
+    std::vector<std::string> keys = {"U", "V", "T", "P", "RHO"};
+    const char* units[] = {"m/s", "m/s", "K", "Pa", "kg/m3"};
+    for (size_t i = 0; i < keys.size(); ++i) {
+        pp.vectors[keys[i]] = get(keys[i]);
+        pp.vector_units[keys[i]] = units[i];
+    }
+    if (s_.has_c0) {
+        keys.push_back("C0");
+        pp.vectors["C0"] = s_.c0;
+        pp.vector_units["C0"] = "m/s";
+    }
+    if (s_.has_z0) {
+        pp.scalars["Z0"] = s_.z0;
+        pp.scalar_units["Z0"] = "m";
+    }
+    ncpa::write_ncpa_profile(pp, keys, path);
+}
+
 int ESSModeSolver::solve() {
-    ncpa_cli::run_ess(param_, false);
+    if (atm_) {
+        const ncpa_profile_desc d = atm_->desc();
+        ncpa_cli::run_ess(param_, false, &d);
+    } else {
+        ncpa_cli::run_ess(param_, false);
+    }
     return 0;
 }
 
 int WModeSolver::solve() {
-    ncpa_cli::run_ess(param_, true);
+    if (atm_) {
+        const ncpa_profile_desc d = atm_->desc();
+        ncpa_cli::run_ess(param_, true, &d);
+    } else {
+        ncpa_cli::run_ess(param_, true);
+    }
     return 0;
 }
 

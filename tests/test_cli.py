@@ -395,3 +395,24 @@ def test_modbb_propagation_reference_example(binaries, tmp_path):
         ref = z["grid_amp"][i].astype(float)
         g = a[:, 2] * (1.6191256 / 2.0)
         assert np.linalg.norm(g - ref) <= 1e-4 * np.linalg.norm(ref)
+
+
+@pytest.mark.gpu
+def test_solver_class_takes_the_callers_atmosphere(binaries, canonical_profile, tmp_path):
+    """ESSModeSolver(Params*, Atmosphere1D*) -- the reference's
+    ESSModeSolver(ParameterSet*, Atmosphere1D*) (ESSModeSolver.h:53-80): a
+    profile changed in memory gives the same files as the same profile
+    written out and read back, and not those of the unchanged profile."""
+    obj = os.path.join(PKG, "_obj")
+    exe = str(tmp_path / "solver_atmosphere")
+    cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(PKG, "csrc"),
+           os.path.join(ROOT, "tests", "cpp", "solver_atmosphere.cpp")]
+    cmd += [os.path.join(obj, o) for o in ("cli_params.o", "cli_common.o", "cli_ess.o", "cli_bb.o", "solvers.o")]
+    cmd += ["-L" + os.path.join(PKG, "lib"), "-lncpa_gpu", "-Wl,-rpath," + os.path.join(PKG, "lib"), "-o", exe]
+    subprocess.run(cmd, check=True)
+    p = subprocess.run([exe, canonical_profile, str(tmp_path)], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout + p.stderr
+    for name in ("tloss_1d.nm", "tloss_2d.nm"):
+        mem = (tmp_path / ("mem." + name)).read_bytes()
+        assert mem == (tmp_path / ("file." + name)).read_bytes(), name
+        assert mem != (tmp_path / ("orig." + name)).read_bytes(), name
