@@ -191,6 +191,19 @@ typedef struct {
  * three as NULL to keep the result in HBM (owned by the modes object) */
 ncpa_status ncpa_tl_1d(ncpa_ctx *ctx, const ncpa_modes *modes, const ncpa_tl_params *tp,
                        double *re, double *im, double *incoh);
+/* 1-D TL of problems first .. first + count - 1 only; re/im/incoh are
+ * [count x n_ranges] host arrays (ModeSolver::getTLoss1D, ModeSolver.cpp:
+ * 292-381, for a slice of a batch: each served request its own range grid) */
+ncpa_status ncpa_tl_1d_range(ncpa_ctx *ctx, const ncpa_modes *modes, int first, int count,
+                             const ncpa_tl_params *tp, double *re, double *im, double *incoh);
+/* A modes object from host arrays (no counterpart in the reference): n
+ * problems with CSR offsets mode_off[n + 1] (mode_off[0] = 0) into k = re_k +
+ * i im_k and the mode values at the source and receiver.  The arrays are
+ * uploaded and stay in HBM with the object; it serves ncpa_tl_1d /
+ * ncpa_tl_1d_range / ncpa_modes_get / ncpa_modes_get_all (no grid, vectors
+ * or group speeds: ncpa_modes_info reports zeros and unit densities). */
+ncpa_status ncpa_modes_from_host(ncpa_ctx *ctx, int n_problems, const int *mode_off, const double *re_k,
+                                 const double *im_k, const double *v_src, const double *v_rcv, ncpa_modes **out);
 /* one problem on the reference's height sampling (every nz/500-th grid
  * point); heights [m] in z_out (n_heights entries), re/im [n_ranges x n_heights] */
 ncpa_status ncpa_tl_2d_heights(const ncpa_modes *modes, int problem, int *n_heights);
@@ -308,13 +321,20 @@ typedef struct ncpa_server ncpa_server;
 typedef struct {
     int device;
     ncpa_ess_params params;  /* shared by every request (grid, heights, flags) */
-    int n_ranges;            /* 1-D TL range grid of every request: (i+1)*dr_m */
+    int n_ranges;            /* default 1-D TL range grid of a request: (i+1)*dr_m */
     double dr_m;
     int lanes;               /* batches in flight at once; 0 -> 2 */
     int max_batch_problems;  /* problems merged into one solve; 0 -> 1024 */
     double hbm_budget_bytes; /* admission limit on in-flight requests' estimated
-                                device footprint; 0 -> 8 GiB.  One request is
-                                always admitted when nothing else runs. */
+                                device footprint plus the mode cache; 0 -> 8 GiB.
+                                One request is always admitted when nothing else
+                                runs. */
+    double cache_bytes;      /* device-resident mode cache (0: none).  A request
+                                whose profile (knot values), frequencies and
+                                azimuth match a solved one skips the eigen-solve:
+                                its modes stay in HBM, keyed by a hash of the
+                                profile, the frequencies and the azimuth; least
+                                recently used entries are evicted. */
 } ncpa_server_opts;
 
 typedef struct {
@@ -322,6 +342,14 @@ typedef struct {
     const double *freqs;
     int n_freq;
     double az_deg;
+    int n_ranges;              /* this request's 1-D TL grid (i+1)*dr_m; 0 -> the server's */
+    double dr_m;
+    int n_wave_ranges;         /* > 0: pulse waveforms at wave_ranges_m (broadband
+                                  requests; frequencies k df, k = 1..n_freq) */
+    const double *wave_ranges_m;
+    double max_celerity;       /* t0 = r / max_celerity; 0 -> 340 m/s */
+    int nfft;                  /* 0 -> the NFFT rule: 4 (n_freq + 1) */
+    int source;                /* built-in source spectrum: 0 impulse, 1 pulse1, 2 pulse2 */
 } ncpa_request;
 
 typedef struct {
@@ -332,6 +360,11 @@ typedef struct {
     const double *tl_re, *tl_im, *tl_incoh; /* [n_freq x n_ranges] */
     double latency_ms;         /* submit -> results ready */
     int batch_requests;        /* requests in the batch it was solved in */
+    int n_ranges;              /* the TL grid's length */
+    int n_wave_ranges, nfft;
+    const double *waveforms;   /* [n_wave_ranges x nfft] (ncpa_bb_synthesize's
+                                  layout), NULL without waveforms */
+    int from_cache;            /* 1: modes from the cache, no eigen-solve */
 } ncpa_result;
 
 typedef struct {
@@ -339,6 +372,8 @@ typedef struct {
     double mean_batch_requests;
     double p50_ms, p99_ms, max_ms; /* latency over completed requests */
     double peak_admitted_bytes;
+    long long cache_hits, cache_entries;
+    double cache_used_bytes;
 } ncpa_server_stats;
 
 void ncpa_server_opts_default(ncpa_server_opts *opts);

@@ -220,6 +220,61 @@ struct SturmState {
             d1 *= sc;
         }
     }
+    // 32 steps carrying the first and second x-derivatives:
+    // e_i = (s_i - x) e_{i-1} - (2 d_{i-1} + e_{i-2}), rescaled with p
+    __device__ __forceinline__ void word32_deriv2(const double* __restrict__ s, double x, double& d0, double& d1,
+                                                  double& e0, double& e1) {
+        unsigned w = 0u;
+#pragma unroll
+        for (int u = 0; u < 32; u += 2) {
+            double2 sv = *reinterpret_cast<const double2*>(s + u);
+            double a0 = sv.x - x;
+            double q0 = fma(a0, p1, -p0);
+            double f0 = fma(a0, d1, -(p1 + d0));
+            double g0 = fma(a0, e1, -fma(2.0, d1, e0));
+            double a1 = sv.y - x;
+            double q1 = fma(a1, q0, -p1);
+            double f1 = fma(a1, f0, -(q0 + d1));
+            double g1 = fma(a1, g0, -fma(2.0, f0, e1));
+            w = __funnelshift_l(__double2hiint(q0), w, 1);
+            w = __funnelshift_l(__double2hiint(q1), w, 1);
+            p0 = q0;
+            p1 = q1;
+            d0 = f0;
+            d1 = f1;
+            e0 = g0;
+            e1 = g1;
+        }
+        unsigned prev = (w >> 1) | (prevbit << 31);
+        cnt += __popc(w ^ prev);
+        prevbit = w & 1u;
+        int sh = rescale_shift(fmax(fmax(fabs(p0), fabs(d0)), fabs(e0)), fmax(fmax(fabs(p1), fabs(d1)), fabs(e1)));
+        if (sh) {
+            double sc = pow2(-sh);
+            p0 *= sc;
+            p1 *= sc;
+            d0 *= sc;
+            d1 *= sc;
+            e0 *= sc;
+            e1 *= sc;
+        }
+    }
+    __device__ __forceinline__ void step_deriv2(double si, double x, double& d0, double& d1, double& e0,
+                                                double& e1) {
+        double a = si - x;
+        double q = fma(a, p1, -p0);
+        double f = fma(a, d1, -(p1 + d0));
+        double g = fma(a, e1, -fma(2.0, d1, e0));
+        unsigned b = static_cast<unsigned>(__double2hiint(q)) >> 31;
+        cnt += static_cast<int>(b ^ prevbit);
+        prevbit = b;
+        p0 = p1;
+        p1 = q;
+        d0 = d1;
+        d1 = f;
+        e0 = e1;
+        e1 = g;
+    }
     __device__ __forceinline__ void step_deriv(double si, double x, double& d0, double& d1) {
         double a = si - x;
         double q = fma(a, p1, -p0);
@@ -271,6 +326,24 @@ __device__ __forceinline__ void sturm_fold_deriv(SturmState& S, unsigned w, doub
         S.p1 *= sc;
         d0 *= sc;
         d1 *= sc;
+    }
+}
+
+// the same with the second-derivative chain (e0, e1) rescaled alongside
+__device__ __forceinline__ void sturm_fold_deriv2(SturmState& S, unsigned w, double& d0, double& d1, double& e0,
+                                                  double& e1) {
+    const unsigned prev = (w >> 1) | (S.prevbit << 31);
+    S.cnt += __popc(w ^ prev);
+    S.prevbit = w & 1u;
+    const int sh = rescale_shift(fmax(fmax(fabs(S.p0), fabs(d0)), fabs(e0)), fmax(fmax(fabs(S.p1), fabs(d1)), fabs(e1)));
+    if (sh) {
+        const double sc = pow2(-sh);
+        S.p0 *= sc;
+        S.p1 *= sc;
+        d0 *= sc;
+        d1 *= sc;
+        e0 *= sc;
+        e1 *= sc;
     }
 }
 
@@ -351,6 +424,59 @@ __device__ __forceinline__ void sturm_word32_deriv_pair(SturmState& A, double& d
     sturm_fold(B, wb);
 }
 
+// chain A with first and second derivatives, chain B counts only
+__device__ __forceinline__ void sturm_word32_deriv2_pair(SturmState& A, double& d0, double& d1, double& e0,
+                                                         double& e1, SturmState& B, const double* __restrict__ s,
+                                                         double xa, double xb) {
+    unsigned wa = 0u, wb = 0u;
+    double pa0 = A.p0, pa1 = A.p1, pb0 = B.p0, pb1 = B.p1;
+#pragma unroll
+    for (int u = 0; u < 32; u += 2) {
+        const double2 sv = *reinterpret_cast<const double2*>(s + u);
+        const double a0 = sv.x - xa, a1 = sv.y - xa;
+        const double qa0 = fma(a0, pa1, -pa0);
+        const double qb0 = fma(sv.x - xb, pb1, -pb0);
+        const double f0 = fma(a0, d1, -(pa1 + d0));
+        const double g0 = fma(a0, e1, -fma(2.0, d1, e0));
+        const double qa1 = fma(a1, qa0, -pa1);
+        const double qb1 = fma(sv.y - xb, qb0, -pb1);
+        const double f1 = fma(a1, f0, -(qa0 + d1));
+        const double g1 = fma(a1, g0, -fma(2.0, f0, e1));
+        wa = __funnelshift_l(__double2hiint(qa0), wa, 1);
+        wb = __funnelshift_l(__double2hiint(qb0), wb, 1);
+        wa = __funnelshift_l(__double2hiint(qa1), wa, 1);
+        wb = __funnelshift_l(__double2hiint(qb1), wb, 1);
+        pa0 = qa0;
+        pa1 = qa1;
+        pb0 = qb0;
+        pb1 = qb1;
+        d0 = f0;
+        d1 = f1;
+        e0 = g0;
+        e1 = g1;
+    }
+    A.p0 = pa0;
+    A.p1 = pa1;
+    B.p0 = pb0;
+    B.p1 = pb1;
+    sturm_fold_deriv2(A, wa, d0, d1, e0, e1);
+    sturm_fold(B, wb);
+}
+
+// One Laguerre step for the degree-n polynomial det(T - x), all of whose
+// roots are real, from g = det'/det and h = g^2 - det''/det (Laguerre's method;
+// e.g. Li & Zeng, SIAM J. Sci. Comput. 15 (1994), for symmetric tridiagonal
+// matrices): x_new = x - n / (g +- sqrt((n - 1)(n h - g^2))).  The two signs
+// step to the nearest root above and below x; up selects the root above.
+// Returns the correction subtracted from x (not finite when g and h are not).
+__device__ __forceinline__ double laguerre_step(double g, double h, double n, bool up) {
+    const double disc = fmax((n - 1.0) * fma(n, h, -g * g), 0.0);
+    const double sq = sqrt(disc);
+    const double dp = n / (g + sq), dm = n / (g - sq);
+    // x - dp and x - dm: the one above x has the negative correction
+    return up ? (dp < 0.0 ? dp : dm) : (dp > 0.0 ? dp : dm);
+}
+
 // ---------------------------------------------------------------------------
 // Row formats of the scaled tridiagonal matrices (unit off-diagonal) that the
 // eigenvector kernel streams, and the diagonal entry t_i at a shift.
@@ -366,6 +492,9 @@ __device__ __forceinline__ void sturm_word32_deriv_pair(SturmState& A, double& d
 struct EssRows {
     static constexpr int kW = 1;  // doubles per row
     static constexpr bool kTwist = true;  // bisection sweeps as twisted counts (measured faster)
+    // det(S - x) has only real roots (S symmetric): Laguerre steps, which
+    // need the second derivative chain as well
+    static constexpr bool kLaguerre = true;
     struct Shift {
         double x;
     };
@@ -399,6 +528,19 @@ struct EssRows {
                                                       double& d0, double& d1) {
         A.step_deriv(b[i], x, d0, d1);
     }
+    __device__ static __forceinline__ void deriv2_pair(SturmState& A, double& d0, double& d1, double& e0,
+                                                       double& e1, SturmState& B, const double* __restrict__ b,
+                                                       double xa, double xb) {
+        sturm_word32_deriv2_pair(A, d0, d1, e0, e1, B, b, xa, xb);
+    }
+    __device__ static __forceinline__ void word_deriv2(SturmState& A, const double* __restrict__ b, double x,
+                                                       double& d0, double& d1, double& e0, double& e1) {
+        A.word32_deriv2(b, x, d0, d1, e0, e1);
+    }
+    __device__ static __forceinline__ void step_deriv2(SturmState& A, const double* __restrict__ b, int i,
+                                                       double x, double& d0, double& d1, double& e0, double& e1) {
+        A.step_deriv2(b[i], x, d0, d1, e0, e1);
+    }
     // Newton correction (subtracted from x) from the last p and its derivative chain
     __device__ static __forceinline__ double newton(double p, double d) { return p / d; }
 };
@@ -406,6 +548,8 @@ struct EssRows {
 struct WmodRows {
     static constexpr int kW = 2;
     static constexpr bool kTwist = false;  // twisted sweeps measured 6 % slower here (register spills)
+    // det T(kappa) also has non-real roots: Newton steps
+    static constexpr bool kLaguerre = false;
     struct Shift {
         double kap, c;  // kappa and -(kappa^2 + 2)
     };

@@ -642,11 +642,13 @@ __device__ __forceinline__ int nth_bit(unsigned m, int n) {
 
 // One sweep over the rows (Row format; kWChunk doubles per ring chunk, so
 // kWChunk / Row::kW rows).  mode 0: chains A and B, counts only; 1: chain A
-// with derivative + chain B; 2: chain A with derivative only.  p_init starts
-// both chains (Row::p_init); rat0 is chain A's Newton correction.
+// with derivative(s) + chain B; 2: chain A with derivative(s) only.  p_init
+// starts both chains (Row::p_init).  For Newton rows rat0 is chain A's Newton
+// correction; for Laguerre rows (Row::kLaguerre) chain A also carries the
+// second derivative and rat0 = det'/det, h0 = rat0^2 - det''/det.
 template <class Row>
 __device__ void warp_sweep(const double* __restrict__ s, int nz, double p_init, double x0, double x1, int mode,
-                           WarpRing& r, unsigned* err, int& c0, int& c1, double& rat0) {
+                           WarpRing& r, unsigned* err, int& c0, int& c1, double& rat0, double& h0) {
     constexpr int kW = Row::kW;
     constexpr int kRows = kWChunk / kW;
     const int lane = threadIdx.x & 31;
@@ -662,7 +664,7 @@ __device__ void warp_sweep(const double* __restrict__ s, int nz, double p_init, 
         A.p0 = p_init;
         B.p0 = p_init;
     }
-    double da0 = 0.0, da1 = 0.0;
+    double da0 = 0.0, da1 = 0.0, ea0 = 0.0, ea1 = 0.0;
     for (int c = 0; c < nch; ++c) {
         const unsigned k = base + c;
         const int slot = k % kWBuf;
@@ -675,6 +677,17 @@ __device__ void warp_sweep(const double* __restrict__ s, int nz, double p_init, 
             for (int i = nw * 32; i < valid; ++i) {
                 Row::step(A, b, i, x0);
                 Row::step(B, b, i, x1);
+            }
+        } else if constexpr (Row::kLaguerre) {
+            if (mode == 1) {
+                for (int w = 0; w < nw; ++w) Row::deriv2_pair(A, da0, da1, ea0, ea1, B, b + 32 * kW * w, x0, x1);
+                for (int i = nw * 32; i < valid; ++i) {
+                    Row::step_deriv2(A, b, i, x0, da0, da1, ea0, ea1);
+                    Row::step(B, b, i, x1);
+                }
+            } else {
+                for (int w = 0; w < nw; ++w) Row::word_deriv2(A, b + 32 * kW * w, x0, da0, da1, ea0, ea1);
+                for (int i = nw * 32; i < valid; ++i) Row::step_deriv2(A, b, i, x0, da0, da1, ea0, ea1);
             }
         } else if (mode == 1) {
             for (int w = 0; w < nw; ++w) Row::deriv_pair(A, da0, da1, B, b + 32 * kW * w, x0, x1);
@@ -695,7 +708,13 @@ __device__ void warp_sweep(const double* __restrict__ s, int nz, double p_init, 
     r.loads = base + nch;
     c0 = A.cnt;
     c1 = B.cnt;
-    rat0 = mode >= 1 ? Row::newton(A.p1, da1) : 0.0;
+    h0 = 0.0;
+    if constexpr (Row::kLaguerre) {
+        rat0 = mode >= 1 ? da1 / A.p1 : 0.0;
+        h0 = mode >= 1 ? fma(rat0, rat0, -(ea1 / A.p1)) : 0.0;
+    } else {
+        rat0 = mode >= 1 ? Row::newton(A.p1, da1) : 0.0;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -724,12 +743,13 @@ __device__ __forceinline__ int twist_count(const SturmState& F, const SturmState
 
 // 32 front rows (ascending, fb) and 32 back rows (descending, bb) in one
 // loop.  kMode 0: four count chains (A, B forward and backward); 1: A chains
-// with derivatives + B chains; 2: A chains with derivatives only.
+// with derivatives + B chains; 2: A chains with derivatives only.  With kMode
+// >= 1 the A chains also carry second derivatives (fe, be: Laguerre steps).
 template <int kMode>
 __device__ __forceinline__ void tw_word(EssRows, SturmState& Af, SturmState& Bf, SturmState& Ab, SturmState& Bb,
-                                        double& fd0, double& fd1, double& bd0, double& bd1,
-                                        const double* __restrict__ fb, const double* __restrict__ bb, double xa,
-                                        double xb) {
+                                        double& fd0, double& fd1, double& bd0, double& bd1, double& fe0,
+                                        double& fe1, double& be0, double& be1, const double* __restrict__ fb,
+                                        const double* __restrict__ bb, double xa, double xb) {
     unsigned waf = 0u, wbf = 0u, wab = 0u, wbb = 0u;
     double af0 = Af.p0, af1 = Af.p1, ab0 = Ab.p0, ab1 = Ab.p1;
     double bf0 = Bf.p0, bf1 = Bf.p1, bb0 = Bb.p0, bb1 = Bb.p1;
@@ -742,10 +762,15 @@ __device__ __forceinline__ void tw_word(EssRows, SturmState& Af, SturmState& Bf,
         const double qaf = fma(ta, af1, -af0), qab = fma(ua, ab1, -ab0);
         if (kMode >= 1) {
             const double ef = fma(ta, fd1, -(af1 + fd0)), eb = fma(ua, bd1, -(ab1 + bd0));
+            const double gf = fma(ta, fe1, -fma(2.0, fd1, fe0)), gb = fma(ua, be1, -fma(2.0, bd1, be0));
             fd0 = fd1;
             fd1 = ef;
             bd0 = bd1;
             bd1 = eb;
+            fe0 = fe1;
+            fe1 = gf;
+            be0 = be1;
+            be1 = gb;
         }
         waf = __funnelshift_l(__double2hiint(qaf), waf, 1);
         wab = __funnelshift_l(__double2hiint(qab), wab, 1);
@@ -767,10 +792,15 @@ __device__ __forceinline__ void tw_word(EssRows, SturmState& Af, SturmState& Bf,
         const double qaf2 = fma(ta2, af1, -af0), qab2 = fma(ua2, ab1, -ab0);
         if (kMode >= 1) {
             const double ef = fma(ta2, fd1, -(af1 + fd0)), eb = fma(ua2, bd1, -(ab1 + bd0));
+            const double gf = fma(ta2, fe1, -fma(2.0, fd1, fe0)), gb = fma(ua2, be1, -fma(2.0, bd1, be0));
             fd0 = fd1;
             fd1 = ef;
             bd0 = bd1;
             bd1 = eb;
+            fe0 = fe1;
+            fe1 = gf;
+            be0 = be1;
+            be1 = gb;
         }
         waf = __funnelshift_l(__double2hiint(qaf2), waf, 1);
         wab = __funnelshift_l(__double2hiint(qab2), wab, 1);
@@ -793,8 +823,8 @@ __device__ __forceinline__ void tw_word(EssRows, SturmState& Af, SturmState& Bf,
     Ab.p0 = ab0;
     Ab.p1 = ab1;
     if (kMode >= 1) {
-        sturm_fold_deriv(Af, waf, fd0, fd1);
-        sturm_fold_deriv(Ab, wab, bd0, bd1);
+        sturm_fold_deriv2(Af, waf, fd0, fd1, fe0, fe1);
+        sturm_fold_deriv2(Ab, wab, bd0, bd1, be0, be1);
     } else {
         sturm_fold(Af, waf);
         sturm_fold(Ab, wab);
@@ -811,9 +841,9 @@ __device__ __forceinline__ void tw_word(EssRows, SturmState& Af, SturmState& Bf,
 
 template <int kMode>
 __device__ __forceinline__ void tw_word(WmodRows, SturmState& Af, SturmState& Bf, SturmState& Ab, SturmState& Bb,
-                                        double& fd0, double& fd1, double& bd0, double& bd1,
-                                        const double* __restrict__ fb, const double* __restrict__ bb, double xa,
-                                        double xb) {
+                                        double& fd0, double& fd1, double& bd0, double& bd1, double&, double&, double&,
+                                        double&, const double* __restrict__ fb, const double* __restrict__ bb,
+                                        double xa, double xb) {
     const double ca = fma(-xa, xa, -2.0), cb = fma(-xb, xb, -2.0);
     unsigned waf = 0u, wbf = 0u, wab = 0u, wbb = 0u;
     double af0 = Af.p0, af1 = Af.p1, ab0 = Ab.p0, ab1 = Ab.p1;
@@ -875,7 +905,7 @@ __device__ __forceinline__ void tw_word(WmodRows, SturmState& Af, SturmState& Bf
 // front part and a back part of kWChunk / 2 doubles
 template <class Row, int kMode>
 __device__ void warp_sweep_tw_mode(const double* __restrict__ s, int nz, double p_init, double x0, double x1,
-                                   WarpRing& r, unsigned* err, int& c0, int& c1, double& rat0) {
+                                   WarpRing& r, unsigned* err, int& c0, int& c1, double& rat0, double& h0) {
     constexpr int kW = Row::kW;
     constexpr int kHD = kWChunk / 2;  // doubles per part
     constexpr int kHR = kHD / kW;     // rows per part
@@ -903,7 +933,7 @@ __device__ void warp_sweep_tw_mode(const double* __restrict__ s, int nz, double 
         Af.p0 = p_init;
         Bf.p0 = p_init;
     }
-    double fd0 = 0.0, fd1 = 0.0, bd0 = 0.0, bd1 = 0.0;
+    double fd0 = 0.0, fd1 = 0.0, bd0 = 0.0, bd1 = 0.0, fe0 = 0.0, fe1 = 0.0, be0 = 0.0, be1 = 0.0;
     for (int j = 0; j < nf; ++j) {
         const unsigned k = base + j;
         const int slot = k % kWBuf;
@@ -915,18 +945,28 @@ __device__ void warp_sweep_tw_mode(const double* __restrict__ s, int nz, double 
             const int valid_b = min(kHR, nz - (nparts - 1 - j) * kHR);
             nwb = valid_b >> 5;
             for (int i = valid_b - 1; i >= nwb * 32; --i) {  // ragged top of the last part, descending
-                if (kMode >= 1) Row::step_deriv(Ab, bb, i, x0, bd0, bd1);
-                else Row::step(Ab, bb, i, x0);
+                if (kMode >= 1) {
+                    if constexpr (Row::kLaguerre) Row::step_deriv2(Ab, bb, i, x0, bd0, bd1, be0, be1);
+                    else Row::step_deriv(Ab, bb, i, x0, bd0, bd1);
+                } else {
+                    Row::step(Ab, bb, i, x0);
+                }
                 if (kMode <= 1) Row::step(Bb, bb, i, x1);
             }
             for (int w = 0; w < nwb; ++w)
-                tw_word<kMode>(Row{}, Af, Bf, Ab, Bb, fd0, fd1, bd0, bd1, fb + 32 * kW * w,
+                tw_word<kMode>(Row{}, Af, Bf, Ab, Bb, fd0, fd1, bd0, bd1, fe0, fe1, be0, be1, fb + 32 * kW * w,
                                bb + 32 * kW * (nwb - 1 - w), x0, x1);
         }
         for (int w = nwb; w < kHW; ++w) {  // front words without a back partner
-            if (kMode == 0) Row::pair(Af, Bf, fb + 32 * kW * w, x0, x1);
-            else if (kMode == 1) Row::deriv_pair(Af, fd0, fd1, Bf, fb + 32 * kW * w, x0, x1);
-            else Row::word_deriv(Af, fb + 32 * kW * w, x0, fd0, fd1);
+            if (kMode == 0) {
+                Row::pair(Af, Bf, fb + 32 * kW * w, x0, x1);
+            } else if constexpr (Row::kLaguerre) {
+                if (kMode == 1) Row::deriv2_pair(Af, fd0, fd1, fe0, fe1, Bf, fb + 32 * kW * w, x0, x1);
+                else Row::word_deriv2(Af, fb + 32 * kW * w, x0, fd0, fd1, fe0, fe1);
+            } else {
+                if (kMode == 1) Row::deriv_pair(Af, fd0, fd1, Bf, fb + 32 * kW * w, x0, x1);
+                else Row::word_deriv(Af, fb + 32 * kW * w, x0, fd0, fd1);
+            }
         }
         __syncwarp();
         if (lane == 0 && j + kWBuf < nf) {
@@ -943,9 +983,19 @@ __device__ void warp_sweep_tw_mode(const double* __restrict__ s, int nz, double 
         c1 = twist_count(Bf, Bb, detb);
     }
     rat0 = 0.0;
+    h0 = 0.0;
     if (kMode >= 1) {
+        // det = F1 B1 - F0 B0 (F the forward chain p_{h-1}, p_{h-2}; B the
+        // backward chain q_h, q_{h+1}); derivatives by the product rule
         const double dd = fd1 * Ab.p1 + Af.p1 * bd1 - fd0 * Ab.p0 - Af.p0 * bd0;
-        rat0 = Row::newton(det, dd);
+        if constexpr (Row::kLaguerre) {
+            const double d2 = fe1 * Ab.p1 + 2.0 * fd1 * bd1 + Af.p1 * be1 -
+                              (fe0 * Ab.p0 + 2.0 * fd0 * bd0 + Af.p0 * be0);
+            rat0 = dd / det;
+            h0 = fma(rat0, rat0, -(d2 / det));
+        } else {
+            rat0 = Row::newton(det, dd);
+        }
     }
 }
 
@@ -953,14 +1003,14 @@ __device__ void warp_sweep_tw_mode(const double* __restrict__ s, int nz, double 
 // sequential sweep
 template <class Row>
 __device__ void warp_sweep_tw(const double* __restrict__ s, int nz, double p_init, double x0, double x1, int mode,
-                              WarpRing& r, unsigned* err, int& c0, int& c1, double& rat0) {
+                              WarpRing& r, unsigned* err, int& c0, int& c1, double& rat0, double& h0) {
     if (!Row::kTwist || nz <= kWChunk / 2 / Row::kW) {
-        warp_sweep<Row>(s, nz, p_init, x0, x1, mode, r, err, c0, c1, rat0);
+        warp_sweep<Row>(s, nz, p_init, x0, x1, mode, r, err, c0, c1, rat0, h0);
         return;
     }
-    if (mode == 0) warp_sweep_tw_mode<Row, 0>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0);
-    else if (mode == 1) warp_sweep_tw_mode<Row, 1>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0);
-    else warp_sweep_tw_mode<Row, 2>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0);
+    if (mode == 0) warp_sweep_tw_mode<Row, 0>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0, h0);
+    else if (mode == 1) warp_sweep_tw_mode<Row, 1>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0, h0);
+    else warp_sweep_tw_mode<Row, 2>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0, h0);
 }
 
 // One bisection work item (<= 32 eigenvalues of one problem) on this warp,
@@ -1032,9 +1082,9 @@ __device__ __forceinline__ void bisect_item(const ProblemInfo* __restrict__ pinf
         }
         (void)newton0;
         int cv0, cv1;
-        double rat;
+        double rat, hq;
         const int smode = nN == 0 ? 0 : (nB > 0 ? 1 : 2);
-        warp_sweep_tw<Row>(sp, nz, p_init, xv[0], xv[1], smode, r, err, cv0, cv1, rat);
+        warp_sweep_tw<Row>(sp, nz, p_init, xv[0], xv[1], smode, r, err, cv0, cv1, rat, hq);
         if (step_counter && lane == 0)
             atomicAdd(step_counter, (unsigned long long)(smode == 2 ? 32 : 64) * (unsigned long long)nz);
         // updates.  Every __shfl_sync is executed by all 32 lanes.
@@ -1042,6 +1092,7 @@ __device__ __forceinline__ void bisect_item(const ProblemInfo* __restrict__ pinf
         const int vN = isN ? __popc(nm & ((1u << lane) - 1u)) : 0;  // Newton virtual lane (chain 0)
         const int cN = __shfl_sync(0xffffffffu, cv0, vN);
         const double rN = __shfl_sync(0xffffffffu, rat, vN);
+        const double hN = Row::kLaguerre ? __shfl_sync(0xffffffffu, hq, vN) : 0.0;
         const int k = isB ? __popc(bm & ((1u << lane) - 1u)) : 0;
         const int G = isB ? (nlB - 1 - k) / nB + 1 : 0;
         const int Gmax = nB > 0 ? (nlB - 1) / nB + 1 : 0;
@@ -1068,19 +1119,26 @@ __device__ __forceinline__ void bisect_item(const ProblemInfo* __restrict__ pinf
                 b = xo;
                 cb = cN;
             }
-            const double ad = fabs(rN);
+            // the correction: Laguerre's step toward the eigenvalue (above x
+            // when x lies below it) or Newton's
+            const double corr = Row::kLaguerre ? laguerre_step(rN, hN, (double)nz, cN <= J) : rN;
+            const double ad = fabs(corr);
             if (ad <= tol) {
-                x = fmin(fmax(xo - rN, a), b);
+                x = fmin(fmax(xo - corr, a), b);
                 mode = 2;
             } else {
-                const double xn = xo - rN;
+                const double xn = xo - corr;
                 const bool ok = isfinite(xn) && xn > a && xn < b;
                 x = ok ? xn : 0.5 * (a + b);
+                const double ad2 = ad * ad, dp2 = dprev * dprev;
+                // cubic (Laguerre) / quadratic (Newton) convergence: the next
+                // correction would be about ad^4 / dprev^3 (ad^3 / dprev^2) <= tol,
+                // so x = xn is final
+                const bool settled =
+                    Row::kLaguerre ? ad2 * ad2 <= tol * dp2 * dprev : ad2 * ad <= tol * dp2;
                 if (!(b - a > tol)) {
                     mode = 2;
-                } else if (ok && dprev > 0.0 && ad <= 0.25 * dprev && ad * ad * ad <= tol * dprev * dprev) {
-                    // quadratic convergence: the next correction would be
-                    // about ad^2 (ad / dprev^2) <= tol, so x = xn is final
+                } else if (ok && dprev > 0.0 && ad <= 0.25 * dprev && settled) {
                     mode = 2;
                 }
                 dprev = ok ? ad : 0.0;
@@ -1396,12 +1454,279 @@ __device__ __forceinline__ void fwd_step(FwdState& F, int i, int nz, const doubl
     F.pm1 = pn;
 }
 
+// Reduction-only eigenvector item (no full vector wanted): two passes and a
+// twist chosen among the coarse rows c = 0, kCk, 2 kCk, ...
+//  pass 1  backward recurrence q with the sums T = sum_{i > c} q_{i+1}^2 (1, w,
+//          g) over the rows above; at every coarse row c the slot keeps
+//          q_{c+1}, its exponent and T (5 values per kCk rows instead of the
+//          q checkpoints every kBlk rows that a full vector needs);
+//  pass 2  forward recurrence p with the sums A = sum_{i <= c} p_{i-1}^2 (1, w,
+//          g); at each coarse row the twist key |p_{c-1} q_{c+1}| (proportional
+//          to |z_c|) picks the best twist r so far.
+// Then sum z^2 / z_r^2 = A_r / p_{r-1}^2 + T_r / q_{r+1}^2 (each in its own
+// recurrence's scale).  Restricting r to the coarse rows costs at most the
+// ratio of the largest |z_i| to the largest |z_c| in residual (one
+// inverse-iteration step from e_r, residual |gamma_r| / |z|): measured on
+// the 20000- to 100000-point grids of 0.05-2 Hz, at most 1.06 for every
+// mode with 64-row spacing and 1.8 with 256.
+constexpr int kCk = kCkRows;  // rows between coarse twist candidates
+static_assert(kEvC % kCk == 0 && kCk % kBlk == 0, "coarse rows start blocks and chunks");
+
+template <class Row, bool kGroup>
+__device__ __forceinline__ void eigvec_item_coarse(const EigvecArgs& A, const WorkItem w, EvRing& R, double* ckq,
+                                                   double* ckt, int* cke) {
+    constexpr int kW = Row::kW;
+    const int lane = threadIdx.x & 31;
+    const ProblemInfo pi = A.pinfo[w.problem];
+    const int nz = pi.nz;
+    const int nch = (nz + kEvC - 1) / kEvC;
+    const int isrc = pi.isrc, ircv = pi.ircv;
+    const double* sp = A.s + (size_t)pi.s_off * kW;
+    const double* wp = A.w + pi.w_off;
+    const double* gp = kGroup ? A.g + pi.s_off : nullptr;
+    const bool active = lane < w.m;
+    // through L2: in the fused launch another warp wrote mu in this kernel
+    const double mu = active ? __ldcg(A.mu + pi.off + w.j0 + lane) : Row::idle_shift(pi);
+    const typename Row::Shift sh = Row::shift(mu);
+
+    // ---------------- pass 1: backward recurrence, coarse checkpoints ----------
+    double qs = 1.0, qrc = 1.0;  // q_{isrc+1}, q_{ircv+1}
+    int Eqs = 0, Eqrc = 0;
+    {
+        const unsigned base = R.loads;
+        if (lane == 0)
+            for (int o = 0; o < nch && o < kEvB; ++o) evr_issue<kW>(R, base + o, nch - 1 - o, sp, wp, gp);
+        __syncwarp();
+        double q1 = 1.0, q2 = 0.0;  // q_{i+1}, q_{i+2} before row i; q_n = 1, q_{n+1} = 0
+        double Tn = 0.0, Tw = 0.0, Tg = 0.0;
+        int E = 0;
+        for (int o = 0; o < nch; ++o) {
+            const int c = nch - 1 - o;
+            const unsigned k = base + o;
+            const int slot = k % kEvB;
+            mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
+            const double* sb = R.s + slot * kEvC * kW;
+            const double* wb = R.w + slot * kEvC;
+            const double* gb = kGroup ? R.g + slot * kEvC : nullptr;
+            const int valid = min(kEvC, nz - c * kEvC);
+            auto row = [&](int li) {
+                const double qq = q1 * q1;
+                Tn = Tn + qq;
+                Tw = fma(qq, wb[li], Tw);
+                if (kGroup) Tg = fma(qq, gb[li], Tg);
+                const double qi = fma(Row::t(sb, li, sh), q1, -q2);
+                q2 = q1;
+                q1 = qi;
+            };
+            auto store = [&](int gbase) {
+                const size_t ci = (size_t)(gbase / kCk) * 32 + lane;
+                ckq[ci] = q1;
+                cke[ci] = E;
+                ckt[ci * 3] = Tn;
+                ckt[ci * 3 + 1] = Tw;
+                ckt[ci * 3 + 2] = Tg;
+            };
+            for (int lb = ((valid - 1) / kBlk) * kBlk; lb >= 0; lb -= kBlk) {
+                const int gbase = c * kEvC + lb;
+                const bool coarse = (gbase % kCk) == 0;
+                const bool special = lb + kBlk > valid || (isrc >= gbase && isrc < gbase + kBlk) ||
+                                     (ircv >= gbase && ircv < gbase + kBlk);
+                if (!special) {
+#pragma unroll
+                    for (int u = kBlk - 1; u >= 0; --u) {
+                        if (u == 0 && coarse) store(gbase);
+                        row(lb + u);
+                    }
+                } else {
+                    for (int u = min(kBlk, valid - lb) - 1; u >= 0; --u) {
+                        const int i = gbase + u;
+                        if (i == isrc) {
+                            qs = q1;
+                            Eqs = E;
+                        }
+                        if (i == ircv) {
+                            qrc = q1;
+                            Eqrc = E;
+                        }
+                        if (u == 0 && coarse) store(gbase);
+                        row(lb + u);
+                    }
+                }
+                const int sft = grow_shift(q1, q2);
+                if (sft) {
+                    const double sc = pow2(-sft), sc2 = pow2(-2 * sft);
+                    q1 *= sc;
+                    q2 *= sc;
+                    Tn *= sc2;
+                    Tw *= sc2;
+                    Tg *= sc2;
+                    E += sft;
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && o + kEvB < nch) {
+                fence_proxy_async();
+                evr_issue<kW>(R, base + o + kEvB, nch - 1 - (o + kEvB), sp, wp, gp);
+            }
+        }
+        R.loads = base + nch;
+    }
+    __syncwarp();  // the slot's checkpoints written by every lane before they are read
+
+    // ---------------- pass 2: forward recurrence, coarse twist ----------------
+    double pm2 = Row::p_init(pi), pm1 = 1.0;  // p_{i-2}, p_{i-1}
+    int Ep = 0;
+    double An = 0.0, Aw = 0.0, Ag = 0.0;
+    double best = -INFINITY;
+    int r = 0, Epr = 0, Eqr = 0;
+    double Anr = 1.0, Awr = 0.0, Agr = 0.0, pr = 1.0, qr = 1.0, Tnr = 0.0, Twr = 0.0, Tgr = 0.0;
+    double ps = 1.0, prc = 1.0;  // p_{isrc-1}, p_{ircv-1}
+    int Eps = 0, Eprc = 0;
+    {
+        const unsigned base = R.loads;
+        if (lane == 0)
+            for (int c = 0; c < nch && c < kEvB; ++c) evr_issue<kW>(R, base + c, c, sp, wp, gp);
+        __syncwarp();
+        // checkpoint of the next coarse row, loaded one candidate ahead
+        double nq = ckq[lane], nt0 = ckt[lane * 3], nt1 = ckt[lane * 3 + 1], nt2 = ckt[lane * 3 + 2];
+        int nE = cke[lane];
+        const int n_coarse = (nz + kCk - 1) / kCk;
+        for (int c = 0; c < nch; ++c) {
+            const unsigned k = base + c;
+            const int slot = k % kEvB;
+            mbar_wait_bounded(&R.bars[slot], (k / kEvB) & 1u, A.err);
+            const double* sb = R.s + slot * kEvC * kW;
+            const double* wb = R.w + slot * kEvC;
+            const double* gb = kGroup ? R.g + slot * kEvC : nullptr;
+            const int valid = min(kEvC, nz - c * kEvC);
+            auto row = [&](int li) {
+                const double sq = pm1 * pm1;
+                An = An + sq;
+                Aw = fma(sq, wb[li], Aw);
+                if (kGroup) Ag = fma(sq, gb[li], Ag);
+            };
+            auto step = [&](int li) {
+                const double pn = fma(Row::t(sb, li, sh), pm1, -pm2);
+                pm2 = pm1;
+                pm1 = pn;
+            };
+            auto candidate = [&](int gbase) {
+                // key log2 |p_{c-1} q_{c+1}| with both recurrences' exponents
+                const double key = log2(fabs(pm1 * nq)) + (double)(Ep + nE);
+                if (key > best) {
+                    best = key;
+                    r = gbase;
+                    Anr = An;
+                    Awr = Aw;
+                    Agr = Ag;
+                    pr = pm1;
+                    Epr = Ep;
+                    qr = nq;
+                    Eqr = nE;
+                    Tnr = nt0;
+                    Twr = nt1;
+                    Tgr = nt2;
+                }
+                const int kc = gbase / kCk + 1;
+                if (kc < n_coarse) {
+                    const size_t ci = (size_t)kc * 32 + lane;
+                    nq = ckq[ci];
+                    nE = cke[ci];
+                    nt0 = ckt[ci * 3];
+                    nt1 = ckt[ci * 3 + 1];
+                    nt2 = ckt[ci * 3 + 2];
+                }
+            };
+            for (int lb = 0; lb < valid; lb += kBlk) {
+                const int gbase = c * kEvC + lb;
+                const bool coarse = (gbase % kCk) == 0;
+                const bool special = lb + kBlk > valid || (isrc >= gbase && isrc < gbase + kBlk) ||
+                                     (ircv >= gbase && ircv < gbase + kBlk);
+                if (!special) {
+#pragma unroll
+                    for (int u = 0; u < kBlk; ++u) {
+                        row(lb + u);
+                        if (u == 0 && coarse) candidate(gbase);
+                        step(lb + u);
+                    }
+                } else {
+                    const int nrow = min(kBlk, valid - lb);
+                    for (int u = 0; u < nrow; ++u) {
+                        const int i = gbase + u;
+                        if (i == isrc) {
+                            ps = pm1;
+                            Eps = Ep;
+                        }
+                        if (i == ircv) {
+                            prc = pm1;
+                            Eprc = Ep;
+                        }
+                        row(lb + u);
+                        if (u == 0 && coarse) candidate(gbase);
+                        step(lb + u);
+                    }
+                }
+                const int sft = grow_shift(pm1, pm2);
+                if (sft) {
+                    const double sc = pow2(-sft), sc2 = pow2(-2 * sft);
+                    pm1 *= sc;
+                    pm2 *= sc;
+                    An *= sc2;
+                    Aw *= sc2;
+                    Ag *= sc2;
+                    Ep += sft;
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && c + kEvB < nch) {
+                fence_proxy_async();
+                evr_issue<kW>(R, base + c + kEvB, c + kEvB, sp, wp, gp);
+            }
+        }
+        R.loads = base + nch;
+    }
+    // ---------------- combine ----------------------------------------
+    const double ip2 = 1.0 / (pr * pr), iq2 = 1.0 / (qr * qr);
+    const double nrm = Anr * ip2 + Tnr * iq2;
+    // the wide-angle vectors carry SLEPc's normalisation of the linearised
+    // pencil's [v; k v] (EigenEngine.cpp:368-379): sum v^2 dz = 1 / (1 + k^2)
+    const double f2 = kW == 1 ? 1.0 : 1.0 / (1.0 + (mu / pi.dz) * (mu / pi.dz));
+    const double scale = kW == 1 ? 1.0 / sqrt(nrm * pi.dz) : sqrt(f2 / (nrm * pi.dz));
+    double zs = (isrc <= r) ? (ps / pr) * pow2(Eps - Epr) : (qs / qr) * pow2(Eqs - Eqr);
+    double zr = (ircv <= r) ? (prc / pr) * pow2(Eprc - Epr) : (qrc / qr) * pow2(Eqrc - Eqr);
+    if ((isrc - r) & 1) zs = -zs;
+    if ((ircv - r) & 1) zr = -zr;
+    const double absorption = (Awr * ip2 + Twr * iq2) / nrm * f2;
+    const double ks = kW == 1 ? sqrt(mu / (pi.dz * pi.dz)) : mu / pi.dz;
+    const double kk = ks * ks;
+    const auto kp = csqrt_principal(kk, absorption);
+    if (active) {
+        const int o = pi.off + w.j0 + lane;
+        A.kr[o] = kp.real();
+        A.ki[o] = kp.imag();
+        A.vs[o] = zs * scale;
+        A.vr[o] = zr * scale;
+        if (kGroup) {
+            const double gsum = (Agr * ip2 + Tgr * iq2) / nrm;
+            const double vph = pi.omega / kp.real();
+            A.vg[o] = 1.0 / (vph * gsum);
+        } else if (A.vg) {
+            A.vg[o] = 0.0;
+        }
+    }
+}
+
 // One eigenvector work item (<= 32 modes of one problem) on this warp, with
 // its TMA ring R and its checkpoint slot (ck1, ck2, cke).
 template <class Row, bool kGroup, bool kVec>
 __device__ __forceinline__ void eigvec_item(const EigvecArgs& A, const WorkItem w, EvRing& R, double* ck1,
                                             double* ck2, int* cke) {
     constexpr int kW = Row::kW;
+    if constexpr (!kVec) {
+        // reductions only: the two-pass coarse-twist item
+        eigvec_item_coarse<Row, kGroup>(A, w, R, ck1, ck2, cke);
+        return;
+    }
     const int lane = threadIdx.x & 31;
     const ProblemInfo pi = A.pinfo[w.problem];
     const int nz = pi.nz;

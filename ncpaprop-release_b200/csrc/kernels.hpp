@@ -45,6 +45,14 @@ struct WorkItem {
 constexpr int kScanPoints = 256;  // Sturm counts per problem in the isolation scan
 constexpr int kChunk = 1024;      // doubles per TMA chunk of the diagonal
 constexpr int kBlk = 16;          // eigenvector checkpoint interval
+constexpr int kCkRows = 128;      // twist candidates of the reduction-only eigenvector items
+// elements of each eigenvector checkpoint array per warp slot for grids of up
+// to nz points: q every kBlk rows (items that write full vectors) or three
+// sums every kCkRows rows (items that only reduce)
+inline long long ck_slot_elems(long long nz) {
+    const long long a = (nz + kBlk - 1) / kBlk, b = 3 * ((nz + kCkRows - 1) / kCkRows);
+    return (a > b ? a : b) * 32;
+}
 constexpr int kThreads = 256;     // threads of the scan CTAs
 constexpr int kWItem = 32;        // eigenvalues per warp work item of the bisection
 constexpr int kEvItem = 32;       // eigenvalues per warp work item of the eigenvector kernel

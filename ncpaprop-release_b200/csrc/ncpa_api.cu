@@ -513,7 +513,7 @@ void prepare_solve(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, int
     M->d_vg.alloc(mcap * 8, st);
     const ncpa::EigvecArgs ea = eigvec_args(ctx, M, prm, s, w, gs, b);
     const int grid_e = eigvec_grid(ctx, ea, b.ev_cap, 0);  // the largest grid
-    const long long slot = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
+    const long long slot = ncpa::ck_slot_elems(M->nz_max);
     const size_t need = (size_t)grid_e * ncpa::kEvWarpsPerCta * slot;
     DevBuf& c1 = b.own_ck ? b.ck1 : ctx->ck1;
     DevBuf& c2 = b.own_ck ? b.ck2 : ctx->ck2;
@@ -559,7 +559,7 @@ void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_
     ea.ck_q1 = (b.own_ck ? b.ck1 : ctx->ck1).as<double>();
     ea.ck_q2 = (b.own_ck ? b.ck2 : ctx->ck2).as<double>();
     ea.ck_e = (b.own_ck ? b.cke : ctx->cke).as<int>();
-    ea.ck_slot_stride = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
+    ea.ck_slot_stride = ncpa::ck_slot_elems(M->nz_max);
     if (fuse) {
         int* fq = b.fq.as<int>();
         CK(cudaMemsetAsync(fq, 0, ((size_t)2 * b.ev_cap + 2) * sizeof(int), st));
@@ -755,8 +755,7 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
         ea.vfull_off = prm->want_vectors ? M->d_vfull_off.as<long long>() : nullptr;
         const int ewpc = ncpa::kEvWarpsPerCta;
         const int grid_e = std::min((n_ev + ewpc - 1) / ewpc, ctx->num_sms * ncpa::eigvec_ctas_per_sm(ea));
-        const long long nblk = (M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk;
-        const long long slot = nblk * 32;
+        const long long slot = ncpa::ck_slot_elems(M->nz_max);
         const size_t need = (size_t)grid_e * ewpc * slot;
         if (ctx->ck1.bytes < need * 8) {
             ctx->ck1.alloc(need * 8, st);
@@ -1034,7 +1033,7 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
     // the fused launch runs on every SM (idle warps take eigenvector items from
     // the start), so the checkpoint scratch has a slot for each of its warps
     const int grid_f = fused ? ctx->num_sms * ncpa::fused_wmod_ctas_per_sm() : 0;
-    const long long slot = (long long)((M->nz_max + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
+    const long long slot = ncpa::ck_slot_elems(M->nz_max);
     const size_t need = (size_t)std::max(grid_e, grid_f) * ncpa::kEvWarpsPerCta * slot;
     if (n_ev > 0 && ctx->ck1.bytes < need * 8) {
         ctx->ck1.alloc(need * 8, st);
@@ -1826,6 +1825,78 @@ ncpa_status ncpa_tl_1d(ncpa_ctx* ctx, const ncpa_modes* m, const ncpa_tl_params*
         CK(cudaStreamSynchronize(st));
         return NCPA_OK;
     });
+}
+
+ncpa_status ncpa_tl_1d_range(ncpa_ctx* ctx, const ncpa_modes* m, int first, int count, const ncpa_tl_params* tp,
+                             double* re, double* im, double* incoh) {
+    if (!ctx || !m || !tp || !re || !im || !incoh || first < 0 || count < 1 || first + count > m->P)
+        return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        if (tp->n_ranges < 1 || !(tp->dr_m > 0)) throw ApiError(NCPA_EINVAL, "bad range grid");
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        const size_t n = (size_t)count * tp->n_ranges;
+        DevBuf dre, dim, dinc;
+        dre.alloc(n * 8, st);
+        dim.alloc(n * 8, st);
+        dinc.alloc(n * 8, st);
+        // the problem records carry absolute mode offsets: start at `first`
+        check_launch(ctx, ncpa::launch_tl1d(st, count, m->d_pinfo.as<ProblemInfo>() + first, m->d_kr.as<double>(),
+                                            m->d_ki.as<double>(), m->d_vs.as<double>(), m->d_vr.as<double>(),
+                                            tp->n_ranges, tp->dr_m, tp->lossless, dre.as<double>(), dim.as<double>(),
+                                            dinc.as<double>()));
+        CK(cudaMemcpyAsync(re, dre.p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(im, dim.p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(incoh, dinc.p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return NCPA_OK;
+    });
+}
+
+ncpa_status ncpa_modes_from_host(ncpa_ctx* ctx, int n_problems, const int* mode_off, const double* re_k,
+                                 const double* im_k, const double* v_src, const double* v_rcv, ncpa_modes** out) {
+    if (!ctx || !out || n_problems < 1 || !mode_off) return NCPA_EINVAL;
+    *out = nullptr;
+    if (mode_off[0] != 0) return fail(ctx, NCPA_EINVAL, "mode offsets must start at 0");
+    for (int p = 0; p < n_problems; ++p)
+        if (mode_off[p + 1] < mode_off[p]) return fail(ctx, NCPA_EINVAL, "mode offsets must not decrease");
+    const int Mtot = mode_off[n_problems];
+    if (Mtot > 0 && (!re_k || !im_k || !v_src || !v_rcv)) return NCPA_EINVAL;
+    auto m = std::make_unique<ncpa_modes>();
+    m->ctx = ctx;
+    ncpa_status s = guarded(ctx, [&]() -> ncpa_status {
+        CK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        m->P = n_problems;
+        m->nf = n_problems;
+        m->na = 1;
+        ncpa_ess_params_default(&m->prm);
+        m->Mtot = Mtot;
+        m->info.assign(n_problems, ProblemInfo{});
+        for (int p = 0; p < n_problems; ++p) {
+            m->info[p].off = mode_off[p];
+            m->info[p].M = mode_off[p + 1] - mode_off[p];
+        }
+        m->rho_src_p.assign(n_problems, 1.0);
+        m->rho_rcv_p.assign(n_problems, 1.0);
+        m->kr.assign(re_k, re_k + Mtot);
+        m->ki.assign(im_k, im_k + Mtot);
+        m->vs.assign(v_src, v_src + Mtot);
+        m->vr.assign(v_rcv, v_rcv + Mtot);
+        m->vg.assign(Mtot, 0.0);
+        m->host_valid = true;
+        upload(m->d_pinfo, m->info, st);
+        upload(m->d_kr, m->kr, st);
+        upload(m->d_ki, m->ki, st);
+        upload(m->d_vs, m->vs, st);
+        upload(m->d_vr, m->vr, st);
+        upload(m->d_vg, m->vg, st);
+        CK(cudaStreamSynchronize(st));
+        return NCPA_OK;
+    });
+    if (s != NCPA_OK) return s;
+    *out = m.release();
+    return NCPA_OK;
 }
 
 ncpa_status ncpa_tl_2d_heights(const ncpa_modes* m, int problem, int* n_heights) {

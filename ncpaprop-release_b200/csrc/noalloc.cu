@@ -39,6 +39,8 @@ constexpr int kStaticMaxModes = 4000;      // eigenvalues per call
 constexpr int kStaticWarps = 16;           // eigenvector warps (4 CTAs)
 constexpr int kStaticChunk = 256;          // padding of the diagonal copies
 constexpr int kStaticBlocks = kStaticMaxNz / ncpa::kBlk;
+static_assert((long long)kStaticBlocks * 32 >= 3LL * ((kStaticMaxNz + ncpa::kCkRows - 1) / ncpa::kCkRows) * 32,
+              "checkpoint slots cover the coarse sums of the largest grid");
 constexpr int kStaticItems = (kStaticMaxModes + ncpa::kEvItem - 1) / ncpa::kEvItem;
 
 // byte layout of the scratch array
@@ -149,7 +151,7 @@ extern "C" ncpa_status ncpa_eigvec_static(const double* s, const double* w, int 
     a.ck_q1 = reinterpret_cast<double*>(base + kOffQ1);
     a.ck_q2 = reinterpret_cast<double*>(base + kOffQ2);
     a.ck_e = reinterpret_cast<int*>(base + kOffE);
-    a.ck_slot_stride = (long long)((nz + ncpa::kBlk - 1) / ncpa::kBlk) * 32;
+    a.ck_slot_stride = ncpa::ck_slot_elems(nz);
     a.err = reinterpret_cast<unsigned*>(base + kOffCounter) + 1;
     ncpa::launch_eigvec(st, kStaticWarps / ncpa::kEvWarpsPerCta, a);
     if (cudaGetLastError() != cudaSuccess) return NCPA_ECUDA;

@@ -34,6 +34,7 @@ EXPORTED = [
     "ncpa_ess_plan_create", "ncpa_ess_plan_run", "ncpa_ess_plan_modes", "ncpa_ess_plan_tl", "ncpa_ess_plan_tuning",
     "ncpa_ess_plan_destroy", "ncpa_profile_update", "ncpa_g2s_convert", "ncpa_profile_load_g2s",
     "ncpa_dispersion_read", "ncpa_dispersion_desc_get", "ncpa_dispersion_destroy", "ncpa_ctx_sum_fixups",
+    "ncpa_tl_1d_range", "ncpa_modes_from_host",
 ]
 
 
@@ -571,23 +572,28 @@ class Plan:
 # ---------------------------------------------------------------------------
 class _ServerOpts(ctypes.Structure):
     _fields_ = [("device", _c_int), ("params", EssParams), ("n_ranges", _c_int), ("dr_m", _c_double),
-                ("lanes", _c_int), ("max_batch_problems", _c_int), ("hbm_budget_bytes", _c_double)]
+                ("lanes", _c_int), ("max_batch_problems", _c_int), ("hbm_budget_bytes", _c_double),
+                ("cache_bytes", _c_double)]
 
 
 class _Request(ctypes.Structure):
-    _fields_ = [("profile", _ProfileDesc), ("freqs", _dp), ("n_freq", _c_int), ("az_deg", _c_double)]
+    _fields_ = [("profile", _ProfileDesc), ("freqs", _dp), ("n_freq", _c_int), ("az_deg", _c_double),
+                ("n_ranges", _c_int), ("dr_m", _c_double), ("n_wave_ranges", _c_int), ("wave_ranges_m", _dp),
+                ("max_celerity", _c_double), ("nfft", _c_int), ("source", _c_int)]
 
 
 class _Result(ctypes.Structure):
     _fields_ = [("status", _c_int), ("n_freq", _c_int), ("mode_off", _ip), ("re_k", _dp), ("im_k", _dp),
                 ("v_src", _dp), ("v_rcv", _dp), ("tl_re", _dp), ("tl_im", _dp), ("tl_incoh", _dp),
-                ("latency_ms", _c_double), ("batch_requests", _c_int)]
+                ("latency_ms", _c_double), ("batch_requests", _c_int), ("n_ranges", _c_int),
+                ("n_wave_ranges", _c_int), ("nfft", _c_int), ("waveforms", _dp), ("from_cache", _c_int)]
 
 
 class _ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong), ("batches", ctypes.c_longlong),
                 ("mean_batch_requests", _c_double), ("p50_ms", _c_double), ("p99_ms", _c_double),
-                ("max_ms", _c_double), ("peak_admitted_bytes", _c_double)]
+                ("max_ms", _c_double), ("peak_admitted_bytes", _c_double), ("cache_hits", ctypes.c_longlong),
+                ("cache_entries", ctypes.c_longlong), ("cache_used_bytes", _c_double)]
 
 
 _SERVER_SIGS = False
@@ -611,10 +617,15 @@ def _server_sigs():
 
 class Server:
     """Serving loop: submit requests (profile knots in SI, frequencies,
-    azimuth) at any time; each returns dispersion and 1-D TL."""
+    azimuth, optionally their own TL range grid and waveform ranges) at any
+    time; each returns dispersion, 1-D TL and, when asked, waveforms.  With
+    cache_bytes > 0 solved modes stay in HBM and repeated requests skip the
+    eigen-solve."""
+
+    SOURCES = {"impulse": 0, "pulse1": 1, "pulse2": 2}
 
     def __init__(self, device=0, params=None, n_ranges=2000, dr_m=500.0, lanes=2, max_batch_problems=1024,
-                 hbm_budget_bytes=0.0):
+                 hbm_budget_bytes=0.0, cache_bytes=0.0):
         _server_sigs()
         o = _ServerOpts()
         lib().ncpa_server_opts_default(ctypes.byref(o))
@@ -623,17 +634,21 @@ class Server:
             o.params = params
         o.n_ranges, o.dr_m, o.lanes = int(n_ranges), float(dr_m), int(lanes)
         o.max_batch_problems, o.hbm_budget_bytes = int(max_batch_problems), float(hbm_budget_bytes)
+        o.cache_bytes = float(cache_bytes)
         self.n_ranges = int(n_ranges)
         self.h = _vp()
         st = lib().ncpa_server_create(ctypes.byref(o), ctypes.byref(self.h))
         if st != 0:
             raise NcpaError(st, "ncpa_server_create")
 
-    def submit(self, z, u, v, t, p, rho, freqs, az_deg, z0=None):
+    def submit(self, z, u, v, t, p, rho, freqs, az_deg, z0=None, n_ranges=0, dr_m=0.0, wave_ranges_m=None,
+               max_celerity=0.0, nfft=0, source="pulse1"):
         arrs = [_f64(x) for x in (z, u, v, t, p, rho)]
         f = _f64(np.atleast_1d(freqs))
         d = _ProfileDesc(len(arrs[0]), *[_p(a) for a in arrs], None, None, float(z0 or 0.0), int(z0 is not None))
-        req = _Request(d, _p(f), len(f), float(az_deg))
+        wr = _f64(wave_ranges_m) if wave_ranges_m is not None else None
+        req = _Request(d, _p(f), len(f), float(az_deg), int(n_ranges), float(dr_m), len(wr) if wr is not None else 0,
+                       _p(wr) if wr is not None else None, float(max_celerity), int(nfft), self.SOURCES[source])
         rid = ctypes.c_ulonglong()
         st = lib().ncpa_server_submit(self.h, ctypes.byref(req), ctypes.byref(rid))
         if st != 0:
@@ -645,8 +660,9 @@ class Server:
         st = lib().ncpa_server_wait(self.h, ctypes.c_ulonglong(rid), int(timeout_ms), ctypes.byref(r))
         if st != 0:
             raise NcpaError(st, "ncpa_server_wait")
-        nf, nr = r.n_freq, self.n_ranges
-        out = {"status": r.status, "latency_ms": r.latency_ms, "batch_requests": r.batch_requests}
+        nf, nr = r.n_freq, r.n_ranges
+        out = {"status": r.status, "latency_ms": r.latency_ms, "batch_requests": r.batch_requests,
+               "from_cache": bool(r.from_cache)}
         if r.status == 0:
             off = np.ctypeslib.as_array(r.mode_off, shape=(nf + 1,)).copy()
             nm = int(off[-1])
@@ -656,6 +672,9 @@ class Server:
                 out[k] = np.ctypeslib.as_array(ptr, shape=(nm,)).copy() if nm else np.empty(0)
             for k in ("tl_re", "tl_im", "tl_incoh"):
                 out[k] = np.ctypeslib.as_array(getattr(r, k), shape=(nf * nr,)).copy().reshape(nf, nr)
+            if r.n_wave_ranges > 0:
+                out["waveforms"] = np.ctypeslib.as_array(r.waveforms, shape=(r.n_wave_ranges * r.nfft,)).copy() \
+                    .reshape(r.n_wave_ranges, r.nfft)
         if release:
             lib().ncpa_server_release(self.h, ctypes.c_ulonglong(rid))
         return out

@@ -110,3 +110,96 @@ def test_tight_hbm_budget_admits_one_request_at_a_time(gpu):
     assert all(r["status"] == 0 for r in res)
     assert all(r["batch_requests"] == 1 for r in res)
     assert st["batches"] == len(jobs)
+
+
+def _alone_grid(gpu, prof, freqs, az, nr, dr):
+    p = gpu.profile_from_arrays(*prof)
+    m = gpu.solve(p, _params(), freqs, [az])
+    re, im, inc = m.tl1d(nr, dr)
+    return p, m, re, im, inc
+
+
+def test_per_request_range_grids_and_waveforms(gpu):
+    """Each request's own TL range grid, and waveforms for broadband
+    requests, equal the same request solved alone (synthesis of the solve's
+    own dispersion, ModBB's built-in pulse)."""
+    import ncpa_gpu
+
+    jobs = _jobs(31, 9)
+    grids = [(0, 0.0), (150, 3000.0), (NR, DR), (420, 1000.0)]
+    with ncpa_gpu.Server(0, params=_params(), n_ranges=NR, dr_m=DR, lanes=2) as srv:
+        ids = []
+        for k, (prof, freqs, az) in enumerate(jobs):
+            nr, dr = grids[k % len(grids)]
+            wr = np.array([80e3, 140e3]) if len(freqs) > 1 else None
+            ids.append(srv.submit(*prof, freqs, az, n_ranges=nr, dr_m=dr, wave_ranges_m=wr, max_celerity=330.0))
+        res = [srv.wait(i, timeout_ms=120000) for i in ids]
+    n_wave = 0
+    for k, ((prof, freqs, az), r) in enumerate(zip(jobs, res)):
+        assert r["status"] == 0 and not r["from_cache"]
+        nr, dr = grids[k % len(grids)]
+        if nr == 0:
+            nr, dr = NR, DR
+        p, m, re, im, inc = _alone_grid(gpu, prof, freqs, az, nr, dr)
+        assert r["tl_re"].shape == (len(freqs), nr)
+        assert np.array_equal(r["tl_re"], re) and np.array_equal(r["tl_im"], im)
+        assert np.array_equal(r["tl_incoh"], inc)
+        if len(freqs) > 1:
+            n_wave += 1
+            f = np.concatenate([[0.0], freqs])
+            nfft = 4 * len(f)
+            sre, sim = gpu.source_spectrum_builtin("pulse1", f, nfft)
+            w = m.bb_synthesize(np.array([80e3, 140e3]), 330.0, nfft, sre, sim)
+            assert r["waveforms"].shape == w.shape
+            assert np.linalg.norm(r["waveforms"] - w) <= 1e-12 * np.linalg.norm(w)
+        else:
+            assert "waveforms" not in r
+        m.close()
+        p.close()
+    assert n_wave > 0
+
+
+def test_mode_cache_skips_the_solve_and_equals_a_fresh_one(gpu):
+    """With a cache, a repeated request is served from its modes kept in HBM
+    (no eigen-solve) and gives the fresh result bit for bit, on its own range
+    grid too; a changed profile is not a hit."""
+    import ncpa_gpu
+
+    jobs = _jobs(41, 6)
+    with ncpa_gpu.Server(0, params=_params(), n_ranges=NR, dr_m=DR, lanes=2, cache_bytes=float(1 << 30)) as srv:
+        first = [srv.wait(srv.submit(*prof, freqs, az), timeout_ms=120000) for prof, freqs, az in jobs]
+        again = [srv.wait(srv.submit(*prof, freqs, az), timeout_ms=120000) for prof, freqs, az in jobs]
+        grid = [srv.wait(srv.submit(*prof, freqs, az, n_ranges=77, dr_m=3500.0), timeout_ms=120000)
+                for prof, freqs, az in jobs]
+        prof, freqs, az = jobs[0]
+        changed = list(prof)
+        changed[3] = changed[3] + 0.5  # temperature
+        other = srv.wait(srv.submit(*changed, freqs, az), timeout_ms=120000)
+        st = srv.stats()
+    assert all(not r["from_cache"] for r in first)
+    assert all(r["from_cache"] for r in again) and all(r["from_cache"] for r in grid)
+    assert not other["from_cache"]
+    assert st["cache_hits"] == 2 * len(jobs) and st["cache_entries"] == len(jobs) + 1
+    for a, b in zip(first, again):
+        for k in ("mode_off", "re_k", "im_k", "v_src", "v_rcv", "tl_re", "tl_im", "tl_incoh"):
+            assert np.array_equal(a[k], b[k]), k
+    for (prof, freqs, az), r in zip(jobs, grid):
+        p, m, re, im, inc = _alone_grid(gpu, prof, freqs, az, 77, 3500.0)
+        assert np.array_equal(r["tl_re"], re) and np.array_equal(r["tl_im"], im)
+        m.close()
+        p.close()
+
+
+def test_mode_cache_evicts_within_its_budget(gpu):
+    import ncpa_gpu
+
+    jobs = _jobs(43, 8)
+    with ncpa_gpu.Server(0, params=_params(), n_ranges=NR, dr_m=DR, lanes=2, cache_bytes=60e3) as srv:
+        res = [srv.wait(srv.submit(*prof, freqs, az), timeout_ms=120000) for prof, freqs, az in jobs]
+        again = [srv.wait(srv.submit(*prof, freqs, az), timeout_ms=120000) for prof, freqs, az in jobs]
+        st = srv.stats()
+    assert st["cache_used_bytes"] <= 60e3
+    assert st["cache_entries"] < len(jobs)
+    for a, b in zip(res, again):
+        assert b["status"] == 0
+        assert np.array_equal(a["tl_re"], b["tl_re"]) and np.array_equal(a["re_k"], b["re_k"])

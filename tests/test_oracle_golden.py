@@ -5,9 +5,23 @@ Fixtures (tests/golden/, made by make_golden.py from the reference tree):
     incoherent TL).  The file predates the reference's 2.0.1 scaling change
     (modal sums x 1000), so levels differ by exactly +60 dB.
   * ModBB dispersion files (canonical profile, azimuth 90): mode counts at
-    every frequency and Re k / Im k / V_s V_r at a few frequencies.  Both
-    files come from older releases; Im k follows an older attenuation and is
-    only checked for order of magnitude.
+    every frequency and Re k / Im k / V_s V_r at a few frequencies.
+
+Both come from older releases.  Each allowance below is the measured
+difference with its cause:
+  * TL: the complex pressure differs by at most 8.8e-4 of the modal terms'
+    magnitude S = sum_m |V_s V_r e^{i k r} / sqrt(k)| at every range (bound
+    1e-3); in dB this stays below 0.08 dB wherever |P| > 0.05 S and grows only
+    in cancellation nulls.  Median 0.007 dB.
+  * Mode counts: equal at every frequency except the ones listed in
+    EXTRA_MODE, where the oracle (like the current reference) keeps one more
+    mode, lying within 2.6e-4 of k_min: the older release cut the window
+    differently at k_min.
+  * Re k within 2e-5 relative at 0.002 Hz (two modes) and 1e-5 above;
+    V_s V_r within 4e-5 of the largest.
+  * Im k: the older release's attenuation gives Im k that the current formula
+    reproduces to a factor 0.986 on most modes (median ratio 0.986-0.987 from
+    0.1 Hz up, 0.89 at 0.002 Hz; every ratio between 0.66 and 0.99).
 """
 import os
 
@@ -15,6 +29,10 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN
+
+# frequency indices where the older file has one mode fewer (the extra mode
+# within 2.6e-4 of k_min), measured over every frequency of each file
+EXTRA_MODE = {"s256": [136, 201], "manual": [66, 113, 160, 221, 235]}
 
 
 @pytest.fixture(scope="module")
@@ -25,43 +43,43 @@ def canon(canonical_profile):
     return O, prm, O.prepare(O.read_profile(canonical_profile), prm)
 
 
-def test_tl_modess_0p1hz(canonical_profile):
-    from oracle import oracle as O
-
+def test_tl_modess_0p1hz(canon):
+    O, prm, pp = canon
     g = np.load(os.path.join(GOLDEN, "modess_tloss_1d.npz"))["lossy"]
+    assert np.allclose(g[:, 0], np.arange(1, 1001))
     # the manual's run used --write_2d_tloss, which turns the WKB cut off
-    prm = O.EssParams(forces_no_wkb=True)
-    ms = O.solve_problem(O.prepare(O.read_profile(canonical_profile), prm), prm, 0.1, 90.0)
+    ms = O.solve_problem(pp, prm, 0.1, 90.0)
     assert ms.M == 61
     re, im, inc = O.tl1d(ms, 1000, 1000.0)
-    tl = 20 * np.log10(np.hypot(re, im))
-    tlg = 20 * np.log10(np.hypot(g[:, 1], g[:, 2])) + 60.0
-    d = np.abs(tl - tlg)
-    assert np.median(d) < 0.02
-    assert np.percentile(d, 90) < 0.2
+    r = np.arange(1, 1001) * 1000.0
+    k = ms.kr + 1j * ms.ki
+    a = np.abs(ms.vs * ms.vr / np.sqrt(k))
+    S = np.array([np.sum(a * np.exp(-ms.ki * rr)) for rr in r]) * 1000.0 * 4 * np.pi / np.sqrt(8 * np.pi * r)
+    p = re + 1j * im
+    pg = (g[:, 1] + 1j * g[:, 2]) * 1000.0  # +60 dB
+    assert np.max(np.abs(p - pg) / S) < 1e-3
+    d = np.abs(20 * np.log10(np.abs(p)) - 20 * np.log10(np.abs(pg)))
+    assert np.median(d) < 0.01
+    away = np.abs(p) > 0.05 * S
+    assert away.mean() > 0.8 and d[away].max() < 0.08
     di = np.abs(20 * np.log10(inc) - (20 * np.log10(g[:, 3]) + 60.0))
     assert di.max() < 0.02
-    assert np.allclose(g[:, 0], np.arange(1, 1001))
 
 
 @pytest.mark.parametrize("key", ["s256", "manual"])
 def test_dispersion_mode_counts(canon, key):
-    """Mode counts at every frequency of the golden dispersion files.  Where
-    the counts differ, the extra mode sits within 3e-4 of k_min: the older
-    release placed the k_min cut differently."""
+    """Mode counts at every frequency of the golden dispersion files."""
     O, prm, pp = canon
     z = np.load(os.path.join(GOLDEN, "dispersion_goldens.npz"))
     f, M = z[key + "_f"], z[key + "_M"]
-    step = 3 if key == "s256" else 5
-    idx = sorted(set(range(0, len(f), step)) | {len(f) - 1})
-    mism = 0
-    for i in idx:
+    extra = []
+    for i in range(len(f)):
         ms = O.solve_problem(pp, prm, float(f[i]), 90.0)
         if ms.M != M[i]:
-            mism += 1
-            assert ms.M == M[i] + 1
-            assert (ms.kr[0] - ms.k_min) / ms.k_min < 3e-4
-    assert mism <= max(2, len(idx) // 25)
+            assert ms.M == M[i] + 1, (i, ms.M, M[i])
+            assert (ms.kr[0] - ms.k_min) / ms.k_min < 2.6e-4
+            extra.append(i)
+    assert extra == EXTRA_MODE[key]
 
 
 @pytest.mark.parametrize("key", ["s256", "manual"])
@@ -72,10 +90,13 @@ def test_dispersion_wavenumbers(canon, key):
     for j in z[key + "_pick"]:
         g = z["%s_modes_%d" % (key, j)]
         ms = O.solve_problem(pp, prm, float(f[j]), 90.0)
-        if ms.M != len(g):
-            continue
-        assert np.max(np.abs(ms.kr - g[:, 0]) / g[:, 0]) < 3e-5
+        assert ms.M == len(g), (j, ms.M, len(g))
+        assert np.max(np.abs(ms.kr - g[:, 0]) / g[:, 0]) < (2e-5 if f[j] < 0.01 else 1e-5)
         vv, gv = np.abs(ms.vs * ms.vr), np.abs(g[:, 2] * g[:, 3])
-        assert np.max(np.abs(vv - gv)) < 1e-4 * gv.max()
+        assert np.max(np.abs(vv - gv)) < 4e-5 * gv.max()
         ratio = ms.ki / g[:, 1]
-        assert 0.5 < np.median(ratio) < 1.5
+        assert 0.66 < ratio.min() and ratio.max() < 0.99
+        if f[j] >= 0.1:
+            assert 0.985 < np.median(ratio) < 0.988
+        else:
+            assert 0.88 < np.median(ratio) < 0.9
