@@ -125,12 +125,18 @@ def perturbed_profile(rng, dz_km=0.1):
     return z * 1000.0, u, v, T, p, rho
 
 
-def request_stream(n, rate_hz, seed=0):
+def request_stream(n, rate_hz, seed=0, dr_m=500.0):
     """n requests with Poisson arrivals at rate_hz: 80 % single frequency
     (log-uniform 0.05-2 Hz), 20 % broadband (32-256 frequencies, uniform
-    spacing f_max/n up to 0.5 Hz); azimuth uniform in [0, 360).  Yields dicts
-    with the arrival time [s], profile arrays, frequencies and azimuth."""
+    spacing f_max/n up to 0.5 Hz); azimuth uniform in [0, 360).  Each request
+    has its own range grid: dr_m spacing out to a maximum range uniform in
+    100-1000 km; broadband requests also ask for pulse waveforms at a third,
+    two thirds and all of that range.  Yields dicts with the arrival time [s],
+    profile arrays, frequencies, azimuth, n_ranges and wave_ranges_m (None for
+    single frequencies).  The grids come from a second generator, so the
+    other draws are those of the stream without them."""
     rng = np.random.default_rng(seed)
+    rng_grid = np.random.default_rng(seed + 7919)
     t = 0.0
     out = []
     for _ in range(n):
@@ -141,5 +147,9 @@ def request_stream(n, rate_hz, seed=0):
             nf = int(rng.integers(32, 257))
             freqs = 0.5 / nf * np.arange(1, nf + 1)
         az = rng.uniform(0.0, 360.0)
-        out.append({"t": t, "profile": perturbed_profile(rng), "freqs": freqs, "az": az})
+        r_max = rng_grid.uniform(100e3, 1000e3)
+        nr = max(1, int(round(r_max / dr_m)))
+        waves = np.array([1.0, 2.0, 3.0]) * (nr * dr_m / 3.0) if len(freqs) > 1 else None
+        out.append({"t": t, "profile": perturbed_profile(rng), "freqs": freqs, "az": az, "n_ranges": nr,
+                    "wave_ranges_m": waves})
     return out
