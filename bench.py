@@ -434,6 +434,7 @@ def modal_sum_leg(ctx, stream, bf16, k=10):
         return per["ms-tc"], per
 
     ms_call_g = timed(G, k)
+    sched_ts, sched_gs, sched_times = ctx.sum_schedule()
     ms_call = timed(X3, k)
     ms_call_tf32 = timed(T32, k)
     ms_fp64 = timed(F64, 2)
@@ -469,6 +470,9 @@ def modal_sum_leg(ctx, stream, bf16, k=10):
         "ms_per_call": round(ms_call_g, 4), "ms_kernel": round(ms_kernel_g, 4),
         "ms_fp64_cuda_cores": round(ms_fp64, 3), "phases_ms": phases_g,
         "recomputed_fp64": {"points": int(fixed), "of": int(points), "frac": fixed / max(points, 1)},
+        "schedule": {"tma_ring": int(sched_ts), "operand_ring": int(sched_gs),
+                     "variant_ms": [round(float(t), 4) for t in sched_times],
+                     "what": "ring depths picked by the autotuner (first call of the shape times every variant)"},
         "roofline": {"kernel": "k_ms_tc<guarded> (tcgen05 6-term split-BF16)", "bound": "tensor",
                      "achieved": round(achieved_g, 1), "peak": bf16_peak, "unit": "TFLOP/s",
                      "frac": round(achieved_g / bf16_peak, 4),

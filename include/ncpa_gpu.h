@@ -442,6 +442,13 @@ ncpa_status ncpa_ctx_sturm_steps(ncpa_ctx *ctx, long long *steps);
 /* Points the last NCPA_SUM_TC_GUARDED modal sum of this context recomputed
  * in FP64, and its receivers x ranges (waits for the context's stream). */
 ncpa_status ncpa_ctx_sum_fixups(ncpa_ctx *ctx, long long *recomputed, long long *points);
+/* Schedule of the last tensor-core modal sum of this context: the depths of
+ * its TMA ring and generated-operand ring.  The first tensor-core call of
+ * each shape (format, receiver groups, mode chunks, range tiles) times every
+ * schedule (variants of them, times_ms[v] in ms; the call waits for that)
+ * and the context keeps the fastest; NCPA_MS_TUNE=0 at context creation
+ * keeps the first (deepest rings).  Results do not depend on the schedule. */
+ncpa_status ncpa_ctx_sum_schedule(ncpa_ctx *ctx, int *t_stages, int *g_stages, int *variants, double *times_ms);
 /* Measured FP64 FMA throughput of this device [TFLOP/s, FMA = 2 flops]: a
  * dependent-FMA kernel on every SM for about 50 ms. */
 ncpa_status ncpa_probe_fp64_peak(ncpa_ctx *ctx, double *tflops);

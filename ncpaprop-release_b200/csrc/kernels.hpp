@@ -235,8 +235,12 @@ int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const do
 int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int M, const double* kr,
                       const double* ki, const double* vs, const int* idx, const double* vfull, double dr, int lossless,
                       void* a_img, void* q, void* tab, void* b64, void* tp64, void* a64);
+// variant: the schedule (ring depths) of the tensor-core kernel, 0 ..
+// ms_tc_variants() - 1 (0: the deepest rings); results do not depend on it
 int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const void* a_img, const void* q,
-                 const void* tab, float* raw, float* s_part, unsigned* err);
+                 const void* tab, float* raw, float* s_part, unsigned* err, int variant);
+int ms_tc_variants();
+void ms_tc_variant_shape(int fmt, int variant, int* t_stages, int* g_stages);
 // s_part non-NULL: flag the points the guarded sum must recompute into
 // fix_list / fix_count (zeroed by the caller)
 int launch_ms_finish(cudaStream_t st, const MsPlan& p, int n_rcv, int n_ranges, double dr, const float* raw,

@@ -93,8 +93,10 @@ constexpr double kMsGuardEps = 1.0e-6;
 // shared-memory plan of a format: a TMA stage holds the chunk's B' image
 // (kParts parts of 16 KB; TF32: one 32-bit image of the same size as two),
 // A as complex FP32 and the tile phases (1 KB aligned); a generated A' stage
-// holds kParts parts of 8 KB
-template <int F>
+// holds kParts parts of 8 KB.  TS / GS: depths of the TMA and generated-A'
+// rings (the schedule the autotuner picks among; the defaults are the
+// deepest that fit).
+template <int F, int TS = (F == kMsBf16x6 ? 3 : 4), int GS = (F == kMsBf16x6 ? 2 : 3)>
 struct MsCfg {
     static constexpr int kParts = F == kMsBf16x6 ? 3 : 2;
     static constexpr int kBChunk = kParts * kMsBBytes;   // B' image bytes per chunk
@@ -102,9 +104,9 @@ struct MsCfg {
     static constexpr int kOffQ = kOffAC + kMsACBytes;
     static constexpr int kTx = kBChunk + kMsACBytes + kMsQBytes;
     static constexpr int kTStageBytes = (kOffQ + kMsQBytes + 1023) / 1024 * 1024;
-    static constexpr int kTStages = F == kMsBf16x6 ? 3 : 4;
+    static constexpr int kTStages = TS;
     static constexpr int kGStageBytes = kParts * kMsABytes;
-    static constexpr int kGStages = F == kMsBf16x6 ? 2 : 3;
+    static constexpr int kGStages = GS;
     static constexpr int kOffGRing = kTStages * kTStageBytes;
     static constexpr int kSmem = kOffGRing + kGStages * kGStageBytes + 1024;
     static_assert(kSmem <= 232448 - 256, "shared memory per block");
@@ -419,9 +421,9 @@ struct UnitPos {
     }
 };
 
-template <int F>
+template <int F, int TS, int GS>
 __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
-    using C = MsCfg<F>;
+    using C = MsCfg<F, TS, GS>;
     constexpr int kTStages = C::kTStages, kGStages = C::kGStages;
     extern __shared__ unsigned char ms_dyn[];
     __shared__ __align__(8) uint64_t full_t[kMsMaxStages], empty_t[kMsMaxStages], full_g[kMsMaxStages],
@@ -900,20 +902,49 @@ int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int 
     return 1;
 }
 
+namespace {
+// the schedules of each format: (TMA ring depth, generated-A' ring depth)
+struct MsVariant {
+    const void* fn;
+    int smem, ts, gs;
+};
+template <int F, int TS, int GS>
+MsVariant ms_variant() {
+    return MsVariant{(const void*)k_ms_tc<F, TS, GS>, MsCfg<F, TS, GS>::kSmem, TS, GS};
+}
+constexpr int kMsVariants = 4;
+const MsVariant& ms_variant_of(int fmt, int v) {
+    static const MsVariant x3[kMsVariants] = {ms_variant<kMsBf16x3, 4, 3>(), ms_variant<kMsBf16x3, 3, 3>(),
+                                              ms_variant<kMsBf16x3, 4, 2>(), ms_variant<kMsBf16x3, 2, 3>()};
+    static const MsVariant tf[kMsVariants] = {ms_variant<kMsTf32, 4, 3>(), ms_variant<kMsTf32, 3, 3>(),
+                                              ms_variant<kMsTf32, 4, 2>(), ms_variant<kMsTf32, 2, 3>()};
+    static const MsVariant x6[kMsVariants] = {ms_variant<kMsBf16x6, 3, 2>(), ms_variant<kMsBf16x6, 2, 3>(),
+                                              ms_variant<kMsBf16x6, 2, 2>(), ms_variant<kMsBf16x6, 3, 1>()};
+    return fmt == kMsTf32 ? tf[v] : (fmt == kMsBf16x6 ? x6[v] : x3[v]);
+}
+}  // namespace
+
+int ms_tc_variants() { return kMsVariants; }
+
+void ms_tc_variant_shape(int fmt, int variant, int* t_stages, int* g_stages) {
+    const MsVariant& v = ms_variant_of(fmt, variant < 0 || variant >= kMsVariants ? 0 : variant);
+    *t_stages = v.ts;
+    *g_stages = v.gs;
+}
+
 int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const void* a_img, const void* q,
-                 const void* tab, float* raw, float* s_part, unsigned* err) {
+                 const void* tab, float* raw, float* s_part, unsigned* err, int variant) {
     if (p.n_units <= 0) return 0;
     if (fmt != kMsBf16x3 && fmt != kMsTf32 && fmt != kMsBf16x6) return -1;
-    auto kern = fmt == kMsTf32 ? k_ms_tc<kMsTf32> : (fmt == kMsBf16x6 ? k_ms_tc<kMsBf16x6> : k_ms_tc<kMsBf16x3>);
-    const int smem = fmt == kMsTf32 ? MsCfg<kMsTf32>::kSmem
-                                    : (fmt == kMsBf16x6 ? MsCfg<kMsBf16x6>::kSmem : MsCfg<kMsBf16x3>::kSmem);
-    static bool attr_set[3][64] = {};
+    if (variant < 0 || variant >= kMsVariants) return -1;
+    const MsVariant& var = ms_variant_of(fmt, variant);
+    static bool attr_set[3][kMsVariants][64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
-    if (!attr_set[fmt][dev]) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    if (!attr_set[fmt][variant][dev]) {
+        if (cudaFuncSetAttribute(var.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, var.smem) != cudaSuccess)
             return -1;
-        attr_set[fmt][dev] = true;  // setting it twice from two threads is harmless
+        attr_set[fmt][variant][dev] = true;  // setting it twice from two threads is harmless
     }
     MsArgs a;
     a.ac = (const float2*)a_img;
@@ -928,7 +959,9 @@ int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const 
     a.raw = raw;
     a.s_part = fmt == kMsBf16x6 ? s_part : nullptr;
     a.err = err;
-    kern<<<p.n_ctas, kMsThreads, smem, st>>>(a);
+    void* args[] = {&a};
+    if (cudaLaunchKernel(var.fn, dim3(p.n_ctas), dim3(kMsThreads), args, (size_t)var.smem, st) != cudaSuccess)
+        return -1;
     return 1;
 }
 

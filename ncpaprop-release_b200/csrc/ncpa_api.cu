@@ -116,6 +116,13 @@ struct ncpa_ctx {
     DevBuf ms_img, ms_q, ms_tab, ms_raw, ms_vz, ms_idx, ms_re, ms_im;  // modal-sum scratch (grow-only)
     DevBuf ms_spart, ms_b64, ms_tp64, ms_a64, ms_fix, ms_fixcnt;        // guarded sum: bounds, FP64 tables, flags
     long long ms_last_points = 0;  // receivers x ranges of the last guarded modal sum
+    // modal-sum schedule autotuner: (format, groups, chunks, tiles) -> the
+    // fastest ring-depth variant of the tensor-core kernel; NCPA_MS_TUNE=0
+    // keeps variant 0
+    bool ms_tune = true;
+    std::map<std::array<long long, 4>, int> ms_choice;
+    int ms_last_variant = 0, ms_last_fmt = 0;
+    std::vector<double> ms_last_times;  // per variant, ms, of the last tuning run
     int item_override = 0;         // eigenvalues per bisection item (0: chosen per solve); NCPA_BISECT_ITEM
     bool fuse_solve = true;        // fused bisection + eigenvector launch; NCPA_FUSE_SOLVE=0 turns it off
     // how long a consumer of the fused launch waits for an empty queue slot
@@ -1292,6 +1299,15 @@ ncpa_status ncpa_ctx_sum_fixups(ncpa_ctx* ctx, long long* recomputed, long long*
     });
 }
 
+ncpa_status ncpa_ctx_sum_schedule(ncpa_ctx* ctx, int* t_stages, int* g_stages, int* variants, double* times_ms) {
+    if (!ctx || !t_stages || !g_stages) return NCPA_EINVAL;
+    ncpa::ms_tc_variant_shape(ctx->ms_last_fmt, ctx->ms_last_variant, t_stages, g_stages);
+    if (variants) *variants = ncpa::ms_tc_variants();
+    if (times_ms)
+        for (size_t v = 0; v < ctx->ms_last_times.size(); ++v) times_ms[v] = ctx->ms_last_times[v];
+    return NCPA_OK;
+}
+
 ncpa_status ncpa_probe_fp64_peak(ncpa_ctx* ctx, double* tflops) {
     if (!ctx || !tflops) return NCPA_EINVAL;
     return guarded(ctx, [&]() -> ncpa_status {
@@ -1352,6 +1368,7 @@ ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
         ctx->timing = tv && tv[0] == '1';
         if (const char* fv = std::getenv("NCPA_FUSE_SOLVE")) ctx->fuse_solve = fv[0] != '0';
         if (const char* wv = std::getenv("NCPA_FUSE_WAIT_NS")) ctx->fuse_wait_ns = std::strtoull(wv, nullptr, 10);
+        if (const char* mv = std::getenv("NCPA_MS_TUNE")) ctx->ms_tune = mv[0] != '0';
         // tuning override of the eigenvalues per bisection item (1..32)
         if (const char* iv = std::getenv("NCPA_BISECT_ITEM")) {
             const int v = std::atoi(iv);
@@ -2021,10 +2038,46 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
                                                           guard ? ctx->ms_tp64.p : nullptr,
                                                           guard ? ctx->ms_a64.p : nullptr));
                 tm.mark("ms-prep");
-                check_launch(ctx, ncpa::launch_ms_tc(st, pl, fmt, nr, ctx->ms_img.p, ctx->ms_q.p, ctx->ms_tab.p,
-                                                     ctx->ms_raw.as<float>(),
-                                                     guard ? ctx->ms_spart.as<float>() : nullptr,
-                                                     ctx->d_err.as<unsigned>()));
+                auto tc = [&](int variant) {
+                    check_launch(ctx, ncpa::launch_ms_tc(st, pl, fmt, nr, ctx->ms_img.p, ctx->ms_q.p, ctx->ms_tab.p,
+                                                         ctx->ms_raw.as<float>(),
+                                                         guard ? ctx->ms_spart.as<float>() : nullptr,
+                                                         ctx->d_err.as<unsigned>(), variant));
+                };
+                // schedule: the fastest ring depths for this shape, timed
+                // once per context (each variant computes the same sums)
+                int variant = 0;
+                if (ctx->ms_tune) {
+                    const std::array<long long, 4> key{fmt, pl.groups, pl.n_chunks, pl.n_tiles};
+                    auto it = ctx->ms_choice.find(key);
+                    if (it == ctx->ms_choice.end()) {
+                        const int nv = ncpa::ms_tc_variants();
+                        std::vector<double> best_ms(nv, 0.0);
+                        cudaEvent_t e0, e1;
+                        CK(cudaEventCreate(&e0));
+                        CK(cudaEventCreate(&e1));
+                        int best = 0;
+                        for (int v = 0; v < nv; ++v) {
+                            tc(v);  // warm-up (function attributes, caches)
+                            CK(cudaEventRecord(e0, st));
+                            for (int r = 0; r < 3; ++r) tc(v);
+                            CK(cudaEventRecord(e1, st));
+                            CK(cudaEventSynchronize(e1));
+                            float ms = 0.f;
+                            CK(cudaEventElapsedTime(&ms, e0, e1));
+                            best_ms[v] = ms / 3.0;
+                            if (best_ms[v] < best_ms[best]) best = v;
+                        }
+                        cudaEventDestroy(e0);
+                        cudaEventDestroy(e1);
+                        it = ctx->ms_choice.emplace(key, best).first;
+                        ctx->ms_last_times = best_ms;
+                    }
+                    variant = it->second;
+                }
+                ctx->ms_last_variant = variant;
+                ctx->ms_last_fmt = fmt;
+                tc(variant);
                 tm.mark("ms-tc");
                 check_launch(ctx, ncpa::launch_ms_finish(st, pl, n_rcv, nr, tp->dr_m, ctx->ms_raw.as<float>(),
                                                          ctx->ms_re.as<double>(), ctx->ms_im.as<double>(),

@@ -142,3 +142,28 @@ def test_guarded_sum_is_reproducible(solved):
     a = m.tl_multi(0, h, 800, 500.0, method=m.SUM_TC_GUARDED)
     b = m.tl_multi(0, h, 800, 500.0, method=m.SUM_TC_GUARDED)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("method", [1, 2, 3])
+def test_schedule_autotuner_keeps_the_sums(solved, method, monkeypatch):
+    """The first tensor-core call of a shape times every ring-depth schedule
+    and keeps the fastest; whatever it picks, the sums equal those of a
+    context that keeps the default schedule (NCPA_MS_TUNE=0), bit for bit."""
+    import ncpa_gpu
+
+    m, g, v, nz = solved
+    h = _heights(70, g.dz)
+    tuned = m.tl_multi(0, h, 900, 500.0, method=method)
+    ts, gs, times = m.ctx.sum_schedule()
+    assert len(times) >= 2 and np.all(times > 0) and ts >= 2 and gs >= 1
+    monkeypatch.setenv("NCPA_MS_TUNE", "0")
+    own = m.ctx
+    with ncpa_gpu.Context(0) as plain_ctx:
+        m.ctx = plain_ctx  # the same modes, summed on a context that does not tune
+        try:
+            plain = m.tl_multi(0, h, 900, 500.0, method=method)
+            ts0, gs0, _ = plain_ctx.sum_schedule()
+        finally:
+            m.ctx = own
+    assert (ts0, gs0) == ((3, 2) if method == 3 else (4, 3))
+    assert np.array_equal(tuned, plain)
