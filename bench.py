@@ -296,7 +296,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     ctx.set_timing(False)
     bis_ms, bis_n = ctx.phase_stats("bisect")
-    sturm_steps = ctx.sturm_steps()
+    sturm_steps, deriv_steps = ctx.bisect_steps()
     phases = {ph: ctx.phase_stats(ph)[0] / n_ph for ph in
               ("knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec", "fetch")}
     if args.quick:
@@ -335,9 +335,10 @@ def run_ours(args):
         solves = NFREQ * args.steps * world
         value = solves / (ms_dev / 1e3)
         e2e_value = solves / (ms_e2e / 1e3)
-        # bisection kernel roofline: 3 FP64 flops per Sturm step (subtract +
-        # fused multiply-add), steps counted by the kernel
-        flops = 3.0 * sturm_steps  # over the bis_n timed launches
+        # bisection kernel roofline, steps counted by the kernel: 3 FP64 flops
+        # per step of a count-only chain (subtract + fused multiply-add), 10
+        # per step of a Laguerre chain (p, p', p'': subtract, four FMAs, one add)
+        flops = 3.0 * (sturm_steps - deriv_steps) + 10.0 * deriv_steps  # over the bis_n timed launches
         achieved = flops / (bis_ms / 1e3) / 1e12 if bis_ms > 0 else None
         cpu = cpu_baseline(freqs, max_seconds=args.cpu_seconds)
         cpu_lapack = lapack_baseline(freqs) if not args.no_lapack else None
@@ -363,7 +364,10 @@ def run_ours(args):
                          "peak_source": "measured in this run (dependent-FMA probe on all SMs)",
                          "traffic": None, "traffic_source": "not measured by this run (DRAM counters need ncu)",
                          "avg_launch_ms": round(bis_ms / max(bis_n, 1), 4),
-                         "flops_per_launch": flops / bis_n if bis_n else None},
+                         "flops_per_launch": flops / bis_n if bis_n else None,
+                         "flops": "3 per count-chain step, 10 per Laguerre-chain step (p, p', p'')",
+                         "chain_steps_per_launch": sturm_steps / bis_n if bis_n else None,
+                         "laguerre_chain_steps_per_launch": deriv_steps / bis_n if bis_n else None},
             "phases_ms": {k: round(v, 4) for k, v in phases.items()},
             "plain_gpu": {"value": round(plain_rate, 2), "unit": METRIC,
                           "what": "one ncpa_ess_solve + TL per frequency, same workload"},
@@ -609,10 +613,10 @@ def wmod_leg(ctx, stream, prof, freqs, az, fp64_peak, flush, cpu_seconds, k=5):
     torch.cuda.synchronize()
     ctx.set_timing(False)
     bis_ms, bis_n = ctx.phase_stats("bisect")
-    steps = ctx.sturm_steps()
+    steps, dsteps = ctx.bisect_steps()
     phases = {ph: round(ctx.phase_stats(ph)[0] / n_ph, 4) for ph in
               ("knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec", "fetch")}
-    flops = 6.0 * steps
+    flops = 6.0 * (steps - dsteps) + 12.0 * dsteps
     achieved = flops / (bis_ms / 1e3) / 1e12 if bis_ms > 0 else None
     # CPU: the oracle's WMod restatement on a stratified sample
     O, pp, prm = _oracle_setup()
@@ -634,7 +638,7 @@ def wmod_leg(ctx, stream, prof, freqs, az, fp64_peak, flush, cpu_seconds, k=5):
                      "achieved": round(achieved, 3) if achieved else None,
                      "peak": round(fp64_peak, 3) if fp64_peak else None, "unit": "TFLOP/s",
                      "frac": round(achieved / fp64_peak, 4) if achieved and fp64_peak else None,
-                     "flops": "6 per counted chain step (3 FMA; derivative FMAs not counted)",
+                     "flops": "6 per count-chain step (3 FMA), 12 per Newton-chain step (with the derivative)",
                      "avg_launch_ms": round(bis_ms / max(bis_n, 1), 4)},
         "cpu_baseline": {"value": round(done / el, 3), "unit": METRIC, "cores": O.lib().orc_num_threads(),
                          "kind": "port",

@@ -439,6 +439,9 @@ ncpa_status ncpa_ctx_set_timing(ncpa_ctx *ctx, int on);
 ncpa_status ncpa_ctx_phase_stats(const ncpa_ctx *ctx, const char *phase, double *total_ms, long long *calls);
 ncpa_status ncpa_ctx_reset_stats(ncpa_ctx *ctx);
 ncpa_status ncpa_ctx_sturm_steps(ncpa_ctx *ctx, long long *steps);
+/* the same steps, and how many of them belong to chains that also carry
+ * derivatives (the Laguerre / Newton chains of the isolated eigenvalues) */
+ncpa_status ncpa_ctx_bisect_steps(ncpa_ctx *ctx, long long *steps, long long *deriv_steps);
 /* Points the last NCPA_SUM_TC_GUARDED modal sum of this context recomputed
  * in FP64, and its receivers x ranges (waits for the context's stream). */
 ncpa_status ncpa_ctx_sum_fixups(ncpa_ctx *ctx, long long *recomputed, long long *points);

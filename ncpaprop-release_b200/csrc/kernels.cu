@@ -1085,8 +1085,12 @@ __device__ __forceinline__ void bisect_item(const ProblemInfo* __restrict__ pinf
         double rat, hq;
         const int smode = nN == 0 ? 0 : (nB > 0 ? 1 : 2);
         warp_sweep_tw<Row>(sp, nz, p_init, xv[0], xv[1], smode, r, err, cv0, cv1, rat, hq);
-        if (step_counter && lane == 0)
+        if (step_counter && lane == 0) {
+            // [0]: chain steps of every kind; [1]: steps of chains carrying
+            // derivatives (Laguerre / Newton chains: 32 per sweep in modes 1, 2)
             atomicAdd(step_counter, (unsigned long long)(smode == 2 ? 32 : 64) * (unsigned long long)nz);
+            if (smode >= 1) atomicAdd(step_counter + 1, 32ull * (unsigned long long)nz);
+        }
         // updates.  Every __shfl_sync is executed by all 32 lanes.
         const bool isN = mode == 1, isB = mode == 0;
         const int vN = isN ? __popc(nm & ((1u << lane) - 1u)) : 0;  // Newton virtual lane (chain 0)

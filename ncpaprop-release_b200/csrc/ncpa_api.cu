@@ -1285,6 +1285,18 @@ ncpa_status ncpa_ctx_sturm_steps(ncpa_ctx* ctx, long long* steps) {
     });
 }
 
+ncpa_status ncpa_ctx_bisect_steps(ncpa_ctx* ctx, long long* steps, long long* deriv_steps) {
+    if (!ctx || !steps || !deriv_steps) return NCPA_EINVAL;
+    return guarded(ctx, [&]() -> ncpa_status {
+        unsigned long long h[2] = {0, 0};
+        CK(cudaMemcpyAsync(h, ctx->d_stats.p, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        *steps = (long long)h[0];
+        *deriv_steps = (long long)h[1];
+        return NCPA_OK;
+    });
+}
+
 ncpa_status ncpa_ctx_sum_fixups(ncpa_ctx* ctx, long long* recomputed, long long* points) {
     if (!ctx || !recomputed || !points) return NCPA_EINVAL;
     return guarded(ctx, [&]() -> ncpa_status {

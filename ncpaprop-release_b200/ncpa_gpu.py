@@ -34,7 +34,7 @@ EXPORTED = [
     "ncpa_ess_plan_create", "ncpa_ess_plan_run", "ncpa_ess_plan_modes", "ncpa_ess_plan_tl", "ncpa_ess_plan_tuning",
     "ncpa_ess_plan_destroy", "ncpa_profile_update", "ncpa_g2s_convert", "ncpa_profile_load_g2s",
     "ncpa_dispersion_read", "ncpa_dispersion_desc_get", "ncpa_dispersion_destroy", "ncpa_ctx_sum_fixups",
-    "ncpa_tl_1d_range", "ncpa_modes_from_host", "ncpa_ctx_sum_schedule",
+    "ncpa_tl_1d_range", "ncpa_modes_from_host", "ncpa_ctx_sum_schedule", "ncpa_ctx_bisect_steps",
 ]
 
 
@@ -180,6 +180,7 @@ def lib():
         L.ncpa_ctx_sturm_steps.argtypes = [_vp, ctypes.POINTER(_c_ll)]
         L.ncpa_ctx_sum_fixups.argtypes = [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]
         L.ncpa_ctx_sum_schedule.argtypes = [_vp, _ip, _ip, _ip, _dp]
+        L.ncpa_ctx_bisect_steps.argtypes = [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]
         L.ncpa_probe_fp64_peak.argtypes = [_vp, _dp]
         L.ncpa_source_spectrum_builtin.argtypes = [_vp, _c_int, _dp, _c_int, _c_double, _c_int, _dp, _dp]
         _lib = L
@@ -278,6 +279,14 @@ class Context:
         self.check(lib().ncpa_ctx_sum_schedule(self.h, ctypes.byref(t), ctypes.byref(g), ctypes.byref(n),
                                                _p(times)), "ncpa_ctx_sum_schedule")
         return t.value, g.value, times[:n.value].copy()
+
+    def bisect_steps(self):
+        """(all Sturm chain steps, steps of the chains carrying derivatives)
+        of the bisection kernel since the last reset (counted while per-phase
+        timing is on)"""
+        a, b = _c_ll(), _c_ll()
+        self.check(lib().ncpa_ctx_bisect_steps(self.h, ctypes.byref(a), ctypes.byref(b)), "ncpa_ctx_bisect_steps")
+        return a.value, b.value
 
     def fp64_peak_tflops(self):
         t = _c_double()
