@@ -2238,13 +2238,18 @@ int launch_bisect_eigvec_wmod(cudaStream_t st, int grid, const FusedArgs& a) {
 
 // ===========================================================================
 // K5: 1-D transmission loss, modes staged in shared memory.  Each thread
-// covers kTlRun consecutive ranges: per mode the phase k r of its first range
-// is formed in FP64 (sincos, exp), the next ones follow by the per-mode step
-// e^{(i k_r - k_i) dr} (a few ulps after kTlRun - 1 complex products).
+// covers kTlRun consecutive ranges: per mode the phase of its first range is
+// e^{(i k_r - k_i) r_b} (the block's first range, one sincos per mode and
+// block) times the powers e^{(i k_r - k_i) kTlRun dr 2^b} for the set bits b
+// of the thread index (each from its own sincos, staged per mode), and the
+// next ranges follow by the per-mode step e^{(i k_r - k_i) dr}: at most
+// kTlBits + kTlRun - 1 complex products, a few ulps each.
 // ===========================================================================
 constexpr int kTlTile = 128;
 constexpr int kTlRun = 4;      // consecutive ranges per thread
 constexpr int kTlThreads = 256;
+constexpr int kTlBits = 8;     // thread index bits (kTlThreads = 2^kTlBits)
+static_assert(kTlThreads == 1 << kTlBits, "the powers cover every thread index");
 
 __global__ void __launch_bounds__(kTlThreads) k_tl1d(const ProblemInfo* __restrict__ pinfo,
                                                      const double* __restrict__ kr, const double* __restrict__ ki,
@@ -2254,9 +2259,10 @@ __global__ void __launch_bounds__(kTlThreads) k_tl1d(const ProblemInfo* __restri
     const int p = blockIdx.y;
     const int i0 = (blockIdx.x * kTlThreads + threadIdx.x) * kTlRun;  // first range of this thread
     const ProblemInfo pi = pinfo[p];
-    __shared__ double m_kr[kTlTile], m_ki[kTlTile], m_vv[kTlTile], m_sr[kTlTile], m_si[kTlTile], m_ia[kTlTile];
-    __shared__ double m_wr[kTlTile], m_wi[kTlTile];
-    const double r0 = (i0 + 1) * dr;
+    __shared__ double m_vv[kTlTile], m_sr[kTlTile], m_si[kTlTile], m_ia[kTlTile];
+    __shared__ double m_wr[kTlTile], m_wi[kTlTile], m_br[kTlTile], m_bi[kTlTile];
+    __shared__ double2 m_pw[kTlBits][kTlTile];
+    const double rb = ((double)blockIdx.x * kTlThreads * kTlRun + 1.0) * dr;  // the block's first range
     double sre[kTlRun], sim[kTlRun], sinc[kTlRun];
 #pragma unroll
     for (int j = 0; j < kTlRun; ++j) sre[j] = sim[j] = sinc[j] = 0.0;
@@ -2268,8 +2274,6 @@ __global__ void __launch_bounds__(kTlThreads) k_tl1d(const ProblemInfo* __restri
             // 1/sqrt(k): principal root of k, then the reciprocal
             const auto sk = csqrt_principal(a, b);
             const double den = sk.real() * sk.real() + sk.imag() * sk.imag();
-            m_kr[t] = a;
-            m_ki[t] = b;
             m_vv[t] = vs[o] * vr[o];
             m_sr[t] = sk.real() / den;
             m_si[t] = -sk.imag() / den;
@@ -2279,17 +2283,36 @@ __global__ void __launch_bounds__(kTlThreads) k_tl1d(const ProblemInfo* __restri
             const double w = exp(-b * dr);
             m_wr[t] = w * cs;
             m_wi[t] = w * sn;
+            sincos(a * rb, &sn, &cs);
+            const double wb = exp(-b * rb);
+            m_br[t] = wb * cs;
+            m_bi[t] = wb * sn;
+#pragma unroll
+            for (int bit = 0; bit < kTlBits; ++bit) {
+                const double x = (double)(kTlRun << bit) * dr;
+                sincos(a * x, &sn, &cs);
+                const double wp = exp(-b * x);
+                m_pw[bit][t] = make_double2(wp * cs, wp * sn);
+            }
         }
         __syncthreads();
         const int mt = min(kTlTile, pi.M - m0);
         if (i0 < nr) {
             for (int t = 0; t < mt; ++t) {
-                double sn, cs;
-                sincos(m_kr[t] * r0, &sn, &cs);
-                const double amp = exp(-m_ki[t] * r0);
+                // e^{i k r} at this thread's first range: the block's phase
+                // times the powers of the thread index's set bits
+                double er = m_br[t], ei = m_bi[t];
+#pragma unroll
+                for (int bit = 0; bit < kTlBits; ++bit) {
+                    if ((threadIdx.x >> bit) & 1) {
+                        const double2 q = m_pw[bit][t];
+                        const double nr_ = er * q.x - ei * q.y;
+                        ei = er * q.y + ei * q.x;
+                        er = nr_;
+                    }
+                }
                 const double vv = m_vv[t], sr = m_sr[t], si = m_si[t], ia = m_ia[t];
                 const double wr = m_wr[t], wi = m_wi[t];
-                double er = amp * cs, ei = amp * sn;  // e^{i k r} at the current range
 #pragma unroll
                 for (int j = 0; j < kTlRun; ++j) {
                     const double ar = vv * er, ai = vv * ei;
