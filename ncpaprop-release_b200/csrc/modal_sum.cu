@@ -836,9 +836,14 @@ __global__ void __launch_bounds__(256) k_ms_fix(const int* __restrict__ fix_coun
                                                 const double2* __restrict__ b64, double* __restrict__ re,
                                                 double* __restrict__ im) {
     const int lane = threadIdx.x & 31;
-    const int warps = gridDim.x * (blockDim.x >> 5);
+    const int wpc = blockDim.x >> 5;
     const int cnt = *fix_count;
-    for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < cnt; w += warps) {
+    // each CTA takes a contiguous block of the list: neighbouring entries
+    // come from one finishing warp (one receiver, one tile), so their A and
+    // tile-phase rows are shared through L1
+    const int per_cta = (cnt + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int w0 = blockIdx.x * per_cta, w1 = min(w0 + per_cta, cnt);
+    for (int w = w0 + (threadIdx.x >> 5); w < w1; w += wpc) {
         const int2 pt = fix_list[w];
         const int j = pt.x, n = pt.y;
         const int tile = n / kMsNT, o = n % kMsNT;
@@ -847,7 +852,7 @@ __global__ void __launch_bounds__(256) k_ms_fix(const int* __restrict__ fix_coun
         const double2* br = b64 + (size_t)o * M_pad;
         double sre = 0.0, sim = 0.0;
         for (int m = lane; m < M; m += 32) {
-            const double2 t = tr[m], b = br[m], av = ar[m];
+            const double2 t = __ldg(tr + m), b = __ldg(br + m), av = __ldg(ar + m);
             const double er = fma(t.x, b.x, -t.y * b.y), ei = fma(t.x, b.y, t.y * b.x);
             sre = fma(av.x, er, fma(-av.y, ei, sre));
             sim = fma(av.x, ei, fma(av.y, er, sim));
