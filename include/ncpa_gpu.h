@@ -445,6 +445,13 @@ ncpa_status ncpa_ctx_bisect_steps(ncpa_ctx *ctx, long long *steps, long long *de
 /* Points the last NCPA_SUM_TC_GUARDED modal sum of this context recomputed
  * in FP64, and its receivers x ranges (waits for the context's stream). */
 ncpa_status ncpa_ctx_sum_fixups(ncpa_ctx *ctx, long long *recomputed, long long *points);
+/* Error model of the last NCPA_SUM_TC_GUARDED modal sum of this context:
+ * eps bounds the tensor-core error of a point relative to S, the sum of the
+ * magnitudes of its modal terms at the first range of its 256-range tile
+ * (|P_tc - P| <= eps S); points with |P_tc| < tau S were recomputed in FP64
+ * (tau = eps (1 + 1 / d), d = 1 - 10^(-0.05 / 20)).  Both 0 before the
+ * first guarded sum. */
+ncpa_status ncpa_ctx_sum_guard(ncpa_ctx *ctx, double *eps, double *tau);
 /* Schedule of the last tensor-core modal sum of this context: the depths of
  * its TMA ring and generated-operand ring.  The first tensor-core call of
  * each shape (format, receiver groups, mode chunks, range tiles) times every

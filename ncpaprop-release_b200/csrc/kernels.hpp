@@ -225,7 +225,9 @@ struct MsPlan {
 };
 MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms);
 // flag threshold of the guarded sum: a point with |P| < tau S is recomputed
-double ms_guard_tau();
+double ms_guard_tau(const MsPlan& p);
+// the error bound eps behind it: |P_tc - P| <= eps S
+double ms_guard_eps(const MsPlan& p);
 int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const double* vfull, double* vz);
 // fmt: 0 = 3-term split-BF16 (kind::f16), 1 = TF32 (kind::tf32), 2 = guarded
 // 6-term split-BF16.  Buffers: a_img = A as complex FP32 per (receiver group,

@@ -38,12 +38,14 @@
 // Persistent kernel: the (receiver group, 256-range tile, 16-mode chunk)
 // units are split evenly over one CTA per SM; a CTA accumulates the chunks of
 // one (group, tile) in TMEM (two accumulators, so a finished tile's epilogue
-// overlaps the next tile's MMAs) and stores its partial sum of the tile in
-// its own slot; the finishing kernel adds the slots of the CTAs that shared
-// the tile.  Warp 0: TMEM allocation and tcgen05.mma issue.  Warp 9: bulk
-// TMA of the chunk's B' image, A and tile phases into a 4-deep ring.
-// Warps 1-8: generate A'(tile) into a 3-deep ring of shared memory, and read
-// the accumulators out.
+// overlaps the next tile's MMAs; the guarded sum restarts the accumulation
+// every kMsAccChunks chunks and adds the blocks in the epilogue) and stores
+// its partial sum of the tile in its own slot; the finishing kernel adds the
+// slots of the CTAs that shared the tile.  Warp 0: TMEM allocation and
+// tcgen05.mma issue.  Warp 9: bulk TMA of the chunk's B' image, A and tile
+// phases into a 4-deep ring.  Warps 1-8: generate A'(tile) into a 3-deep
+// ring of shared memory.  Warps 10-13: read the accumulators out (one TMEM
+// lane quarter each), so that the generators never wait for an epilogue.
 //
 // Shared-memory operand layout: K-major, each operand row holds the 32 k of a
 // chunk; bf16: 64 B rows, 64-byte swizzle, 8-row atoms of 512 B (sw64_off);
@@ -70,10 +72,13 @@ constexpr int kMsABytes = kMsRows * kMsKC * 2;   // one A' part (hi or lo) of a 
 constexpr int kMsBBytes = kMsNT * kMsKC * 2;     // one B' part of a chunk: 16 KB
 constexpr int kMsACBytes = kMsModes * kMsRcv * 8;  // a chunk's A as complex FP32, [mode][receiver]: 8 KB
 constexpr int kMsQBytes = kMsModes * 8;            // tile phases of one chunk
-constexpr int kMsGenWarps = 8;      // A' generators / epilogue
+constexpr int kMsGenWarps = 8;      // A' generators
 constexpr int kMsGenThreads = 32 * kMsGenWarps;
 constexpr int kMsProducerWarp = 1 + kMsGenWarps;  // warp 0: MMA issuer, 1-8: generators, 9: TMA producer
-constexpr int kMsThreads = 32 * (kMsProducerWarp + 1);
+constexpr int kMsEpiWarp0 = kMsProducerWarp + 1;  // 10-13: epilogue (TMEM -> partial tiles)
+constexpr int kMsEpiWarps = 4;
+constexpr int kMsThreads = 32 * (kMsEpiWarp0 + kMsEpiWarps);
+static_assert(kMsEpiWarps == 4 && kMsEpiWarp0 % 4 == 2, "one epilogue warp per TMEM lane quarter (warp % 4)");
 constexpr int kMsAcc = 2;           // TMEM accumulators (kMsNT columns each): all 512 columns
 constexpr int kMsMaxStages = 4;     // barrier arrays are sized for the deepest ring
 static_assert(kMsAcc * kMsNT <= 512, "TMEM columns");
@@ -84,11 +89,24 @@ enum : int { kMsBf16x3 = 0, kMsTf32 = 1, kMsBf16x6 = 2 };
 // guarded sum: the TL tolerance it keeps, and the bound eps of its error
 // relative to S = sum_m |A'_jm| (the magnitude of the modal terms at the
 // tile's first range): |P_tc - P| <= eps S.  The six-product split drops
-// terms ~2^-24 relative and accumulates in FP32; eps covers the measured
-// worst case of the 64-receiver x 20000-range x 1362-mode workload with a
-// wide margin.
+// terms ~2^-24 relative, so the error is that of the FP32 accumulation in
+// TMEM: each tcgen05.mma rounds the accumulator (12 per chunk), and the error
+// grows with the accumulator's magnitude and the number of roundings.  So one
+// accumulation covers at most kMsAccChunks chunks (64 modes) and the epilogue
+// adds the blocks' partial tiles in FP32 (round to nearest).  kMsGuardEps is
+// twice the largest |P_tc - P| / S measured over every point of a 1362-mode,
+// 64-receiver x 20000-range sum (4.7e-7 with 12 block additions per CTA and
+// tile; without blocks it was 2.2e-6, with 16-chunk blocks 1.3e-6); a CTA
+// that adds more blocks than that calibration is charged 2^-24 S per extra
+// addition (ms_guard_eps).  kMsAccChunks can be set at compile time for such
+// calibration runs; kMsGuardEps holds for the default.
 constexpr double kMsGuardTlDb = 0.05;
 constexpr double kMsGuardEps = 1.0e-6;
+constexpr long long kMsGuardCalAdds = 12;
+#ifndef NCPA_MS_ACC_CHUNKS
+#define NCPA_MS_ACC_CHUNKS 4
+#endif
+constexpr int kMsAccChunks = NCPA_MS_ACC_CHUNKS;
 
 // shared-memory plan of a format: a TMA stage holds the chunk's B' image
 // (kParts parts of 16 KB; TF32: one 32-bit image of the same size as two),
@@ -431,24 +449,30 @@ struct MsArgs {
     const float2* q;             // [n_tiles][M_pad]
     const unsigned char* b_img;  // B' images: [n_chunks][32 KB]
     int M_pad, n_chunks, n_tiles, n_ranges, groups;
+    int acc_chunks;              // chunks per TMEM accumulation (the guarded sum's block)
     long long n_units;           // groups * n_tiles * n_chunks
     float* raw;                  // [n_parts][groups][n_tiles][256 columns][128 rows] per-CTA partial tiles
     float* s_part;               // guarded sum: [n_parts][groups][n_tiles][64 receivers][4] partial sums of |A'|
     unsigned* err;
 };
 
-// position of a CTA's current unit, advanced chunk by chunk without division
+// position of a CTA's current unit, advanced chunk by chunk without division;
+// cib = the chunk's place in its accumulation block (blocks of acc_chunks
+// chunks from the tile's first chunk)
 struct UnitPos {
-    int chunk, tile, group;
-    __device__ void init(long long u, int n_chunks, int n_tiles) {
+    int chunk, tile, group, cib;
+    __device__ void init(long long u, int n_chunks, int n_tiles, int acc_chunks) {
         chunk = (int)(u % n_chunks);
         const long long gt = u / n_chunks;
         tile = (int)(gt % n_tiles);
         group = (int)(gt / n_tiles);
+        cib = chunk % acc_chunks;
     }
-    __device__ void next(int n_chunks, int n_tiles) {
+    __device__ void next(int n_chunks, int n_tiles, int acc_chunks) {
+        if (++cib == acc_chunks) cib = 0;
         if (++chunk == n_chunks) {
             chunk = 0;
+            cib = 0;
             if (++tile == n_tiles) {
                 tile = 0;
                 ++group;
@@ -484,7 +508,7 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
         }
         for (int b = 0; b < kMsAcc; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], kMsGenWarps);
+            mbar_init(&acc_empty[b], kMsEpiWarps);
         }
         mbar_init(&drain, 1);
         fence_mbar_init();
@@ -505,10 +529,10 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             // producer: bulk TMA of the B' image, A and tile phases of chunk c
             // into TMA stage c % kTStages once the MMAs of chunk c - kTStages are done
             UnitPos pos;
-            pos.init(u0, a.n_chunks, a.n_tiles);
+            pos.init(u0, a.n_chunks, a.n_tiles, a.acc_chunks);
             int issued = 0, landed = 0;
             bool ok = true;
-            for (int c = 0; c < nc; ++c, pos.next(a.n_chunks, a.n_tiles)) {
+            for (int c = 0; c < nc; ++c, pos.next(a.n_chunks, a.n_tiles, a.acc_chunks)) {
                 const int slot = c % kTStages;
                 if (c >= kTStages) {
                     ok = mbar_wait_bounded(&empty_t[slot], (uint32_t)(((c / kTStages) - 1) & 1), a.err);
@@ -532,13 +556,14 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
         if (lane == 0 && nc > 0) {
             // MMA issuer
             UnitPos pos;
-            pos.init(u0, a.n_chunks, a.n_tiles);
+            pos.init(u0, a.n_chunks, a.n_tiles, a.acc_chunks);
             bool ok = true;
             int sg = -1;  // segment (one group and tile) counter
             const uint64_t dsc0 = F == kMsTf32 ? smem_desc_sw128(sm_addr) : smem_desc(sm_addr);
-            for (int c = 0; c < nc && ok; ++c, pos.next(a.n_chunks, a.n_tiles)) {
-                const bool first = c == 0 || pos.chunk == 0;
-                const bool last = c == nc - 1 || pos.chunk == a.n_chunks - 1;
+            for (int c = 0; c < nc && ok; ++c, pos.next(a.n_chunks, a.n_tiles, a.acc_chunks)) {
+                // one accumulation: this CTA's chunks of one tile inside one block
+                const bool first = c == 0 || pos.cib == 0;
+                const bool last = c == nc - 1 || pos.chunk == a.n_chunks - 1 || pos.cib == a.acc_chunks - 1;
                 if (first) {
                     ++sg;
                     if (sg >= kMsAcc) {  // accumulator sg % 2 read out by the epilogue of segment sg - 2
@@ -604,26 +629,21 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             umma_commit(&drain);
             mbar_wait_drain(&drain, 0u);
         }
-    } else {
+    } else if (warp <= kMsGenWarps) {
         // A' generators: thread -> (receiver j of the group, mode quad q4);
         // A'(tile) = A diag(e^{i k r_n0}) in the real block form
         // [[Re, -Im], [Im, Re]]: row j holds (Re, -Im) and row j + 64 (Im, Re)
         // of the 4 modes' products at k = 8 q4 .. 8 q4 + 7
         const int t = threadIdx.x - 32;
         const int j = t & (kMsRcv - 1), q4 = t >> 6;
-        const int col_half = (warp - 1) >> 2;  // epilogue: accumulator columns [128 col_half, +128)
         bool ok = true;
-        int sg = -1;
-        float s_abs = 0.f;  // guarded sum: sum of |A'| over this thread's modes of the segment
+        float s_abs = 0.f;  // guarded sum: sum of |A'| over this thread's modes of the tile
         UnitPos pos;
-        pos.init(u0, a.n_chunks, a.n_tiles);
-        for (int c = 0; c < nc && ok; ++c, pos.next(a.n_chunks, a.n_tiles)) {
-            const bool first = c == 0 || pos.chunk == 0;
-            const bool last = c == nc - 1 || pos.chunk == a.n_chunks - 1;
-            if (first) {
-                ++sg;
-                s_abs = 0.f;
-            }
+        pos.init(u0, a.n_chunks, a.n_tiles, a.acc_chunks);
+        for (int c = 0; c < nc && ok; ++c, pos.next(a.n_chunks, a.n_tiles, a.acc_chunks)) {
+            const bool tile_first = c == 0 || pos.chunk == 0;
+            const bool tile_last = c == nc - 1 || pos.chunk == a.n_chunks - 1;
+            if (tile_first) s_abs = 0.f;
             const int stt = c % kTStages, sgs = c % kGStages;
             if (c >= kGStages) {  // A' stage free once the MMAs of chunk c - kGStages are done
                 ok = mbar_wait_bounded(&empty_g[sgs], (uint32_t)(((c / kGStages) - 1) & 1), a.err);
@@ -681,9 +701,46 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             __syncwarp();
             if (lane == 0)
                 asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full_g[sgs])) : "memory");
-            if (!last) continue;
-            // epilogue of segment sg: TMEM lanes 32 (warp % 4) .. +31 = rows;
-            // the partial sum goes to slot (this CTA - first CTA of the tile)
+            if (F == kMsBf16x6 && a.s_part && tile_last) {
+                // the tile's sum of |A'| goes to slot (this CTA - first CTA of the tile)
+                const long long gt = (long long)pos.group * a.n_tiles + pos.tile;
+                const int part_slot = blockIdx.x - ms_cta_of(gt * a.n_chunks, a.n_units, gridDim.x);
+                a.s_part[(((size_t)part_slot * a.groups + pos.group) * a.n_tiles + pos.tile) * (kMsRcv * 4) + j * 4 +
+                         q4] = s_abs;
+            }
+        }
+    } else if (warp >= kMsEpiWarp0) {
+        // epilogue: thread -> accumulator row 32 (warp % 4) + lane (TMEM lane
+        // quarter warp % 4), all kMsNT columns.  The partial sum of a tile
+        // goes to slot (this CTA - first CTA of the tile), stored by the
+        // tile's first accumulation and added to (FP32, round to nearest) by
+        // the later ones; each thread reads back only the addresses it wrote
+        // itself, 32 columns ahead of the ones it adds.
+        const int row = 32 * (warp & 3) + lane;
+        bool ok = true;
+        int sg = -1;
+        bool fresh = true;  // no accumulation of this tile stored yet by this CTA
+        UnitPos pos;
+        pos.init(u0, a.n_chunks, a.n_tiles, a.acc_chunks);
+        for (int c = 0; c < nc && ok; ++c, pos.next(a.n_chunks, a.n_tiles, a.acc_chunks)) {
+            const bool tile_first = c == 0 || pos.chunk == 0;
+            const bool tile_last = c == nc - 1 || pos.chunk == a.n_chunks - 1;
+            if (tile_first) fresh = true;
+            if (tile_first || pos.cib == 0) ++sg;
+            if (!(tile_last || pos.cib == a.acc_chunks - 1)) continue;
+            const long long gt = (long long)pos.group * a.n_tiles + pos.tile;
+            const int part_slot = blockIdx.x - ms_cta_of(gt * a.n_chunks, a.n_units, gridDim.x);
+            // partial tile stored column-major (the 128 rows of a column
+            // contiguous), so each store instruction of the warp writes 128 B;
+            // columns past n_ranges (last tile) land in the tile's own padding
+            // and are never read
+            float* tcol = a.raw + (((size_t)part_slot * a.groups + pos.group) * a.n_tiles + pos.tile) * kMsNT * kMsRows +
+                          row;
+            float o[32];
+            if (!fresh) {
+#pragma unroll
+                for (int x = 0; x < 32; ++x) o[x] = tcol[(size_t)x * kMsRows];
+            }
             bool acc_ok = mbar_wait_bounded(&acc_full[sg & 1], (uint32_t)((sg >> 1) & 1), a.err);
             acc_ok = __all_sync(0xffffffffu, acc_ok);  // tcgen05.ld is warp-collective
             if (!acc_ok) {
@@ -691,21 +748,11 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                 break;
             }
             tc_fence_after();
-            const int row = 32 * (warp & 3) + lane;
-            const long long gt = (long long)pos.group * a.n_tiles + pos.tile;
-            const int part_slot = blockIdx.x - ms_cta_of(gt * a.n_chunks, a.n_units, gridDim.x);
-            if (F == kMsBf16x6 && a.s_part)
-                a.s_part[(((size_t)part_slot * a.groups + pos.group) * a.n_tiles + pos.tile) * (kMsRcv * 4) + j * 4 +
-                         q4] = s_abs;
-            // partial tile stored column-major (the 128 rows of a column
-            // contiguous), so each store instruction of the warp writes 128 B
-            float* tcol = a.raw + (((size_t)part_slot * a.groups + pos.group) * a.n_tiles + pos.tile) * kMsNT * kMsRows +
-                          (size_t)((kMsNT / 2) * col_half) * kMsRows + row;
 #pragma unroll 1
-            for (int cb = 0; cb < kMsNT / 64; ++cb) {
+            for (int cb = 0; cb < kMsNT / 32; ++cb) {
                 uint32_t v[32];
-                const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) +
-                                       (uint32_t)((sg & 1) * kMsNT + (kMsNT / 2) * col_half + cb * 32);
+                const uint32_t taddr =
+                    tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((sg & 1) * kMsNT + cb * 32);
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
                     "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
@@ -716,12 +763,25 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                       "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
                       "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                     : "r"(taddr));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                // columns past n_ranges (last tile) land in the tile's own
-                // padding and are never read
+                float on[32];
+                float* tc = tcol + (size_t)(cb * 32) * kMsRows;
+                if (!fresh && cb + 1 < kMsNT / 32) {
 #pragma unroll
-                for (int x = 0; x < 32; ++x) tcol[(size_t)(cb * 32 + x) * kMsRows] = __uint_as_float(v[x]);
+                    for (int x = 0; x < 32; ++x) on[x] = tc[(size_t)(32 + x) * kMsRows];
+                }
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (fresh) {
+#pragma unroll
+                    for (int x = 0; x < 32; ++x) tc[(size_t)x * kMsRows] = __uint_as_float(v[x]);
+                } else {
+#pragma unroll
+                    for (int x = 0; x < 32; ++x) {
+                        tc[(size_t)x * kMsRows] = o[x] + __uint_as_float(v[x]);
+                        o[x] = on[x];
+                    }
+                }
             }
+            fresh = false;
             tc_fence_before();
             __syncwarp();
             if (lane == 0)
@@ -830,6 +890,7 @@ __global__ void __launch_bounds__(256) k_ms_finish(int n_rcv, int n_ranges, doub
 // point: P = C(r) sum_m A_jm e^{i k_m r_n} with e^{i k r_n} = (tile phase)
 // (offset phase), both FP64 tables of the preparation, the same
 // factorisation as the tensor-core sum (r_n = r_n0 + o dr).
+constexpr int kFixCtasPerSm = 2;
 __global__ void __launch_bounds__(256) k_ms_fix(const int* __restrict__ fix_count, const int2* __restrict__ fix_list,
                                                 int M, int M_pad, int n_ranges, double dr, double cr, double ci,
                                                 const double2* __restrict__ a64, const double2* __restrict__ tp64,
@@ -912,11 +973,22 @@ MsPlan ms_plan(int n_rcv, int M, int n_ranges, int num_sms) {
     return p;
 }
 
-double ms_guard_tau() {
+double ms_guard_eps(const MsPlan& p) {
+    // the calibrated bound, plus one FP32 rounding (2^-24 of at most S) per
+    // block addition beyond the calibration's: a CTA's share of a tile (at
+    // most per_cta chunks) touches at most ceil(per_cta / B) + 1 blocks of B
+    // chunks
+    const long long per_cta = p.n_ctas > 0 ? (p.n_units + p.n_ctas - 1) / p.n_ctas : 0;
+    const long long blocks = (p.n_chunks + kMsAccChunks - 1) / kMsAccChunks;
+    const long long adds = std::max(0LL, std::min(blocks, (per_cta + kMsAccChunks - 1) / kMsAccChunks + 1) - 1);
+    return kMsGuardEps + (double)std::max(0LL, adds - kMsGuardCalAdds) * std::ldexp(1.0, -24);
+}
+
+double ms_guard_tau(const MsPlan& p) {
     // |dTL| <= 0.05 dB needs |dP| <= d |P| with d = 1 - 10^(-0.05 / 20); with
     // |dP| <= eps S, a point with |P_tc| >= eps S (1 + 1 / d) satisfies it
     const double d = 1.0 - std::pow(10.0, -kMsGuardTlDb / 20.0);
-    return kMsGuardEps * (1.0 + 1.0 / d);
+    return ms_guard_eps(p) * (1.0 + 1.0 / d);
 }
 
 int launch_ms_gather(cudaStream_t st, int n_rcv, int M, const int* idx, const double* vfull, double* vz) {
@@ -997,6 +1069,7 @@ int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const 
     a.n_ranges = n_ranges;
     a.groups = p.groups;
     a.n_units = p.n_units;
+    a.acc_chunks = fmt == kMsBf16x6 ? std::min(kMsAccChunks, p.n_chunks) : p.n_chunks;
     a.raw = raw;
     a.s_part = fmt == kMsBf16x6 ? s_part : nullptr;
     a.err = err;
@@ -1021,7 +1094,7 @@ int launch_ms_finish(cudaStream_t st, const MsPlan& p, int n_rcv, int n_ranges, 
     ms_scale(cr, ci);
     const unsigned blocks = (unsigned)(p.groups * p.n_tiles * (kMsNT / kMsFinCols));
     k_ms_finish<<<blocks, 256, 0, st>>>(n_rcv, n_ranges, dr, p.groups, p.n_tiles, p.n_chunks, p.n_units, p.n_ctas, cr,
-                                        ci, raw, re, im, s_part, s_part ? ms_guard_tau() : 0.0, fix_count,
+                                        ci, raw, re, im, s_part, s_part ? ms_guard_tau(p) : 0.0, fix_count,
                                         (int2*)fix_list);
     return 1;
 }
@@ -1030,7 +1103,7 @@ int launch_ms_fix(cudaStream_t st, int num_sms, int M, int M_pad, int n_ranges, 
                   const void* fix_list, const void* a64, const void* tp64, const void* b64, double* re, double* im) {
     double cr, ci;
     ms_scale(cr, ci);
-    k_ms_fix<<<2 * num_sms, 256, 0, st>>>(fix_count, (const int2*)fix_list, M, M_pad, n_ranges, dr, cr, ci,
+    k_ms_fix<<<kFixCtasPerSm * num_sms, 256, 0, st>>>(fix_count, (const int2*)fix_list, M, M_pad, n_ranges, dr, cr, ci,
                                           (const double2*)a64, (const double2*)tp64, (const double2*)b64, re, im);
     return 1;
 }

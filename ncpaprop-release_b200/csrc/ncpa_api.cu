@@ -116,6 +116,7 @@ struct ncpa_ctx {
     DevBuf ms_img, ms_q, ms_tab, ms_raw, ms_vz, ms_idx, ms_re, ms_im;  // modal-sum scratch (grow-only)
     DevBuf ms_spart, ms_b64, ms_tp64, ms_a64, ms_fix, ms_fixcnt;        // guarded sum: bounds, FP64 tables, flags
     long long ms_last_points = 0;  // receivers x ranges of the last guarded modal sum
+    double ms_last_eps = 0.0, ms_last_tau = 0.0;  // its error bound and flag threshold (relative to S)
     // modal-sum schedule autotuner: (format, groups, chunks, tiles) -> the
     // fastest ring-depth variant of the tensor-core kernel; NCPA_MS_TUNE=0
     // keeps variant 0
@@ -1311,6 +1312,13 @@ ncpa_status ncpa_ctx_sum_fixups(ncpa_ctx* ctx, long long* recomputed, long long*
     });
 }
 
+ncpa_status ncpa_ctx_sum_guard(ncpa_ctx* ctx, double* eps, double* tau) {
+    if (!ctx || !eps || !tau) return NCPA_EINVAL;
+    *eps = ctx->ms_last_eps;
+    *tau = ctx->ms_last_tau;
+    return NCPA_OK;
+}
+
 ncpa_status ncpa_ctx_sum_schedule(ncpa_ctx* ctx, int* t_stages, int* g_stages, int* variants, double* times_ms) {
     if (!ctx || !t_stages || !g_stages) return NCPA_EINVAL;
     ncpa::ms_tc_variant_shape(ctx->ms_last_fmt, ctx->ms_last_variant, t_stages, g_stages);
@@ -2043,6 +2051,8 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
                     ctx->ms_fixcnt.alloc(sizeof(int), st);
                     CK(cudaMemsetAsync(ctx->ms_fixcnt.p, 0, sizeof(int), st));
                     ctx->ms_last_points = (long long)n_rcv * nr;
+                    ctx->ms_last_eps = ncpa::ms_guard_eps(pl);
+                    ctx->ms_last_tau = ncpa::ms_guard_tau(pl);
                 }
                 check_launch(ctx, ncpa::launch_ms_prepare(st, pl, fmt, n_rcv, M, kr, ki, vs, ctx->ms_idx.as<int>(),
                                                           vfull, tp->dr_m, tp->lossless, ctx->ms_img.p, ctx->ms_q.p,

@@ -34,7 +34,7 @@ EXPORTED = [
     "ncpa_ess_plan_create", "ncpa_ess_plan_run", "ncpa_ess_plan_modes", "ncpa_ess_plan_tl", "ncpa_ess_plan_tuning",
     "ncpa_ess_plan_destroy", "ncpa_profile_update", "ncpa_g2s_convert", "ncpa_profile_load_g2s",
     "ncpa_dispersion_read", "ncpa_dispersion_desc_get", "ncpa_dispersion_destroy", "ncpa_ctx_sum_fixups",
-    "ncpa_tl_1d_range", "ncpa_modes_from_host", "ncpa_ctx_sum_schedule", "ncpa_ctx_bisect_steps",
+    "ncpa_ctx_sum_guard", "ncpa_tl_1d_range", "ncpa_modes_from_host", "ncpa_ctx_sum_schedule", "ncpa_ctx_bisect_steps",
 ]
 
 
@@ -179,6 +179,7 @@ def lib():
         L.ncpa_ctx_reset_stats.argtypes = [_vp]
         L.ncpa_ctx_sturm_steps.argtypes = [_vp, ctypes.POINTER(_c_ll)]
         L.ncpa_ctx_sum_fixups.argtypes = [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]
+        L.ncpa_ctx_sum_guard.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.ncpa_ctx_sum_schedule.argtypes = [_vp, _ip, _ip, _ip, _dp]
         L.ncpa_ctx_bisect_steps.argtypes = [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]
         L.ncpa_probe_fp64_peak.argtypes = [_vp, _dp]
@@ -270,6 +271,15 @@ class Context:
         a, b = _c_ll(), _c_ll()
         self.check(lib().ncpa_ctx_sum_fixups(self.h, ctypes.byref(a), ctypes.byref(b)), "ncpa_ctx_sum_fixups")
         return a.value, b.value
+
+    def sum_guard(self):
+        """(eps, tau) of the last guarded tensor-core modal sum: its error is
+        at most eps S (S = sum of the magnitudes of a point's modal terms at
+        its tile's first range) and points with |P| < tau S were recomputed
+        in FP64"""
+        e, t = ctypes.c_double(), ctypes.c_double()
+        self.check(lib().ncpa_ctx_sum_guard(self.h, ctypes.byref(e), ctypes.byref(t)), "ncpa_ctx_sum_guard")
+        return e.value, t.value
 
     def sum_schedule(self):
         """(TMA ring depth, operand ring depth, per-variant times in ms of the
