@@ -79,6 +79,8 @@ constexpr int kMsEpiWarp0 = kMsProducerWarp + 1;  // 10-13: epilogue (TMEM -> pa
 constexpr int kMsEpiWarps = 4;
 constexpr int kMsThreads = 32 * (kMsEpiWarp0 + kMsEpiWarps);
 static_assert(kMsEpiWarps == 4 && kMsEpiWarp0 % 4 == 2, "one epilogue warp per TMEM lane quarter (warp % 4)");
+constexpr int kEpiCols = 16;        // epilogue: accumulator columns per tcgen05.ld
+constexpr int kEpiAhead = 4;        // column groups of old partial sums loaded ahead
 constexpr int kMsAcc = 2;           // TMEM accumulators (kMsNT columns each): all 512 columns
 constexpr int kMsMaxStages = 4;     // barrier arrays are sized for the deepest ring
 static_assert(kMsAcc * kMsNT <= 512, "TMEM columns");
@@ -715,7 +717,7 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
         // goes to slot (this CTA - first CTA of the tile), stored by the
         // tile's first accumulation and added to (FP32, round to nearest) by
         // the later ones; each thread reads back only the addresses it wrote
-        // itself, 32 columns ahead of the ones it adds.
+        // itself, kEpiAhead * kEpiCols columns ahead of the ones it adds.
         const int row = 32 * (warp & 3) + lane;
         bool ok = true;
         int sg = -1;
@@ -736,10 +738,14 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
             // and are never read
             float* tcol = a.raw + (((size_t)part_slot * a.groups + pos.group) * a.n_tiles + pos.tile) * kMsNT * kMsRows +
                           row;
-            float o[32];
+            // old partial sums kEpiAhead column groups ahead of the adds (the
+            // first ones loaded while the accumulator is still being filled)
+            float o[kEpiAhead][kEpiCols];
             if (!fresh) {
 #pragma unroll
-                for (int x = 0; x < 32; ++x) o[x] = tcol[(size_t)x * kMsRows];
+                for (int d = 0; d < kEpiAhead; ++d)
+#pragma unroll
+                    for (int x = 0; x < kEpiCols; ++x) o[d][x] = tcol[(size_t)(d * kEpiCols + x) * kMsRows];
             }
             bool acc_ok = mbar_wait_bounded(&acc_full[sg & 1], (uint32_t)((sg >> 1) & 1), a.err);
             acc_ok = __all_sync(0xffffffffu, acc_ok);  // tcgen05.ld is warp-collective
@@ -748,36 +754,31 @@ __global__ void __launch_bounds__(kMsThreads, 1) k_ms_tc(MsArgs a) {
                 break;
             }
             tc_fence_after();
-#pragma unroll 1
-            for (int cb = 0; cb < kMsNT / 32; ++cb) {
-                uint32_t v[32];
+#pragma unroll
+            for (int cb = 0; cb < kMsNT / kEpiCols; ++cb) {
+                uint32_t v[kEpiCols];
                 const uint32_t taddr =
-                    tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((sg & 1) * kMsNT + cb * 32);
+                    tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((sg & 1) * kMsNT + cb * kEpiCols);
                 asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-                    "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
-                    "%30, %31}, [%32];"
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                    "%12, %13, %14, %15}, [%16];"
                     : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
                       "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
-                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
-                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                      "=r"(v[14]), "=r"(v[15])
                     : "r"(taddr));
-                float on[32];
-                float* tc = tcol + (size_t)(cb * 32) * kMsRows;
-                if (!fresh && cb + 1 < kMsNT / 32) {
-#pragma unroll
-                    for (int x = 0; x < 32; ++x) on[x] = tc[(size_t)(32 + x) * kMsRows];
-                }
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float* tc = tcol + (size_t)(cb * kEpiCols) * kMsRows;
+                float* slot = o[cb % kEpiAhead];
                 if (fresh) {
 #pragma unroll
-                    for (int x = 0; x < 32; ++x) tc[(size_t)x * kMsRows] = __uint_as_float(v[x]);
+                    for (int x = 0; x < kEpiCols; ++x) tc[(size_t)x * kMsRows] = __uint_as_float(v[x]);
                 } else {
 #pragma unroll
-                    for (int x = 0; x < 32; ++x) {
-                        tc[(size_t)x * kMsRows] = o[x] + __uint_as_float(v[x]);
-                        o[x] = on[x];
+                    for (int x = 0; x < kEpiCols; ++x) tc[(size_t)x * kMsRows] = slot[x] + __uint_as_float(v[x]);
+                    if (cb + kEpiAhead < kMsNT / kEpiCols) {
+#pragma unroll
+                        for (int x = 0; x < kEpiCols; ++x)
+                            slot[x] = tc[(size_t)(kEpiAhead * kEpiCols + x) * kMsRows];
                     }
                 }
             }
@@ -890,7 +891,7 @@ __global__ void __launch_bounds__(256) k_ms_finish(int n_rcv, int n_ranges, doub
 // point: P = C(r) sum_m A_jm e^{i k_m r_n} with e^{i k r_n} = (tile phase)
 // (offset phase), both FP64 tables of the preparation, the same
 // factorisation as the tensor-core sum (r_n = r_n0 + o dr).
-constexpr int kFixCtasPerSm = 2;
+constexpr int kFixCtasPerSm = 4;
 __global__ void __launch_bounds__(256) k_ms_fix(const int* __restrict__ fix_count, const int2* __restrict__ fix_list,
                                                 int M, int M_pad, int n_ranges, double dr, double cr, double ci,
                                                 const double2* __restrict__ a64, const double2* __restrict__ tp64,
