@@ -246,21 +246,21 @@ __device__ __forceinline__ void sts128(uint32_t addr, uint32_t a, uint32_t b, ui
 // ---------------------------------------------------------------------------
 // preparation
 // ---------------------------------------------------------------------------
-// per-mode FP32 factors from FP64: entries 0-7 e^{i k i dr}, 8-15
 // B' chunk images: B'[o][2m] = Re, B'[o][2m + 1] = Im of e^{i k_m o dr}
 // (o = 0 .. 255, the range offset inside a tile; attenuation included unless
-// lossless) in FP64, then split (bf16 hi, lo) or rounded (TF32), in the
-// shared-memory layout of the operand; zero for the padding modes m >= M.
-// The images do not depend on the tile: the tile's phase e^{i k r_n0} goes
-// into A'.  A thread covers kMsBRun consecutive ranges of one mode: one
-// sincos / exp at the first, FP64 complex steps by e^{i k dr} after it.
-constexpr int kMsBRun = 8;
-
+// lossless) in FP64, then split (bf16 hi, mid, lo or hi, lo) or rounded
+// (TF32), in the shared-memory layout of the operand; zero for the padding
+// modes m >= M.  The images do not depend on the tile: the tile's phase
+// e^{i k r_n0} goes into A'.
+//
 // b64, when given, receives the same FP64 values as [o][M_pad] complex (the
-// guarded sum's fix-up reads them).  A thread covers kMsBRun ranges of four
-// consecutive modes (a quad q4 of the chunk), so each operand part of a range
-// is one 16-byte chunk of the swizzled row (k = 8 q4 .. 8 q4 + 7: Re, Im of
-// the four modes) written with one store; padding modes m >= M get zeros.
+// guarded sum's fix-up reads them).  A thread covers one range offset of four
+// consecutive modes (a quad q4 of the chunk), so each operand part is one
+// 16-byte chunk of the swizzled row (k = 8 q4 .. 8 q4 + 7: Re, Im of the four
+// modes) written with one store.  Each value is evaluated directly (the
+// phase k o dr reduced mod 2 pi in FP64, then sine / cosine and the
+// attenuation factor): the threads are independent, so the launch spreads
+// over every SM.
 constexpr int kMsBQuads = kMsModes / 4;
 
 __device__ __forceinline__ uint32_t bf16_pair(__nv_bfloat16 lo, __nv_bfloat16 hi) {
@@ -271,92 +271,76 @@ template <int F>
 __device__ void ms_b_entry(long long id, int M, int M_pad, int n_chunks, const double* __restrict__ kr,
                            const double* __restrict__ ki, double dr, int lossless, unsigned char* __restrict__ img,
                            double2* __restrict__ b64) {
-    constexpr int kRuns = kMsNT / kMsBRun;
-    const long long per_chunk = (long long)kRuns * kMsBQuads;
+    const long long per_chunk = (long long)kMsNT * kMsBQuads;
     if (id >= (long long)n_chunks * per_chunk) return;
-    const int o0 = (int)(id % kRuns) * kMsBRun;
-    const int q4 = (int)((id / kRuns) % kMsBQuads);
+    const int o = (int)(id % kMsNT);
+    const int q4 = (int)((id / kMsNT) % kMsBQuads);
     const int chunk = (int)(id / per_chunk);
     const int m0 = chunk * kMsModes + 4 * q4;
-    double cr[4], ci[4], sr[4], si[4];  // value at o0 and the step, per mode
+    const double x = (double)o * dr;
+    double cr[4], ci[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
         cr[v] = 0.0;
         ci[v] = 0.0;
-        sr[v] = 1.0;
-        si[v] = 0.0;
         const int m = m0 + v;
         if (m < M) {
-            const double b = lossless ? 0.0 : ki[m];
-            const double x = (double)o0 * dr;
+            const double th = kr[m] * x;
+            const double red = fma(-rint(th * (0.5 / kPi)), 2.0 * kPi, th);
             double sn, cs;
-            sincos(kr[m] * x, &sn, &cs);
-            const double amp = exp(-b * x);
+            sincos(red, &sn, &cs);
+            const double amp = lossless ? 1.0 : exp(-ki[m] * x);
             cr[v] = amp * cs;
             ci[v] = amp * sn;
-            sincos(kr[m] * dr, &sn, &cs);
-            const double ad = exp(-b * dr);
-            sr[v] = ad * cs;
-            si[v] = ad * sn;
         }
     }
     unsigned char* cimg = img + (size_t)chunk * MsCfg<F>::kBChunk;
-#pragma unroll 1
-    for (int u = 0; u < kMsBRun; ++u) {
-        const int o = o0 + u;
-        if (b64) {
-            double2* row = b64 + (size_t)o * M_pad + m0;
+    if (b64) {
+        double2* row = b64 + (size_t)o * M_pad + m0;
 #pragma unroll
-            for (int v = 0; v < 4; ++v) row[v] = make_double2(cr[v], ci[v]);
-        }
-        if (F == kMsBf16x6) {
-            // three bf16 parts of the FP64 value: hi, then the remainders
-            uint32_t h[4], md[4], l[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const __nv_bfloat16 hr = __double2bfloat16(cr[v]), hm = __double2bfloat16(ci[v]);
-                const double rr = cr[v] - (double)__bfloat162float(hr), ri = ci[v] - (double)__bfloat162float(hm);
-                const __nv_bfloat16 mr = __double2bfloat16(rr), mi = __double2bfloat16(ri);
-                const __nv_bfloat16 lr = __double2bfloat16(rr - (double)__bfloat162float(mr));
-                const __nv_bfloat16 li = __double2bfloat16(ri - (double)__bfloat162float(mi));
-                h[v] = bf16_pair(hr, hm);
-                md[v] = bf16_pair(mr, mi);
-                l[v] = bf16_pair(lr, li);
-            }
-            const uint32_t off = sw64_off(o, 8 * q4);
-            *reinterpret_cast<uint4*>(cimg + off) = make_uint4(h[0], h[1], h[2], h[3]);
-            *reinterpret_cast<uint4*>(cimg + kMsBBytes + off) = make_uint4(md[0], md[1], md[2], md[3]);
-            *reinterpret_cast<uint4*>(cimg + 2 * kMsBBytes + off) = make_uint4(l[0], l[1], l[2], l[3]);
-        } else if (F == kMsTf32) {
-            uint32_t t[8];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                t[2 * v] = to_tf32((float)cr[v]);
-                t[2 * v + 1] = to_tf32((float)ci[v]);
-            }
-            *reinterpret_cast<uint4*>(cimg + sw128_off(o, 8 * q4)) = make_uint4(t[0], t[1], t[2], t[3]);
-            *reinterpret_cast<uint4*>(cimg + sw128_off(o, 8 * q4 + 4)) = make_uint4(t[4], t[5], t[6], t[7]);
-        } else {
-            uint32_t h[4], l[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const float re = (float)cr[v], im = (float)ci[v];
-                const __nv_bfloat16 hr = __float2bfloat16_rn(re), hm = __float2bfloat16_rn(im);
-                const __nv_bfloat16 lr = __float2bfloat16_rn(re - __bfloat162float(hr));
-                const __nv_bfloat16 li = __float2bfloat16_rn(im - __bfloat162float(hm));
-                h[v] = bf16_pair(hr, hm);
-                l[v] = bf16_pair(lr, li);
-            }
-            const uint32_t off = sw64_off(o, 8 * q4);
-            *reinterpret_cast<uint4*>(cimg + off) = make_uint4(h[0], h[1], h[2], h[3]);
-            *reinterpret_cast<uint4*>(cimg + kMsBBytes + off) = make_uint4(l[0], l[1], l[2], l[3]);
-        }
+        for (int v = 0; v < 4; ++v) row[v] = make_double2(cr[v], ci[v]);
+    }
+    if (F == kMsBf16x6) {
+        // three bf16 parts of the FP64 value: hi, then the remainders
+        uint32_t h[4], md[4], l[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            const double nr = fma(cr[v], sr[v], -ci[v] * si[v]), ni = fma(cr[v], si[v], ci[v] * sr[v]);
-            cr[v] = nr;
-            ci[v] = ni;
+            const __nv_bfloat16 hr = __double2bfloat16(cr[v]), hm = __double2bfloat16(ci[v]);
+            const double rr = cr[v] - (double)__bfloat162float(hr), ri = ci[v] - (double)__bfloat162float(hm);
+            const __nv_bfloat16 mr = __double2bfloat16(rr), mi = __double2bfloat16(ri);
+            const __nv_bfloat16 lr = __double2bfloat16(rr - (double)__bfloat162float(mr));
+            const __nv_bfloat16 li = __double2bfloat16(ri - (double)__bfloat162float(mi));
+            h[v] = bf16_pair(hr, hm);
+            md[v] = bf16_pair(mr, mi);
+            l[v] = bf16_pair(lr, li);
         }
+        const uint32_t off = sw64_off(o, 8 * q4);
+        *reinterpret_cast<uint4*>(cimg + off) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(cimg + kMsBBytes + off) = make_uint4(md[0], md[1], md[2], md[3]);
+        *reinterpret_cast<uint4*>(cimg + 2 * kMsBBytes + off) = make_uint4(l[0], l[1], l[2], l[3]);
+    } else if (F == kMsTf32) {
+        uint32_t t[8];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            t[2 * v] = to_tf32((float)cr[v]);
+            t[2 * v + 1] = to_tf32((float)ci[v]);
+        }
+        *reinterpret_cast<uint4*>(cimg + sw128_off(o, 8 * q4)) = make_uint4(t[0], t[1], t[2], t[3]);
+        *reinterpret_cast<uint4*>(cimg + sw128_off(o, 8 * q4 + 4)) = make_uint4(t[4], t[5], t[6], t[7]);
+    } else {
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const float re = (float)cr[v], im = (float)ci[v];
+            const __nv_bfloat16 hr = __float2bfloat16_rn(re), hm = __float2bfloat16_rn(im);
+            const __nv_bfloat16 lr = __float2bfloat16_rn(re - __bfloat162float(hr));
+            const __nv_bfloat16 li = __float2bfloat16_rn(im - __bfloat162float(hm));
+            h[v] = bf16_pair(hr, hm);
+            l[v] = bf16_pair(lr, li);
+        }
+        const uint32_t off = sw64_off(o, 8 * q4);
+        *reinterpret_cast<uint4*>(cimg + off) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(cimg + kMsBBytes + off) = make_uint4(l[0], l[1], l[2], l[3]);
     }
 }
 
@@ -1004,7 +988,7 @@ int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int 
                       const double* ki, const double* vs, const int* idx, const double* vfull, double dr, int lossless,
                       void* a_img, void* q, void* tab, void* b64, void* tp64, void* a64) {
     if (fmt != kMsBf16x3 && fmt != kMsTf32 && fmt != kMsBf16x6) return -1;
-    const long long n_b = (long long)p.n_chunks * (kMsNT / kMsBRun) * kMsBQuads;
+    const long long n_b = (long long)p.n_chunks * kMsNT * kMsBQuads;
     const long long n_q = (long long)p.n_tiles * p.M_pad;
     const long long n_a = (long long)p.groups * p.n_chunks * kMsModes * kMsRcv;
     const long long b_b = (n_b + 255) / 256, b_q = (n_q + 255) / 256, b_a = (n_a + 255) / 256;
