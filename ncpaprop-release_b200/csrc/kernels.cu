@@ -480,6 +480,7 @@ __global__ void __launch_bounds__(kWkbThreads) k_window(ProblemInfo* __restrict_
         pinfo[p].lo = (k_min * k_min) * h2;
         pinfo[p].hi = (k_max * k_max) * h2;
         pinfo[p].used_wkb = used_wkb;
+        pinfo[p].n_scan = kScanDefault;
     }
 }
 
@@ -489,101 +490,48 @@ int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2,
     return 1;
 }
 
-// ===========================================================================
-// CTA-cooperative Sturm sweep: the diagonal streams through shared memory in
-// kChunk-double chunks by TMA bulk copies (kNbuf-deep ring, one mbarrier per
-// slot); every thread runs its own recurrences at its own two shifts.
-// ===========================================================================
-constexpr int kNbuf = 4;
-
-struct Ring {
-    double* buf;     // [kNbuf][kChunk]
-    uint64_t* bars;  // [kNbuf]
-    unsigned loads;  // loads issued so far; identical in every thread
-};
-
-__device__ __forceinline__ void ring_issue(Ring& r, unsigned k, const double* src) {
-    int slot = k % kNbuf;
-    mbar_expect_tx(&r.bars[slot], kChunk * 8);
-    tma_load_1d(r.buf + slot * kChunk, src, kChunk * 8, &r.bars[slot]);
-}
-
-// Two shifts per thread: two independent chains interleaved step by step
-// (sturm_word32_pair: each chain's arithmetic is that of SturmState::word32)
-__device__ void cta_sturm_sweep_pair(const double* __restrict__ s, int nz, double x0, double x1, Ring& r,
-                                     unsigned* err, int& c0, int& c1) {
-    const int nch = (nz + kChunk - 1) / kChunk;
-    const unsigned base = r.loads;
-    if (threadIdx.x == 0) {
-        for (int c = 0; c < nch && c < kNbuf; ++c) ring_issue(r, base + c, s + (size_t)c * kChunk);
-    }
-    SturmState A, B;
-    A.reset();
-    B.reset();
-    for (int c = 0; c < nch; ++c) {
-        const unsigned k = base + c;
-        const int slot = k % kNbuf;
-        mbar_wait_bounded(&r.bars[slot], (k / kNbuf) & 1u, err);
-        const double* b = r.buf + slot * kChunk;
-        const int valid = min(kChunk, nz - c * kChunk);
-        const int nw = valid >> 5;
-        for (int w = 0; w < nw; ++w) sturm_word32_pair(A, B, b + 32 * w, x0, x1);
-        for (int i = nw * 32; i < valid; ++i) {
-            A.step(b[i], x0);
-            B.step(b[i], x1);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0 && c + kNbuf < nch) {
-            fence_proxy_async();
-            ring_issue(r, base + c + kNbuf, s + (size_t)(c + kNbuf) * kChunk);
-        }
-    }
-    r.loads = base + nch;
-    c0 = A.cnt;
-    c1 = B.cnt;
-}
-
-__device__ __forceinline__ void ring_init(Ring& r, double* buf, uint64_t* bars) {
-    r.buf = buf;
-    r.bars = bars;
-    r.loads = 0;
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < kNbuf; ++k) mbar_init(&bars[k], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-}
-
-__device__ __forceinline__ double scan_x(double lo, double hi, int t) {
+// shift t of an isolation scan of n points on an even grid of [lo, hi]
+__device__ __forceinline__ double scan_x(double lo, double hi, int t, int n) {
     if (t == 0) return lo;
-    if (t == kScanPoints - 1) return hi;
-    return lo + (hi - lo) * ((double)t / (double)(kScanPoints - 1));
+    if (t == n - 1) return hi;
+    return lo + (hi - lo) * ((double)t / (double)(n - 1));
 }
 
-// K3a: kScanPoints counts per problem on an even grid of [lo, hi]; thread t
-// sweeps shifts t and t + kScanPoints / 2
-constexpr int kScanThreads = kScanPoints / 2;
-__global__ void __launch_bounds__(kScanThreads) k_scan(const ProblemInfo* __restrict__ pinfo,
-                                                      const double* __restrict__ s, int* __restrict__ counts,
-                                                      unsigned* err) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    double* buf = reinterpret_cast<double*>(smem_raw);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + kNbuf * kChunk * 8);
-    Ring r;
-    ring_init(r, buf, bars);
+// K3a-1: the size of each problem's isolation scan.  The number of
+// eigenvalues of S (diagonal s_i, unit off-diagonals) below x is close to the
+// sum over the rows of theta_i / pi with cos theta_i = (s_i - x) / 2 clipped
+// to [-1, 1] (each row's local band is [s_i - 2, s_i + 2]); on the 20000-point
+// grids of 0.002-0.5 Hz it gives the mode count in [lo, hi] within one mode.
+// The scan takes about two shifts per mode plus 32, in steps of 64 (one scan
+// unit), between 64 and kScanMax: problems with many close
+// eigenvalues start their bisection better isolated, those with few stop
+// paying for shifts that isolate nothing.
+constexpr int kScanStep = 64;  // shifts per scan unit (one warp, two per lane)
+constexpr int kSizeThreads = 256;
+__global__ void __launch_bounds__(kSizeThreads) k_scan_size(ProblemInfo* __restrict__ pinfo,
+                                                           const double* __restrict__ s) {
+    __shared__ float part[kSizeThreads / 32];
     const int p = blockIdx.x;
-    const double lo = pinfo[p].lo, hi = pinfo[p].hi;
-    const int t0 = threadIdx.x, t1 = threadIdx.x + kScanThreads;
-    int c0, c1;
-    cta_sturm_sweep_pair(s + pinfo[p].s_off, pinfo[p].nz, scan_x(lo, hi, t0), scan_x(lo, hi, t1), r, err, c0, c1);
-    counts[(size_t)p * kScanPoints + t0] = c0;
-    counts[(size_t)p * kScanPoints + t1] = c1;
-}
-
-int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* s, int* counts, unsigned* err) {
-    size_t sm = kNbuf * kChunk * 8 + kNbuf * 8;
-    k_scan<<<P, kScanThreads, sm, st>>>(pinfo, s, counts, err);
-    return 1;
+    const ProblemInfo pi = pinfo[p];
+    const double* row = s + pi.s_off;
+    float acc = 0.f;
+    for (int i = threadIdx.x; i < pi.nz; i += kSizeThreads) {
+        const double v = row[i];
+        const float ch = fminf(fmaxf((float)((v - pi.hi) * 0.5), -1.f), 1.f);
+        const float cl = fminf(fmaxf((float)((v - pi.lo) * 0.5), -1.f), 1.f);
+        acc += acosf(ch) - acosf(cl);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < kSizeThreads / 32; ++w) t += part[w];
+        const float m_est = fmaxf(t * (float)(1.0 / kPi), 0.f);
+        const int n = ((int)(2.f * m_est) + 32 + kScanStep - 1) / kScanStep * kScanStep;
+        pinfo[p].n_scan = min(max(n, kScanStep), kScanMax);
+    }
 }
 
 // K3: per-warp multisection + safeguarded Newton.
@@ -1013,6 +961,71 @@ __device__ void warp_sweep_tw(const double* __restrict__ s, int nz, double p_ini
     else warp_sweep_tw_mode<Row, 2>(s, nz, p_init, x0, x1, r, err, c0, c1, rat0, h0);
 }
 
+// K3a-2: the isolation scan in units of kScanStep shifts, numbered over the
+// problems in order (problem p has n_scan / kScanStep units).  Warp w of the
+// grid sweeps unit w (warp_sweep: the sequential count, two shifts per lane)
+// through its own ring; it finds its problem with a warp-wide prefix sum of
+// the units per problem, 32 problems at a time.  Every unit is the same work
+// and the units go to consecutive warps, so the SMs share the scan evenly
+// whatever the problems' sizes; warps past the last unit return.
+__global__ void __launch_bounds__(kWarpsPerCta * 32) k_scan(int P, const ProblemInfo* __restrict__ pinfo,
+                                                           const double* __restrict__ s, int* __restrict__ counts,
+                                                           unsigned* err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const long long w = (long long)blockIdx.x * kWarpsPerCta + wid;
+    long long before = 0;  // units of the problems before the current block of 32
+    int p = -1, tb = 0;
+    for (int base = 0; base < P && p < 0; base += 32) {
+        const int q = base + lane;
+        const int units = q < P ? pinfo[q].n_scan / kScanStep : 0;
+        int incl = units;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += v;
+        }
+        const bool mine = w >= before + incl - units && w < before + incl;
+        const unsigned hit = __ballot_sync(0xffffffffu, mine);
+        if (hit) {
+            const int src = __ffs(hit) - 1;
+            const int excl = __shfl_sync(0xffffffffu, incl - units, src);
+            p = base + src;
+            tb = (int)(w - before - excl) * kScanStep;
+        }
+        before += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (p < 0) return;  // past the last unit: the whole warp
+    const ProblemInfo pi = pinfo[p];
+    const int n = pi.n_scan;
+    WarpRing r;
+    r.buf = reinterpret_cast<double*>(smem_raw) + (size_t)wid * kWBuf * kWChunk;
+    r.bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarpsPerCta * kWBuf * kWChunk * 8) + wid * kWBuf;
+    r.loads = 0;
+    if (lane == 0) {
+        for (int k = 0; k < kWBuf; ++k) mbar_init(&r.bars[k], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    const int t0 = tb + 2 * lane, t1 = t0 + 1;
+    int c0, c1;
+    double rat, hq;
+    warp_sweep<EssRows>(s + pi.s_off, pi.nz, 0.0, scan_x(pi.lo, pi.hi, t0, n), scan_x(pi.lo, pi.hi, t1, n), 0, r,
+                        err, c0, c1, rat, hq);
+    counts[(size_t)p * kScanMax + t0] = c0;
+    counts[(size_t)p * kScanMax + t1] = c1;
+}
+
+int launch_scan(cudaStream_t st, int P, ProblemInfo* pinfo, const double* s, int* counts, unsigned* err) {
+    k_scan_size<<<P, kSizeThreads, 0, st>>>(pinfo, s);
+    const size_t sm = (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8 + kWBuf * 8);
+    const long long units = (long long)P * (kScanMax / kScanStep);
+    cudaFuncSetAttribute(k_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_scan<<<(unsigned)((units + kWarpsPerCta - 1) / kWarpsPerCta), kWarpsPerCta * 32, sm, st>>>(P, pinfo, s,
+                                                                                                  counts, err);
+    return 2;
+}
+
 // One bisection work item (<= 32 eigenvalues of one problem) on this warp,
 // with its TMA ring r: the eigenvalues to mu in the row format's units.
 template <class Row>
@@ -1022,7 +1035,7 @@ __device__ __forceinline__ void bisect_item(const ProblemInfo* __restrict__ pinf
                                             unsigned long long* step_counter, WarpRing& r) {
     const int lane = threadIdx.x & 31;
     const ProblemInfo pi = pinfo[w.problem];
-    const int* cnt = counts + (size_t)w.problem * kScanPoints;
+    const int* cnt = counts + (size_t)w.problem * kScanMax;
     const double* sp = s + (size_t)pi.s_off * Row::kW;
     const int nz = pi.nz;
     const double lo = Row::scan_lo(pi), hi = Row::scan_hi(pi);
@@ -1035,14 +1048,15 @@ __device__ __forceinline__ void bisect_item(const ProblemInfo* __restrict__ pinf
     int ca = 0, cb = 0, mode = 2;
     if (lane < w.m) {  // initial bracket from the isolation scan
         int t0 = 0;
-        for (int t = 0; t < kScanPoints; ++t)
+        const int n_scan = pi.n_scan;
+        for (int t = 0; t < n_scan; ++t)
             if (cnt[t] <= J) t0 = t;
-        int t1 = kScanPoints - 1;
-        for (int t = kScanPoints - 1; t > t0; --t)
+        int t1 = n_scan - 1;
+        for (int t = n_scan - 1; t > t0; --t)
             if (cnt[t] > J) t1 = t;
         if (cnt[t1] <= J) atomicOr(err, kErrBracket);
-        a = scan_x(lo, hi, t0);
-        b = scan_x(lo, hi, t1);
+        a = scan_x(lo, hi, t0, n_scan);
+        b = scan_x(lo, hi, t1, n_scan);
         ca = cnt[t0];
         cb = cnt[t1];
         x = 0.5 * (a + b);
@@ -1271,8 +1285,8 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
         const int p = p0 + threadIdx.x;
         int M = 0, nb = 0, ne = 0;
         if (p < P) {
-            const int c_lo = counts[(size_t)p * kScanPoints];
-            const int c_hi = counts[(size_t)p * kScanPoints + kScanPoints - 1];
+            const int c_lo = counts[(size_t)p * kScanMax];
+            const int c_hi = counts[(size_t)p * kScanMax + pinfo[p].n_scan - 1];
             M = max(0, c_hi - c_lo);
             if (M > max_modes) {
                 atomicOr(err, kErrTooMany);

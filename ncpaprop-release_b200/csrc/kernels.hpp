@@ -32,6 +32,7 @@ struct ProblemInfo {
     int c_lo, c_hi;        // Sturm counts at lo, hi
     int M, off;            // number of modes and offset into the mode arrays
     int used_wkb;
+    int n_scan;            // shifts of the isolation scan (<= kScanMax)
     double g0;             // wide-angle rows: ground term of row 0, 1 / (dz admittance + 1)
 };
 
@@ -42,7 +43,8 @@ struct WorkItem {
     int pad;
 };
 
-constexpr int kScanPoints = 256;  // Sturm counts per problem in the isolation scan
+constexpr int kScanMax = 512;      // count slots per problem of the isolation scan
+constexpr int kScanDefault = 256;  // shifts per problem unless the scan sizes them (wide-angle rows)
 constexpr int kChunk = 1024;      // doubles per TMA chunk of the diagonal
 constexpr int kBlk = 16;          // eigenvector checkpoint interval
 constexpr int kCkRows = 128;      // twist candidates of the reduction-only eigenvector items
@@ -86,8 +88,10 @@ int launch_build_matrix(cudaStream_t st, int nk, const double* zk, const double*
 // WKB window and scaled bounds (K2)
 int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2, int wkb, int wvnum,
                   double c_min, double c_max, unsigned* err);
-// isolation scan: kScanPoints Sturm counts per problem (K3a)
-int launch_scan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* s, int* counts, unsigned* err);
+// isolation scan (K3a): sizes each problem's scan (ProblemInfo::n_scan) from
+// an estimate of its mode count, then pinfo[p].n_scan Sturm counts per
+// problem at counts[p * kScanMax + t]
+int launch_scan(cudaStream_t st, int P, ProblemInfo* pinfo, const double* s, int* counts, unsigned* err);
 // multisection/bisection over work items (K3); step_counter (optional)
 // accumulates the Sturm recurrence steps swept
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,

@@ -504,7 +504,7 @@ void prepare_solve(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, int
     const int P = M->P;
     const int cap_modes = M->prm.max_modes;
     const size_t mcap = (size_t)P * cap_modes;
-    b.counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
+    b.counts.alloc((size_t)P * ncpa::kScanMax * 4, st);
     b.bis_cap = P * ((cap_modes + min_bis_item - 1) / min_bis_item);
     b.ev_cap = P * ((cap_modes + ncpa::kEvItem - 1) / ncpa::kEvItem);
     b.bis.alloc((size_t)b.bis_cap * sizeof(WorkItem), st);
@@ -662,10 +662,10 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
     tm.mark("window");
     // ---- K3a scan ----
     DevBuf counts;
-    counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
+    counts.alloc((size_t)P * ncpa::kScanMax * 4, st);
     check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), counts.as<int>(), ctx->d_err.as<unsigned>()));
     tm.mark("scan");
-    std::vector<int> hcounts((size_t)P * ncpa::kScanPoints);
+    std::vector<int> hcounts((size_t)P * ncpa::kScanMax);
     CK(cudaMemcpyAsync(hcounts.data(), counts.p, hcounts.size() * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(M->info.data(), d_pinfo, P * sizeof(ProblemInfo), cudaMemcpyDeviceToHost, st));
     check_device_status(ctx);
@@ -674,8 +674,8 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
     int off = 0;
     for (int p = 0; p < P; ++p) {
         ProblemInfo& pi = M->info[p];
-        pi.c_lo = hcounts[(size_t)p * ncpa::kScanPoints];
-        pi.c_hi = hcounts[(size_t)p * ncpa::kScanPoints + ncpa::kScanPoints - 1];
+        pi.c_lo = hcounts[(size_t)p * ncpa::kScanMax];
+        pi.c_hi = hcounts[(size_t)p * ncpa::kScanMax + pi.n_scan - 1];
         pi.M = std::max(0, pi.c_hi - pi.c_lo);
         if (pi.M > M->prm.max_modes) {
             char buf[160];
@@ -971,7 +971,7 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
                                           prm->wvnum_filter, prm->c_min, prm->c_max, err));
     tm.mark("window");
     DevBuf counts, bis, ev, tot;
-    counts.alloc((size_t)P * ncpa::kScanPoints * 4, st);
+    counts.alloc((size_t)P * ncpa::kScanMax * 4, st);
     check_launch(ctx, ncpa::launch_wscan(st, P, d_pinfo, rows.as<double>(), counts.as<int>(), err));
     tm.mark("scan");
     const int cap_modes = M->prm.max_modes;

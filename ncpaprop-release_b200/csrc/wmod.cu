@@ -25,14 +25,14 @@ namespace ncpa {
 
 namespace {
 
-constexpr int kWScanThreads = kScanPoints / 2;  // two shifts per thread
+constexpr int kWScanThreads = kScanDefault / 2;  // two shifts per thread
 constexpr int kWsRows = 512;                    // rows per scan ring chunk (8 KB)
 constexpr int kWsBuf = 4;                       // scan ring slots
 
 __device__ __forceinline__ double wscan_x(double lo, double hi, int t) {
     if (t == 0) return lo;
-    if (t == kScanPoints - 1) return hi;
-    return lo + (hi - lo) * ((double)t / (double)(kScanPoints - 1));
+    if (t == kScanDefault - 1) return hi;
+    return lo + (hi - lo) * ((double)t / (double)(kScanDefault - 1));
 }
 
 }  // namespace
@@ -143,7 +143,7 @@ int launch_wmod_build(cudaStream_t st, int nk, const double* zk, const double* c
 }
 
 // ---------------------------------------------------------------------------
-// Isolation scan: kScanPoints counts per problem on an even grid of
+// Isolation scan: kScanDefault counts per problem on an even grid of
 // [kappa_min, kappa_max] (the layout k_make_items reads); the CTA streams the
 // rows through a kWsBuf-deep TMA ring, each thread runs two shifts
 // (WmodRows::pair: p_{-2} = -g0, p_{-1} = 1, p_i = t_i p_{i-1} - p_{i-2}).
@@ -195,8 +195,8 @@ __global__ void __launch_bounds__(kWScanThreads) k_wscan(const ProblemInfo* __re
                         &bars[slot]);
         }
     }
-    counts[(size_t)p * kScanPoints + t0] = A.cnt;
-    counts[(size_t)p * kScanPoints + t1] = B.cnt;
+    counts[(size_t)p * kScanMax + t0] = A.cnt;
+    counts[(size_t)p * kScanMax + t1] = B.cnt;
 }
 
 int launch_wscan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* rows, int* counts, unsigned* err) {
