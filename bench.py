@@ -236,6 +236,9 @@ def run_ours(args):
     # pinned host buffers the results of the end-to-end leg land in
     pin_tl = [torch.empty((NFREQ, N_TL), dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
     pin_wav = torch.empty((len(RANGES_KM), nfft), dtype=torch.float64).pin_memory().numpy()
+    # pinned buffers for the modes (k, attenuation, source / receiver values,
+    # group speeds), sized after the first end-to-end step
+    pin_modes = []
 
     def step_device():
         sre, sim = ctx.source_spectrum_waveform(x_w, t_w[1] - t_w[0], nfft, nf_dc)
@@ -252,7 +255,9 @@ def run_ours(args):
         xw = pin["x"].numpy()
         sre, sim = ctx.source_spectrum_waveform(xw, t_w[1] - t_w[0], nfft, nf_dc)
         m = ctx.solve(pr, params_dev, pin["f"].numpy(), az)
-        disp = m.all_modes()  # CSR offsets + k, attenuation, source / receiver values, group speeds
+        if not pin_modes or pin_modes[0].size < m.total_modes():
+            pin_modes[:] = [torch.empty(m.total_modes(), dtype=torch.float64).pin_memory().numpy() for _ in range(5)]
+        disp = m.all_modes(out=pin_modes)  # CSR offsets + k, attenuation, source / receiver values, group speeds
         tl = m.tl1d(N_TL, DR_TL, out=pin_tl)
         wav = m.bb_synthesize(ranges_m, MAX_CEL, nfft, sre, sim, out=pin_wav)
         nm = int(disp[0][-1])

@@ -474,6 +474,13 @@ class Modes:
     def counts(self):
         return np.array([self.count(p) for p in range(self.P)])
 
+    def total_modes(self):
+        """modes of all problems together (host bookkeeping, no device wait)"""
+        off = np.empty(self.P + 1, dtype=np.int32)
+        self.ctx.check(lib().ncpa_modes_get_all(self.h, off.ctypes.data_as(_ip), None, None, None, None, None),
+                       "ncpa_modes_get_all")
+        return int(off[-1])
+
     def problem(self, p) -> ProblemModes:
         M = self.count(p)
         vals = [_c_double() for _ in range(7)]
@@ -482,13 +489,21 @@ class Modes:
         self.ctx.check(lib().ncpa_modes_get(self.h, p, _p(kr), _p(ki), _p(vs), _p(vr), _p(vg)), "ncpa_modes_get")
         return ProblemModes(*[v.value for v in vals], kr, ki, vs, vr, vg)
 
-    def all_modes(self):
-        """(mode_off, kr, ki, vs, vr, vg) of every problem in CSR order."""
+    def all_modes(self, out=None):
+        """(mode_off, kr, ki, vs, vr, vg) of every problem in CSR order.  out:
+        five float64 arrays of at least the total mode count to copy into
+        (page-locked ones make the copies direct); the returned arrays are
+        views of their first entries."""
         off = np.empty(self.P + 1, dtype=np.int32)
         self.ctx.check(lib().ncpa_modes_get_all(self.h, off.ctypes.data_as(_ip), None, None, None, None, None),
                        "ncpa_modes_get_all")
         n = int(off[-1])
-        arrs = [np.empty(n) for _ in range(5)]
+        if out is None:
+            arrs = [np.empty(n) for _ in range(5)]
+        else:
+            if len(out) != 5 or any(a.dtype != np.float64 or a.size < n or not a.flags.c_contiguous for a in out):
+                raise ValueError("out: five contiguous float64 arrays of at least %d entries" % n)
+            arrs = [a.reshape(-1)[:n] for a in out]
         self.ctx.check(lib().ncpa_modes_get_all(self.h, off.ctypes.data_as(_ip), *[_p(a) for a in arrs]),
                        "ncpa_modes_get_all")
         return (off, *arrs)

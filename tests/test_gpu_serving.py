@@ -55,6 +55,14 @@ def test_solve_jobs_equals_one_solve_per_job(gpu):
     assert m.P == sum(len(j[1]) for j in jobs)
     re_b, im_b, _ = m.tl1d(NR, DR)
     off, kr, ki, vs, vr, _ = m.all_modes()  # bulk getter, CSR order
+    # the same into caller buffers (larger than needed)
+    n = m.total_modes()
+    assert n == off[-1]
+    bufs = [np.full(n + 7, np.nan) for _ in range(5)]
+    off2, kr2, ki2, vs2, vr2, _ = m.all_modes(out=bufs)
+    assert np.array_equal(off2, off) and np.array_equal(kr2, kr) and np.array_equal(vr2, vr)
+    assert kr2.base is bufs[0] or np.shares_memory(kr2, bufs[0])
+    assert np.isnan(bufs[0][n:]).all()
     for i in range(m.P):
         b = m.problem(i)
         assert off[i + 1] - off[i] == b.M
