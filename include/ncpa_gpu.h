@@ -447,11 +447,11 @@ ncpa_status ncpa_ctx_bisect_steps(ncpa_ctx *ctx, long long *steps, long long *de
 ncpa_status ncpa_ctx_sum_fixups(ncpa_ctx *ctx, long long *recomputed, long long *points);
 /* Error model of the last NCPA_SUM_TC_GUARDED modal sum of this context:
  * eps bounds the tensor-core error of a point relative to S, the sum of the
- * magnitudes of its modal terms at the first range of its 256-range tile
- * (|P_tc - P| <= eps S); points with |P_tc| < tau S were recomputed in FP64
- * (tau = eps (1 + 1 / d), d = 1 - 10^(-0.05 / 20)).  Both 0 before the
- * first guarded sum. */
-ncpa_status ncpa_ctx_sum_guard(ncpa_ctx *ctx, double *eps, double *tau);
+ * magnitudes of its modal terms at the first range of its tile of
+ * *tile_ranges ranges (|P_tc - P| <= eps S); points with |P_tc| < tau S were
+ * recomputed in FP64 (tau = eps (1 + 1 / d), d = 1 - 10^(-0.05 / 20)).  eps
+ * and tau are 0 before the first guarded sum; tile_ranges may be NULL. */
+ncpa_status ncpa_ctx_sum_guard(ncpa_ctx *ctx, double *eps, double *tau, int *tile_ranges);
 /* Schedule of the last tensor-core modal sum of this context: the depths of
  * its TMA ring and generated-operand ring.  The first tensor-core call of
  * each shape (format, receiver groups, mode chunks, range tiles) times every

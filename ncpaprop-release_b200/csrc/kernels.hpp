@@ -246,6 +246,8 @@ int launch_ms_prepare(cudaStream_t st, const MsPlan& p, int fmt, int n_rcv, int 
 int launch_ms_tc(cudaStream_t st, const MsPlan& p, int fmt, int n_ranges, const void* a_img, const void* q,
                  const void* tab, float* raw, float* s_part, unsigned* err, int variant);
 int ms_tc_variants();
+// ranges per tile of the tensor-core sums (the UMMA N)
+int ms_tile_ranges();
 void ms_tc_variant_shape(int fmt, int variant, int* t_stages, int* g_stages);
 // s_part non-NULL: flag the points the guarded sum must recompute into
 // fix_list / fix_count (zeroed by the caller)

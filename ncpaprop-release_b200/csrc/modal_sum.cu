@@ -1024,6 +1024,8 @@ const MsVariant& ms_variant_of(int fmt, int v) {
 
 int ms_tc_variants() { return kMsVariants; }
 
+int ms_tile_ranges() { return kMsNT; }
+
 void ms_tc_variant_shape(int fmt, int variant, int* t_stages, int* g_stages) {
     const MsVariant& v = ms_variant_of(fmt, variant < 0 || variant >= kMsVariants ? 0 : variant);
     *t_stages = v.ts;

@@ -1312,10 +1312,11 @@ ncpa_status ncpa_ctx_sum_fixups(ncpa_ctx* ctx, long long* recomputed, long long*
     });
 }
 
-ncpa_status ncpa_ctx_sum_guard(ncpa_ctx* ctx, double* eps, double* tau) {
+ncpa_status ncpa_ctx_sum_guard(ncpa_ctx* ctx, double* eps, double* tau, int* tile_ranges) {
     if (!ctx || !eps || !tau) return NCPA_EINVAL;
     *eps = ctx->ms_last_eps;
     *tau = ctx->ms_last_tau;
+    if (tile_ranges) *tile_ranges = ncpa::ms_tile_ranges();
     return NCPA_OK;
 }
 

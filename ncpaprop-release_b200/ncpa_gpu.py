@@ -179,7 +179,8 @@ def lib():
         L.ncpa_ctx_reset_stats.argtypes = [_vp]
         L.ncpa_ctx_sturm_steps.argtypes = [_vp, ctypes.POINTER(_c_ll)]
         L.ncpa_ctx_sum_fixups.argtypes = [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]
-        L.ncpa_ctx_sum_guard.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.ncpa_ctx_sum_guard.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(_c_int)]
         L.ncpa_ctx_sum_schedule.argtypes = [_vp, _ip, _ip, _ip, _dp]
         L.ncpa_ctx_bisect_steps.argtypes = [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]
         L.ncpa_probe_fp64_peak.argtypes = [_vp, _dp]
@@ -273,13 +274,14 @@ class Context:
         return a.value, b.value
 
     def sum_guard(self):
-        """(eps, tau) of the last guarded tensor-core modal sum: its error is
-        at most eps S (S = sum of the magnitudes of a point's modal terms at
-        its tile's first range) and points with |P| < tau S were recomputed
-        in FP64"""
-        e, t = ctypes.c_double(), ctypes.c_double()
-        self.check(lib().ncpa_ctx_sum_guard(self.h, ctypes.byref(e), ctypes.byref(t)), "ncpa_ctx_sum_guard")
-        return e.value, t.value
+        """(eps, tau, tile_ranges) of the last guarded tensor-core modal sum:
+        its error is at most eps S (S = sum of the magnitudes of a point's
+        modal terms at the first range of its tile of tile_ranges ranges) and
+        points with |P| < tau S were recomputed in FP64"""
+        e, t, n = ctypes.c_double(), ctypes.c_double(), _c_int()
+        self.check(lib().ncpa_ctx_sum_guard(self.h, ctypes.byref(e), ctypes.byref(t), ctypes.byref(n)),
+                   "ncpa_ctx_sum_guard")
+        return e.value, t.value, n.value
 
     def sum_schedule(self):
         """(TMA ring depth, operand ring depth, per-variant times in ms of the

@@ -127,7 +127,8 @@ def test_guarded_tensor_core_sum_every_point(gpu, solved, n_rcv, n_ranges, dr, l
     P, S = _ref_sum(g.kr, g.ki, g.vs, v[idx, :], n_ranges, dr, lossless=lossless)
     pg = m.tl_multi(0, h, n_ranges, dr, method=m.SUM_TC_GUARDED, lossless=lossless)
     fixed, points = gpu.sum_fixups()
-    eps, tau = gpu.sum_guard()
+    eps, tau, tile = gpu.sum_guard()
+    assert tile > 0
     assert points == n_rcv * n_ranges and 0 <= fixed < points
     # the guard's error model: |P_tc - P| <= eps S (S here at the point's own
     # range, which is at most the tile-start S the guard uses)

@@ -228,7 +228,7 @@ def test_tall_atmosphere_vs_oracle(gpu, workdir):
     nr2, dr2 = 20000, 100.0
     ptc = m.tl_multi(0, h, nr2, dr2, method=m.SUM_TC_GUARDED)
     fixed, points = gpu.sum_fixups()
-    guard_eps, guard_tau = gpu.sum_guard()
+    guard_eps, guard_tau, tile = gpu.sum_guard()
     m.close()
     prof.close()
     ore2, oim2 = np.empty((nr2, len(idx))), np.empty((nr2, len(idx)))
@@ -241,15 +241,15 @@ def test_tall_atmosphere_vs_oracle(gpu, workdir):
     # the error model behind the guard: |P_tc - P| <= eps S_tile at every
     # point the guard left to the tensor cores (eps as the library reports
     # it), S_tile = sum_m |A_jm| e^{-Im k_m r_0} at the first range r_0 of the
-    # point's 256-range tile (with the same 1000 * 4 pi / sqrt(8 pi r)
-    # scaling as P)
+    # point's tile (of the library's tile width; with the same
+    # 1000 * 4 pi / sqrt(8 pi r) scaling as P)
     k = o.kr + 1j * o.ki
     absA = np.abs(o.vs[None, :] * vz / np.sqrt(k)[None, :])
     r2 = (np.arange(nr2) + 1) * dr2
     c2 = 1000.0 * 4 * np.pi / np.sqrt(8 * np.pi * r2)
-    r_tile = (np.arange(nr2) // 256 * 256 + 1) * dr2
+    r_tile = (np.arange(nr2) // tile * tile + 1) * dr2
     po = (ore2 + 1j * oim2).T
-    st = (absA @ np.exp(-np.outer(o.ki, r_tile[::256]))).repeat(256, axis=1)[:, :nr2] * c2[None, :]
+    st = (absA @ np.exp(-np.outer(o.ki, r_tile[::tile]))).repeat(tile, axis=1)[:, :nr2] * c2[None, :]
     err_t = np.abs(ptc - po) / st
     kept = err_t > 1e-11  # the recomputed points agree with the oracle to round-off
     raw = float(err_t[kept].max())
