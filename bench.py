@@ -304,6 +304,20 @@ def run_ours(args):
     sturm_steps, deriv_steps = ctx.bisect_steps()
     phases = {ph: ctx.phase_stats(ph)[0] / n_ph for ph in
               ("knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec", "fetch")}
+    # the fused bisection + eigenvector launch the timed steps run, timed alone
+    ctx.reset_stats()
+    ctx.set_timing(2)
+    for _ in range(n_ph):
+        flush.zero_()
+        step_device()
+    torch.cuda.synchronize()
+    ctx.set_timing(False)
+    fused_ms, fused_n = ctx.phase_stats("bisect+eigvec")
+    phases["bisect+eigvec (fused)"] = fused_ms / max(fused_n, 1)
+    phases["eigvec-rest"] = ctx.phase_stats("eigvec-rest")[0] / n_ph
+    m_cnt = ctx.solve(prof, params_dev, freqs, az)
+    modes_total = m_cnt.total_modes()
+    m_cnt.close()
     if args.quick:
         if sampler:
             sampler.stop()
@@ -345,6 +359,14 @@ def run_ours(args):
         # per step of a Laguerre chain (p, p', p'': subtract, four FMAs, one add)
         flops = 3.0 * (sturm_steps - deriv_steps) + 10.0 * deriv_steps  # over the bis_n timed launches
         achieved = flops / (bis_ms / 1e3) / 1e12 if bis_ms > 0 else None
+        # the fused launch: the same bisection work plus the reduction-only
+        # eigenvector items, 7 flops per row and pass (square, add, multiply-
+        # add with the weight, subtract, multiply-add of the recurrence), two
+        # passes per mode
+        ev_flops = 14.0 * NZ * modes_total
+        fused_flops = (flops / bis_n if bis_n else 0.0) + ev_flops
+        fused_launch_ms = fused_ms / max(fused_n, 1)
+        fused_achieved = fused_flops / (fused_launch_ms / 1e3) / 1e12 if fused_ms > 0 else None
         cpu = cpu_baseline(freqs, max_seconds=args.cpu_seconds)
         cpu_lapack = lapack_baseline(freqs) if not args.no_lapack else None
         line = {
@@ -357,7 +379,7 @@ def run_ours(args):
                        "synthesis_ranges_km": "200-300/10", "nfft": nfft, "l2": "flushed (256 MiB write) between steps",
                        "eigen_solve": "fused bisection + eigenvector launch in the timed steps; phases_ms and the "
                                       "roofline time k_bisect and k_eigvec alone (per-phase timing runs them "
-                                      "separately)",
+                                      "separately) and the fused launch alone (roofline.fused)",
                        "parallelism": "replicas (one 256-frequency job per GPU)"},
             "e2e": {"value": round(e2e_value, 2), "unit": METRIC, "h2d_bytes_per_step": int(h2d[0]),
                     "d2h_bytes_per_step": int(d2h[0])},
@@ -372,7 +394,14 @@ def run_ours(args):
                          "flops_per_launch": flops / bis_n if bis_n else None,
                          "flops": "3 per count-chain step, 10 per Laguerre-chain step (p, p', p'')",
                          "chain_steps_per_launch": sturm_steps / bis_n if bis_n else None,
-                         "laguerre_chain_steps_per_launch": deriv_steps / bis_n if bis_n else None},
+                         "laguerre_chain_steps_per_launch": deriv_steps / bis_n if bis_n else None,
+                         "fused": {"kernel": "k_bisect_eigvec (the launch the timed steps run)",
+                                   "avg_launch_ms": round(fused_launch_ms, 4),
+                                   "flops_per_launch": fused_flops,
+                                   "achieved": round(fused_achieved, 3) if fused_achieved else None,
+                                   "frac": round(fused_achieved / fp64_peak, 4) if fused_achieved else None,
+                                   "flops": "the bisection's counted flops + 14 per grid row per mode for the "
+                                            "two eigenvector passes (%d modes)" % modes_total}},
             "phases_ms": {k: round(v, 4) for k, v in phases.items()},
             "plain_gpu": {"value": round(plain_rate, 2), "unit": METRIC,
                           "what": "one ncpa_ess_solve + TL per frequency, same workload"},

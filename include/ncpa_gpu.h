@@ -432,9 +432,13 @@ ncpa_status ncpa_profile_update(ncpa_profile *prof, const ncpa_profile_desc *des
 /* Diagnostics (no counterpart in the reference): per-phase device times of
  * ncpa_ess_solve measured with CUDA events on the context stream.  Phases:
  * "knots+grid", "matrix", "window", "scan", "host-items", "bisect", "eigvec",
- * "fetch".  stats() returns accumulated milliseconds and calls since the last
- * reset; sturm_steps() the number of Sturm recurrence steps (one shift over
- * one grid point) run by the bisection kernel since the last reset. */
+ * "fetch".  set_timing(ctx, 1) runs the bisection and eigenvector kernels
+ * apart; set_timing(ctx, 2) keeps the fused launch that solves without
+ * timing run, recorded as "bisect+eigvec" and "eigvec-rest" (the follow-up
+ * launch that runs only items the fused launch left).  stats() returns
+ * accumulated milliseconds and calls since the last reset; sturm_steps() the
+ * number of Sturm recurrence steps (one shift over one grid point) run by the
+ * bisection kernel since the last reset. */
 ncpa_status ncpa_ctx_set_timing(ncpa_ctx *ctx, int on);
 ncpa_status ncpa_ctx_phase_stats(const ncpa_ctx *ctx, const char *phase, double *total_ms, long long *calls);
 ncpa_status ncpa_ctx_reset_stats(ncpa_ctx *ctx);

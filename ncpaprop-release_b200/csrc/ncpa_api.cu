@@ -135,6 +135,7 @@ struct ncpa_ctx {
     DevBuf d_stats;                // device counters (Sturm sequences)
     bool timing = false;           // NCPA_TIMING=1: per-phase times on stderr
     bool stats = false;            // ncpa_ctx_set_timing: accumulate per phase
+    bool stats_fused = false;      // ncpa_ctx_set_timing(ctx, 2): ... keeping the fused launch
     std::map<std::string, std::pair<double, long long>> phase;
     std::map<std::string, std::array<int, 3>> tune_cache;  // plan shape -> tuned launch shapes
     void count(int n) { launches += n; }
@@ -554,7 +555,8 @@ void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_
     // fused bisection + eigenvectors (one launch, eigenvectors of finished
     // problems overlapping the others' bisection), unless per-phase timing or
     // step counts ask for the kernels alone, or group speeds are wanted
-    const bool fuse = ctx->fuse_solve && !ctx->timing && !ctx->stats && !count_steps && !prm->want_group_speed;
+    const bool fuse = ctx->fuse_solve && !ctx->timing && (!ctx->stats || ctx->stats_fused) && !count_steps &&
+                      !prm->want_group_speed;
     check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, b.counts.as<int>(), M->prm.max_modes, t.bis_item,
                                               b.bis.as<WorkItem>(), b.bis_cap, b.ev.as<WorkItem>(), b.ev_cap,
                                               b.tot.as<int>(), err, fuse ? b.pstat.as<int>() : nullptr));
@@ -593,10 +595,10 @@ void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_
         const int grid_f =
             std::min(grid_e, ctx->num_sms * (t.bis_ctas > 0 ? std::min(t.bis_ctas, fit_f) : fit_f));
         check_launch(ctx, ncpa::launch_bisect_eigvec(st, grid_f, fa));
-        tm.mark("bisect");
+        tm.mark("bisect+eigvec");
         ea.ev_done = fa.ev_done;  // the items the fused launch did not finish
         check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
-        tm.mark("eigvec");
+        tm.mark("eigvec-rest");
     } else {
         // ---- K3 bisection ----
         check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s, b.counts.as<int>(), b.bis.as<WorkItem>(), 0,
@@ -982,7 +984,7 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
     tot.alloc(4 * sizeof(int), st);
     // fused bisection + eigenvector launch, as on the ESS path (full vectors
     // excepted; kernels alone under per-phase timing)
-    const bool fuse = ctx->fuse_solve && !ctx->timing && !ctx->stats && !prm->want_vectors;
+    const bool fuse = ctx->fuse_solve && !ctx->timing && (!ctx->stats || ctx->stats_fused) && !prm->want_vectors;
     DevBuf pstat, fq;
     if (fuse) pstat.alloc((size_t)3 * P * sizeof(int), st);
     check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, counts.as<int>(), cap_modes, ncpa::kWItem,
@@ -1073,7 +1075,7 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
         fa.q_tail = fq.as<int>() + 2 * ev_cap + 1;
         fa.ea = ea;
         check_launch(ctx, ncpa::launch_bisect_eigvec_wmod(st, grid_f, fa));
-        tm.mark("bisect");
+        tm.mark("bisect+eigvec");
         ea.ev_done = fa.ev_done;  // the items the fused launch did not finish
         check_launch(ctx, ncpa::launch_eigvec_wmod(st, grid_e, ea));
     } else {
@@ -1087,7 +1089,7 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
         tm.mark("bisect");
         if (n_ev > 0) check_launch(ctx, ncpa::launch_eigvec_wmod(st, grid_e, ea));
     }
-    tm.mark("eigvec");
+    tm.mark(fused ? "eigvec-rest" : "eigvec");
     M->host_valid = false;
     if (!prm->keep_on_device) fetch_modes(M);
     check_device_status(ctx);
@@ -1252,8 +1254,9 @@ long long ncpa_kernel_launches(const ncpa_ctx* ctx) { return ctx ? ctx->launches
 void* ncpa_ctx_stream(ncpa_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 ncpa_status ncpa_ctx_set_timing(ncpa_ctx* ctx, int on) {
-    if (!ctx) return NCPA_EINVAL;
+    if (!ctx || on < 0 || on > 2) return NCPA_EINVAL;
     ctx->stats = on != 0;
+    ctx->stats_fused = on == 2;
     return NCPA_OK;
 }
 

@@ -248,6 +248,8 @@ class Context:
         return int(lib().ncpa_ctx_stream(self.h) or 0)
 
     def set_timing(self, on=True):
+        """per-phase device times: on = True / 1 runs the bisection and
+        eigenvector kernels apart, 2 keeps the fused launch ("bisect+eigvec")"""
         self.check(lib().ncpa_ctx_set_timing(self.h, int(on)), "ncpa_ctx_set_timing")
 
     def reset_stats(self):
