@@ -654,7 +654,7 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
         prepare_solve(ctx, M, prm, t.bis_item, b, s.as<double>(), w.as<double>(), g.as<double>());
         unsigned h_err = 0;
         enqueue_solve(ctx, tm, M, prm, wkb, s.as<double>(), w.as<double>(), g.as<double>(), kz2.as<double>(), b, t,
-                      ctx->stats, ctx->h_tot, M->info.data(), &h_err);
+                      ctx->stats && !ctx->stats_fused, ctx->h_tot, M->info.data(), &h_err);
         finish_solve(ctx, tm, M, ctx->h_tot, &h_err);
         return;
     }

@@ -51,3 +51,36 @@ def test_fused_unfused_and_fallback_identical(analytic_profile, method):
         for f in ("kr", "ki", "vs", "vr"):
             assert np.array_equal(getattr(a, f), getattr(b, f))
             assert np.array_equal(getattr(a, f), getattr(c, f))
+
+
+@pytest.mark.parametrize("method", [0, 1])
+def test_timing_that_keeps_the_fused_launch(gpu, analytic_profile, method):
+    """set_timing(2) times the fused launch as one phase ("bisect+eigvec") and
+    gives the modes of an untimed solve bit for bit; set_timing(1) times the
+    kernels apart ("bisect", "eigvec")."""
+    import ncpa_gpu
+
+    prof = gpu.load_profile(analytic_profile)
+    freqs = np.linspace(0.01, 0.4, 24)
+    prm = ncpa_gpu.default_params(nz_grid=8000, turnoff_wkb=1, method=method)
+
+    def solve():
+        m = gpu.solve(prof, prm, freqs, [90.0])
+        out = [m.problem(p) for p in range(m.P)]
+        m.close()
+        return out
+
+    ref = solve()
+    for mode, phase, other in ((2, "bisect+eigvec", "bisect"), (1, "bisect", "bisect+eigvec")):
+        gpu.reset_stats()
+        gpu.set_timing(mode)
+        got = solve()
+        gpu.set_timing(False)
+        ms, n = gpu.phase_stats(phase)
+        assert n == 1 and ms > 0, (mode, phase, ms, n)
+        assert gpu.phase_stats(other)[1] == 0, (mode, other)
+        for a, b in zip(ref, got):
+            assert a.M == b.M
+            for k in ("kr", "ki", "vs", "vr"):
+                assert np.array_equal(getattr(a, k), getattr(b, k)), (mode, k)
+    prof.close()
