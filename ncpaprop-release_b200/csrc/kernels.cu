@@ -1182,13 +1182,63 @@ __device__ __forceinline__ void bisect_item(const ProblemInfo* __restrict__ pinf
     if (lane < w.m) mu[pi.off + w.j0 + lane] = x;
 }
 
+// Bisection item scheduler.  The item list is cost-ordered, heaviest first
+// (k_make_items with order 1).  On each warp scheduler (SM and sub-partition)
+// the first warp to arrive takes items from the heavy end of the list and the
+// next workers - 1 from the light end, so a scheduler runs a heavy and a
+// light item side by side; later warps run no bisection (in the fused launch
+// they go straight to the eigenvector queue).  A worker first draws a ticket
+// (n tickets for n items) and then an index from its end of the list: front
+// and back indices never meet, so every item runs exactly once.  Where the
+// CTAs land only decides the balance: the first warp on every scheduler is a
+// worker.  sched: kSchedInts ints zeroed before the launch; null keeps plain
+// round-robin (item q to warp q mod (grid x kWarpsPerCta)).
+struct ItemSched {
+    int* S;
+    int role;     // 0: none, 1: heavy end, 2: light end
+    bool worker;  // the warp runs bisection items (every warp without sched)
+    __device__ ItemSched(int* sched, int workers) : S(sched), role(0), worker(true) {
+        if (!S) return;
+        const int lane = threadIdx.x & 31;
+        if (lane == 0) {
+            // the warp's SM and its sub-partition (hardware warp slot mod 4; a
+            // CTA's warp index does not determine it)
+            unsigned smid, slot;
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+            asm volatile("mov.u32 %0, %%warpid;" : "=r"(slot));
+            const int key = smid < (unsigned)kSchedSms ? (int)(smid * 4 + (slot & 3u)) : -1;
+            const int k = key >= 0 ? atomicAdd(S + 3 + key, 1) : 0;
+            role = k == 0 ? 1 : (k < workers ? 2 : 0);
+        }
+        role = __shfl_sync(0xffffffffu, role, 0);
+        worker = role != 0;
+    }
+    // next item of this warp (-1: none left); walk = plain round-robin position
+    __device__ long long next(int n, long long& walk, long long stride) {
+        if (!S) {
+            const long long it = walk;
+            walk += stride;
+            return it < n ? it : -1;
+        }
+        if (!role) return -1;
+        int it = -1;
+        if ((threadIdx.x & 31) == 0) {
+            if (atomicAdd(S, 1) < n) it = role == 1 ? atomicAdd(S + 1, 1) : n - 1 - atomicAdd(S + 2, 1);
+        }
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it < 0) role = 0;
+        return it;
+    }
+};
+
 // Row: the row format (EssRows: shifts in h^2 k^2; WmodRows: kappa = h k);
 // tol is scaled per problem by Row::tol_scale.
 template <class Row>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
     k_bisect(const ProblemInfo* __restrict__ pinfo, const double* __restrict__ s, const int* __restrict__ counts,
              const WorkItem* __restrict__ items, int n_items, int* counter, double tol_in, double* __restrict__ mu,
-             unsigned* err, unsigned long long* step_counter, const int* __restrict__ n_items_dev) {
+             unsigned* err, unsigned long long* step_counter, const int* __restrict__ n_items_dev, int* sched,
+             int workers) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     if (n_items_dev) n_items = *n_items_dev;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1201,11 +1251,11 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
         fence_mbar_init();
     }
     __syncwarp();
-    // static round-robin over the grid's warps: item g goes to warp g of the
-    // first wave, so the items spread evenly over the SMs whatever the grid
+    // items to warps: ItemSched
     (void)counter;
-    const int warps_total = gridDim.x * kWarpsPerCta;
-    for (int it = blockIdx.x * kWarpsPerCta + wid; it < n_items; it += warps_total)
+    ItemSched sc(sched, workers);
+    long long walk = (long long)blockIdx.x * kWarpsPerCta + wid;
+    for (long long it; (it = sc.next(n_items, walk, (long long)gridDim.x * kWarpsPerCta)) >= 0;)
         bisect_item<Row>(pinfo, s, counts, items[it], tol_in, mu, err, step_counter, r);
 }
 
@@ -1214,11 +1264,11 @@ static size_t bisect_smem() { return (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8
 template <class Row>
 static int bisect_launch(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
                          const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
-                         unsigned long long* step_counter, const int* n_items_dev) {
+                         unsigned long long* step_counter, const int* n_items_dev, int* sched, int workers) {
     const size_t sm = bisect_smem();
     cudaFuncSetAttribute(k_bisect<Row>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_bisect<Row><<<grid, kWarpsPerCta * 32, sm, st>>>(pinfo, s, counts, items, n_items, counter, tol, mu, err,
-                                                       step_counter, n_items_dev);
+                                                       step_counter, n_items_dev, sched, workers);
     return 1;
 }
 
@@ -1234,18 +1284,18 @@ static int bisect_fit() {
 
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
                   const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
-                  unsigned long long* step_counter, const int* n_items_dev) {
+                  unsigned long long* step_counter, const int* n_items_dev, int* sched, int workers) {
     return bisect_launch<EssRows>(st, grid, pinfo, s, counts, items, n_items, counter, tol, mu, err, step_counter,
-                                  n_items_dev);
+                                  n_items_dev, sched, workers);
 }
 
 int bisect_ctas_per_sm() { return bisect_fit<EssRows>(); }
 
 int launch_bisect_wmod(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* rows, const int* counts,
                        const WorkItem* items, double tol, double* mu, unsigned* err,
-                       unsigned long long* step_counter, const int* n_items_dev) {
+                       unsigned long long* step_counter, const int* n_items_dev, int* sched, int workers) {
     return bisect_launch<WmodRows>(st, grid, pinfo, rows, counts, items, 0, nullptr, tol, mu, err, step_counter,
-                                   n_items_dev);
+                                   n_items_dev, sched, workers);
 }
 
 int bisect_wmod_ctas_per_sm() { return bisect_fit<WmodRows>(); }
@@ -1273,13 +1323,31 @@ __device__ int block_exclusive_scan(int v, int* sh, int* total) {
     return incl - v;
 }
 
+// Cost-ordered bisection items.  Every item of a problem sweeps the problem's
+// nz rows once per multisection round, and the items of problems with more
+// eigenvalues per item and more modes need more rounds, so an item's cost is
+// taken as nz x m x (1 + M / 512) (m = M / items of the problem).  With order
+// set and P <= kRankMax, the problems are ranked by that cost (descending,
+// ties by index, so the list is deterministic) and their bisection items are
+// listed in rank order; the warp mapping of the bisection kernels then puts
+// the heaviest items on different warp schedulers.  Eigenvector items and the
+// mode offsets stay in problem order.
+constexpr int kRankMax = 4096;
+
+__device__ __forceinline__ float item_cost(int nz, int M, int nb) {
+    return nb > 0 ? (float)nz * ((float)M / (float)nb) * (1.0f + (float)M * (1.0f / 512.0f)) : 0.0f;
+}
+
 __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo* __restrict__ pinfo,
                                                              const int* __restrict__ counts, int max_modes,
                                                              int bis_item, WorkItem* __restrict__ bis, int bis_cap,
                                                              WorkItem* __restrict__ ev, int ev_cap,
                                                              int* __restrict__ tot, unsigned* __restrict__ err,
-                                                             int* __restrict__ pstat) {
+                                                             int* __restrict__ pstat, int order) {
     __shared__ int sh[kItemThreads];
+    __shared__ float skey[kRankMax];
+    __shared__ int sperm[kRankMax];
+    const bool ranked = order != 0 && P <= kRankMax;
     int base_m = 0, base_b = 0, base_e = 0;
     for (int p0 = 0; p0 < P; p0 += kItemThreads) {
         const int p = p0 + threadIdx.x;
@@ -1297,6 +1365,7 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
             pinfo[p].M = M;
             nb = (M + bis_item - 1) / bis_item;
             ne = (M + kEvItem - 1) / kEvItem;
+            if (ranked) skey[p] = item_cost(pinfo[p].nz, M, nb);
         }
         int tm, tb, te;
         const int om = block_exclusive_scan(M, sh, &tm);
@@ -1310,11 +1379,12 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
         }
         if (p < P) {
             pinfo[p].off = base_m + om;
-            for (int k = 0; k < nb; ++k) {
-                const int j0 = (int)((long long)M * k / nb), j1 = (int)((long long)M * (k + 1) / nb);
-                const int q = base_b + ob + k;
-                if (q < bis_cap) bis[q] = WorkItem{p, j0, j1 - j0, 0};
-            }
+            if (!ranked)
+                for (int k = 0; k < nb; ++k) {
+                    const int j0 = (int)((long long)M * k / nb), j1 = (int)((long long)M * (k + 1) / nb);
+                    const int q = base_b + ob + k;
+                    if (q < bis_cap) bis[q] = WorkItem{p, j0, j1 - j0, 0};
+                }
             for (int k = 0; k < ne; ++k) {
                 const int q = base_e + oe + k;
                 if (q < ev_cap) ev[q] = WorkItem{p, k * kEvItem, min(kEvItem, M - k * kEvItem), 0};
@@ -1323,6 +1393,37 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
         base_m += tm;
         base_b += tb;
         base_e += te;
+    }
+    if (ranked) {
+        __syncthreads();  // skey and this block's pinfo[].M writes visible
+        for (int p = threadIdx.x; p < P; p += kItemThreads) {
+            const float kp = skey[p];
+            int r = 0;
+            for (int q = 0; q < P; ++q) {
+                const float kq = skey[q];
+                r += (kq > kp || (kq == kp && q < p)) ? 1 : 0;
+            }
+            sperm[r] = p;
+        }
+        __syncthreads();
+        int base_r = 0;
+        for (int r0 = 0; r0 < P; r0 += kItemThreads) {
+            const int r = r0 + threadIdx.x;
+            int p = 0, M = 0, nb = 0;
+            if (r < P) {
+                p = sperm[r];
+                M = pinfo[p].M;
+                nb = (M + bis_item - 1) / bis_item;
+            }
+            int tb;
+            const int ob = block_exclusive_scan(nb, sh, &tb);
+            for (int k = 0; k < nb; ++k) {
+                const int j0 = (int)((long long)M * k / nb), j1 = (int)((long long)M * (k + 1) / nb);
+                const int q = base_r + ob + k;
+                if (q < bis_cap) bis[q] = WorkItem{p, j0, j1 - j0, 0};
+            }
+            base_r += tb;
+        }
     }
     if (threadIdx.x == 0) {
         if (base_b > bis_cap || base_e > ev_cap) atomicOr(err, kErrTooMany);
@@ -1334,10 +1435,10 @@ __global__ void __launch_bounds__(kItemThreads) k_make_items(int P, ProblemInfo*
 
 int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes, int bis_item,
                       WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err,
-                      int* pstat) {
+                      int* pstat, int order) {
     if (bis_item < 1 || bis_item > kWItem) return -1;
     k_make_items<<<1, kItemThreads, 0, st>>>(P, pinfo, counts, max_modes, bis_item, bis_items, bis_cap, ev_items,
-                                             ev_cap, tot, err, pstat);
+                                             ev_cap, tot, err, pstat, order);
     return 1;
 }
 
@@ -2166,8 +2267,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4) k_bisect_eigvec(FusedArg
     const int P = F.P;
     // ---- bisection items; the last item of a problem publishes its eigenvector items ----
     const int n_bis = *F.n_bis_dev;
-    const int warps_total = gridDim.x * kWarpsPerCta;
-    for (int it = blockIdx.x * kWarpsPerCta + wid; it < n_bis; it += warps_total) {
+    ItemSched sc(F.sched, F.workers);
+    long long walk = (long long)blockIdx.x * kWarpsPerCta + wid;
+    for (long long it; (it = sc.next(n_bis, walk, (long long)gridDim.x * kWarpsPerCta)) >= 0;) {
         const WorkItem w = F.bis[it];
         bisect_item<Row>(F.pinfo, F.s, F.counts, w, F.tol, F.mu, F.err, nullptr, r);
         __threadfence();  // this lane's eigenvalues visible before the count below
@@ -2182,6 +2284,10 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 4) k_bisect_eigvec(FusedArg
         __syncwarp();
     }
     // ---- eigenvector items from the ready queue ----
+    // with ev_workers_only, warps that ran no bisection leave the eigenvector
+    // items to the bisection warps (as those finish) and to the k_eigvec
+    // launch that follows, instead of competing with the bisection
+    if (F.ev_workers_only && !sc.worker) return;
     const int n_ev = *F.ea.n_items_dev;
     const size_t gw = (size_t)blockIdx.x * kEvWarps + wid;
     double* ck1 = F.ea.ck_q1 + gw * F.ea.ck_slot_stride;

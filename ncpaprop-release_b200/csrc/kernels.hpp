@@ -59,6 +59,11 @@ constexpr int kThreads = 256;     // threads of the scan CTAs
 constexpr int kWItem = 32;        // eigenvalues per warp work item of the bisection
 constexpr int kEvItem = 32;       // eigenvalues per warp work item of the eigenvector kernel
 constexpr int kEvWarpsPerCta = 4; // warps per eigenvector CTA
+// bisection item scheduler state (ints): ticket, heavy-end and light-end
+// counters, then one arrival counter per (SM < kSchedSms, sub-partition)
+constexpr int kSchedSms = 256;
+constexpr int kSchedInts = 3 + 4 * kSchedSms;
+constexpr int kSchedWorkers = 2;  // default bisection warps per warp scheduler
 
 // knot-level derived quantities
 int launch_steffen(cudaStream_t st, int n, const double* x, const double* y, int batch, int ystride,
@@ -93,10 +98,14 @@ int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2,
 // problem at counts[p * kScanMax + t]
 int launch_scan(cudaStream_t st, int P, ProblemInfo* pinfo, const double* s, int* counts, unsigned* err);
 // multisection/bisection over work items (K3); step_counter (optional)
-// accumulates the Sturm recurrence steps swept
+// accumulates the Sturm recurrence steps swept; sched (kSchedInts ints,
+// zeroed) runs a cost-ordered item list (order = 1 in launch_make_items) with
+// `workers` warps per warp scheduler (the first from the heavy end of the
+// list, the others from the light end); null maps items round-robin
 int launch_bisect(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* s, const int* counts,
                   const WorkItem* items, int n_items, int* counter, double tol, double* mu, unsigned* err,
-                  unsigned long long* step_counter, const int* n_items_dev = nullptr);
+                  unsigned long long* step_counter, const int* n_items_dev = nullptr, int* sched = nullptr,
+                  int workers = kSchedWorkers);
 int bisect_ctas_per_sm();
 // FP64 throughput probe: each thread runs n_iter iterations of 8 independent
 // FMA chains; out receives a value that keeps the chains live
@@ -149,6 +158,9 @@ struct FusedArgs {
     int* q_tail;
     int* ev_done;
     unsigned long long wait_ns;  // a consumer gives up on an empty slot after this long
+    int* sched;                  // bisection item scheduler (kSchedInts, zeroed) or null (round-robin)
+    int workers;                 // bisection warps per warp scheduler with sched
+    int ev_workers_only;         // only warps that ran bisection take eigenvector items
     EigvecArgs ea;
 };
 int launch_bisect_eigvec(cudaStream_t st, int grid, const FusedArgs& a);
@@ -162,10 +174,12 @@ int fused_wmod_ctas_per_sm();
 // tot = {n_bisect_items, n_eigvec_items, total modes}.  Sets kErrTooMany if a
 // problem exceeds max_modes (its M is then clamped) or a capacity is exceeded.
 // pstat (optional, 3 P ints): per problem the number of bisection items, the
-// first eigenvector item and the number of eigenvector items
+// first eigenvector item and the number of eigenvector items.  order = 1
+// lists the bisection items by estimated cost, heaviest problems first (for
+// P <= 4096; problem order otherwise)
 int launch_make_items(cudaStream_t st, int P, ProblemInfo* pinfo, const int* counts, int max_modes, int bis_item,
                       WorkItem* bis_items, int bis_cap, WorkItem* ev_items, int ev_cap, int* tot, unsigned* err,
-                      int* pstat = nullptr);
+                      int* pstat = nullptr, int order = 0);
 // resident eigenvector CTAs per SM for the variant selected by a
 int eigvec_ctas_per_sm(const EigvecArgs& a);
 // modal sums
@@ -212,7 +226,8 @@ int launch_wscan(cudaStream_t st, int P, const ProblemInfo* pinfo, const double*
 // launch_bisect does
 int launch_bisect_wmod(cudaStream_t st, int grid, const ProblemInfo* pinfo, const double* rows, const int* counts,
                        const WorkItem* items, double tol, double* mu, unsigned* err,
-                       unsigned long long* step_counter, const int* n_items_dev);
+                       unsigned long long* step_counter, const int* n_items_dev, int* sched = nullptr,
+                       int workers = kSchedWorkers);
 int bisect_wmod_ctas_per_sm();
 // eigenvectors of the wide-angle rows: EigvecArgs with s = rows, mu = kappa,
 // g = null; vectors normalised to sum v^2 dz = 1 / (1 + k^2)

@@ -125,6 +125,15 @@ struct ncpa_ctx {
     int ms_last_variant = 0, ms_last_fmt = 0;
     std::vector<double> ms_last_times;  // per variant, ms, of the last tuning run
     int item_override = 0;         // eigenvalues per bisection item (0: chosen per solve); NCPA_BISECT_ITEM
+    // bisection items listed by estimated cost and spread over the warp
+    // schedulers (heaviest first); NCPA_BISECT_ORDER=0 keeps problem order and
+    // round-robin warps.  Results do not depend on it.
+    bool bis_order = true;
+    int bis_workers = ncpa::kSchedWorkers;  // bisection warps per warp scheduler; NCPA_BISECT_WORKERS
+    // fused launch: only the bisection warps take eigenvector items (as their
+    // bisection ends), the others leave them to the k_eigvec launch that
+    // follows; NCPA_FUSE_EV_WORKERS=0 lets every warp of the launch take them
+    bool fuse_ev_workers = true;
     bool fuse_solve = true;        // fused bisection + eigenvector launch; NCPA_FUSE_SOLVE=0 turns it off
     // how long a consumer of the fused launch waits for an empty queue slot
     // before leaving the item to the following launch; NCPA_FUSE_WAIT_NS
@@ -461,7 +470,7 @@ struct Tuning {
 // scratch is the context's (grown on demand) unless own_ck is set (a
 // captured graph must keep its addresses for good).
 struct SolveBufs {
-    DevBuf counts, bis, ev, tot, mu, counter;
+    DevBuf counts, bis, ev, tot, mu, counter, sched;
     DevBuf pstat, fq;  // fused launch: per-problem readiness; ready queue, done flags, queue counters
     DevBuf ck1, ck2, cke;
     bool own_ck = false;
@@ -515,6 +524,7 @@ void prepare_solve(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, int
     b.fq.alloc(((size_t)2 * b.ev_cap + 2) * sizeof(int), st);
     b.mu.alloc(mcap * 8, st);
     b.counter.alloc(2 * sizeof(int), st);
+    b.sched.alloc(ncpa::kSchedInts * sizeof(int), st);
     M->d_kr.alloc(mcap * 8, st);
     M->d_ki.alloc(mcap * 8, st);
     M->d_vs.alloc(mcap * 8, st);
@@ -559,8 +569,14 @@ void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_
                       !prm->want_group_speed;
     check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, b.counts.as<int>(), M->prm.max_modes, t.bis_item,
                                               b.bis.as<WorkItem>(), b.bis_cap, b.ev.as<WorkItem>(), b.ev_cap,
-                                              b.tot.as<int>(), err, fuse ? b.pstat.as<int>() : nullptr));
+                                              b.tot.as<int>(), err, fuse ? b.pstat.as<int>() : nullptr,
+                                              ctx->bis_order ? 1 : 0));
     CK(cudaMemsetAsync(b.counter.p, 0, 2 * sizeof(int), st));
+    int* sched = nullptr;
+    if (ctx->bis_order) {
+        sched = b.sched.as<int>();
+        CK(cudaMemsetAsync(sched, 0, ncpa::kSchedInts * sizeof(int), st));
+    }
     tm.mark("host-items");
     const int fit_b = ncpa::bisect_ctas_per_sm();
     const int grid_b = ctx->num_sms * (t.bis_ctas > 0 ? std::min(t.bis_ctas, fit_b) : fit_b);
@@ -587,6 +603,9 @@ void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_
         fa.queue = fq;
         fa.ev_done = fq + b.ev_cap;
         fa.wait_ns = ctx->fuse_wait_ns;
+        fa.sched = sched;
+        fa.workers = ctx->bis_workers;
+        fa.ev_workers_only = ctx->fuse_ev_workers && sched ? 1 : 0;
         fa.q_head = fq + 2 * b.ev_cap;
         fa.q_tail = fq + 2 * b.ev_cap + 1;
         fa.ea = ea;
@@ -604,7 +623,7 @@ void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_
         check_launch(ctx, ncpa::launch_bisect(st, grid_b, d_pinfo, s, b.counts.as<int>(), b.bis.as<WorkItem>(), 0,
                                               b.counter.as<int>(), kBisectTol, b.mu.as<double>(), err,
                                               count_steps ? ctx->d_stats.as<unsigned long long>() : nullptr,
-                                              b.tot.as<int>()));
+                                              b.tot.as<int>(), sched, ctx->bis_workers));
         tm.mark("bisect");
         // ---- K4 eigenvectors ----
         check_launch(ctx, ncpa::launch_eigvec(st, grid_e, ea));
@@ -985,11 +1004,18 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
     // fused bisection + eigenvector launch, as on the ESS path (full vectors
     // excepted; kernels alone under per-phase timing)
     const bool fuse = ctx->fuse_solve && !ctx->timing && (!ctx->stats || ctx->stats_fused) && !prm->want_vectors;
-    DevBuf pstat, fq;
+    DevBuf pstat, fq, sched_buf;
     if (fuse) pstat.alloc((size_t)3 * P * sizeof(int), st);
+    int* sched = nullptr;
+    if (ctx->bis_order) {
+        sched_buf.alloc(ncpa::kSchedInts * sizeof(int), st);
+        sched = sched_buf.as<int>();
+        CK(cudaMemsetAsync(sched, 0, ncpa::kSchedInts * sizeof(int), st));
+    }
     check_launch(ctx, ncpa::launch_make_items(st, P, d_pinfo, counts.as<int>(), cap_modes, ncpa::kWItem,
                                               bis.as<WorkItem>(), bis_cap, ev.as<WorkItem>(), ev_cap,
-                                              tot.as<int>(), err, fuse ? pstat.as<int>() : nullptr));
+                                              tot.as<int>(), err, fuse ? pstat.as<int>() : nullptr,
+                                              ctx->bis_order ? 1 : 0));
     // mode counts to the host (sizes of the outputs and of the vectors)
     int* h_tot = ctx->h_tot;
     unsigned h_err = 0;
@@ -1071,6 +1097,9 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
         fa.queue = fq.as<int>();
         fa.ev_done = fq.as<int>() + ev_cap;
         fa.wait_ns = ctx->fuse_wait_ns;
+        fa.sched = sched;
+        fa.workers = ctx->bis_workers;
+        fa.ev_workers_only = ctx->fuse_ev_workers && sched ? 1 : 0;
         fa.q_head = fq.as<int>() + 2 * ev_cap;
         fa.q_tail = fq.as<int>() + 2 * ev_cap + 1;
         fa.ea = ea;
@@ -1084,7 +1113,7 @@ void solve_wmod(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, std::v
             check_launch(ctx, ncpa::launch_bisect_wmod(st, grid_b, d_pinfo, rows.as<double>(), counts.as<int>(),
                                                        bis.as<WorkItem>(), kWmodTol, mu.as<double>(), err,
                                                        ctx->stats ? ctx->d_stats.as<unsigned long long>() : nullptr,
-                                                       tot.as<int>()));
+                                                       tot.as<int>(), sched, ctx->bis_workers));
         }
         tm.mark("bisect");
         if (n_ev > 0) check_launch(ctx, ncpa::launch_eigvec_wmod(st, grid_e, ea));
@@ -1393,6 +1422,12 @@ ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
         if (const char* fv = std::getenv("NCPA_FUSE_SOLVE")) ctx->fuse_solve = fv[0] != '0';
         if (const char* wv = std::getenv("NCPA_FUSE_WAIT_NS")) ctx->fuse_wait_ns = std::strtoull(wv, nullptr, 10);
         if (const char* mv = std::getenv("NCPA_MS_TUNE")) ctx->ms_tune = mv[0] != '0';
+        if (const char* ov = std::getenv("NCPA_BISECT_ORDER")) ctx->bis_order = ov[0] != '0';
+        if (const char* ev = std::getenv("NCPA_FUSE_EV_WORKERS")) ctx->fuse_ev_workers = ev[0] != '0';
+        if (const char* wv = std::getenv("NCPA_BISECT_WORKERS")) {
+            const int v = std::atoi(wv);
+            if (v >= 1 && v <= 16) ctx->bis_workers = v;
+        }
         // tuning override of the eigenvalues per bisection item (1..32)
         if (const char* iv = std::getenv("NCPA_BISECT_ITEM")) {
             const int v = std::atoi(iv);

@@ -84,3 +84,62 @@ def test_timing_that_keeps_the_fused_launch(gpu, analytic_profile, method):
             for k in ("kr", "ki", "vs", "vr"):
                 assert np.array_equal(getattr(a, k), getattr(b, k)), (mode, k)
     prof.close()
+
+
+@pytest.mark.parametrize("method", [0, 1])
+def test_bisection_scheduling_modes_identical(analytic_profile, method):
+    """The bisection item scheduler (cost-ordered items, two warps per warp
+    scheduler taking items from the two ends of the list) decides only which
+    warp runs an item: plain round-robin, other worker counts, and letting
+    every warp of the fused launch take eigenvector items give the same modes
+    bit for bit."""
+    ref = _solve(analytic_profile, {}, method)
+    variants = (
+        {"NCPA_BISECT_ORDER": "0"},
+        {"NCPA_BISECT_WORKERS": "1"},
+        {"NCPA_BISECT_WORKERS": "3", "NCPA_FUSE_EV_WORKERS": "0"},
+        {"NCPA_FUSE_SOLVE": "0"},
+    )
+    for env in variants:
+        got = _solve(analytic_profile, env, method)
+        assert len(got) == len(ref)
+        for a, b in zip(ref, got):
+            assert a.M == b.M, env
+            for f in ("kr", "ki", "vs", "vr"):
+                assert np.array_equal(getattr(a, f), getattr(b, f)), (env, f)
+
+
+def test_scheduler_with_more_problems_than_the_ranking_covers(analytic_profile):
+    """Above 4096 problems the item list stays in problem order (no cost
+    ranking); the scheduler still runs every item once: same modes as plain
+    round-robin."""
+    import ncpa_gpu
+
+    def solve(env):
+        old = {k: os.environ.get(k) for k in env}
+        os.environ.update(env)
+        try:
+            ctx = ncpa_gpu.Context(0)
+        finally:
+            for k, v in old.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        prof = ctx.load_profile(analytic_profile)
+        freqs = np.linspace(0.005, 0.05, 41)
+        az = np.linspace(0.0, 357.0, 101)
+        m = ctx.solve(prof, ncpa_gpu.default_params(nz_grid=1500, turnoff_wkb=1, max_modes=200), freqs, az)
+        assert m.P == 4141
+        off, kr, ki, vs, vr, _ = m.all_modes()
+        out = (off.copy(), kr.copy(), ki.copy(), vs.copy(), vr.copy())
+        m.close()
+        prof.close()
+        ctx.close()
+        return out
+
+    a = solve({})
+    b = solve({"NCPA_BISECT_ORDER": "0"})
+    assert a[0][-1] > 4141
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
