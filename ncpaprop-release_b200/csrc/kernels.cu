@@ -2357,18 +2357,22 @@ int launch_bisect_eigvec_wmod(cudaStream_t st, int grid, const FusedArgs& a) {
 }
 
 // ===========================================================================
-// K5: 1-D transmission loss, modes staged in shared memory.  Each thread
-// covers kTlRun consecutive ranges: per mode the phase of its first range is
-// e^{(i k_r - k_i) r_b} (the block's first range, one sincos per mode and
-// block) times the powers e^{(i k_r - k_i) kTlRun dr 2^b} for the set bits b
-// of the thread index (each from its own sincos, staged per mode), and the
-// next ranges follow by the per-mode step e^{(i k_r - k_i) dr}: at most
-// kTlBits + kTlRun - 1 complex products, a few ulps each.
+// K5: 1-D transmission loss.  One CTA per (problem, chunk of kTlRanges
+// ranges), so a batch's problems (2 to ~300 modes each) spread over many
+// small CTAs instead of one CTA per problem.  Modes are staged in shared
+// memory in tiles: per mode the amplitude c = V_s V_r / sqrt(k) (principal
+// root), V_s^2 V_r^2 / |k| for the incoherent sum, the step w = e^{(i k_r -
+// k_i) dr}, the chunk's first phase e^{(i k_r - k_i) r_b} and the powers
+// w4^(2^b), w4 = e^{(i k_r - k_i) kTlRun dr} (each from the one before by
+// squaring: the relative error grows to about 2^6 ulps).  A thread covers kTlRun
+// consecutive ranges: its first phase is the chunk's times the powers of
+// its index's set bits, the next ones follow by w.
 // ===========================================================================
-constexpr int kTlTile = 128;
 constexpr int kTlRun = 4;      // consecutive ranges per thread
-constexpr int kTlThreads = 256;
-constexpr int kTlBits = 8;     // thread index bits (kTlThreads = 2^kTlBits)
+constexpr int kTlThreads = 64;
+constexpr int kTlBits = 6;     // thread index bits (kTlThreads = 2^kTlBits)
+constexpr int kTlRanges = kTlThreads * kTlRun;
+constexpr int kTlTile = 128;   // modes per shared-memory tile
 static_assert(kTlThreads == 1 << kTlBits, "the powers cover every thread index");
 
 __global__ void __launch_bounds__(kTlThreads) k_tl1d(const ProblemInfo* __restrict__ pinfo,
@@ -2377,51 +2381,53 @@ __global__ void __launch_bounds__(kTlThreads) k_tl1d(const ProblemInfo* __restri
                                                      int nr, double dr, int lossless, double* __restrict__ re,
                                                      double* __restrict__ im, double* __restrict__ incoh) {
     const int p = blockIdx.y;
-    const int i0 = (blockIdx.x * kTlThreads + threadIdx.x) * kTlRun;  // first range of this thread
-    const ProblemInfo pi = pinfo[p];
-    __shared__ double m_vv[kTlTile], m_sr[kTlTile], m_si[kTlTile], m_ia[kTlTile];
-    __shared__ double m_wr[kTlTile], m_wi[kTlTile], m_br[kTlTile], m_bi[kTlTile];
+    const int i0 = blockIdx.x * kTlRanges + threadIdx.x * kTlRun;  // first range of this thread
+    const int M = pinfo[p].M, off = pinfo[p].off;
+    __shared__ double2 m_c[kTlTile], m_w[kTlTile], m_b[kTlTile];
+    __shared__ double m_inc[kTlTile];
     __shared__ double2 m_pw[kTlBits][kTlTile];
-    const double rb = ((double)blockIdx.x * kTlThreads * kTlRun + 1.0) * dr;  // the block's first range
+    const double rb = ((double)blockIdx.x * kTlRanges + 1.0) * dr;  // the chunk's first range
     double sre[kTlRun], sim[kTlRun], sinc[kTlRun];
 #pragma unroll
     for (int j = 0; j < kTlRun; ++j) sre[j] = sim[j] = sinc[j] = 0.0;
-    for (int m0 = 0; m0 < pi.M; m0 += kTlTile) {
+    for (int m0 = 0; m0 < M; m0 += kTlTile) {
         __syncthreads();
-        for (int t = threadIdx.x; t < kTlTile && m0 + t < pi.M; t += blockDim.x) {
-            const int o = pi.off + m0 + t;
+        for (int t = threadIdx.x; t < kTlTile && m0 + t < M; t += kTlThreads) {
+            const int o = off + m0 + t;
             const double a = kr[o], b = lossless ? 0.0 : ki[o];
-            // 1/sqrt(k): principal root of k, then the reciprocal
+            // V_s V_r / sqrt(k): principal root of k, then the reciprocal
             const auto sk = csqrt_principal(a, b);
             const double den = sk.real() * sk.real() + sk.imag() * sk.imag();
-            m_vv[t] = vs[o] * vr[o];
-            m_sr[t] = sk.real() / den;
-            m_si[t] = -sk.imag() / den;
-            m_ia[t] = lossless ? 1.0 / a : 1.0 / hypot(a, b);
+            const double vv = vs[o] * vr[o];
+            m_c[t] = make_double2(vv * sk.real() / den, -vv * sk.imag() / den);
+            m_inc[t] = (vv * vv) * (lossless ? 1.0 / a : 1.0 / hypot(a, b));
             double sn, cs;
             sincos(a * dr, &sn, &cs);
             const double w = exp(-b * dr);
-            m_wr[t] = w * cs;
-            m_wi[t] = w * sn;
+            m_w[t] = make_double2(w * cs, w * sn);
             sincos(a * rb, &sn, &cs);
             const double wb = exp(-b * rb);
-            m_br[t] = wb * cs;
-            m_bi[t] = wb * sn;
+            m_b[t] = make_double2(wb * cs, wb * sn);
+            const double x = (double)kTlRun * dr;
+            sincos(a * x, &sn, &cs);
+            const double wp = exp(-b * x);
+            double qr = wp * cs, qi = wp * sn;
 #pragma unroll
             for (int bit = 0; bit < kTlBits; ++bit) {
-                const double x = (double)(kTlRun << bit) * dr;
-                sincos(a * x, &sn, &cs);
-                const double wp = exp(-b * x);
-                m_pw[bit][t] = make_double2(wp * cs, wp * sn);
+                m_pw[bit][t] = make_double2(qr, qi);
+                const double nq = qr * qr - qi * qi;
+                qi = 2.0 * qr * qi;
+                qr = nq;
             }
         }
         __syncthreads();
-        const int mt = min(kTlTile, pi.M - m0);
+        const int mt = min(kTlTile, M - m0);
         if (i0 < nr) {
             for (int t = 0; t < mt; ++t) {
-                // e^{i k r} at this thread's first range: the block's phase
+                // e^{i k r} at this thread's first range: the chunk's phase
                 // times the powers of the thread index's set bits
-                double er = m_br[t], ei = m_bi[t];
+                const double2 b0 = m_b[t];
+                double er = b0.x, ei = b0.y;
 #pragma unroll
                 for (int bit = 0; bit < kTlBits; ++bit) {
                     if ((threadIdx.x >> bit) & 1) {
@@ -2431,16 +2437,15 @@ __global__ void __launch_bounds__(kTlThreads) k_tl1d(const ProblemInfo* __restri
                         er = nr_;
                     }
                 }
-                const double vv = m_vv[t], sr = m_sr[t], si = m_si[t], ia = m_ia[t];
-                const double wr = m_wr[t], wi = m_wi[t];
+                const double2 c = m_c[t], w = m_w[t];
+                const double inc = m_inc[t];
 #pragma unroll
                 for (int j = 0; j < kTlRun; ++j) {
-                    const double ar = vv * er, ai = vv * ei;
-                    sre[j] += ar * sr - ai * si;
-                    sim[j] += ar * si + ai * sr;
-                    sinc[j] += (vv * vv) * (er * er + ei * ei) * ia;
-                    const double nr_ = er * wr - ei * wi;
-                    ei = er * wi + ei * wr;
+                    sre[j] += er * c.x - ei * c.y;
+                    sim[j] += er * c.y + ei * c.x;
+                    sinc[j] += inc * (er * er + ei * ei);
+                    const double nr_ = er * w.x - ei * w.y;
+                    ei = er * w.y + ei * w.x;
                     er = nr_;
                 }
             }
@@ -2465,8 +2470,7 @@ __global__ void __launch_bounds__(kTlThreads) k_tl1d(const ProblemInfo* __restri
 int launch_tl1d(cudaStream_t st, int P, const ProblemInfo* pinfo, const double* kr, const double* ki,
                 const double* vs, const double* vr, int nr, double dr, int lossless, double* re, double* im,
                 double* incoh) {
-    const int per_block = kTlThreads * kTlRun;
-    dim3 grid((nr + per_block - 1) / per_block, P);
+    dim3 grid((nr + kTlRanges - 1) / kTlRanges, P);
     k_tl1d<<<grid, kTlThreads, 0, st>>>(pinfo, kr, ki, vs, vr, nr, dr, lossless, re, im, incoh);
     return 1;
 }
