@@ -205,7 +205,10 @@ ncpa_status ncpa_tl_1d_range(ncpa_ctx *ctx, const ncpa_modes *modes, int first, 
 ncpa_status ncpa_modes_from_host(ncpa_ctx *ctx, int n_problems, const int *mode_off, const double *re_k,
                                  const double *im_k, const double *v_src, const double *v_rcv, ncpa_modes **out);
 /* one problem on the reference's height sampling (every nz/500-th grid
- * point); heights [m] in z_out (n_heights entries), re/im [n_ranges x n_heights] */
+ * point); heights [m] in z_out (n_heights entries), re/im [n_ranges x n_heights].
+ * The sum runs in FP64 on the CUDA cores, or on the guarded tcgen05 sum
+ * (NCPA_SUM_TC_GUARDED, within 0.05 dB wherever TL > -140 dB) in a context
+ * created with NCPA_TL2D_SUM=3 in the environment. */
 ncpa_status ncpa_tl_2d_heights(const ncpa_modes *modes, int problem, int *n_heights);
 ncpa_status ncpa_tl_2d(ncpa_ctx *ctx, const ncpa_modes *modes, int problem, const ncpa_tl_params *tp,
                        double *z_out, double *re, double *im);

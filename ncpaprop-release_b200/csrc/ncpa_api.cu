@@ -134,6 +134,9 @@ struct ncpa_ctx {
     // bisection ends), the others leave them to the k_eigvec launch that
     // follows; NCPA_FUSE_EV_WORKERS=0 lets every warp of the launch take them
     bool fuse_ev_workers = true;
+    // modal sum of ncpa_tl_2d (the front ends' tloss_2d.nm): NCPA_SUM_FP64,
+    // or NCPA_SUM_TC_GUARDED with NCPA_TL2D_SUM=3
+    int tl2d_method = NCPA_SUM_FP64;
     bool fuse_solve = true;        // fused bisection + eigenvector launch; NCPA_FUSE_SOLVE=0 turns it off
     // how long a consumer of the fused launch waits for an empty queue slot
     // before leaving the item to the following launch; NCPA_FUSE_WAIT_NS
@@ -1424,6 +1427,8 @@ ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
         if (const char* mv = std::getenv("NCPA_MS_TUNE")) ctx->ms_tune = mv[0] != '0';
         if (const char* ov = std::getenv("NCPA_BISECT_ORDER")) ctx->bis_order = ov[0] != '0';
         if (const char* ev = std::getenv("NCPA_FUSE_EV_WORKERS")) ctx->fuse_ev_workers = ev[0] != '0';
+        if (const char* tv2 = std::getenv("NCPA_TL2D_SUM"))
+            ctx->tl2d_method = std::atoi(tv2) == NCPA_SUM_TC_GUARDED ? NCPA_SUM_TC_GUARDED : NCPA_SUM_FP64;
         if (const char* wv = std::getenv("NCPA_BISECT_WORKERS")) {
             const int v = std::atoi(wv);
             if (v >= 1 && v <= 16) ctx->bis_workers = v;
@@ -1984,6 +1989,130 @@ ncpa_status ncpa_tl_2d_heights(const ncpa_modes* m, int problem, int* n_heights)
     return NCPA_OK;
 }
 
+namespace {
+
+// The modal sum at grid rows idx (receiver-major [idx.size() x n_ranges]
+// into ctx->ms_re / ms_im) by `method`; shared by ncpa_tl_multi and the
+// tensor-core form of ncpa_tl_2d.
+void modal_sum_rows(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const std::vector<int>& idx,
+                    const ncpa_tl_params* tp, int method) {
+    cudaStream_t st = ctx->stream;
+    PhaseTimer tm(ctx);
+    tm.mark("start");
+    const ProblemInfo& pi = m->info[problem];
+    const int M = pi.M, nr = tp->n_ranges;
+    const int n_rcv = (int)idx.size();
+    const size_t nout = (size_t)n_rcv * nr;
+    ctx->ms_re.alloc(nout * 8, st);
+    ctx->ms_im.alloc(nout * 8, st);
+    if (M == 0) {
+        CK(cudaMemsetAsync(ctx->ms_re.p, 0, nout * 8, st));
+        CK(cudaMemsetAsync(ctx->ms_im.p, 0, nout * 8, st));
+    } else {
+        // receiver indices through pinned memory: no host synchronisation
+        int* hidx = reinterpret_cast<int*>(pinned(ctx, (size_t)(n_rcv + 1) / 2));
+        std::memcpy(hidx, idx.data(), (size_t)n_rcv * 4);
+        ctx->ms_idx.alloc((size_t)n_rcv * 4, st);
+        CK(cudaMemcpyAsync(ctx->ms_idx.p, hidx, (size_t)n_rcv * 4, cudaMemcpyHostToDevice, st));
+        const double* vfull = m->d_vfull.as<double>() + m->vfull_off[problem];
+        const double* kr = m->d_kr.as<double>() + pi.off;
+        const double* ki = m->d_ki.as<double>() + pi.off;
+        const double* vs = m->d_vs.as<double>() + pi.off;
+        if (method == NCPA_SUM_FP64) {
+            ctx->ms_vz.alloc((size_t)n_rcv * M * 8, st);
+            check_launch(ctx, ncpa::launch_ms_gather(st, n_rcv, M, ctx->ms_idx.as<int>(), vfull,
+                                                     ctx->ms_vz.as<double>()));
+            tm.mark("ms-prep");
+            check_launch(ctx, ncpa::launch_tl2d_rcv_major(st, M, kr, ki, vs, ctx->ms_vz.as<double>(), n_rcv, nr,
+                                                          tp->dr_m, tp->lossless, ctx->ms_re.as<double>(),
+                                                          ctx->ms_im.as<double>()));
+            tm.mark("ms-fp64");
+        } else {
+            const ncpa::MsPlan pl = ncpa::ms_plan(n_rcv, M, nr, ctx->num_sms);
+            ctx->ms_img.alloc(pl.a_img_bytes, st);
+            ctx->ms_q.alloc(pl.q_bytes, st);
+            ctx->ms_tab.alloc(pl.tab_bytes, st);
+            ctx->ms_raw.alloc(pl.raw_bytes, st);
+            const bool guard = method == NCPA_SUM_TC_GUARDED;
+            const int fmt = method == NCPA_SUM_TC_TF32 ? 1 : (guard ? 2 : 0);
+            if (guard) {
+                ctx->ms_spart.alloc(pl.s_part_bytes, st);
+                ctx->ms_b64.alloc(pl.b64_bytes, st);
+                ctx->ms_tp64.alloc(pl.tp64_bytes, st);
+                ctx->ms_a64.alloc(pl.a64_bytes, st);
+                ctx->ms_fix.alloc(pl.fix_list_bytes, st);
+                ctx->ms_fixcnt.alloc(sizeof(int), st);
+                CK(cudaMemsetAsync(ctx->ms_fixcnt.p, 0, sizeof(int), st));
+                ctx->ms_last_points = (long long)n_rcv * nr;
+                ctx->ms_last_eps = ncpa::ms_guard_eps(pl);
+                ctx->ms_last_tau = ncpa::ms_guard_tau(pl);
+            }
+            check_launch(ctx, ncpa::launch_ms_prepare(st, pl, fmt, n_rcv, M, kr, ki, vs, ctx->ms_idx.as<int>(),
+                                                      vfull, tp->dr_m, tp->lossless, ctx->ms_img.p, ctx->ms_q.p,
+                                                      ctx->ms_tab.p, guard ? ctx->ms_b64.p : nullptr,
+                                                      guard ? ctx->ms_tp64.p : nullptr,
+                                                      guard ? ctx->ms_a64.p : nullptr));
+            tm.mark("ms-prep");
+            auto tc = [&](int variant) {
+                check_launch(ctx, ncpa::launch_ms_tc(st, pl, fmt, nr, ctx->ms_img.p, ctx->ms_q.p, ctx->ms_tab.p,
+                                                     ctx->ms_raw.as<float>(),
+                                                     guard ? ctx->ms_spart.as<float>() : nullptr,
+                                                     ctx->d_err.as<unsigned>(), variant));
+            };
+            // schedule: the fastest ring depths for this shape, timed
+            // once per context (each variant computes the same sums)
+            int variant = 0;
+            if (ctx->ms_tune) {
+                const std::array<long long, 4> key{fmt, pl.groups, pl.n_chunks, pl.n_tiles};
+                auto it = ctx->ms_choice.find(key);
+                if (it == ctx->ms_choice.end()) {
+                    const int nv = ncpa::ms_tc_variants();
+                    std::vector<double> best_ms(nv, 0.0);
+                    cudaEvent_t e0, e1;
+                    CK(cudaEventCreate(&e0));
+                    CK(cudaEventCreate(&e1));
+                    int best = 0;
+                    for (int v = 0; v < nv; ++v) {
+                        tc(v);  // warm-up (function attributes, caches)
+                        CK(cudaEventRecord(e0, st));
+                        for (int r = 0; r < 3; ++r) tc(v);
+                        CK(cudaEventRecord(e1, st));
+                        CK(cudaEventSynchronize(e1));
+                        float ms = 0.f;
+                        CK(cudaEventElapsedTime(&ms, e0, e1));
+                        best_ms[v] = ms / 3.0;
+                        if (best_ms[v] < best_ms[best]) best = v;
+                    }
+                    cudaEventDestroy(e0);
+                    cudaEventDestroy(e1);
+                    it = ctx->ms_choice.emplace(key, best).first;
+                    ctx->ms_last_times = best_ms;
+                }
+                variant = it->second;
+            }
+            ctx->ms_last_variant = variant;
+            ctx->ms_last_fmt = fmt;
+            tc(variant);
+            tm.mark("ms-tc");
+            check_launch(ctx, ncpa::launch_ms_finish(st, pl, n_rcv, nr, tp->dr_m, ctx->ms_raw.as<float>(),
+                                                     ctx->ms_re.as<double>(), ctx->ms_im.as<double>(),
+                                                     guard ? ctx->ms_spart.as<float>() : nullptr,
+                                                     guard ? ctx->ms_fixcnt.as<int>() : nullptr,
+                                                     guard ? ctx->ms_fix.p : nullptr));
+            tm.mark("ms-finish");
+            if (guard) {
+                check_launch(ctx, ncpa::launch_ms_fix(st, ctx->num_sms, M, pl.M_pad, nr, tp->dr_m,
+                                                      ctx->ms_fixcnt.as<int>(), ctx->ms_fix.p, ctx->ms_a64.p,
+                                                      ctx->ms_tp64.p, ctx->ms_b64.p, ctx->ms_re.as<double>(),
+                                                      ctx->ms_im.as<double>()));
+                tm.mark("ms-fix");
+            }
+        }
+    }
+}
+
+}  // namespace
+
 ncpa_status ncpa_tl_2d(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const ncpa_tl_params* tp, double* z_out,
                        double* re, double* im) {
     if (!ctx || !m || !tp || !re || !im || problem < 0 || problem >= m->P) return NCPA_EINVAL;
@@ -1997,6 +2126,28 @@ ncpa_status ncpa_tl_2d(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const nc
         if (stepj == 0) stepj = 10;
         const int nzo = (nz + stepj - 1) / stepj;
         if (nzo > 1024) throw ApiError(NCPA_EINVAL, "too many output heights");
+        if (ctx->tl2d_method == NCPA_SUM_TC_GUARDED) {
+            // the guarded tensor-core sum at the sampled rows (receiver-major),
+            // written out range-major as the FP64 kernel does
+            std::vector<int> idx(nzo);
+            for (int j = 0; j < nzo; ++j) {
+                idx[j] = j * stepj;
+                if (z_out) z_out[j] = (j * stepj) * pi.dz;
+            }
+            const int nr = tp->n_ranges;
+            modal_sum_rows(ctx, m, problem, idx, tp, NCPA_SUM_TC_GUARDED);
+            std::vector<double> hre((size_t)nzo * nr), him((size_t)nzo * nr);
+            CK(cudaMemcpyAsync(hre.data(), ctx->ms_re.p, hre.size() * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(him.data(), ctx->ms_im.p, him.size() * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            check_device_status(ctx);
+            for (int j = 0; j < nzo; ++j)
+                for (int i = 0; i < nr; ++i) {
+                    re[(size_t)i * nzo + j] = hre[(size_t)j * nr + i];
+                    im[(size_t)i * nzo + j] = him[(size_t)j * nr + i];
+                }
+            return NCPA_OK;
+        }
         // rows of the sampled heights, the source row, gathered on the host
         std::vector<double> vfull((size_t)Mm * nz), vz((size_t)nzo * Mm), vsrc(Mm);
         if (Mm)
@@ -2024,6 +2175,7 @@ ncpa_status ncpa_tl_2d(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const nc
     });
 }
 
+
 ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n_rcv, const double* rcv_height_m,
                           const ncpa_tl_params* tp, int method, double* re, double* im) {
     if (!ctx || !m || !tp || !rcv_height_m || n_rcv < 1 || problem < 0 || problem >= m->P) return NCPA_EINVAL;
@@ -2037,10 +2189,8 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
         if (method == NCPA_SUM_FP64 && n_rcv > 1024) throw ApiError(NCPA_EINVAL, "FP64 sum: at most 1024 receivers");
         CK(cudaSetDevice(ctx->device));
         cudaStream_t st = ctx->stream;
-        PhaseTimer tm(ctx);
-        tm.mark("start");
         const ProblemInfo& pi = m->info[problem];
-        const int M = pi.M, nr = tp->n_ranges;
+        const int nr = tp->n_ranges;
         // receiver grid points: ceil(z / dz) as ModeSolver.cpp:301 does
         std::vector<int> idx(n_rcv);
         for (int j = 0; j < n_rcv; ++j) {
@@ -2049,112 +2199,7 @@ ncpa_status ncpa_tl_multi(ncpa_ctx* ctx, const ncpa_modes* m, int problem, int n
             idx[j] = k;
         }
         const size_t nout = (size_t)n_rcv * nr;
-        ctx->ms_re.alloc(nout * 8, st);
-        ctx->ms_im.alloc(nout * 8, st);
-        if (M == 0) {
-            CK(cudaMemsetAsync(ctx->ms_re.p, 0, nout * 8, st));
-            CK(cudaMemsetAsync(ctx->ms_im.p, 0, nout * 8, st));
-        } else {
-            // receiver indices through pinned memory: no host synchronisation
-            int* hidx = reinterpret_cast<int*>(pinned(ctx, (size_t)(n_rcv + 1) / 2));
-            std::memcpy(hidx, idx.data(), (size_t)n_rcv * 4);
-            ctx->ms_idx.alloc((size_t)n_rcv * 4, st);
-            CK(cudaMemcpyAsync(ctx->ms_idx.p, hidx, (size_t)n_rcv * 4, cudaMemcpyHostToDevice, st));
-            const double* vfull = m->d_vfull.as<double>() + m->vfull_off[problem];
-            const double* kr = m->d_kr.as<double>() + pi.off;
-            const double* ki = m->d_ki.as<double>() + pi.off;
-            const double* vs = m->d_vs.as<double>() + pi.off;
-            if (method == NCPA_SUM_FP64) {
-                ctx->ms_vz.alloc((size_t)n_rcv * M * 8, st);
-                check_launch(ctx, ncpa::launch_ms_gather(st, n_rcv, M, ctx->ms_idx.as<int>(), vfull,
-                                                         ctx->ms_vz.as<double>()));
-                tm.mark("ms-prep");
-                check_launch(ctx, ncpa::launch_tl2d_rcv_major(st, M, kr, ki, vs, ctx->ms_vz.as<double>(), n_rcv, nr,
-                                                              tp->dr_m, tp->lossless, ctx->ms_re.as<double>(),
-                                                              ctx->ms_im.as<double>()));
-                tm.mark("ms-fp64");
-            } else {
-                const ncpa::MsPlan pl = ncpa::ms_plan(n_rcv, M, nr, ctx->num_sms);
-                ctx->ms_img.alloc(pl.a_img_bytes, st);
-                ctx->ms_q.alloc(pl.q_bytes, st);
-                ctx->ms_tab.alloc(pl.tab_bytes, st);
-                ctx->ms_raw.alloc(pl.raw_bytes, st);
-                const bool guard = method == NCPA_SUM_TC_GUARDED;
-                const int fmt = method == NCPA_SUM_TC_TF32 ? 1 : (guard ? 2 : 0);
-                if (guard) {
-                    ctx->ms_spart.alloc(pl.s_part_bytes, st);
-                    ctx->ms_b64.alloc(pl.b64_bytes, st);
-                    ctx->ms_tp64.alloc(pl.tp64_bytes, st);
-                    ctx->ms_a64.alloc(pl.a64_bytes, st);
-                    ctx->ms_fix.alloc(pl.fix_list_bytes, st);
-                    ctx->ms_fixcnt.alloc(sizeof(int), st);
-                    CK(cudaMemsetAsync(ctx->ms_fixcnt.p, 0, sizeof(int), st));
-                    ctx->ms_last_points = (long long)n_rcv * nr;
-                    ctx->ms_last_eps = ncpa::ms_guard_eps(pl);
-                    ctx->ms_last_tau = ncpa::ms_guard_tau(pl);
-                }
-                check_launch(ctx, ncpa::launch_ms_prepare(st, pl, fmt, n_rcv, M, kr, ki, vs, ctx->ms_idx.as<int>(),
-                                                          vfull, tp->dr_m, tp->lossless, ctx->ms_img.p, ctx->ms_q.p,
-                                                          ctx->ms_tab.p, guard ? ctx->ms_b64.p : nullptr,
-                                                          guard ? ctx->ms_tp64.p : nullptr,
-                                                          guard ? ctx->ms_a64.p : nullptr));
-                tm.mark("ms-prep");
-                auto tc = [&](int variant) {
-                    check_launch(ctx, ncpa::launch_ms_tc(st, pl, fmt, nr, ctx->ms_img.p, ctx->ms_q.p, ctx->ms_tab.p,
-                                                         ctx->ms_raw.as<float>(),
-                                                         guard ? ctx->ms_spart.as<float>() : nullptr,
-                                                         ctx->d_err.as<unsigned>(), variant));
-                };
-                // schedule: the fastest ring depths for this shape, timed
-                // once per context (each variant computes the same sums)
-                int variant = 0;
-                if (ctx->ms_tune) {
-                    const std::array<long long, 4> key{fmt, pl.groups, pl.n_chunks, pl.n_tiles};
-                    auto it = ctx->ms_choice.find(key);
-                    if (it == ctx->ms_choice.end()) {
-                        const int nv = ncpa::ms_tc_variants();
-                        std::vector<double> best_ms(nv, 0.0);
-                        cudaEvent_t e0, e1;
-                        CK(cudaEventCreate(&e0));
-                        CK(cudaEventCreate(&e1));
-                        int best = 0;
-                        for (int v = 0; v < nv; ++v) {
-                            tc(v);  // warm-up (function attributes, caches)
-                            CK(cudaEventRecord(e0, st));
-                            for (int r = 0; r < 3; ++r) tc(v);
-                            CK(cudaEventRecord(e1, st));
-                            CK(cudaEventSynchronize(e1));
-                            float ms = 0.f;
-                            CK(cudaEventElapsedTime(&ms, e0, e1));
-                            best_ms[v] = ms / 3.0;
-                            if (best_ms[v] < best_ms[best]) best = v;
-                        }
-                        cudaEventDestroy(e0);
-                        cudaEventDestroy(e1);
-                        it = ctx->ms_choice.emplace(key, best).first;
-                        ctx->ms_last_times = best_ms;
-                    }
-                    variant = it->second;
-                }
-                ctx->ms_last_variant = variant;
-                ctx->ms_last_fmt = fmt;
-                tc(variant);
-                tm.mark("ms-tc");
-                check_launch(ctx, ncpa::launch_ms_finish(st, pl, n_rcv, nr, tp->dr_m, ctx->ms_raw.as<float>(),
-                                                         ctx->ms_re.as<double>(), ctx->ms_im.as<double>(),
-                                                         guard ? ctx->ms_spart.as<float>() : nullptr,
-                                                         guard ? ctx->ms_fixcnt.as<int>() : nullptr,
-                                                         guard ? ctx->ms_fix.p : nullptr));
-                tm.mark("ms-finish");
-                if (guard) {
-                    check_launch(ctx, ncpa::launch_ms_fix(st, ctx->num_sms, M, pl.M_pad, nr, tp->dr_m,
-                                                          ctx->ms_fixcnt.as<int>(), ctx->ms_fix.p, ctx->ms_a64.p,
-                                                          ctx->ms_tp64.p, ctx->ms_b64.p, ctx->ms_re.as<double>(),
-                                                          ctx->ms_im.as<double>()));
-                    tm.mark("ms-fix");
-                }
-            }
-        }
+        modal_sum_rows(ctx, m, problem, idx, tp, method);
         if (re) {
             CK(cudaMemcpyAsync(re, ctx->ms_re.p, nout * 8, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(im, ctx->ms_im.p, nout * 8, cudaMemcpyDeviceToHost, st));
