@@ -2684,6 +2684,8 @@ int launch_src_pulse2(cudaStream_t st, int n, double dt, double scale, double* x
 // p(t_k) = 2 Re( df sum_n e^{-2 pi i f_n t0} S_n H_n e^{-2 pi i k n / nfft} )
 constexpr int kPulseMaxFreq = 4096;
 
+constexpr int kPulseBins = 64;  // time bins per CTA of k_bb_pulse (8 warps x 8)
+
 __global__ void __launch_bounds__(256) k_bb_pulse(int nfreq, const double* __restrict__ f,
                                                   const double* __restrict__ s_src, const double* __restrict__ h,
                                                   int nr, const double* __restrict__ t0s, int nfft,
@@ -2702,43 +2704,53 @@ __global__ void __launch_bounds__(256) k_bb_pulse(int nfreq, const double* __res
     }
     __syncthreads();
     const double df = f[2] - f[1];  // f_step of ModalBroadbandPropagator.cpp:65
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nfft; k += gridDim.x * blockDim.x) {
+    // one warp per time bin k: lanes split the frequencies, then a shuffle sum
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int kend = min(nfft, (blockIdx.x + 1) * kPulseBins);
+    for (int k = blockIdx.x * kPulseBins + wid; k < kend; k += blockDim.x >> 5) {
         double accr = 0.0;
-        int idx = 0;
-        for (int n = 0; n < nfreq; ++n) {
+        for (int n = lane; n < nfreq; n += 32) {
+            const int idx = (int)(((long long)n * k) % nfft);
             accr += arg[2 * n] * tw[2 * idx] - arg[2 * n + 1] * tw[2 * idx + 1];
-            idx += k;
-            if (idx >= nfft) idx -= nfft;
         }
-        out[(size_t)ir * nfft + k] = 2.0 * (df * accr);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) accr += __shfl_xor_sync(0xffffffffu, accr, o);
+        if (lane == 0) out[(size_t)ir * nfft + k] = 2.0 * (df * accr);
     }
 }
 
 int launch_bb_pulse(cudaStream_t st, int nfreq, const double* f, const double* s_src, const double* h, int nr,
                     const double* t0, int nfft, const double* tw, double* out) {
-    dim3 grid((nfft + 255) / 256, nr);
+    dim3 grid((nfft + kPulseBins - 1) / kPulseBins, nr);
     size_t sm = (size_t)2 * nfreq * sizeof(double);
     if (sm > 48 * 1024) cudaFuncSetAttribute(k_bb_pulse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_bb_pulse<<<grid, 256, sm, st>>>(nfreq, f, s_src, h, nr, t0, nfft, tw, out);
     return 1;
 }
 
-// source spectrum of a sampled waveform: dt sum_n x_n e^{+2 pi i k n/nfft}
-__global__ void k_src_dft(int n, const double* __restrict__ x, double dt, int nfft, int nfreq,
-                          const double* __restrict__ tw, double* __restrict__ s) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nfreq) return;
+// source spectrum of a sampled waveform: dt sum_n x_n e^{+2 pi i k n/nfft};
+// one warp per frequency bin k, lanes split the samples, then a shuffle sum
+__global__ void __launch_bounds__(256) k_src_dft(int n, const double* __restrict__ x, double dt, int nfft,
+                                                 int nfreq, const double* __restrict__ tw, double* __restrict__ s) {
+    const int lane = threadIdx.x & 31;
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (k >= nfreq) return;  // warp-uniform
     double ar = 0.0, ai = 0.0;
-    long long idx = 0;
     const int nn = min(n, nfft);
-    for (int j = 0; j < nn; ++j) {
+    for (int j = lane; j < nn; j += 32) {
+        const int idx = (int)(((long long)j * k) % nfft);
         ar += x[j] * tw[2 * idx];
         ai -= x[j] * tw[2 * idx + 1];  // conjugate twiddle: e^{+i}
-        idx += k;
-        if (idx >= nfft) idx -= nfft;
     }
-    s[2 * k] = ar * dt;
-    s[2 * k + 1] = ai * dt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ar += __shfl_xor_sync(0xffffffffu, ar, o);
+        ai += __shfl_xor_sync(0xffffffffu, ai, o);
+    }
+    if (lane == 0) {
+        s[2 * k] = ar * dt;
+        s[2 * k + 1] = ai * dt;
+    }
 }
 
 // values of a Steffen spline at m points (clamped outside the knots)
@@ -2790,7 +2802,7 @@ int launch_fill_unit(cudaStream_t st, int n, double* h) {
 
 int launch_src_dft(cudaStream_t st, int n, const double* x, double dt, int nfft, int nfreq, const double* tw,
                    double* s) {
-    k_src_dft<<<(nfreq + 127) / 128, 128, 0, st>>>(n, x, dt, nfft, nfreq, tw, s);
+    k_src_dft<<<(nfreq * 32 + 255) / 256, 256, 0, st>>>(n, x, dt, nfft, nfreq, tw, s);
     return 1;
 }
 
