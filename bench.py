@@ -428,6 +428,48 @@ def run_ours(args):
 MS_NZ, MS_FREQ, MS_TOP_KM, MS_NR, MS_DR, MS_RCV = 100000, 2.0, 180.0, 20000, 100.0, 64
 
 
+def _tl2d_at_scale(m, path, n_ranges=2000, dr=1000.0, reps=3):
+    """The 2-D TL of ncpa_tl_2d (the reference's tloss_2d.nm: every
+    Nz/500-th height) on the same 2 Hz, Nz = 100000 modes: the FP64
+    CUDA-core sum of m's context against the guarded tensor-core sum of a
+    context created with NCPA_TL2D_SUM=3 (its own solve, untimed).  Times are
+    whole calls (results copied to host memory)."""
+    import ncpa_gpu
+
+    def timed(mm):
+        mm.tl2d(0, n_ranges, dr)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            out = mm.tl2d(0, n_ranges, dr)
+        return (time.perf_counter() - t0) * 1e3 / reps, out
+
+    ms64, (z, re64, im64) = timed(m)
+    old = os.environ.get("NCPA_TL2D_SUM")
+    os.environ["NCPA_TL2D_SUM"] = "3"
+    try:
+        ctx2 = ncpa_gpu.Context(0)
+    finally:
+        if old is None:
+            os.environ.pop("NCPA_TL2D_SUM", None)
+        else:
+            os.environ["NCPA_TL2D_SUM"] = old
+    prof2 = ctx2.load_profile(path)
+    m2 = ctx2.solve(prof2, ncpa_gpu.default_params(nz_grid=MS_NZ, maxheight_km=MS_TOP_KM, want_vectors=1,
+                                                   turnoff_wkb=1), [MS_FREQ], [90.0])
+    mstc, (_, retc, imtc) = timed(m2)
+    m2.close()
+    prof2.close()
+    ctx2.close()
+    tl64 = 20 * np.log10(np.maximum(np.hypot(re64, im64), 1e-300))
+    tltc = 20 * np.log10(np.maximum(np.hypot(retc, imtc), 1e-300))
+    sel = tl64 > -140.0
+    return {"workload": "ncpa_tl_2d (tloss_2d.nm): %d heights x %d ranges x %d km, same modes" %
+                        (len(z), n_ranges, int(dr / 1000)),
+            "ms_per_call_fp64": round(ms64, 3), "ms_per_call_tc_guarded": round(mstc, 3),
+            "tl_db_max": float(np.abs(tltc - tl64)[sel].max()),
+            "where": "every point with TL > -140 dB (%d of %d)" % (int(sel.sum()), sel.size)}
+
+
 def modal_sum_leg(ctx, stream, bf16, k=10):
     """Solve the 2 Hz, 180 km, Nz = 100000 problem once (untimed), then time
     the modal sum at 64 receivers (0-10 km) x 20000 ranges (0.1 km to 2000 km)
@@ -484,6 +526,7 @@ def modal_sum_leg(ctx, stream, bf16, k=10):
     fixed, points = ctx.sum_fixups()
     p_tc = m.tl_multi(0, h, MS_NR, MS_DR, method=X3)
     p_32 = m.tl_multi(0, h, MS_NR, MS_DR, method=T32)
+    tl2d = _tl2d_at_scale(m, path)
     m.close()
     prof.close()
     alg = 8.0 * MS_RCV * M * MS_NR          # complex multiply-adds x 8 flops
@@ -519,6 +562,7 @@ def modal_sum_leg(ctx, stream, bf16, k=10):
                      "flops_per_launch": tensor_g, "algorithmic_flops_per_launch": alg, "traffic": None,
                      "traffic_source": "not measured by this run (DRAM counters need ncu)"},
         "error_vs_fp64": err(p_g),
+        "tl2d": tl2d,
         "bf16x3": {"ms_per_call": round(ms_call, 4), "ms_kernel": round(ms_kernel, 4), "phases_ms": phases,
                    "achieved_tflops": round(achieved3, 1), "frac": round(achieved3 / bf16_peak, 4),
                    "note": "unguarded: stated error only", "error_vs_fp64": err(p_tc)},

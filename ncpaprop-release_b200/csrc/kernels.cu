@@ -2753,6 +2753,31 @@ __global__ void __launch_bounds__(256) k_src_dft(int n, const double* __restrict
     }
 }
 
+// out[c][r] = in[r][c] for a rows x cols matrix of doubles, 32 x 32 tiles
+// staged in shared memory (both sides coalesced)
+__global__ void __launch_bounds__(256) k_transpose(int rows, int cols, const double* __restrict__ in,
+                                                   double* __restrict__ out) {
+    __shared__ double t[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+    for (int k = ty; k < 32; k += 8) {
+        const int r = r0 + k, c = c0 + tx;
+        if (r < rows && c < cols) t[k][tx] = in[(size_t)r * cols + c];
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int c = c0 + k, r = r0 + tx;
+        if (r < rows && c < cols) out[(size_t)c * rows + r] = t[tx][k];
+    }
+}
+
+int launch_transpose(cudaStream_t st, int rows, int cols, const double* in, double* out) {
+    if (rows < 1 || cols < 1) return 0;
+    dim3 grid((cols + 31) / 32, (rows + 31) / 32);
+    k_transpose<<<grid, 256, 0, st>>>(rows, cols, in, out);
+    return 1;
+}
+
 // values of a Steffen spline at m points (clamped outside the knots)
 __global__ void k_spline_eval(int n, const double* __restrict__ x, const double* __restrict__ y,
                               const double* __restrict__ coef, int m, const double* __restrict__ xq,

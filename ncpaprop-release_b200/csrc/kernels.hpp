@@ -191,6 +191,8 @@ int launch_tl2d(cudaStream_t st, int M, const double* kr, const double* ki, cons
 // same sum with [n_rcv x nr] output (receiver-major)
 int launch_tl2d_rcv_major(cudaStream_t st, int M, const double* kr, const double* ki, const double* vs_src,
                           const double* vz, int n_rcv, int nr, double dr, int lossless, double* re, double* im);
+// out[c][r] = in[r][c] (rows x cols doubles)
+int launch_transpose(cudaStream_t st, int rows, int cols, const double* in, double* out);
 // broadband synthesis
 int launch_twiddle(cudaStream_t st, int nfft, double* tw);
 // fac: scratch of 4 doubles per mode

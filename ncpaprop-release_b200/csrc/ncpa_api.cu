@@ -2136,38 +2136,37 @@ ncpa_status ncpa_tl_2d(ncpa_ctx* ctx, const ncpa_modes* m, int problem, const nc
             }
             const int nr = tp->n_ranges;
             modal_sum_rows(ctx, m, problem, idx, tp, NCPA_SUM_TC_GUARDED);
-            std::vector<double> hre((size_t)nzo * nr), him((size_t)nzo * nr);
-            CK(cudaMemcpyAsync(hre.data(), ctx->ms_re.p, hre.size() * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(him.data(), ctx->ms_im.p, him.size() * 8, cudaMemcpyDeviceToHost, st));
+            const size_t n = (size_t)nzo * nr;
+            DevBuf tre, tim;
+            tre.alloc(n * 8, st);
+            tim.alloc(n * 8, st);
+            check_launch(ctx, ncpa::launch_transpose(st, nzo, nr, ctx->ms_re.as<double>(), tre.as<double>()));
+            check_launch(ctx, ncpa::launch_transpose(st, nzo, nr, ctx->ms_im.as<double>(), tim.as<double>()));
+            CK(cudaMemcpyAsync(re, tre.p, n * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(im, tim.p, n * 8, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             check_device_status(ctx);
-            for (int j = 0; j < nzo; ++j)
-                for (int i = 0; i < nr; ++i) {
-                    re[(size_t)i * nzo + j] = hre[(size_t)j * nr + i];
-                    im[(size_t)i * nzo + j] = him[(size_t)j * nr + i];
-                }
             return NCPA_OK;
         }
-        // rows of the sampled heights, the source row, gathered on the host
-        std::vector<double> vfull((size_t)Mm * nz), vz((size_t)nzo * Mm), vsrc(Mm);
-        if (Mm)
-            CK(cudaMemcpyAsync(vfull.data(), m->d_vfull.as<double>() + m->vfull_off[problem], vfull.size() * 8,
-                               cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
+        // rows of the sampled heights and the source row (last), gathered on
+        // the device: the full vectors never leave HBM
+        std::vector<int> rows(nzo + 1);
         for (int j = 0; j < nzo; ++j) {
-            std::memcpy(&vz[(size_t)j * Mm], &vfull[(size_t)j * stepj * Mm], Mm * 8);
+            rows[j] = j * stepj;
             if (z_out) z_out[j] = (j * stepj) * pi.dz;
         }
-        if (Mm) std::memcpy(vsrc.data(), &vfull[(size_t)pi.isrc * Mm], Mm * 8);
-        DevBuf dvz, dvs, dre, dim;
-        upload(dvz, vz, st);
-        upload(dvs, vsrc, st);
+        rows[nzo] = pi.isrc;
+        DevBuf drows, dvz, dre, dim;
+        upload(drows, rows, st);
+        dvz.alloc((size_t)(nzo + 1) * std::max(Mm, 1) * 8, st);
+        check_launch(ctx, ncpa::launch_ms_gather(st, nzo + 1, Mm, drows.as<int>(),
+                                                 m->d_vfull.as<double>() + m->vfull_off[problem], dvz.as<double>()));
         const size_t n = (size_t)tp->n_ranges * nzo;
         dre.alloc(n * 8, st);
         dim.alloc(n * 8, st);
         check_launch(ctx, ncpa::launch_tl2d(st, Mm, m->d_kr.as<double>() + pi.off, m->d_ki.as<double>() + pi.off,
-                                            dvs.as<double>(), dvz.as<double>(), nzo, tp->n_ranges, tp->dr_m,
-                                            tp->lossless, dre.as<double>(), dim.as<double>()));
+                                            dvz.as<double>() + (size_t)nzo * Mm, dvz.as<double>(), nzo, tp->n_ranges,
+                                            tp->dr_m, tp->lossless, dre.as<double>(), dim.as<double>()));
         CK(cudaMemcpyAsync(re, dre.p, n * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(im, dim.p, n * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
