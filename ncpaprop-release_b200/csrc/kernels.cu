@@ -481,6 +481,8 @@ __global__ void __launch_bounds__(kWkbThreads) k_window(ProblemInfo* __restrict_
         pinfo[p].hi = (k_max * k_max) * h2;
         pinfo[p].used_wkb = used_wkb;
         pinfo[p].n_scan = kScanDefault;
+        pinfo[p].n_scan_raw = kScanDefault;
+        pinfo[p].m_est = -1.f;
     }
 }
 
@@ -531,6 +533,8 @@ __global__ void __launch_bounds__(kSizeThreads) k_scan_size(ProblemInfo* __restr
         const float m_est = fmaxf(t * (float)(1.0 / kPi), 0.f);
         const int n = ((int)(2.f * m_est) + 32 + kScanStep - 1) / kScanStep * kScanStep;
         pinfo[p].n_scan = min(max(n, kScanStep), kScanMax);
+        pinfo[p].n_scan_raw = pinfo[p].n_scan;
+        pinfo[p].m_est = m_est;
     }
 }
 
@@ -962,67 +966,186 @@ __device__ void warp_sweep_tw(const double* __restrict__ s, int nz, double p_ini
 }
 
 // K3a-2: the isolation scan in units of kScanStep shifts, numbered over the
-// problems in order (problem p has n_scan / kScanStep units).  Warp w of the
-// grid sweeps unit w (warp_sweep: the sequential count, two shifts per lane)
-// through its own ring; it finds its problem with a warp-wide prefix sum of
-// the units per problem, 32 problems at a time.  Every unit is the same work
-// and the units go to consecutive warps, so the SMs share the scan evenly
-// whatever the problems' sizes; warps past the last unit return.
-__global__ void __launch_bounds__(kWarpsPerCta * 32) k_scan(int P, const ProblemInfo* __restrict__ pinfo,
-                                                           const double* __restrict__ s, int* __restrict__ counts,
-                                                           unsigned* err) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const long long w = (long long)blockIdx.x * kWarpsPerCta + wid;
+// problems in order (problem p has n_scan_raw / kScanStep units, less the
+// trim below).  Warp w of the grid sweeps unit w (warp_sweep: the sequential
+// count, two shifts per lane) through its own ring; it finds its problem with
+// a warp-wide prefix sum of the units per problem, 32 problems at a time.
+// Every unit is the same work.  Trim: with slots > 0 (the device's warp
+// schedulers) and U units in all, the batch drops U mod slots units when that
+// is at most a quarter of U, so each scheduler sweeps the same whole number of
+// units: one unit each from the first problems (in order) that keep at least
+// 1.75 shifts per estimated mode.  Every warp computes the same trim from the
+// raw sizes; the warp that sweeps a problem's first unit records the final
+// size in n_scan for the kernels that follow.  Warps past the last unit
+// return.
+__device__ __forceinline__ bool scan_trimmable(const ProblemInfo& q) {
+    const int u = q.n_scan_raw / kScanStep;
+    return u >= 2 && q.m_est >= 0.f && (float)((u - 1) * kScanStep) >= 1.75f * q.m_est;
+}
+
+// Item scheduler of the bisection (and of the isolation scan's units, all of
+// equal cost).  The bisection's item list is cost-ordered, heaviest first
+// (k_make_items with order 1).  On each warp scheduler (SM and sub-partition)
+// the first warp to arrive takes items from the heavy end of the list and the
+// next workers - 1 from the light end, so a scheduler runs a heavy and a
+// light item side by side; later warps run no bisection (in the fused launch
+// they go straight to the eigenvector queue).  A worker first draws a ticket
+// (n tickets for n items) and then an index from its end of the list: front
+// and back indices never meet, so every item runs exactly once.  Where the
+// CTAs land only decides the balance: the first warp on every scheduler is a
+// worker.  sched: kSchedInts ints zeroed before the launch; null keeps plain
+// round-robin (item q to warp q mod (grid x kWarpsPerCta)).
+struct ItemSched {
+    int* S;
+    int role;     // 0: none, 1: heavy end, 2: light end
+    bool worker;  // the warp runs bisection items (every warp without sched)
+    __device__ ItemSched(int* sched, int workers) : S(sched), role(0), worker(true) {
+        if (!S) return;
+        const int lane = threadIdx.x & 31;
+        if (lane == 0) {
+            // the warp's SM and its sub-partition (hardware warp slot mod 4; a
+            // CTA's warp index does not determine it)
+            unsigned smid, slot;
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+            asm volatile("mov.u32 %0, %%warpid;" : "=r"(slot));
+            const int key = smid < (unsigned)kSchedSms ? (int)(smid * 4 + (slot & 3u)) : -1;
+            const int k = key >= 0 ? atomicAdd(S + 3 + key, 1) : 0;
+            role = k == 0 ? 1 : (k < workers ? 2 : 0);
+        }
+        role = __shfl_sync(0xffffffffu, role, 0);
+        worker = role != 0;
+    }
+    // next item of this warp (-1: none left); walk = plain round-robin position
+    __device__ long long next(int n, long long& walk, long long stride) {
+        if (!S) {
+            const long long it = walk;
+            walk += stride;
+            return it < n ? it : -1;
+        }
+        if (!role) return -1;
+        int it = -1;
+        if ((threadIdx.x & 31) == 0) {
+            if (atomicAdd(S, 1) < n) it = role == 1 ? atomicAdd(S + 1, 1) : n - 1 - atomicAdd(S + 2, 1);
+        }
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it < 0) role = 0;
+        return it;
+    }
+};
+
+// unit u of the (trimmed) scan: its problem p, first shift tb and the
+// problem's scan size n; p = -1 past the last unit.  Every warp lane takes
+// part (warp-wide prefix sums over the problems, 32 at a time).
+__device__ void scan_unit(int P, const ProblemInfo* pinfo, int remove, long long u, int& p, int& tb, int& n) {
+    const int lane = threadIdx.x & 31;
     long long before = 0;  // units of the problems before the current block of 32
-    int p = -1, tb = 0;
+    int trimmed = 0;       // trimmable problems before the current block of 32
+    p = -1;
+    tb = n = 0;
     for (int base = 0; base < P && p < 0; base += 32) {
         const int q = base + lane;
-        const int units = q < P ? pinfo[q].n_scan / kScanStep : 0;
+        int units = 0, tr = 0;
+        if (q < P) {
+            const ProblemInfo& pq = pinfo[q];
+            units = pq.n_scan_raw / kScanStep;
+            tr = remove > 0 && scan_trimmable(pq) ? 1 : 0;
+        }
+        int tincl = tr;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, tincl, off);
+            if (lane >= off) tincl += v;
+        }
+        if (tr && trimmed + tincl - 1 < remove) --units;
+        trimmed += __shfl_sync(0xffffffffu, tincl, 31);
         int incl = units;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
             const int v = __shfl_up_sync(0xffffffffu, incl, off);
             if (lane >= off) incl += v;
         }
-        const bool mine = w >= before + incl - units && w < before + incl;
+        const bool mine = u >= before + incl - units && u < before + incl;
         const unsigned hit = __ballot_sync(0xffffffffu, mine);
         if (hit) {
             const int src = __ffs(hit) - 1;
             const int excl = __shfl_sync(0xffffffffu, incl - units, src);
             p = base + src;
-            tb = (int)(w - before - excl) * kScanStep;
+            tb = (int)(u - before - excl) * kScanStep;
+            n = __shfl_sync(0xffffffffu, units, src) * kScanStep;
         }
         before += __shfl_sync(0xffffffffu, incl, 31);
     }
-    if (p < 0) return;  // past the last unit: the whole warp
-    const ProblemInfo pi = pinfo[p];
-    const int n = pi.n_scan;
+}
+
+// With sched (kSchedInts ints, zeroed), the units are claimed through the
+// bisection's item scheduler: on each warp scheduler the first
+// ceil(units / slots) warps to arrive take units until none are left, so
+// every scheduler sweeps the same number of units wherever the CTAs land
+// (launch slots CTAs: the whole grid resident).  Without it, warp w of the
+// grid sweeps unit w.
+__global__ void __launch_bounds__(kWarpsPerCta * 32) k_scan(int P, ProblemInfo* pinfo, const double* __restrict__ s,
+                                                           int* __restrict__ counts, unsigned* err, int slots,
+                                                           int* sched) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int remove = 0;  // units the trim takes off (one per trimmable problem)
+    int U = 0, E = 0;
+    for (int q = lane; q < P; q += 32) {
+        U += pinfo[q].n_scan_raw / kScanStep;
+        E += scan_trimmable(pinfo[q]) ? 1 : 0;
+    }
+    U = __reduce_add_sync(0xffffffffu, U);
+    E = __reduce_add_sync(0xffffffffu, E);
+    if (slots > 0) {
+        const int rem = U % slots;
+        if (U >= slots && 4 * rem <= U) remove = rem;
+    }
+    const int total = U - min(remove, E);  // the units after the trim
     WarpRing r;
     r.buf = reinterpret_cast<double*>(smem_raw) + (size_t)wid * kWBuf * kWChunk;
     r.bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarpsPerCta * kWBuf * kWChunk * 8) + wid * kWBuf;
     r.loads = 0;
-    if (lane == 0) {
-        for (int k = 0; k < kWBuf; ++k) mbar_init(&r.bars[k], 1);
-        fence_mbar_init();
+    bool ring_ready = false;
+    ItemSched sc(slots > 0 ? sched : nullptr, slots > 0 ? max(1, (total + slots - 1) / slots) : 1);
+    long long walk = (long long)blockIdx.x * kWarpsPerCta + wid;
+    for (long long u; (u = sc.next(total, walk, (long long)gridDim.x * kWarpsPerCta)) >= 0;) {
+        int p, tb, n;
+        scan_unit(P, pinfo, remove, u, p, tb, n);
+        if (p < 0) continue;  // past the last unit (warp-uniform)
+        if (tb == 0 && lane == 0) pinfo[p].n_scan = n;
+        if (!ring_ready) {
+            if (lane == 0) {
+                for (int k = 0; k < kWBuf; ++k) mbar_init(&r.bars[k], 1);
+                fence_mbar_init();
+            }
+            __syncwarp();
+            ring_ready = true;
+        }
+        const double lo = pinfo[p].lo, hi = pinfo[p].hi;
+        const long long s_off = pinfo[p].s_off;
+        const int nz = pinfo[p].nz;
+        const int t0 = tb + 2 * lane, t1 = t0 + 1;
+        int c0, c1;
+        double rat, hq;
+        warp_sweep<EssRows>(s + s_off, nz, 0.0, scan_x(lo, hi, t0, n), scan_x(lo, hi, t1, n), 0, r, err, c0, c1,
+                            rat, hq);
+        counts[(size_t)p * kScanMax + t0] = c0;
+        counts[(size_t)p * kScanMax + t1] = c1;
+        __syncwarp();
+        if (lane == 0) fence_proxy_async();  // the ring's buffers are refilled by the next unit's copies
+        __syncwarp();
     }
-    __syncwarp();
-    const int t0 = tb + 2 * lane, t1 = t0 + 1;
-    int c0, c1;
-    double rat, hq;
-    warp_sweep<EssRows>(s + pi.s_off, pi.nz, 0.0, scan_x(pi.lo, pi.hi, t0, n), scan_x(pi.lo, pi.hi, t1, n), 0, r,
-                        err, c0, c1, rat, hq);
-    counts[(size_t)p * kScanMax + t0] = c0;
-    counts[(size_t)p * kScanMax + t1] = c1;
 }
 
-int launch_scan(cudaStream_t st, int P, ProblemInfo* pinfo, const double* s, int* counts, unsigned* err) {
+int launch_scan(cudaStream_t st, int P, ProblemInfo* pinfo, const double* s, int* counts, unsigned* err,
+                int slots, int* sched) {
     k_scan_size<<<P, kSizeThreads, 0, st>>>(pinfo, s);
     const size_t sm = (size_t)kWarpsPerCta * (kWBuf * kWChunk * 8 + kWBuf * 8);
     const long long units = (long long)P * (kScanMax / kScanStep);
     cudaFuncSetAttribute(k_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_scan<<<(unsigned)((units + kWarpsPerCta - 1) / kWarpsPerCta), kWarpsPerCta * 32, sm, st>>>(P, pinfo, s,
-                                                                                                  counts, err);
+    // claimed units: one CTA per slot (4 per SM, the whole grid resident)
+    const long long grid = (sched && slots > 0) ? slots : (units + kWarpsPerCta - 1) / kWarpsPerCta;
+    k_scan<<<(unsigned)grid, kWarpsPerCta * 32, sm, st>>>(P, pinfo, s, counts, err, slots, sched);
     return 2;
 }
 
@@ -1181,55 +1304,6 @@ __device__ __forceinline__ void bisect_item(const ProblemInfo* __restrict__ pinf
     }
     if (lane < w.m) mu[pi.off + w.j0 + lane] = x;
 }
-
-// Bisection item scheduler.  The item list is cost-ordered, heaviest first
-// (k_make_items with order 1).  On each warp scheduler (SM and sub-partition)
-// the first warp to arrive takes items from the heavy end of the list and the
-// next workers - 1 from the light end, so a scheduler runs a heavy and a
-// light item side by side; later warps run no bisection (in the fused launch
-// they go straight to the eigenvector queue).  A worker first draws a ticket
-// (n tickets for n items) and then an index from its end of the list: front
-// and back indices never meet, so every item runs exactly once.  Where the
-// CTAs land only decides the balance: the first warp on every scheduler is a
-// worker.  sched: kSchedInts ints zeroed before the launch; null keeps plain
-// round-robin (item q to warp q mod (grid x kWarpsPerCta)).
-struct ItemSched {
-    int* S;
-    int role;     // 0: none, 1: heavy end, 2: light end
-    bool worker;  // the warp runs bisection items (every warp without sched)
-    __device__ ItemSched(int* sched, int workers) : S(sched), role(0), worker(true) {
-        if (!S) return;
-        const int lane = threadIdx.x & 31;
-        if (lane == 0) {
-            // the warp's SM and its sub-partition (hardware warp slot mod 4; a
-            // CTA's warp index does not determine it)
-            unsigned smid, slot;
-            asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
-            asm volatile("mov.u32 %0, %%warpid;" : "=r"(slot));
-            const int key = smid < (unsigned)kSchedSms ? (int)(smid * 4 + (slot & 3u)) : -1;
-            const int k = key >= 0 ? atomicAdd(S + 3 + key, 1) : 0;
-            role = k == 0 ? 1 : (k < workers ? 2 : 0);
-        }
-        role = __shfl_sync(0xffffffffu, role, 0);
-        worker = role != 0;
-    }
-    // next item of this warp (-1: none left); walk = plain round-robin position
-    __device__ long long next(int n, long long& walk, long long stride) {
-        if (!S) {
-            const long long it = walk;
-            walk += stride;
-            return it < n ? it : -1;
-        }
-        if (!role) return -1;
-        int it = -1;
-        if ((threadIdx.x & 31) == 0) {
-            if (atomicAdd(S, 1) < n) it = role == 1 ? atomicAdd(S + 1, 1) : n - 1 - atomicAdd(S + 2, 1);
-        }
-        it = __shfl_sync(0xffffffffu, it, 0);
-        if (it < 0) role = 0;
-        return it;
-    }
-};
 
 // Row: the row format (EssRows: shifts in h^2 k^2; WmodRows: kappa = h k);
 // tol is scaled per problem by Row::tol_scale.

@@ -33,6 +33,8 @@ struct ProblemInfo {
     int M, off;            // number of modes and offset into the mode arrays
     int used_wkb;
     int n_scan;            // shifts of the isolation scan (<= kScanMax)
+    int n_scan_raw;        // the size estimated from the problem alone (before the batch-wide trim)
+    float m_est;           // estimated mode count in [lo, hi] (-1: not estimated)
     double g0;             // wide-angle rows: ground term of row 0, 1 / (dz admittance + 1)
 };
 
@@ -96,7 +98,11 @@ int launch_window(cudaStream_t st, int P, ProblemInfo* pinfo, const double* kz2,
 // isolation scan (K3a): sizes each problem's scan (ProblemInfo::n_scan) from
 // an estimate of its mode count, then pinfo[p].n_scan Sturm counts per
 // problem at counts[p * kScanMax + t]
-int launch_scan(cudaStream_t st, int P, ProblemInfo* pinfo, const double* s, int* counts, unsigned* err);
+// slots > 0 (warp schedulers of the device: 4 x SMs) trims the batch's scan
+// to a whole number of units per scheduler; sched (kSchedInts ints, zeroed)
+// then has the units claimed per scheduler (see k_scan)
+int launch_scan(cudaStream_t st, int P, ProblemInfo* pinfo, const double* s, int* counts, unsigned* err,
+                int slots = 0, int* sched = nullptr);
 // multisection/bisection over work items (K3); step_counter (optional)
 // accumulates the Sturm recurrence steps swept; sched (kSchedInts ints,
 // zeroed) runs a cost-ordered item list (order = 1 in launch_make_items) with

@@ -137,6 +137,9 @@ struct ncpa_ctx {
     // modal sum of ncpa_tl_2d (the front ends' tloss_2d.nm): NCPA_SUM_FP64,
     // or NCPA_SUM_TC_GUARDED with NCPA_TL2D_SUM=3
     int tl2d_method = NCPA_SUM_FP64;
+    // isolation scan trimmed to a whole number of units per warp scheduler;
+    // NCPA_SCAN_TRIM=0 keeps every problem's own estimate
+    bool scan_trim = true;
     bool fuse_solve = true;        // fused bisection + eigenvector launch; NCPA_FUSE_SOLVE=0 turns it off
     // how long a consumer of the fused launch waits for an empty queue slot
     // before leaving the item to the following launch; NCPA_FUSE_WAIT_NS
@@ -549,6 +552,9 @@ void prepare_solve(ncpa_ctx* ctx, ncpa_modes* M, const ncpa_ess_params* prm, int
 
 // Window, Sturm scan, device-built work items, bisection and eigenvectors
 // over all problems of M, then copies of the item/mode totals, the problem
+// warp schedulers of the device for the scan trim (0: no trim)
+int scan_slots(const ncpa_ctx* ctx) { return ctx->scan_trim ? 4 * ctx->num_sms : 0; }
+
 // records and the device status word to tot_dst, info_dst and err_dst.  No
 // host synchronisation: the whole sequence can be captured in a CUDA graph.
 void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_params* prm, bool wkb, double* s,
@@ -563,7 +569,14 @@ void enqueue_solve(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_
                                           prm->c_min, prm->c_max, err));
     tm.mark("window");
     // ---- K3a scan ----
-    check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s, b.counts.as<int>(), err));
+    // the scan's units claimed per warp scheduler through the item scheduler's
+    // state (zeroed again below before the bisection uses it)
+    int* scan_sched = nullptr;
+    if (scan_slots(ctx) > 0) {
+        scan_sched = b.sched.as<int>();
+        CK(cudaMemsetAsync(scan_sched, 0, ncpa::kSchedInts * sizeof(int), st));
+    }
+    check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s, b.counts.as<int>(), err, scan_slots(ctx), scan_sched));
     tm.mark("scan");
     // fused bisection + eigenvectors (one launch, eigenvectors of finished
     // problems overlapping the others' bisection), unless per-phase timing or
@@ -687,7 +700,8 @@ void solve_core(ncpa_ctx* ctx, PhaseTimer& tm, ncpa_modes* M, const ncpa_ess_par
     // ---- K3a scan ----
     DevBuf counts;
     counts.alloc((size_t)P * ncpa::kScanMax * 4, st);
-    check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), counts.as<int>(), ctx->d_err.as<unsigned>()));
+    check_launch(ctx, ncpa::launch_scan(st, P, d_pinfo, s.as<double>(), counts.as<int>(), ctx->d_err.as<unsigned>(),
+                                        scan_slots(ctx)));
     tm.mark("scan");
     std::vector<int> hcounts((size_t)P * ncpa::kScanMax);
     CK(cudaMemcpyAsync(hcounts.data(), counts.p, hcounts.size() * 4, cudaMemcpyDeviceToHost, st));
@@ -1427,6 +1441,7 @@ ncpa_status ncpa_ctx_create(ncpa_ctx** out, const ncpa_ctx_opts* opts) {
         if (const char* mv = std::getenv("NCPA_MS_TUNE")) ctx->ms_tune = mv[0] != '0';
         if (const char* ov = std::getenv("NCPA_BISECT_ORDER")) ctx->bis_order = ov[0] != '0';
         if (const char* ev = std::getenv("NCPA_FUSE_EV_WORKERS")) ctx->fuse_ev_workers = ev[0] != '0';
+        if (const char* sv = std::getenv("NCPA_SCAN_TRIM")) ctx->scan_trim = sv[0] != '0';
         if (const char* tv2 = std::getenv("NCPA_TL2D_SUM"))
             ctx->tl2d_method = std::atoi(tv2) == NCPA_SUM_TC_GUARDED ? NCPA_SUM_TC_GUARDED : NCPA_SUM_FP64;
         if (const char* wv = std::getenv("NCPA_BISECT_WORKERS")) {
