@@ -143,3 +143,43 @@ def test_scheduler_with_more_problems_than_the_ranking_covers(analytic_profile):
     assert a[0][-1] > 4141
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+def test_scan_trim_keeps_counts_and_modes(analytic_profile):
+    """The isolation scan's batch-wide trim (whole units per warp scheduler,
+    claimed per scheduler) only changes the bisection's starting brackets:
+    on the 256-frequency job (1329 units trimmed to 1184) mode counts are
+    identical and the modes agree with the untrimmed scan's within the
+    bisection tolerance."""
+    import ncpa_gpu
+    import workloads
+
+    def solve(env):
+        old = {k: os.environ.get(k) for k in env}
+        os.environ.update(env)
+        try:
+            ctx = ncpa_gpu.Context(0)
+        finally:
+            for k, v in old.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        prof = ctx.load_profile(analytic_profile)
+        m = ctx.solve(prof, ncpa_gpu.default_params(nz_grid=20000, turnoff_wkb=1),
+                      workloads.broadband_freqs(256, 0.5), [90.0])
+        off, kr, ki, vs, vr, _ = m.all_modes()
+        out = (off.copy(), kr.copy(), ki.copy(), vs * vr)
+        m.close()
+        prof.close()
+        ctx.close()
+        return out
+
+    a = solve({})
+    b = solve({"NCPA_SCAN_TRIM": "0"})
+    assert np.array_equal(a[0], b[0]) and a[0][-1] > 30000
+    # the bisection stops within 1e-15 (units of h^2 A) of each eigenvalue from
+    # either set of brackets; the parity bound on k is 1e-9 relative
+    assert np.max(np.abs(a[1] - b[1]) / b[1]) < 1e-9
+    assert np.max(np.abs(a[2] - b[2]) / np.abs(b[2])) < 1e-6
+    assert np.max(np.abs(a[3] - b[3])) < 1e-6 * np.max(np.abs(b[3]))
