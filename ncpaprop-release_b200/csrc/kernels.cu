@@ -967,17 +967,16 @@ __device__ void warp_sweep_tw(const double* __restrict__ s, int nz, double p_ini
 
 // K3a-2: the isolation scan in units of kScanStep shifts, numbered over the
 // problems in order (problem p has n_scan_raw / kScanStep units, less the
-// trim below).  Warp w of the grid sweeps unit w (warp_sweep: the sequential
-// count, two shifts per lane) through its own ring; it finds its problem with
-// a warp-wide prefix sum of the units per problem, 32 problems at a time.
-// Every unit is the same work.  Trim: with slots > 0 (the device's warp
+// trim below).  A warp sweeps a unit (warp_sweep: the sequential count, two
+// shifts per lane) through its own ring; it finds the unit's problem with a
+// warp-wide prefix sum of the units per problem, 32 problems at a time.
+// Every unit is the same work; k_scan says which warp takes which unit.  Trim: with slots > 0 (the device's warp
 // schedulers) and U units in all, the batch drops U mod slots units when that
 // is at most a quarter of U, so each scheduler sweeps the same whole number of
 // units: one unit each from the first problems (in order) that keep at least
 // 1.75 shifts per estimated mode.  Every warp computes the same trim from the
 // raw sizes; the warp that sweeps a problem's first unit records the final
-// size in n_scan for the kernels that follow.  Warps past the last unit
-// return.
+// size in n_scan for the kernels that follow.
 __device__ __forceinline__ bool scan_trimmable(const ProblemInfo& q) {
     const int u = q.n_scan_raw / kScanStep;
     return u >= 2 && q.m_est >= 0.f && (float)((u - 1) * kScanStep) >= 1.75f * q.m_est;
@@ -989,7 +988,7 @@ __device__ __forceinline__ bool scan_trimmable(const ProblemInfo& q) {
 // the first warp to arrive takes items from the heavy end of the list and the
 // next workers - 1 from the light end, so a scheduler runs a heavy and a
 // light item side by side; later warps run no bisection (in the fused launch
-// they go straight to the eigenvector queue).  A worker first draws a ticket
+// they exit, or take eigenvector items when ev_workers_only is off).  A worker first draws a ticket
 // (n tickets for n items) and then an index from its end of the list: front
 // and back indices never meet, so every item runs exactly once.  Where the
 // CTAs land only decides the balance: the first warp on every scheduler is a
