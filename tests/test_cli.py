@@ -211,6 +211,28 @@ def test_modess_2d_and_starter(modess_single):
 
 
 @pytest.mark.gpu
+def test_modess_2d_tloss_on_tensor_cores(modess_single, binaries, analytic_profile, tmp_path):
+    """Modess --write_2d_tloss with NCPA_TL2D_SUM=3 writes tloss_2d.nm from the
+    guarded tcgen05 modal sum: the same layout as the FP64 file and TL within
+    0.05 dB of it wherever TL > -140 dB."""
+    d, _, _ = modess_single
+    args = ["--singleprop", "--atmosfile", analytic_profile, "--freq", "0.1", "--azimuth", "90",
+            "--Nz_grid", str(NZ), "--maxrange_km", "500", "--Nrng_steps", "250", "--write_2d_tloss",
+            "--filetag", "tc"]
+    p = subprocess.run([os.path.join(binaries, "Modess")] + args, cwd=tmp_path, capture_output=True, text=True,
+                       timeout=600, env=dict(os.environ, NCPA_TL2D_SUM="3"))
+    assert p.returncode == 0, p.stdout + p.stderr
+    ref = np.loadtxt(d / "run.tloss_2d.nm")
+    got = np.loadtxt(tmp_path / "tc.tloss_2d.nm")
+    assert got.shape == ref.shape
+    assert np.array_equal(got[:, :2], ref[:, :2])
+    tl_ref, tl_got = _tl_db(ref[:, 2], ref[:, 3]), _tl_db(got[:, 2], got[:, 3])
+    sel = tl_ref > -140.0
+    assert sel.mean() > 0.5
+    assert np.max(np.abs(tl_got[sel] - tl_ref[sel])) < 0.05
+
+
+@pytest.mark.gpu
 def test_modess_atm_profile(modess_single, analytic_profile):
     from oracle import oracle as O
 
